@@ -1,0 +1,185 @@
+/*
+ * ipglasma_b200 -- C ABI of the B200 implementation of IP-Glasma's per-event
+ * hot path: colour-charge sampling -> Poisson solve -> Wilson lines -> tau=0
+ * Newton link solve -> boost-invariant leapfrog -> T^{mu nu} and Landau
+ * matching.
+ *
+ * The reference has no plugin or FFI layer; its hot path is entered through
+ * two calls in the event loop (main.cpp:347-359):
+ *     init.init(&lat, &group, param, random, &glauber, READFROMFILE);
+ *     evolution.run(&lat, &group, param);
+ * with all state in a Lattice of heap Cells (Lattice.h, Cell.h) and every
+ * error ending the process (exit(1)). The entry points below replace those
+ * two calls and the Cell getters their callers use; each cites what it
+ * replaces.
+ *
+ * Conventions
+ *   - Opaque context, one CUDA stream per context; a context is not
+ *     re-entrant, separate contexts may be driven from separate host threads.
+ *   - The caller owns host buffers, the library owns device memory.
+ *   - Lattice site index pos = ix * N + iy (Lattice.cpp:15-28).
+ *   - 3x3 matrices cross the ABI as 9 complex numbers, row-major, (re, im)
+ *     pairs: 18 doubles per site, sites in pos order.
+ *   - Lattice units as in the reference: g2mu2 is g^2 mu^2 a^2, tau and dtau
+ *     are in units of a.
+ *   - Every function returns an ipg_status; nothing calls exit().
+ */
+#ifndef IPGLASMA_B200_H
+#define IPGLASMA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    IPG_OK = 0,
+    IPG_ERR_BAD_CONFIG = 1,        /* invalid configuration or argument */
+    IPG_ERR_CUDA = 2,              /* CUDA runtime error (message kept) */
+    IPG_ERR_NEWTON_NONCONVERGED = 3, /* some tau=0 links used their best estimate */
+    IPG_ERR_NAN = 4,               /* NaN/Inf detected in the fields */
+    IPG_ERR_STATE = 5,             /* call out of order */
+    IPG_ERR_NOMEM = 6,             /* device allocation failed */
+    IPG_ERR_TIMEOUT = 7            /* a device wait hit its limit */
+} ipg_status;
+
+typedef enum {
+    IPG_FP64 = 0, /* plain form: FP64 everywhere, no reunitarisation */
+    IPG_FP32 = 1  /* bulk form: FP32 leapfrog with per-step reunitarisation,
+                     FP64 initial conditions, observables and reductions */
+} ipg_precision;
+
+typedef struct ipg_ctx ipg_ctx;
+
+/* Per-event configuration; the keys of the reference input file that the
+ * hot path reads (main.cpp:448-578). */
+typedef struct {
+    int size;          /* N, sites per side: power of two, 8 <= N <= 4096 */
+    int Nc;            /* colours, must be 3 */
+    int Ny;            /* longitudinal sheets per nucleus */
+    double L;          /* transverse box, fm */
+    double g;          /* coupling */
+    double m;          /* IR regulator, GeV */
+    double UVdamp;     /* UV damping, GeV^-1 */
+    double maxtime;    /* final proper time, fm */
+    double dtau;       /* lattice units; <= 0 derives it like main.cpp:531-534 */
+    int precision;     /* ipg_precision */
+    int newton_max_iterations; /* 0 -> 2000 (Init.cpp:3345) */
+    int newton_max_restarts;   /* 0 -> 200  (Init.cpp:3346) */
+    uint64_t seed;     /* key of the device random streams (noise, restarts) */
+    int device;        /* CUDA device ordinal */
+} ipg_config;
+
+/* Summary of the initial-condition stage. */
+typedef struct {
+    int newton_links;         /* 2 N^2 */
+    int newton_restarted;     /* links that drew a random restart */
+    int newton_failed;        /* links left at their best estimate */
+    int newton_max_iterations;
+    double newton_mean_iterations;
+    double ms_wilson;         /* rho -> V_A, V_B */
+    double ms_newton;         /* link products + Newton */
+    double ms_fields;         /* initial pi */
+} ipg_init_report;
+
+/* Scalars of a finished event. */
+typedef struct {
+    int itmax;                /* leapfrog steps (Evolution.cpp:396) */
+    double dtau;              /* lattice units */
+    double tau_final;         /* fm, it*dtau*a at the observables */
+    double gauss_violation;   /* Evolution.cpp:295-364 */
+    double unitarity_max;     /* max |U^dag U - 1| over links, entrywise */
+    double sum_Ttautau;       /* sum over cells of T^tautau (fm^-4) */
+    double sum_eps;           /* sum over cells of e (fm^-4) */
+    double E_T;               /* tau a^2 hbarc sum T^tautau, GeV */
+    double eccentricity[6];   /* epsilon_1 .. epsilon_6 (Evolution.cpp:1660-1672) */
+    double psi[6];            /* Psi_1 .. Psi_6 */
+    int cells_without_u;      /* cells with no time-like eigenvector */
+    double ms_evolution;
+    double ms_observables;
+} ipg_result;
+
+/* Error text of the last failing call on ctx (never NULL). */
+const char *ipg_last_error(const ipg_ctx *ctx);
+
+/* Replaces the per-event construction of Parameters, Lattice, Init and
+ * Evolution (main.cpp:66-336) and the derived time step (main.cpp:531-534). */
+ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out);
+ipg_status ipg_destroy(ipg_ctx *ctx);
+
+/* Effective dtau (lattice units) and leapfrog step count of ctx. */
+ipg_status ipg_time_grid(const ipg_ctx *ctx, double *dtau, int *itmax);
+
+/* g^2 mu^2 maps of both nuclei, lattice units, [N*N] host arrays; replaces
+ * Cell::setg2mu2A/B as filled by Init::setColorChargeDensity
+ * (Init.cpp:753-1676). */
+ipg_status ipg_set_g2mu(ipg_ctx *ctx, const double *g2mu2A,
+                        const double *g2mu2B);
+/* same, device pointers (no host copy) */
+ipg_status ipg_set_g2mu_device(ipg_ctx *ctx, const double *d_g2mu2A,
+                               const double *d_g2mu2B);
+
+/* Unit Gaussian noise xi[k][pos][a] (k < Ny, a < 8) of both nuclei in the
+ * draw order of Init::setV, so rho = g sqrt(g2mu2/Ny) xi reproduces
+ * Init.cpp:1695-1705 and 1773-1783. Host arrays of Ny*N*N*8 doubles. */
+ipg_status ipg_set_noise(ipg_ctx *ctx, const double *xiA, const double *xiB);
+/* same, device pointers; they must stay valid until ipg_init_fields returns */
+ipg_status ipg_set_noise_device(ipg_ctx *ctx, const double *d_xiA,
+                                const double *d_xiB);
+/* Draw the noise on the device (Philox4x32-10 keyed by cfg.seed) instead of
+ * reading it; replaces the serial Random::Gauss stream (Random.cpp:178-204). */
+ipg_status ipg_use_device_noise(ipg_ctx *ctx);
+
+/* Wilson lines, tau=0 Newton link solve and initial fields; replaces
+ * Init::setV (Init.cpp:1678-1849) and the tau=0 block of Init::init
+ * (Init.cpp:2437-2691). report may be NULL. Returns
+ * IPG_ERR_NEWTON_NONCONVERGED (fields still set) if any link failed. */
+ipg_status ipg_init_fields(ipg_ctx *ctx, ipg_init_report *report);
+
+/* The whole schedule of Evolution::run (Evolution.cpp:366-657): tau=0 half
+ * step, itmax-1 full steps, T^{mu nu} + Landau matching at it = itmax
+ * before the final half step of pi and E, then Gauss law and
+ * eccentricities. result may be NULL. */
+ipg_status ipg_run(ipg_ctx *ctx, ipg_result *result);
+
+/* Leapfrog only: the tau=0 half step (evolvePhi/evolveU at tau=0,
+ * Evolution.cpp:393-394) when the context is fresh from ipg_init_fields,
+ * then `steps` full steps it = 1..steps (Evolution.cpp:416-421). */
+ipg_status ipg_evolve(ipg_ctx *ctx, int steps);
+
+/* Per-cell observables after ipg_run, [N*N] (eps, fm^-4) and component-major
+ * [k][N*N] arrays: u4 = (u^tau, u^x, u^y, u^eta); pi10 and T10 in the order
+ * tautau xx yy etaeta taux tauy taueta xy xeta yeta (Cell.h getters,
+ * MyEigen.cpp:259-305, Evolution.cpp:759-1238). Any pointer may be NULL. */
+ipg_status ipg_get_observables(ipg_ctx *ctx, double *eps, double *u4,
+                               double *pi10, double *T10);
+
+/* Field access for stage-wise checks; which = IPG_UX, IPG_UY, IPG_E1, IPG_E2,
+ * IPG_PHI, IPG_PI, IPG_VA, IPG_VB: N*N*18 doubles (Cell::getUx ...,
+ * Cell.h:141-166). ipg_set_field loads a state, e.g. a tau=0 state written
+ * by the reference. */
+enum { IPG_UX = 0, IPG_UY, IPG_E1, IPG_E2, IPG_PHI, IPG_PI, IPG_VA, IPG_VB };
+ipg_status ipg_get_field(ipg_ctx *ctx, int which, double *out);
+ipg_status ipg_set_field(ipg_ctx *ctx, int which, const double *in);
+
+/* Mark a state loaded with ipg_set_field as the tau=0 state (as if
+ * ipg_init_fields had run). */
+ipg_status ipg_mark_initialized(ipg_ctx *ctx);
+
+/* Newton iteration counts [2*N*N] (link 2*pos + dir) after ipg_init_fields. */
+ipg_status ipg_get_newton_iterations(ipg_ctx *ctx, int *iters, int *status);
+
+/* Device time of the last leapfrog launch sequence run by ipg_evolve or
+ * ipg_run, and the number of leapfrog launches it contained. */
+ipg_status ipg_last_leapfrog_ms(ipg_ctx *ctx, double *ms, int *launches);
+
+/* Number of kernels this library launched on ctx since creation. */
+ipg_status ipg_kernel_launches(const ipg_ctx *ctx, long long *count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

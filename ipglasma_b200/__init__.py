@@ -1,0 +1,310 @@
+"""B200 implementation of IP-Glasma's per-event hot path.
+
+Python host mirror of the C ABI in ``include/ipglasma_b200.h``. The reference
+drives an event with two calls (main.cpp:347-359)::
+
+    init.init(&lat, &group, param, random, &glauber, READFROMFILE)
+    evolution.run(&lat, &group, param)
+
+Here the same event is::
+
+    ev = Event(Config(size=256, L=30.0, Ny=50, g=2.0, m=0.2, maxtime=0.4))
+    ev.set_g2mu(g2mu2A, g2mu2B)          # Cell::setg2mu2A/B
+    ev.use_device_noise()                # or ev.set_noise(xiA, xiB)
+    report = ev.init_fields()            # Init::setV + tau=0 block
+    result = ev.run()                    # Evolution::run
+    eps, u, pi, T = ev.observables()     # Cell getters
+
+All compute runs in ``libipglasma_b200.so`` (hand-written sm_100a kernels);
+this module only marshals host arrays. If the library is missing the import
+of :func:`lib` raises; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+__all__ = ["Config", "Event", "IPGError", "lib", "FP64", "FP32",
+           "UX", "UY", "E1", "E2", "PHI", "PI", "VA", "VB", "HBARC"]
+
+HBARC = 0.1973269718  # GeV fm, Phys_consts.h
+FP64, FP32 = 0, 1
+UX, UY, E1, E2, PHI, PI, VA, VB = range(8)
+
+_STATUS = {
+    0: "IPG_OK", 1: "IPG_ERR_BAD_CONFIG", 2: "IPG_ERR_CUDA",
+    3: "IPG_ERR_NEWTON_NONCONVERGED", 4: "IPG_ERR_NAN", 5: "IPG_ERR_STATE",
+    6: "IPG_ERR_NOMEM", 7: "IPG_ERR_TIMEOUT",
+}
+
+LIB_PATH = Path(__file__).resolve().parent / "libipglasma_b200.so"
+
+
+class IPGError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{_STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class _Config(ct.Structure):
+    _fields_ = [
+        ("size", ct.c_int), ("Nc", ct.c_int), ("Ny", ct.c_int),
+        ("L", ct.c_double), ("g", ct.c_double), ("m", ct.c_double),
+        ("UVdamp", ct.c_double), ("maxtime", ct.c_double), ("dtau", ct.c_double),
+        ("precision", ct.c_int), ("newton_max_iterations", ct.c_int),
+        ("newton_max_restarts", ct.c_int), ("seed", ct.c_uint64),
+        ("device", ct.c_int),
+    ]
+
+
+class _InitReport(ct.Structure):
+    _fields_ = [
+        ("newton_links", ct.c_int), ("newton_restarted", ct.c_int),
+        ("newton_failed", ct.c_int), ("newton_max_iterations", ct.c_int),
+        ("newton_mean_iterations", ct.c_double), ("ms_wilson", ct.c_double),
+        ("ms_newton", ct.c_double), ("ms_fields", ct.c_double),
+    ]
+
+
+class _Result(ct.Structure):
+    _fields_ = [
+        ("itmax", ct.c_int), ("dtau", ct.c_double), ("tau_final", ct.c_double),
+        ("gauss_violation", ct.c_double), ("unitarity_max", ct.c_double),
+        ("sum_Ttautau", ct.c_double), ("sum_eps", ct.c_double),
+        ("E_T", ct.c_double), ("eccentricity", ct.c_double * 6),
+        ("psi", ct.c_double * 6), ("cells_without_u", ct.c_int),
+        ("ms_evolution", ct.c_double), ("ms_observables", ct.c_double),
+    ]
+
+
+_lib = None
+
+_SIGNATURES = {
+    "ipg_last_error": (ct.c_char_p, [ct.c_void_p]),
+    "ipg_create": (ct.c_int, [ct.POINTER(_Config), ct.POINTER(ct.c_void_p)]),
+    "ipg_destroy": (ct.c_int, [ct.c_void_p]),
+    "ipg_time_grid": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double), ct.POINTER(ct.c_int)]),
+    "ipg_set_g2mu": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "ipg_set_g2mu_device": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "ipg_set_noise": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "ipg_set_noise_device": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "ipg_use_device_noise": (ct.c_int, [ct.c_void_p]),
+    "ipg_init_fields": (ct.c_int, [ct.c_void_p, ct.POINTER(_InitReport)]),
+    "ipg_run": (ct.c_int, [ct.c_void_p, ct.POINTER(_Result)]),
+    "ipg_evolve": (ct.c_int, [ct.c_void_p, ct.c_int]),
+    "ipg_get_observables": (ct.c_int, [ct.c_void_p] + [ct.c_void_p] * 4),
+    "ipg_get_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p]),
+    "ipg_set_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p]),
+    "ipg_mark_initialized": (ct.c_int, [ct.c_void_p]),
+    "ipg_get_newton_iterations": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "ipg_last_leapfrog_ms": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double), ct.POINTER(ct.c_int)]),
+    "ipg_kernel_launches": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_longlong)]),
+}
+
+
+def lib() -> ct.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m ipglasma_b200.build`")
+        handle = ct.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def _ptr(a: np.ndarray) -> ct.c_void_p:
+    return ct.c_void_p(a.ctypes.data)
+
+
+def _f64(a, n: int | None = None) -> np.ndarray:
+    arr = np.ascontiguousarray(a, dtype=np.float64)
+    if n is not None and arr.size != n:
+        raise ValueError(f"expected {n} values, got {arr.size}")
+    return arr
+
+
+@dataclass
+class Config:
+    """Per-event configuration (the hot-path keys of the reference input)."""
+    size: int = 64
+    L: float = 8.0
+    Ny: int = 50
+    g: float = 2.0
+    m: float = 0.2
+    UVdamp: float = 0.0
+    maxtime: float = 0.4
+    dtau: float = 0.0
+    precision: int = FP64
+    newton_max_iterations: int = 2000
+    newton_max_restarts: int = 200
+    seed: int = 1
+    device: int = 0
+    Nc: int = 3
+
+    def to_c(self) -> _Config:
+        return _Config(self.size, self.Nc, self.Ny, self.L, self.g, self.m,
+                       self.UVdamp, self.maxtime, self.dtau, self.precision,
+                       self.newton_max_iterations, self.newton_max_restarts,
+                       self.seed, self.device)
+
+
+@dataclass
+class InitReport:
+    newton_links: int
+    newton_restarted: int
+    newton_failed: int
+    newton_max_iterations: int
+    newton_mean_iterations: float
+    ms_wilson: float
+    ms_newton: float
+    ms_fields: float
+
+
+@dataclass
+class Result:
+    itmax: int
+    dtau: float
+    tau_final: float
+    gauss_violation: float
+    unitarity_max: float
+    sum_Ttautau: float
+    sum_eps: float
+    E_T: float
+    eccentricity: list = field(default_factory=list)
+    psi: list = field(default_factory=list)
+    cells_without_u: int = 0
+    ms_evolution: float = 0.0
+    ms_observables: float = 0.0
+
+
+class Event:
+    """One event on one GPU (an ``ipg_ctx``)."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        self._lib = lib()
+        h = ct.c_void_p()
+        c = cfg.to_c()
+        st = self._lib.ipg_create(ct.byref(c), ct.byref(h))
+        self._h = h
+        if st != 0:
+            msg = self._lib.ipg_last_error(h).decode() if h.value else "ipg_create failed"
+            if h.value:
+                self._lib.ipg_destroy(h)
+            self._h = ct.c_void_p()
+            raise IPGError(st, msg)
+        self.N = cfg.size
+        self.n = cfg.size * cfg.size
+        d, it = ct.c_double(), ct.c_int()
+        self._check(self._lib.ipg_time_grid(self._h, ct.byref(d), ct.byref(it)))
+        self.dtau, self.itmax = d.value, it.value
+
+    # -- plumbing -----------------------------------------------------------
+    def _check(self, st: int, allow: tuple = ()) -> int:
+        if st != 0 and st not in allow:
+            raise IPGError(st, self._lib.ipg_last_error(self._h).decode())
+        return st
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.ipg_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- inputs ---------------------------------------------------------------
+    def set_g2mu(self, g2mu2A, g2mu2B) -> None:
+        a, b = _f64(g2mu2A, self.n), _f64(g2mu2B, self.n)
+        self._check(self._lib.ipg_set_g2mu(self._h, _ptr(a), _ptr(b)))
+
+    def set_g2mu_device(self, ptr_a: int, ptr_b: int) -> None:
+        self._check(self._lib.ipg_set_g2mu_device(self._h, ct.c_void_p(ptr_a),
+                                                  ct.c_void_p(ptr_b)))
+
+    def set_noise(self, xiA, xiB) -> None:
+        cnt = self.cfg.Ny * self.n * 8
+        a, b = _f64(xiA, cnt), _f64(xiB, cnt)
+        self._check(self._lib.ipg_set_noise(self._h, _ptr(a), _ptr(b)))
+
+    def set_noise_device(self, ptr_a: int, ptr_b: int) -> None:
+        self._check(self._lib.ipg_set_noise_device(self._h, ct.c_void_p(ptr_a),
+                                                   ct.c_void_p(ptr_b)))
+
+    def use_device_noise(self) -> None:
+        self._check(self._lib.ipg_use_device_noise(self._h))
+
+    # -- stages ---------------------------------------------------------------
+    def init_fields(self, allow_nonconverged: bool = False) -> InitReport:
+        rep = _InitReport()
+        allow = (3,) if allow_nonconverged else ()
+        self._check(self._lib.ipg_init_fields(self._h, ct.byref(rep)), allow)
+        return InitReport(*(getattr(rep, f) for f, _ in _InitReport._fields_))
+
+    def run(self) -> Result:
+        res = _Result()
+        self._check(self._lib.ipg_run(self._h, ct.byref(res)))
+        vals = {f: getattr(res, f) for f, _ in _Result._fields_}
+        vals["eccentricity"] = list(res.eccentricity)
+        vals["psi"] = list(res.psi)
+        return Result(**vals)
+
+    def evolve(self, steps: int) -> None:
+        self._check(self._lib.ipg_evolve(self._h, steps))
+
+    # -- outputs --------------------------------------------------------------
+    def observables(self):
+        n = self.n
+        eps = np.empty(n)
+        u4 = np.empty((4, n))
+        pi10 = np.empty((10, n))
+        T10 = np.empty((10, n))
+        self._check(self._lib.ipg_get_observables(self._h, _ptr(eps), _ptr(u4),
+                                                  _ptr(pi10), _ptr(T10)))
+        return eps, u4, pi10, T10
+
+    def get_field(self, which: int) -> np.ndarray:
+        out = np.empty((self.n, 9), dtype=np.complex128)
+        self._check(self._lib.ipg_get_field(self._h, which, _ptr(out)))
+        return out.reshape(self.n, 3, 3)
+
+    def set_field(self, which: int, mats) -> None:
+        arr = np.ascontiguousarray(np.asarray(mats, dtype=np.complex128).reshape(self.n, 9))
+        self._check(self._lib.ipg_set_field(self._h, which, _ptr(arr)))
+
+    def mark_initialized(self) -> None:
+        self._check(self._lib.ipg_mark_initialized(self._h))
+
+    def newton_iterations(self):
+        it = np.empty(2 * self.n, dtype=np.int32)
+        st = np.empty(2 * self.n, dtype=np.int32)
+        self._check(self._lib.ipg_get_newton_iterations(self._h, _ptr(it), _ptr(st)))
+        return it, st
+
+    def last_leapfrog_ms(self):
+        ms, k = ct.c_double(), ct.c_int()
+        self._check(self._lib.ipg_last_leapfrog_ms(self._h, ct.byref(ms), ct.byref(k)))
+        return ms.value, k.value
+
+    def kernel_launches(self) -> int:
+        c = ct.c_longlong()
+        self._check(self._lib.ipg_kernel_launches(self._h, ct.byref(c)))
+        return c.value

@@ -1,0 +1,810 @@
+// C ABI (include/ipglasma_b200.h): context, buffers, schedule.
+//
+// One context is one event of one lattice size. Device memory per event is
+// allocated once at ipg_create and reused by every call; nothing on the hot
+// path allocates.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/ipglasma_b200.h"
+#include "ipg_internal.h"
+
+using namespace ipg;
+
+namespace {
+constexpr double kHbarc = 0.1973269718;  // GeV fm (Phys_consts.h)
+}
+
+struct ipg_ctx {
+    ipg_config cfg{};
+    int N = 0, logN = 0;
+    size_t n = 0;
+    double a = 0, dtau = 0, m_lat = 0, uv_lat = 0;
+    int itmax = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::string err;
+    long long launches = 0;
+
+    // inputs
+    double *g2mu2A = nullptr, *g2mu2B = nullptr;
+    double *xiA_own = nullptr, *xiB_own = nullptr;
+    const double *xiA = nullptr, *xiB = nullptr;
+    bool have_g2mu = false, have_noise = false, device_noise = false;
+
+    // initial-condition scratch
+    double2 *twiddle = nullptr;
+    double *green = nullptr;
+    double2 *work = nullptr;
+    int work_sheets = 0;
+    C<double> *VA = nullptr, *VB = nullptr;
+    C<double> *u1x = nullptr, *u2x = nullptr, *u1y = nullptr, *u2y = nullptr;
+    int *newton_iters = nullptr, *newton_status = nullptr;
+
+    // fields: FP64 state (+ second U/phi buffer), FP32 state (+ second buffer)
+    State<double> s64{};
+    C<double> *ux64b = nullptr, *uy64b = nullptr;
+    double *phi64b = nullptr;
+    State<float> s32{};
+    C<float> *ux32b = nullptr, *uy32b = nullptr;
+    float *phi32b = nullptr;
+
+    // observables
+    double *T10 = nullptr, *eps = nullptr, *u4 = nullptr, *pi10 = nullptr;
+    double *carry = nullptr;
+    int *wrote = nullptr, *found = nullptr;
+    double *partial = nullptr, *scal = nullptr;
+    EventGeom *d_ev = nullptr;
+
+    bool initialized = false, half_done = false, finished = false;
+    int it = 0;  // completed full steps
+    double last_leapfrog_ms = 0;
+    int last_leapfrog_launches = 0;
+
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+ipg_status fail(ipg_ctx *c, ipg_status st, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return st;
+}
+
+ipg_status cuda_check(ipg_ctx *c, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return IPG_OK;
+    return fail(c, IPG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define IPG_CUDA(c, expr)                                        \
+    do {                                                         \
+        ipg_status _s = cuda_check((c), (expr), #expr);          \
+        if (_s != IPG_OK) return _s;                             \
+    } while (0)
+
+#define IPG_LAUNCHED(c, k)                                                 \
+    do {                                                                   \
+        (c)->launches += (k);                                              \
+        ipg_status _s = cuda_check((c), cudaGetLastError(), "kernel launch"); \
+        if (_s != IPG_OK) return _s;                                       \
+    } while (0)
+
+template <typename P>
+ipg_status dalloc(ipg_ctx *c, P **p, size_t count) {
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, count * sizeof(P));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, IPG_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s",
+                    count * sizeof(P), cudaGetErrorString(e));
+    }
+    c->allocs.push_back(q);
+    *p = reinterpret_cast<P *>(q);
+    return IPG_OK;
+}
+
+#define IPG_TRY(expr)                    \
+    do {                                 \
+        ipg_status _s = (expr);          \
+        if (_s != IPG_OK) return _s;     \
+    } while (0)
+
+__global__ void k_identity(size_t n, C<double> *V) {
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+#pragma unroll
+    for (int k = 0; k < 9; k++)
+        V[k * n + pos] = {(k == 0 || k == 4 || k == 8) ? 1. : 0., 0.};
+}
+
+__global__ void k_count_nan(size_t n, const double *x, int *count) {
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    if (!isfinite(x[pos])) atomicAdd(count, 1);
+}
+
+int ilog2(int v) {
+    int l = 0;
+    while ((1 << l) < v) l++;
+    return l;
+}
+
+ipg_status alloc_state64(ipg_ctx *c, State<double> &s) {
+    const size_t n = c->n;
+    IPG_TRY(dalloc(c, &s.ux, 9 * n));
+    IPG_TRY(dalloc(c, &s.uy, 9 * n));
+    IPG_TRY(dalloc(c, &s.e1, 8 * n));
+    IPG_TRY(dalloc(c, &s.e2, 8 * n));
+    IPG_TRY(dalloc(c, &s.phi, 9 * n));
+    IPG_TRY(dalloc(c, &s.pi, 9 * n));
+    return IPG_OK;
+}
+
+ipg_status alloc_state32(ipg_ctx *c, State<float> &s) {
+    const size_t n = c->n;
+    IPG_TRY(dalloc(c, &s.ux, 9 * n));
+    IPG_TRY(dalloc(c, &s.uy, 9 * n));
+    IPG_TRY(dalloc(c, &s.e1, 8 * n));
+    IPG_TRY(dalloc(c, &s.e2, 8 * n));
+    IPG_TRY(dalloc(c, &s.phi, 9 * n));
+    IPG_TRY(dalloc(c, &s.pi, 9 * n));
+    return IPG_OK;
+}
+
+bool is_fp32(const ipg_ctx *c) { return c->cfg.precision == IPG_FP32; }
+
+// one leapfrog launch on the active precision, then swap the U/phi buffers
+template <typename T>
+ipg_status step_impl(ipg_ctx *c, State<T> &s, C<T> *&uxb, C<T> *&uyb,
+                     T *&phib, double tau, double dt_pe, double dt_pu,
+                     int do_pe, int do_pu, bool reunit) {
+    StepCoef<T> cf;
+    cf.tau = (T)tau;
+    cf.dt_pe = (T)dt_pe;
+    cf.dt_pu = (T)dt_pu;
+    cf.g = (T)c->cfg.g;
+    cf.do_pe = do_pe;
+    cf.do_pu = do_pu;
+    launch_leapfrog<T>(c->d_ev, c->N, s, uxb, uyb, phib, cf, reunit, c->stream);
+    IPG_LAUNCHED(c, 1);
+    if (do_pu) {
+        std::swap(s.ux, uxb);
+        std::swap(s.uy, uyb);
+        std::swap(s.phi, phib);
+    }
+    return IPG_OK;
+}
+
+ipg_status step(ipg_ctx *c, double tau, double dt_pe, double dt_pu, int do_pe,
+                int do_pu) {
+    if (is_fp32(c))
+        return step_impl<float>(c, c->s32, c->ux32b, c->uy32b, c->phi32b, tau,
+                                dt_pe, dt_pu, do_pe, do_pu, true);
+    return step_impl<double>(c, c->s64, c->ux64b, c->uy64b, c->phi64b, tau,
+                             dt_pe, dt_pu, do_pe, do_pu, false);
+}
+
+ipg_status sync(ipg_ctx *c) {
+    IPG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return IPG_OK;
+}
+
+float elapsed(ipg_ctx *c) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    return ms;
+}
+
+// host layout helpers: per-site 3x3 (18 doubles) <-> device planes
+void planes_to_sites_m3(const std::vector<double> &pl, size_t n, double *out) {
+    // pl: [9][n] complex = 18 n doubles, interleaved per component
+    for (size_t p = 0; p < n; p++)
+        for (int k = 0; k < 9; k++) {
+            out[18 * p + 2 * k] = pl[2 * (k * n + p)];
+            out[18 * p + 2 * k + 1] = pl[2 * (k * n + p) + 1];
+        }
+}
+
+void herm_to_sites(const std::vector<double> &pl, size_t n, bool traceless,
+                   double *out) {
+    for (size_t p = 0; p < n; p++) {
+        double d0, d1, d2, o[6];
+        if (traceless) {
+            d0 = pl[0 * n + p];
+            d1 = pl[1 * n + p];
+            d2 = -(d0 + d1);
+            for (int q = 0; q < 6; q++) o[q] = pl[(2 + q) * n + p];
+        } else {
+            d0 = pl[0 * n + p];
+            d1 = pl[1 * n + p];
+            d2 = pl[2 * n + p];
+            for (int q = 0; q < 6; q++) o[q] = pl[(3 + q) * n + p];
+        }
+        double *m = out + 18 * p;
+        const double v[18] = {d0,   0.,    o[0], o[1],  o[2], o[3],
+                              o[0], -o[1], d1,   0.,    o[4], o[5],
+                              o[2], -o[3], o[4], -o[5], d2,   0.};
+        std::memcpy(m, v, sizeof(v));
+    }
+}
+
+void sites_to_herm(const double *in, size_t n, bool traceless,
+                   std::vector<double> &pl) {
+    pl.assign((traceless ? 8 : 9) * n, 0.);
+    for (size_t p = 0; p < n; p++) {
+        const double *m = in + 18 * p;
+        const double d0 = m[0], d1 = m[8], d2 = m[16];
+        const double o[6] = {m[2], m[3], m[4], m[5], m[10], m[11]};
+        if (traceless) {
+            const double t = (d0 + d1 + d2) / 3.;
+            pl[0 * n + p] = d0 - t;
+            pl[1 * n + p] = d1 - t;
+            for (int q = 0; q < 6; q++) pl[(2 + q) * n + p] = o[q];
+        } else {
+            pl[0 * n + p] = d0;
+            pl[1 * n + p] = d1;
+            pl[2 * n + p] = d2;
+            for (int q = 0; q < 6; q++) pl[(3 + q) * n + p] = o[q];
+        }
+    }
+}
+
+ipg_status to_fp32_if_needed(ipg_ctx *c) {
+    if (!is_fp32(c)) return IPG_OK;
+    launch_convert_state_down<float>(c->n, c->s64, c->s32, c->stream);
+    IPG_LAUNCHED(c, 1);
+    return IPG_OK;
+}
+
+// make c->s64 hold the current state (converts from FP32 when needed)
+ipg_status state64(ipg_ctx *c) {
+    if (!is_fp32(c)) return IPG_OK;
+    launch_convert_state<float>(c->n, c->s32, c->s64, c->stream);
+    IPG_LAUNCHED(c, 1);
+    return IPG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *ipg_last_error(const ipg_ctx *ctx) {
+    return ctx ? ctx->err.c_str() : "null context";
+}
+
+ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
+    if (!cfg || !out) return IPG_ERR_BAD_CONFIG;
+    *out = nullptr;
+    ipg_ctx *c = new (std::nothrow) ipg_ctx();
+    if (!c) return IPG_ERR_NOMEM;
+    c->cfg = *cfg;
+    const int N = cfg->size;
+    auto bad = [&](const char *msg) {
+        c->err = msg;
+        *out = c;  // caller can read the message, then destroy
+        return IPG_ERR_BAD_CONFIG;
+    };
+    if (N < 8 || N > 2048 || (N & (N - 1)) != 0)
+        return bad("size must be a power of two in [8, 2048]");
+    if (cfg->Nc != 3) return bad("only SU(3) (Nc = 3) is supported");
+    if (cfg->Ny < 1) return bad("Ny must be >= 1");
+    if (!(cfg->L > 0) || !(cfg->g > 0) || !(cfg->maxtime > 0) || cfg->m < 0 ||
+        cfg->UVdamp < 0)
+        return bad("L, g, maxtime must be > 0 and m, UVdamp >= 0");
+    if (cfg->precision != IPG_FP64 && cfg->precision != IPG_FP32)
+        return bad("precision must be IPG_FP64 or IPG_FP32");
+    if (c->cfg.newton_max_iterations <= 0) c->cfg.newton_max_iterations = 2000;
+    if (c->cfg.newton_max_restarts <= 0) c->cfg.newton_max_restarts = 200;
+    c->N = N;
+    c->logN = ilog2(N);
+    c->n = (size_t)N * N;
+    c->a = cfg->L / N;
+    if (cfg->dtau > 0) {
+        c->dtau = cfg->dtau;
+    } else {
+        const int steps = static_cast<int>(10 * cfg->maxtime / c->a) + 1;
+        c->dtau = cfg->maxtime / (steps * c->a);
+    }
+    c->itmax = static_cast<int>(cfg->maxtime / (c->a * c->dtau) + 0.1);
+    if (c->itmax < 1) return bad("maxtime shorter than one time step");
+    c->m_lat = cfg->m * c->a / kHbarc;
+    c->uv_lat = cfg->UVdamp / c->a * kHbarc;
+    *out = c;
+
+    IPG_CUDA(c, cudaSetDevice(cfg->device));
+    IPG_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    IPG_CUDA(c, cudaEventCreate(&c->ev0));
+    IPG_CUDA(c, cudaEventCreate(&c->ev1));
+
+    const size_t n = c->n;
+    IPG_TRY(dalloc(c, &c->g2mu2A, n));
+    IPG_TRY(dalloc(c, &c->g2mu2B, n));
+    IPG_TRY(dalloc(c, &c->twiddle, (size_t)N / 2));
+    IPG_TRY(dalloc(c, &c->green, n));
+    // work buffer of a sheet batch: ~64 MB so it stays in L2
+    const size_t per_sheet = 4 * n * sizeof(double2);
+    c->work_sheets = (int)std::max<size_t>(1, (64ull << 20) / per_sheet);
+    c->work_sheets = std::min(c->work_sheets, cfg->Ny);
+    IPG_TRY(dalloc(c, &c->work, (size_t)c->work_sheets * 4 * n));
+    IPG_TRY(dalloc(c, &c->VA, 9 * n));
+    IPG_TRY(dalloc(c, &c->VB, 9 * n));
+    IPG_TRY(dalloc(c, &c->u1x, 9 * n));
+    IPG_TRY(dalloc(c, &c->u2x, 9 * n));
+    IPG_TRY(dalloc(c, &c->u1y, 9 * n));
+    IPG_TRY(dalloc(c, &c->u2y, 9 * n));
+    IPG_TRY(dalloc(c, &c->newton_iters, 2 * n));
+    IPG_TRY(dalloc(c, &c->newton_status, 2 * n));
+    IPG_TRY(alloc_state64(c, c->s64));
+    IPG_TRY(dalloc(c, &c->ux64b, 9 * n));
+    IPG_TRY(dalloc(c, &c->uy64b, 9 * n));
+    IPG_TRY(dalloc(c, &c->phi64b, 9 * n));
+    if (is_fp32(c)) {
+        IPG_TRY(alloc_state32(c, c->s32));
+        IPG_TRY(dalloc(c, &c->ux32b, 9 * n));
+        IPG_TRY(dalloc(c, &c->uy32b, 9 * n));
+        IPG_TRY(dalloc(c, &c->phi32b, 9 * n));
+    }
+    IPG_TRY(dalloc(c, &c->T10, 10 * n));
+    IPG_TRY(dalloc(c, &c->eps, n));
+    IPG_TRY(dalloc(c, &c->u4, 4 * n));
+    IPG_TRY(dalloc(c, &c->pi10, 10 * n));
+    IPG_TRY(dalloc(c, &c->carry, 5 * n));
+    IPG_TRY(dalloc(c, &c->wrote, n));
+    IPG_TRY(dalloc(c, &c->found, n));
+    IPG_TRY(dalloc(c, &c->partial, ((n + 255) / 256) * 18 + 64));
+    IPG_TRY(dalloc(c, &c->scal, 64));
+    IPG_TRY(dalloc(c, &c->d_ev, 1));
+
+    // twiddles exp(-2 pi i k/N), evaluated on the host in double precision
+    std::vector<double2> tw(N / 2);
+    for (int k = 0; k < N / 2; k++) {
+        const double ang = 2.0 * M_PI * (double)k / (double)N;
+        tw[k] = make_double2(std::cos(ang), -std::sin(ang));
+    }
+    IPG_CUDA(c, cudaMemcpyAsync(c->twiddle, tw.data(), sizeof(double2) * tw.size(),
+                                cudaMemcpyHostToDevice, c->stream));
+    EventGeom geom{N, cfg->Ny, c->a, cfg->g, c->m_lat, c->uv_lat};
+    IPG_CUDA(c, cudaMemcpyAsync(c->d_ev, &geom, sizeof(geom),
+                                cudaMemcpyHostToDevice, c->stream));
+    launch_green(N, c->m_lat, c->uv_lat, c->green, c->stream);
+    IPG_LAUNCHED(c, 1);
+    IPG_TRY(sync(c));
+    c->err.clear();
+    return IPG_OK;
+}
+
+ipg_status ipg_destroy(ipg_ctx *ctx) {
+    if (!ctx) return IPG_OK;
+    if (ctx->stream) {
+        cudaSetDevice(ctx->cfg.device);
+        cudaStreamSynchronize(ctx->stream);
+    }
+    for (void *p : ctx->allocs) cudaFree(p);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return IPG_OK;
+}
+
+ipg_status ipg_time_grid(const ipg_ctx *ctx, double *dtau, int *itmax) {
+    if (!ctx) return IPG_ERR_BAD_CONFIG;
+    if (dtau) *dtau = ctx->dtau;
+    if (itmax) *itmax = ctx->itmax;
+    return IPG_OK;
+}
+
+ipg_status ipg_set_g2mu(ipg_ctx *c, const double *A, const double *B) {
+    if (!c || !A || !B) return fail(c, IPG_ERR_BAD_CONFIG, "null argument");
+    IPG_CUDA(c, cudaMemcpyAsync(c->g2mu2A, A, sizeof(double) * c->n,
+                                cudaMemcpyHostToDevice, c->stream));
+    IPG_CUDA(c, cudaMemcpyAsync(c->g2mu2B, B, sizeof(double) * c->n,
+                                cudaMemcpyHostToDevice, c->stream));
+    c->have_g2mu = true;
+    return IPG_OK;
+}
+
+ipg_status ipg_set_g2mu_device(ipg_ctx *c, const double *A, const double *B) {
+    if (!c || !A || !B) return fail(c, IPG_ERR_BAD_CONFIG, "null argument");
+    IPG_CUDA(c, cudaMemcpyAsync(c->g2mu2A, A, sizeof(double) * c->n,
+                                cudaMemcpyDeviceToDevice, c->stream));
+    IPG_CUDA(c, cudaMemcpyAsync(c->g2mu2B, B, sizeof(double) * c->n,
+                                cudaMemcpyDeviceToDevice, c->stream));
+    c->have_g2mu = true;
+    return IPG_OK;
+}
+
+ipg_status ipg_set_noise(ipg_ctx *c, const double *A, const double *B) {
+    if (!c || !A || !B) return fail(c, IPG_ERR_BAD_CONFIG, "null argument");
+    const size_t cnt = (size_t)c->cfg.Ny * c->n * 8;
+    if (!c->xiA_own) {
+        IPG_TRY(dalloc(c, &c->xiA_own, cnt));
+        IPG_TRY(dalloc(c, &c->xiB_own, cnt));
+    }
+    IPG_CUDA(c, cudaMemcpyAsync(c->xiA_own, A, sizeof(double) * cnt,
+                                cudaMemcpyHostToDevice, c->stream));
+    IPG_CUDA(c, cudaMemcpyAsync(c->xiB_own, B, sizeof(double) * cnt,
+                                cudaMemcpyHostToDevice, c->stream));
+    c->xiA = c->xiA_own;
+    c->xiB = c->xiB_own;
+    c->have_noise = true;
+    c->device_noise = false;
+    return IPG_OK;
+}
+
+ipg_status ipg_set_noise_device(ipg_ctx *c, const double *A, const double *B) {
+    if (!c || !A || !B) return fail(c, IPG_ERR_BAD_CONFIG, "null argument");
+    c->xiA = A;
+    c->xiB = B;
+    c->have_noise = true;
+    c->device_noise = false;
+    return IPG_OK;
+}
+
+ipg_status ipg_use_device_noise(ipg_ctx *c) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    c->xiA = c->xiB = nullptr;
+    c->have_noise = true;
+    c->device_noise = true;
+    return IPG_OK;
+}
+
+ipg_status ipg_init_fields(ipg_ctx *c, ipg_init_report *rep) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (!c->have_g2mu || !c->have_noise)
+        return fail(c, IPG_ERR_STATE, "set g2mu and noise before ipg_init_fields");
+    const size_t n = c->n;
+    const int N = c->N;
+    cudaEvent_t e[4];
+    for (auto &x : e) IPG_CUDA(c, cudaEventCreate(&x));
+    IPG_CUDA(c, cudaEventRecord(e[0], c->stream));
+
+    // Wilson lines, nucleus A then B (Init.cpp:1688-1847)
+    for (int nuc = 0; nuc < 2; nuc++) {
+        C<double> *V = nuc ? c->VB : c->VA;
+        k_identity<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, V);
+        IPG_LAUNCHED(c, 1);
+        WilsonArgs w;
+        w.N = N;
+        w.logN = c->logN;
+        w.Ny = c->cfg.Ny;
+        w.g = c->cfg.g;
+        w.g2mu2 = nuc ? c->g2mu2B : c->g2mu2A;
+        w.xi = nuc ? c->xiB : c->xiA;
+        w.philox_key = c->cfg.seed;
+        w.nucleus = (uint32_t)nuc;
+        w.twiddle = c->twiddle;
+        w.green = c->green;
+        w.work = c->work;
+        w.V = V;
+        for (int k0 = 0; k0 < c->cfg.Ny; k0 += c->work_sheets) {
+            const int ns = std::min(c->work_sheets, c->cfg.Ny - k0);
+            launch_wilson_sheets(w, k0, ns, c->stream);
+            IPG_LAUNCHED(c, 4);
+        }
+    }
+    IPG_CUDA(c, cudaEventRecord(e[1], c->stream));
+
+    // tau = 0 links (Init.cpp:2462-2517)
+    launch_link_products(N, c->VA, c->VB, c->u1x, c->u2x, c->u1y, c->u2y, c->stream);
+    IPG_LAUNCHED(c, 1);
+    NewtonArgs na;
+    na.N = N;
+    na.max_iter = c->cfg.newton_max_iterations;
+    na.max_restart = c->cfg.newton_max_restarts;
+    na.philox_key = c->cfg.seed ^ 0x5DEECE66DULL;
+    na.u1x = c->u1x;
+    na.u2x = c->u2x;
+    na.u1y = c->u1y;
+    na.u2y = c->u2y;
+    na.ux = c->s64.ux;
+    na.uy = c->s64.uy;
+    na.iters = c->newton_iters;
+    na.status = c->newton_status;
+    launch_newton(na, c->stream);
+    IPG_LAUNCHED(c, 1);
+    IPG_CUDA(c, cudaEventRecord(e[2], c->stream));
+
+    // initial fields: pi from the minus stencil, E = phi = 0 (Init.cpp:2521-2690)
+    launch_initial_pi(N, c->cfg.g, c->u1x, c->u2x, c->u1y, c->u2y, c->s64.ux,
+                      c->s64.uy, c->s64.pi, c->stream);
+    IPG_LAUNCHED(c, 1);
+    IPG_CUDA(c, cudaMemsetAsync(c->s64.e1, 0, sizeof(double) * 8 * n, c->stream));
+    IPG_CUDA(c, cudaMemsetAsync(c->s64.e2, 0, sizeof(double) * 8 * n, c->stream));
+    IPG_CUDA(c, cudaMemsetAsync(c->s64.phi, 0, sizeof(double) * 9 * n, c->stream));
+    IPG_TRY(to_fp32_if_needed(c));
+    IPG_CUDA(c, cudaEventRecord(e[3], c->stream));
+    IPG_TRY(sync(c));
+
+    std::vector<int> it(2 * n), stv(2 * n);
+    IPG_CUDA(c, cudaMemcpy(it.data(), c->newton_iters, sizeof(int) * 2 * n,
+                           cudaMemcpyDeviceToHost));
+    IPG_CUDA(c, cudaMemcpy(stv.data(), c->newton_status, sizeof(int) * 2 * n,
+                           cudaMemcpyDeviceToHost));
+    int restarted = 0, failed = 0, mx = 0;
+    double sum = 0;
+    for (size_t k = 0; k < 2 * n; k++) {
+        restarted += stv[k] >= 1;
+        failed += stv[k] == 2;
+        mx = std::max(mx, it[k]);
+        sum += it[k];
+    }
+    if (rep) {
+        rep->newton_links = (int)(2 * n);
+        rep->newton_restarted = restarted;
+        rep->newton_failed = failed;
+        rep->newton_max_iterations = mx;
+        rep->newton_mean_iterations = sum / (2.0 * n);
+        float ms;
+        cudaEventElapsedTime(&ms, e[0], e[1]);
+        rep->ms_wilson = ms;
+        cudaEventElapsedTime(&ms, e[1], e[2]);
+        rep->ms_newton = ms;
+        cudaEventElapsedTime(&ms, e[2], e[3]);
+        rep->ms_fields = ms;
+    }
+    for (auto &x : e) cudaEventDestroy(x);
+    c->initialized = true;
+    c->half_done = false;
+    c->finished = false;
+    c->it = 0;
+    if (failed)
+        return fail(c, IPG_ERR_NEWTON_NONCONVERGED,
+                    "%d of %zu links did not converge", failed, 2 * n);
+    return IPG_OK;
+}
+
+ipg_status ipg_evolve(ipg_ctx *c, int steps) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (!c->initialized || c->finished)
+        return fail(c, IPG_ERR_STATE, "ipg_evolve needs fresh initial fields");
+    if (steps < 0) return fail(c, IPG_ERR_BAD_CONFIG, "steps < 0");
+    IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    int launched = 0;
+    if (!c->half_done) {
+        IPG_TRY(step(c, 0., c->dtau, c->dtau, 0, 1));
+        c->half_done = true;
+        launched++;
+    }
+    for (int k = 0; k < steps; k++) {
+        const int itn = c->it + 1;
+        IPG_TRY(step(c, itn * c->dtau, c->dtau, c->dtau, 1, 1));
+        c->it = itn;
+        launched++;
+    }
+    IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    IPG_TRY(sync(c));
+    c->last_leapfrog_ms = elapsed(c);
+    c->last_leapfrog_launches = launched;
+    return IPG_OK;
+}
+
+ipg_status ipg_run(ipg_ctx *c, ipg_result *res) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (!c->initialized || c->half_done || c->finished)
+        return fail(c, IPG_ERR_STATE, "ipg_run needs fresh initial fields");
+    const int itmax = c->itmax;
+    const double dtau = c->dtau;
+    const size_t n = c->n;
+    const int N = c->N;
+
+    IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    IPG_TRY(step(c, 0., dtau, dtau, 0, 1));  // Evolution.cpp:393-394
+    c->half_done = true;
+    for (int it = 1; it < itmax; it++) {
+        IPG_TRY(step(c, it * dtau, dtau, dtau, 1, 1));  // 416-421
+        c->it = it;
+    }
+    IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    IPG_TRY(sync(c));
+    c->last_leapfrog_ms = elapsed(c);
+    c->last_leapfrog_launches = itmax;
+    const double ms_evo = c->last_leapfrog_ms;
+
+    // observables at it = itmax before the last half step (406-410)
+    IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    IPG_TRY(state64(c));
+    TmunuArgs ta;
+    ta.N = N;
+    ta.g = c->cfg.g;
+    ta.tau = itmax * dtau;
+    ta.a = c->a;
+    ta.s = c->s64;
+    ta.T10 = c->T10;
+    launch_tmunu(ta, c->stream);
+    IPG_LAUNCHED(c, 2);
+    LandauArgs la;
+    la.N = N;
+    la.tau_fm = itmax * dtau * c->a;
+    la.tau2_fm = c->a * itmax * dtau * c->a * itmax * dtau;
+    la.tau_fm_parts[0] = itmax;
+    la.tau_fm_parts[1] = dtau;
+    la.tau_fm_parts[2] = c->a;
+    la.T10 = c->T10;
+    la.eps = c->eps;
+    la.u4 = c->u4;
+    la.pi10 = c->pi10;
+    la.found = c->found;
+    launch_landau(la, c->carry, c->wrote, c->stream);
+    IPG_LAUNCHED(c, 2);
+    double *scal = c->scal;
+    launch_eccentricity(N, c->cfg.L, c->a, c->eps, c->u4, c->T10, c->partial,
+                        scal + 0, scal + 8, c->stream);
+    IPG_LAUNCHED(c, 4);
+
+    // last half step of pi and E (426-431), then the Gauss law (633-635)
+    IPG_TRY(step(c, itmax * dtau, dtau / 2., dtau, 1, 0));
+    c->it = itmax;
+    IPG_TRY(state64(c));
+    launch_gauss_law(N, c->s64, c->partial, scal + 32, c->stream);
+    IPG_LAUNCHED(c, 2);
+    launch_unitarity(N, c->s64.ux, c->s64.uy, c->partial, scal + 33, c->stream);
+    IPG_LAUNCHED(c, 2);
+    IPG_CUDA(c, cudaMemsetAsync(reinterpret_cast<int *>(scal + 34), 0, sizeof(int),
+                                c->stream));
+    k_count_nan<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+        n, c->eps, reinterpret_cast<int *>(scal + 34));
+    IPG_LAUNCHED(c, 1);
+    IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    IPG_TRY(sync(c));
+    const double ms_obs = elapsed(c);
+    c->finished = true;
+
+    double h[40];
+    IPG_CUDA(c, cudaMemcpy(h, scal, sizeof(double) * 35, cudaMemcpyDeviceToHost));
+    std::vector<int> found(n);
+    IPG_CUDA(c, cudaMemcpy(found.data(), c->found, sizeof(int) * n,
+                           cudaMemcpyDeviceToHost));
+    int nan_count = 0;
+    std::memcpy(&nan_count, &h[34], sizeof(int));
+    if (res) {
+        std::memset(res, 0, sizeof(*res));
+        res->itmax = itmax;
+        res->dtau = dtau;
+        res->tau_final = itmax * dtau * c->a;
+        res->gauss_violation = h[32];
+        res->unitarity_max = h[33];
+        res->sum_Ttautau = h[3];
+        res->sum_eps = h[4];
+        res->E_T = res->tau_final * c->a * c->a * kHbarc * h[3];
+        // radial moments: [0..5] avr1 avrSq avr3 avr4 avr5 avr6,
+        // [6 + 2(n-1)], [7 + 2(n-1)] cos/sin moments for n = 1..6
+        const double *m = h + 8;
+        const double avr[6] = {m[0], m[1], m[2], m[3], m[4], m[5]};
+        for (int k = 0; k < 6; k++) {
+            const double cs = m[6 + 2 * k], sn = m[7 + 2 * k];
+            res->eccentricity[k] = std::sqrt(cs * cs + sn * sn) / avr[k];
+            res->psi[k] = (std::atan(sn / cs) + M_PI) / (k + 1);
+        }
+        int nf = 0;
+        for (size_t p = 0; p < n; p++) nf += found[p] == 0;
+        res->cells_without_u = nf;
+        res->ms_evolution = ms_evo;
+        res->ms_observables = ms_obs;
+    }
+    if (nan_count) return fail(c, IPG_ERR_NAN, "%d cells with non-finite e", nan_count);
+    return IPG_OK;
+}
+
+ipg_status ipg_get_observables(ipg_ctx *c, double *eps, double *u4,
+                               double *pi10, double *T10) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (!c->finished) return fail(c, IPG_ERR_STATE, "call ipg_run first");
+    const size_t n = c->n;
+    if (eps) IPG_CUDA(c, cudaMemcpy(eps, c->eps, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (u4) IPG_CUDA(c, cudaMemcpy(u4, c->u4, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost));
+    if (pi10) IPG_CUDA(c, cudaMemcpy(pi10, c->pi10, sizeof(double) * 10 * n, cudaMemcpyDeviceToHost));
+    if (T10) IPG_CUDA(c, cudaMemcpy(T10, c->T10, sizeof(double) * 10 * n, cudaMemcpyDeviceToHost));
+    return IPG_OK;
+}
+
+ipg_status ipg_get_field(ipg_ctx *c, int which, double *out) {
+    if (!c || !out) return IPG_ERR_BAD_CONFIG;
+    IPG_TRY(sync(c));
+    const size_t n = c->n;
+    if (which == IPG_VA || which == IPG_VB || which == IPG_UX || which == IPG_UY) {
+        if (which == IPG_UX || which == IPG_UY) IPG_TRY(state64(c));
+        const C<double> *src = which == IPG_VA ? c->VA
+                               : which == IPG_VB ? c->VB
+                               : which == IPG_UX ? c->s64.ux
+                                                 : c->s64.uy;
+        std::vector<double> pl(18 * n);
+        IPG_CUDA(c, cudaMemcpy(pl.data(), src, sizeof(double) * 18 * n,
+                               cudaMemcpyDeviceToHost));
+        planes_to_sites_m3(pl, n, out);
+        return IPG_OK;
+    }
+    IPG_TRY(state64(c));
+    const bool tl = (which == IPG_E1 || which == IPG_E2);
+    const double *src = which == IPG_E1 ? c->s64.e1
+                        : which == IPG_E2 ? c->s64.e2
+                        : which == IPG_PHI ? c->s64.phi
+                        : which == IPG_PI ? c->s64.pi
+                                          : nullptr;
+    if (!src) return fail(c, IPG_ERR_BAD_CONFIG, "unknown field %d", which);
+    std::vector<double> pl((tl ? 8 : 9) * n);
+    IPG_CUDA(c, cudaMemcpy(pl.data(), src, sizeof(double) * pl.size(),
+                           cudaMemcpyDeviceToHost));
+    herm_to_sites(pl, n, tl, out);
+    return IPG_OK;
+}
+
+ipg_status ipg_set_field(ipg_ctx *c, int which, const double *in) {
+    if (!c || !in) return IPG_ERR_BAD_CONFIG;
+    const size_t n = c->n;
+    IPG_TRY(sync(c));
+    if (which == IPG_VA || which == IPG_VB || which == IPG_UX || which == IPG_UY) {
+        C<double> *dst = which == IPG_VA ? c->VA
+                         : which == IPG_VB ? c->VB
+                         : which == IPG_UX ? c->s64.ux
+                                           : c->s64.uy;
+        std::vector<double> pl(18 * n);
+        for (size_t p = 0; p < n; p++)
+            for (int k = 0; k < 9; k++) {
+                pl[2 * (k * n + p)] = in[18 * p + 2 * k];
+                pl[2 * (k * n + p) + 1] = in[18 * p + 2 * k + 1];
+            }
+        IPG_CUDA(c, cudaMemcpy(dst, pl.data(), sizeof(double) * 18 * n,
+                               cudaMemcpyHostToDevice));
+        return IPG_OK;
+    }
+    const bool tl = (which == IPG_E1 || which == IPG_E2);
+    double *dst = which == IPG_E1 ? c->s64.e1
+                  : which == IPG_E2 ? c->s64.e2
+                  : which == IPG_PHI ? c->s64.phi
+                  : which == IPG_PI ? c->s64.pi
+                                    : nullptr;
+    if (!dst) return fail(c, IPG_ERR_BAD_CONFIG, "unknown field %d", which);
+    std::vector<double> pl;
+    sites_to_herm(in, n, tl, pl);
+    IPG_CUDA(c, cudaMemcpy(dst, pl.data(), sizeof(double) * pl.size(),
+                           cudaMemcpyHostToDevice));
+    return IPG_OK;
+}
+
+ipg_status ipg_mark_initialized(ipg_ctx *c) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    IPG_TRY(to_fp32_if_needed(c));
+    IPG_TRY(sync(c));
+    c->initialized = true;
+    c->half_done = false;
+    c->finished = false;
+    c->it = 0;
+    return IPG_OK;
+}
+
+ipg_status ipg_get_newton_iterations(ipg_ctx *c, int *iters, int *status) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    const size_t n = c->n;
+    if (iters) IPG_CUDA(c, cudaMemcpy(iters, c->newton_iters, sizeof(int) * 2 * n, cudaMemcpyDeviceToHost));
+    if (status) IPG_CUDA(c, cudaMemcpy(status, c->newton_status, sizeof(int) * 2 * n, cudaMemcpyDeviceToHost));
+    return IPG_OK;
+}
+
+ipg_status ipg_last_leapfrog_ms(ipg_ctx *c, double *ms, int *launches) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (ms) *ms = c->last_leapfrog_ms;
+    if (launches) *launches = c->last_leapfrog_launches;
+    return IPG_OK;
+}
+
+ipg_status ipg_kernel_launches(const ipg_ctx *c, long long *count) {
+    if (!c || !count) return IPG_ERR_BAD_CONFIG;
+    *count = c->launches;
+    return IPG_OK;
+}
+
+}  // extern "C"

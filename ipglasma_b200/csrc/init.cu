@@ -1,0 +1,517 @@
+// Initial conditions: colour charges -> Poisson solve -> Wilson lines ->
+// tau = 0 links (Newton) -> initial longitudinal field.
+//
+// Reference: Init::setV (Init.cpp:1678-1849) and the tau = 0 block of
+// Init::init (Init.cpp:2437-2691).
+//
+// Poisson solve. The reference transforms each of the 8 colours of a sheet
+// separately with FFTW after an fftshift, multiplies by the lattice Green
+// function on the centred k-grid and transforms back (FFT.cpp:492-605,
+// Init.cpp:1707-1747). For an even N the fftshifts on both sides cancel
+// (cyclic convolution commutes with a shift by N/2), so here the multiplier
+// is applied on the plain DFT grid with the centred index (p + N/2) mod N,
+// which gives the same k~ values. Two real colours are packed into one
+// complex transform (colour 2c in the real part, 2c+1 in the imaginary part):
+// the Green function is real and even, so the two results separate into the
+// real and imaginary parts of the inverse transform.
+//
+// Kernels per batch of sheets:
+//   k_rows_fwd   rho = g sqrt(g2mu2/Ny) xi, row FFTs          (smem, 4 channels)
+//   k_cols       column FFT, Green multiply, inverse column FFT (smem)
+//   k_rows_inv   inverse row FFTs, 1/N^2
+//   k_wilson     per site: V <- exp(-i A_k.t) V over the batch, in order
+// The work buffer of a batch is sized to stay resident in the 126 MB L2.
+#include <cstdint>
+#include <cstdio>
+
+#include "expm.cuh"
+#include "fields.cuh"
+#include "ipg_internal.h"
+#include "philox.cuh"
+
+namespace ipg {
+
+// ---------------------------------------------------------------------------
+// shared-memory radix-2 FFT on `batch` sequences of length n = 2^logn;
+// element i of sequence b lives at data[b * ld + i]. Forward uses
+// exp(-2 pi i jk/n) (FFTW_FORWARD), inverse exp(+...); unnormalised.
+// ---------------------------------------------------------------------------
+__device__ void smem_fft(double2 *data, int ld, int batch, int logn,
+                         const double2 *__restrict__ tw, bool inverse) {
+    const int n = 1 << logn;
+    const int total = batch << logn;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int b = idx >> logn, i = idx & (n - 1);
+        const int r = __brev(i) >> (32 - logn);
+        if (r > i) {
+            double2 t = data[b * ld + i];
+            data[b * ld + i] = data[b * ld + r];
+            data[b * ld + r] = t;
+        }
+    }
+    __syncthreads();
+    const int halfn = n >> 1;
+    for (int s = 1; s <= logn; s++) {
+        const int half = 1 << (s - 1);
+        const int tshift = logn - s;
+        for (int idx = threadIdx.x; idx < (batch * halfn); idx += blockDim.x) {
+            const int b = idx / halfn, q = idx - b * halfn;
+            const int k = q & (half - 1);
+            const int i0 = ((q >> (s - 1)) << s) + k, i1 = i0 + half;
+            double2 w = __ldg(&tw[k << tshift]);
+            if (inverse) w.y = -w.y;
+            double2 x0 = data[b * ld + i0], x1 = data[b * ld + i1];
+            double tr = x1.x * w.x - x1.y * w.y;
+            double ti = x1.x * w.y + x1.y * w.x;
+            data[b * ld + i0] = make_double2(x0.x + tr, x0.y + ti);
+            data[b * ld + i1] = make_double2(x0.x - tr, x0.y - ti);
+        }
+        __syncthreads();
+    }
+}
+
+// Green function of the lattice Laplacian on the DFT grid (Init.cpp:1712-1742)
+__global__ void k_green(int N, double m_lat, double uvdamp_lat, double *green) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N * N) return;
+    const int pi = p / N, pj = p % N;
+    const int i = (pi + N / 2) % N, j = (pj + N / 2) % N;  // centred index
+    const double kx = 2. * M_PI * (-0.5 + (double)i / (double)N);
+    const double ky = 2. * M_PI * (-0.5 + (double)j / (double)N);
+    const double kt2 = 4. * (sin(kx / 2.) * sin(kx / 2.) + sin(ky / 2.) * sin(ky / 2.));
+    double gk;
+    if (m_lat == 0) {
+        gk = (kt2 != 0) ? 1. / kt2 : 0.;
+    } else {
+        gk = (1. / (kt2 + m_lat * m_lat)) * exp(-sqrt(kt2) * uvdamp_lat);
+    }
+    green[p] = gk;
+}
+
+void launch_green(int N, double m_lat, double uvdamp_lat, double *green,
+                  cudaStream_t st) {
+    const int n = N * N;
+    k_green<<<(n + 255) / 256, 256, 0, st>>>(N, m_lat, uvdamp_lat, green);
+}
+
+// rho for one row of one sheet into 4 packed channels, then row FFTs
+__global__ void k_rows_fwd(WilsonArgs w, int k0) {
+    extern __shared__ double2 sm[];
+    const int N = w.N;
+    const size_t n = (size_t)N * N;
+    const int ix = blockIdx.x;
+    const int s = blockIdx.y;
+    const int k = k0 + s;
+    const double invNy = (double)w.Ny;
+    if (w.xi) {
+        const double *src = w.xi + ((size_t)k * n + (size_t)ix * N) * 8;
+        for (int idx = threadIdx.x; idx < 8 * N; idx += blockDim.x) {
+            const int j = idx >> 3, a = idx & 7;
+            const double amp = w.g * sqrt(w.g2mu2[(size_t)ix * N + j] / invNy);
+            const double rho = amp * src[idx];
+            double *dst = reinterpret_cast<double *>(&sm[(a >> 1) * N + j]);
+            dst[a & 1] = rho;
+        }
+    } else {
+        for (int j = threadIdx.x; j < N; j += blockDim.x) {
+            const size_t pos = (size_t)ix * N + j;
+            const double amp = w.g * sqrt(w.g2mu2[pos] / invNy);
+            double z[8];
+            normal4({(uint32_t)pos, (uint32_t)k, (w.nucleus << 1) | 0u, 0u},
+                    w.philox_key, z);
+            normal4({(uint32_t)pos, (uint32_t)k, (w.nucleus << 1) | 1u, 0u},
+                    w.philox_key, z + 4);
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+                sm[c * N + j] = make_double2(amp * z[2 * c], amp * z[2 * c + 1]);
+        }
+    }
+    __syncthreads();
+    smem_fft(sm, N, 4, w.logN, w.twiddle, false);
+    for (int idx = threadIdx.x; idx < 4 * N; idx += blockDim.x) {
+        const int c = idx / N, j = idx - c * N;
+        w.work[((size_t)s * 4 + c) * n + (size_t)ix * N + j] = sm[idx];
+    }
+}
+
+// column FFT + Green multiply + inverse column FFT on JB columns
+template <int JB>
+__global__ void k_cols(WilsonArgs w) {
+    extern __shared__ double2 sm[];
+    const int N = w.N;
+    const size_t n = (size_t)N * N;
+    const int jb = blockIdx.x * JB;
+    const int c = blockIdx.y;
+    const int s = blockIdx.z;
+    double2 *base = w.work + ((size_t)s * 4 + c) * n;
+    for (int idx = threadIdx.x; idx < N * JB; idx += blockDim.x) {
+        const int i = idx / JB, q = idx - i * JB;
+        sm[q * N + i] = base[(size_t)i * N + jb + q];
+    }
+    __syncthreads();
+    smem_fft(sm, N, JB, w.logN, w.twiddle, false);
+    for (int idx = threadIdx.x; idx < N * JB; idx += blockDim.x) {
+        const int q = idx / N, i = idx - q * N;
+        const double gk = w.green[(size_t)i * N + jb + q];
+        double2 v = sm[idx];
+        sm[idx] = make_double2(v.x * gk, v.y * gk);
+    }
+    __syncthreads();
+    smem_fft(sm, N, JB, w.logN, w.twiddle, true);
+    for (int idx = threadIdx.x; idx < N * JB; idx += blockDim.x) {
+        const int i = idx / JB, q = idx - i * JB;
+        base[(size_t)i * N + jb + q] = sm[q * N + i];
+    }
+}
+
+// inverse row FFTs and 1/N^2 normalisation, in place
+__global__ void k_rows_inv(WilsonArgs w) {
+    extern __shared__ double2 sm[];
+    const int N = w.N;
+    const size_t n = (size_t)N * N;
+    const int ix = blockIdx.x;
+    const int s = blockIdx.y;
+    for (int idx = threadIdx.x; idx < 4 * N; idx += blockDim.x) {
+        const int c = idx / N, j = idx - c * N;
+        sm[idx] = w.work[((size_t)s * 4 + c) * n + (size_t)ix * N + j];
+    }
+    __syncthreads();
+    smem_fft(sm, N, 4, w.logN, w.twiddle, true);
+    const double ntot = (double)n;
+    for (int idx = threadIdx.x; idx < 4 * N; idx += blockDim.x) {
+        const int c = idx / N, j = idx - c * N;
+        double2 v = sm[idx];
+        w.work[((size_t)s * 4 + c) * n + (size_t)ix * N + j] =
+            make_double2(v.x / ntot, v.y / ntot);
+    }
+}
+
+// V <- exp(-i A_k.t) V for the sheets of the batch, in ascending k
+// (Init.cpp:1750-1768: new * old)
+__global__ void k_wilson(WilsonArgs w, int ns) {
+    const size_t n = (size_t)w.N * w.N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    M3<double> V = ld_m3(w.V, pos, n);
+    for (int s = 0; s < ns; s++) {
+        double in[8];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const double2 v = w.work[((size_t)s * 4 + c) * n + pos];
+            in[2 * c] = -v.x;
+            in[2 * c + 1] = -v.y;
+        }
+        const M3<double> e = exp_from_coeff(in);
+        V = mul(e, V);
+    }
+    st_m3(w.V, pos, n, V);
+}
+
+static int fft_threads(int N) { return N >= 512 ? 512 : (N >= 256 ? 256 : 128); }
+
+void launch_wilson_sheets(const WilsonArgs &w, int k0, int ns,
+                          cudaStream_t st) {
+    const int N = w.N;
+    const size_t row_smem = sizeof(double2) * 4 * N;
+    const int thr = fft_threads(N);
+    cudaFuncSetAttribute(k_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)row_smem);
+    cudaFuncSetAttribute(k_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)row_smem);
+    k_rows_fwd<<<dim3(N, ns), thr, row_smem, st>>>(w, k0);
+    constexpr int JB = 8;
+    const size_t col_smem = sizeof(double2) * JB * N;
+    cudaFuncSetAttribute(k_cols<JB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)col_smem);
+    k_cols<JB><<<dim3(N / JB, 4, ns), thr, col_smem, st>>>(w);
+    k_rows_inv<<<dim3(N, ns), thr, row_smem, st>>>(w);
+    const size_t n = (size_t)N * N;
+    k_wilson<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
+}
+
+// ---------------------------------------------------------------------------
+// link products U1 = V_A(x) V_A(x+i)^dag, U2 likewise for V_B, with the NaN
+// guard of Init.cpp:2462-2470
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool nan_trace(const M3<double> &v) {
+    C<double> t = trace(v);
+    return isnan(t.r) || isnan(t.i);
+}
+
+__global__ void k_link_products(int N, const C<double> *VA, const C<double> *VB,
+                                C<double> *u1x, C<double> *u2x, C<double> *u1y,
+                                C<double> *u2y) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    const int ix = (int)(pos / N), iy = (int)(pos % N);
+    const size_t pX = (size_t)min(N - 1, ix + 1) * N + iy;
+    const size_t pY = (size_t)ix * N + min(N - 1, iy + 1);
+    M3<double> one;
+    set_identity(one);
+    auto get = [&](const C<double> *V, size_t p) {
+        M3<double> v = ld_m3(V, p, n);
+        return nan_trace(v) ? one : v;
+    };
+    const M3<double> a = get(VA, pos), b = get(VB, pos);
+    st_m3(u1x, pos, n, mul_nd(a, get(VA, pX)));
+    st_m3(u1y, pos, n, mul_nd(a, get(VA, pY)));
+    st_m3(u2x, pos, n, mul_nd(b, get(VB, pX)));
+    st_m3(u2y, pos, n, mul_nd(b, get(VB, pY)));
+}
+
+void launch_link_products(int N, C<double> *VA, C<double> *VB, C<double> *u1x,
+                          C<double> *u2x, C<double> *u1y, C<double> *u2y,
+                          cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    k_link_products<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(
+        N, VA, VB, u1x, u2x, u1y, u2y);
+}
+
+// ---------------------------------------------------------------------------
+// Newton solve of the tau = 0 matching condition per link
+// (Init::findUInForwardLightconeChun, Init.cpp:3344-3481)
+// ---------------------------------------------------------------------------
+
+// LU with partial pivoting and solve, in the elimination order of the
+// GSL 2.5 routines the reference calls (Init.cpp:47-63)
+__device__ void lu_solve8(double J[64], const double F[8], double x[8]) {
+    int perm[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) perm[i] = i;
+    for (int col = 0; col < 7; col++) {
+        int piv = col;
+        double best = fabs(J[col * 8 + col]);
+        for (int row = col + 1; row < 8; row++) {
+            double c = fabs(J[row * 8 + col]);
+            if (c > best) {
+                best = c;
+                piv = row;
+            }
+        }
+        if (piv != col) {
+            for (int k = 0; k < 8; k++) {
+                double t = J[col * 8 + k];
+                J[col * 8 + k] = J[piv * 8 + k];
+                J[piv * 8 + k] = t;
+            }
+            int t = perm[col];
+            perm[col] = perm[piv];
+            perm[piv] = t;
+        }
+        const double d = J[col * 8 + col];
+        if (d != 0.0) {
+            for (int row = col + 1; row < 8; row++) {
+                const double l = J[row * 8 + col] / d;
+                J[row * 8 + col] = l;
+                for (int k = col + 1; k < 8; k++) J[row * 8 + k] -= l * J[col * 8 + k];
+            }
+        }
+    }
+    double y[8];
+    for (int i = 0; i < 8; i++) y[i] = F[perm[i]];
+    for (int i = 1; i < 8; i++) {
+        double acc = y[i];
+        for (int j = 0; j < i; j++) acc -= J[i * 8 + j] * y[j];
+        y[i] = acc;
+    }
+    for (int i = 7; i >= 0; i--) {
+        double acc = y[i];
+        for (int j = i + 1; j < 8; j++) acc -= J[i * 8 + j] * y[j];
+        y[i] = acc / J[i * 8 + i];
+    }
+    for (int i = 0; i < 8; i++) x[i] = y[i];
+}
+
+__device__ __forceinline__ void restart_alpha(double alpha[8], uint64_t key,
+                                              uint32_t link, uint32_t draw) {
+    double z[8];
+    normal4({link, draw, 0xA11CEu, 0u}, key, z);
+    normal4({link, draw, 0xA11CEu, 1u}, key, z + 4);
+#pragma unroll
+    for (int a = 0; a < 8; a++) alpha[a] = z[a];
+}
+
+__global__ void __launch_bounds__(128) k_newton(NewtonArgs A) {
+    const size_t n = (size_t)A.N * A.N;
+    const size_t lid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (lid >= 2 * n) return;
+    // link order of the reference loop: per site, x then y (Init.cpp:2498-2516)
+    const size_t pos = lid >> 1;
+    const int dir = (int)(lid & 1);
+    const M3<double> U1 = ld_m3(dir ? A.u1y : A.u1x, pos, n);
+    const M3<double> U2 = ld_m3(dir ? A.u2y : A.u2x, pos, n);
+
+    const M3<double> U0 = mul(U1, U2);
+    M3<double> S = U1;
+    add_to(S, U2);
+    const M3<double> Sd = dagger(S);
+    C<double> traceCache[8];
+    trace_ta(minus(S, Sd), traceCache);
+
+    double alpha[8], dalpha[8], Fa[8], J[64];
+#pragma unroll
+    for (int a = 0; a < 8; a++) alpha[a] = 0.;
+    M3<double> Usol = mul(exp_from_coeff(alpha), U0);
+    M3<double> Usold = dagger(Usol);
+    M3<double> best;
+    set_identity(best);
+    double Fzero = 10., FzeroMin = 1e6;
+    int iter = 0, nRestart = 0, total = 0;
+    uint32_t draws = 0;
+    while (Fzero > 1e-6 && iter < A.max_iter && nRestart < A.max_restart) {
+        iter++;
+        total++;
+        Fzero = 0.;
+        {
+            M3<double> Mt = mul(S, Usold);
+            sub_from(Mt, mul(Usol, Sd));
+            C<double> tl[8];
+            trace_ta(Mt, tl);
+#pragma unroll
+            for (int a = 0; a < 8; a++) {
+                // -(traceCache + traceLoc), imaginary part
+                Fa[a] = -(traceCache[a].i + tl[a].i);
+                Fzero += fabs(Fa[a]);
+            }
+        }
+        bool good = true;
+        for (int b = 0; b < 8; b++) {
+            const double d = fmax(0.001, fmin(10., 0.01 * fabs(alpha[b])));
+            alpha[b] = alpha[b] + d;
+            M3<double> Mt = dagger(mul(exp_from_coeff(alpha), U0));
+            Mt = mul(S, minus(Mt, Usold));
+            C<double> tl[8];
+            trace_ta(Mt, tl);
+            double mcheck = 0.;
+            for (int a = 0; a < 8; a++) {
+                J[a * 8 + b] = 2. * tl[a].i / d;
+                mcheck += fabs(J[a * 8 + b]);
+                if (mcheck < 1e-15) good = false;
+            }
+            alpha[b] = alpha[b] - d;
+        }
+        if (!good) {
+            // analytic approximation (Init.cpp:3419-3431)
+            for (int b = 0; b < 8; b++) {
+                const M3<double> Mt = ta_mul(b, Usold);
+                for (int a = 0; a < 8; a++) {
+                    const M3<double> Ma = ta_mul(a, S);
+                    J[a * 8 + b] = -2. * re_trace_mul(Ma, Mt);
+                }
+            }
+        }
+        lu_solve8(J, Fa, dalpha);
+        bool ok = true;
+        for (int a = 0; a < 8; a++)
+            if (fabs(dalpha[a]) > 1e5) {
+                ok = false;
+                break;
+            }
+        if (ok) {
+            for (int a = 0; a < 8; a++) alpha[a] = alpha[a] + dalpha[a];
+        } else {
+            restart_alpha(alpha, A.philox_key, (uint32_t)lid, draws++);
+        }
+        Usol = mul(exp_from_coeff(alpha), U0);
+        Usold = dagger(Usol);
+        if (Fzero < FzeroMin) {
+            FzeroMin = Fzero;
+            best = Usol;
+        }
+        if (iter == A.max_iter) {
+            restart_alpha(alpha, A.philox_key, (uint32_t)lid, draws++);
+            Usol = mul(exp_from_coeff(alpha), U0);
+            Usold = dagger(Usol);
+            nRestart++;
+            iter = 0;
+        }
+    }
+    int status = draws ? 1 : 0;
+    if (nRestart == A.max_restart) {
+        Usol = best;
+        status = 2;
+    }
+    st_m3(dir ? A.uy : A.ux, pos, n, Usol);
+    A.iters[lid] = total;
+    A.status[lid] = status;
+}
+
+void launch_newton(const NewtonArgs &a, cudaStream_t st) {
+    const size_t links = 2 * (size_t)a.N * a.N;
+    k_newton<<<(unsigned)((links + 127) / 128), 128, 0, st>>>(a);
+}
+
+// ---------------------------------------------------------------------------
+// pi(tau=0) = (-2i/g) E1 with E1 from the "minus" stencil / 8
+// (Init.cpp:2521-2584, 2664-2681). The stencil value t is anti-Hermitian, so
+// pi = -(i / (4 g)) t is Hermitian.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void stencil_term(M3<double> &t, const M3<double> &D,
+                                             const M3<double> &Dd,
+                                             const M3<double> &U, bool here) {
+    // here:  + D U^dag - D - U D^dag + D^dag
+    // minus: - U^dag D + D + D^dag U - D^dag
+    if (here) {
+        add_to(t, mul_nd(D, U));
+        sub_from(t, D);
+        sub_from(t, mul(U, Dd));
+        add_to(t, Dd);
+    } else {
+        sub_from(t, mul_dn(U, D));
+        add_to(t, D);
+        add_to(t, mul(Dd, U));
+        sub_from(t, Dd);
+    }
+}
+
+__global__ void k_initial_pi(int N, double g, const C<double> *u1x,
+                             const C<double> *u2x, const C<double> *u1y,
+                             const C<double> *u2y, const C<double> *ux,
+                             const C<double> *uy, double *pi) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    const int ix = (int)(pos / N), iy = (int)(pos % N);
+    const size_t mX = (size_t)max(0, ix - 1) * N + iy;
+    const size_t mY = (size_t)ix * N + max(0, iy - 1);
+    M3<double> t;
+#pragma unroll
+    for (int k = 0; k < 9; k++) t.m[k] = {0., 0.};
+    {
+        M3<double> D = minus(ld_m3(u1x, pos, n), ld_m3(u2x, pos, n));
+        stencil_term(t, D, dagger(D), ld_m3(ux, pos, n), true);
+    }
+    {
+        M3<double> D = minus(ld_m3(u1x, mX, n), ld_m3(u2x, mX, n));
+        stencil_term(t, D, dagger(D), ld_m3(ux, mX, n), false);
+    }
+    {
+        M3<double> D = minus(ld_m3(u1y, pos, n), ld_m3(u2y, pos, n));
+        stencil_term(t, D, dagger(D), ld_m3(uy, pos, n), true);
+    }
+    {
+        M3<double> D = minus(ld_m3(u1y, mY, n), ld_m3(u2y, mY, n));
+        stencil_term(t, D, dagger(D), ld_m3(uy, mY, n), false);
+    }
+    // pi = (-2i/g) * (t / 8): entry (r,s) = (2/(8g)) * (Im t, -Re t)
+    const double f = 2. / g;
+    M3<double> p;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const double er = t.m[k].r / 8., ei = t.m[k].i / 8.;
+        p.m[k] = {f * ei, -f * er};
+    }
+    st_h(pi, pos, n, to_h(p));
+}
+
+void launch_initial_pi(int N, double g, const C<double> *u1x,
+                       const C<double> *u2x, const C<double> *u1y,
+                       const C<double> *u2y, const C<double> *ux,
+                       const C<double> *uy, double *pi, cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    k_initial_pi<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(
+        N, g, u1x, u2x, u1y, u2y, ux, uy, pi);
+}
+
+}  // namespace ipg

@@ -1,0 +1,135 @@
+// Internal declarations shared by the CUDA translation units of the library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "fields.cuh"
+
+namespace ipg {
+
+// Per-event constants visible to kernels (one entry per event of a batch).
+struct EventGeom {
+    int N;         // sites per side
+    int Ny;        // longitudinal sheets
+    double a;      // lattice spacing, fm
+    double g;      // coupling
+    double m_lat;  // IR mass in lattice units (m a / hbar c)
+    double uvdamp_lat;
+};
+
+template <typename T>
+struct StepCoef {
+    T tau;    // current time (lattice units)
+    T dt_pe;  // time step used for the pi and E updates
+    T dt_pu;  // time step used for the phi and U updates
+    T g;
+    int do_pe;
+    int do_pu;
+};
+
+template <typename T>
+void launch_leapfrog(const EventGeom *d_ev, int N, const State<T> &s,
+                     C<T> *ux_out, C<T> *uy_out, T *phi_out,
+                     const StepCoef<T> &cf, bool reunit, cudaStream_t st);
+
+// ---- initial conditions -------------------------------------------------
+
+// Colour-charge sheets -> Wilson lines for one nucleus, sheets [k0, k0+ns).
+struct WilsonArgs {
+    int N;
+    int logN;
+    int Ny;
+    double g;
+    const double *g2mu2;     // [n] lattice units
+    const double *xi;        // [Ny][n][8] unit normals, or null (Philox)
+    uint64_t philox_key;     // used when xi == null
+    uint32_t nucleus;        // 0 = A, 1 = B (Philox stream selector)
+    const double2 *twiddle;  // [N/2] exp(-2 pi i k / N)
+    const double *green;     // [N*N] Poisson multiplier on the DFT grid
+    double2 *work;           // [ns][4][n] complex scratch
+    C<double> *V;            // [9][n] Wilson line, updated in place
+};
+void launch_wilson_sheets(const WilsonArgs &w, int k0, int ns,
+                          cudaStream_t st);
+
+void launch_green(int N, double m_lat, double uvdamp_lat, double *green,
+                  cudaStream_t st);
+
+// V_A, V_B -> link products U1, U2 for both directions (Init.cpp:2462-2491)
+void launch_link_products(int N, C<double> *VA, C<double> *VB,
+                          C<double> *u1x, C<double> *u2x, C<double> *u1y,
+                          C<double> *u2y, cudaStream_t st);
+
+struct NewtonArgs {
+    int N;
+    int max_iter;
+    int max_restart;
+    uint64_t philox_key;
+    const C<double> *u1x, *u2x, *u1y, *u2y;
+    C<double> *ux, *uy;  // solutions
+    int *iters;          // [2n] iterations used (total over restarts)
+    int *status;         // [2n] 0 ok, 1 restarted then converged, 2 failed
+};
+void launch_newton(const NewtonArgs &a, cudaStream_t st);
+
+// Initial longitudinal field pi from the "minus" stencil (Init.cpp:2521-2584,
+// 2664-2681).
+void launch_initial_pi(int N, double g, const C<double> *u1x,
+                       const C<double> *u2x, const C<double> *u1y,
+                       const C<double> *u2y, const C<double> *ux,
+                       const C<double> *uy, double *pi, cudaStream_t st);
+
+// ---- observables ----------------------------------------------------------
+
+struct TmunuArgs {
+    int N;
+    double g;
+    double tau;  // lattice units (it * dtau)
+    double a;
+    State<double> s;
+    double *T10;  // [10][n]: tautau xx yy etaeta taux tauy taueta xy xeta yeta
+};
+void launch_tmunu(const TmunuArgs &a, cudaStream_t st);
+
+struct LandauArgs {
+    int N;
+    double tau_fm;        // it * dtau * a
+    double tau2_fm;       // a * it * dtau * a * it * dtau (MyEigen.cpp:101)
+    double tau_fm_parts[3];  // it, dtau, a (for eps/3/it/dtau/a/it/dtau/a)
+    const double *T10;
+    double *eps;     // [n]
+    double *u4;      // [4][n]
+    double *pi10;    // [10][n]
+    int *found;      // [n]
+};
+void launch_landau(const LandauArgs &a, double *carry, int *wrote,
+                   cudaStream_t st);
+
+// reductions; out receives the per-event scalars
+struct Reductions {
+    double gauss_max;
+    double unitarity_max;
+    double etot;
+};
+// d_partial needs ceil(N*N/256) * 18 doubles
+void launch_gauss_law(int N, const State<double> &s, double *d_partial,
+                      double *d_out, cudaStream_t st);
+void launch_unitarity(int N, const C<double> *ux, const C<double> *uy,
+                      double *d_partial, double *d_out, cudaStream_t st);
+// sums1[5] = {sum x w, sum y w, sum w, sum T^tautau, sum eps},
+// sums2[18] = radial moments (see reduce.cu)
+void launch_eccentricity(int N, double L, double a, const double *eps,
+                         const double *utau, const double *Ttt,
+                         double *d_partial, double *d_sums1, double *d_sums2,
+                         cudaStream_t st);
+
+template <typename T>
+void launch_convert_state(size_t n, const State<T> &src, State<double> &dst,
+                          cudaStream_t st);
+template <typename T>
+void launch_convert_state_down(size_t n, const State<double> &src,
+                               State<T> &dst, cudaStream_t st);
+
+}  // namespace ipg

@@ -1,0 +1,63 @@
+// Counter-based Philox4x32-10 generator (Salmon, Moraes, Dror, Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC'11) and Box-Muller
+// normals. Used for the device-side colour-charge noise and the Newton
+// restart draws: every (nucleus, sheet, site, colour) gets its own counter,
+// so draws are independent of the launch shape.
+#pragma once
+
+#include <cstdint>
+
+namespace ipg {
+
+struct U4 {
+    uint32_t x, y, z, w;
+};
+
+__host__ __device__ __forceinline__ uint32_t mulhilo(uint32_t a, uint32_t b,
+                                                     uint32_t *hi) {
+    uint64_t p = (uint64_t)a * (uint64_t)b;
+    *hi = (uint32_t)(p >> 32);
+    return (uint32_t)p;
+}
+
+__host__ __device__ __forceinline__ U4 philox4x32_10(U4 ctr, uint32_t k0,
+                                                     uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        uint32_t hi0, hi1;
+        uint32_t lo0 = mulhilo(M0, ctr.x, &hi0);
+        uint32_t lo1 = mulhilo(M1, ctr.z, &hi1);
+        ctr = {hi1 ^ ctr.y ^ k0, lo1, hi0 ^ ctr.w ^ k1, lo0};
+        k0 += W0;
+        k1 += W1;
+    }
+    return ctr;
+}
+
+// uniform in (0, 1]
+__host__ __device__ __forceinline__ double u01(uint32_t a, uint32_t b) {
+    uint64_t v = ((uint64_t)a << 21) ^ (uint64_t)b;  // 53 random bits
+    v &= ((1ull << 53) - 1);
+    return ((double)v + 1.0) * (1.0 / 9007199254740992.0);
+}
+
+// four standard normals from one counter
+__device__ __forceinline__ void normal4(U4 ctr, uint64_t key, double out[4]) {
+    U4 r = philox4x32_10(ctr, (uint32_t)key, (uint32_t)(key >> 32));
+    U4 r2 = philox4x32_10({ctr.x, ctr.y, ctr.z, ctr.w ^ 0x80000000u},
+                          (uint32_t)key, (uint32_t)(key >> 32));
+    double u1 = u01(r.x, r.y), u2 = u01(r.z, r.w);
+    double u3 = u01(r2.x, r2.y), u4 = u01(r2.z, r2.w);
+    double rad1 = sqrt(-2.0 * log(u1)), rad2 = sqrt(-2.0 * log(u3));
+    double s1, c1, s2, c2;
+    sincospi(2.0 * u2, &s1, &c1);
+    sincospi(2.0 * u4, &s2, &c2);
+    out[0] = rad1 * c1;
+    out[1] = rad1 * s1;
+    out[2] = rad2 * c2;
+    out[3] = rad2 * s2;
+}
+
+}  // namespace ipg

@@ -1,0 +1,270 @@
+// Per-event reductions with FP64 accumulation: Gauss-law violation
+// (Evolution::checkGaussLaw, Evolution.cpp:295-364), link unitarity,
+// total energy and the eccentricities epsilon_n, Psi_n
+// (Evolution::eccentricity, Evolution.cpp:1280-1810, cutoff 0, constant
+// coupling). Sums are deterministic: each block writes a partial in a fixed
+// order and one block folds the partials, so repeated runs agree bit for bit.
+#include <cstdint>
+
+#include "fields.cuh"
+#include "ipg_internal.h"
+
+namespace ipg {
+
+namespace {
+
+constexpr int RB = 256;  // threads per reduction block
+
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double *out) {
+    __shared__ double sh[K][RB / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        double x = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[k][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double s = 0.;
+        for (int w = 0; w < RB / 32; w++) s += sh[threadIdx.x][w];
+        out[threadIdx.x] = s;
+    }
+}
+
+__device__ __forceinline__ double block_max(double v) {
+    __shared__ double sh[RB / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double m = 0.;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < RB / 32; w++) m = fmax(m, sh[w]);
+    return m;
+}
+
+// fold `nb` partial rows of K values into out[K]
+template <int K>
+__global__ void k_fold(const double *partial, int nb, double *out) {
+    const int k = threadIdx.x;
+    if (k >= K) return;
+    double s = 0.;
+    for (int b = 0; b < nb; b++) s += partial[(size_t)b * K + k];
+    out[k] = s;
+}
+
+__global__ void k_fold_max(const double *partial, int nb, double *out) {
+    if (threadIdx.x != 0) return;
+    double m = 0.;
+    for (int b = 0; b < nb; b++) m = fmax(m, partial[b]);
+    *out = m;
+}
+
+}  // namespace
+
+// --------------------------------------------------------------------------
+// Gauss law: G = UxXm1^dag E1(x-1) UxXm1 - E1 + UyYm1^dag E2(y-1) UyYm1 - E2
+//               - i (phi pi - pi phi);  max over sites of |G|^2 / 2
+// --------------------------------------------------------------------------
+__global__ void k_gauss(int N, State<double> s, double *partial) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * RB + threadIdx.x;
+    double val = 0.;
+    if (pos < n) {
+        const int ix = (int)(pos / N), iy = (int)(pos % N);
+        const size_t mX = (size_t)max(0, ix - 1) * N + iy;
+        const size_t mY = (size_t)ix * N + max(0, iy - 1);
+        M3<double> G = mul(mul_dn(ld_m3(s.ux, mX, n), from_h(ld_h8(s.e1, mX, n))),
+                           ld_m3(s.ux, mX, n));
+        sub_from(G, from_h(ld_h8(s.e1, pos, n)));
+        add_to(G, mul(mul_dn(ld_m3(s.uy, mY, n), from_h(ld_h8(s.e2, mY, n))),
+                      ld_m3(s.uy, mY, n)));
+        sub_from(G, from_h(ld_h8(s.e2, pos, n)));
+        const M3<double> ph = from_h(ld_h(s.phi, pos, n)), pi = from_h(ld_h(s.pi, pos, n));
+        const M3<double> c = minus(mul(ph, pi), mul(pi, ph));
+        // - i c
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            G.m[k].r += c.m[k].i;
+            G.m[k].i -= c.m[k].r;
+        }
+        double sq = 0.;
+#pragma unroll
+        for (int k = 0; k < 9; k++) sq += G.m[k].r * G.m[k].r + G.m[k].i * G.m[k].i;
+        val = 0.5 * sq;
+    }
+    const double m = block_max(val);
+    if (threadIdx.x == 0) partial[blockIdx.x] = m;
+}
+
+void launch_gauss_law(int N, const State<double> &s, double *d_partial,
+                      double *d_out, cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    const int nb = (int)((n + RB - 1) / RB);
+    k_gauss<<<nb, RB, 0, st>>>(N, s, d_partial);
+    k_fold_max<<<1, 32, 0, st>>>(d_partial, nb, d_out);
+}
+
+// --------------------------------------------------------------------------
+// max over links of the largest |(U^dag U - 1)_ij|
+// --------------------------------------------------------------------------
+__global__ void k_unitarity(int N, const C<double> *ux, const C<double> *uy,
+                            double *partial) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * RB + threadIdx.x;
+    double val = 0.;
+    if (pos < n) {
+        for (int d = 0; d < 2; d++) {
+            const M3<double> u = ld_m3(d ? uy : ux, pos, n);
+            M3<double> p = mul_dn(u, u);
+            p.m[0].r -= 1.;
+            p.m[4].r -= 1.;
+            p.m[8].r -= 1.;
+#pragma unroll
+            for (int k = 0; k < 9; k++)
+                val = fmax(val, sqrt(p.m[k].r * p.m[k].r + p.m[k].i * p.m[k].i));
+        }
+    }
+    const double m = block_max(val);
+    if (threadIdx.x == 0) partial[blockIdx.x] = m;
+}
+
+void launch_unitarity(int N, const C<double> *ux, const C<double> *uy,
+                      double *d_partial, double *d_out, cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    const int nb = (int)((n + RB - 1) / RB);
+    k_unitarity<<<nb, RB, 0, st>>>(N, ux, uy, d_partial);
+    k_fold_max<<<1, 32, 0, st>>>(d_partial, nb, d_out);
+}
+
+// --------------------------------------------------------------------------
+// eccentricities
+// --------------------------------------------------------------------------
+// pass 1: sum x w, y w, w, T^tautau, eps   (w = eps u^tau where eps >= 0)
+__global__ void k_ecc1(int N, double L, double a, const double *eps,
+                       const double *utau, const double *Ttt,
+                       double *partial) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * RB + threadIdx.x;
+    double v[5] = {0., 0., 0., 0., 0.};
+    if (pos < n) {
+        const int ix = (int)(pos / N), iy = (int)(pos % N);
+        const double x = -L / 2. + a * ix, y = -L / 2. + a * iy;
+        const double e = eps[pos];
+        const double w = (e < 0.) ? 0. : e * utau[pos];
+        v[0] = x * w;
+        v[1] = y * w;
+        v[2] = w;
+        v[3] = Ttt[pos];
+        v[4] = e;
+    }
+    block_sum<5>(v, partial + (size_t)blockIdx.x * 5);
+}
+
+// pass 2 over [2, N-2)^2 about the centroid: r^n, r^n cos(n phi), r^n sin(n phi)
+// in the reference's choice of powers (avr1 and the n = 1 moments use r^3)
+__global__ void k_ecc2(int N, double L, double a, const double *eps,
+                       const double *utau, const double *cent,
+                       double *partial) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * RB + threadIdx.x;
+    double v[18];
+#pragma unroll
+    for (int k = 0; k < 18; k++) v[k] = 0.;
+    if (pos < n) {
+        const int ix = (int)(pos / N), iy = (int)(pos % N);
+        if (ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2) {
+            const double avx = cent[0] / cent[2], avy = cent[1] / cent[2];
+            const double x = -L / 2. + a * ix - avx, y = -L / 2. + a * iy - avy;
+            double phiA;
+            if (x >= 0) {
+                phiA = atan(y / x);
+                if (x == 0) phiA = (y >= 0) ? M_PI / 2. : 3. * M_PI / 2.;
+            } else {
+                phiA = atan(y / x) + M_PI;
+            }
+            const double e = eps[pos];
+            const double w = (e < 0.) ? 0. : e * utau[pos];
+            const double r = sqrt(x * x + y * y);
+            const double r2 = r * r, r3 = r * r * r, r4 = r * r * r * r;
+            const double r5 = r * r * r * r * r, r6 = r * r * r * r * r * r;
+            // 0..5: avr1 avrSq avr3 avr4 avr5 avr6
+            v[0] = r3 * w;
+            v[1] = r2 * w;
+            v[2] = r3 * w;
+            v[3] = r4 * w;
+            v[4] = r5 * w;
+            v[5] = r6 * w;
+            // 6..17: cos/sin moments for n = 1..6
+            v[6] = r3 * cos(phiA) * w;
+            v[7] = r3 * sin(phiA) * w;
+            v[8] = r2 * cos(2. * phiA) * w;
+            v[9] = r2 * sin(2. * phiA) * w;
+            v[10] = r3 * cos(3. * phiA) * w;
+            v[11] = r3 * sin(3. * phiA) * w;
+            v[12] = r4 * cos(4. * phiA) * w;
+            v[13] = r4 * sin(4. * phiA) * w;
+            v[14] = r5 * cos(5. * phiA) * w;
+            v[15] = r5 * sin(5. * phiA) * w;
+            v[16] = r6 * cos(6. * phiA) * w;
+            v[17] = r6 * sin(6. * phiA) * w;
+        }
+    }
+    block_sum<18>(v, partial + (size_t)blockIdx.x * 18);
+}
+
+void launch_eccentricity(int N, double L, double a, const double *eps,
+                         const double *utau, const double *Ttt,
+                         double *d_partial, double *d_sums1,
+                         double *d_sums2, cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    const int nb = (int)((n + RB - 1) / RB);
+    k_ecc1<<<nb, RB, 0, st>>>(N, L, a, eps, utau, Ttt, d_partial);
+    k_fold<5><<<1, 32, 0, st>>>(d_partial, nb, d_sums1);
+    k_ecc2<<<nb, RB, 0, st>>>(N, L, a, eps, utau, d_sums1, d_partial);
+    k_fold<18><<<1, 32, 0, st>>>(d_partial, nb, d_sums2);
+}
+
+// --------------------------------------------------------------------------
+// FP32 <-> FP64 state conversion
+// --------------------------------------------------------------------------
+template <typename S, typename D>
+__global__ void k_convert(size_t n, State<S> src, State<D> dst) {
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        dst.ux[k * n + pos] = {(D)src.ux[k * n + pos].r, (D)src.ux[k * n + pos].i};
+        dst.uy[k * n + pos] = {(D)src.uy[k * n + pos].r, (D)src.uy[k * n + pos].i};
+        dst.phi[k * n + pos] = (D)src.phi[k * n + pos];
+        dst.pi[k * n + pos] = (D)src.pi[k * n + pos];
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        dst.e1[k * n + pos] = (D)src.e1[k * n + pos];
+        dst.e2[k * n + pos] = (D)src.e2[k * n + pos];
+    }
+}
+
+template <typename T>
+void launch_convert_state(size_t n, const State<T> &src, State<double> &dst,
+                          cudaStream_t st) {
+    k_convert<T, double><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, src, dst);
+}
+
+template <typename T>
+void launch_convert_state_down(size_t n, const State<double> &src,
+                               State<T> &dst, cudaStream_t st) {
+    k_convert<double, T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, src, dst);
+}
+
+template void launch_convert_state<float>(size_t, const State<float> &,
+                                          State<double> &, cudaStream_t);
+template void launch_convert_state_down<float>(size_t, const State<double> &,
+                                               State<float> &, cudaStream_t);
+
+}  // namespace ipg
