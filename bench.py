@@ -1,0 +1,454 @@
+"""Benchmark of the IP-Glasma hot path on B200.
+
+One step = one Pb+Pb event of the 512^2 workload (L = 40 fm, b = 6 fm,
+Ny = 50, tau up to 0.6 fm/c, 77 leapfrog steps): colour-charge noise ->
+Poisson solve -> Wilson lines -> tau = 0 Newton links -> leapfrog ->
+T^{mu nu} + Landau matching + eccentricities. Each step draws fresh noise
+(device Philox, new key per event) on the same g^2 mu^2 maps, which stay
+resident in HBM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Reported (one JSON line, rank 0):
+  value       events/s of the FP32-bulk form (whole job, all ranks)
+  fp64        the plain FP64 form on the same events
+  error       FP32-bulk vs FP64 on the same event: per-cell e, epsilon_2, E_T
+  e2e         the same events through the C ABI with host buffers: g^2 mu^2
+              maps copied in and e, u, pi, T^{mu nu} copied out every event
+  roofline    the fused leapfrog kernel of the FP32 form against measured HBM
+  cpu_baseline the reference (oracle/_ref, OpenMP, all host cores) on a
+              bounded sample of the same event, scaled to one event
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = dict(name="PbPb_512", N=512, L=40.0, nucleus="Pb", b=6.0, Ny=50,
+                maxtime=0.6, g=2.0, m=0.2)
+METRIC = "site-updates/s & events/s: FP32-batched vs plain FP64 at stated err; adjoint/fwd"
+# algorithmic bytes per site-update of the fused leapfrog: every state word read
+# once and written once (links 2 x 18, E 2 x 8, phi 9, pi 9 = 70 reals)
+BYTES_PER_SITE_UPDATE = {"fp32": 2 * 70 * 4, "fp64": 2 * 70 * 8}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(
+                    ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                     "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                parts = [p.strip() for p in out.stdout.strip().split(",")]
+                if len(parts) == 7:
+                    self.samples.append(parts)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if s[3 + k].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def make_inputs():
+    from ipglasma_b200.synthetic import make_event
+    w = WORKLOAD
+    A, B, _, _ = make_event(w["N"], w["L"], w["nucleus"], w["b"], seed=11, g=w["g"])
+    return A, B
+
+
+def cfg_for(precision: int, seed: int):
+    import ipglasma_b200 as ipg
+    w = WORKLOAD
+    return ipg.Config(size=w["N"], L=w["L"], Ny=w["Ny"], g=w["g"], m=w["m"],
+                      maxtime=w["maxtime"], precision=precision, seed=seed)
+
+
+def flush_l2(torch, buf):
+    buf.fill_(1.0)  # 256 MB > 126 MB L2
+
+
+def run_events(torch, ev, d_A, d_B, K, seed0, l2buf, host=None):
+    """K events on one context; returns (device ms per event list, leapfrog ms)."""
+    import ctypes as ct
+    lib = ev._lib
+    times, lf = [], []
+    for k in range(K):
+        flush_l2(torch, l2buf)
+        torch.cuda.synchronize()
+        st = torch.cuda.Event(enable_timing=True)
+        en = torch.cuda.Event(enable_timing=True)
+        st.record()
+        ev_reset(ev, seed0 + k)
+        ev.set_g2mu_device(d_A.data_ptr(), d_B.data_ptr())
+        ev.use_device_noise()
+        ev.init_fields(allow_nonconverged=True)
+        ev.run()
+        en.record()
+        torch.cuda.synchronize()
+        times.append(st.elapsed_time(en))
+        lf.append(ev.last_leapfrog_ms()[0])
+    return times, lf
+
+
+def ev_reset(ev, seed):
+    """Re-key the device noise of an existing context (no reallocation)."""
+    ev.reseed(seed)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", choices=["fp32", "fp64", "both"], default=None,
+                    help="run one warm-up and one timed event per form and exit "
+                         "(the command profiled under ncu)")
+    args = ap.parse_args()
+    world, rank, local = dist_env()
+    if args.profile:
+        return run_profile(args.profile, local)
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    return run_ours(args, world, rank, local)
+
+
+def run_profile(which, local):
+    import torch
+    import ipglasma_b200 as ipg
+
+    torch.cuda.set_device(local)
+    A, B = make_inputs()
+    d_A = torch.tensor(A, dtype=torch.float64, device="cuda")
+    d_B = torch.tensor(B, dtype=torch.float64, device="cuda")
+    l2buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    forms = {"fp32": [ipg.FP32], "fp64": [ipg.FP64], "both": [ipg.FP32, ipg.FP64]}[which]
+    for prec in forms:
+        ev = ipg.Event(cfg_for(prec, 77))
+        t, lf = run_events(torch, ev, d_A, d_B, 2, 77, l2buf)
+        print(f"precision={prec} event_ms={t} leapfrog_ms={lf}")
+        ev.close()
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    import ipglasma_b200 as ipg
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = dist_mod
+    K, W = args.steps, max(3, args.warmup)
+    A, B = make_inputs()
+    d_A = torch.tensor(A, dtype=torch.float64, device="cuda")
+    d_B = torch.tensor(B, dtype=torch.float64, device="cuda")
+    l2buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    N = WORKLOAD["N"]
+    seed_base = 1000 * (rank + 1)
+
+    ev32 = ipg.Event(cfg_for(ipg.FP32, seed_base))
+    ev64 = ipg.Event(cfg_for(ipg.FP64, seed_base))
+    itmax = ev32.itmax
+    launches0 = ev32.kernel_launches()
+
+    # warm-up (untimed)
+    run_events(torch, ev32, d_A, d_B, W, seed_base, l2buf)
+    run_events(torch, ev64, d_A, d_B, min(W, 3), seed_base, l2buf)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # --- timed: FP32-bulk form (the headline) -------------------------------
+    launches_before = ev32.kernel_launches()
+    with ClockSampler(local) as clk:
+        barrier()
+        t32, lf32 = run_events(torch, ev32, d_A, d_B, K, seed_base + 100, l2buf)
+        barrier()
+    launches_timed = ev32.kernel_launches() - launches_before
+    # --- timed: plain FP64 form ----------------------------------------------
+    barrier()
+    t64, lf64 = run_events(torch, ev64, d_A, d_B, K, seed_base + 100, l2buf)
+    barrier()
+
+    ms32 = float(np.sum(t32))
+    ms64 = float(np.sum(t64))
+    if dist:
+        tt = torch.tensor([ms32, ms64], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms32, ms64 = tt.tolist()
+    ev_per_s32 = world * K / (ms32 * 1e-3)
+    ev_per_s64 = world * K / (ms64 * 1e-3)
+    su32 = N * N * itmax / (np.mean(lf32) * 1e-3)
+    su64 = N * N * itmax / (np.mean(lf64) * 1e-3)
+
+    # --- error of the FP32 form against FP64 on one event -------------------
+    err = compare_forms(ev32, ev64, d_A, d_B, seed_base + 7)
+
+    # --- end to end through the C ABI with host buffers ---------------------
+    e2e = measure_e2e(torch, ipg, A, B, K, seed_base + 500, l2buf, dist)
+    if dist:
+        et = torch.tensor([e2e["ms"]], dtype=torch.float64, device="cuda")
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        e2e["ms"] = et.item()
+
+    peaks = load_peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    achieved = su32 * BYTES_PER_SITE_UPDATE["fp32"] / 1e9
+    traffic = load_traffic()
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(achieved / hbm, 4), "traffic": traffic,
+            "kernel": "k_leapfrog<float> (FP32 bulk)",
+            "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp32"],
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "fp64_kernel": {"achieved": round(su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9, 1),
+                            "frac": round(su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9 / hbm, 4),
+                            "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp64"]}}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample()
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": round(ev_per_s32, 3),
+            "unit": "events/s",
+            "n_gpus": world,
+            "steps": K,
+            "warmup": W,
+            "ms_per_step": round(ms32 / K, 3),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 (FP64 Newton, Wilson lines, observables, reductions)",
+            "data": "synthetic (seeded Woods-Saxon Pb+Pb, g2mu ~ sqrt(T_A), device Philox noise)",
+            "config": {"workload": WORKLOAD["name"], "N": N, "L_fm": WORKLOAD["L"],
+                       "Ny": WORKLOAD["Ny"], "b_fm": WORKLOAD["b"], "tau_fm": WORKLOAD["maxtime"],
+                       "leapfrog_steps": itmax, "events_per_gpu": K,
+                       "l2": "flushed (256 MB write) before every event",
+                       "parallelism": f"events sharded over {world} GPU(s), no collective"},
+            "site_updates_per_s": round(world * su32, 1),
+            "fp64": {"events_per_s": round(ev_per_s64, 3), "ms_per_event": round(ms64 / K, 3),
+                     "site_updates_per_s": round(world * su64, 1)},
+            "fp32_over_fp64_events": round(ev_per_s32 / ev_per_s64, 3),
+            "error": err,
+            "e2e": {"value": round(world * K / (e2e["ms"] * 1e-3), 3), "unit": "events/s",
+                    "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
+                    "form": "fp32"},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "gpu_launches": int(launches_timed),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    ev32.close()
+    ev64.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def compare_forms(ev32, ev64, d_A, d_B, seed):
+    outs = {}
+    for name, ev in (("fp32", ev32), ("fp64", ev64)):
+        ev_reset(ev, seed)
+        ev.set_g2mu_device(d_A.data_ptr(), d_B.data_ptr())
+        ev.use_device_noise()
+        ev.init_fields(allow_nonconverged=True)
+        res = ev.run()
+        eps = ev.observables()[0]
+        outs[name] = (eps, res)
+    e32, r32 = outs["fp32"]
+    e64, r64 = outs["fp64"]
+    out = {}
+    for frac in (1e-2, 1e-3):
+        m = e64 > frac * e64.max()
+        rel = np.abs(e32[m] - e64[m]) / np.abs(e64[m])
+        out[f"e_rel_max_gt{frac:g}max"] = float(rel.max())
+        out[f"e_rel_rms_gt{frac:g}max"] = float(np.sqrt(np.mean(rel ** 2)))
+    out["eps2_rel"] = abs(r32.eccentricity[1] - r64.eccentricity[1]) / abs(r64.eccentricity[1])
+    out["E_T_rel"] = abs(r32.E_T - r64.E_T) / abs(r64.E_T)
+    out["gauss_fp32"] = r32.gauss_violation
+    out["gauss_fp64"] = r64.gauss_violation
+    out["unitarity_fp32"] = r32.unitarity_max
+    out["unitarity_fp64"] = r64.unitarity_max
+    return out
+
+
+def measure_e2e(torch, ipg, A, B, K, seed0, l2buf, dist):
+    """Events through the C ABI with host buffers: g2mu maps in, observables out."""
+    ev = ipg.Event(cfg_for(ipg.FP32, seed0))
+    n = ev.n
+    hA = np.ascontiguousarray(A)
+    hB = np.ascontiguousarray(B)
+    eps, u4, pi10, T10 = np.empty(n), np.empty((4, n)), np.empty((10, n)), np.empty((10, n))
+    import ctypes as ct
+
+    def one(seed):
+        ev_reset(ev, seed)
+        ev.set_g2mu(hA, hB)
+        ev.use_device_noise()
+        ev.init_fields(allow_nonconverged=True)
+        ev.run()
+        ev._check(ev._lib.ipg_get_observables(ev._h, ct.c_void_p(eps.ctypes.data),
+                                              ct.c_void_p(u4.ctypes.data),
+                                              ct.c_void_p(pi10.ctypes.data),
+                                              ct.c_void_p(T10.ctypes.data)))
+    for k in range(3):
+        one(seed0 + k)
+    total = 0.0
+    for k in range(K):
+        flush_l2(torch, l2buf)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        one(seed0 + 10 + k)
+        torch.cuda.synchronize()
+        total += time.perf_counter() - t0
+    ev.close()
+    return {"ms": total * 1e3, "h2d": int(2 * n * 8), "d2h": int(25 * n * 8)}
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return {}
+    return {}
+
+
+def load_traffic():
+    """DRAM bytes per launch of the FP32 leapfrog kernel from the committed ncu
+    summary (profiles/leapfrog_fp32_PbPb512.json), or None."""
+    p = ROOT / "profiles" / "leapfrog_fp32_PbPb512.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get("dram_bytes_per_launch")
+        except Exception:
+            return None
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference itself (oracle/_ref), all host cores
+# ---------------------------------------------------------------------------
+SAMPLE = dict(N=128, L=10.0, Ny=50)  # same lattice spacing as the 512^2 event
+
+
+def cpu_baseline_sample(threads: int | None = None):
+    """Time the reference on a bounded sample of the workload: the same lattice
+    spacing (a = 0.078125 fm), Ny, tau and schedule on a 128^2 patch centred on
+    a Pb+Pb collision; scaled by the site count (512^2 / 128^2 = 16) to one
+    event, which is how every stage of the reference scales (the FFTs by a
+    further log factor, ignored here in the reference's favour)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from refcase import HARNESS, run_harness
+    from ipglasma_b200.synthetic import make_event
+    if not HARNESS.exists():
+        return {"value": None, "unit": "events/s", "cores": 0, "kind": "reference",
+                "sample": "oracle/_ref/ipg_ref_harness not built"}
+    threads = threads or os.cpu_count() or 1
+    s = SAMPLE
+    A, B, _, _ = make_event(s["N"], s["L"], WORKLOAD["nucleus"], WORKLOAD["b"], seed=11)
+    with tempfile.TemporaryDirectory() as tmp:
+        t0 = time.perf_counter()
+        r = run_harness(Path(tmp) / "ref", A, B, s["N"], s["L"], s["Ny"], WORKLOAD["g"],
+                        WORKLOAD["m"], 5, WORKLOAD["maxtime"], threads=threads)
+        wall = time.perf_counter() - t0
+    scale = (WORKLOAD["N"] / s["N"]) ** 2
+    t_event = wall * scale
+    return {"value": round(1.0 / t_event, 6), "unit": "events/s", "cores": threads,
+            "kind": "reference",
+            "sample": (f"reference -O2 OpenMP harness, one event at N={s['N']} L={s['L']} fm "
+                       f"(same a, Ny={s['Ny']}, tau={WORKLOAD['maxtime']} fm) in {wall:.1f} s, "
+                       f"x{scale:.0f} sites -> {t_event:.1f} s per 512^2 event"),
+            "phases_s": {k: r.meta[k] for k in ("t_setV", "t_tau0", "t_evolution")}}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    K, W = args.steps, args.warmup
+    threads = os.cpu_count() or 1
+    vals = []
+    for k in range(max(1, min(K, 3))):
+        cb = cpu_baseline_sample(threads)
+        if cb["value"] is None:
+            print(json.dumps({"impl": "reference", "unavailable": cb["sample"]}))
+            return
+        vals.append(cb["value"])
+    v = float(np.mean(vals))
+    line = {"metric": METRIC, "value": round(v, 6), "unit": "events/s", "n_gpus": world,
+            "steps": len(vals), "warmup": 0, "ms_per_step": round(1e3 / v, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (same generator as the GPU arm)",
+            "config": {"workload": WORKLOAD["name"], "N": WORKLOAD["N"]},
+            "impl": "reference",
+            "cpu_baseline": dict(cb, value=round(v, 6)),
+            "e2e": {"value": round(v, 6), "unit": "events/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

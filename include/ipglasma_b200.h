@@ -109,6 +109,10 @@ const char *ipg_last_error(const ipg_ctx *ctx);
 ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out);
 ipg_status ipg_destroy(ipg_ctx *ctx);
 
+/* New key for the device random streams of the next ipg_init_fields (a new
+ * event on the same context, no reallocation). */
+ipg_status ipg_reseed(ipg_ctx *ctx, uint64_t seed);
+
 /* Effective dtau (lattice units) and leapfrog step count of ctx. */
 ipg_status ipg_time_grid(const ipg_ctx *ctx, double *dtau, int *itmax);
 

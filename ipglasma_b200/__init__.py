@@ -86,6 +86,7 @@ _SIGNATURES = {
     "ipg_last_error": (ct.c_char_p, [ct.c_void_p]),
     "ipg_create": (ct.c_int, [ct.POINTER(_Config), ct.POINTER(ct.c_void_p)]),
     "ipg_destroy": (ct.c_int, [ct.c_void_p]),
+    "ipg_reseed": (ct.c_int, [ct.c_void_p, ct.c_uint64]),
     "ipg_time_grid": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double), ct.POINTER(ct.c_int)]),
     "ipg_set_g2mu": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "ipg_set_g2mu_device": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
@@ -248,6 +249,10 @@ class Event:
     def set_noise_device(self, ptr_a: int, ptr_b: int) -> None:
         self._check(self._lib.ipg_set_noise_device(self._h, ct.c_void_p(ptr_a),
                                                    ct.c_void_p(ptr_b)))
+
+    def reseed(self, seed: int) -> None:
+        self.cfg.seed = seed
+        self._check(self._lib.ipg_reseed(self._h, seed))
 
     def use_device_noise(self) -> None:
         self._check(self._lib.ipg_use_device_noise(self._h))

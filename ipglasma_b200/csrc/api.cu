@@ -130,12 +130,6 @@ __global__ void k_identity(size_t n, C<double> *V) {
         V[k * n + pos] = {(k == 0 || k == 4 || k == 8) ? 1. : 0., 0.};
 }
 
-__global__ void k_count_nan(size_t n, const double *x, int *count) {
-    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (pos >= n) return;
-    if (!isfinite(x[pos])) atomicAdd(count, 1);
-}
-
 int ilog2(int v) {
     int l = 0;
     while ((1 << l) < v) l++;
@@ -400,6 +394,12 @@ ipg_status ipg_destroy(ipg_ctx *ctx) {
     return IPG_OK;
 }
 
+ipg_status ipg_reseed(ipg_ctx *ctx, uint64_t seed) {
+    if (!ctx) return IPG_ERR_BAD_CONFIG;
+    ctx->cfg.seed = seed;
+    return IPG_OK;
+}
+
 ipg_status ipg_time_grid(const ipg_ctx *ctx, double *dtau, int *itmax) {
     if (!ctx) return IPG_ERR_BAD_CONFIG;
     if (dtau) *dtau = ctx->dtau;
@@ -526,22 +526,16 @@ ipg_status ipg_init_fields(ipg_ctx *c, ipg_init_report *rep) {
     IPG_CUDA(c, cudaMemsetAsync(c->s64.e2, 0, sizeof(double) * 8 * n, c->stream));
     IPG_CUDA(c, cudaMemsetAsync(c->s64.phi, 0, sizeof(double) * 9 * n, c->stream));
     IPG_TRY(to_fp32_if_needed(c));
+    launch_newton_stats(2 * n, c->newton_iters, c->newton_status, c->partial,
+                        c->scal + 40, c->stream);
+    IPG_LAUNCHED(c, 2);
     IPG_CUDA(c, cudaEventRecord(e[3], c->stream));
+    double ns[4];
+    IPG_CUDA(c, cudaMemcpyAsync(ns, c->scal + 40, sizeof(ns), cudaMemcpyDeviceToHost,
+                                c->stream));
     IPG_TRY(sync(c));
-
-    std::vector<int> it(2 * n), stv(2 * n);
-    IPG_CUDA(c, cudaMemcpy(it.data(), c->newton_iters, sizeof(int) * 2 * n,
-                           cudaMemcpyDeviceToHost));
-    IPG_CUDA(c, cudaMemcpy(stv.data(), c->newton_status, sizeof(int) * 2 * n,
-                           cudaMemcpyDeviceToHost));
-    int restarted = 0, failed = 0, mx = 0;
-    double sum = 0;
-    for (size_t k = 0; k < 2 * n; k++) {
-        restarted += stv[k] >= 1;
-        failed += stv[k] == 2;
-        mx = std::max(mx, it[k]);
-        sum += it[k];
-    }
+    const int mx = (int)ns[0], restarted = (int)ns[2], failed = (int)ns[3];
+    const double sum = ns[1];
     if (rep) {
         rep->newton_links = (int)(2 * n);
         rep->newton_restarted = restarted;
@@ -653,23 +647,16 @@ ipg_status ipg_run(ipg_ctx *c, ipg_result *res) {
     IPG_LAUNCHED(c, 2);
     launch_unitarity(N, c->s64.ux, c->s64.uy, c->partial, scal + 33, c->stream);
     IPG_LAUNCHED(c, 2);
-    IPG_CUDA(c, cudaMemsetAsync(reinterpret_cast<int *>(scal + 34), 0, sizeof(int),
-                                c->stream));
-    k_count_nan<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
-        n, c->eps, reinterpret_cast<int *>(scal + 34));
-    IPG_LAUNCHED(c, 1);
+    launch_cell_flags(n, c->found, c->eps, c->partial, scal + 36, c->stream);
+    IPG_LAUNCHED(c, 2);
     IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     IPG_TRY(sync(c));
     const double ms_obs = elapsed(c);
     c->finished = true;
 
     double h[40];
-    IPG_CUDA(c, cudaMemcpy(h, scal, sizeof(double) * 35, cudaMemcpyDeviceToHost));
-    std::vector<int> found(n);
-    IPG_CUDA(c, cudaMemcpy(found.data(), c->found, sizeof(int) * n,
-                           cudaMemcpyDeviceToHost));
-    int nan_count = 0;
-    std::memcpy(&nan_count, &h[34], sizeof(int));
+    IPG_CUDA(c, cudaMemcpy(h, scal, sizeof(double) * 38, cudaMemcpyDeviceToHost));
+    const int nan_count = (int)h[37];
     if (res) {
         std::memset(res, 0, sizeof(*res));
         res->itmax = itmax;
@@ -689,9 +676,7 @@ ipg_status ipg_run(ipg_ctx *c, ipg_result *res) {
             res->eccentricity[k] = std::sqrt(cs * cs + sn * sn) / avr[k];
             res->psi[k] = (std::atan(sn / cs) + M_PI) / (k + 1);
         }
-        int nf = 0;
-        for (size_t p = 0; p < n; p++) nf += found[p] == 0;
-        res->cells_without_u = nf;
+        res->cells_without_u = (int)h[36];
         res->ms_evolution = ms_evo;
         res->ms_observables = ms_obs;
     }

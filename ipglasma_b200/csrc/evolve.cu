@@ -200,18 +200,292 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+// ===========================================================================
+// FP32 bulk form: links stored as their deviation from the identity,
+// W = U - 1. Every product of links is formed as
+//   (1 + a)(1 + b) - 1 = a + b + ab,
+// so plaquettes, staples and parallel transports keep FP32 *relative*
+// precision on the small deviations that carry the physics; the identity
+// part (which would swallow them in a plain FP32 3x3) cancels exactly in
+// U - U^dag and in U phi U^dag - phi. The observables are evaluated in FP64
+// from U = 1 + W. Links are reunitarised every step (Gram-Schmidt on the
+// first two rows, third row = conj(row0 x row1), as Matrix::reu,
+// Matrix.h:67-109), also in deviation form.
+// ===========================================================================
+
+// (1+a)(1+b) - 1
+template <typename T>
+__device__ __forceinline__ M3<T> dmul(const M3<T> &a, const M3<T> &b) {
+    M3<T> c = mul(a, b);
+    add_to(c, a);
+    add_to(c, b);
+    return c;
+}
+// (1+a)(1+b)^dag - 1
+template <typename T>
+__device__ __forceinline__ M3<T> dmul_nd(const M3<T> &a, const M3<T> &b) {
+    M3<T> c = mul_nd(a, b);
+    add_to(c, a);
+    add_to(c, dagger(b));
+    return c;
+}
+// (1+a)^dag (1+b) - 1
+template <typename T>
+__device__ __forceinline__ M3<T> dmul_dn(const M3<T> &a, const M3<T> &b) {
+    M3<T> c = mul_dn(a, b);
+    add_to(c, dagger(a));
+    add_to(c, b);
+    return c;
+}
+
+// connection part of (1+w) H (1+w)^dag, i.e. the transport minus H:
+// X + X^dag + X w^dag with X = w H
+template <typename T>
+__device__ __forceinline__ H3<T> transport_dev(const M3<T> &w, const H3<T> &h) {
+    const M3<T> x = mul(w, from_h(h));
+    const M3<T> y = mul_nd(x, w);
+    H3<T> o;
+    o.d0 = T(2) * x.m[0].r + y.m[0].r;
+    o.d1 = T(2) * x.m[4].r + y.m[4].r;
+    o.d2 = T(2) * x.m[8].r + y.m[8].r;
+    o.o01 = {x.m[1].r + x.m[3].r + y.m[1].r, x.m[1].i - x.m[3].i + y.m[1].i};
+    o.o02 = {x.m[2].r + x.m[6].r + y.m[2].r, x.m[2].i - x.m[6].i + y.m[2].i};
+    o.o12 = {x.m[5].r + x.m[7].r + y.m[5].r, x.m[5].i - x.m[7].i + y.m[5].i};
+    return o;
+}
+// connection part of (1+w)^dag H (1+w): X + X^dag + w^dag X with X = H w
+template <typename T>
+__device__ __forceinline__ H3<T> transport_dev_back(const M3<T> &w, const H3<T> &h) {
+    const M3<T> x = mul(from_h(h), w);
+    const M3<T> y = mul_dn(w, x);
+    H3<T> o;
+    o.d0 = T(2) * x.m[0].r + y.m[0].r;
+    o.d1 = T(2) * x.m[4].r + y.m[4].r;
+    o.d2 = T(2) * x.m[8].r + y.m[8].r;
+    o.o01 = {x.m[1].r + x.m[3].r + y.m[1].r, x.m[1].i - x.m[3].i + y.m[1].i};
+    o.o02 = {x.m[2].r + x.m[6].r + y.m[2].r, x.m[2].i - x.m[6].i + y.m[2].i};
+    o.o12 = {x.m[5].r + x.m[7].r + y.m[5].r, x.m[5].i - x.m[7].i + y.m[5].i};
+    return o;
+}
+
+template <typename T>
+__device__ __forceinline__ H3<T> h_diff(const H3<T> &a, const H3<T> &b) {
+    H3<T> r;
+    r.d0 = a.d0 - b.d0;
+    r.d1 = a.d1 - b.d1;
+    r.d2 = a.d2 - b.d2;
+    r.o01 = {a.o01.r - b.o01.r, a.o01.i - b.o01.i};
+    r.o02 = {a.o02.r - b.o02.r, a.o02.i - b.o02.i};
+    r.o12 = {a.o12.r - b.o12.r, a.o12.i - b.o12.i};
+    return r;
+}
+
+// 1/sqrt(1 + e) - 1 without cancellation
+template <typename T>
+__device__ __forceinline__ T inv_sqrt1p_m1(T e) {
+    const T s = sqrt(T(1) + e);
+    return -e / (s * (T(1) + s));
+}
+
+// Gram-Schmidt reunitarisation of U = 1 + w, in deviation form
+template <typename T>
+__device__ __forceinline__ void reunitarize_dev(M3<T> &w) {
+    // row 0: r0 = e0 + w0
+    {
+        const T e = T(2) * w.m[0].r + w.m[0].r * w.m[0].r + w.m[0].i * w.m[0].i +
+                    w.m[1].r * w.m[1].r + w.m[1].i * w.m[1].i + w.m[2].r * w.m[2].r +
+                    w.m[2].i * w.m[2].i;
+        const T f = inv_sqrt1p_m1(e);
+        w.m[0] = {w.m[0].r + f * (T(1) + w.m[0].r), w.m[0].i + f * w.m[0].i};
+        w.m[1] = {w.m[1].r + f * w.m[1].r, w.m[1].i + f * w.m[1].i};
+        w.m[2] = {w.m[2].r + f * w.m[2].r, w.m[2].i + f * w.m[2].i};
+    }
+    // row 1: r1 - <r0, r1> r0, proj = conj(r0) . r1
+    {
+        const C<T> a0 = w.m[0], a1 = w.m[1], a2 = w.m[2];
+        const C<T> b0 = w.m[3], b1 = w.m[4], b2 = w.m[5];
+        // (1 + conj a0) b0 + conj(a1) (1 + b1) + conj(a2) b2
+        C<T> pr = {b0.r + a1.r, b0.i - a1.i};
+        const C<T> t0 = cmulc(b0, a0), t1 = cmulc(b1, a1), t2 = cmulc(b2, a2);
+        pr.r += t0.r + t1.r + t2.r;
+        pr.i += t0.i + t1.i + t2.i;
+        const C<T> p0 = cmul(pr, a0), p1 = cmul(pr, a1), p2 = cmul(pr, a2);
+        w.m[3] = {b0.r - pr.r - p0.r, b0.i - pr.i - p0.i};
+        w.m[4] = {b1.r - p1.r, b1.i - p1.i};
+        w.m[5] = {b2.r - p2.r, b2.i - p2.i};
+        const T e = T(2) * w.m[4].r + w.m[3].r * w.m[3].r + w.m[3].i * w.m[3].i +
+                    w.m[4].r * w.m[4].r + w.m[4].i * w.m[4].i + w.m[5].r * w.m[5].r +
+                    w.m[5].i * w.m[5].i;
+        const T f = inv_sqrt1p_m1(e);
+        w.m[3] = {w.m[3].r + f * w.m[3].r, w.m[3].i + f * w.m[3].i};
+        w.m[4] = {w.m[4].r + f * (T(1) + w.m[4].r), w.m[4].i + f * w.m[4].i};
+        w.m[5] = {w.m[5].r + f * w.m[5].r, w.m[5].i + f * w.m[5].i};
+    }
+    // row 2 = conj((e0 + a) x (e1 + b)) - e2
+    {
+        const C<T> a0 = w.m[0], a1 = w.m[1], a2 = w.m[2];
+        const C<T> b0 = w.m[3], b1 = w.m[4], b2 = w.m[5];
+        const C<T> a1b2 = cmul(a1, b2), a2b1 = cmul(a2, b1), a2b0 = cmul(a2, b0);
+        const C<T> a0b2 = cmul(a0, b2), a0b1 = cmul(a0, b1), a1b0 = cmul(a1, b0);
+        const C<T> c0 = {a1b2.r - a2.r - a2b1.r, a1b2.i - a2.i - a2b1.i};
+        const C<T> c1 = {a2b0.r - b2.r - a0b2.r, a2b0.i - b2.i - a0b2.i};
+        const C<T> c2 = {a0.r + b1.r + a0b1.r - a1b0.r, a0.i + b1.i + a0b1.i - a1b0.i};
+        w.m[6] = {c0.r, -c0.i};
+        w.m[7] = {c1.r, -c1.i};
+        w.m[8] = {c2.r, -c2.i};
+    }
+}
+
+// (1 + t)(1 + w) - 1 with t = T2(i c E) - 1 = i c E - (c^2/2) E^2
+template <typename T>
+__device__ __forceinline__ M3<T> taylor2_update_dev(const H3<T> &e, T c,
+                                                    const M3<T> &w) {
+    const M3<T> em = from_h(e);
+    const M3<T> e2 = mul(em, em);
+    M3<T> t;
+    const T h = T(-0.5) * c * c;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        t.m[k].r = h * e2.m[k].r - c * em.m[k].i;
+        t.m[k].i = h * e2.m[k].i + c * em.m[k].r;
+    }
+    return dmul(t, w);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128)
+    k_leapfrog_dev(const EventGeom *__restrict__ ev, State<T> s, C<T> *wx_out,
+                   C<T> *wy_out, T *phi_out, StepCoef<T> cf) {
+    const int N = ev->N;
+    const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ix = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= N || iy >= N) return;
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)ix * N + iy;
+
+    if (cf.do_pe) {
+        const int ixp = min(N - 1, ix + 1), ixm = max(0, ix - 1);
+        const int iyp = min(N - 1, iy + 1), iym = max(0, iy - 1);
+        const size_t pX = (size_t)ixp * N + iy, mX = (size_t)ixm * N + iy;
+        const size_t pY = (size_t)ix * N + iyp, mY = (size_t)ix * N + iym;
+        const size_t mXpY = (size_t)ixm * N + iyp, pXmY = (size_t)ixp * N + iym;
+
+        const M3<T> wx = ld_m3(s.ux, pos, n);
+        const M3<T> wy = ld_m3(s.uy, pos, n);
+        H3<T> h12;
+        {
+            const M3<T> a = dmul(wx, ld_m3(s.uy, pX, n));
+            const M3<T> b = dmul(wy, ld_m3(s.ux, pY, n));
+            h12 = i_antiherm(dmul_nd(a, b));
+        }
+        H3<T> t1 = h12;
+        {
+            const M3<T> p = dmul_nd(wx, ld_m3(s.uy, pXmY, n));
+            const M3<T> q = dmul_dn(ld_m3(s.ux, mY, n), ld_m3(s.uy, mY, n));
+            h_add(t1, i_antiherm(dmul(p, q)));
+        }
+        H3<T> t2;
+        {
+            const M3<T> p = dmul_nd(wy, ld_m3(s.ux, mXpY, n));
+            const M3<T> q = dmul_dn(ld_m3(s.uy, mX, n), ld_m3(s.ux, mX, n));
+            t2 = i_antiherm(dmul(p, q));
+            h_axpy(t2, T(-1), h12);
+        }
+        h_traceless(t1);
+        h_traceless(t2);
+
+        const H3<T> phi = ld_h(s.phi, pos, n);
+        H3<T> pi = ld_h(s.pi, pos, n);
+        H3<T> e1 = ld_h8(s.e1, pos, n);
+        H3<T> e2 = ld_h8(s.e2, pos, n);
+        const T cst = cf.tau * cf.dt_pe / (T(2) * cf.g * cf.g);
+        const T cdt = cf.dt_pe / cf.tau;
+        h_axpy(e1, cst, t1);
+        h_axpy(e2, cst, t2);
+
+        // bracket = sum_dirs (phi_nb - phi) + connection parts
+        H3<T> br;
+        {
+            const H3<T> fX = ld_h(s.phi, pX, n);
+            const H3<T> cX = transport_dev(wx, fX);
+            H3<T> pt = fX;
+            h_add(pt, cX);
+            h_axpy(e1, cdt, i_commutator(pt, phi));
+            br = h_diff(fX, phi);
+            h_add(br, cX);
+        }
+        {
+            const H3<T> fY = ld_h(s.phi, pY, n);
+            const H3<T> cY = transport_dev(wy, fY);
+            H3<T> pt = fY;
+            h_add(pt, cY);
+            h_axpy(e2, cdt, i_commutator(pt, phi));
+            h_add(br, h_diff(fY, phi));
+            h_add(br, cY);
+        }
+        {
+            const H3<T> f = ld_h(s.phi, mX, n);
+            h_add(br, h_diff(f, phi));
+            h_add(br, transport_dev_back(ld_m3(s.ux, mX, n), f));
+        }
+        {
+            const H3<T> f = ld_h(s.phi, mY, n);
+            h_add(br, h_diff(f, phi));
+            h_add(br, transport_dev_back(ld_m3(s.uy, mY, n), f));
+        }
+        h_axpy(pi, cdt, br);
+        h_traceless(e1);
+        h_traceless(e2);
+        st_h(s.pi, pos, n, pi);
+        st_h8(s.e1, pos, n, e1);
+        st_h8(s.e2, pos, n, e2);
+
+        if (cf.do_pu) {
+            H3<T> phin = phi;
+            h_axpy(phin, (cf.tau + cf.dt_pu / T(2)) * cf.dt_pu, pi);
+            st_h(phi_out, pos, n, phin);
+            const T c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / T(2));
+            M3<T> nx = taylor2_update_dev(e1, c, wx);
+            reunitarize_dev(nx);
+            st_m3(wx_out, pos, n, nx);
+            M3<T> ny = taylor2_update_dev(e2, c, wy);
+            reunitarize_dev(ny);
+            st_m3(wy_out, pos, n, ny);
+        }
+    } else if (cf.do_pu) {
+        H3<T> phin = ld_h(s.phi, pos, n);
+        const H3<T> pi = ld_h(s.pi, pos, n);
+        h_axpy(phin, (cf.tau + cf.dt_pu / T(2)) * cf.dt_pu, pi);
+        st_h(phi_out, pos, n, phin);
+        const T c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / T(2));
+        M3<T> nx = taylor2_update_dev(ld_h8(s.e1, pos, n), c, ld_m3(s.ux, pos, n));
+        reunitarize_dev(nx);
+        st_m3(wx_out, pos, n, nx);
+        M3<T> ny = taylor2_update_dev(ld_h8(s.e2, pos, n), c, ld_m3(s.uy, pos, n));
+        reunitarize_dev(ny);
+        st_m3(wy_out, pos, n, ny);
+    }
+}
+
 template <typename T>
 void launch_leapfrog(const EventGeom *d_ev, int N, const State<T> &s,
                      C<T> *ux_out, C<T> *uy_out, T *phi_out,
                      const StepCoef<T> &cf, bool reunit, cudaStream_t st) {
     dim3 block(32, 4);
     dim3 grid((N + 31) / 32, (N + 3) / 4);
-    if (reunit)
-        k_leapfrog<T, true><<<grid, block, 0, st>>>(d_ev, s, ux_out, uy_out,
-                                                   phi_out, cf);
-    else
-        k_leapfrog<T, false><<<grid, block, 0, st>>>(d_ev, s, ux_out, uy_out,
-                                                    phi_out, cf);
+    if constexpr (sizeof(T) == 4) {
+        // FP32 bulk form: deviation storage, reunitarised every step
+        (void)reunit;
+        k_leapfrog_dev<T><<<grid, block, 0, st>>>(d_ev, s, ux_out, uy_out,
+                                                  phi_out, cf);
+    } else {
+        if (reunit)
+            k_leapfrog<T, true><<<grid, block, 0, st>>>(d_ev, s, ux_out, uy_out,
+                                                       phi_out, cf);
+        else
+            k_leapfrog<T, false><<<grid, block, 0, st>>>(d_ev, s, ux_out, uy_out,
+                                                        phi_out, cf);
+    }
 }
 
 template void launch_leapfrog<double>(const EventGeom *, int,

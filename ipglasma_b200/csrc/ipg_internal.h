@@ -125,6 +125,14 @@ void launch_eccentricity(int N, double L, double a, const double *eps,
                          double *d_partial, double *d_sums1, double *d_sums2,
                          cudaStream_t st);
 
+// out[4] = {max iterations, sum of iterations, restarted links, failed links};
+// d_partial needs 4 * ceil(links/256) doubles
+void launch_newton_stats(size_t links, const int *iters, const int *status,
+                         double *d_partial, double *d_out, cudaStream_t st);
+// out[2] = {cells without a time-like eigenvector, cells with non-finite e}
+void launch_cell_flags(size_t n, const int *found, const double *eps,
+                       double *d_partial, double *d_out, cudaStream_t st);
+
 template <typename T>
 void launch_convert_state(size_t n, const State<T> &src, State<double> &dst,
                           cudaStream_t st);

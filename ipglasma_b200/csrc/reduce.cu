@@ -232,14 +232,22 @@ void launch_eccentricity(int N, double L, double a, const double *eps,
 // --------------------------------------------------------------------------
 // FP32 <-> FP64 state conversion
 // --------------------------------------------------------------------------
+// The FP32 form stores links as their deviation from the identity, W = U - 1
+// (see k_leapfrog_dev): down-conversion forms U - 1 in FP64 before rounding,
+// up-conversion adds the identity back in FP64 (exact).
 template <typename S, typename D>
 __global__ void k_convert(size_t n, State<S> src, State<D> dst) {
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
+    const bool down = sizeof(D) < sizeof(S);
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-        dst.ux[k * n + pos] = {(D)src.ux[k * n + pos].r, (D)src.ux[k * n + pos].i};
-        dst.uy[k * n + pos] = {(D)src.uy[k * n + pos].r, (D)src.uy[k * n + pos].i};
+        const bool diag = (k == 0 || k == 4 || k == 8);
+        const double shift = diag ? (down ? -1.0 : 1.0) : 0.0;
+        dst.ux[k * n + pos] = {(D)((double)src.ux[k * n + pos].r + shift),
+                               (D)src.ux[k * n + pos].i};
+        dst.uy[k * n + pos] = {(D)((double)src.uy[k * n + pos].r + shift),
+                               (D)src.uy[k * n + pos].i};
         dst.phi[k * n + pos] = (D)src.phi[k * n + pos];
         dst.pi[k * n + pos] = (D)src.pi[k * n + pos];
     }
@@ -266,5 +274,69 @@ template void launch_convert_state<float>(size_t, const State<float> &,
                                           State<double> &, cudaStream_t);
 template void launch_convert_state_down<float>(size_t, const State<double> &,
                                                State<float> &, cudaStream_t);
+
+}  // namespace ipg
+
+namespace ipg {
+
+// Newton statistics: out[0] = max iterations, out[1] = sum of iterations,
+// out[2] = links that restarted, out[3] = links that failed (as doubles)
+__global__ void k_newton_stats(size_t links, const int *iters, const int *status,
+                               double *partial) {
+    const size_t k = (size_t)blockIdx.x * RB + threadIdx.x;
+    double v[4] = {0., 0., 0., 0.};
+    if (k < links) {
+        v[0] = iters[k];
+        v[1] = iters[k];
+        v[2] = status[k] >= 1;
+        v[3] = status[k] == 2;
+    }
+    // max in slot 0 via a separate max reduction, sums for the rest
+    const double m = block_max(v[0]);
+    double s[3] = {v[1], v[2], v[3]};
+    block_sum<3>(s, partial + (size_t)blockIdx.x * 4 + 1);
+    if (threadIdx.x == 0) partial[(size_t)blockIdx.x * 4] = m;
+}
+
+__global__ void k_fold_newton(const double *partial, int nb, double *out) {
+    if (threadIdx.x != 0) return;
+    double m = 0., s1 = 0., s2 = 0., s3 = 0.;
+    for (int b = 0; b < nb; b++) {
+        m = fmax(m, partial[4 * b]);
+        s1 += partial[4 * b + 1];
+        s2 += partial[4 * b + 2];
+        s3 += partial[4 * b + 3];
+    }
+    out[0] = m;
+    out[1] = s1;
+    out[2] = s2;
+    out[3] = s3;
+}
+
+void launch_newton_stats(size_t links, const int *iters, const int *status,
+                         double *d_partial, double *d_out, cudaStream_t st) {
+    const int nb = (int)((links + RB - 1) / RB);
+    k_newton_stats<<<nb, RB, 0, st>>>(links, iters, status, d_partial);
+    k_fold_newton<<<1, 32, 0, st>>>(d_partial, nb, d_out);
+}
+
+// number of cells with found == 0 and of non-finite e
+__global__ void k_cell_flags(size_t n, const int *found, const double *eps,
+                             double *partial) {
+    const size_t k = (size_t)blockIdx.x * RB + threadIdx.x;
+    double v[2] = {0., 0.};
+    if (k < n) {
+        v[0] = found[k] == 0;
+        v[1] = !isfinite(eps[k]);
+    }
+    block_sum<2>(v, partial + (size_t)blockIdx.x * 2);
+}
+
+void launch_cell_flags(size_t n, const int *found, const double *eps,
+                       double *d_partial, double *d_out, cudaStream_t st) {
+    const int nb = (int)((n + RB - 1) / RB);
+    k_cell_flags<<<nb, RB, 0, st>>>(n, found, eps, d_partial);
+    k_fold<2><<<1, 32, 0, st>>>(d_partial, nb, d_out);
+}
 
 }  // namespace ipg

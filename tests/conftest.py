@@ -1,0 +1,52 @@
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(Path(__file__).resolve().parent))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built library")
+
+
+def _ensure_oracle(target: str, path: Path) -> None:
+    if path.exists():
+        return
+    src = os.environ.get("IPG_REF_SRC", "/root/reference/src")
+    if target == "ref" and not Path(src).exists():
+        pytest.skip(f"{path} not built and the reference sources are absent")
+    subprocess.run(["make", "-C", str(ROOT / "oracle"), target, f"REF_SRC={src}"],
+                   check=True, capture_output=True)
+
+
+@pytest.fixture(scope="session")
+def oracle_port():
+    import oracle_port as op
+    _ensure_oracle("port", op.LIB)
+    return op
+
+
+@pytest.fixture(scope="session")
+def ref_harness():
+    import refcase
+    _ensure_oracle("ref", refcase.HARNESS)
+    return refcase
+
+
+@pytest.fixture(scope="session")
+def golden():
+    import json
+
+    import numpy as np
+
+    def load(name: str):
+        d = dict(np.load(ROOT / "tests" / "golden" / f"{name}.npz"))
+        d["meta"] = json.loads(str(d["meta"]))
+        return d
+
+    return load
