@@ -156,9 +156,13 @@ def main():
     ap.add_argument("--profile", choices=["fp32", "fp64", "both"], default=None,
                     help="run one warm-up and one timed event per form and exit "
                          "(the command profiled under ncu)")
+    ap.add_argument("--profile-n", type=int, default=512,
+                    help="lattice size of the profiled events (L = 40 fm)")
     args = ap.parse_args()
     world, rank, local = dist_env()
     if args.profile:
+        if args.profile_n != WORKLOAD["N"]:
+            WORKLOAD["N"] = args.profile_n
         return run_profile(args.profile, local)
     if args.impl == "reference":
         return run_reference(args, world, rank)

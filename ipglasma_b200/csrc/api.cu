@@ -326,7 +326,7 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
     const size_t n = c->n;
     IPG_TRY(dalloc(c, &c->g2mu2A, n));
     IPG_TRY(dalloc(c, &c->g2mu2B, n));
-    IPG_TRY(dalloc(c, &c->twiddle, (size_t)N / 2));
+    IPG_TRY(dalloc(c, &c->twiddle, (size_t)N));
     IPG_TRY(dalloc(c, &c->green, n));
     // work buffer of a sheet batch: ~64 MB so it stays in L2
     const size_t per_sheet = 4 * n * sizeof(double2);
@@ -358,13 +358,13 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
     IPG_TRY(dalloc(c, &c->carry, 5 * n));
     IPG_TRY(dalloc(c, &c->wrote, n));
     IPG_TRY(dalloc(c, &c->found, n));
-    IPG_TRY(dalloc(c, &c->partial, ((n + 255) / 256) * 18 + 64));
+    IPG_TRY(dalloc(c, &c->partial, 8192));  // 296 reduction blocks x <= 18 slots
     IPG_TRY(dalloc(c, &c->scal, 64));
     IPG_TRY(dalloc(c, &c->d_ev, 1));
 
     // twiddles exp(-2 pi i k/N), evaluated on the host in double precision
-    std::vector<double2> tw(N / 2);
-    for (int k = 0; k < N / 2; k++) {
+    std::vector<double2> tw(N);
+    for (int k = 0; k < N; k++) {
         const double ang = 2.0 * M_PI * (double)k / (double)N;
         tw[k] = make_double2(std::cos(ang), -std::sin(ang));
     }

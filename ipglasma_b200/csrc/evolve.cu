@@ -467,10 +467,187 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+// ===========================================================================
+// Direction-split leapfrog: two threads per site, thread d (0 = x, 1 = y)
+// owns the link U_d and the field E_d. The update of E_d, U_d and the share
+// of the pi bracket that comes from the +-d neighbours are symmetric under
+// x <-> y once written with the plaquette in the (d, o) orientation:
+//   P_do  = U_d U_o(x+d) U_d(x+o)^dag U_o^dag        (for d = x this is U12,
+//           for d = y it is U12^dag, so AH(P_do) = +-h12 as in evolveE)
+//   S_d   = (U_d U_o(x+d-o)^dag)(U_d(x-o)^dag U_o(x-o))   (U1m2 / U2m1)
+//   E_d  += tau dtau/(2 g^2) TL(AH(P_do) + AH(S_d)) + dtau/tau i[D_+d, phi]
+//   br_d  = D_+d + D_-d,  D_+d = U_d phi(x+d) U_d^dag - phi,
+//                         D_-d = U_d(x-d)^dag phi(x-d) U_d(x-d) - phi
+//   pi   += dtau/tau (br_x + br_y)           (br exchanged with a shuffle)
+// Each thread thus holds one direction's matrices, half the live state of a
+// one-thread-per-site kernel, which doubles the resident warps. DEV selects
+// the FP32 deviation storage W = U - 1 (products (1+a)(1+b) - 1 = a + b + ab,
+// reunitarised every step); otherwise links are full matrices (FP64 plain).
+// ===========================================================================
+template <typename T, bool DEV>
+__device__ __forceinline__ M3<T> lmul(const M3<T> &a, const M3<T> &b) {
+    if constexpr (DEV) return dmul(a, b);
+    else return mul(a, b);
+}
+template <typename T, bool DEV>
+__device__ __forceinline__ M3<T> lmul_nd(const M3<T> &a, const M3<T> &b) {
+    if constexpr (DEV) return dmul_nd(a, b);
+    else return mul_nd(a, b);
+}
+template <typename T, bool DEV>
+__device__ __forceinline__ M3<T> lmul_dn(const M3<T> &a, const M3<T> &b) {
+    if constexpr (DEV) return dmul_dn(a, b);
+    else return mul_dn(a, b);
+}
+// U phi_nb U^dag - phi
+template <typename T, bool DEV>
+__device__ __forceinline__ H3<T> transport_fwd_minus(const M3<T> &u, const H3<T> &nb,
+                                                     const H3<T> &phi) {
+    if constexpr (DEV) {
+        H3<T> d = h_diff(nb, phi);
+        h_add(d, transport_dev(u, nb));
+        return d;
+    } else {
+        return h_diff(conj_h(u, nb), phi);
+    }
+}
+// U^dag phi_nb U - phi
+template <typename T, bool DEV>
+__device__ __forceinline__ H3<T> transport_bwd_minus(const M3<T> &u, const H3<T> &nb,
+                                                     const H3<T> &phi) {
+    if constexpr (DEV) {
+        H3<T> d = h_diff(nb, phi);
+        h_add(d, transport_dev_back(u, nb));
+        return d;
+    } else {
+        return h_diff(conj_h_dag(u, nb), phi);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ H3<T> shfl_xor_h(const H3<T> &h, int m) {
+    H3<T> r;
+    r.d0 = __shfl_xor_sync(0xffffffffu, h.d0, m);
+    r.d1 = __shfl_xor_sync(0xffffffffu, h.d1, m);
+    r.d2 = __shfl_xor_sync(0xffffffffu, h.d2, m);
+    r.o01.r = __shfl_xor_sync(0xffffffffu, h.o01.r, m);
+    r.o01.i = __shfl_xor_sync(0xffffffffu, h.o01.i, m);
+    r.o02.r = __shfl_xor_sync(0xffffffffu, h.o02.r, m);
+    r.o02.i = __shfl_xor_sync(0xffffffffu, h.o02.i, m);
+    r.o12.r = __shfl_xor_sync(0xffffffffu, h.o12.r, m);
+    r.o12.i = __shfl_xor_sync(0xffffffffu, h.o12.i, m);
+    return r;
+}
+
+// block: 256 threads = 128 sites (32 along y, the fast index, x 4 along x)
+// x 2 directions; lanes 2k and 2k+1 share a site
+template <typename T, bool DEV>
+// FP32: 128 registers, two blocks (16 warps) per SM; FP64: one block per SM
+// (the FP64 state needs ~250 registers per thread without spilling)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+    k_leapfrog_split(const EventGeom *__restrict__ ev, State<T> s, C<T> *ux_out,
+                     C<T> *uy_out, T *phi_out, StepCoef<T> cf) {
+    const int N = ev->N;
+    const int d = threadIdx.x & 1;
+    const int iy = blockIdx.x * 32 + ((threadIdx.x >> 1) & 31);
+    const int ix = blockIdx.y * 4 + (threadIdx.x >> 6);
+    // whole warps stay together for the shuffle: a warp is 16 sites of one
+    // row, and N is a multiple of 8, so either all lanes or none are past N
+    const bool live = (ix < N) && (iy < N);
+    if (!live) return;
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)ix * N + iy;
+    const C<T> *Ud_p = d ? s.uy : s.ux;
+    const C<T> *Uo_p = d ? s.ux : s.uy;
+    T *E_p = d ? s.e2 : s.e1;
+    // neighbour offsets along own (d) and other (o) direction, clamped
+    const int id = d ? iy : ix, io = d ? ix : iy;
+    const long sd = d ? 1 : N, so = d ? N : 1;
+    const long pd = (id + 1 < N) ? sd : 0, md = (id > 0) ? -sd : 0;
+    const long po = (io + 1 < N) ? so : 0, mo = (io > 0) ? -so : 0;
+
+    const M3<T> Ud = ld_m3(Ud_p, pos, n);
+    const H3<T> phi = ld_h(s.phi, pos, n);
+    H3<T> pi = ld_h(s.pi, pos, n);
+    H3<T> Ed = ld_h8(E_p, pos, n);
+
+    if (cf.do_pe) {
+        H3<T> stap;
+        {
+            // P_do = (U_d U_o(+d)) (U_o U_d(+o))^dag
+            const M3<T> Uo = ld_m3(Uo_p, pos, n);
+            const M3<T> a = lmul<T, DEV>(Ud, ld_m3(Uo_p, pos + pd, n));
+            const M3<T> b = lmul<T, DEV>(Uo, ld_m3(Ud_p, pos + po, n));
+            stap = i_antiherm(lmul_nd<T, DEV>(a, b));
+        }
+        {
+            // S_d = (U_d U_o(+d-o)^dag) (U_d(-o)^dag U_o(-o))
+            const M3<T> p = lmul_nd<T, DEV>(Ud, ld_m3(Uo_p, pos + pd + mo, n));
+            const M3<T> q = lmul_dn<T, DEV>(ld_m3(Ud_p, pos + mo, n), ld_m3(Uo_p, pos + mo, n));
+            h_add(stap, i_antiherm(lmul<T, DEV>(p, q)));
+        }
+        h_traceless(stap);
+        const T cst = cf.tau * cf.dt_pe / (T(2) * cf.g * cf.g);
+        const T cdt = cf.dt_pe / cf.tau;
+        h_axpy(Ed, cst, stap);
+        H3<T> br = transport_fwd_minus<T, DEV>(Ud, ld_h(s.phi, pos + pd, n), phi);
+        h_axpy(Ed, cdt, i_commutator(br, phi));  // i[phi~ - phi, phi] = i[phi~, phi]
+        h_add(br, transport_bwd_minus<T, DEV>(ld_m3(Ud_p, pos + md, n),
+                                              ld_h(s.phi, pos + md, n), phi));
+        h_add(br, shfl_xor_h(br, 1));
+        h_axpy(pi, cdt, br);
+        h_traceless(Ed);
+        st_h8(E_p, pos, n, Ed);
+        if (d == 0) st_h(s.pi, pos, n, pi);
+    }
+    if (cf.do_pu) {
+        const T c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / T(2));
+        M3<T> nu;
+        if constexpr (DEV) {
+            nu = taylor2_update_dev(Ed, c, Ud);
+            reunitarize_dev(nu);
+        } else {
+            nu = taylor2_update(Ed, c, Ud);
+        }
+        st_m3(d ? uy_out : ux_out, pos, n, nu);
+        if (d == 1) {
+            H3<T> phin = phi;
+            h_axpy(phin, (cf.tau + cf.dt_pu / T(2)) * cf.dt_pu, pi);
+            st_h(phi_out, pos, n, phin);
+        }
+    }
+}
+
+template <typename T>
+void launch_leapfrog_site(const EventGeom *d_ev, int N, const State<T> &s,
+                          C<T> *ux_out, C<T> *uy_out, T *phi_out,
+                          const StepCoef<T> &cf, bool reunit, cudaStream_t st);
+
 template <typename T>
 void launch_leapfrog(const EventGeom *d_ev, int N, const State<T> &s,
                      C<T> *ux_out, C<T> *uy_out, T *phi_out,
                      const StepCoef<T> &cf, bool reunit, cudaStream_t st) {
+    if (N >= 32) {
+        // N is a power of two >= 32: every warp is 16 full sites of one row
+        dim3 grid(N / 32, (N + 3) / 4);
+        if constexpr (sizeof(T) == 4) {
+            (void)reunit;
+            k_leapfrog_split<T, true><<<grid, 256, 0, st>>>(d_ev, s, ux_out, uy_out,
+                                                            phi_out, cf);
+        } else {
+            k_leapfrog_split<T, false><<<grid, 256, 0, st>>>(d_ev, s, ux_out, uy_out,
+                                                             phi_out, cf);
+        }
+        return;
+    }
+    launch_leapfrog_site(d_ev, N, s, ux_out, uy_out, phi_out, cf, reunit, st);
+}
+
+// one thread per site (lattices smaller than 32 sites per side)
+template <typename T>
+void launch_leapfrog_site(const EventGeom *d_ev, int N, const State<T> &s,
+                          C<T> *ux_out, C<T> *uy_out, T *phi_out,
+                          const StepCoef<T> &cf, bool reunit, cudaStream_t st) {
     dim3 block(32, 4);
     dim3 grid((N + 31) / 32, (N + 3) / 4);
     if constexpr (sizeof(T) == 4) {

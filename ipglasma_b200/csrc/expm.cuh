@@ -46,18 +46,25 @@ __device__ __forceinline__ void expm_coeff(const double Q[8], C<double> u[9]) {
 #pragma unroll
     for (int a = 0; a < 8; a++) c1 += Q[a] * Q[a];
     c1 *= 0.25;
-    const double c0max = fmax(1e-15, 2. * pow(c1 / 3., 1.5));
+    // (c1/3)^{3/2} as t sqrt(t): same value as pow() to rounding, without the
+    // log/exp pair
+    const double t3 = c1 / 3.;
+    const double st3 = sqrt(t3);
+    const double c0max = fmax(1e-15, 2. * (t3 * st3));
     const double theta3 = acos(c0 / c0max) / 3.;
-    const double uu = sqrt(c1 / 3.) * cos(theta3);
-    const double w = sqrt(c1) * sin(theta3);
-    const double xi0 = sin(w) / w;
+    double sth, cth;
+    sincos(theta3, &sth, &cth);
+    const double uu = st3 * cth;
+    const double w = sqrt(c1) * sth;
+    double sw, cosw;
+    sincos(w, &sw, &cosw);
+    const double xi0 = sw / w;
     const double den = 9. * uu * uu - w * w;
-    double s2u, c2u, su, cu;
-    sincos(2. * uu, &s2u, &c2u);
+    // e^{-iu} directly, e^{2iu} by the double-angle identities
+    double su, cu;
     sincos(uu, &su, &cu);
-    const C<double> exp2iu = {c2u, s2u};
+    const C<double> exp2iu = {(cu - su) * (cu + su), 2. * su * cu};
     const C<double> expmiu = {cu, -su};
-    const double cosw = cos(w);
     // f0 = (u^2 - w^2) e^{2iu} + e^{-iu} (8 u^2 cos w + 2 i u xi0 (3u^2 + w^2))
     C<double> f0, f1, f2;
     {

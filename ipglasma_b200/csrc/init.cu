@@ -4,23 +4,7 @@
 // Reference: Init::setV (Init.cpp:1678-1849) and the tau = 0 block of
 // Init::init (Init.cpp:2437-2691).
 //
-// Poisson solve. The reference transforms each of the 8 colours of a sheet
-// separately with FFTW after an fftshift, multiplies by the lattice Green
-// function on the centred k-grid and transforms back (FFT.cpp:492-605,
-// Init.cpp:1707-1747). For an even N the fftshifts on both sides cancel
-// (cyclic convolution commutes with a shift by N/2), so here the multiplier
-// is applied on the plain DFT grid with the centred index (p + N/2) mod N,
-// which gives the same k~ values. Two real colours are packed into one
-// complex transform (colour 2c in the real part, 2c+1 in the imaginary part):
-// the Green function is real and even, so the two results separate into the
-// real and imaginary parts of the inverse transform.
-//
-// Kernels per batch of sheets:
-//   k_rows_fwd   rho = g sqrt(g2mu2/Ny) xi, row FFTs          (smem, 4 channels)
-//   k_cols       column FFT, Green multiply, inverse column FFT (smem)
-//   k_rows_inv   inverse row FFTs, 1/N^2
-//   k_wilson     per site: V <- exp(-i A_k.t) V over the batch, in order
-// The work buffer of a batch is sized to stay resident in the 126 MB L2.
+// The Poisson solve and Wilson-line products of Init::setV are in poisson.cu.
 #include <cstdint>
 #include <cstdio>
 
@@ -30,204 +14,6 @@
 #include "philox.cuh"
 
 namespace ipg {
-
-// ---------------------------------------------------------------------------
-// shared-memory radix-2 FFT on `batch` sequences of length n = 2^logn;
-// element i of sequence b lives at data[b * ld + i]. Forward uses
-// exp(-2 pi i jk/n) (FFTW_FORWARD), inverse exp(+...); unnormalised.
-// ---------------------------------------------------------------------------
-__device__ void smem_fft(double2 *data, int ld, int batch, int logn,
-                         const double2 *__restrict__ tw, bool inverse) {
-    const int n = 1 << logn;
-    const int total = batch << logn;
-    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-        const int b = idx >> logn, i = idx & (n - 1);
-        const int r = __brev(i) >> (32 - logn);
-        if (r > i) {
-            double2 t = data[b * ld + i];
-            data[b * ld + i] = data[b * ld + r];
-            data[b * ld + r] = t;
-        }
-    }
-    __syncthreads();
-    const int halfn = n >> 1;
-    for (int s = 1; s <= logn; s++) {
-        const int half = 1 << (s - 1);
-        const int tshift = logn - s;
-        for (int idx = threadIdx.x; idx < (batch * halfn); idx += blockDim.x) {
-            const int b = idx / halfn, q = idx - b * halfn;
-            const int k = q & (half - 1);
-            const int i0 = ((q >> (s - 1)) << s) + k, i1 = i0 + half;
-            double2 w = __ldg(&tw[k << tshift]);
-            if (inverse) w.y = -w.y;
-            double2 x0 = data[b * ld + i0], x1 = data[b * ld + i1];
-            double tr = x1.x * w.x - x1.y * w.y;
-            double ti = x1.x * w.y + x1.y * w.x;
-            data[b * ld + i0] = make_double2(x0.x + tr, x0.y + ti);
-            data[b * ld + i1] = make_double2(x0.x - tr, x0.y - ti);
-        }
-        __syncthreads();
-    }
-}
-
-// Green function of the lattice Laplacian on the DFT grid (Init.cpp:1712-1742)
-__global__ void k_green(int N, double m_lat, double uvdamp_lat, double *green) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= N * N) return;
-    const int pi = p / N, pj = p % N;
-    const int i = (pi + N / 2) % N, j = (pj + N / 2) % N;  // centred index
-    const double kx = 2. * M_PI * (-0.5 + (double)i / (double)N);
-    const double ky = 2. * M_PI * (-0.5 + (double)j / (double)N);
-    const double kt2 = 4. * (sin(kx / 2.) * sin(kx / 2.) + sin(ky / 2.) * sin(ky / 2.));
-    double gk;
-    if (m_lat == 0) {
-        gk = (kt2 != 0) ? 1. / kt2 : 0.;
-    } else {
-        gk = (1. / (kt2 + m_lat * m_lat)) * exp(-sqrt(kt2) * uvdamp_lat);
-    }
-    green[p] = gk;
-}
-
-void launch_green(int N, double m_lat, double uvdamp_lat, double *green,
-                  cudaStream_t st) {
-    const int n = N * N;
-    k_green<<<(n + 255) / 256, 256, 0, st>>>(N, m_lat, uvdamp_lat, green);
-}
-
-// rho for one row of one sheet into 4 packed channels, then row FFTs
-__global__ void k_rows_fwd(WilsonArgs w, int k0) {
-    extern __shared__ double2 sm[];
-    const int N = w.N;
-    const size_t n = (size_t)N * N;
-    const int ix = blockIdx.x;
-    const int s = blockIdx.y;
-    const int k = k0 + s;
-    const double invNy = (double)w.Ny;
-    if (w.xi) {
-        const double *src = w.xi + ((size_t)k * n + (size_t)ix * N) * 8;
-        for (int idx = threadIdx.x; idx < 8 * N; idx += blockDim.x) {
-            const int j = idx >> 3, a = idx & 7;
-            const double amp = w.g * sqrt(w.g2mu2[(size_t)ix * N + j] / invNy);
-            const double rho = amp * src[idx];
-            double *dst = reinterpret_cast<double *>(&sm[(a >> 1) * N + j]);
-            dst[a & 1] = rho;
-        }
-    } else {
-        for (int j = threadIdx.x; j < N; j += blockDim.x) {
-            const size_t pos = (size_t)ix * N + j;
-            const double amp = w.g * sqrt(w.g2mu2[pos] / invNy);
-            double z[8];
-            normal4({(uint32_t)pos, (uint32_t)k, (w.nucleus << 1) | 0u, 0u},
-                    w.philox_key, z);
-            normal4({(uint32_t)pos, (uint32_t)k, (w.nucleus << 1) | 1u, 0u},
-                    w.philox_key, z + 4);
-#pragma unroll
-            for (int c = 0; c < 4; c++)
-                sm[c * N + j] = make_double2(amp * z[2 * c], amp * z[2 * c + 1]);
-        }
-    }
-    __syncthreads();
-    smem_fft(sm, N, 4, w.logN, w.twiddle, false);
-    for (int idx = threadIdx.x; idx < 4 * N; idx += blockDim.x) {
-        const int c = idx / N, j = idx - c * N;
-        w.work[((size_t)s * 4 + c) * n + (size_t)ix * N + j] = sm[idx];
-    }
-}
-
-// column FFT + Green multiply + inverse column FFT on JB columns
-template <int JB>
-__global__ void k_cols(WilsonArgs w) {
-    extern __shared__ double2 sm[];
-    const int N = w.N;
-    const size_t n = (size_t)N * N;
-    const int jb = blockIdx.x * JB;
-    const int c = blockIdx.y;
-    const int s = blockIdx.z;
-    double2 *base = w.work + ((size_t)s * 4 + c) * n;
-    for (int idx = threadIdx.x; idx < N * JB; idx += blockDim.x) {
-        const int i = idx / JB, q = idx - i * JB;
-        sm[q * N + i] = base[(size_t)i * N + jb + q];
-    }
-    __syncthreads();
-    smem_fft(sm, N, JB, w.logN, w.twiddle, false);
-    for (int idx = threadIdx.x; idx < N * JB; idx += blockDim.x) {
-        const int q = idx / N, i = idx - q * N;
-        const double gk = w.green[(size_t)i * N + jb + q];
-        double2 v = sm[idx];
-        sm[idx] = make_double2(v.x * gk, v.y * gk);
-    }
-    __syncthreads();
-    smem_fft(sm, N, JB, w.logN, w.twiddle, true);
-    for (int idx = threadIdx.x; idx < N * JB; idx += blockDim.x) {
-        const int i = idx / JB, q = idx - i * JB;
-        base[(size_t)i * N + jb + q] = sm[q * N + i];
-    }
-}
-
-// inverse row FFTs and 1/N^2 normalisation, in place
-__global__ void k_rows_inv(WilsonArgs w) {
-    extern __shared__ double2 sm[];
-    const int N = w.N;
-    const size_t n = (size_t)N * N;
-    const int ix = blockIdx.x;
-    const int s = blockIdx.y;
-    for (int idx = threadIdx.x; idx < 4 * N; idx += blockDim.x) {
-        const int c = idx / N, j = idx - c * N;
-        sm[idx] = w.work[((size_t)s * 4 + c) * n + (size_t)ix * N + j];
-    }
-    __syncthreads();
-    smem_fft(sm, N, 4, w.logN, w.twiddle, true);
-    const double ntot = (double)n;
-    for (int idx = threadIdx.x; idx < 4 * N; idx += blockDim.x) {
-        const int c = idx / N, j = idx - c * N;
-        double2 v = sm[idx];
-        w.work[((size_t)s * 4 + c) * n + (size_t)ix * N + j] =
-            make_double2(v.x / ntot, v.y / ntot);
-    }
-}
-
-// V <- exp(-i A_k.t) V for the sheets of the batch, in ascending k
-// (Init.cpp:1750-1768: new * old)
-__global__ void k_wilson(WilsonArgs w, int ns) {
-    const size_t n = (size_t)w.N * w.N;
-    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (pos >= n) return;
-    M3<double> V = ld_m3(w.V, pos, n);
-    for (int s = 0; s < ns; s++) {
-        double in[8];
-#pragma unroll
-        for (int c = 0; c < 4; c++) {
-            const double2 v = w.work[((size_t)s * 4 + c) * n + pos];
-            in[2 * c] = -v.x;
-            in[2 * c + 1] = -v.y;
-        }
-        const M3<double> e = exp_from_coeff(in);
-        V = mul(e, V);
-    }
-    st_m3(w.V, pos, n, V);
-}
-
-static int fft_threads(int N) { return N >= 512 ? 512 : (N >= 256 ? 256 : 128); }
-
-void launch_wilson_sheets(const WilsonArgs &w, int k0, int ns,
-                          cudaStream_t st) {
-    const int N = w.N;
-    const size_t row_smem = sizeof(double2) * 4 * N;
-    const int thr = fft_threads(N);
-    cudaFuncSetAttribute(k_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)row_smem);
-    cudaFuncSetAttribute(k_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)row_smem);
-    k_rows_fwd<<<dim3(N, ns), thr, row_smem, st>>>(w, k0);
-    constexpr int JB = 8;
-    const size_t col_smem = sizeof(double2) * JB * N;
-    cudaFuncSetAttribute(k_cols<JB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)col_smem);
-    k_cols<JB><<<dim3(N / JB, 4, ns), thr, col_smem, st>>>(w);
-    k_rows_inv<<<dim3(N, ns), thr, row_smem, st>>>(w);
-    const size_t n = (size_t)N * N;
-    k_wilson<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
-}
 
 // ---------------------------------------------------------------------------
 // link products U1 = V_A(x) V_A(x+i)^dag, U2 likewise for V_B, with the NaN

@@ -46,7 +46,7 @@ struct WilsonArgs {
     const double *xi;        // [Ny][n][8] unit normals, or null (Philox)
     uint64_t philox_key;     // used when xi == null
     uint32_t nucleus;        // 0 = A, 1 = B (Philox stream selector)
-    const double2 *twiddle;  // [N/2] exp(-2 pi i k / N)
+    const double2 *twiddle;  // [N] exp(-2 pi i k / N)
     const double *green;     // [N*N] Poisson multiplier on the DFT grid
     double2 *work;           // [ns][4][n] complex scratch
     C<double> *V;            // [9][n] Wilson line, updated in place

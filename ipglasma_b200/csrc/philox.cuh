@@ -43,17 +43,20 @@ __host__ __device__ __forceinline__ double u01(uint32_t a, uint32_t b) {
     return ((double)v + 1.0) * (1.0 / 9007199254740992.0);
 }
 
-// four standard normals from one counter
+// uniform in (0, 1] with 24 random bits
+__host__ __device__ __forceinline__ float u01f(uint32_t a) {
+    return ((float)(a >> 8) + 1.0f) * (1.0f / 16777216.0f);
+}
+
+// four standard normals from one counter (Box-Muller in single precision:
+// the noise only has to be Gaussian, not reproducible to more than 24 bits)
 __device__ __forceinline__ void normal4(U4 ctr, uint64_t key, double out[4]) {
-    U4 r = philox4x32_10(ctr, (uint32_t)key, (uint32_t)(key >> 32));
-    U4 r2 = philox4x32_10({ctr.x, ctr.y, ctr.z, ctr.w ^ 0x80000000u},
-                          (uint32_t)key, (uint32_t)(key >> 32));
-    double u1 = u01(r.x, r.y), u2 = u01(r.z, r.w);
-    double u3 = u01(r2.x, r2.y), u4 = u01(r2.z, r2.w);
-    double rad1 = sqrt(-2.0 * log(u1)), rad2 = sqrt(-2.0 * log(u3));
-    double s1, c1, s2, c2;
-    sincospi(2.0 * u2, &s1, &c1);
-    sincospi(2.0 * u4, &s2, &c2);
+    const U4 r = philox4x32_10(ctr, (uint32_t)key, (uint32_t)(key >> 32));
+    const float rad1 = sqrtf(-2.0f * logf(u01f(r.x)));
+    const float rad2 = sqrtf(-2.0f * logf(u01f(r.z)));
+    float s1, c1, s2, c2;
+    sincospif(2.0f * u01f(r.y), &s1, &c1);
+    sincospif(2.0f * u01f(r.w), &s2, &c2);
     out[0] = rad1 * c1;
     out[1] = rad1 * s1;
     out[2] = rad2 * c2;

@@ -2,8 +2,11 @@
 // (Evolution::checkGaussLaw, Evolution.cpp:295-364), link unitarity,
 // total energy and the eccentricities epsilon_n, Psi_n
 // (Evolution::eccentricity, Evolution.cpp:1280-1810, cutoff 0, constant
-// coupling). Sums are deterministic: each block writes a partial in a fixed
-// order and one block folds the partials, so repeated runs agree bit for bit.
+// coupling), Newton statistics and cell flags.
+//
+// Every reduction runs on a fixed grid of RG blocks with a grid-stride loop,
+// each block writes one partial, and a single thread folds the RG partials in
+// order, so results are deterministic (bit-identical run to run).
 #include <cstdint>
 
 #include "fields.cuh"
@@ -14,6 +17,7 @@ namespace ipg {
 namespace {
 
 constexpr int RB = 256;  // threads per reduction block
+constexpr int RG = 296;  // reduction blocks (2 per SM)
 
 template <int K>
 __device__ __forceinline__ void block_sum(double (&v)[K], double *out) {
@@ -34,35 +38,36 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double *out) {
     }
 }
 
-__device__ __forceinline__ double block_max(double v) {
+__device__ __forceinline__ void block_max(double v, double *out) {
     __shared__ double sh[RB / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
     if (lane == 0) sh[wid] = v;
     __syncthreads();
-    double m = 0.;
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
+        double m = 0.;
         for (int w = 0; w < RB / 32; w++) m = fmax(m, sh[w]);
-    return m;
+        *out = m;
+    }
 }
 
-// fold `nb` partial rows of K values into out[K]
+// fold RG partial rows of K values into out[K]; slots in max_mask take the max
 template <int K>
-__global__ void k_fold(const double *partial, int nb, double *out) {
+__global__ void k_fold(const double *partial, double *out, unsigned max_mask) {
     const int k = threadIdx.x;
     if (k >= K) return;
+    const bool mx = (max_mask >> k) & 1u;
     double s = 0.;
-    for (int b = 0; b < nb; b++) s += partial[(size_t)b * K + k];
+    for (int b = 0; b < RG; b++) {
+        const double v = partial[(size_t)b * K + k];
+        s = mx ? fmax(s, v) : s + v;
+    }
     out[k] = s;
 }
 
-__global__ void k_fold_max(const double *partial, int nb, double *out) {
-    if (threadIdx.x != 0) return;
-    double m = 0.;
-    for (int b = 0; b < nb; b++) m = fmax(m, partial[b]);
-    *out = m;
-}
+#define GRID_STRIDE(i, n) \
+    for (size_t i = (size_t)blockIdx.x * RB + threadIdx.x; i < (n); i += (size_t)RG * RB)
 
 }  // namespace
 
@@ -70,11 +75,10 @@ __global__ void k_fold_max(const double *partial, int nb, double *out) {
 // Gauss law: G = UxXm1^dag E1(x-1) UxXm1 - E1 + UyYm1^dag E2(y-1) UyYm1 - E2
 //               - i (phi pi - pi phi);  max over sites of |G|^2 / 2
 // --------------------------------------------------------------------------
-__global__ void k_gauss(int N, State<double> s, double *partial) {
+__global__ void __launch_bounds__(RB) k_gauss(int N, State<double> s, double *partial) {
     const size_t n = (size_t)N * N;
-    const size_t pos = (size_t)blockIdx.x * RB + threadIdx.x;
     double val = 0.;
-    if (pos < n) {
+    GRID_STRIDE(pos, n) {
         const int ix = (int)(pos / N), iy = (int)(pos % N);
         const size_t mX = (size_t)max(0, ix - 1) * N + iy;
         const size_t mY = (size_t)ix * N + max(0, iy - 1);
@@ -86,38 +90,33 @@ __global__ void k_gauss(int N, State<double> s, double *partial) {
         sub_from(G, from_h(ld_h8(s.e2, pos, n)));
         const M3<double> ph = from_h(ld_h(s.phi, pos, n)), pi = from_h(ld_h(s.pi, pos, n));
         const M3<double> c = minus(mul(ph, pi), mul(pi, ph));
-        // - i c
 #pragma unroll
-        for (int k = 0; k < 9; k++) {
+        for (int k = 0; k < 9; k++) {  // - i c
             G.m[k].r += c.m[k].i;
             G.m[k].i -= c.m[k].r;
         }
         double sq = 0.;
 #pragma unroll
         for (int k = 0; k < 9; k++) sq += G.m[k].r * G.m[k].r + G.m[k].i * G.m[k].i;
-        val = 0.5 * sq;
+        val = fmax(val, 0.5 * sq);
     }
-    const double m = block_max(val);
-    if (threadIdx.x == 0) partial[blockIdx.x] = m;
+    block_max(val, partial + blockIdx.x);
 }
 
 void launch_gauss_law(int N, const State<double> &s, double *d_partial,
                       double *d_out, cudaStream_t st) {
-    const size_t n = (size_t)N * N;
-    const int nb = (int)((n + RB - 1) / RB);
-    k_gauss<<<nb, RB, 0, st>>>(N, s, d_partial);
-    k_fold_max<<<1, 32, 0, st>>>(d_partial, nb, d_out);
+    k_gauss<<<RG, RB, 0, st>>>(N, s, d_partial);
+    k_fold<1><<<1, 32, 0, st>>>(d_partial, d_out, 1u);
 }
 
 // --------------------------------------------------------------------------
 // max over links of the largest |(U^dag U - 1)_ij|
 // --------------------------------------------------------------------------
-__global__ void k_unitarity(int N, const C<double> *ux, const C<double> *uy,
-                            double *partial) {
+__global__ void __launch_bounds__(RB) k_unitarity(int N, const C<double> *ux,
+                                                  const C<double> *uy, double *partial) {
     const size_t n = (size_t)N * N;
-    const size_t pos = (size_t)blockIdx.x * RB + threadIdx.x;
     double val = 0.;
-    if (pos < n) {
+    GRID_STRIDE(pos, n) {
         for (int d = 0; d < 2; d++) {
             const M3<double> u = ld_m3(d ? uy : ux, pos, n);
             M3<double> p = mul_dn(u, u);
@@ -129,90 +128,84 @@ __global__ void k_unitarity(int N, const C<double> *ux, const C<double> *uy,
                 val = fmax(val, sqrt(p.m[k].r * p.m[k].r + p.m[k].i * p.m[k].i));
         }
     }
-    const double m = block_max(val);
-    if (threadIdx.x == 0) partial[blockIdx.x] = m;
+    block_max(val, partial + blockIdx.x);
 }
 
 void launch_unitarity(int N, const C<double> *ux, const C<double> *uy,
                       double *d_partial, double *d_out, cudaStream_t st) {
-    const size_t n = (size_t)N * N;
-    const int nb = (int)((n + RB - 1) / RB);
-    k_unitarity<<<nb, RB, 0, st>>>(N, ux, uy, d_partial);
-    k_fold_max<<<1, 32, 0, st>>>(d_partial, nb, d_out);
+    k_unitarity<<<RG, RB, 0, st>>>(N, ux, uy, d_partial);
+    k_fold<1><<<1, 32, 0, st>>>(d_partial, d_out, 1u);
 }
 
 // --------------------------------------------------------------------------
 // eccentricities
 // --------------------------------------------------------------------------
 // pass 1: sum x w, y w, w, T^tautau, eps   (w = eps u^tau where eps >= 0)
-__global__ void k_ecc1(int N, double L, double a, const double *eps,
-                       const double *utau, const double *Ttt,
-                       double *partial) {
+__global__ void __launch_bounds__(RB) k_ecc1(int N, double L, double a, const double *eps,
+                                             const double *utau, const double *Ttt,
+                                             double *partial) {
     const size_t n = (size_t)N * N;
-    const size_t pos = (size_t)blockIdx.x * RB + threadIdx.x;
     double v[5] = {0., 0., 0., 0., 0.};
-    if (pos < n) {
+    GRID_STRIDE(pos, n) {
         const int ix = (int)(pos / N), iy = (int)(pos % N);
         const double x = -L / 2. + a * ix, y = -L / 2. + a * iy;
         const double e = eps[pos];
         const double w = (e < 0.) ? 0. : e * utau[pos];
-        v[0] = x * w;
-        v[1] = y * w;
-        v[2] = w;
-        v[3] = Ttt[pos];
-        v[4] = e;
+        v[0] += x * w;
+        v[1] += y * w;
+        v[2] += w;
+        v[3] += Ttt[pos];
+        v[4] += e;
     }
     block_sum<5>(v, partial + (size_t)blockIdx.x * 5);
 }
 
 // pass 2 over [2, N-2)^2 about the centroid: r^n, r^n cos(n phi), r^n sin(n phi)
 // in the reference's choice of powers (avr1 and the n = 1 moments use r^3)
-__global__ void k_ecc2(int N, double L, double a, const double *eps,
-                       const double *utau, const double *cent,
-                       double *partial) {
+__global__ void __launch_bounds__(RB) k_ecc2(int N, double L, double a, const double *eps,
+                                             const double *utau, const double *cent,
+                                             double *partial) {
     const size_t n = (size_t)N * N;
-    const size_t pos = (size_t)blockIdx.x * RB + threadIdx.x;
     double v[18];
 #pragma unroll
     for (int k = 0; k < 18; k++) v[k] = 0.;
-    if (pos < n) {
+    const double avx = cent[0] / cent[2], avy = cent[1] / cent[2];
+    GRID_STRIDE(pos, n) {
         const int ix = (int)(pos / N), iy = (int)(pos % N);
-        if (ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2) {
-            const double avx = cent[0] / cent[2], avy = cent[1] / cent[2];
-            const double x = -L / 2. + a * ix - avx, y = -L / 2. + a * iy - avy;
-            double phiA;
-            if (x >= 0) {
-                phiA = atan(y / x);
-                if (x == 0) phiA = (y >= 0) ? M_PI / 2. : 3. * M_PI / 2.;
-            } else {
-                phiA = atan(y / x) + M_PI;
-            }
-            const double e = eps[pos];
-            const double w = (e < 0.) ? 0. : e * utau[pos];
-            const double r = sqrt(x * x + y * y);
-            const double r2 = r * r, r3 = r * r * r, r4 = r * r * r * r;
-            const double r5 = r * r * r * r * r, r6 = r * r * r * r * r * r;
-            // 0..5: avr1 avrSq avr3 avr4 avr5 avr6
-            v[0] = r3 * w;
-            v[1] = r2 * w;
-            v[2] = r3 * w;
-            v[3] = r4 * w;
-            v[4] = r5 * w;
-            v[5] = r6 * w;
-            // 6..17: cos/sin moments for n = 1..6
-            v[6] = r3 * cos(phiA) * w;
-            v[7] = r3 * sin(phiA) * w;
-            v[8] = r2 * cos(2. * phiA) * w;
-            v[9] = r2 * sin(2. * phiA) * w;
-            v[10] = r3 * cos(3. * phiA) * w;
-            v[11] = r3 * sin(3. * phiA) * w;
-            v[12] = r4 * cos(4. * phiA) * w;
-            v[13] = r4 * sin(4. * phiA) * w;
-            v[14] = r5 * cos(5. * phiA) * w;
-            v[15] = r5 * sin(5. * phiA) * w;
-            v[16] = r6 * cos(6. * phiA) * w;
-            v[17] = r6 * sin(6. * phiA) * w;
+        if (ix < 2 || ix >= N - 2 || iy < 2 || iy >= N - 2) continue;
+        const double x = -L / 2. + a * ix - avx, y = -L / 2. + a * iy - avy;
+        double phiA;
+        if (x >= 0) {
+            phiA = atan(y / x);
+            if (x == 0) phiA = (y >= 0) ? M_PI / 2. : 3. * M_PI / 2.;
+        } else {
+            phiA = atan(y / x) + M_PI;
         }
+        const double e = eps[pos];
+        const double w = (e < 0.) ? 0. : e * utau[pos];
+        const double r = sqrt(x * x + y * y);
+        const double r2 = r * r, r3 = r * r * r, r4 = r * r * r * r;
+        const double r5 = r * r * r * r * r, r6 = r * r * r * r * r * r;
+        // 0..5: avr1 avrSq avr3 avr4 avr5 avr6
+        v[0] += r3 * w;
+        v[1] += r2 * w;
+        v[2] += r3 * w;
+        v[3] += r4 * w;
+        v[4] += r5 * w;
+        v[5] += r6 * w;
+        // 6..17: cos/sin moments for n = 1..6
+        v[6] += r3 * cos(phiA) * w;
+        v[7] += r3 * sin(phiA) * w;
+        v[8] += r2 * cos(2. * phiA) * w;
+        v[9] += r2 * sin(2. * phiA) * w;
+        v[10] += r3 * cos(3. * phiA) * w;
+        v[11] += r3 * sin(3. * phiA) * w;
+        v[12] += r4 * cos(4. * phiA) * w;
+        v[13] += r4 * sin(4. * phiA) * w;
+        v[14] += r5 * cos(5. * phiA) * w;
+        v[15] += r5 * sin(5. * phiA) * w;
+        v[16] += r6 * cos(6. * phiA) * w;
+        v[17] += r6 * sin(6. * phiA) * w;
     }
     block_sum<18>(v, partial + (size_t)blockIdx.x * 18);
 }
@@ -221,12 +214,51 @@ void launch_eccentricity(int N, double L, double a, const double *eps,
                          const double *utau, const double *Ttt,
                          double *d_partial, double *d_sums1,
                          double *d_sums2, cudaStream_t st) {
-    const size_t n = (size_t)N * N;
-    const int nb = (int)((n + RB - 1) / RB);
-    k_ecc1<<<nb, RB, 0, st>>>(N, L, a, eps, utau, Ttt, d_partial);
-    k_fold<5><<<1, 32, 0, st>>>(d_partial, nb, d_sums1);
-    k_ecc2<<<nb, RB, 0, st>>>(N, L, a, eps, utau, d_sums1, d_partial);
-    k_fold<18><<<1, 32, 0, st>>>(d_partial, nb, d_sums2);
+    k_ecc1<<<RG, RB, 0, st>>>(N, L, a, eps, utau, Ttt, d_partial);
+    k_fold<5><<<1, 32, 0, st>>>(d_partial, d_sums1, 0u);
+    k_ecc2<<<RG, RB, 0, st>>>(N, L, a, eps, utau, d_sums1, d_partial);
+    k_fold<18><<<1, 32, 0, st>>>(d_partial, d_sums2, 0u);
+}
+
+// --------------------------------------------------------------------------
+// Newton statistics: out = {max iterations, sum of iterations, links that
+// restarted, links that failed}
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(RB) k_newton_stats(size_t links, const int *iters,
+                                                     const int *status, double *partial) {
+    double mx = 0.;
+    double v[3] = {0., 0., 0.};
+    GRID_STRIDE(k, links) {
+        mx = fmax(mx, (double)iters[k]);
+        v[0] += iters[k];
+        v[1] += status[k] >= 1;
+        v[2] += status[k] == 2;
+    }
+    block_max(mx, partial + (size_t)blockIdx.x * 4);
+    block_sum<3>(v, partial + (size_t)blockIdx.x * 4 + 1);
+}
+
+void launch_newton_stats(size_t links, const int *iters, const int *status,
+                         double *d_partial, double *d_out, cudaStream_t st) {
+    k_newton_stats<<<RG, RB, 0, st>>>(links, iters, status, d_partial);
+    k_fold<4><<<1, 32, 0, st>>>(d_partial, d_out, 1u);
+}
+
+// cells with found == 0 and cells with non-finite e
+__global__ void __launch_bounds__(RB) k_cell_flags(size_t n, const int *found,
+                                                   const double *eps, double *partial) {
+    double v[2] = {0., 0.};
+    GRID_STRIDE(k, n) {
+        v[0] += found[k] == 0;
+        v[1] += !isfinite(eps[k]);
+    }
+    block_sum<2>(v, partial + (size_t)blockIdx.x * 2);
+}
+
+void launch_cell_flags(size_t n, const int *found, const double *eps,
+                       double *d_partial, double *d_out, cudaStream_t st) {
+    k_cell_flags<<<RG, RB, 0, st>>>(n, found, eps, d_partial);
+    k_fold<2><<<1, 32, 0, st>>>(d_partial, d_out, 0u);
 }
 
 // --------------------------------------------------------------------------
@@ -274,69 +306,5 @@ template void launch_convert_state<float>(size_t, const State<float> &,
                                           State<double> &, cudaStream_t);
 template void launch_convert_state_down<float>(size_t, const State<double> &,
                                                State<float> &, cudaStream_t);
-
-}  // namespace ipg
-
-namespace ipg {
-
-// Newton statistics: out[0] = max iterations, out[1] = sum of iterations,
-// out[2] = links that restarted, out[3] = links that failed (as doubles)
-__global__ void k_newton_stats(size_t links, const int *iters, const int *status,
-                               double *partial) {
-    const size_t k = (size_t)blockIdx.x * RB + threadIdx.x;
-    double v[4] = {0., 0., 0., 0.};
-    if (k < links) {
-        v[0] = iters[k];
-        v[1] = iters[k];
-        v[2] = status[k] >= 1;
-        v[3] = status[k] == 2;
-    }
-    // max in slot 0 via a separate max reduction, sums for the rest
-    const double m = block_max(v[0]);
-    double s[3] = {v[1], v[2], v[3]};
-    block_sum<3>(s, partial + (size_t)blockIdx.x * 4 + 1);
-    if (threadIdx.x == 0) partial[(size_t)blockIdx.x * 4] = m;
-}
-
-__global__ void k_fold_newton(const double *partial, int nb, double *out) {
-    if (threadIdx.x != 0) return;
-    double m = 0., s1 = 0., s2 = 0., s3 = 0.;
-    for (int b = 0; b < nb; b++) {
-        m = fmax(m, partial[4 * b]);
-        s1 += partial[4 * b + 1];
-        s2 += partial[4 * b + 2];
-        s3 += partial[4 * b + 3];
-    }
-    out[0] = m;
-    out[1] = s1;
-    out[2] = s2;
-    out[3] = s3;
-}
-
-void launch_newton_stats(size_t links, const int *iters, const int *status,
-                         double *d_partial, double *d_out, cudaStream_t st) {
-    const int nb = (int)((links + RB - 1) / RB);
-    k_newton_stats<<<nb, RB, 0, st>>>(links, iters, status, d_partial);
-    k_fold_newton<<<1, 32, 0, st>>>(d_partial, nb, d_out);
-}
-
-// number of cells with found == 0 and of non-finite e
-__global__ void k_cell_flags(size_t n, const int *found, const double *eps,
-                             double *partial) {
-    const size_t k = (size_t)blockIdx.x * RB + threadIdx.x;
-    double v[2] = {0., 0.};
-    if (k < n) {
-        v[0] = found[k] == 0;
-        v[1] = !isfinite(eps[k]);
-    }
-    block_sum<2>(v, partial + (size_t)blockIdx.x * 2);
-}
-
-void launch_cell_flags(size_t n, const int *found, const double *eps,
-                       double *d_partial, double *d_out, cudaStream_t st) {
-    const int nb = (int)((n + RB - 1) / RB);
-    k_cell_flags<<<nb, RB, 0, st>>>(n, found, eps, d_partial);
-    k_fold<2><<<1, 32, 0, st>>>(d_partial, nb, d_out);
-}
 
 }  // namespace ipg
