@@ -182,6 +182,25 @@ ipg_status ipg_last_leapfrog_ms(ipg_ctx *ctx, double *ms, int *launches);
 /* Number of kernels this library launched on ctx since creation. */
 ipg_status ipg_kernel_launches(const ipg_ctx *ctx, long long *count);
 
+/* Wilson lines of one nucleus without allocating anything: no counterpart in
+ * the reference (it is an addition of this library). For callers that cannot
+ * allocate device memory (code inside another framework's memory pool or
+ * allocator hooks, hosts that forbid allocation after start-up, callers that
+ * must avoid the synchronisation cudaMalloc/cudaFree can imply). Computes what
+ * ipg_init_fields computes for V_A (or V_B): rho = g sqrt(g2mu2/Ny) xi, the
+ * Poisson solve and the ordered product of the Ny sheet exponentials, on the
+ * given stream (NULL = default stream). All pointers are device pointers the
+ * caller owns: d_g2mu2[N*N], d_xi[Ny][N*N][8], output d_V[N*N*18] (3x3 per
+ * site, row-major (re, im)). Scratch lives in one fixed device array sized for
+ * N <= 256 (about 14 MB per GPU that loads the library, kept until exit);
+ * larger N returns IPG_ERR_BAD_CONFIG. The first call on a device looks up
+ * that array's address (make it before any stream capture). Calls share the
+ * array: calls that overlap on the GPU race and must be serialised. */
+ipg_status ipg_wilson_lines_noalloc(int N, int Ny, double L, double g, double m,
+                                    double UVdamp, const double *d_g2mu2,
+                                    const double *d_xi, double *d_V,
+                                    void *stream);
+
 #ifdef __cplusplus
 }
 #endif
