@@ -142,6 +142,11 @@ ipg_status ipg_use_device_noise(ipg_ctx *ctx);
  * IPG_ERR_NEWTON_NONCONVERGED (fields still set) if any link failed. */
 ipg_status ipg_init_fields(ipg_ctx *ctx, ipg_init_report *report);
 
+/* tau=0 link solve and initial fields from Wilson lines loaded with
+ * ipg_set_field(IPG_VA / IPG_VB); replaces the READFROMFILE > 0 path of
+ * Init::init (readV then the tau=0 block, Init.cpp:2377-2381, 2437-2691). */
+ipg_status ipg_init_from_wilson_lines(ipg_ctx *ctx, ipg_init_report *report);
+
 /* The whole schedule of Evolution::run (Evolution.cpp:366-657): tau=0 half
  * step, itmax-1 full steps, T^{mu nu} + Landau matching at it = itmax
  * before the final half step of pi and E, then Gauss law and
@@ -181,6 +186,27 @@ ipg_status ipg_last_leapfrog_ms(ipg_ctx *ctx, double *ms, int *launches);
 
 /* Number of kernels this library launched on ctx since creation. */
 ipg_status ipg_kernel_launches(const ipg_ctx *ctx, long long *count);
+
+/* Output files in the reference's formats from host observables (as returned
+ * by ipg_get_observables); replace the writer part of
+ * MyEigen::flowVelocity4D: the hydro file epsilon-u-Hydro-... (MyEigen.cpp:
+ * 380-797, writeOutputs odd) and the KoMPoST file Tmunu-t... (MyEigen.cpp:
+ * 801-1045, writeOutputs/4 == 1). it and dtau give the proper time
+ * it*dtau*a of the observables; gfactor is 1 for a fixed coupling. Etot (may
+ * be NULL) receives the energy the reference prints as "Etot". */
+ipg_status ipg_write_hydro(const char *path, int N, double L, int sizeOutput,
+                           double LOutput, int etaSizeOutput, double detaOutput,
+                           int it, double dtau, const double *eps,
+                           const double *u4, const double *pi10, double gfactor,
+                           double *Etot);
+ipg_status ipg_write_tmunu(const char *path, int N, double L, int sizeOutput,
+                           double LOutput, int etaSizeOutput, double detaOutput,
+                           int it, double dtau, const double *T10, double gfactor);
+/* The reference's output file names for an event id (MyEigen.cpp:376-383,
+ * 804-807); buffers of at least 64 bytes. */
+ipg_status ipg_output_names(int event_id, int it, double dtau, double a,
+                            char *hydro, size_t hydro_len, char *tmunu,
+                            size_t tmunu_len);
 
 /* Wilson lines of one nucleus without allocating anything: no counterpart in
  * the reference (it is an addition of this library). For callers that cannot

@@ -27,6 +27,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC"]
 CU_SOURCES = ["api.cu", "evolve.cu", "init.cu", "poisson.cu", "observables.cu", "reduce.cu",
               "noalloc.cu"]
+CPP_SOURCES = ["writers.cpp"]
 
 
 def _nvcc() -> str:
@@ -53,7 +54,8 @@ def _stale(target: Path, deps: list[Path]) -> bool:
 
 def build_library(verbose: bool = False, force: bool = False) -> Path:
     deps = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + \
-        sorted(CSRC.glob("*.h")) + [ROOT / "include" / "ipglasma_b200.h"]
+        sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cpp")) + \
+        [ROOT / "include" / "ipglasma_b200.h"]
     if not force and not _stale(LIB, deps):
         return LIB
     objdir = PKG / "_build"
@@ -69,6 +71,14 @@ def build_library(verbose: bool = False, force: bool = False) -> Path:
         out = _run(cmd)
         if verbose and out:
             print(out)
+        objs.append(str(obj))
+    # host-only sources (writers): plain g++, no FP contraction, so the text
+    # output is computed with the reference's operation order and rounding
+    cxx = shutil.which("g++") or "g++"
+    for src in CPP_SOURCES:
+        obj = objdir / (Path(src).stem + ".o")
+        _run([cxx, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I",
+              str(ROOT / "include"), "-c", str(CSRC / src), "-o", str(obj)])
         objs.append(str(obj))
     tmp = LIB.with_suffix(".so.tmp")
     _run([nvcc, *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"])

@@ -462,9 +462,10 @@ ipg_status ipg_use_device_noise(ipg_ctx *c) {
     return IPG_OK;
 }
 
-ipg_status ipg_init_fields(ipg_ctx *c, ipg_init_report *rep) {
+// from_wilson: V_A and V_B were loaded with ipg_set_field, skip setV
+static ipg_status init_impl(ipg_ctx *c, ipg_init_report *rep, bool from_wilson) {
     if (!c) return IPG_ERR_BAD_CONFIG;
-    if (!c->have_g2mu || !c->have_noise)
+    if (!from_wilson && (!c->have_g2mu || !c->have_noise))
         return fail(c, IPG_ERR_STATE, "set g2mu and noise before ipg_init_fields");
     const size_t n = c->n;
     const int N = c->N;
@@ -473,7 +474,7 @@ ipg_status ipg_init_fields(ipg_ctx *c, ipg_init_report *rep) {
     IPG_CUDA(c, cudaEventRecord(e[0], c->stream));
 
     // Wilson lines, nucleus A then B (Init.cpp:1688-1847)
-    for (int nuc = 0; nuc < 2; nuc++) {
+    for (int nuc = 0; nuc < (from_wilson ? 0 : 2); nuc++) {
         C<double> *V = nuc ? c->VB : c->VA;
         k_identity<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, V);
         IPG_LAUNCHED(c, 1);
@@ -559,6 +560,14 @@ ipg_status ipg_init_fields(ipg_ctx *c, ipg_init_report *rep) {
         return fail(c, IPG_ERR_NEWTON_NONCONVERGED,
                     "%d of %zu links did not converge", failed, 2 * n);
     return IPG_OK;
+}
+
+ipg_status ipg_init_fields(ipg_ctx *c, ipg_init_report *rep) {
+    return init_impl(c, rep, false);
+}
+
+ipg_status ipg_init_from_wilson_lines(ipg_ctx *c, ipg_init_report *rep) {
+    return init_impl(c, rep, true);
 }
 
 ipg_status ipg_evolve(ipg_ctx *c, int steps) {

@@ -1,0 +1,368 @@
+// ipglasma_b200 [input] [nev] -- drop-in for the reference executable's event
+// loop (main.cpp:47-399) on the per-event hot path.
+//
+// Reads the reference's key/value input file with the reference's lookup
+// rules (Setup.cpp:24-104: keys and values alternate, the file ends with
+// EndOfFile, a missing key ends the program), derives dtau like main.cpp:531-534,
+// and for each event either
+//   - reads V_A, V_B from the binary Wilson-line files of
+//     readInitialWilsonLines = 2 (format of Init.cpp:1914-1973 / 2120-2296),
+//   - or samples the two nuclei (Woods-Saxon with minimum distance, the
+//     algorithm of Init.cpp:2749-2816) and builds the g^2 mu^2 maps from the
+//     nucleon thickness: T_A = sum of Gaussians of width BG (GeV^-2), and
+//     Q_s(x) = QsMax sqrt(T_A(x)/max T_A) with QsMax from the optional key
+//     QsMax (default 1.5 GeV), g^2 mu^2 a^2 = Q_s^2/QsmuRatio^2 a^2/(hbar c)^2/g^2.
+//     (The reference's IP-Sat Q_s(T_p, y) table is not used.)
+// then runs the event on the GPU through the C ABI and writes the reference's
+// output files (writeOutputs 1, 4, 5) and, on request, the V files
+// (writeInitialWilsonLines = 2).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <random>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "ipglasma_b200.h"
+
+namespace {
+
+constexpr double kHbarc = 0.1973269718;
+
+// ---------------------------------------------------------------- input file
+class InputFile {
+  public:
+    explicit InputFile(const std::string &name) : name_(name) {
+        std::ifstream in(name.c_str());
+        if (!in) {
+            std::cerr << "The input file named " << name << " is absent. Exiting." << std::endl;
+            std::exit(1);
+        }
+        std::string k, v;
+        while (in >> k) {
+            if (k == "EndOfFile") break;
+            if (!(in >> v)) break;
+            pairs_.push_back({k, v});
+        }
+    }
+    bool has(const std::string &key) const {
+        for (const auto &p : pairs_)
+            if (p.first == key) return true;
+        return false;
+    }
+    std::string str(const std::string &key) const {
+        for (const auto &p : pairs_)
+            if (p.first == key) return p.second;
+        std::cerr << key << " not found in " << name_ << std::endl;
+        std::cout << "Create a complete input file." << std::endl;
+        std::exit(1);
+    }
+    double d(const std::string &key) const { return std::atof(str(key).c_str()); }
+    int i(const std::string &key) const { return static_cast<int>(d(key)); }
+    unsigned long long ull(const std::string &key) const {
+        return static_cast<unsigned long long>(d(key) + 0.5);
+    }
+    double d_or(const std::string &key, double def) const { return has(key) ? d(key) : def; }
+
+  private:
+    std::string name_;
+    std::vector<std::pair<std::string, std::string>> pairs_;
+};
+
+// ------------------------------------------------------------ nuclei, g2mu
+struct Species {
+    int A;
+    double R, a;
+};
+
+Species species(const std::string &name, const InputFile &in) {
+    static const std::map<std::string, Species> table = {
+        {"p", {1, 0.0, 0.0}},        {"O", {16, 2.608, 0.513}},
+        {"Cu", {63, 4.20641, 0.5977}}, {"Xe", {129, 5.36, 0.59}},
+        {"Au", {197, 6.38, 0.535}},  {"Pb", {208, 6.62, 0.546}},
+        {"U", {238, 6.81, 0.6}}};
+    auto it = table.find(name);
+    if (it == table.end()) {
+        std::cerr << "nucleus " << name << " is not supported by this executable" << std::endl;
+        std::exit(1);
+    }
+    Species s = it->second;
+    if (in.i("setWSDeformParams")) {  // the input's R_WS, a_WS for both nuclei
+        s.R = in.d("R_WS");
+        s.a = in.d("a_WS");
+    }
+    return s;
+}
+
+std::vector<double> sample_nucleus(std::mt19937_64 &rng, const Species &s, double dmin) {
+    std::uniform_real_distribution<double> U(0.0, 1.0);
+    std::vector<double> xyz(3 * s.A, 0.0);
+    if (s.A == 1) return xyz;
+    const double rmax = s.R + 10.0 * s.a;
+    std::vector<double> r(s.A);
+    for (int i = 0; i < s.A; i++) {
+        for (;;) {
+            const double ri = rmax * std::pow(U(rng), 1.0 / 3.0);
+            if (U(rng) <= 1.0 / (1.0 + std::exp((ri - s.R) / s.a))) {
+                r[i] = ri;
+                break;
+            }
+        }
+    }
+    std::sort(r.begin(), r.end());
+    const double d2 = dmin * dmin;
+    for (int i = 0; i < s.A; i++) {
+        double x = 0, y = 0, z = 0;
+        for (int tries = 0; tries < 100; tries++) {
+            const double phi = 2.0 * M_PI * U(rng);
+            const double th = std::acos(1.0 - 2.0 * U(rng));
+            x = r[i] * std::sin(th) * std::cos(phi);
+            y = r[i] * std::sin(th) * std::sin(phi);
+            z = r[i] * std::cos(th);
+            bool ok = true;
+            for (int j = i - 1; j >= 0 && (r[i] - r[j]) * (r[i] - r[j]) <= d2; j--) {
+                const double dx = x - xyz[3 * j], dy = y - xyz[3 * j + 1], dz = z - xyz[3 * j + 2];
+                if (dx * dx + dy * dy + dz * dz < d2) {
+                    ok = false;
+                    break;
+                }
+            }
+            if (ok) break;
+        }
+        xyz[3 * i] = x;
+        xyz[3 * i + 1] = y;
+        xyz[3 * i + 2] = z;
+    }
+    double m[3] = {0, 0, 0};
+    for (int i = 0; i < s.A; i++)
+        for (int k = 0; k < 3; k++) m[k] += xyz[3 * i + k] / s.A;
+    for (int i = 0; i < s.A; i++)
+        for (int k = 0; k < 3; k++) xyz[3 * i + k] -= m[k];
+    // uniform random orientation: rotate by a random unit quaternion
+    std::normal_distribution<double> G(0.0, 1.0);
+    double q[4] = {G(rng), G(rng), G(rng), G(rng)};
+    const double qn = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    for (double &v : q) v /= qn;
+    const double w = q[0], a = q[1], b = q[2], c = q[3];
+    const double R[9] = {1 - 2 * (b * b + c * c), 2 * (a * b - c * w), 2 * (a * c + b * w),
+                         2 * (a * b + c * w), 1 - 2 * (a * a + c * c), 2 * (b * c - a * w),
+                         2 * (a * c - b * w), 2 * (b * c + a * w), 1 - 2 * (a * a + b * b)};
+    for (int i = 0; i < s.A; i++) {
+        const double v[3] = {xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
+        for (int k = 0; k < 3; k++) xyz[3 * i + k] = R[3 * k] * v[0] + R[3 * k + 1] * v[1] + R[3 * k + 2] * v[2];
+    }
+    return xyz;
+}
+
+// g^2 mu^2 (lattice units) from nucleon positions shifted by xshift along x
+std::vector<double> g2mu_map(const std::vector<double> &xyz, double xshift, int N, double L,
+                             double BG, double g, double QsMax, double QsmuRatio) {
+    const double a = L / N, B = BG * kHbarc * kHbarc;
+    const int A = (int)xyz.size() / 3;
+    std::vector<double> gx((size_t)A * N), gy((size_t)A * N), T((size_t)N * N, 0.0);
+    for (int k = 0; k < A; k++)
+        for (int i = 0; i < N; i++) {
+            const double x = -L / 2. + a * i;
+            gx[(size_t)k * N + i] = std::exp(-(x - xyz[3 * k] - xshift) * (x - xyz[3 * k] - xshift) / (2 * B));
+            gy[(size_t)k * N + i] = std::exp(-(x - xyz[3 * k + 1]) * (x - xyz[3 * k + 1]) / (2 * B));
+        }
+    double tmax = 0;
+    for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) {
+            double s = 0;
+            for (int k = 0; k < A; k++) s += gx[(size_t)k * N + i] * gy[(size_t)k * N + j];
+            T[(size_t)i * N + j] = s / (2 * M_PI * B);
+            tmax = std::max(tmax, T[(size_t)i * N + j]);
+        }
+    for (double &t : T) {
+        const double qs2 = QsMax * QsMax * (tmax > 0 ? t / tmax : 0.0);
+        t = qs2 / (QsmuRatio * QsmuRatio) * a * a / (kHbarc * kHbarc) / (g * g);
+    }
+    return T;
+}
+
+// ------------------------------------------------------------- V files
+void write_vfile(const std::string &name, int N, double L, double y, const std::vector<double> &V) {
+    std::ofstream f(name.c_str(), std::ios::out | std::ios::binary);
+    int nc = 3;
+    double a = L / N;
+    f.write((const char *)&N, sizeof(int));
+    f.write((const char *)&nc, sizeof(int));
+    f.write((const char *)&L, sizeof(double));
+    f.write((const char *)&a, sizeof(double));
+    f.write((const char *)&y, sizeof(double));
+    // record ix*N+iy holds the cell N*iy+ix (Init.cpp:1943-1957)
+    for (int ix = 0; ix < N; ix++)
+        for (int iy = 0; iy < N; iy++)
+            f.write((const char *)&V[18 * ((size_t)N * iy + ix)], 18 * sizeof(double));
+}
+
+bool read_vfile(const std::string &name, int N, double L, double shift, std::vector<double> &V) {
+    std::ifstream f(name.c_str(), std::ios::in | std::ios::binary);
+    if (!f) return false;
+    int n = 0, nc = 0;
+    double l = 0, a = 0, y = 0;
+    f.read((char *)&n, sizeof(int));
+    f.read((char *)&nc, sizeof(int));
+    f.read((char *)&l, sizeof(double));
+    f.read((char *)&a, sizeof(double));
+    f.read((char *)&y, sizeof(double));
+    if (n != N || std::abs(l - L) > 1e-5) {
+        std::cerr << "# ERROR V file " << name << " has N=" << n << " L=" << l << std::endl;
+        return false;
+    }
+    V.assign((size_t)18 * N * N, 0.0);
+    for (int k = 0; k < N * N; k++) V[18 * (size_t)k] = V[18 * (size_t)k + 8] = V[18 * (size_t)k + 16] = 1.0;
+    const double aa = L / N;
+    std::vector<double> rec(18);
+    for (long r = 0; r < (long)N * N; r++) {
+        if (!f.read((char *)rec.data(), 18 * sizeof(double))) break;
+        const int iy = (int)(r / N), ixIn = (int)(r - (long)N * iy);
+        const int ix = (int)std::round((aa * ixIn + shift) / aa);  // Init.cpp:2190-2194
+        const long idx = (long)N * ix + iy;
+        if (idx < 0 || idx >= (long)N * N) continue;
+        std::memcpy(&V[18 * (size_t)idx], rec.data(), 18 * sizeof(double));
+    }
+    return true;
+}
+
+void check(ipg_ctx *ctx, ipg_status st, const char *what) {
+    if (st == IPG_OK) return;
+    std::cerr << what << " failed (" << st << "): " << ipg_last_error(ctx) << std::endl;
+    if (st != IPG_ERR_NEWTON_NONCONVERGED) std::exit(1);
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    const std::string file = argc > 1 ? argv[1] : "input";
+    const int nev = argc == 3 ? std::atoi(argv[2]) : 1;
+    InputFile in(file);
+
+    ipg_config cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.size = in.i("size");
+    cfg.Nc = in.i("Nc");
+    cfg.Ny = in.i("Ny");
+    cfg.L = in.d("L");
+    cfg.g = in.d("g");
+    cfg.m = in.d("m");
+    cfg.UVdamp = in.d("UVdamp");
+    cfg.maxtime = in.d("maxtime");
+    cfg.dtau = in.d_or("dtauOverride", 0.0);  // the reference derives dtau
+    cfg.precision = in.d_or("precisionFP32", 0.0) > 0 ? IPG_FP32 : IPG_FP64;
+    cfg.device = (int)in.d_or("device", 0.0);
+    const int writeOutputs = in.i("writeOutputs");
+    const int sizeOutput = in.i("sizeOutput");
+    const double LOutput = in.d("LOutput");
+    const int etaSizeOutput = in.i("etaSizeOutput");
+    const double detaOutput = in.d("detaOutput");
+    const int readV = in.i("readInitialWilsonLines");
+    const int writeV = in.i("writeInitialWilsonLines");
+    const int useNucleus = in.i("useNucleus");
+    const double bmin = in.d("bmin"), bmax = in.d("bmax");
+    const int linearb = in.i("samplebFromLinearDistribution");
+    const double BG = in.d("BG"), QsmuRatio = in.d("QsmuRatio");
+    const double QsMax = in.d_or("QsMax", 1.5);
+    const double rapidity = in.d("Rapidity");
+    unsigned long long seed = in.ull("seed");
+    if (in.i("useTimeForSeed") == 1) seed = std::random_device{}();
+    if ((readV != 0 && readV != 2) || (writeV != 0 && writeV != 2)) {
+        std::cerr << "only the binary Wilson-line format (2) is supported" << std::endl;
+        return 1;
+    }
+    std::cout << "Random seed = " << seed << std::endl;
+
+    std::mt19937_64 rng(seed);
+    ipg_ctx *ctx = nullptr;
+    cfg.seed = seed;
+    check(ctx, ipg_create(&cfg, &ctx), "ipg_create");
+    double dtau = 0;
+    int itmax = 0;
+    ipg_time_grid(ctx, &dtau, &itmax);
+    const int N = cfg.size;
+    const size_t n = (size_t)N * N;
+    const double a = cfg.L / N;
+
+    for (int iev = 0; iev < nev; iev++) {
+        const int event_id = iev;  // rank + iev * size with one rank
+        const auto t0 = std::chrono::steady_clock::now();
+        std::uniform_real_distribution<double> U(0.0, 1.0);
+        const double xb = U(rng);
+        double b = 0.0;
+        if (useNucleus)
+            b = linearb ? std::sqrt((bmax * bmax - bmin * bmin) * xb + bmin * bmin)
+                        : (bmax - bmin) * xb + bmin;
+        ipg_init_report rep;
+        std::memset(&rep, 0, sizeof(rep));
+        if (readV == 2) {
+            std::vector<double> VA, VB;
+            std::ostringstream n1, n2;
+            n1 << "V-" << event_id + 2 * seed;
+            n2 << "V-" << event_id + (1 + 2 * seed);
+            if (!read_vfile(n1.str(), N, cfg.L, -b / 2., VA) ||
+                !read_vfile(n2.str(), N, cfg.L, b / 2., VB)) {
+                std::cerr << "cannot read the Wilson-line files " << n1.str() << ", " << n2.str()
+                          << std::endl;
+                return 1;
+            }
+            check(ctx, ipg_set_field(ctx, IPG_VA, VA.data()), "ipg_set_field");
+            check(ctx, ipg_set_field(ctx, IPG_VB, VB.data()), "ipg_set_field");
+            check(ctx, ipg_init_from_wilson_lines(ctx, &rep), "ipg_init_from_wilson_lines");
+        } else {
+            const Species sA = species(in.str("Projectile"), in);
+            const Species sB = species(in.str("Target"), in);
+            const double dmin = in.i("setWSDeformParams") ? in.d("d_min") : 0.4;
+            const auto nA = sample_nucleus(rng, sA, dmin);
+            const auto nB = sample_nucleus(rng, sB, dmin);
+            const auto gA = g2mu_map(nA, -b / 2., N, cfg.L, BG, cfg.g, QsMax, QsmuRatio);
+            const auto gB = g2mu_map(nB, b / 2., N, cfg.L, BG, cfg.g, QsMax, QsmuRatio);
+            check(ctx, ipg_set_g2mu(ctx, gA.data(), gB.data()), "ipg_set_g2mu");
+            check(ctx, ipg_reseed(ctx, seed * 1000003ULL + event_id), "ipg_reseed");
+            check(ctx, ipg_use_device_noise(ctx), "ipg_use_device_noise");
+            check(ctx, ipg_init_fields(ctx, &rep), "ipg_init_fields");
+            if (writeV == 2) {
+                std::vector<double> V(18 * n);
+                std::ostringstream n1, n2;
+                n1 << "V-" << event_id + 2 * seed;
+                n2 << "V-" << event_id + (1 + 2 * seed);
+                check(ctx, ipg_get_field(ctx, IPG_VA, V.data()), "ipg_get_field");
+                write_vfile(n1.str(), N, cfg.L, rapidity, V);
+                check(ctx, ipg_get_field(ctx, IPG_VB, V.data()), "ipg_get_field");
+                write_vfile(n2.str(), N, cfg.L, rapidity, V);
+            }
+        }
+        ipg_result res;
+        check(ctx, ipg_run(ctx, &res), "ipg_run");
+        std::vector<double> eps(n), u4(4 * n), pi10(10 * n), T10(10 * n);
+        check(ctx, ipg_get_observables(ctx, eps.data(), u4.data(), pi10.data(), T10.data()),
+              "ipg_get_observables");
+        char hname[256], tname[256];
+        ipg_output_names(event_id, itmax, dtau, a, hname, sizeof(hname), tname, sizeof(tname));
+        if (writeOutputs % 2 == 1) {
+            double etot = 0;
+            ipg_write_hydro(hname, N, cfg.L, sizeOutput, LOutput, etaSizeOutput, detaOutput,
+                            itmax, dtau, eps.data(), u4.data(), pi10.data(), 1.0, &etot);
+            std::cout << "Etot = " << etot << " GeV " << std::endl;
+        }
+        if (writeOutputs / 4 == 1)
+            ipg_write_tmunu(tname, N, cfg.L, sizeOutput, LOutput, etaSizeOutput, detaOutput,
+                            itmax, dtau, T10.data(), 1.0);
+        const double sec =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::cout << "event " << event_id << ": b=" << b << " fm, itmax=" << res.itmax
+                  << ", Gauss violation=" << res.gauss_violation
+                  << ", eps2=" << res.eccentricity[1] << ", E_T=" << res.E_T
+                  << " GeV, Newton restarts/failures=" << rep.newton_restarted << "/"
+                  << rep.newton_failed << ", " << sec << " s" << std::endl;
+    }
+    ipg_destroy(ctx);
+    return 0;
+}
