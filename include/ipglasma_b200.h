@@ -129,7 +129,8 @@ ipg_status ipg_set_g2mu_device(ipg_ctx *ctx, const double *d_g2mu2A,
  * draw order of Init::setV, so rho = g sqrt(g2mu2/Ny) xi reproduces
  * Init.cpp:1695-1705 and 1773-1783. Host arrays of Ny*N*N*8 doubles. */
 ipg_status ipg_set_noise(ipg_ctx *ctx, const double *xiA, const double *xiB);
-/* same, device pointers; they must stay valid until ipg_init_fields returns */
+/* same, device pointers, 16-byte aligned; they must stay valid until
+ * ipg_init_fields returns */
 ipg_status ipg_set_noise_device(ipg_ctx *ctx, const double *d_xiA,
                                 const double *d_xiB);
 /* Draw the noise on the device (Philox4x32-10 keyed by cfg.seed) instead of
@@ -216,7 +217,8 @@ ipg_status ipg_output_names(int event_id, int it, double dtau, double a,
  * ipg_init_fields computes for V_A (or V_B): rho = g sqrt(g2mu2/Ny) xi, the
  * Poisson solve and the ordered product of the Ny sheet exponentials, on the
  * given stream (NULL = default stream). All pointers are device pointers the
- * caller owns: d_g2mu2[N*N], d_xi[Ny][N*N][8], output d_V[N*N*18] (3x3 per
+ * caller owns: d_g2mu2[N*N], d_xi[Ny][N*N][8] (16-byte aligned), output
+ * d_V[N*N*18] (3x3 per
  * site, row-major (re, im)). Scratch lives in one fixed device array sized for
  * N <= 256 (about 14 MB per GPU that loads the library, kept until exit);
  * larger N returns IPG_ERR_BAD_CONFIG. The first call on a device looks up

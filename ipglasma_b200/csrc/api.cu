@@ -43,6 +43,7 @@ struct ipg_ctx {
     // initial-condition scratch
     double2 *twiddle = nullptr;
     double *green = nullptr;
+    double *amp = nullptr;
     double2 *work = nullptr;
     int work_sheets = 0;
     C<double> *VA = nullptr, *VB = nullptr;
@@ -328,6 +329,7 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
     IPG_TRY(dalloc(c, &c->g2mu2B, n));
     IPG_TRY(dalloc(c, &c->twiddle, (size_t)N));
     IPG_TRY(dalloc(c, &c->green, n));
+    IPG_TRY(dalloc(c, &c->amp, n));
     // work buffer of a sheet batch: ~64 MB so it stays in L2
     const size_t per_sheet = 4 * n * sizeof(double2);
     c->work_sheets = (int)std::max<size_t>(1, (64ull << 20) / per_sheet);
@@ -447,6 +449,9 @@ ipg_status ipg_set_noise(ipg_ctx *c, const double *A, const double *B) {
 
 ipg_status ipg_set_noise_device(ipg_ctx *c, const double *A, const double *B) {
     if (!c || !A || !B) return fail(c, IPG_ERR_BAD_CONFIG, "null argument");
+    // colour pairs are read as 16-byte vectors
+    if (((uintptr_t)A | (uintptr_t)B) & 15)
+        return fail(c, IPG_ERR_BAD_CONFIG, "noise arrays must be 16-byte aligned");
     c->xiA = A;
     c->xiB = B;
     c->have_noise = true;
@@ -489,8 +494,11 @@ static ipg_status init_impl(ipg_ctx *c, ipg_init_report *rep, bool from_wilson) 
         w.nucleus = (uint32_t)nuc;
         w.twiddle = c->twiddle;
         w.green = c->green;
+        w.amp = c->amp;
         w.work = c->work;
         w.V = V;
+        launch_wilson_amp(w, c->stream);
+        IPG_LAUNCHED(c, 1);
         for (int k0 = 0; k0 < c->cfg.Ny; k0 += c->work_sheets) {
             const int ns = std::min(c->work_sheets, c->cfg.Ny - k0);
             launch_wilson_sheets(w, k0, ns, c->stream);

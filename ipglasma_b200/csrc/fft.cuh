@@ -3,7 +3,8 @@
 // Length N = 2^LOGN (8 <= N <= 2048), N/8 threads per sequence, each thread
 // holding 8 points in registers per pass. Passes are radix 8 while at least
 // three factors of two remain, then one radix-4 or radix-2 pass, so N = 512
-// takes 3 shared-memory passes instead of 9 radix-2 passes. The autosort
+// takes 3 passes instead of 9 radix-2 passes, and only the data exchange
+// between consecutive passes goes through shared memory. The autosort
 // (Stockham) indexing keeps input and output in natural order:
 //   pass with radix R, sub-length Ns:  for butterfly j < N/R,
 //     v[r] = x[j + r N/R] * w^(r (j mod Ns) N/(Ns R)),  v = DFT_R(v),
@@ -91,55 +92,128 @@ __device__ __forceinline__ void dft_r(C<T> *v) {
 __host__ __device__ constexpr int fft_pad(int p) { return p + (p >> 3); }
 __host__ __device__ constexpr int fft_seq_stride(int N) { return N + (N >> 3) + 1; }
 
-// One Stockham pass on the sequence in `buf`; t = thread index within the
-// sequence (0 .. N/8-1). Caller brackets with __syncthreads().
-template <int LOGN, int R, typename T, bool INV>
-__device__ __forceinline__ void stockham_pass(C<T> *buf, int t, int Ns,
-                                              const C<T> *__restrict__ tw) {
-    constexpr int N = 1 << LOGN;
-    constexpr int NB = 8 / R;  // butterflies per thread
-    C<T> v[8];
+// Pass schedule of a length-2^LOGN transform: LOGN/3 radix-8 passes, then
+// one radix-4 or radix-2 pass for the remaining factors. Every pass before
+// pass p is radix 8, so its sub-length is Ns = 8^p.
+template <int LOGN>
+struct FftPlan {
+    static constexpr int N = 1 << LOGN;
+    static constexpr int P8 = LOGN / 3, REM = LOGN % 3;
+    static constexpr int PASSES = P8 + (REM ? 1 : 0);
+    static constexpr int radix(int p) { return p < P8 ? 8 : (REM == 2 ? 4 : 2); }
+    static constexpr int ns(int p) { return 1 << (3 * p); }
+};
+
+// The eight points of thread t (0 .. N/8-1) in pass p: butterfly b < 8/R
+// works on j = t + b N/8 and reads points j + r N/R into v[b R + r].
+template <int LOGN, int PASS, typename T>
+__device__ __forceinline__ void pass_load(const C<T> *buf, int t, C<T> v[8]) {
+    constexpr int N = 1 << LOGN, R = FftPlan<LOGN>::radix(PASS), NB = 8 / R;
 #pragma unroll
     for (int b = 0; b < NB; b++) {
         const int j = t + b * (N / 8);
 #pragma unroll
         for (int r = 0; r < R; r++) v[b * R + r] = buf[fft_pad(j + r * (N / R))];
     }
-    __syncthreads();
+}
+
+// Twiddle factors of pass p for thread t (none in pass 0, where Ns = 1).
+template <int LOGN, int PASS, typename T, bool INV>
+__device__ __forceinline__ void pass_twiddles(int t, const C<T> *__restrict__ tw,
+                                              C<T> w[8]) {
+    constexpr int N = 1 << LOGN, R = FftPlan<LOGN>::radix(PASS), NB = 8 / R;
+    constexpr int NS = FftPlan<LOGN>::ns(PASS);
+    if constexpr (NS > 1) {
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            const int j = t + b * (N / 8);
+            const int step = (j & (NS - 1)) * (N / (NS * R));
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                C<T> x = tw[r * step];
+                if (INV) x.i = -x.i;
+                w[b * R + r] = x;
+            }
+        }
+    }
+}
+
+template <int LOGN, int PASS, typename T, bool INV>
+__device__ __forceinline__ void pass_butterflies(C<T> v[8], const C<T> w[8]) {
+    constexpr int R = FftPlan<LOGN>::radix(PASS), NB = 8 / R;
+    constexpr int NS = FftPlan<LOGN>::ns(PASS);
+#pragma unroll
+    for (int b = 0; b < NB; b++) {
+        if constexpr (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; r++) v[b * R + r] = cmul(v[b * R + r], w[b * R + r]);
+        }
+        dft_r<R, T, INV>(v + b * R);
+    }
+}
+
+// Stockham output positions: butterfly output r goes to (j - k) R + k + r Ns
+// with k = j mod Ns.
+template <int LOGN, int PASS, typename T>
+__device__ __forceinline__ void pass_store(C<T> *buf, int t, const C<T> v[8]) {
+    constexpr int N = 1 << LOGN, R = FftPlan<LOGN>::radix(PASS), NB = 8 / R;
+    constexpr int NS = FftPlan<LOGN>::ns(PASS);
 #pragma unroll
     for (int b = 0; b < NB; b++) {
         const int j = t + b * (N / 8);
-        const int k = j & (Ns - 1);
-        const int step = k * (N / (Ns * R));
-#pragma unroll
-        for (int r = 1; r < R; r++) {
-            C<T> w = tw[r * step];
-            if (INV) w.i = -w.i;
-            v[b * R + r] = cmul(v[b * R + r], w);
-        }
-        dft_r<R, T, INV>(v + b * R);
+        const int k = j & (NS - 1);
         const int base = (j - k) * R + k;
 #pragma unroll
-        for (int r = 0; r < R; r++) buf[fft_pad(base + r * Ns)] = v[b * R + r];
+        for (int r = 0; r < R; r++) buf[fft_pad(base + r * NS)] = v[b * R + r];
     }
-    __syncthreads();
 }
 
-// Full transform of the N points in buf (natural order in and out, padded
-// layout fft_pad). All threads of the block must call it (it synchronises
-// the block).
-template <int LOGN, typename T, bool INV>
-__device__ __forceinline__ void block_fft(C<T> *buf, int t,
-                                          const C<T> *__restrict__ tw) {
-    int Ns = 1;
-    constexpr int P8 = LOGN / 3, REM = LOGN % 3;
-#pragma unroll
-    for (int p = 0; p < P8; p++) {
-        stockham_pass<LOGN, 8, T, INV>(buf, t, Ns, tw);
-        Ns *= 8;
+template <int LOGN, int PASS, typename T, bool INV>
+__device__ __forceinline__ void middle_passes(C<T> *buf, int t,
+                                              const C<T> *__restrict__ tw) {
+    if constexpr (PASS < FftPlan<LOGN>::PASSES - 1) {
+        C<T> v[8], w[8];
+        pass_twiddles<LOGN, PASS, T, INV>(t, tw, w);
+        pass_load<LOGN, PASS, T>(buf, t, v);
+        __syncthreads();
+        pass_butterflies<LOGN, PASS, T, INV>(v, w);
+        pass_store<LOGN, PASS, T>(buf, t, v);
+        __syncthreads();
+        middle_passes<LOGN, PASS + 1, T, INV>(buf, t, tw);
     }
-    if constexpr (REM == 2) stockham_pass<LOGN, 4, T, INV>(buf, t, Ns, tw);
-    if constexpr (REM == 1) stockham_pass<LOGN, 2, T, INV>(buf, t, Ns, tw);
+}
+
+// Transform of one length-N sequence spread over N/8 threads, with input and
+// output in registers: on entry x[m] is point t + m N/8 of the sequence, on
+// return x[m] is the transform at frequency t + m N/8. The first pass works on
+// x directly (its input points are exactly these) and the last pass leaves
+// its outputs in the same slots, so shared memory (buf, padded layout
+// fft_pad) carries only the passes in between. All threads of the block call
+// it together; buf may be overwritten as soon as it returns.
+template <int LOGN, typename T, bool INV>
+__device__ __forceinline__ void fft_regs(C<T> x[8], C<T> *buf, int t,
+                                         const C<T> *__restrict__ tw) {
+    using P = FftPlan<LOGN>;
+    constexpr int LAST = P::PASSES - 1;
+    // pass 0: radix 8, Ns = 1, v[r] = point t + r N/8 = x[r]
+    dft8<T, INV>(x);
+    if constexpr (LAST > 0) {
+        pass_store<LOGN, 0, T>(buf, t, x);
+        __syncthreads();
+        middle_passes<LOGN, 1, T, INV>(buf, t, tw);
+        C<T> v[8], w[8];
+        pass_twiddles<LOGN, LAST, T, INV>(t, tw, w);
+        pass_load<LOGN, LAST, T>(buf, t, v);
+        __syncthreads();
+        pass_butterflies<LOGN, LAST, T, INV>(v, w);
+        // in the last pass j < Ns, so output r of butterfly b is frequency
+        // j + r N/R = t + (b + r NB) N/8
+        constexpr int R = P::radix(LAST), NB = 8 / R;
+#pragma unroll
+        for (int b = 0; b < NB; b++)
+#pragma unroll
+            for (int r = 0; r < R; r++) x[b + r * NB] = v[b * R + r];
+    }
 }
 
 }  // namespace ipg

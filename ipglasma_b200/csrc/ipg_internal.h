@@ -43,6 +43,7 @@ struct WilsonArgs {
     int Ny;
     double g;
     const double *g2mu2;     // [n] lattice units
+    double *amp;             // [n] scratch: g sqrt(g2mu2 / Ny) (launch_wilson_amp)
     const double *xi;        // [Ny][n][8] unit normals, or null (Philox)
     uint64_t philox_key;     // used when xi == null
     uint32_t nucleus;        // 0 = A, 1 = B (Philox stream selector)
@@ -53,6 +54,8 @@ struct WilsonArgs {
 };
 void launch_wilson_sheets(const WilsonArgs &w, int k0, int ns,
                           cudaStream_t st);
+// charge amplitude of every site, once per nucleus before its sheets
+void launch_wilson_amp(const WilsonArgs &w, cudaStream_t st);
 
 void launch_green(int N, double m_lat, double uvdamp_lat, double *green,
                   cudaStream_t st);

@@ -45,6 +45,7 @@ struct NoAllocScratch {
     double2 work[4 * kMaxSites];  // one sheet, 4 packed colour channels
     double2 V[9 * kMaxSites];     // Wilson line, 9 complex planes
     double green[kMaxSites];      // Poisson multiplier
+    double amp[kMaxSites];        // charge amplitude g sqrt(g2mu2 / Ny)
     double2 twiddle[kMaxN];       // exp(-2 pi i k / N)
 };
 
@@ -119,6 +120,11 @@ extern "C" ipg_status ipg_wilson_lines_noalloc(int N, int Ny, double L, double g
         fprintf(stderr, "ipg_wilson_lines_noalloc: invalid argument\n");
         return IPG_ERR_BAD_CONFIG;
     }
+    if ((uintptr_t)d_xi & 15) {
+        // colour pairs are read as 16-byte vectors
+        fprintf(stderr, "ipg_wilson_lines_noalloc: d_xi must be 16-byte aligned\n");
+        return IPG_ERR_BAD_CONFIG;
+    }
     NoAllocScratch *S = nullptr;
     cudaError_t e = scratch_address(&S);
     if (e != cudaSuccess) {
@@ -148,8 +154,10 @@ extern "C" ipg_status ipg_wilson_lines_noalloc(int N, int Ny, double L, double g
     w.nucleus = 0;
     w.twiddle = S->twiddle;
     w.green = S->green;
+    w.amp = S->amp;
     w.work = S->work;
     w.V = V;
+    launch_wilson_amp(w, st);
     for (int k = 0; k < Ny; k++) launch_wilson_sheets(w, k, 1, st);
     k_na_to_sites<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, V, d_V);
     e = cudaGetLastError();

@@ -19,7 +19,14 @@
 //   k_rows_inv  inverse row FFTs, 1/N^2
 //   k_wilson    per site: V <- exp(-i A_k.t) V over the batch, sheets in order
 //               (new * old, Init.cpp:1750-1768)
-// The FFTs are the block-level Stockham transforms of fft.cuh.
+// The FFTs are the block-level Stockham transforms of fft.cuh with input and
+// output in registers: thread t of a sequence loads points t + m N/8
+// (m = 0..7) straight from global memory, which is the first pass's operand
+// order, and the last pass leaves frequencies t + m N/8 in the same slots, so
+// they are stored straight back (and, in k_cols, multiplied by the Green
+// function on the way from the forward to the inverse transform). For
+// fixed m, consecutive t (rows) or consecutive columns (k_cols) are
+// consecutive addresses.
 #include <cstdint>
 
 #include "expm.cuh"
@@ -54,126 +61,132 @@ void launch_green(int N, double m_lat, double uvdamp_lat, double *green,
     k_green<<<(n + 255) / 256, 256, 0, st>>>(N, m_lat, uvdamp_lat, green);
 }
 
+// rho = amp xi with amp = g sqrt(g2mu2 / Ny) (Init.cpp:1695-1705), evaluated
+// once per nucleus instead of once per sheet and colour channel
+__global__ void k_amp(int n, double g, double Nyd, const double *g2mu2, double *amp) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) amp[p] = g * sqrt(g2mu2[p] / Nyd);
+}
+
+void launch_wilson_amp(const WilsonArgs &w, cudaStream_t st) {
+    const int n = w.N * w.N;
+    k_amp<<<(n + 255) / 256, 256, 0, st>>>(n, w.g, (double)w.Ny, w.g2mu2, w.amp);
+}
+
 namespace {
 
 // rows of one CTA in the row kernels: a CTA is RPB rows x 4 channels x N/8
+// threads, sequence seq = 4 rl + c
 template <int LOGN>
 constexpr int rows_per_block() {
     return (1 << LOGN) >= 512 ? 1 : ((512 >> LOGN) < (1 << LOGN) ? (512 >> LOGN) : (1 << LOGN));
 }
-// columns of one CTA in the column kernel
+// columns of one CTA in the column kernel: JB columns x N/8 threads, column
+// fastest in the thread index
 template <int LOGN>
 constexpr int cols_per_block() {
     return (1 << LOGN) >= 512 ? 4096 >> LOGN : ((1 << LOGN) < 16 ? (1 << LOGN) : 16);
 }
-
-// eight unit normals of one (nucleus, sheet, site) from the counter stream
-__device__ __forceinline__ void philox_normals8(uint64_t key, uint32_t nucleus,
-                                                uint32_t k, uint32_t pos,
-                                                double z[8]) {
-    normal4({pos, k, (nucleus << 1) | 0u, 0u}, key, z);
-    normal4({pos, k, (nucleus << 1) | 1u, 0u}, key, z + 4);
+template <int LOGN>
+constexpr int row_threads() {
+    return rows_per_block<LOGN>() * 4 * ((1 << LOGN) / 8);
+}
+template <int LOGN>
+constexpr int col_threads() {
+    return cols_per_block<LOGN>() * ((1 << LOGN) / 8);
 }
 
 }  // namespace
 
 template <int LOGN>
-__global__ void __launch_bounds__(LOGN >= 11 ? 1024 : 512) k_rows_fwd(WilsonArgs w, int k0) {
+__global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_fwd(WilsonArgs w, int k0) {
     constexpr int N = 1 << LOGN, TPS = N / 8, RPB = rows_per_block<LOGN>();
     constexpr int S = fft_seq_stride(N);
     extern __shared__ __align__(16) unsigned char smraw[];
     C<double> *sm = reinterpret_cast<C<double> *>(smraw);
     const size_t n = (size_t)N * N;
-    const int ix0 = blockIdx.x * RPB;
-    const int s = blockIdx.y, k = k0 + s;
-    const double Nyd = (double)w.Ny;
-    const C<double> *tw = reinterpret_cast<const C<double> *>(w.twiddle);
-    for (int idx = threadIdx.x; idx < RPB * N; idx += blockDim.x) {
-        const int rl = idx / N, j = idx - rl * N;
-        const size_t pos = (size_t)(ix0 + rl) * N + j;
-        const double amp = w.g * sqrt(w.g2mu2[pos] / Nyd);
-        double z[8];
-        if (w.xi) {
-            const double *src = w.xi + ((size_t)k * n + pos) * 8;
-#pragma unroll
-            for (int a = 0; a < 8; a++) z[a] = src[a];
-        } else {
-            philox_normals8(w.philox_key, w.nucleus, (uint32_t)k, (uint32_t)pos, z);
-        }
-#pragma unroll
-        for (int c = 0; c < 4; c++) sm[(rl * 4 + c) * S + fft_pad(j)] = {amp * z[2 * c], amp * z[2 * c + 1]};
-    }
-    __syncthreads();
     const int seq = threadIdx.x / TPS, t = threadIdx.x - seq * TPS;
-    block_fft<LOGN, double, false>(sm + seq * S, t, tw);
-    for (int idx = threadIdx.x; idx < RPB * 4 * N; idx += blockDim.x) {
-        const int q = idx / N, j = idx - q * N;
-        const int rl = q >> 2, c = q & 3;
-        const C<double> v = sm[q * S + fft_pad(j)];
-        w.work[((size_t)s * 4 + c) * n + (size_t)(ix0 + rl) * N + j] = make_double2(v.r, v.i);
+    const int rl = seq >> 2, c = seq & 3;
+    const int s = blockIdx.y, k = k0 + s;
+    const size_t row = (size_t)(blockIdx.x * RPB + rl) * N;
+    const C<double> *tw = reinterpret_cast<const C<double> *>(w.twiddle);
+    double amp[8], z[8][2];
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        const size_t pos = row + t + m * TPS;
+        amp[m] = w.amp[pos];
+        if (w.xi) {
+            // colours 2c, 2c+1 of the site
+            const double2 v =
+                *reinterpret_cast<const double2 *>(w.xi + ((size_t)k * n + pos) * 8 + 2 * c);
+            z[m][0] = v.x;
+            z[m][1] = v.y;
+        } else {
+            // colours 0-3 come from counter half 0, 4-7 from half 1
+            normal2({(uint32_t)pos, (uint32_t)k, (w.nucleus << 1) | (uint32_t)(c >> 1), 0u},
+                    w.philox_key, c & 1, z[m]);
+        }
     }
+    C<double> x[8];
+#pragma unroll
+    for (int m = 0; m < 8; m++) x[m] = {amp[m] * z[m][0], amp[m] * z[m][1]};
+    fft_regs<LOGN, double, false>(x, sm + seq * S, t, tw);
+    double2 *out = w.work + ((size_t)s * 4 + c) * n + row + t;
+#pragma unroll
+    for (int m = 0; m < 8; m++) out[m * TPS] = make_double2(x[m].r, x[m].i);
 }
 
 template <int LOGN>
-__global__ void __launch_bounds__(512) k_cols(WilsonArgs w) {
+__global__ void __launch_bounds__(col_threads<LOGN>()) k_cols(WilsonArgs w) {
     constexpr int N = 1 << LOGN, TPS = N / 8, JB = cols_per_block<LOGN>();
     constexpr int S = fft_seq_stride(N);
     extern __shared__ __align__(16) unsigned char smraw[];
     C<double> *sm = reinterpret_cast<C<double> *>(smraw);
     const size_t n = (size_t)N * N;
-    const int jb = blockIdx.x * JB;
+    const int q = threadIdx.x & (JB - 1), t = threadIdx.x / JB;
+    const int col = blockIdx.x * JB + q;
     const int c = blockIdx.y, s = blockIdx.z;
-    double2 *base = w.work + ((size_t)s * 4 + c) * n;
+    double2 *base = w.work + ((size_t)s * 4 + c) * n + col;
     const C<double> *tw = reinterpret_cast<const C<double> *>(w.twiddle);
-    for (int idx = threadIdx.x; idx < N * JB; idx += blockDim.x) {
-        const int i = idx / JB, q = idx - i * JB;
-        const double2 v = base[(size_t)i * N + jb + q];
-        sm[q * S + fft_pad(i)] = {v.x, v.y};
+    C<double> x[8];
+    double gk[8];
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        const double2 v = base[(size_t)(t + m * TPS) * N];
+        x[m] = {v.x, v.y};
     }
-    __syncthreads();
-    const int seq = threadIdx.x / TPS, t = threadIdx.x - seq * TPS;
-    block_fft<LOGN, double, false>(sm + seq * S, t, tw);
-    for (int idx = threadIdx.x; idx < N * JB; idx += blockDim.x) {
-        const int q = idx / N, i = idx - q * N;
-        const double gk = w.green[(size_t)i * N + jb + q];
-        sm[q * S + fft_pad(i)] = {sm[q * S + fft_pad(i)].r * gk, sm[q * S + fft_pad(i)].i * gk};
-    }
-    __syncthreads();
-    block_fft<LOGN, double, true>(sm + seq * S, t, tw);
-    for (int idx = threadIdx.x; idx < N * JB; idx += blockDim.x) {
-        const int i = idx / JB, q = idx - i * JB;
-        const C<double> v = sm[q * S + fft_pad(i)];
-        base[(size_t)i * N + jb + q] = make_double2(v.r, v.i);
-    }
+#pragma unroll
+    for (int m = 0; m < 8; m++) gk[m] = w.green[(size_t)(t + m * TPS) * N + col];
+    fft_regs<LOGN, double, false>(x, sm + q * S, t, tw);
+#pragma unroll
+    for (int m = 0; m < 8; m++) x[m] = {x[m].r * gk[m], x[m].i * gk[m]};
+    fft_regs<LOGN, double, true>(x, sm + q * S, t, tw);
+#pragma unroll
+    for (int m = 0; m < 8; m++) base[(size_t)(t + m * TPS) * N] = make_double2(x[m].r, x[m].i);
 }
 
 template <int LOGN>
-__global__ void __launch_bounds__(LOGN >= 11 ? 1024 : 512) k_rows_inv(WilsonArgs w) {
+__global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_inv(WilsonArgs w) {
     constexpr int N = 1 << LOGN, TPS = N / 8, RPB = rows_per_block<LOGN>();
     constexpr int S = fft_seq_stride(N);
     extern __shared__ __align__(16) unsigned char smraw[];
     C<double> *sm = reinterpret_cast<C<double> *>(smraw);
     const size_t n = (size_t)N * N;
-    const int ix0 = blockIdx.x * RPB;
-    const int s = blockIdx.y;
-    const C<double> *tw = reinterpret_cast<const C<double> *>(w.twiddle);
-    for (int idx = threadIdx.x; idx < RPB * 4 * N; idx += blockDim.x) {
-        const int q = idx / N, j = idx - q * N;
-        const int rl = q >> 2, c = q & 3;
-        const double2 v = w.work[((size_t)s * 4 + c) * n + (size_t)(ix0 + rl) * N + j];
-        sm[q * S + fft_pad(j)] = {v.x, v.y};
-    }
-    __syncthreads();
     const int seq = threadIdx.x / TPS, t = threadIdx.x - seq * TPS;
-    block_fft<LOGN, double, true>(sm + seq * S, t, tw);
-    const double ntot = (double)n;
-    for (int idx = threadIdx.x; idx < RPB * 4 * N; idx += blockDim.x) {
-        const int q = idx / N, j = idx - q * N;
-        const int rl = q >> 2, c = q & 3;
-        const C<double> v = sm[q * S + fft_pad(j)];
-        w.work[((size_t)s * 4 + c) * n + (size_t)(ix0 + rl) * N + j] =
-            make_double2(v.r / ntot, v.i / ntot);
+    const int rl = seq >> 2, c = seq & 3;
+    const int s = blockIdx.y;
+    double2 *p = w.work + ((size_t)s * 4 + c) * n + (size_t)(blockIdx.x * RPB + rl) * N + t;
+    const C<double> *tw = reinterpret_cast<const C<double> *>(w.twiddle);
+    C<double> x[8];
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        const double2 v = p[m * TPS];
+        x[m] = {v.x, v.y};
     }
+    fft_regs<LOGN, double, true>(x, sm + seq * S, t, tw);
+    const double ntot = (double)n;
+#pragma unroll
+    for (int m = 0; m < 8; m++) p[m * TPS] = make_double2(x[m].r / ntot, x[m].i / ntot);
 }
 
 // V <- exp(-i A_k.t) V for the sheets of the batch, in ascending k
@@ -198,23 +211,21 @@ __global__ void __launch_bounds__(128) k_wilson(WilsonArgs w, int ns) {
 
 template <int LOGN>
 static void launch_sheets(const WilsonArgs &w, int k0, int ns, cudaStream_t st) {
-    constexpr int N = 1 << LOGN, TPS = N / 8;
+    constexpr int N = 1 << LOGN;
     constexpr int RPB = rows_per_block<LOGN>(), JB = cols_per_block<LOGN>();
     const size_t row_smem = sizeof(double2) * RPB * 4 * fft_seq_stride(N);
     const size_t col_smem = sizeof(double2) * JB * fft_seq_stride(N);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_rows_fwd<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)row_smem);
-        cudaFuncSetAttribute(k_rows_inv<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)row_smem);
-        cudaFuncSetAttribute(k_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)col_smem);
-        attr = true;
-    }
-    k_rows_fwd<LOGN><<<dim3(N / RPB, ns), RPB * 4 * TPS, row_smem, st>>>(w, k0);
-    k_cols<LOGN><<<dim3(N / JB, 4, ns), JB * TPS, col_smem, st>>>(w);
-    k_rows_inv<LOGN><<<dim3(N / RPB, ns), RPB * 4 * TPS, row_smem, st>>>(w);
+    // the attribute is per device: set it on every launch (a host-side call
+    // without a device round trip)
+    cudaFuncSetAttribute(k_rows_fwd<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)row_smem);
+    cudaFuncSetAttribute(k_rows_inv<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)row_smem);
+    cudaFuncSetAttribute(k_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)col_smem);
+    k_rows_fwd<LOGN><<<dim3(N / RPB, ns), row_threads<LOGN>(), row_smem, st>>>(w, k0);
+    k_cols<LOGN><<<dim3(N / JB, 4, ns), col_threads<LOGN>(), col_smem, st>>>(w);
+    k_rows_inv<LOGN><<<dim3(N / RPB, ns), row_threads<LOGN>(), row_smem, st>>>(w);
     const size_t n = (size_t)N * N;
     k_wilson<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
 }
