@@ -213,29 +213,26 @@ __global__ void __launch_bounds__(128)
 // Matrix.h:67-109), also in deviation form.
 // ===========================================================================
 
-// (1+a)(1+b) - 1
+// (1+a)(1+b) - 1 = (a + b) + ab, the product chained onto a + b
 template <typename T>
 __device__ __forceinline__ M3<T> dmul(const M3<T> &a, const M3<T> &b) {
-    M3<T> c = mul(a, b);
-    add_to(c, a);
-    add_to(c, b);
-    return c;
+    M3<T> z = a;
+    add_to(z, b);
+    return mul_acc<false, false>(a, b, z);
 }
 // (1+a)(1+b)^dag - 1
 template <typename T>
 __device__ __forceinline__ M3<T> dmul_nd(const M3<T> &a, const M3<T> &b) {
-    M3<T> c = mul_nd(a, b);
-    add_to(c, a);
-    add_to(c, dagger(b));
-    return c;
+    M3<T> z = a;
+    add_to(z, dagger(b));
+    return mul_acc<false, true>(a, b, z);
 }
 // (1+a)^dag (1+b) - 1
 template <typename T>
 __device__ __forceinline__ M3<T> dmul_dn(const M3<T> &a, const M3<T> &b) {
-    M3<T> c = mul_dn(a, b);
-    add_to(c, dagger(a));
-    add_to(c, b);
-    return c;
+    M3<T> z = dagger(a);
+    add_to(z, b);
+    return mul_acc<true, false>(a, b, z);
 }
 
 // connection part of (1+w) H (1+w)^dag, i.e. the transport minus H:

@@ -44,74 +44,82 @@ __host__ __device__ __forceinline__ void set_identity(M3<T> &a) {
     a.m[0].r = a.m[4].r = a.m[8].r = T(1);
 }
 
-// C = A * B
-template <typename T>
-__host__ __device__ __forceinline__ M3<T> mul(const M3<T> &a, const M3<T> &b) {
+// Entry (r, k) of A (DAG = false) or of A^dag (DAG = true).
+template <bool DAG, typename T>
+__host__ __device__ __forceinline__ C<T> entry(const M3<T> &a, int r, int k) {
+    if constexpr (DAG)
+        return {a.m[3 * k + r].r, -a.m[3 * k + r].i};
+    else
+        return a.m[3 * r + k];
+}
+
+// Z + op(A) op(B), each entry one chain of 12 fused multiply-adds that starts
+// from the accumulator, so every real product is one FMA (the negations fold
+// into the FMA operands).
+template <bool DA, bool DB, typename T>
+__host__ __device__ __forceinline__ M3<T> mul_acc(const M3<T> &a, const M3<T> &b,
+                                                  const M3<T> &z) {
     M3<T> c;
 #pragma unroll
     for (int r = 0; r < 3; r++)
 #pragma unroll
         for (int s = 0; s < 3; s++) {
-            T re = a.m[3 * r].r * b.m[s].r - a.m[3 * r].i * b.m[s].i;
-            T im = a.m[3 * r].r * b.m[s].i + a.m[3 * r].i * b.m[s].r;
+            T re = z.m[3 * r + s].r, im = z.m[3 * r + s].i;
 #pragma unroll
-            for (int k = 1; k < 3; k++) {
-                re += a.m[3 * r + k].r * b.m[3 * k + s].r -
-                      a.m[3 * r + k].i * b.m[3 * k + s].i;
-                im += a.m[3 * r + k].r * b.m[3 * k + s].i +
-                      a.m[3 * r + k].i * b.m[3 * k + s].r;
+            for (int k = 0; k < 3; k++) {
+                const C<T> x = entry<DA>(a, r, k), y = entry<DB>(b, k, s);
+                re += x.r * y.r;
+                re -= x.i * y.i;
+                im += x.r * y.i;
+                im += x.i * y.r;
             }
             c.m[3 * r + s] = {re, im};
         }
     return c;
+}
+
+template <bool DA, bool DB, typename T>
+__host__ __device__ __forceinline__ M3<T> mul_g(const M3<T> &a, const M3<T> &b) {
+    M3<T> c;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int s = 0; s < 3; s++) {
+            const C<T> x0 = entry<DA>(a, r, 0), y0 = entry<DB>(b, 0, s);
+            T re = x0.r * y0.r, im = x0.r * y0.i;
+            re -= x0.i * y0.i;
+            im += x0.i * y0.r;
+#pragma unroll
+            for (int k = 1; k < 3; k++) {
+                const C<T> x = entry<DA>(a, r, k), y = entry<DB>(b, k, s);
+                re += x.r * y.r;
+                re -= x.i * y.i;
+                im += x.r * y.i;
+                im += x.i * y.r;
+            }
+            c.m[3 * r + s] = {re, im};
+        }
+    return c;
+}
+
+// C = A * B
+template <typename T>
+__host__ __device__ __forceinline__ M3<T> mul(const M3<T> &a, const M3<T> &b) {
+    return mul_g<false, false>(a, b);
 }
 
 // C = A * B^dag
 template <typename T>
 __host__ __device__ __forceinline__ M3<T> mul_nd(const M3<T> &a,
                                                  const M3<T> &b) {
-    M3<T> c;
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-#pragma unroll
-        for (int s = 0; s < 3; s++) {
-            // sum_k a[r][k] * conj(b[s][k])
-            T re = a.m[3 * r].r * b.m[3 * s].r + a.m[3 * r].i * b.m[3 * s].i;
-            T im = a.m[3 * r].i * b.m[3 * s].r - a.m[3 * r].r * b.m[3 * s].i;
-#pragma unroll
-            for (int k = 1; k < 3; k++) {
-                re += a.m[3 * r + k].r * b.m[3 * s + k].r +
-                      a.m[3 * r + k].i * b.m[3 * s + k].i;
-                im += a.m[3 * r + k].i * b.m[3 * s + k].r -
-                      a.m[3 * r + k].r * b.m[3 * s + k].i;
-            }
-            c.m[3 * r + s] = {re, im};
-        }
-    return c;
+    return mul_g<false, true>(a, b);
 }
 
 // C = A^dag * B
 template <typename T>
 __host__ __device__ __forceinline__ M3<T> mul_dn(const M3<T> &a,
                                                  const M3<T> &b) {
-    M3<T> c;
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-#pragma unroll
-        for (int s = 0; s < 3; s++) {
-            // sum_k conj(a[k][r]) * b[k][s]
-            T re = a.m[r].r * b.m[s].r + a.m[r].i * b.m[s].i;
-            T im = a.m[r].r * b.m[s].i - a.m[r].i * b.m[s].r;
-#pragma unroll
-            for (int k = 1; k < 3; k++) {
-                re += a.m[3 * k + r].r * b.m[3 * k + s].r +
-                      a.m[3 * k + r].i * b.m[3 * k + s].i;
-                im += a.m[3 * k + r].r * b.m[3 * k + s].i -
-                      a.m[3 * k + r].i * b.m[3 * k + s].r;
-            }
-            c.m[3 * r + s] = {re, im};
-        }
-    return c;
+    return mul_g<true, false>(a, b);
 }
 
 template <typename T>
@@ -138,9 +146,10 @@ __host__ __device__ __forceinline__ T re_trace_mul(const M3<T> &a,
 #pragma unroll
     for (int r = 0; r < 3; r++)
 #pragma unroll
-        for (int k = 0; k < 3; k++)
-            s += a.m[3 * r + k].r * b.m[3 * k + r].r -
-                 a.m[3 * r + k].i * b.m[3 * k + r].i;
+        for (int k = 0; k < 3; k++) {
+            s += a.m[3 * r + k].r * b.m[3 * k + r].r;
+            s -= a.m[3 * r + k].i * b.m[3 * k + r].i;
+        }
     return s;
 }
 
@@ -152,9 +161,10 @@ __host__ __device__ __forceinline__ T im_trace_mul(const M3<T> &a,
 #pragma unroll
     for (int r = 0; r < 3; r++)
 #pragma unroll
-        for (int k = 0; k < 3; k++)
-            s += a.m[3 * r + k].r * b.m[3 * k + r].i +
-                 a.m[3 * r + k].i * b.m[3 * k + r].r;
+        for (int k = 0; k < 3; k++) {
+            s += a.m[3 * r + k].r * b.m[3 * k + r].i;
+            s += a.m[3 * r + k].i * b.m[3 * k + r].r;
+        }
     return s;
 }
 
@@ -240,8 +250,10 @@ __host__ __device__ __forceinline__ H3<T> conj_h(const M3<T> &u,
     for (int r = 0; r < 3; r++) {
         T re = T(0);
 #pragma unroll
-        for (int k = 0; k < 3; k++)
-            re += w.m[3 * r + k].r * u.m[3 * r + k].r + w.m[3 * r + k].i * u.m[3 * r + k].i;
+        for (int k = 0; k < 3; k++) {
+            re += w.m[3 * r + k].r * u.m[3 * r + k].r;
+            re += w.m[3 * r + k].i * u.m[3 * r + k].i;
+        }
         dr[r] = re;
     }
     out.d0 = dr[0];
@@ -255,8 +267,10 @@ __host__ __device__ __forceinline__ H3<T> conj_h(const M3<T> &u,
         T re = T(0), im = T(0);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            re += w.m[3 * r + k].r * u.m[3 * s + k].r + w.m[3 * r + k].i * u.m[3 * s + k].i;
-            im += w.m[3 * r + k].i * u.m[3 * s + k].r - w.m[3 * r + k].r * u.m[3 * s + k].i;
+            re += w.m[3 * r + k].r * u.m[3 * s + k].r;
+            re += w.m[3 * r + k].i * u.m[3 * s + k].i;
+            im += w.m[3 * r + k].i * u.m[3 * s + k].r;
+            im -= w.m[3 * r + k].r * u.m[3 * s + k].i;
         }
         o[q] = {re, im};
     }
@@ -279,8 +293,10 @@ __host__ __device__ __forceinline__ H3<T> conj_h_dag(const M3<T> &u,
     for (int r = 0; r < 3; r++) {
         T re = T(0);
 #pragma unroll
-        for (int k = 0; k < 3; k++)
-            re += u.m[3 * k + r].r * w.m[3 * k + r].r + u.m[3 * k + r].i * w.m[3 * k + r].i;
+        for (int k = 0; k < 3; k++) {
+            re += u.m[3 * k + r].r * w.m[3 * k + r].r;
+            re += u.m[3 * k + r].i * w.m[3 * k + r].i;
+        }
         dr[r] = re;
     }
     out.d0 = dr[0];
@@ -294,8 +310,10 @@ __host__ __device__ __forceinline__ H3<T> conj_h_dag(const M3<T> &u,
         T re = T(0), im = T(0);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            re += u.m[3 * k + r].r * w.m[3 * k + s].r + u.m[3 * k + r].i * w.m[3 * k + s].i;
-            im += u.m[3 * k + r].r * w.m[3 * k + s].i - u.m[3 * k + r].i * w.m[3 * k + s].r;
+            re += u.m[3 * k + r].r * w.m[3 * k + s].r;
+            re += u.m[3 * k + r].i * w.m[3 * k + s].i;
+            im += u.m[3 * k + r].r * w.m[3 * k + s].i;
+            im -= u.m[3 * k + r].i * w.m[3 * k + s].r;
         }
         o[q] = {re, im};
     }
