@@ -100,6 +100,33 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+# ---------------------------------------------------------------------------
+# ranks: events shard across ranks (no data-path collective); each rank draws
+# its own events, the timed region ends with a barrier on every rank and the
+# whole-job figure uses the slowest rank's time
+# ---------------------------------------------------------------------------
+def rank_seed_base(rank: int) -> int:
+    """Seeds of rank r's events start at 1000 (r + 1): disjoint event sets for
+    up to 1000 events per rank."""
+    return 1000 * (rank + 1)
+
+
+def max_over_ranks(dist, values, device):
+    """Element-wise max of per-rank timings (identity without a process group)."""
+    if not dist:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def whole_job_rate(world: int, per_rank: int, ms_max: float) -> float:
+    """Events per second of the whole job: all ranks' events over the slowest
+    rank's time."""
+    return world * per_rank / (ms_max * 1e-3)
+
+
 def make_inputs():
     from ipglasma_b200.synthetic import make_event
     w = WORKLOAD
@@ -153,6 +180,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched uneven-events measurement")
     ap.add_argument("--profile", choices=["fp32", "fp64", "both"], default=None,
                     help="run one warm-up and one timed event per form and exit "
                          "(the command profiled under ncu)")
@@ -203,7 +232,7 @@ def run_ours(args, world, rank, local):
     d_B = torch.tensor(B, dtype=torch.float64, device="cuda")
     l2buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     N = WORKLOAD["N"]
-    seed_base = 1000 * (rank + 1)
+    seed_base = rank_seed_base(rank)
 
     ev32 = ipg.Event(cfg_for(ipg.FP32, seed_base))
     ev64 = ipg.Event(cfg_for(ipg.FP64, seed_base))
@@ -231,14 +260,9 @@ def run_ours(args, world, rank, local):
     t64, lf64 = run_events(torch, ev64, d_A, d_B, K, seed_base + 100, l2buf)
     barrier()
 
-    ms32 = float(np.sum(t32))
-    ms64 = float(np.sum(t64))
-    if dist:
-        tt = torch.tensor([ms32, ms64], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms32, ms64 = tt.tolist()
-    ev_per_s32 = world * K / (ms32 * 1e-3)
-    ev_per_s64 = world * K / (ms64 * 1e-3)
+    ms32, ms64 = max_over_ranks(dist, [float(np.sum(t32)), float(np.sum(t64))], "cuda")
+    ev_per_s32 = whole_job_rate(world, K, ms32)
+    ev_per_s64 = whole_job_rate(world, K, ms64)
     su32 = N * N * itmax / (np.mean(lf32) * 1e-3)
     su64 = N * N * itmax / (np.mean(lf64) * 1e-3)
 
@@ -247,10 +271,7 @@ def run_ours(args, world, rank, local):
 
     # --- end to end through the C ABI with host buffers ---------------------
     e2e = measure_e2e(torch, ipg, A, B, K, seed_base + 500, l2buf, dist)
-    if dist:
-        et = torch.tensor([e2e["ms"]], dtype=torch.float64, device="cuda")
-        dist.all_reduce(et, op=dist.ReduceOp.MAX)
-        e2e["ms"] = et.item()
+    e2e["ms"] = max_over_ranks(dist, [e2e["ms"]], "cuda")[0]
 
     peaks = load_peaks()
     hbm = peaks.get("hbm_gbs", 6650.0)
@@ -258,12 +279,14 @@ def run_ours(args, world, rank, local):
     traffic = load_traffic()
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "traffic": traffic,
-            "kernel": "k_leapfrog<float> (FP32 bulk)",
+            "kernel": "k_leapfrog_split<float,1> (FP32 bulk)",
             "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp32"],
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
             "fp64_kernel": {"achieved": round(su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9, 1),
                             "frac": round(su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9 / hbm, 4),
                             "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp64"]}}
+
+    batched = None if args.no_batched else measure_batched(torch, ipg, rank, dist)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -293,10 +316,11 @@ def run_ours(args, world, rank, local):
                      "site_updates_per_s": round(world * su64, 1)},
             "fp32_over_fp64_events": round(ev_per_s32 / ev_per_s64, 3),
             "error": err,
-            "e2e": {"value": round(world * K / (e2e["ms"] * 1e-3), 3), "unit": "events/s",
+            "e2e": {"value": round(whole_job_rate(world, K, e2e["ms"]), 3), "unit": "events/s",
                     "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
                     "form": "fp32"},
             "roofline": roof,
+            "batched": batched,
             "cpu_baseline": cpu,
             "gpu_launches": int(launches_timed),
             "clocks": clk.summary(),
@@ -307,6 +331,74 @@ def run_ours(args, world, rank, local):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+BATCH = dict(oo=64, pb=16, maxtime=0.4, reps=2)
+
+
+def measure_batched(torch, ipg, rank, dist):
+    """Batched uneven events: 64 O+O at 256^2 (L = 20 fm) and 16 Pb+Pb at 512^2
+    (L = 40 fm), impact parameters uniform in [0, 2R], Ny = 50, FP32 bulk, to
+    tau = 0.4 fm (52 steps for both sizes, a = 0.078125 fm). Per batch: the
+    initial conditions of every event, then one persistent leapfrog launch per
+    step over all 80 lattices (a replayed CUDA graph, launch shape from the
+    autotuner), then the observables of every event."""
+    from ipglasma_b200.synthetic import make_event
+    rng = np.random.default_rng(5 + rank)
+    evs = []
+    for k in range(BATCH["oo"] + BATCH["pb"]):
+        oo = k < BATCH["oo"]
+        N, L, nuc, R = (256, 20.0, "O", 2.61) if oo else (512, 40.0, "Pb", 6.62)
+        A, B, _, _ = make_event(N, L, nuc, rng.uniform(0.0, 2.0 * R), 7000 + 100 * rank + k)
+        ev = ipg.Event(ipg.Config(size=N, L=L, Ny=50, maxtime=BATCH["maxtime"],
+                                  precision=ipg.FP32, seed=rank_seed_base(rank) + 600 + k))
+        ev.set_g2mu(A, B)
+        ev.use_device_noise()
+        evs.append(ev)
+
+    def init_all():
+        for ev in evs:
+            ev.init_fields(allow_nonconverged=True)
+
+    init_all()
+    batch = ipg.Batch(evs)
+    tune = batch.tune()
+    batch.run()  # warm-up: captures the graph
+    times, evo = [], []
+    for r in range(BATCH["reps"]):
+        torch.cuda.synchronize()
+        st = torch.cuda.Event(enable_timing=True)
+        en = torch.cuda.Event(enable_timing=True)
+        st.record()
+        init_all()
+        batch.run()
+        en.record()
+        torch.cuda.synchronize()
+        times.append(st.elapsed_time(en))
+        evo.append(batch.stats()[0])
+    launches = batch.stats()[2]
+    batch.close()
+    for ev in evs:
+        ev.close()
+    ms = max_over_ranks(dist, [float(np.mean(times))], "cuda")[0]
+    n_ev = len(evs)
+    world = dist.get_world_size() if dist else 1
+    sites = BATCH["oo"] * 256 ** 2 + BATCH["pb"] * 512 ** 2
+    steps = evs[0].itmax
+    return {"workload": f"{BATCH['oo']} O+O 256^2 + {BATCH['pb']} Pb+Pb 512^2, "
+                        f"Ny 50, tau {BATCH['maxtime']} fm, FP32 bulk",
+            "events_per_s": round(whole_job_rate(world, n_ev, ms), 2),
+            "ms_per_batch": round(ms, 2),
+            "evolution_ms": round(float(np.mean(evo)), 2),
+            "leapfrog_steps": steps,
+            "site_updates_per_s_evolution": round(sites * steps / (np.mean(evo) * 1e-3), 1),
+            "launches_per_batch_evolution": steps,
+            "cuda_graph": True,
+            "tuned_shape": {"tile_rows": tune.tile_rows, "threads": tune.threads_per_block,
+                            "blocks_per_sm": tune.blocks_per_sm, "grid": tune.grid,
+                            "candidates": tune.candidates},
+            "timing": "CUDA events around init of all events + batched run, mean of "
+                      f"{BATCH['reps']}; total batched launches {launches}"}
 
 
 def compare_forms(ev32, ev64, d_A, d_B, seed):

@@ -209,6 +209,48 @@ ipg_status ipg_output_names(int event_id, int it, double dtau, double a,
                             char *hydro, size_t hydro_len, char *tmunu,
                             size_t tmunu_len);
 
+/* ---- batches of events -------------------------------------------------
+ * The reference runs one event per process (main.cpp:347-359, events handed
+ * to MPI ranks). A batch advances many events -- contexts of possibly
+ * different N (each >= 32) sharing one device, precision and time grid --
+ * together: every leapfrog step is one persistent kernel launch over all
+ * sites of all events, and the whole step sequence is a CUDA graph captured
+ * on the first run and replayed afterwards. This is the multi-event form of
+ * "ipg_evolve(ctx, ev_first, ev_count, nsteps)": each context is one event.
+ * The batch does not own its contexts; destroy it before them. */
+typedef struct ipg_batch ipg_batch;
+
+/* Launch shape chosen by ipg_batch_tune. */
+typedef struct {
+    int variant;            /* tile-shape variant */
+    int tile_rows;          /* a tile is 32 sites along y x tile_rows along x */
+    int threads_per_block;  /* 2 threads per site */
+    int blocks_per_sm;      /* resident blocks of the persistent grid */
+    int grid;               /* blocks_per_sm x SM count */
+    double ms_per_step;     /* measured time of one full step of the batch */
+    int candidates;         /* shapes timed (0 when taken from the cache) */
+    int from_cache;         /* 1 if the shape came from the tuning cache */
+} ipg_tune_report;
+
+const char *ipg_batch_last_error(const ipg_batch *batch);
+ipg_status ipg_batch_create(ipg_ctx *const *events, int count, ipg_batch **out);
+ipg_status ipg_batch_destroy(ipg_batch *batch);
+/* Time every tile shape and resident-block count on one full step of this
+ * batch (events freshly initialised; their E and pi are restored) and keep
+ * the fastest. Results are cached per (device, precision, lattice sizes) in
+ * the process and, if the environment variable IPG_TUNE_CACHE names a file,
+ * in that file. */
+ipg_status ipg_batch_tune(ipg_batch *batch, ipg_tune_report *report);
+/* Evolve every event (freshly initialised with ipg_init_fields) through the
+ * schedule of Evolution::run and compute its observables; results[count].
+ * ms_evolution of each result is the batch's shared leapfrog time. */
+ipg_status ipg_batch_run(ipg_batch *batch, ipg_result *results);
+/* Set the launch shape by hand (variant < 3 for FP32, < 2 for FP64;
+ * 1 <= blocks_per_sm <= what fits on an SM). */
+ipg_status ipg_batch_set_shape(ipg_batch *batch, int variant, int blocks_per_sm);
+ipg_status ipg_batch_stats(const ipg_batch *batch, double *ms_evolution,
+                           double *ms_total, long long *launches);
+
 /* Wilson lines of one nucleus without allocating anything: no counterpart in
  * the reference (it is an addition of this library). For callers that cannot
  * allocate device memory (code inside another framework's memory pool or

@@ -27,7 +27,7 @@ from pathlib import Path
 
 import numpy as np
 
-__all__ = ["Config", "Event", "IPGError", "lib", "FP64", "FP32",
+__all__ = ["Config", "Event", "Batch", "IPGError", "lib", "FP64", "FP32",
            "UX", "UY", "E1", "E2", "PHI", "PI", "VA", "VB", "HBARC"]
 
 HBARC = 0.1973269718  # GeV fm, Phys_consts.h
@@ -69,6 +69,14 @@ class _InitReport(ct.Structure):
     ]
 
 
+class _TuneReport(ct.Structure):
+    _fields_ = [
+        ("variant", ct.c_int), ("tile_rows", ct.c_int), ("threads_per_block", ct.c_int),
+        ("blocks_per_sm", ct.c_int), ("grid", ct.c_int), ("ms_per_step", ct.c_double),
+        ("candidates", ct.c_int), ("from_cache", ct.c_int),
+    ]
+
+
 class _Result(ct.Structure):
     _fields_ = [
         ("itmax", ct.c_int), ("dtau", ct.c_double), ("tau_final", ct.c_double),
@@ -103,6 +111,14 @@ _SIGNATURES = {
     "ipg_get_newton_iterations": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "ipg_last_leapfrog_ms": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double), ct.POINTER(ct.c_int)]),
     "ipg_kernel_launches": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_longlong)]),
+    "ipg_batch_last_error": (ct.c_char_p, [ct.c_void_p]),
+    "ipg_batch_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.c_int, ct.POINTER(ct.c_void_p)]),
+    "ipg_batch_destroy": (ct.c_int, [ct.c_void_p]),
+    "ipg_batch_tune": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
+    "ipg_batch_run": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
+    "ipg_batch_set_shape": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int]),
+    "ipg_batch_stats": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double),
+                                   ct.POINTER(ct.c_longlong)]),
 }
 
 
@@ -313,3 +329,80 @@ class Event:
         c = ct.c_longlong()
         self._check(self._lib.ipg_kernel_launches(self._h, ct.byref(c)))
         return c.value
+
+
+@dataclass
+class TuneReport:
+    variant: int
+    tile_rows: int
+    threads_per_block: int
+    blocks_per_sm: int
+    grid: int
+    ms_per_step: float
+    candidates: int
+    from_cache: int
+
+
+class Batch:
+    """Events advanced together: one persistent launch per leapfrog step over
+    every site of every event, the step sequence replayed as a CUDA graph
+    (``ipg_batch_*``). The events are :class:`Event` objects sharing device,
+    precision and time grid; the batch keeps references to them."""
+
+    def __init__(self, events):
+        self.events = list(events)
+        self._lib = lib()
+        arr = (ct.c_void_p * len(self.events))(*[e._h.value for e in self.events])
+        h = ct.c_void_p()
+        st = self._lib.ipg_batch_create(arr, len(self.events), ct.byref(h))
+        self._h = h
+        if st != 0:
+            msg = self._lib.ipg_batch_last_error(h).decode() if h.value else "allocation"
+            self.close()
+            raise IPGError(st, msg)
+
+    def _check(self, st: int, allow=()):
+        if st != 0 and st not in allow:
+            raise IPGError(st, self._lib.ipg_batch_last_error(self._h).decode())
+        return st
+
+    def tune(self) -> TuneReport:
+        rep = _TuneReport()
+        self._check(self._lib.ipg_batch_tune(self._h, ct.byref(rep)))
+        return TuneReport(*(getattr(rep, f) for f, _ in _TuneReport._fields_))
+
+    def run(self):
+        res = (_Result * len(self.events))()
+        self._check(self._lib.ipg_batch_run(self._h, res))
+        out = []
+        for r in res:
+            vals = {f: getattr(r, f) for f, _ in _Result._fields_}
+            vals["eccentricity"] = list(r.eccentricity)
+            vals["psi"] = list(r.psi)
+            out.append(Result(**vals))
+        return out
+
+    def set_shape(self, variant: int, blocks_per_sm: int) -> None:
+        self._check(self._lib.ipg_batch_set_shape(self._h, variant, blocks_per_sm))
+
+    def stats(self):
+        ev, tot, k = ct.c_double(), ct.c_double(), ct.c_longlong()
+        self._check(self._lib.ipg_batch_stats(self._h, ct.byref(ev), ct.byref(tot), ct.byref(k)))
+        return ev.value, tot.value, k.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.ipg_batch_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -6,6 +6,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdlib>
+#include <map>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -63,6 +66,7 @@ struct ipg_ctx {
     double *carry = nullptr;
     int *wrote = nullptr, *found = nullptr;
     double *partial = nullptr, *scal = nullptr;
+    double *h_scal = nullptr;  // pinned host copy of scal
     EventGeom *d_ev = nullptr;
 
     bool initialized = false, half_done = false, finished = false;
@@ -272,6 +276,115 @@ ipg_status state64(ipg_ctx *c) {
     return IPG_OK;
 }
 
+// The leapfrog schedule of Evolution::run up to it = itmax - 1: the tau = 0
+// half step of phi and U (Evolution.cpp:393-394), then full steps
+// it = 1 .. itmax-1 (416-421).
+ipg_status run_evolution(ipg_ctx *c) {
+    const int itmax = c->itmax;
+    const double dtau = c->dtau;
+    IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    IPG_TRY(step(c, 0., dtau, dtau, 0, 1));
+    c->half_done = true;
+    for (int it = 1; it < itmax; it++) {
+        IPG_TRY(step(c, it * dtau, dtau, dtau, 1, 1));
+        c->it = it;
+    }
+    IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    IPG_TRY(sync(c));
+    c->last_leapfrog_ms = elapsed(c);
+    c->last_leapfrog_launches = itmax;
+    return IPG_OK;
+}
+
+// Observables at it = itmax before the last half step (Evolution.cpp:406-410),
+// the last half step of pi and E (426-431), the Gauss law (633-635) and the
+// checks, all enqueued on the context's stream; the scalars are copied to
+// pinned host memory. observables_finish waits and fills the result.
+ipg_status observables_enqueue(ipg_ctx *c) {
+    const int itmax = c->itmax;
+    const double dtau = c->dtau;
+    const size_t n = c->n;
+    const int N = c->N;
+    IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    IPG_TRY(state64(c));
+    TmunuArgs ta;
+    ta.N = N;
+    ta.g = c->cfg.g;
+    ta.tau = itmax * dtau;
+    ta.a = c->a;
+    ta.s = c->s64;
+    ta.T10 = c->T10;
+    launch_tmunu(ta, c->stream);
+    IPG_LAUNCHED(c, 2);
+    LandauArgs la;
+    la.N = N;
+    la.tau_fm = itmax * dtau * c->a;
+    la.tau2_fm = c->a * itmax * dtau * c->a * itmax * dtau;
+    la.tau_fm_parts[0] = itmax;
+    la.tau_fm_parts[1] = dtau;
+    la.tau_fm_parts[2] = c->a;
+    la.T10 = c->T10;
+    la.eps = c->eps;
+    la.u4 = c->u4;
+    la.pi10 = c->pi10;
+    la.found = c->found;
+    launch_landau(la, c->carry, c->wrote, c->stream);
+    IPG_LAUNCHED(c, 2);
+    double *scal = c->scal;
+    launch_eccentricity(N, c->cfg.L, c->a, c->eps, c->u4, c->T10, c->partial,
+                        scal + 0, scal + 8, c->stream);
+    IPG_LAUNCHED(c, 4);
+
+    IPG_TRY(step(c, itmax * dtau, dtau / 2., dtau, 1, 0));
+    c->it = itmax;
+    IPG_TRY(state64(c));
+    launch_gauss_law(N, c->s64, c->partial, scal + 32, c->stream);
+    IPG_LAUNCHED(c, 2);
+    launch_unitarity(N, c->s64.ux, c->s64.uy, c->partial, scal + 33, c->stream);
+    IPG_LAUNCHED(c, 2);
+    launch_cell_flags(n, c->found, c->eps, c->partial, scal + 36, c->stream);
+    IPG_LAUNCHED(c, 2);
+    IPG_CUDA(c, cudaMemcpyAsync(c->h_scal, scal, sizeof(double) * 38,
+                                cudaMemcpyDeviceToHost, c->stream));
+    IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    return IPG_OK;
+}
+
+ipg_status observables_finish(ipg_ctx *c, ipg_result *res) {
+    IPG_TRY(sync(c));
+    const double ms_obs = elapsed(c);
+    c->finished = true;
+    const int itmax = c->itmax;
+    const double dtau = c->dtau;
+    const double *h = c->h_scal;
+    const int nan_count = (int)h[37];
+    if (res) {
+        std::memset(res, 0, sizeof(*res));
+        res->itmax = itmax;
+        res->dtau = dtau;
+        res->tau_final = itmax * dtau * c->a;
+        res->gauss_violation = h[32];
+        res->unitarity_max = h[33];
+        res->sum_Ttautau = h[3];
+        res->sum_eps = h[4];
+        res->E_T = res->tau_final * c->a * c->a * kHbarc * h[3];
+        // radial moments: [0..5] avr1 avrSq avr3 avr4 avr5 avr6,
+        // [6 + 2(n-1)], [7 + 2(n-1)] cos/sin moments for n = 1..6
+        const double *m = h + 8;
+        const double avr[6] = {m[0], m[1], m[2], m[3], m[4], m[5]};
+        for (int k = 0; k < 6; k++) {
+            const double cs = m[6 + 2 * k], sn = m[7 + 2 * k];
+            res->eccentricity[k] = std::sqrt(cs * cs + sn * sn) / avr[k];
+            res->psi[k] = (std::atan(sn / cs) + M_PI) / (k + 1);
+        }
+        res->cells_without_u = (int)h[36];
+        res->ms_evolution = c->last_leapfrog_ms;
+        res->ms_observables = ms_obs;
+    }
+    if (nan_count) return fail(c, IPG_ERR_NAN, "%d cells with non-finite e", nan_count);
+    return IPG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -362,6 +475,7 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
     IPG_TRY(dalloc(c, &c->found, n));
     IPG_TRY(dalloc(c, &c->partial, 8192));  // 296 reduction blocks x <= 18 slots
     IPG_TRY(dalloc(c, &c->scal, 64));
+    IPG_CUDA(c, cudaMallocHost(&c->h_scal, 64 * sizeof(double)));
     IPG_TRY(dalloc(c, &c->d_ev, 1));
 
     // twiddles exp(-2 pi i k/N), evaluated on the host in double precision
@@ -389,6 +503,7 @@ ipg_status ipg_destroy(ipg_ctx *ctx) {
         cudaStreamSynchronize(ctx->stream);
     }
     for (void *p : ctx->allocs) cudaFree(p);
+    if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -607,98 +722,9 @@ ipg_status ipg_run(ipg_ctx *c, ipg_result *res) {
     if (!c) return IPG_ERR_BAD_CONFIG;
     if (!c->initialized || c->half_done || c->finished)
         return fail(c, IPG_ERR_STATE, "ipg_run needs fresh initial fields");
-    const int itmax = c->itmax;
-    const double dtau = c->dtau;
-    const size_t n = c->n;
-    const int N = c->N;
-
-    IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-    IPG_TRY(step(c, 0., dtau, dtau, 0, 1));  // Evolution.cpp:393-394
-    c->half_done = true;
-    for (int it = 1; it < itmax; it++) {
-        IPG_TRY(step(c, it * dtau, dtau, dtau, 1, 1));  // 416-421
-        c->it = it;
-    }
-    IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
-    IPG_TRY(sync(c));
-    c->last_leapfrog_ms = elapsed(c);
-    c->last_leapfrog_launches = itmax;
-    const double ms_evo = c->last_leapfrog_ms;
-
-    // observables at it = itmax before the last half step (406-410)
-    IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-    IPG_TRY(state64(c));
-    TmunuArgs ta;
-    ta.N = N;
-    ta.g = c->cfg.g;
-    ta.tau = itmax * dtau;
-    ta.a = c->a;
-    ta.s = c->s64;
-    ta.T10 = c->T10;
-    launch_tmunu(ta, c->stream);
-    IPG_LAUNCHED(c, 2);
-    LandauArgs la;
-    la.N = N;
-    la.tau_fm = itmax * dtau * c->a;
-    la.tau2_fm = c->a * itmax * dtau * c->a * itmax * dtau;
-    la.tau_fm_parts[0] = itmax;
-    la.tau_fm_parts[1] = dtau;
-    la.tau_fm_parts[2] = c->a;
-    la.T10 = c->T10;
-    la.eps = c->eps;
-    la.u4 = c->u4;
-    la.pi10 = c->pi10;
-    la.found = c->found;
-    launch_landau(la, c->carry, c->wrote, c->stream);
-    IPG_LAUNCHED(c, 2);
-    double *scal = c->scal;
-    launch_eccentricity(N, c->cfg.L, c->a, c->eps, c->u4, c->T10, c->partial,
-                        scal + 0, scal + 8, c->stream);
-    IPG_LAUNCHED(c, 4);
-
-    // last half step of pi and E (426-431), then the Gauss law (633-635)
-    IPG_TRY(step(c, itmax * dtau, dtau / 2., dtau, 1, 0));
-    c->it = itmax;
-    IPG_TRY(state64(c));
-    launch_gauss_law(N, c->s64, c->partial, scal + 32, c->stream);
-    IPG_LAUNCHED(c, 2);
-    launch_unitarity(N, c->s64.ux, c->s64.uy, c->partial, scal + 33, c->stream);
-    IPG_LAUNCHED(c, 2);
-    launch_cell_flags(n, c->found, c->eps, c->partial, scal + 36, c->stream);
-    IPG_LAUNCHED(c, 2);
-    IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
-    IPG_TRY(sync(c));
-    const double ms_obs = elapsed(c);
-    c->finished = true;
-
-    double h[40];
-    IPG_CUDA(c, cudaMemcpy(h, scal, sizeof(double) * 38, cudaMemcpyDeviceToHost));
-    const int nan_count = (int)h[37];
-    if (res) {
-        std::memset(res, 0, sizeof(*res));
-        res->itmax = itmax;
-        res->dtau = dtau;
-        res->tau_final = itmax * dtau * c->a;
-        res->gauss_violation = h[32];
-        res->unitarity_max = h[33];
-        res->sum_Ttautau = h[3];
-        res->sum_eps = h[4];
-        res->E_T = res->tau_final * c->a * c->a * kHbarc * h[3];
-        // radial moments: [0..5] avr1 avrSq avr3 avr4 avr5 avr6,
-        // [6 + 2(n-1)], [7 + 2(n-1)] cos/sin moments for n = 1..6
-        const double *m = h + 8;
-        const double avr[6] = {m[0], m[1], m[2], m[3], m[4], m[5]};
-        for (int k = 0; k < 6; k++) {
-            const double cs = m[6 + 2 * k], sn = m[7 + 2 * k];
-            res->eccentricity[k] = std::sqrt(cs * cs + sn * sn) / avr[k];
-            res->psi[k] = (std::atan(sn / cs) + M_PI) / (k + 1);
-        }
-        res->cells_without_u = (int)h[36];
-        res->ms_evolution = ms_evo;
-        res->ms_observables = ms_obs;
-    }
-    if (nan_count) return fail(c, IPG_ERR_NAN, "%d cells with non-finite e", nan_count);
-    return IPG_OK;
+    IPG_TRY(run_evolution(c));
+    IPG_TRY(observables_enqueue(c));
+    return observables_finish(c, res);
 }
 
 ipg_status ipg_get_observables(ipg_ctx *c, double *eps, double *u4,
@@ -806,6 +832,483 @@ ipg_status ipg_last_leapfrog_ms(ipg_ctx *c, double *ms, int *launches) {
 ipg_status ipg_kernel_launches(const ipg_ctx *c, long long *count) {
     if (!c || !count) return IPG_ERR_BAD_CONFIG;
     *count = c->launches;
+    return IPG_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batches: many events (contexts, possibly of different N) advanced together,
+// one persistent launch per leapfrog step over all their sites, the step
+// sequence captured once as a CUDA graph and replayed on every run. Per-step
+// pointers and coefficients live in a device table that is refreshed before
+// each replay, so the graph stays valid while the events' U/phi buffers swap
+// roles from run to run.
+// ===========================================================================
+
+struct ipg_batch {
+    std::vector<ipg_ctx *> ev;
+    int device = 0;
+    bool fp32 = false;
+    int itmax = 0;
+    double dtau = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::string err;
+    int variant = 1, blocks_per_sm = 0, grid = 0;
+    int tiles_variant = -1, total_tiles = 0;
+    int *d_tile_begin = nullptr;
+    void *d_table = nullptr, *h_table = nullptr;
+    size_t event_bytes = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_variant = -1, graph_grid = -1;
+    double last_ms_evolution = 0, last_ms_total = 0;
+    long long launches = 0;
+    bool tuned = false;
+};
+
+namespace {
+
+ipg_status bfail(ipg_batch *b, ipg_status st, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (b) b->err = buf;
+    return st;
+}
+
+#define IPG_BCUDA(b, expr)                                                        \
+    do {                                                                          \
+        cudaError_t _e = (expr);                                                  \
+        if (_e != cudaSuccess)                                                    \
+            return bfail((b), IPG_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(_e)); \
+    } while (0)
+
+template <typename T>
+struct Bufs {
+    State<T> *s;
+    C<T> **uxb, **uyb;
+    T **phib;
+};
+template <typename T>
+Bufs<T> bufs(ipg_ctx *c);
+template <>
+Bufs<float> bufs<float>(ipg_ctx *c) {
+    return {&c->s32, &c->ux32b, &c->uy32b, &c->phi32b};
+}
+template <>
+Bufs<double> bufs<double>(ipg_ctx *c) {
+    return {&c->s64, &c->ux64b, &c->uy64b, &c->phi64b};
+}
+
+int tile_rows(const ipg_batch *b, int variant) {
+    return b->fp32 ? batch_tile_rows<float>(variant) : batch_tile_rows<double>(variant);
+}
+
+int max_blocks(const ipg_batch *b, int variant) {
+    const int E = (int)b->ev.size();
+    return b->fp32 ? batch_max_blocks_per_sm<float>(variant, E)
+                   : batch_max_blocks_per_sm<double>(variant, E);
+}
+
+// variants the precision supports (FP64 needs <= 256 threads per block)
+int n_variants(const ipg_batch *b) { return b->fp32 ? kBatchVariants : 2; }
+
+ipg_status upload_tiles(ipg_batch *b, int variant) {
+    if (b->tiles_variant == variant) return IPG_OK;
+    const int E = (int)b->ev.size();
+    std::vector<int> begin(E + 1, 0);
+    const int rows = tile_rows(b, variant);
+    for (int e = 0; e < E; e++) {
+        const int N = b->ev[e]->N;
+        begin[e + 1] = begin[e] + (N / 32) * (N / rows);
+    }
+    IPG_BCUDA(b, cudaMemcpyAsync(b->d_tile_begin, begin.data(), sizeof(int) * (E + 1),
+                                 cudaMemcpyHostToDevice, b->stream));
+    IPG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    b->total_tiles = begin[E];
+    b->tiles_variant = variant;
+    return IPG_OK;
+}
+
+// descriptors of steps [0, steps) for every event, following the schedule of
+// run_evolution: step 0 is the tau = 0 half step of phi and U, step k > 0 the
+// full step it = k. U/phi buffers alternate after every step. With
+// full_first, step 0 is laid out on the current buffers but carries the
+// coefficients of the full step it = 1 (the step the tuner times: it reads
+// the current U/phi and writes only the other buffers, E and pi).
+template <typename T>
+void fill_table(ipg_batch *b, BatchEvent<T> *tab, int steps, bool full_first = false) {
+    const int E = (int)b->ev.size();
+    for (int e = 0; e < E; e++) {
+        ipg_ctx *c = b->ev[e];
+        Bufs<T> B = bufs<T>(c);
+        State<T> s = *B.s;
+        C<T> *uxb = *B.uxb, *uyb = *B.uyb;
+        T *phib = *B.phib;
+        for (int k = 0; k < steps; k++) {
+            BatchEvent<T> &d = tab[(size_t)k * E + e];
+            d.s = s;
+            d.ux_out = uxb;
+            d.uy_out = uyb;
+            d.phi_out = phib;
+            const int it = (full_first && k == 0) ? 1 : k;
+            d.cf.tau = (T)(it * c->dtau);
+            d.cf.dt_pe = (T)c->dtau;
+            d.cf.dt_pu = (T)c->dtau;
+            d.cf.g = (T)c->cfg.g;
+            d.cf.do_pe = it > 0;
+            d.cf.do_pu = 1;
+            d.N = c->N;
+            d.active = 1;
+            std::swap(s.ux, uxb);
+            std::swap(s.uy, uyb);
+            std::swap(s.phi, phib);
+        }
+    }
+}
+
+// the events' buffers after `swaps` U/phi exchanges
+template <typename T>
+void apply_swaps(ipg_batch *b, int swaps) {
+    if ((swaps & 1) == 0) return;
+    for (ipg_ctx *c : b->ev) {
+        Bufs<T> B = bufs<T>(c);
+        std::swap(B.s->ux, *B.uxb);
+        std::swap(B.s->uy, *B.uyb);
+        std::swap(B.s->phi, *B.phib);
+    }
+}
+
+ipg_status launch_batch(ipg_batch *b, int step) {
+    const int E = (int)b->ev.size();
+    if (b->fp32) {
+        auto *t = static_cast<BatchEvent<float> *>(b->d_table) + (size_t)step * E;
+        launch_leapfrog_batch<float>(t, E, b->d_tile_begin, b->total_tiles, b->variant, b->grid,
+                                     b->stream);
+    } else {
+        auto *t = static_cast<BatchEvent<double> *>(b->d_table) + (size_t)step * E;
+        launch_leapfrog_batch<double>(t, E, b->d_tile_begin, b->total_tiles, b->variant, b->grid,
+                                      b->stream);
+    }
+    b->launches++;
+    return IPG_OK;
+}
+
+ipg_status capture_graph(ipg_batch *b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    IPG_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < b->itmax; k++) launch_batch(b, k);
+    b->launches -= b->itmax;  // counted when the graph is launched
+    cudaError_t e = cudaStreamEndCapture(b->stream, &b->graph);
+    if (e != cudaSuccess) return bfail(b, IPG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    IPG_BCUDA(b, cudaGraphInstantiate(&b->exec, b->graph, 0));
+    b->graph_variant = b->variant;
+    b->graph_grid = b->grid;
+    return IPG_OK;
+}
+
+// tuning cache: key -> (variant, blocks per SM); optionally persisted in the
+// file named by IPG_TUNE_CACHE (one "key variant blocks" line per entry)
+std::map<std::string, std::pair<int, int>> &tune_cache() {
+    static std::map<std::string, std::pair<int, int>> m;
+    static bool loaded = false;
+    if (!loaded) {
+        loaded = true;
+        if (const char *path = std::getenv("IPG_TUNE_CACHE")) {
+            if (FILE *f = std::fopen(path, "r")) {
+                char key[512];
+                int v, bps;
+                while (std::fscanf(f, "%511s %d %d", key, &v, &bps) == 3) m[key] = {v, bps};
+                std::fclose(f);
+            }
+        }
+    }
+    return m;
+}
+
+std::string tune_key(const ipg_batch *b) {
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, b->device);
+    std::map<int, int> sizes;
+    for (const ipg_ctx *c : b->ev) sizes[c->N]++;
+    std::string k = std::string(prop.name) + "|sm" + std::to_string(b->sms) +
+                    (b->fp32 ? "|fp32" : "|fp64");
+    for (auto &p : sizes) k += "|" + std::to_string(p.first) + "x" + std::to_string(p.second);
+    for (char &ch : k)
+        if (ch == ' ') ch = '_';
+    return k;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *ipg_batch_last_error(const ipg_batch *b) {
+    return b ? b->err.c_str() : "null batch";
+}
+
+ipg_status ipg_batch_create(ipg_ctx *const *events, int count, ipg_batch **out) {
+    if (!out) return IPG_ERR_BAD_CONFIG;
+    *out = nullptr;
+    if (!events || count < 1) return IPG_ERR_BAD_CONFIG;
+    ipg_batch *b = new (std::nothrow) ipg_batch();
+    if (!b) return IPG_ERR_NOMEM;
+    *out = b;
+    for (int e = 0; e < count; e++) {
+        if (!events[e]) return bfail(b, IPG_ERR_BAD_CONFIG, "event %d is null", e);
+        b->ev.push_back(events[e]);
+    }
+    const ipg_ctx *c0 = events[0];
+    b->device = c0->cfg.device;
+    b->fp32 = is_fp32(c0);
+    b->itmax = c0->itmax;
+    b->dtau = c0->dtau;
+    for (int e = 0; e < count; e++) {
+        const ipg_ctx *c = events[e];
+        if (c->cfg.device != b->device)
+            return bfail(b, IPG_ERR_BAD_CONFIG, "event %d is on another device", e);
+        if (is_fp32(c) != b->fp32)
+            return bfail(b, IPG_ERR_BAD_CONFIG, "event %d has another precision", e);
+        if (c->itmax != b->itmax || c->dtau != b->dtau)
+            return bfail(b, IPG_ERR_BAD_CONFIG,
+                         "event %d has another time grid (itmax %d vs %d)", e, c->itmax,
+                         b->itmax);
+        if (c->N < 32)
+            return bfail(b, IPG_ERR_BAD_CONFIG, "event %d: batched lattices need N >= 32", e);
+    }
+    IPG_BCUDA(b, cudaSetDevice(b->device));
+    IPG_BCUDA(b, cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device));
+    IPG_BCUDA(b, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    IPG_BCUDA(b, cudaEventCreate(&b->e0));
+    IPG_BCUDA(b, cudaEventCreate(&b->e1));
+    b->event_bytes = b->fp32 ? sizeof(BatchEvent<float>) : sizeof(BatchEvent<double>);
+    const size_t table = b->event_bytes * count * (size_t)b->itmax;
+    IPG_BCUDA(b, cudaMalloc(&b->d_table, table));
+    IPG_BCUDA(b, cudaMallocHost(&b->h_table, table));
+    IPG_BCUDA(b, cudaMalloc(&b->d_tile_begin, sizeof(int) * (count + 1)));
+    const auto it = tune_cache().find(tune_key(b));
+    if (it != tune_cache().end()) {
+        b->variant = it->second.first;
+        b->blocks_per_sm = it->second.second;
+        b->tuned = true;
+    } else {
+        b->variant = 1;
+        b->blocks_per_sm = max_blocks(b, b->variant);
+    }
+    if (b->blocks_per_sm < 1) return bfail(b, IPG_ERR_CUDA, "batched kernel cannot be resident");
+    b->grid = b->blocks_per_sm * b->sms;
+    return IPG_OK;
+}
+
+ipg_status ipg_batch_destroy(ipg_batch *b) {
+    if (!b) return IPG_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->d_table) cudaFree(b->d_table);
+    if (b->h_table) cudaFreeHost(b->h_table);
+    if (b->d_tile_begin) cudaFree(b->d_tile_begin);
+    if (b->e0) cudaEventDestroy(b->e0);
+    if (b->e1) cudaEventDestroy(b->e1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return IPG_OK;
+}
+
+ipg_status ipg_batch_tune(ipg_batch *b, ipg_tune_report *rep) {
+    if (!b) return IPG_ERR_BAD_CONFIG;
+    IPG_BCUDA(b, cudaSetDevice(b->device));
+    const std::string key = tune_key(b);
+    auto fill_report = [&](double ms, int candidates, int from_cache) {
+        if (!rep) return;
+        rep->variant = b->variant;
+        rep->tile_rows = tile_rows(b, b->variant);
+        rep->threads_per_block = 64 * rep->tile_rows;
+        rep->blocks_per_sm = b->blocks_per_sm;
+        rep->grid = b->grid;
+        rep->ms_per_step = ms;
+        rep->candidates = candidates;
+        rep->from_cache = from_cache;
+    };
+    auto hit = tune_cache().find(key);
+    if (hit != tune_cache().end()) {
+        b->variant = hit->second.first;
+        b->blocks_per_sm = hit->second.second;
+        b->grid = b->blocks_per_sm * b->sms;
+        b->tuned = true;
+        fill_report(0., 0, 1);
+        return IPG_OK;
+    }
+    for (ipg_ctx *c : b->ev)
+        if (!c->initialized || c->half_done || c->finished)
+            return bfail(b, IPG_ERR_STATE, "tune needs every event freshly initialised");
+    // E and pi are updated in place by a step: keep a copy and put it back
+    std::vector<void *> saved;
+    const size_t w = b->fp32 ? sizeof(float) : sizeof(double);
+    for (ipg_ctx *c : b->ev) {
+        void *p = nullptr;
+        if (cudaMalloc(&p, 25 * c->n * w) != cudaSuccess) {
+            cudaGetLastError();
+            for (void *q : saved) cudaFree(q);
+            return bfail(b, IPG_ERR_NOMEM, "tuning scratch allocation failed");
+        }
+        saved.push_back(p);
+        char *dst = static_cast<char *>(p);
+        const void *e1 = b->fp32 ? (const void *)c->s32.e1 : (const void *)c->s64.e1;
+        const void *e2 = b->fp32 ? (const void *)c->s32.e2 : (const void *)c->s64.e2;
+        const void *pi = b->fp32 ? (const void *)c->s32.pi : (const void *)c->s64.pi;
+        cudaMemcpyAsync(dst, e1, 8 * c->n * w, cudaMemcpyDeviceToDevice, b->stream);
+        cudaMemcpyAsync(dst + 8 * c->n * w, e2, 8 * c->n * w, cudaMemcpyDeviceToDevice, b->stream);
+        cudaMemcpyAsync(dst + 16 * c->n * w, pi, 9 * c->n * w, cudaMemcpyDeviceToDevice, b->stream);
+    }
+    // one representative full step (it = 1) for every event, in table slot 0
+    const int E = (int)b->ev.size();
+    if (b->fp32)
+        fill_table<float>(b, static_cast<BatchEvent<float> *>(b->h_table), 1, true);
+    else
+        fill_table<double>(b, static_cast<BatchEvent<double> *>(b->h_table), 1, true);
+    const int slot = 0;
+    IPG_BCUDA(b, cudaMemcpyAsync(b->d_table, b->h_table, b->event_bytes * E,
+                                 cudaMemcpyHostToDevice, b->stream));
+    double best = 1e30;
+    int best_v = b->variant, best_bps = b->blocks_per_sm, candidates = 0;
+    for (int v = 0; v < n_variants(b); v++) {
+        const int maxb = max_blocks(b, v);
+        for (int bps = 1; bps <= maxb; bps++) {
+            b->variant = v;
+            b->blocks_per_sm = bps;
+            b->grid = bps * b->sms;
+            IPG_TRY(upload_tiles(b, v));
+            launch_batch(b, slot);  // warm-up
+            IPG_BCUDA(b, cudaEventRecord(b->e0, b->stream));
+            const int reps = 3;
+            for (int r = 0; r < reps; r++) launch_batch(b, slot);
+            IPG_BCUDA(b, cudaEventRecord(b->e1, b->stream));
+            IPG_BCUDA(b, cudaEventSynchronize(b->e1));
+            IPG_BCUDA(b, cudaGetLastError());
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, b->e0, b->e1);
+            candidates++;
+            if (ms / reps < best) {
+                best = ms / reps;
+                best_v = v;
+                best_bps = bps;
+            }
+        }
+    }
+    for (int e = 0; e < E; e++) {
+        ipg_ctx *c = b->ev[e];
+        const char *src = static_cast<const char *>(saved[e]);
+        void *e1 = b->fp32 ? (void *)c->s32.e1 : (void *)c->s64.e1;
+        void *e2 = b->fp32 ? (void *)c->s32.e2 : (void *)c->s64.e2;
+        void *pi = b->fp32 ? (void *)c->s32.pi : (void *)c->s64.pi;
+        cudaMemcpyAsync(e1, src, 8 * c->n * w, cudaMemcpyDeviceToDevice, b->stream);
+        cudaMemcpyAsync(e2, src + 8 * c->n * w, 8 * c->n * w, cudaMemcpyDeviceToDevice, b->stream);
+        cudaMemcpyAsync(pi, src + 16 * c->n * w, 9 * c->n * w, cudaMemcpyDeviceToDevice,
+                        b->stream);
+    }
+    IPG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    for (void *q : saved) cudaFree(q);
+    b->variant = best_v;
+    b->blocks_per_sm = best_bps;
+    b->grid = best_bps * b->sms;
+    b->tuned = true;
+    tune_cache()[key] = {best_v, best_bps};
+    if (const char *path = std::getenv("IPG_TUNE_CACHE")) {
+        if (FILE *f = std::fopen(path, "a")) {
+            std::fprintf(f, "%s %d %d\n", key.c_str(), best_v, best_bps);
+            std::fclose(f);
+        }
+    }
+    fill_report(best, candidates, 0);
+    return IPG_OK;
+}
+
+ipg_status ipg_batch_run(ipg_batch *b, ipg_result *results) {
+    if (!b) return IPG_ERR_BAD_CONFIG;
+    IPG_BCUDA(b, cudaSetDevice(b->device));
+    const int E = (int)b->ev.size();
+    for (int e = 0; e < E; e++) {
+        const ipg_ctx *c = b->ev[e];
+        if (!c->initialized || c->half_done || c->finished)
+            return bfail(b, IPG_ERR_STATE, "event %d needs fresh initial fields", e);
+    }
+    IPG_TRY(upload_tiles(b, b->variant));
+    if (b->fp32)
+        fill_table<float>(b, static_cast<BatchEvent<float> *>(b->h_table), b->itmax);
+    else
+        fill_table<double>(b, static_cast<BatchEvent<double> *>(b->h_table), b->itmax);
+    IPG_BCUDA(b, cudaMemcpyAsync(b->d_table, b->h_table, b->event_bytes * E * b->itmax,
+                                 cudaMemcpyHostToDevice, b->stream));
+    if (!b->exec || b->graph_variant != b->variant || b->graph_grid != b->grid)
+        IPG_TRY(capture_graph(b));
+    IPG_BCUDA(b, cudaEventRecord(b->e0, b->stream));
+    IPG_BCUDA(b, cudaGraphLaunch(b->exec, b->stream));
+    b->launches += b->itmax;
+    IPG_BCUDA(b, cudaEventRecord(b->e1, b->stream));
+    IPG_BCUDA(b, cudaEventSynchronize(b->e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, b->e0, b->e1);
+    b->last_ms_evolution = ms;
+    if (b->fp32)
+        apply_swaps<float>(b, b->itmax);
+    else
+        apply_swaps<double>(b, b->itmax);
+    for (ipg_ctx *c : b->ev) {
+        c->half_done = true;
+        c->it = b->itmax - 1;
+        c->last_leapfrog_ms = ms;
+        c->last_leapfrog_launches = b->itmax;
+    }
+    // observables of all events, each on its own stream
+    const auto t0 = std::chrono::steady_clock::now();
+    ipg_status worst = IPG_OK;
+    for (int e = 0; e < E; e++) {
+        ipg_status st = observables_enqueue(b->ev[e]);
+        if (st != IPG_OK) return bfail(b, st, "event %d: %s", e, b->ev[e]->err.c_str());
+    }
+    for (int e = 0; e < E; e++) {
+        ipg_status st = observables_finish(b->ev[e], results ? results + e : nullptr);
+        if (st == IPG_ERR_NAN) {
+            worst = st;
+            b->err = "event " + std::to_string(e) + ": " + b->ev[e]->err;
+        } else if (st != IPG_OK) {
+            return bfail(b, st, "event %d: %s", e, b->ev[e]->err.c_str());
+        }
+    }
+    const auto t1 = std::chrono::steady_clock::now();
+    b->last_ms_total = ms + std::chrono::duration<double, std::milli>(t1 - t0).count();
+    return worst;
+}
+
+ipg_status ipg_batch_set_shape(ipg_batch *b, int variant, int blocks_per_sm) {
+    if (!b) return IPG_ERR_BAD_CONFIG;
+    if (variant < 0 || variant >= n_variants(b))
+        return bfail(b, IPG_ERR_BAD_CONFIG, "variant %d not available", variant);
+    const int maxb = max_blocks(b, variant);
+    if (blocks_per_sm < 1 || blocks_per_sm > maxb)
+        return bfail(b, IPG_ERR_BAD_CONFIG, "blocks_per_sm must be in [1, %d]", maxb);
+    b->variant = variant;
+    b->blocks_per_sm = blocks_per_sm;
+    b->grid = blocks_per_sm * b->sms;
+    return IPG_OK;
+}
+
+ipg_status ipg_batch_stats(const ipg_batch *b, double *ms_evolution, double *ms_total,
+                           long long *launches) {
+    if (!b) return IPG_ERR_BAD_CONFIG;
+    if (ms_evolution) *ms_evolution = b->last_ms_evolution;
+    if (ms_total) *ms_total = b->last_ms_total;
+    if (launches) *launches = b->launches;
     return IPG_OK;
 }
 

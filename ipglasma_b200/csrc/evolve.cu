@@ -536,22 +536,14 @@ __device__ __forceinline__ H3<T> shfl_xor_h(const H3<T> &h, int m) {
     return r;
 }
 
-// block: 256 threads = 128 sites (32 along y, the fast index, x 4 along x)
-// x 2 directions; lanes 2k and 2k+1 share a site
+// One direction d of one site (ix, iy) of an N x N lattice (N >= 32). Lanes
+// 2k and 2k+1 of a full warp hold the two directions of one site: the pi
+// bracket is summed across them with a shuffle.
 template <typename T, bool DEV>
-// FP32: 128 registers, two blocks (16 warps) per SM; FP64: one block per SM
-// (the FP64 state needs ~250 registers per thread without spilling)
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
-    k_leapfrog_split(const EventGeom *__restrict__ ev, State<T> s, C<T> *ux_out,
-                     C<T> *uy_out, T *phi_out, StepCoef<T> cf) {
-    const int N = ev->N;
-    const int d = threadIdx.x & 1;
-    const int iy = blockIdx.x * 32 + ((threadIdx.x >> 1) & 31);
-    const int ix = blockIdx.y * 4 + (threadIdx.x >> 6);
-    // whole warps stay together for the shuffle: a warp is 16 sites of one
-    // row, and N is a multiple of 8, so either all lanes or none are past N
-    const bool live = (ix < N) && (iy < N);
-    if (!live) return;
+__device__ __forceinline__ void leapfrog_site_dir(int N, int ix, int iy, int d,
+                                                  const State<T> &s, C<T> *ux_out,
+                                                  C<T> *uy_out, T *phi_out,
+                                                  const StepCoef<T> &cf) {
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)ix * N + iy;
     const C<T> *Ud_p = d ? s.uy : s.ux;
@@ -614,6 +606,129 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
         }
     }
 }
+
+// block: 256 threads = 128 sites (32 along y, the fast index, x 4 along x)
+// x 2 directions; lanes 2k and 2k+1 share a site
+template <typename T, bool DEV>
+// FP32: 128 registers, two blocks (16 warps) per SM; FP64: one block per SM
+// (the FP64 state needs ~250 registers per thread without spilling)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
+    k_leapfrog_split(const EventGeom *__restrict__ ev, State<T> s, C<T> *ux_out,
+                     C<T> *uy_out, T *phi_out, StepCoef<T> cf) {
+    const int N = ev->N;
+    const int d = threadIdx.x & 1;
+    const int iy = blockIdx.x * 32 + ((threadIdx.x >> 1) & 31);
+    const int ix = blockIdx.y * 4 + (threadIdx.x >> 6);
+    // the grid covers the lattice exactly (N a multiple of 32)
+    leapfrog_site_dir<T, DEV>(N, ix, iy, d, s, ux_out, uy_out, phi_out, cf);
+}
+
+// ---------------------------------------------------------------------------
+// Batched events: one persistent launch advances every site of every event in
+// a batch (lattices of different N, each a multiple of 32) by one step. The
+// tile list of the batch is the concatenation of the events' tiles (32 sites
+// along y x TX rows along x); event e owns tiles [tile_begin[e],
+// tile_begin[e+1]). Each block takes tiles blockIdx.x, blockIdx.x + gridDim.x,
+// ... and finds the owning event by binary search over tile_begin held in
+// shared memory. Per-event pointers and coefficients of this step come from a
+// descriptor table in device memory, so a captured sequence of launches stays
+// valid when the events' buffers swap roles between runs.
+// ---------------------------------------------------------------------------
+template <int TX, typename T, bool DEV>
+// FP32: 128 registers at every tile shape (512 threads per SM); FP64: up to
+// 255 registers (256 threads per SM), so FP64 uses TX = 2 or 4 only
+__global__ void __launch_bounds__(64 * TX, sizeof(T) == 4 ? 8 / TX : (TX <= 4 ? 4 / TX : 1))
+    k_leapfrog_batch(const BatchEvent<T> *__restrict__ evs, int n_events,
+                     const int *__restrict__ tile_begin, int total_tiles) {
+    // the step's descriptors, then tile_begin[n_events + 1], in shared memory
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    BatchEvent<T> *s_ev = reinterpret_cast<BatchEvent<T> *>(s_raw);
+    int *s_begin = reinterpret_cast<int *>(s_ev + n_events);
+    {
+        const int words = n_events * (int)(sizeof(BatchEvent<T>) / sizeof(int));
+        const int *src = reinterpret_cast<const int *>(evs);
+        int *dst = reinterpret_cast<int *>(s_ev);
+        for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
+    }
+    for (int e = threadIdx.x; e <= n_events; e += blockDim.x) s_begin[e] = tile_begin[e];
+    __syncthreads();
+    const int d = threadIdx.x & 1;
+    const int ly = (threadIdx.x >> 1) & 31, lx = threadIdx.x >> 6;
+    for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+        int lo = 0, hi = n_events - 1;  // last e with s_begin[e] <= t
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s_begin[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const BatchEvent<T> &E = s_ev[lo];
+        if (!E.active) continue;
+        const int local = t - s_begin[lo];
+        const int tiles_y = E.N >> 5;
+        const int ty = local % tiles_y, tx = local / tiles_y;
+        leapfrog_site_dir<T, DEV>(E.N, tx * TX + lx, ty * 32 + ly, d, E.s, E.ux_out,
+                                  E.uy_out, E.phi_out, E.cf);
+    }
+}
+
+template <typename T>
+size_t batch_smem(int n_events) {
+    return sizeof(BatchEvent<T>) * n_events + sizeof(int) * (n_events + 1);
+}
+
+template <typename T>
+int batch_tile_rows(int variant) {
+    return variant == 0 ? 2 : (variant == 1 ? 4 : 8);
+}
+
+template <typename T>
+const void *batch_kernel(int variant) {
+    constexpr bool DEV = sizeof(T) == 4;
+    switch (variant) {
+        case 0: return (const void *)k_leapfrog_batch<2, T, DEV>;
+        case 1: return (const void *)k_leapfrog_batch<4, T, DEV>;
+        default: return (const void *)k_leapfrog_batch<8, T, DEV>;
+    }
+}
+
+template <typename T>
+int batch_max_blocks_per_sm(int variant, int n_events) {
+    int nb = 0;
+    const int threads = 64 * batch_tile_rows<T>(variant);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<T>(variant), threads,
+                                                  batch_smem<T>(n_events));
+    return nb;
+}
+
+template <typename T>
+void launch_leapfrog_batch(const BatchEvent<T> *d_evs, int n_events, const int *d_tile_begin,
+                           int total_tiles, int variant, int grid, cudaStream_t st) {
+    constexpr bool DEV = sizeof(T) == 4;
+    const size_t smem = batch_smem<T>(n_events);
+    switch (variant) {
+        case 0:
+            k_leapfrog_batch<2, T, DEV><<<grid, 128, smem, st>>>(d_evs, n_events, d_tile_begin,
+                                                                 total_tiles);
+            break;
+        case 1:
+            k_leapfrog_batch<4, T, DEV><<<grid, 256, smem, st>>>(d_evs, n_events, d_tile_begin,
+                                                                 total_tiles);
+            break;
+        default:
+            k_leapfrog_batch<8, T, DEV><<<grid, 512, smem, st>>>(d_evs, n_events, d_tile_begin,
+                                                                 total_tiles);
+            break;
+    }
+}
+
+template int batch_tile_rows<float>(int);
+template int batch_tile_rows<double>(int);
+template int batch_max_blocks_per_sm<float>(int, int);
+template int batch_max_blocks_per_sm<double>(int, int);
+template void launch_leapfrog_batch<float>(const BatchEvent<float> *, int, const int *, int,
+                                           int, int, cudaStream_t);
+template void launch_leapfrog_batch<double>(const BatchEvent<double> *, int, const int *, int,
+                                            int, int, cudaStream_t);
 
 template <typename T>
 void launch_leapfrog_site(const EventGeom *d_ev, int N, const State<T> &s,

@@ -34,6 +34,30 @@ void launch_leapfrog(const EventGeom *d_ev, int N, const State<T> &s,
                      C<T> *ux_out, C<T> *uy_out, T *phi_out,
                      const StepCoef<T> &cf, bool reunit, cudaStream_t st);
 
+// One event of a batched leapfrog launch: its buffers for this step and its
+// step coefficients (inactive events are skipped).
+template <typename T>
+struct BatchEvent {
+    State<T> s;
+    C<T> *ux_out, *uy_out;
+    T *phi_out;
+    StepCoef<T> cf;
+    int N;
+    int active;
+};
+
+// Tile-shape variants of the batched kernel: variant v advances tiles of
+// 32 x batch_tile_rows(v) sites with 64 * rows threads.
+constexpr int kBatchVariants = 3;
+template <typename T>
+int batch_tile_rows(int variant);
+template <typename T>
+int batch_max_blocks_per_sm(int variant, int n_events);
+// tile_begin[n_events + 1]: prefix sums of (N/32) (N/rows) per event
+template <typename T>
+void launch_leapfrog_batch(const BatchEvent<T> *d_evs, int n_events, const int *d_tile_begin,
+                           int total_tiles, int variant, int grid, cudaStream_t st);
+
 // ---- initial conditions -------------------------------------------------
 
 // Colour-charge sheets -> Wilson lines for one nucleus, sheets [k0, k0+ns).
