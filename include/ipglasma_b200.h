@@ -70,6 +70,9 @@ typedef struct {
     int newton_max_restarts;   /* 0 -> 200  (Init.cpp:3346) */
     uint64_t seed;     /* key of the device random streams (noise, restarts) */
     int device;        /* CUDA device ordinal */
+    double newton_tolerance; /* stop when sum_a |F_a| < this; <= 0 -> 1e-6, the
+                                reference's criterion (Init.cpp:3372). The
+                                adjoint needs a converged root: use ~1e-12 */
 } ipg_config;
 
 /* Summary of the initial-condition stage. */
@@ -208,6 +211,38 @@ ipg_status ipg_write_tmunu(const char *path, int N, double L, int sizeOutput,
 ipg_status ipg_output_names(int event_id, int it, double dtau, double a,
                             char *hydro, size_t hydro_len, char *tmunu,
                             size_t tmunu_len);
+
+/* ---- adjoint (no counterpart in the reference) ---------------------------
+ * Reverse-mode derivatives of the evolution in FP64, with the autograd
+ * contract: ipg_forward saves what ipg_backward consumes once. The loss is
+ *   L = w_ET * E_T + w_eps2 * eps2
+ * at tau = itmax dtau a, from the state after the itmax leapfrog launches of
+ * Evolution::run (where the reference evaluates T^{mu nu}):
+ *   E_T  = tau a^2 hbarc sum_cells T^tautau (GeV), as ipg_result.E_T;
+ *   eps2 = |sum w (x~ + i y~)^2| / sum w (x~^2 + y~^2) with the smooth weight
+ *          w = T^tautau over cells [2, N-2)^2 and x~, y~ measured from the
+ *          w-weighted centroid (the reference weights with e u^tau from the
+ *          Landau matching, whose branch thresholds are not differentiable).
+ * ipg_forward starts from the context's fresh tau = 0 state (after
+ * ipg_init_fields, or ipg_set_field + ipg_mark_initialized) without changing
+ * it; it stores the state before every checkpoint_every-th step. ipg_backward
+ * walks back by exact time reversal of the step between checkpoints and
+ * returns dL/d(state at tau = 0) for U_x, U_y, E_1, E_2, phi, pi, each [N*N]
+ * sites x 18 doubles (row-major 3x3, (re, im)), in that order (6*18*N*N
+ * doubles; NULL skips the copy). For a complex entry z the pair is
+ * (dL/dRe z, dL/dIm z); for the Hermitian fields it is the Hermitian part
+ * (traceless for E).
+ * When the tau = 0 state came from ipg_init_fields (not ipg_set_field), the
+ * gradient continues through the initial conditions: grad_g2mu receives
+ * dL/d(g2mu2A), dL/d(g2mu2B) ([2][N*N], lattice units) and grad_rho
+ * dL/drho ([2][Ny][N*N][8], the layout of the noise of ipg_set_noise; rho =
+ * g sqrt(g2mu2/Ny) xi); either may be NULL. This chain assumes the Newton
+ * links are converged roots: set cfg.newton_tolerance to ~1e-12 for it (the
+ * reference's 1e-6 leaves errors of that order in the links). Noise given
+ * with ipg_set_noise_device must still be valid. */
+ipg_status ipg_forward(ipg_ctx *ctx, int checkpoint_every, double *E_T, double *eps2);
+ipg_status ipg_backward(ipg_ctx *ctx, double w_ET, double w_eps2, double *grad_state,
+                        double *grad_g2mu, double *grad_rho);
 
 /* ---- batches of events -------------------------------------------------
  * The reference runs one event per process (main.cpp:347-359, events handed

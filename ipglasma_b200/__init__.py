@@ -56,7 +56,7 @@ class _Config(ct.Structure):
         ("UVdamp", ct.c_double), ("maxtime", ct.c_double), ("dtau", ct.c_double),
         ("precision", ct.c_int), ("newton_max_iterations", ct.c_int),
         ("newton_max_restarts", ct.c_int), ("seed", ct.c_uint64),
-        ("device", ct.c_int),
+        ("device", ct.c_int), ("newton_tolerance", ct.c_double),
     ]
 
 
@@ -111,6 +111,10 @@ _SIGNATURES = {
     "ipg_get_newton_iterations": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "ipg_last_leapfrog_ms": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double), ct.POINTER(ct.c_int)]),
     "ipg_kernel_launches": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_longlong)]),
+    "ipg_forward": (ct.c_int, [ct.c_void_p, ct.c_int, ct.POINTER(ct.c_double),
+                               ct.POINTER(ct.c_double)]),
+    "ipg_backward": (ct.c_int, [ct.c_void_p, ct.c_double, ct.c_double, ct.c_void_p, ct.c_void_p,
+                                ct.c_void_p]),
     "ipg_batch_last_error": (ct.c_char_p, [ct.c_void_p]),
     "ipg_batch_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.c_int, ct.POINTER(ct.c_void_p)]),
     "ipg_batch_destroy": (ct.c_int, [ct.c_void_p]),
@@ -166,12 +170,13 @@ class Config:
     seed: int = 1
     device: int = 0
     Nc: int = 3
+    newton_tolerance: float = 0.0
 
     def to_c(self) -> _Config:
         return _Config(self.size, self.Nc, self.Ny, self.L, self.g, self.m,
                        self.UVdamp, self.maxtime, self.dtau, self.precision,
                        self.newton_max_iterations, self.newton_max_restarts,
-                       self.seed, self.device)
+                       self.seed, self.device, self.newton_tolerance)
 
 
 @dataclass
@@ -324,6 +329,35 @@ class Event:
         ms, k = ct.c_double(), ct.c_int()
         self._check(self._lib.ipg_last_leapfrog_ms(self._h, ct.byref(ms), ct.byref(k)))
         return ms.value, k.value
+
+    # -- adjoint -------------------------------------------------------------
+    def forward(self, checkpoint_every: int = 20):
+        """E_T and the T^tautau-weighted eps2 from the fresh tau = 0 state;
+        saves checkpoints for :meth:`backward`."""
+        et, e2 = ct.c_double(), ct.c_double()
+        self._check(self._lib.ipg_forward(self._h, checkpoint_every, ct.byref(et), ct.byref(e2)))
+        return et.value, e2.value
+
+    def backward(self, w_ET: float = 1.0, w_eps2: float = 0.0, inputs: bool = False,
+                 rho: bool = False):
+        """Gradient of w_ET E_T + w_eps2 eps2 w.r.t. the tau = 0 fields:
+        dict field -> (N*N, 3, 3) complex array (dL/dRe + i dL/dIm). With
+        inputs, also "g2mu" -> (2, N*N) (nuclei A, B); with rho, "rho" ->
+        (2, Ny, N*N, 8)."""
+        g = np.empty(6 * 18 * self.n)
+        gm = np.empty(2 * self.n) if inputs else None
+        gr = np.empty(2 * self.cfg.Ny * self.n * 8) if rho else None
+        self._check(self._lib.ipg_backward(
+            self._h, w_ET, w_eps2, _ptr(g), _ptr(gm) if gm is not None else None,
+            _ptr(gr) if gr is not None else None))
+        g = g.reshape(6, self.n, 9, 2)
+        z = g[..., 0] + 1j * g[..., 1]
+        out = {f: z[k].reshape(self.n, 3, 3) for k, f in enumerate((UX, UY, E1, E2, PHI, PI))}
+        if gm is not None:
+            out["g2mu"] = gm.reshape(2, self.n)
+        if gr is not None:
+            out["rho"] = gr.reshape(2, self.cfg.Ny, self.n, 8)
+        return out
 
     def kernel_launches(self) -> int:
         c = ct.c_longlong()

@@ -1,0 +1,732 @@
+// Reverse mode (adjoint) of the FP64 leapfrog evolution and of T^tautau.
+//
+// The reference has no derivative code; these kernels give the gradient of a
+// loss built from T^tautau at the final time (total transverse energy E_T and
+// a T^tautau-weighted eccentricity) with respect to the tau = 0 fields.
+//
+// Conventions. A complex field A has the adjoint A_bar = dL/dRe A + i dL/dIm A,
+// so dL = Re tr(A_bar^dag dA). Products C = A B pass A_bar += C_bar B^dag and
+// B_bar += A^dag C_bar. Hermitian fields (phi, pi) and traceless Hermitian
+// ones (E1, E2) keep full-matrix adjoint buffers; only their Hermitian
+// (traceless) part is meaningful and it is taken where an adjoint is
+// consumed. Adjoint buffers are 9 complex planes per field and site.
+//
+// One leapfrog step (evolve.cu, Evolution.cpp:35-293) is S = S_u o S_e:
+//   S_e: E_d' = TL(E_d + cst (AH-plaquette + AH-staple)_d + cdt i[U_d phi(+d) U_d^dag, phi])
+//        pi'  = pi + cdt sum_d (U_d phi(+d) U_d^dag + U_d(-d)^dag phi(-d) U_d(-d) - 2 phi)
+//   S_u: phi' = phi + c2 pi',   U_d' = T2(i c E_d') U_d,  T2(X) = 1 + X + X^2/2
+// with cst = tau dtau / (2 g^2), cdt = dtau / tau, c = g^2 dtau / (tau + dtau/2),
+// c2 = (tau + dtau/2) dtau. Its vector-Jacobian product is k_adj_su (local)
+// followed by k_adj_se (scatters into neighbouring links and phi with FP64
+// atomics, so the summation order, not the result, varies between runs).
+// The step is inverted exactly in exact arithmetic (k_inv_su, k_inv_se): this
+// is the time reversal used to walk back between checkpoints.
+#include <cstdint>
+
+#include "expm.cuh"
+#include "fields.cuh"
+#include "ipg_internal.h"
+#include "philox.cuh"
+
+namespace ipg {
+
+namespace {
+
+using Md = M3<double>;
+
+__device__ __forceinline__ size_t at(int N, int i, int j) { return (size_t)i * N + j; }
+
+__device__ __forceinline__ Md herm(const Md &a) {
+    Md r;
+#pragma unroll
+    for (int x = 0; x < 3; x++)
+#pragma unroll
+        for (int y = 0; y < 3; y++)
+            r.m[3 * x + y] = {0.5 * (a.m[3 * x + y].r + a.m[3 * y + x].r),
+                              0.5 * (a.m[3 * x + y].i - a.m[3 * y + x].i)};
+    return r;
+}
+
+__device__ __forceinline__ Md tl(const Md &a) {
+    Md r = a;
+    const double t = (a.m[0].r + a.m[4].r + a.m[8].r) / 3.;
+    const double ti = (a.m[0].i + a.m[4].i + a.m[8].i) / 3.;
+    r.m[0].r -= t;
+    r.m[4].r -= t;
+    r.m[8].r -= t;
+    r.m[0].i -= ti;
+    r.m[4].i -= ti;
+    r.m[8].i -= ti;
+    return r;
+}
+
+// s * i * a
+__device__ __forceinline__ Md times_i(const Md &a, double s) {
+    Md r;
+#pragma unroll
+    for (int k = 0; k < 9; k++) r.m[k] = {-s * a.m[k].i, s * a.m[k].r};
+    return r;
+}
+
+__device__ __forceinline__ Md sc(const Md &a, double s) { return scaled(a, s); }
+
+__device__ __forceinline__ Md addm(const Md &a, const Md &b) {
+    Md r = a;
+    add_to(r, b);
+    return r;
+}
+
+// i [A, B]
+__device__ __forceinline__ Md icomm(const Md &a, const Md &b) {
+    return times_i(minus(mul(a, b), mul(b, a)), 1.);
+}
+
+__device__ __forceinline__ Md ld_herm(const double *p, size_t pos, size_t n) {
+    return from_h(ld_h(p, pos, n));
+}
+__device__ __forceinline__ Md ld_herm8(const double *p, size_t pos, size_t n) {
+    return from_h(ld_h8(p, pos, n));
+}
+
+__device__ __forceinline__ void atomic_add_m(C<double> *buf, size_t pos, size_t n,
+                                             const Md &a) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        atomicAdd(&buf[k * n + pos].r, a.m[k].r);
+        atomicAdd(&buf[k * n + pos].i, a.m[k].i);
+    }
+}
+
+__device__ __forceinline__ Md ld_adj(const C<double> *buf, size_t pos, size_t n) {
+    return ld_m3(buf, pos, n);
+}
+
+// T2(X) = 1 + X + X^2 / 2
+__device__ __forceinline__ Md taylor2(const Md &x) {
+    Md r = mul(x, x);
+#pragma unroll
+    for (int k = 0; k < 9; k++) r.m[k] = {0.5 * r.m[k].r + x.m[k].r, 0.5 * r.m[k].i + x.m[k].i};
+    r.m[0].r += 1.;
+    r.m[4].r += 1.;
+    r.m[8].r += 1.;
+    return r;
+}
+
+// inverse of a 3x3 complex matrix (adjugate / determinant)
+__device__ __forceinline__ Md inverse3(const Md &a) {
+    auto e = [&](int r, int c) { return a.m[3 * r + c]; };
+    auto sub = [](C<double> x, C<double> y) { return C<double>{x.r - y.r, x.i - y.i}; };
+    Md adj;
+    adj.m[0] = sub(cmul(e(1, 1), e(2, 2)), cmul(e(1, 2), e(2, 1)));
+    adj.m[1] = sub(cmul(e(0, 2), e(2, 1)), cmul(e(0, 1), e(2, 2)));
+    adj.m[2] = sub(cmul(e(0, 1), e(1, 2)), cmul(e(0, 2), e(1, 1)));
+    adj.m[3] = sub(cmul(e(1, 2), e(2, 0)), cmul(e(1, 0), e(2, 2)));
+    adj.m[4] = sub(cmul(e(0, 0), e(2, 2)), cmul(e(0, 2), e(2, 0)));
+    adj.m[5] = sub(cmul(e(0, 2), e(1, 0)), cmul(e(0, 0), e(1, 2)));
+    adj.m[6] = sub(cmul(e(1, 0), e(2, 1)), cmul(e(1, 1), e(2, 0)));
+    adj.m[7] = sub(cmul(e(0, 1), e(2, 0)), cmul(e(0, 0), e(2, 1)));
+    adj.m[8] = sub(cmul(e(0, 0), e(1, 1)), cmul(e(0, 1), e(1, 0)));
+    C<double> det = {0., 0.};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const C<double> t = cmul(e(0, k), adj.m[3 * k]);
+        det.r += t.r;
+        det.i += t.i;
+    }
+    const double d2 = det.r * det.r + det.i * det.i;
+    const C<double> inv = {det.r / d2, -det.i / d2};
+#pragma unroll
+    for (int k = 0; k < 9; k++) adj.m[k] = cmul(adj.m[k], inv);
+    return adj;
+}
+
+struct StepGeom {
+    int N;
+    size_t pos, pX, pY, mX, mY, pXmY, mXpY;
+};
+
+__device__ __forceinline__ StepGeom step_geom(int N, int ix, int iy) {
+    StepGeom g;
+    g.N = N;
+    const int ixp = min(N - 1, ix + 1), ixm = max(0, ix - 1);
+    const int iyp = min(N - 1, iy + 1), iym = max(0, iy - 1);
+    g.pos = at(N, ix, iy);
+    g.pX = at(N, ixp, iy);
+    g.pY = at(N, ix, iyp);
+    g.mX = at(N, ixm, iy);
+    g.mY = at(N, ix, iym);
+    g.pXmY = at(N, ixp, iym);
+    g.mXpY = at(N, ixm, iyp);
+    return g;
+}
+
+// the E and pi increments of S_e at one site (before the traceless
+// projection of E): dE1, dE2, dpi
+__device__ __forceinline__ void se_increments(const State<double> &s, const StepGeom &G,
+                                              double cst, double cdt, Md &dE1, Md &dE2,
+                                              Md &dpi) {
+    const size_t n = (size_t)G.N * G.N;
+    const Md ux = ld_m3(s.ux, G.pos, n), uy = ld_m3(s.uy, G.pos, n);
+    const Md a = mul(ux, ld_m3(s.uy, G.pX, n));
+    const Md b = mul(uy, ld_m3(s.ux, G.pY, n));
+    const Md h12 = from_h(i_antiherm(mul_nd(a, b)));
+    Md t1 = h12, t2 = sc(h12, -1.);
+    {
+        const Md p = mul_nd(ux, ld_m3(s.uy, G.pXmY, n));
+        const Md q = mul_dn(ld_m3(s.ux, G.mY, n), ld_m3(s.uy, G.mY, n));
+        add_to(t1, from_h(i_antiherm(mul(p, q))));
+    }
+    {
+        const Md p = mul_nd(uy, ld_m3(s.ux, G.mXpY, n));
+        const Md q = mul_dn(ld_m3(s.uy, G.mX, n), ld_m3(s.ux, G.mX, n));
+        add_to(t2, from_h(i_antiherm(mul(p, q))));
+    }
+    const Md phi = ld_herm(s.phi, G.pos, n);
+    const Md phx = mul_nd(mul(ux, ld_herm(s.phi, G.pX, n)), ux);
+    const Md phy = mul_nd(mul(uy, ld_herm(s.phi, G.pY, n)), uy);
+    const Md ux_m = ld_m3(s.ux, G.mX, n), uy_m = ld_m3(s.uy, G.mY, n);
+    const Md bx = mul(mul_dn(ux_m, ld_herm(s.phi, G.mX, n)), ux_m);
+    const Md by = mul(mul_dn(uy_m, ld_herm(s.phi, G.mY, n)), uy_m);
+    dE1 = addm(sc(tl(t1), cst), sc(icomm(phx, phi), cdt));
+    dE2 = addm(sc(tl(t2), cst), sc(icomm(phy, phi), cdt));
+    Md br = addm(addm(phx, phy), addm(bx, by));
+    add_to(br, sc(phi, -4.));
+    dpi = sc(br, cdt);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// time reversal of one step
+// ---------------------------------------------------------------------------
+
+// U_d = T2(i c E_d')^{-1} U_d',  phi = phi' - c2 pi'
+__global__ void k_inv_su(int N, State<double> nxt, State<double> cur, double c, double c2) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    for (int d = 0; d < 2; d++) {
+        const Md E = ld_herm8(d ? nxt.e2 : nxt.e1, pos, n);
+        const Md M = taylor2(times_i(E, c));
+        st_m3(d ? cur.uy : cur.ux, pos, n, mul(inverse3(M), ld_m3(d ? nxt.uy : nxt.ux, pos, n)));
+    }
+    H3<double> phi = ld_h(nxt.phi, pos, n);
+    h_axpy(phi, -c2, ld_h(nxt.pi, pos, n));
+    st_h(cur.phi, pos, n, phi);
+}
+
+// pi = pi' - dpi(U, phi),  E_d = E_d' - TL(dE_d(U, phi)); do_pe = 0 copies
+__global__ void k_inv_se(int N, State<double> nxt, State<double> cur, double cst, double cdt,
+                         int do_pe) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    H3<double> pi = ld_h(nxt.pi, pos, n);
+    H3<double> e1 = ld_h8(nxt.e1, pos, n), e2 = ld_h8(nxt.e2, pos, n);
+    if (do_pe) {
+        const StepGeom G = step_geom(N, (int)(pos / N), (int)(pos % N));
+        Md dE1, dE2, dpi;
+        se_increments(cur, G, cst, cdt, dE1, dE2, dpi);
+        h_axpy(pi, -1., to_h(dpi));
+        h_axpy(e1, -1., to_h(tl(dE1)));
+        h_axpy(e2, -1., to_h(tl(dE2)));
+        h_traceless(e1);
+        h_traceless(e2);
+    }
+    st_h(cur.pi, pos, n, pi);
+    st_h8(cur.e1, pos, n, e1);
+    st_h8(cur.e2, pos, n, e2);
+}
+
+// ---------------------------------------------------------------------------
+// vector-Jacobian products
+// ---------------------------------------------------------------------------
+
+// S_u: reads the adjoints of the step's outputs, leaves the adjoints of its
+// inputs (U before the update, phi before, pi' and E' after S_e). `cur` holds
+// U, phi of the step's input, `nxt` E' of its output.
+__global__ void k_adj_su(int N, State<double> cur, State<double> nxt, AdjState a, double c,
+                         double c2) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    const Md phib = herm(ld_adj(a.phi, pos, n));
+    Md pib = herm(ld_adj(a.pi, pos, n));
+    add_to(pib, sc(phib, c2));
+    st_m3(a.phi, pos, n, phib);
+    st_m3(a.pi, pos, n, pib);
+    for (int d = 0; d < 2; d++) {
+        C<double> *Ub = d ? a.uy : a.ux;
+        C<double> *Eb = d ? a.e2 : a.e1;
+        const Md Ubar = ld_adj(Ub, pos, n);
+        const Md U = ld_m3(d ? cur.uy : cur.ux, pos, n);
+        const Md X = times_i(ld_herm8(d ? nxt.e2 : nxt.e1, pos, n), c);
+        const Md M = taylor2(X);
+        st_m3(Ub, pos, n, mul_dn(M, Ubar));
+        const Md Mb = mul_nd(Ubar, U);
+        // X_bar = M_bar + (M_bar X^dag + X^dag M_bar) / 2
+        Md Xb = Mb;
+        add_to(Xb, sc(addm(mul_nd(Mb, X), mul_dn(X, Mb)), 0.5));
+        // X = i c E  ->  E_bar += Herm(-i c X_bar)
+        Md Eb_ = ld_adj(Eb, pos, n);
+        add_to(Eb_, herm(times_i(Xb, -c)));
+        st_m3(Eb, pos, n, Eb_);
+    }
+}
+
+// S_e: adjoints of E' and pi' (own site) -> adjoints of E (own), and atomic
+// contributions to the link and phi adjoints of the site and its neighbours.
+__global__ void k_adj_se(int N, State<double> cur, AdjState a, double cst, double cdt) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    const StepGeom G = step_geom(N, (int)(pos / N), (int)(pos % N));
+    const Md G1 = tl(herm(ld_adj(a.e1, pos, n)));
+    const Md G2 = tl(herm(ld_adj(a.e2, pos, n)));
+    st_m3(a.e1, pos, n, G1);
+    st_m3(a.e2, pos, n, G2);
+    const Md pib = herm(ld_adj(a.pi, pos, n));
+
+    const Md ux = ld_m3(cur.ux, pos, n), uy = ld_m3(cur.uy, pos, n);
+    const Md t1b = sc(G1, cst), t2b = sc(G2, cst);
+    Md uxb = {}, uyb = {}, phib = {};
+    // plaquette h12 = iAH(a b^dag), a = Ux Uy(+x), b = Uy Ux(+y); enters E1 (+), E2 (-)
+    {
+        const Md uy_px = ld_m3(cur.uy, G.pX, n), ux_py = ld_m3(cur.ux, G.pY, n);
+        const Md A = mul(ux, uy_px), B = mul(uy, ux_py);
+        const Md Mb = times_i(minus(t1b, t2b), -2.);
+        const Md Ab = mul(Mb, B), Bb = mul_dn(Mb, A);
+        add_to(uxb, mul_nd(Ab, uy_px));
+        atomic_add_m(a.uy, G.pX, n, mul_dn(ux, Ab));
+        add_to(uyb, mul_nd(Bb, ux_py));
+        atomic_add_m(a.ux, G.pY, n, mul_dn(uy, Bb));
+    }
+    // staple of E1: p = Ux Uy(+x-y)^dag, q = Ux(-y)^dag Uy(-y)
+    {
+        const Md uy_pxmy = ld_m3(cur.uy, G.pXmY, n);
+        const Md ux_my = ld_m3(cur.ux, G.mY, n), uy_my = ld_m3(cur.uy, G.mY, n);
+        const Md P = mul_nd(ux, uy_pxmy), Q = mul_dn(ux_my, uy_my);
+        const Md Mb = times_i(t1b, -2.);
+        const Md Pb = mul_nd(Mb, Q), Qb = mul_dn(P, Mb);
+        add_to(uxb, mul(Pb, uy_pxmy));
+        atomic_add_m(a.uy, G.pXmY, n, mul_dn(Pb, ux));
+        atomic_add_m(a.ux, G.mY, n, mul_nd(uy_my, Qb));
+        atomic_add_m(a.uy, G.mY, n, mul(ux_my, Qb));
+    }
+    // staple of E2: p = Uy Ux(-x+y)^dag, q = Uy(-x)^dag Ux(-x)
+    {
+        const Md ux_mxpy = ld_m3(cur.ux, G.mXpY, n);
+        const Md uy_mx = ld_m3(cur.uy, G.mX, n), ux_mx = ld_m3(cur.ux, G.mX, n);
+        const Md P = mul_nd(uy, ux_mxpy), Q = mul_dn(uy_mx, ux_mx);
+        const Md Mb = times_i(t2b, -2.);
+        const Md Pb = mul_nd(Mb, Q), Qb = mul_dn(P, Mb);
+        add_to(uyb, mul(Pb, ux_mxpy));
+        atomic_add_m(a.ux, G.mXpY, n, mul_dn(Pb, uy));
+        atomic_add_m(a.uy, G.mX, n, mul_nd(ux_mx, Qb));
+        atomic_add_m(a.ux, G.mX, n, mul(uy_mx, Qb));
+    }
+    // transports of phi: commutator terms of E and the pi bracket
+    const Md phi = ld_herm(cur.phi, pos, n);
+    const Md brb = sc(pib, cdt);
+    add_to(phib, sc(brb, -4.));
+    {
+        const Md f = ld_herm(cur.phi, G.pX, n);
+        const Md phx = mul_nd(mul(ux, f), ux);
+        const Md Cb = sc(G1, cdt);
+        Md phxb = icomm(phi, Cb);
+        add_to(phib, icomm(Cb, phx));
+        add_to(phxb, brb);
+        add_to(uxb, sc(mul(mul(phxb, ux), f), 2.));
+        atomic_add_m(a.phi, G.pX, n, mul(mul_dn(ux, phxb), ux));
+    }
+    {
+        const Md f = ld_herm(cur.phi, G.pY, n);
+        const Md phy = mul_nd(mul(uy, f), uy);
+        const Md Cb = sc(G2, cdt);
+        Md phyb = icomm(phi, Cb);
+        add_to(phib, icomm(Cb, phy));
+        add_to(phyb, brb);
+        add_to(uyb, sc(mul(mul(phyb, uy), f), 2.));
+        atomic_add_m(a.phi, G.pY, n, mul(mul_dn(uy, phyb), uy));
+    }
+    {
+        // U(-x)^dag phi(-x) U(-x): U_bar += 2 phi U C_bar, phi_bar += U C_bar U^dag
+        const Md u = ld_m3(cur.ux, G.mX, n), f = ld_herm(cur.phi, G.mX, n);
+        atomic_add_m(a.ux, G.mX, n, sc(mul(mul(f, u), brb), 2.));
+        atomic_add_m(a.phi, G.mX, n, mul_nd(mul(u, brb), u));
+    }
+    {
+        const Md u = ld_m3(cur.uy, G.mY, n), f = ld_herm(cur.phi, G.mY, n);
+        atomic_add_m(a.uy, G.mY, n, sc(mul(mul(f, u), brb), 2.));
+        atomic_add_m(a.phi, G.mY, n, mul_nd(mul(u, brb), u));
+    }
+    atomic_add_m(a.ux, pos, n, uxb);
+    atomic_add_m(a.uy, pos, n, uyb);
+    atomic_add_m(a.phi, pos, n, phib);
+}
+
+// adjoint of T^tautau (k_tmunu_diag, Evolution.cpp:759-900) in lattice units,
+// tbar[pos] = dL/dTtt_lat(pos)
+__global__ void k_adj_ttt(int N, State<double> s, const double *tbar, AdjState a, double g,
+                          double tau) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    const double tb = tbar[pos];
+    if (tb == 0.) return;
+    const int i = (int)(pos / N), j = (int)(pos % N);
+    const size_t pX = at(N, min(N - 1, i + 1), j), pY = at(N, i, min(N - 1, j + 1));
+    const size_t pXY = at(N, min(N - 1, i + 1), min(N - 1, j + 1));
+    const double ge = g * g / tau / tau, ht = 0.5 / tau / tau;
+    // electric: ge/2 (|E1|^2 + |E1(+y)|^2 + |E2|^2 + |E2(+x)|^2)
+    atomic_add_m(a.e1, pos, n, sc(ld_herm8(s.e1, pos, n), tb * ge));
+    atomic_add_m(a.e1, pY, n, sc(ld_herm8(s.e1, pY, n), tb * ge));
+    atomic_add_m(a.e2, pos, n, sc(ld_herm8(s.e2, pos, n), tb * ge));
+    atomic_add_m(a.e2, pX, n, sc(ld_herm8(s.e2, pX, n), tb * ge));
+    // longitudinal electric: tr pi^2 / 4 over four cells
+    const size_t cells[4] = {pos, pX, pY, pXY};
+    for (int k = 0; k < 4; k++)
+        atomic_add_m(a.pi, cells[k], n, sc(ld_herm(s.pi, cells[k], n), 0.5 * tb));
+    const Md ux = ld_m3(s.ux, pos, n), uy = ld_m3(s.uy, pos, n);
+    // magnetic: 2/g^2 (3 - Re tr(Ux Uy(+x) Ux(+y)^dag Uy^dag)), zero on the last row
+    if (i != N - 1) {
+        const double cb = -2. / (g * g) * tb;
+        const Md uy_px = ld_m3(s.uy, pX, n), ux_py = ld_m3(s.ux, pY, n);
+        const Md A12 = mul(ux, uy_px);
+        // plaq = A1 A2 A3 A4 with A1 = Ux, A2 = Uy(+x), A3 = Ux(+y)^dag, A4 = Uy^dag
+        const Md R = mul_nd(mul_nd(uy_px, ux_py), uy);  // A2 A3 A4
+        atomic_add_m(a.ux, pos, n, sc(dagger(R), cb));
+        atomic_add_m(a.uy, pX, n, sc(mul_dn(ux, mul(uy, ux_py)), cb));
+        atomic_add_m(a.ux, pY, n, sc(mul_dn(uy, A12), cb));
+        atomic_add_m(a.uy, pos, n, sc(mul_nd(A12, ux_py), cb));
+    }
+    // longitudinal magnetic: ht tr(d^2), d = phi_a - U phi_b U^dag
+    struct Term {
+        size_t pa, pb;
+        const C<double> *u;
+        C<double> *ub;
+        size_t pu;
+    };
+    const Term terms[4] = {{pos, pX, s.ux, a.ux, pos},
+                           {pos, pY, s.uy, a.uy, pos},
+                           {pY, pXY, s.ux, a.ux, pY},
+                           {pX, pXY, s.uy, a.uy, pX}};
+    for (int k = 0; k < 4; k++) {
+        const Term &T = terms[k];
+        const Md u = ld_m3(T.u, T.pu, n), fb = ld_herm(s.phi, T.pb, n);
+        const Md C = mul_nd(mul(u, fb), u);
+        const Md d = minus(ld_herm(s.phi, T.pa, n), C);
+        const Md db = sc(d, 2. * ht * tb);
+        atomic_add_m(a.phi, T.pa, n, db);
+        const Md Cb = sc(db, -1.);
+        atomic_add_m(T.ub, T.pu, n, sc(mul(mul(Cb, u), fb), 2.));
+        atomic_add_m(a.phi, T.pb, n, mul(mul_dn(u, Cb), u));
+    }
+}
+
+// Hermitian (and, for E, traceless) parts of the adjoints
+__global__ void k_adj_project(size_t n, AdjState a) {
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    st_m3(a.e1, pos, n, tl(herm(ld_adj(a.e1, pos, n))));
+    st_m3(a.e2, pos, n, tl(herm(ld_adj(a.e2, pos, n))));
+    st_m3(a.phi, pos, n, herm(ld_adj(a.phi, pos, n)));
+    st_m3(a.pi, pos, n, herm(ld_adj(a.pi, pos, n)));
+}
+
+// ---------------------------------------------------------------------------
+// adjoint of the initial conditions (Init.cpp:1678-1849, 2437-2691)
+// ---------------------------------------------------------------------------
+namespace {
+
+// Gaussian elimination with partial pivoting for the 8 x 8 transposed Newton
+// Jacobian (row-major a, solution into x)
+__device__ void solve8(double a[64], double b[8], double x[8]) {
+    for (int col = 0; col < 8; col++) {
+        int piv = col;
+        for (int r = col + 1; r < 8; r++)
+            if (fabs(a[r * 8 + col]) > fabs(a[piv * 8 + col])) piv = r;
+        if (piv != col) {
+            for (int k = 0; k < 8; k++) {
+                const double t = a[col * 8 + k];
+                a[col * 8 + k] = a[piv * 8 + k];
+                a[piv * 8 + k] = t;
+            }
+            const double t = b[col];
+            b[col] = b[piv];
+            b[piv] = t;
+        }
+        const double d = a[col * 8 + col];
+        for (int r = col + 1; r < 8; r++) {
+            const double l = d != 0. ? a[r * 8 + col] / d : 0.;
+            for (int k = col; k < 8; k++) a[r * 8 + k] -= l * a[col * 8 + k];
+            b[r] -= l * b[col];
+        }
+    }
+    for (int r = 7; r >= 0; r--) {
+        double acc = b[r];
+        for (int k = r + 1; k < 8; k++) acc -= a[r * 8 + k] * x[k];
+        x[r] = a[r * 8 + r] != 0. ? acc / a[r * 8 + r] : 0.;
+    }
+}
+
+// Re tr(A^dag B)
+__device__ __forceinline__ double re_dot(const Md &a, const Md &b) {
+    double s = 0.;
+#pragma unroll
+    for (int k = 0; k < 9; k++) s += a.m[k].r * b.m[k].r + a.m[k].i * b.m[k].i;
+    return s;
+}
+
+// central difference of the closed-form exponential exp(i q.t) along q_b
+__device__ __forceinline__ Md dexp(double q[8], int b, double h) {
+    const double q0 = q[b];
+    q[b] = q0 + h;
+    const Md ep = exp_from_coeff(q);
+    q[b] = q0 - h;
+    const Md em = exp_from_coeff(q);
+    q[b] = q0;
+    return sc(minus(ep, em), 0.5 / h);
+}
+
+constexpr double kDexpStep = 1e-5;  // truncation ~1e-10, rounding ~1e-11
+
+}  // namespace
+
+// pi(tau=0) = -i t / (4 g), t the "minus" stencil (init.cu k_initial_pi):
+// pi_bar -> adjoints of U1, U2 (both directions) and of the tau = 0 links
+__global__ void k_adj_initial_pi(int N, double g, const C<double> *u1x, const C<double> *u2x,
+                                 const C<double> *u1y, const C<double> *u2y,
+                                 const C<double> *ux, const C<double> *uy, AdjState a,
+                                 C<double> *b1x, C<double> *b2x, C<double> *b1y,
+                                 C<double> *b2y) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    const int ix = (int)(pos / N), iy = (int)(pos % N);
+    const size_t mX = at(N, max(0, ix - 1), iy), mY = at(N, ix, max(0, iy - 1));
+    const Md tb = times_i(herm(ld_adj(a.pi, pos, n)), 1. / (4. * g));
+    const Md tbd = dagger(tb);
+    for (int dir = 0; dir < 2; dir++) {
+        const C<double> *u1 = dir ? u1y : u1x, *u2 = dir ? u2y : u2x, *u = dir ? uy : ux;
+        C<double> *b1 = dir ? b1y : b1x, *b2 = dir ? b2y : b2x, *ub = dir ? a.uy : a.ux;
+        {
+            // here: D U^dag - D - U D^dag + D^dag
+            const Md U = ld_m3(u, pos, n), D = minus(ld_m3(u1, pos, n), ld_m3(u2, pos, n));
+            Md Db = mul(tb, U);
+            sub_from(Db, tb);
+            sub_from(Db, mul(tbd, U));
+            add_to(Db, tbd);
+            const Md Ub = minus(mul(tbd, D), mul(tb, D));
+            atomic_add_m(b1, pos, n, Db);
+            atomic_add_m(b2, pos, n, sc(Db, -1.));
+            atomic_add_m(ub, pos, n, Ub);
+        }
+        {
+            // minus (at the -dir neighbour): -U^dag D + D + D^dag U - D^dag
+            const size_t q = dir ? mY : mX;
+            const Md U = ld_m3(u, q, n), D = minus(ld_m3(u1, q, n), ld_m3(u2, q, n));
+            Md Db = sc(mul(U, tb), -1.);
+            add_to(Db, tb);
+            add_to(Db, mul(U, tbd));
+            sub_from(Db, tbd);
+            const Md Ub = minus(mul(D, tb), mul(D, tbd));
+            atomic_add_m(b1, q, n, Db);
+            atomic_add_m(b2, q, n, sc(Db, -1.));
+            atomic_add_m(ub, q, n, Ub);
+        }
+    }
+}
+
+// Newton links U = exp(i alpha.t) U1 U2 with F(alpha; U1, U2) = 0 (k_newton):
+// implicit-function adjoint. With alpha_bar_b = Re tr(U_bar^dag dU/dalpha_b)
+// and J^T lambda = alpha_bar, U1 and U2 receive the direct part through
+// U1 U2 minus the adjoint of sum_a lambda_a F_a at fixed alpha.
+__global__ void __launch_bounds__(128)
+    k_adj_newton(int N, const C<double> *u1x, const C<double> *u2x, const C<double> *u1y,
+                 const C<double> *u2y, const double *alpha, AdjState a, C<double> *b1x,
+                 C<double> *b2x, C<double> *b1y, C<double> *b2y) {
+    const size_t n = (size_t)N * N;
+    const size_t lid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (lid >= 2 * n) return;
+    const size_t pos = lid >> 1;
+    const int dir = (int)(lid & 1);
+    const Md U1 = ld_m3(dir ? u1y : u1x, pos, n), U2 = ld_m3(dir ? u2y : u2x, pos, n);
+    const Md S = addm(U1, U2), U0 = mul(U1, U2);
+    double q[8];
+    for (int k = 0; k < 8; k++) q[k] = alpha[(size_t)k * 2 * n + lid];
+    const Md E = exp_from_coeff(q);
+    const Md Ub = ld_adj(dir ? a.uy : a.ux, pos, n);
+    double J[64], abar[8], lam[8];
+    for (int b = 0; b < 8; b++) {
+        const Md dU = mul(dexp(q, b, kDexpStep), U0);
+        abar[b] = re_dot(Ub, dU);
+        // dF_a = -Im tr(t^a (S dU^dag - dU S^dag)); stored transposed
+        C<double> tr[8];
+        trace_ta(minus(mul_nd(S, dU), mul_nd(dU, S)), tr);
+        for (int r = 0; r < 8; r++) J[b * 8 + r] = -tr[r].i;
+    }
+    solve8(J, abar, lam);
+    // Lambda = sum lambda_a t^a, M_bar = -i Lambda
+    Md one, Lam = {};
+    set_identity(one);
+    for (int r = 0; r < 8; r++) add_to(Lam, sc(ta_mul(r, one), lam[r]));
+    const Md Mb = times_i(Lam, -1.), Mbd = dagger(Mb);
+    const Md U = mul(E, U0);
+    // M = S - S^dag + S U^dag - U S^dag
+    Md Sb = minus(Mb, Mbd);
+    add_to(Sb, mul(Mb, U));
+    sub_from(Sb, mul(Mbd, U));
+    const Md Udir = minus(mul(Mbd, S), mul(Mb, S));
+    const Md U0psi = mul_dn(E, Udir);
+    const Md U0d = mul_dn(E, Ub);
+    const Md G0 = minus(U0d, U0psi);  // adjoint of U1 U2 in total
+    Md g1 = mul_nd(G0, U2), g2 = mul_dn(U1, G0);
+    sub_from(g1, Sb);
+    sub_from(g2, Sb);
+    C<double> *B1 = dir ? b1y : b1x, *B2 = dir ? b2y : b2x;
+    atomic_add_m(B1, pos, n, g1);
+    atomic_add_m(B2, pos, n, g2);
+}
+
+// link products U1 = V_A V_A(+i)^dag, U2 = V_B V_B(+i)^dag (k_link_products)
+__global__ void k_adj_link_products(int N, const C<double> *VA, const C<double> *VB,
+                                    const C<double> *b1x, const C<double> *b2x,
+                                    const C<double> *b1y, const C<double> *b2y, C<double> *vbA,
+                                    C<double> *vbB) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    const int ix = (int)(pos / N), iy = (int)(pos % N);
+    const size_t pX = at(N, min(N - 1, ix + 1), iy), pY = at(N, ix, min(N - 1, iy + 1));
+    for (int nuc = 0; nuc < 2; nuc++) {
+        const C<double> *V = nuc ? VB : VA;
+        C<double> *vb = nuc ? vbB : vbA;
+        const Md v = ld_m3(V, pos, n);
+        const Md bx = ld_adj(nuc ? b2x : b1x, pos, n), by = ld_adj(nuc ? b2y : b1y, pos, n);
+        atomic_add_m(vb, pos, n, addm(mul(bx, ld_m3(V, pX, n)), mul(by, ld_m3(V, pY, n))));
+        atomic_add_m(vb, pX, n, mul_dn(bx, v));
+        atomic_add_m(vb, pY, n, mul_dn(by, v));
+    }
+}
+
+// one sheet of V_k = exp(-i A_k.t) V_{k-1}, backwards: V <- V_{k-1} (time
+// reversal by the unitary inverse), V_bar <- V_bar_{k-1}, and the packed A
+// of the sheet in work is replaced by its adjoint A_bar
+__global__ void __launch_bounds__(128) k_adj_wilson_sheet(int N, double2 *work, C<double> *V,
+                                                          C<double> *Vb) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    double q[8];
+    for (int c = 0; c < 4; c++) {
+        const double2 v = work[(size_t)c * n + pos];
+        q[2 * c] = -v.x;
+        q[2 * c + 1] = -v.y;
+    }
+    const Md e = exp_from_coeff(q);
+    const Md Vk = ld_m3(V, pos, n), Vbk = ld_m3(Vb, pos, n);
+    const Md Vprev = mul_dn(e, Vk);
+    const Md eb = mul_nd(Vbk, Vprev);
+    st_m3(V, pos, n, Vprev);
+    st_m3(Vb, pos, n, mul_dn(e, Vbk));
+    double qb[8];
+    for (int b = 0; b < 8; b++) qb[b] = re_dot(eb, dexp(q, b, kDexpStep));
+    for (int c = 0; c < 4; c++) work[(size_t)c * n + pos] = make_double2(-qb[2 * c], -qb[2 * c + 1]);
+}
+
+// rho = g sqrt(g2mu2 / Ny) xi: the packed rho_bar of one sheet in work ->
+// g2mu2_bar (accumulated) and, if rho_out is set, rho_bar as [n][8]
+__global__ void k_adj_rho(int N, int Ny, double g, const double *g2mu2, const double *xi,
+                          uint64_t key, uint32_t nucleus, int k, const double2 *work,
+                          double *g2mu_bar, double *rho_out) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    double z[8];
+    if (xi) {
+        for (int a = 0; a < 8; a++) z[a] = xi[((size_t)k * n + pos) * 8 + a];
+    } else {
+        for (int h = 0; h < 2; h++)
+            for (int p = 0; p < 2; p++)
+                normal2({(uint32_t)pos, (uint32_t)k, (nucleus << 1) | (uint32_t)h, 0u}, key, p,
+                        z + 4 * h + 2 * p);
+    }
+    double acc = 0.;
+    for (int c = 0; c < 4; c++) {
+        const double2 v = work[(size_t)c * n + pos];
+        acc += v.x * z[2 * c] + v.y * z[2 * c + 1];
+        if (rho_out) {
+            rho_out[pos * 8 + 2 * c] = v.x;
+            rho_out[pos * 8 + 2 * c + 1] = v.y;
+        }
+    }
+    const double m = g2mu2[pos];
+    if (m > 0.) g2mu_bar[pos] += acc * g / (2. * sqrt(m * Ny));
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+namespace {
+inline unsigned blocks(size_t n) { return (unsigned)((n + 127) / 128); }
+}  // namespace
+
+void launch_inverse_step(int N, const State<double> &nxt, const State<double> &cur,
+                         const StepCoef<double> &cf, cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    const double c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / 2.);
+    const double c2 = (cf.tau + cf.dt_pu / 2.) * cf.dt_pu;
+    const double cst = cf.tau * cf.dt_pe / (2. * cf.g * cf.g);
+    const double cdt = cf.tau > 0 ? cf.dt_pe / cf.tau : 0.;
+    k_inv_su<<<blocks(n), 128, 0, st>>>(N, nxt, cur, c, c2);
+    k_inv_se<<<blocks(n), 128, 0, st>>>(N, nxt, cur, cst, cdt, cf.do_pe);
+}
+
+void launch_adjoint_step(int N, const State<double> &cur, const State<double> &nxt,
+                         const AdjState &a, const StepCoef<double> &cf, cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    const double c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / 2.);
+    const double c2 = (cf.tau + cf.dt_pu / 2.) * cf.dt_pu;
+    k_adj_su<<<blocks(n), 128, 0, st>>>(N, cur, nxt, a, c, c2);
+    if (cf.do_pe) {
+        const double cst = cf.tau * cf.dt_pe / (2. * cf.g * cf.g);
+        const double cdt = cf.dt_pe / cf.tau;
+        k_adj_se<<<blocks(n), 128, 0, st>>>(N, cur, a, cst, cdt);
+    }
+}
+
+void launch_adjoint_ttt(int N, const State<double> &s, const double *tbar, const AdjState &a,
+                        double g, double tau, cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    k_adj_ttt<<<blocks(n), 128, 0, st>>>(N, s, tbar, a, g, tau);
+}
+
+void launch_adjoint_project(size_t n, const AdjState &a, cudaStream_t st) {
+    k_adj_project<<<blocks(n), 128, 0, st>>>(n, a);
+}
+
+void launch_adjoint_init_links(const AdjInitArgs &A, cudaStream_t st) {
+    const size_t n = (size_t)A.N * A.N;
+    k_adj_initial_pi<<<blocks(n), 128, 0, st>>>(A.N, A.g, A.u1x, A.u2x, A.u1y, A.u2y, A.ux, A.uy,
+                                                A.adj, A.b1x, A.b2x, A.b1y, A.b2y);
+    k_adj_newton<<<blocks(2 * n), 128, 0, st>>>(A.N, A.u1x, A.u2x, A.u1y, A.u2y, A.alpha, A.adj,
+                                                A.b1x, A.b2x, A.b1y, A.b2y);
+    k_adj_link_products<<<blocks(n), 128, 0, st>>>(A.N, A.VA, A.VB, A.b1x, A.b2x, A.b1y, A.b2y,
+                                                   A.vbA, A.vbB);
+}
+
+void launch_adjoint_wilson_sheet(int N, double2 *work, C<double> *V, C<double> *Vb,
+                                 cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    k_adj_wilson_sheet<<<blocks(n), 128, 0, st>>>(N, work, V, Vb);
+}
+
+void launch_adjoint_rho(const WilsonArgs &w, int k, double *g2mu_bar, double *rho_out,
+                        cudaStream_t st) {
+    const size_t n = (size_t)w.N * w.N;
+    k_adj_rho<<<blocks(n), 128, 0, st>>>(w.N, w.Ny, w.g, w.g2mu2, w.xi, w.philox_key, w.nucleus,
+                                         k, w.work, g2mu_bar, rho_out);
+}
+
+}  // namespace ipg

@@ -52,6 +52,7 @@ struct ipg_ctx {
     C<double> *VA = nullptr, *VB = nullptr;
     C<double> *u1x = nullptr, *u2x = nullptr, *u1y = nullptr, *u2y = nullptr;
     int *newton_iters = nullptr, *newton_status = nullptr;
+    double *newton_alpha = nullptr;  // [8][2n] exponents of the tau = 0 links
 
     // fields: FP64 state (+ second U/phi buffer), FP32 state (+ second buffer)
     State<double> s64{};
@@ -73,6 +74,25 @@ struct ipg_ctx {
     int it = 0;  // completed full steps
     double last_leapfrog_ms = 0;
     int last_leapfrog_launches = 0;
+
+    // adjoint workspace (allocated by the first ipg_forward)
+    struct {
+        int k = 0, steps = 0;
+        std::vector<State<double>> cp;  // state before step j k
+        State<double> w[3]{};           // working states
+        AdjState adj{};
+        double *tbar = nullptr;
+        State<double> fin{};            // state after the last step
+        bool ready = false;
+        double sums[6] = {0};            // W, X, Y, Sxx, Syy, Sxy of the weight
+        double sum_ttt = 0, ET = 0, eps2 = 0;
+        bool from_inputs = false;  // the tau = 0 state came from g2mu + noise
+        // initial-condition adjoint: U1/U2 adjoints, V adjoints, a V copy
+        C<double> *b1x = nullptr, *b2x = nullptr, *b1y = nullptr, *b2y = nullptr;
+        C<double> *vbA = nullptr, *vbB = nullptr, *vcur = nullptr;
+        double *g2mu_bar = nullptr, *rho_stage = nullptr;
+    } aw;
+    bool init_from_inputs = false;
 
     std::vector<void *> allocs;
 };
@@ -276,6 +296,61 @@ ipg_status state64(ipg_ctx *c) {
     return IPG_OK;
 }
 
+ipg_status copy_state(ipg_ctx *c, const State<double> &dst, const State<double> &src) {
+    const size_t n = c->n;
+    auto cp = [&](void *d, const void *s_, size_t bytes) {
+        return cudaMemcpyAsync(d, s_, bytes, cudaMemcpyDeviceToDevice, c->stream);
+    };
+    IPG_CUDA(c, cp(dst.ux, src.ux, 9 * n * sizeof(C<double>)));
+    IPG_CUDA(c, cp(dst.uy, src.uy, 9 * n * sizeof(C<double>)));
+    IPG_CUDA(c, cp(dst.e1, src.e1, 8 * n * sizeof(double)));
+    IPG_CUDA(c, cp(dst.e2, src.e2, 8 * n * sizeof(double)));
+    IPG_CUDA(c, cp(dst.phi, src.phi, 9 * n * sizeof(double)));
+    IPG_CUDA(c, cp(dst.pi, src.pi, 9 * n * sizeof(double)));
+    return IPG_OK;
+}
+
+// coefficients of launch s of run_evolution (0: tau = 0 half step)
+StepCoef<double> evolution_coef(const ipg_ctx *c, int s) {
+    StepCoef<double> cf;
+    cf.tau = s * c->dtau;
+    cf.dt_pe = c->dtau;
+    cf.dt_pu = c->dtau;
+    cf.g = c->cfg.g;
+    cf.do_pe = s > 0;
+    cf.do_pu = 1;
+    return cf;
+}
+
+// T^tautau-weighted eccentricity over the cells [2, N-2)^2 (the cells the
+// reference's eccentricity sums over) with the weighted centroid as origin:
+// eps2 = |sum w (x~ + i y~)^2| / sum w (x~^2 + y~^2), from the weight sums
+// W, X = sum w x, Y, Sxx = sum w x^2, Syy, Sxy; d[6] receives d eps2 / d sums.
+double eps2_from_sums(const double *S, double *d) {
+    const double W = S[0], X = S[1], Y = S[2], Sxx = S[3], Syy = S[4], Sxy = S[5];
+    const double cxx = Sxx - X * X / W, cyy = Syy - Y * Y / W, cxy = Sxy - X * Y / W;
+    const double re = cxx - cyy, im = 2. * cxy, den = cxx + cyy;
+    const double mag = std::sqrt(re * re + im * im);
+    const double e = mag / den;
+    if (d) {
+        // d e / d (cxx, cyy, cxy)
+        const double dre = mag > 0 ? re / mag : 0., dim = mag > 0 ? im / mag : 0.;
+        const double gxx = (dre) / den - e / den;
+        const double gyy = (-dre) / den - e / den;
+        const double gxy = 2. * dim / den;
+        // cxx = Sxx - X^2/W, cyy = Syy - Y^2/W, cxy = Sxy - XY/W
+        d[0] = gxx * (X * X / (W * W)) + gyy * (Y * Y / (W * W)) + gxy * (X * Y / (W * W));
+        d[1] = gxx * (-2. * X / W) + gxy * (-Y / W);
+        d[2] = gyy * (-2. * Y / W) + gxy * (-X / W);
+        d[3] = gxx;
+        d[4] = gyy;
+        d[5] = gxy;
+    }
+    return e;
+}
+
+bool in_ecc_window(int N, int i, int j) { return i >= 2 && i < N - 2 && j >= 2 && j < N - 2; }
+
 // The leapfrog schedule of Evolution::run up to it = itmax - 1: the tau = 0
 // half step of phi and U (Evolution.cpp:393-394), then full steps
 // it = 1 .. itmax-1 (416-421).
@@ -416,6 +491,7 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
         return bad("precision must be IPG_FP64 or IPG_FP32");
     if (c->cfg.newton_max_iterations <= 0) c->cfg.newton_max_iterations = 2000;
     if (c->cfg.newton_max_restarts <= 0) c->cfg.newton_max_restarts = 200;
+    if (!(c->cfg.newton_tolerance > 0)) c->cfg.newton_tolerance = 1e-6;
     c->N = N;
     c->logN = ilog2(N);
     c->n = (size_t)N * N;
@@ -456,6 +532,7 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
     IPG_TRY(dalloc(c, &c->u2y, 9 * n));
     IPG_TRY(dalloc(c, &c->newton_iters, 2 * n));
     IPG_TRY(dalloc(c, &c->newton_status, 2 * n));
+    IPG_TRY(dalloc(c, &c->newton_alpha, 16 * n));
     IPG_TRY(alloc_state64(c, c->s64));
     IPG_TRY(dalloc(c, &c->ux64b, 9 * n));
     IPG_TRY(dalloc(c, &c->uy64b, 9 * n));
@@ -629,6 +706,8 @@ static ipg_status init_impl(ipg_ctx *c, ipg_init_report *rep, bool from_wilson) 
     na.N = N;
     na.max_iter = c->cfg.newton_max_iterations;
     na.max_restart = c->cfg.newton_max_restarts;
+    na.tol = c->cfg.newton_tolerance;
+    na.alpha = c->newton_alpha;
     na.philox_key = c->cfg.seed ^ 0x5DEECE66DULL;
     na.u1x = c->u1x;
     na.u2x = c->u2x;
@@ -676,6 +755,7 @@ static ipg_status init_impl(ipg_ctx *c, ipg_init_report *rep, bool from_wilson) 
     }
     for (auto &x : e) cudaEventDestroy(x);
     c->initialized = true;
+    c->init_from_inputs = !from_wilson;
     c->half_done = false;
     c->finished = false;
     c->it = 0;
@@ -773,6 +853,7 @@ ipg_status ipg_get_field(ipg_ctx *c, int which, double *out) {
 ipg_status ipg_set_field(ipg_ctx *c, int which, const double *in) {
     if (!c || !in) return IPG_ERR_BAD_CONFIG;
     const size_t n = c->n;
+    c->init_from_inputs = false;
     IPG_TRY(sync(c));
     if (which == IPG_VA || which == IPG_VB || which == IPG_UX || which == IPG_UY) {
         C<double> *dst = which == IPG_VA ? c->VA
@@ -832,6 +913,257 @@ ipg_status ipg_last_leapfrog_ms(ipg_ctx *c, double *ms, int *launches) {
 ipg_status ipg_kernel_launches(const ipg_ctx *c, long long *count) {
     if (!c || !count) return IPG_ERR_BAD_CONFIG;
     *count = c->launches;
+    return IPG_OK;
+}
+
+}  // extern "C"
+
+// Adjoint of the initial conditions: from the adjoints of the tau = 0 state
+// (c->aw.adj, projected) through the initial pi and the Newton links to U1,
+// U2, V_A, V_B, then sheet by sheet backwards through the Wilson-line
+// products (each sheet's A_k recomputed by the Poisson pipeline), the
+// Poisson map (self-adjoint) and rho = g sqrt(g2mu2 / Ny) xi.
+namespace {
+ipg_status backward_inputs(ipg_ctx *c, double *grad_g2mu, double *grad_rho) {
+    auto &A = c->aw;
+    const size_t n = c->n;
+    const int N = c->N, Ny = c->cfg.Ny;
+    if (!A.b1x) {
+        for (C<double> **p : {&A.b1x, &A.b2x, &A.b1y, &A.b2y, &A.vbA, &A.vbB, &A.vcur})
+            IPG_TRY(dalloc(c, p, 9 * n));
+        IPG_TRY(dalloc(c, &A.g2mu_bar, 2 * n));
+        IPG_TRY(dalloc(c, &A.rho_stage, 8 * n));
+    }
+    for (C<double> *p : {A.b1x, A.b2x, A.b1y, A.b2y, A.vbA, A.vbB})
+        IPG_CUDA(c, cudaMemsetAsync(p, 0, 9 * n * sizeof(C<double>), c->stream));
+    IPG_CUDA(c, cudaMemsetAsync(A.g2mu_bar, 0, 2 * n * sizeof(double), c->stream));
+    AdjInitArgs ai;
+    ai.N = N;
+    ai.g = c->cfg.g;
+    ai.u1x = c->u1x;
+    ai.u2x = c->u2x;
+    ai.u1y = c->u1y;
+    ai.u2y = c->u2y;
+    ai.ux = A.cp[0].ux;  // the tau = 0 links kept by ipg_forward
+    ai.uy = A.cp[0].uy;
+    ai.VA = c->VA;
+    ai.VB = c->VB;
+    ai.alpha = c->newton_alpha;
+    ai.adj = A.adj;
+    ai.b1x = A.b1x;
+    ai.b2x = A.b2x;
+    ai.b1y = A.b1y;
+    ai.b2y = A.b2y;
+    ai.vbA = A.vbA;
+    ai.vbB = A.vbB;
+    launch_adjoint_init_links(ai, c->stream);
+    IPG_LAUNCHED(c, 3);
+    for (int nuc = 0; nuc < 2; nuc++) {
+        IPG_CUDA(c, cudaMemcpyAsync(A.vcur, nuc ? c->VB : c->VA, 9 * n * sizeof(C<double>),
+                                    cudaMemcpyDeviceToDevice, c->stream));
+        C<double> *vb = nuc ? A.vbB : A.vbA;
+        WilsonArgs w;
+        w.N = N;
+        w.logN = c->logN;
+        w.Ny = Ny;
+        w.g = c->cfg.g;
+        w.g2mu2 = nuc ? c->g2mu2B : c->g2mu2A;
+        w.xi = nuc ? c->xiB : c->xiA;
+        w.philox_key = c->cfg.seed;
+        w.nucleus = (uint32_t)nuc;
+        w.twiddle = c->twiddle;
+        w.green = c->green;
+        w.amp = c->amp;
+        w.work = c->work;
+        w.V = A.vcur;
+        w.no_product = 1;
+        launch_wilson_amp(w, c->stream);
+        IPG_LAUNCHED(c, 1);
+        for (int k = Ny - 1; k >= 0; k--) {
+            w.rho_in = nullptr;
+            launch_wilson_sheets(w, k, 1, c->stream);  // work = A_k
+            IPG_LAUNCHED(c, 3);
+            launch_adjoint_wilson_sheet(N, c->work, A.vcur, vb, c->stream);  // work = A_bar_k
+            IPG_LAUNCHED(c, 1);
+            w.rho_in = c->work;
+            launch_poisson_sheets(w, 1, c->stream);  // work = rho_bar_k
+            IPG_LAUNCHED(c, 3);
+            w.rho_in = nullptr;
+            launch_adjoint_rho(w, k, A.g2mu_bar + nuc * n, grad_rho ? A.rho_stage : nullptr,
+                               c->stream);
+            IPG_LAUNCHED(c, 1);
+            if (grad_rho)
+                IPG_CUDA(c, cudaMemcpyAsync(grad_rho + ((size_t)nuc * Ny + k) * n * 8,
+                                            A.rho_stage, 8 * n * sizeof(double),
+                                            cudaMemcpyDeviceToHost, c->stream));
+        }
+    }
+    if (grad_g2mu)
+        IPG_CUDA(c, cudaMemcpyAsync(grad_g2mu, A.g2mu_bar, 2 * n * sizeof(double),
+                                    cudaMemcpyDeviceToHost, c->stream));
+    return sync(c);
+}
+}  // namespace
+
+// ===========================================================================
+// Adjoint: forward with checkpoints, reverse sweep with time reversal
+// ===========================================================================
+extern "C" {
+
+ipg_status ipg_forward(ipg_ctx *c, int checkpoint_every, double *E_T, double *eps2) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (!c->initialized || c->half_done || c->finished)
+        return fail(c, IPG_ERR_STATE, "ipg_forward needs the fresh tau = 0 state");
+    if (checkpoint_every < 1) return fail(c, IPG_ERR_BAD_CONFIG, "checkpoint_every < 1");
+    const size_t n = c->n;
+    const int N = c->N;
+    const int S = c->itmax;
+    auto &A = c->aw;
+    const int ncp = (S - 1) / checkpoint_every + 1;
+    auto alloc_state = [&](State<double> &st) -> ipg_status {
+        IPG_TRY(dalloc(c, &st.ux, 9 * n));
+        IPG_TRY(dalloc(c, &st.uy, 9 * n));
+        IPG_TRY(dalloc(c, &st.e1, 8 * n));
+        IPG_TRY(dalloc(c, &st.e2, 8 * n));
+        IPG_TRY(dalloc(c, &st.phi, 9 * n));
+        IPG_TRY(dalloc(c, &st.pi, 9 * n));
+        return IPG_OK;
+    };
+    if (!A.w[0].ux) {
+        for (auto &st : A.w) IPG_TRY(alloc_state(st));
+        IPG_TRY(dalloc(c, &A.adj.ux, 9 * n));
+        IPG_TRY(dalloc(c, &A.adj.uy, 9 * n));
+        IPG_TRY(dalloc(c, &A.adj.e1, 9 * n));
+        IPG_TRY(dalloc(c, &A.adj.e2, 9 * n));
+        IPG_TRY(dalloc(c, &A.adj.phi, 9 * n));
+        IPG_TRY(dalloc(c, &A.adj.pi, 9 * n));
+        IPG_TRY(dalloc(c, &A.tbar, n));
+    }
+    while ((int)A.cp.size() < ncp) {
+        State<double> st{};
+        IPG_TRY(alloc_state(st));
+        A.cp.push_back(st);
+    }
+    A.k = checkpoint_every;
+    A.steps = S;
+    A.ready = false;
+    A.from_inputs = c->init_from_inputs;
+
+    // forward in FP64 from the tau = 0 state (the context's own state is kept)
+    IPG_TRY(copy_state(c, A.w[0], c->s64));
+    State<double> cur = A.w[0];
+    C<double> *ux_b = A.w[1].ux, *uy_b = A.w[1].uy;
+    double *phi_b = A.w[1].phi;
+    for (int s = 0; s < S; s++) {
+        if (s % checkpoint_every == 0) IPG_TRY(copy_state(c, A.cp[s / checkpoint_every], cur));
+        const StepCoef<double> cf = evolution_coef(c, s);
+        launch_leapfrog<double>(c->d_ev, N, cur, ux_b, uy_b, phi_b, cf, false, c->stream);
+        IPG_LAUNCHED(c, 1);
+        std::swap(cur.ux, ux_b);
+        std::swap(cur.uy, uy_b);
+        std::swap(cur.phi, phi_b);
+    }
+    A.fin = cur;
+    TmunuArgs ta;
+    ta.N = N;
+    ta.g = c->cfg.g;
+    ta.tau = S * c->dtau;
+    ta.a = c->a;
+    ta.s = cur;
+    ta.T10 = c->T10;
+    launch_tmunu_diag(ta, c->stream);
+    IPG_LAUNCHED(c, 1);
+    std::vector<double> ttt(n);
+    IPG_CUDA(c, cudaMemcpyAsync(ttt.data(), c->T10, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+    IPG_TRY(sync(c));
+    double sum = 0., S6[6] = {0};
+    for (size_t p = 0; p < n; p++) {
+        sum += ttt[p];
+        const int i = (int)(p / N), j = (int)(p % N);
+        if (!in_ecc_window(N, i, j)) continue;
+        const double w = ttt[p];
+        S6[0] += w;
+        S6[1] += w * i;
+        S6[2] += w * j;
+        S6[3] += w * i * i;
+        S6[4] += w * j * j;
+        S6[5] += w * i * j;
+    }
+    std::memcpy(A.sums, S6, sizeof(S6));
+    A.sum_ttt = sum;
+    const double tau_fm = S * c->dtau * c->a;
+    A.ET = tau_fm * c->a * c->a * kHbarc * sum;
+    A.eps2 = eps2_from_sums(S6, nullptr);
+    A.ready = true;
+    if (E_T) *E_T = A.ET;
+    if (eps2) *eps2 = A.eps2;
+    return IPG_OK;
+}
+
+ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_state,
+                        double *grad_g2mu, double *grad_rho) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    auto &A = c->aw;
+    if (!A.ready) return fail(c, IPG_ERR_STATE, "call ipg_forward first");
+    if ((grad_g2mu || grad_rho) && !A.from_inputs)
+        return fail(c, IPG_ERR_STATE,
+                    "input gradients need a tau = 0 state made by ipg_init_fields");
+    const size_t n = c->n;
+    const int N = c->N;
+    const int S = A.steps;
+    // dL/dTtt_lat per cell: T^tautau in fm^-4 is Ttt_lat / a^4
+    const double a4 = std::pow(c->a, 4.);
+    const double tau_fm = S * c->dtau * c->a;
+    double d6[6];
+    eps2_from_sums(A.sums, d6);
+    std::vector<double> tb(n);
+    for (size_t p = 0; p < n; p++) {
+        const int i = (int)(p / N), j = (int)(p % N);
+        double v = w_ET * tau_fm * c->a * c->a * kHbarc;
+        if (in_ecc_window(N, i, j))
+            v += w_eps2 * (d6[0] + d6[1] * i + d6[2] * j + d6[3] * i * i + d6[4] * j * j +
+                           d6[5] * i * j);
+        tb[p] = v / a4;
+    }
+    IPG_CUDA(c, cudaMemcpyAsync(A.tbar, tb.data(), n * sizeof(double), cudaMemcpyHostToDevice,
+                                c->stream));
+    for (C<double> *b : {A.adj.ux, A.adj.uy, A.adj.e1, A.adj.e2, A.adj.phi, A.adj.pi})
+        IPG_CUDA(c, cudaMemsetAsync(b, 0, 9 * n * sizeof(C<double>), c->stream));
+    launch_adjoint_ttt(N, A.fin, A.tbar, A.adj, c->cfg.g, S * c->dtau, c->stream);
+    IPG_LAUNCHED(c, 1);
+    // reverse sweep: state s from state s+1 by time reversal, or from the
+    // checkpoint when s is a multiple of k; two state sets alternate
+    State<double> sets[2] = {A.w[2], A.fin};
+    State<double> nxt = A.fin;
+    for (int s = S - 1, q = 0; s >= 0; s--, q++) {
+        const State<double> cur = sets[q & 1];
+        const StepCoef<double> cf = evolution_coef(c, s);
+        if (s % A.k == 0)
+            IPG_TRY(copy_state(c, cur, A.cp[s / A.k]));
+        else {
+            launch_inverse_step(N, nxt, cur, cf, c->stream);
+            IPG_LAUNCHED(c, 2);
+        }
+        launch_adjoint_step(N, cur, nxt, A.adj, cf, c->stream);
+        IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
+        nxt = cur;
+    }
+    launch_adjoint_project(n, A.adj, c->stream);
+    IPG_LAUNCHED(c, 1);
+    A.ready = false;  // the reverse sweep overwrote the final state
+    if (grad_state) {
+        std::vector<double> pl(18 * n);
+        const C<double> *bufs[6] = {A.adj.ux, A.adj.uy, A.adj.e1, A.adj.e2, A.adj.phi, A.adj.pi};
+        for (int f = 0; f < 6; f++) {
+            IPG_CUDA(c, cudaMemcpyAsync(pl.data(), bufs[f], 18 * n * sizeof(double),
+                                        cudaMemcpyDeviceToHost, c->stream));
+            IPG_TRY(sync(c));
+            planes_to_sites_m3(pl, n, grad_state + (size_t)f * 18 * n);
+        }
+    }
+    if (grad_g2mu || grad_rho) IPG_TRY(backward_inputs(c, grad_g2mu, grad_rho));
+    IPG_TRY(sync(c));
     return IPG_OK;
 }
 

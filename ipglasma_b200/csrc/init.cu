@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(128) k_newton(NewtonArgs A) {
     double Fzero = 10., FzeroMin = 1e6;
     int iter = 0, nRestart = 0, total = 0;
     uint32_t draws = 0;
-    while (Fzero > 1e-6 && iter < A.max_iter && nRestart < A.max_restart) {
+    while (Fzero > A.tol && iter < A.max_iter && nRestart < A.max_restart) {
         iter++;
         total++;
         Fzero = 0.;
@@ -219,6 +219,8 @@ __global__ void __launch_bounds__(128) k_newton(NewtonArgs A) {
         status = 2;
     }
     st_m3(dir ? A.uy : A.ux, pos, n, Usol);
+    if (A.alpha)
+        for (int a = 0; a < 8; a++) A.alpha[(size_t)a * 2 * n + lid] = alpha[a];
     A.iters[lid] = total;
     A.status[lid] = status;
 }

@@ -75,7 +75,14 @@ struct WilsonArgs {
     const double *green;     // [N*N] Poisson multiplier on the DFT grid
     double2 *work;           // [ns][4][n] complex scratch
     C<double> *V;            // [9][n] Wilson line, updated in place
+    // when set, the row transform reads this packed field ([ns][4][n], colour
+    // 2c in the real and 2c+1 in the imaginary part of channel c) instead of
+    // generating rho (the adjoint runs the self-adjoint Poisson map on it)
+    const double2 *rho_in = nullptr;
+    int no_product = 0;  // transform only, leave V alone
 };
+// Poisson map only (no Wilson-line product) of w.rho_in -> w.work, sheets [0, ns)
+void launch_poisson_sheets(const WilsonArgs &w, int ns, cudaStream_t st);
 void launch_wilson_sheets(const WilsonArgs &w, int k0, int ns,
                           cudaStream_t st);
 // charge amplitude of every site, once per nucleus before its sheets
@@ -98,6 +105,8 @@ struct NewtonArgs {
     C<double> *ux, *uy;  // solutions
     int *iters;          // [2n] iterations used (total over restarts)
     int *status;         // [2n] 0 ok, 1 restarted then converged, 2 failed
+    double tol;          // stop when sum_a |F_a| < tol (reference: 1e-6)
+    double *alpha;       // [8][2n] the solution's exponent (may be null)
 };
 void launch_newton(const NewtonArgs &a, cudaStream_t st);
 
@@ -119,6 +128,44 @@ struct TmunuArgs {
     double *T10;  // [10][n]: tautau xx yy etaeta taux tauy taueta xy xeta yeta
 };
 void launch_tmunu(const TmunuArgs &a, cudaStream_t st);
+// T^tautau, T^xx, T^yy, T^etaeta only
+void launch_tmunu_diag(const TmunuArgs &a, cudaStream_t st);
+
+// ---- adjoint ---------------------------------------------------------------
+// Adjoint buffers of the six fields, 9 complex planes each.
+struct AdjState {
+    C<double> *ux, *uy, *e1, *e2, *phi, *pi;
+};
+// time reversal of one FP64 step: state after (nxt) -> state before (cur)
+void launch_inverse_step(int N, const State<double> &nxt, const State<double> &cur,
+                         const StepCoef<double> &cf, cudaStream_t st);
+// adjoints of a step's outputs -> adjoints of its inputs (in place); cur is the
+// state before the step, nxt the state after it
+void launch_adjoint_step(int N, const State<double> &cur, const State<double> &nxt,
+                         const AdjState &a, const StepCoef<double> &cf, cudaStream_t st);
+// tbar[n] = dL/dTtt (lattice units) -> field adjoints (accumulated)
+void launch_adjoint_ttt(int N, const State<double> &s, const double *tbar, const AdjState &a,
+                        double g, double tau, cudaStream_t st);
+void launch_adjoint_project(size_t n, const AdjState &a, cudaStream_t st);
+// adjoint of the tau = 0 links and pi: pi_bar, U_bar(tau=0) (in adj) ->
+// U1/U2 adjoints b* (initial-pi stencil, then the Newton solve) -> V_A, V_B
+// adjoints vbA, vbB (link products); b* and vb* must start at zero
+struct AdjInitArgs {
+    int N;
+    double g;
+    const C<double> *u1x, *u2x, *u1y, *u2y, *ux, *uy, *VA, *VB;
+    const double *alpha;  // [8][2n] Newton exponents
+    AdjState adj;
+    C<double> *b1x, *b2x, *b1y, *b2y, *vbA, *vbB;
+};
+void launch_adjoint_init_links(const AdjInitArgs &a, cudaStream_t st);
+// one sheet backwards through V_k = exp(-i A_k.t) V_{k-1}; work holds the
+// packed A_k on entry and A_bar_k on return
+void launch_adjoint_wilson_sheet(int N, double2 *work, C<double> *V, C<double> *Vb,
+                                 cudaStream_t st);
+// packed rho_bar of sheet k in w.work -> g2mu2_bar (+=) and rho_bar [n][8]
+void launch_adjoint_rho(const WilsonArgs &w, int k, double *g2mu_bar, double *rho_out,
+                        cudaStream_t st);
 
 struct LandauArgs {
     int N;

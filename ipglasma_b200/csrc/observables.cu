@@ -280,6 +280,11 @@ __global__ void __launch_bounds__(128) k_tmunu_offdiag(TmunuArgs A) {
     }
 }
 
+void launch_tmunu_diag(const TmunuArgs &a, cudaStream_t st) {
+    const size_t n = (size_t)a.N * a.N;
+    k_tmunu_diag<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a);
+}
+
 void launch_tmunu(const TmunuArgs &a, cudaStream_t st) {
     const size_t n = (size_t)a.N * a.N;
     k_tmunu_diag<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a);

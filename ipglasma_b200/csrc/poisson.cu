@@ -110,26 +110,35 @@ __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_fwd(WilsonArgs w, 
     const int s = blockIdx.y, k = k0 + s;
     const size_t row = (size_t)(blockIdx.x * RPB + rl) * N;
     const C<double> *tw = reinterpret_cast<const C<double> *>(w.twiddle);
-    double amp[8], z[8][2];
-#pragma unroll
-    for (int m = 0; m < 8; m++) {
-        const size_t pos = row + t + m * TPS;
-        amp[m] = w.amp[pos];
-        if (w.xi) {
-            // colours 2c, 2c+1 of the site
-            const double2 v =
-                *reinterpret_cast<const double2 *>(w.xi + ((size_t)k * n + pos) * 8 + 2 * c);
-            z[m][0] = v.x;
-            z[m][1] = v.y;
-        } else {
-            // colours 0-3 come from counter half 0, 4-7 from half 1
-            normal2({(uint32_t)pos, (uint32_t)k, (w.nucleus << 1) | (uint32_t)(c >> 1), 0u},
-                    w.philox_key, c & 1, z[m]);
-        }
-    }
     C<double> x[8];
+    if (w.rho_in) {
+        const double2 *in = w.rho_in + ((size_t)s * 4 + c) * n + row + t;
 #pragma unroll
-    for (int m = 0; m < 8; m++) x[m] = {amp[m] * z[m][0], amp[m] * z[m][1]};
+        for (int m = 0; m < 8; m++) {
+            const double2 v = in[m * TPS];
+            x[m] = {v.x, v.y};
+        }
+    } else {
+        double amp[8], z[8][2];
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+            const size_t pos = row + t + m * TPS;
+            amp[m] = w.amp[pos];
+            if (w.xi) {
+                // colours 2c, 2c+1 of the site
+                const double2 v =
+                    *reinterpret_cast<const double2 *>(w.xi + ((size_t)k * n + pos) * 8 + 2 * c);
+                z[m][0] = v.x;
+                z[m][1] = v.y;
+            } else {
+                // colours 0-3 come from counter half 0, 4-7 from half 1
+                normal2({(uint32_t)pos, (uint32_t)k, (w.nucleus << 1) | (uint32_t)(c >> 1), 0u},
+                        w.philox_key, c & 1, z[m]);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < 8; m++) x[m] = {amp[m] * z[m][0], amp[m] * z[m][1]};
+    }
     fft_regs<LOGN, double, false>(x, sm + seq * S, t, tw);
     double2 *out = w.work + ((size_t)s * 4 + c) * n + row + t;
 #pragma unroll
@@ -227,7 +236,12 @@ static void launch_sheets(const WilsonArgs &w, int k0, int ns, cudaStream_t st) 
     k_cols<LOGN><<<dim3(N / JB, 4, ns), col_threads<LOGN>(), col_smem, st>>>(w);
     k_rows_inv<LOGN><<<dim3(N / RPB, ns), row_threads<LOGN>(), row_smem, st>>>(w);
     const size_t n = (size_t)N * N;
-    k_wilson<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
+    if (!w.rho_in && !w.no_product) k_wilson<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
+}
+
+void launch_poisson_sheets(const WilsonArgs &w, int ns, cudaStream_t st) {
+    // launch_sheets skips the Wilson-line product when rho_in is set
+    launch_wilson_sheets(w, 0, ns, st);
 }
 
 void launch_wilson_sheets(const WilsonArgs &w, int k0, int ns, cudaStream_t st) {

@@ -1,0 +1,156 @@
+"""Adjoint of the evolution (ipg_forward / ipg_backward): gradients of E_T and
+of the T^tautau-weighted eps2 with respect to the tau = 0 fields agree with
+central finite differences along random directions, and time reversal between
+checkpoints gives the same gradient as storing every step."""
+import numpy as np
+import pytest
+
+import ipglasma_b200 as ipg
+from ipglasma_b200.synthetic import gaussian_blobs
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = (ipg.UX, ipg.UY, ipg.E1, ipg.E2, ipg.PHI, ipg.PI)
+
+
+def fresh(N=32, L=4.0, maxtime=0.25, seed=3):
+    ev = ipg.Event(ipg.Config(size=N, L=L, Ny=4, maxtime=maxtime, precision=ipg.FP64,
+                              seed=seed))
+    A, B = gaussian_blobs(N, L)
+    ev.set_g2mu(A, B)
+    ev.use_device_noise()
+    ev.init_fields()
+    return ev
+
+
+def herm(m):
+    return 0.5 * (m + np.conj(np.swapaxes(m, -1, -2)))
+
+
+def random_direction(rng, n):
+    d = {}
+    for f in FIELDS:
+        z = rng.standard_normal((n, 3, 3)) + 1j * rng.standard_normal((n, 3, 3))
+        if f in (ipg.E1, ipg.E2, ipg.PHI, ipg.PI):
+            z = herm(z)
+            if f in (ipg.E1, ipg.E2):
+                tr = np.trace(z, axis1=1, axis2=2) / 3.0
+                z = z - tr[:, None, None] * np.eye(3)
+        d[f] = z
+    return d
+
+
+def loss_at(ev, state, direction, h, w):
+    for f in FIELDS:
+        ev.set_field(f, state[f] + h * direction[f])
+    ev.mark_initialized()
+    et, e2 = ev.forward(5)
+    return w[0] * et + w[1] * e2
+
+
+@pytest.fixture(scope="module")
+def setup():
+    ev = fresh()
+    state = {f: ev.get_field(f) for f in FIELDS}
+    yield ev, state
+    ev.close()
+
+
+def test_forward_energy_equals_run():
+    ev = fresh()
+    et, e2 = ev.forward(5)
+    r = ev.run()
+    assert et == pytest.approx(r.E_T, rel=1e-12)
+    assert 0 < e2 < 1
+    ev.close()
+
+
+@pytest.mark.parametrize("w", [(1.0, 0.0), (0.0, 1.0)], ids=["E_T", "eps2"])
+def test_gradient_matches_finite_differences(setup, w):
+    ev, state = setup
+    for f in FIELDS:
+        ev.set_field(f, state[f])
+    ev.mark_initialized()
+    ev.forward(5)
+    grad = ev.backward(*w)
+    rng = np.random.default_rng(11)
+    n = ev.n
+    # the central difference converges as h^2 onto the adjoint value (measured:
+    # relative gap 3e-5 at h = 1e-5, 3e-7 at 1e-6 for eps2); 1e-6 keeps the
+    # truncation and the rounding of the difference both below 1e-6
+    h = 1e-6
+    for _ in range(3):
+        d = random_direction(rng, n)
+        directional = sum(float(np.sum((np.conj(grad[f]) * d[f]).real)) for f in FIELDS)
+        fd = (loss_at(ev, state, d, h, w) - loss_at(ev, state, d, -h, w)) / (2 * h)
+        assert directional == pytest.approx(fd, rel=2e-6, abs=1e-9 * max(1.0, abs(fd))), \
+            (directional, fd)
+
+
+def test_time_reversal_matches_stored_steps(setup):
+    ev, state = setup
+    out = []
+    for k in (1, 1000):
+        for f in FIELDS:
+            ev.set_field(f, state[f])
+        ev.mark_initialized()
+        ev.forward(k)
+        out.append(ev.backward(1.0, 0.5))
+    for f in FIELDS:
+        a, b = out[0][f], out[1][f]
+        scale = max(np.abs(a).max(), 1e-300)
+        assert np.abs(a - b).max() <= 1e-8 * scale, f
+
+
+# ---- through the initial conditions: g2mu and rho ---------------------------
+
+def input_event(N=32, L=4.0, Ny=4, maxtime=0.25):
+    ev = ipg.Event(ipg.Config(size=N, L=L, Ny=Ny, maxtime=maxtime, precision=ipg.FP64,
+                              seed=5, newton_tolerance=1e-13))
+    A, B = gaussian_blobs(N, L)
+    rng = np.random.default_rng(2)
+    xi = rng.standard_normal((2, Ny, N * N, 8))
+    return ev, A, B, xi
+
+
+def input_loss(ev, A, B, xi, w):
+    ev.set_g2mu(A, B)
+    ev.set_noise(xi[0], xi[1])
+    rep = ev.init_fields()
+    assert rep.newton_restarted == 0 and rep.newton_failed == 0
+    et, e2 = ev.forward(5)
+    return w[0] * et + w[1] * e2
+
+
+@pytest.mark.parametrize("w", [(1.0, 0.0), (0.0, 1.0)], ids=["E_T", "eps2"])
+def test_input_gradients_match_finite_differences(w):
+    ev, A, B, xi = input_event()
+    input_loss(ev, A, B, xi, w)
+    g = ev.backward(*w, inputs=True, rho=True)
+    rng = np.random.default_rng(17)
+    h = 3e-6
+    # g2mu of nucleus A and B: relative perturbations
+    dA = A * rng.uniform(-1, 1, A.shape)
+    dB = B * rng.uniform(-1, 1, B.shape)
+    directional = float(np.sum(g["g2mu"][0] * dA) + np.sum(g["g2mu"][1] * dB))
+    fd = (input_loss(ev, A + h * dA, B + h * dB, xi, w)
+          - input_loss(ev, A - h * dA, B - h * dB, xi, w)) / (2 * h)
+    assert directional == pytest.approx(fd, rel=5e-5), ("g2mu", directional, fd)
+    # the noise: rho = g sqrt(g2mu/Ny) xi, so d rho = amp d xi
+    dxi = rng.standard_normal(xi.shape)
+    amp = np.stack([2.0 * np.sqrt(A / xi.shape[1]), 2.0 * np.sqrt(B / xi.shape[1])])
+    directional = float(np.sum(g["rho"] * amp[:, None, :, None] * dxi))
+    fd = (input_loss(ev, A, B, xi + h * dxi, w) - input_loss(ev, A, B, xi - h * dxi, w)) / (2 * h)
+    assert directional == pytest.approx(fd, rel=5e-5), ("rho", directional, fd)
+    ev.close()
+
+
+def test_input_gradients_need_initial_conditions():
+    ev = fresh()
+    for f in FIELDS:
+        ev.set_field(f, ev.get_field(f))
+    ev.mark_initialized()
+    ev.forward(5)
+    with pytest.raises(ipg.IPGError):
+        ev.backward(1.0, 0.0, inputs=True)
+    ev.close()
