@@ -182,6 +182,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched uneven-events measurement")
+    ap.add_argument("--no-adjoint", action="store_true",
+                    help="skip the adjoint (forward/backward) measurement")
     ap.add_argument("--profile", choices=["fp32", "fp64", "both"], default=None,
                     help="run one warm-up and one timed event per form and exit "
                          "(the command profiled under ncu)")
@@ -287,6 +289,7 @@ def run_ours(args, world, rank, local):
                             "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp64"]}}
 
     batched = None if args.no_batched else measure_batched(torch, ipg, rank, dist)
+    adjoint = None if args.no_adjoint else measure_adjoint(torch, ipg, rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -321,6 +324,7 @@ def run_ours(args, world, rank, local):
                     "form": "fp32"},
             "roofline": roof,
             "batched": batched,
+            "adjoint": adjoint,
             "cpu_baseline": cpu,
             "gpu_launches": int(launches_timed),
             "clocks": clk.summary(),
@@ -399,6 +403,67 @@ def measure_batched(torch, ipg, rank, dist):
                             "candidates": tune.candidates},
             "timing": "CUDA events around init of all events + batched run, mean of "
                       f"{BATCH['reps']}; total batched launches {launches}"}
+
+
+ADJ = dict(N=256, L=30.0, nucleus="Au", b=2.0, Ny=50, steps=400, dtau=0.1, checkpoint=20)
+
+
+def measure_adjoint(torch, ipg, rank):
+    """Adjoint of one Au+Au event at 256^2 (L = 30 fm, b = 2 fm, Ny = 50),
+    400 leapfrog steps at dtau = 0.1 a with a checkpoint every 20 steps: the
+    gradient of E_T + eps2 with respect to the g2mu maps (2 x 256^2) and rho
+    (2 x 50 x 8 x 256^2). Forward = initial conditions (Newton to 1e-12) +
+    ipg_forward; adjoint = ipg_backward through the evolution and the initial
+    conditions."""
+    from ipglasma_b200.synthetic import make_event
+    w = ADJ
+    a = w["L"] / w["N"]
+    maxtime = w["steps"] * w["dtau"] * a
+    A, B, _, _ = make_event(w["N"], w["L"], w["nucleus"], w["b"], 8000 + rank)
+    ev = ipg.Event(ipg.Config(size=w["N"], L=w["L"], Ny=w["Ny"], maxtime=maxtime,
+                              dtau=w["dtau"], precision=ipg.FP64, seed=8100 + rank,
+                              newton_tolerance=1e-12))
+    ev.set_g2mu(A, B)
+    ev.use_device_noise()
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        st = torch.cuda.Event(enable_timing=True)
+        en = torch.cuda.Event(enable_timing=True)
+        st.record()
+        out = fn()
+        en.record()
+        torch.cuda.synchronize()
+        return out, st.elapsed_time(en)
+
+    def forward():
+        ev.init_fields(allow_nonconverged=True)
+        return ev.forward(w["checkpoint"])
+
+    forward()
+    ev.backward(1.0, 1.0, inputs=True, rho=True)  # warm-up
+    (et, e2), ms_f = timed(forward)
+    g, ms_b = timed(lambda: ev.backward(1.0, 1.0, inputs=True, rho=True))
+    dev_f, dev_b = ev.adjoint_stats()
+    _, ms_plain = timed(lambda: (ev.init_fields(allow_nonconverged=True), ev.run()))
+    steps = ev.itmax
+    support = np.concatenate([A, B]) > 1e-6 * max(A.max(), B.max())
+    ev.close()
+    return {"workload": f"Au+Au 256^2, L 30 fm, Ny 50, {steps} steps, checkpoint every "
+                        f"{w['checkpoint']}, FP64",
+            "loss": "E_T + eps2 (T^tautau-weighted)", "E_T": et, "eps2": e2,
+            "device_ms_forward_evolution": round(dev_f, 2),
+            "device_ms_backward": round(dev_b, 2),
+            "adjoint_over_forward": round(dev_b / dev_f, 3),
+            "e2e_ms_forward": round(ms_f, 2), "e2e_ms_backward": round(ms_b, 2),
+            "e2e_adjoint_over_forward": round(ms_b / ms_f, 3),
+            "ms_plain_event": round(ms_plain, 2),
+            "grad_g2mu_norm_on_support": float(np.linalg.norm(g["g2mu"].ravel()[support])),
+            "grad_rho_norm": float(np.linalg.norm(g["rho"])),
+            "timing": "device: CUDA events inside the library (forward: evolution + "
+                      "checkpoints + T^tautau; backward: reverse sweep + initial-condition "
+                      "adjoint). e2e: CUDA events around the API calls, forward including the "
+                      "initial conditions, backward including the 420 MB grad_rho copy"}
 
 
 def compare_forms(ev32, ev64, d_A, d_B, seed):

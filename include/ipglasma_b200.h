@@ -243,6 +243,10 @@ ipg_status ipg_output_names(int event_id, int it, double dtau, double a,
 ipg_status ipg_forward(ipg_ctx *ctx, int checkpoint_every, double *E_T, double *eps2);
 ipg_status ipg_backward(ipg_ctx *ctx, double w_ET, double w_eps2, double *grad_state,
                         double *grad_g2mu, double *grad_rho);
+/* Device time of the last ipg_forward (evolution, checkpoints, T^tautau) and
+ * ipg_backward (reverse sweep and initial-condition adjoint, without the
+ * copies of the gradients to the host). */
+ipg_status ipg_adjoint_stats(const ipg_ctx *ctx, double *ms_forward, double *ms_backward);
 
 /* ---- batches of events -------------------------------------------------
  * The reference runs one event per process (main.cpp:347-359, events handed

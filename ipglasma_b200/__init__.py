@@ -115,6 +115,8 @@ _SIGNATURES = {
                                ct.POINTER(ct.c_double)]),
     "ipg_backward": (ct.c_int, [ct.c_void_p, ct.c_double, ct.c_double, ct.c_void_p, ct.c_void_p,
                                 ct.c_void_p]),
+    "ipg_adjoint_stats": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double),
+                                     ct.POINTER(ct.c_double)]),
     "ipg_batch_last_error": (ct.c_char_p, [ct.c_void_p]),
     "ipg_batch_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.c_int, ct.POINTER(ct.c_void_p)]),
     "ipg_batch_destroy": (ct.c_int, [ct.c_void_p]),
@@ -337,6 +339,12 @@ class Event:
         et, e2 = ct.c_double(), ct.c_double()
         self._check(self._lib.ipg_forward(self._h, checkpoint_every, ct.byref(et), ct.byref(e2)))
         return et.value, e2.value
+
+    def adjoint_stats(self):
+        """Device ms of the last forward and backward."""
+        f, b = ct.c_double(), ct.c_double()
+        self._check(self._lib.ipg_adjoint_stats(self._h, ct.byref(f), ct.byref(b)))
+        return f.value, b.value
 
     def backward(self, w_ET: float = 1.0, w_eps2: float = 0.0, inputs: bool = False,
                  rho: bool = False):

@@ -17,8 +17,9 @@
 //   S_u: phi' = phi + c2 pi',   U_d' = T2(i c E_d') U_d,  T2(X) = 1 + X + X^2/2
 // with cst = tau dtau / (2 g^2), cdt = dtau / tau, c = g^2 dtau / (tau + dtau/2),
 // c2 = (tau + dtau/2) dtau. Its vector-Jacobian product is k_adj_su (local)
-// followed by k_adj_se (scatters into neighbouring links and phi with FP64
-// atomics, so the summation order, not the result, varies between runs).
+// followed by k_adj_se_links and k_adj_se_phi (they scatter into neighbouring
+// links and phi with FP64 atomics, so the summation order, not the result,
+// varies between runs).
 // The step is inverted exactly in exact arithmetic (k_inv_su, k_inv_se): this
 // is the time reversal used to walk back between checkpoints.
 #include <cstdint>
@@ -267,29 +268,26 @@ __global__ void k_adj_su(int N, State<double> cur, State<double> nxt, AdjState a
         // X_bar = M_bar + (M_bar X^dag + X^dag M_bar) / 2
         Md Xb = Mb;
         add_to(Xb, sc(addm(mul_nd(Mb, X), mul_dn(X, Mb)), 0.5));
-        // X = i c E  ->  E_bar += Herm(-i c X_bar)
+        // X = i c E  ->  E_bar += Herm(-i c X_bar); stored traceless Hermitian,
+        // which is also the adjoint of E before S_e (E' = TL(E + ...))
         Md Eb_ = ld_adj(Eb, pos, n);
         add_to(Eb_, herm(times_i(Xb, -c)));
-        st_m3(Eb, pos, n, Eb_);
+        st_m3(Eb, pos, n, tl(herm(Eb_)));
     }
 }
 
-// S_e: adjoints of E' and pi' (own site) -> adjoints of E (own), and atomic
-// contributions to the link and phi adjoints of the site and its neighbours.
-__global__ void k_adj_se(int N, State<double> cur, AdjState a, double cst, double cdt) {
+// S_e, link part: the adjoints G_d of E_d' (traceless Hermitian, from
+// k_adj_su) through the plaquette and staple terms into the link adjoints
+// of the site and its neighbours (atomic)
+__global__ void __launch_bounds__(128) k_adj_se_links(int N, State<double> cur, AdjState a,
+                                                      double cst) {
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
     const StepGeom G = step_geom(N, (int)(pos / N), (int)(pos % N));
-    const Md G1 = tl(herm(ld_adj(a.e1, pos, n)));
-    const Md G2 = tl(herm(ld_adj(a.e2, pos, n)));
-    st_m3(a.e1, pos, n, G1);
-    st_m3(a.e2, pos, n, G2);
-    const Md pib = herm(ld_adj(a.pi, pos, n));
-
+    const Md t1b = sc(ld_adj(a.e1, pos, n), cst), t2b = sc(ld_adj(a.e2, pos, n), cst);
     const Md ux = ld_m3(cur.ux, pos, n), uy = ld_m3(cur.uy, pos, n);
-    const Md t1b = sc(G1, cst), t2b = sc(G2, cst);
-    Md uxb = {}, uyb = {}, phib = {};
+    Md uxb = {}, uyb = {};
     // plaquette h12 = iAH(a b^dag), a = Ux Uy(+x), b = Uy Ux(+y); enters E1 (+), E2 (-)
     {
         const Md uy_px = ld_m3(cur.uy, G.pX, n), ux_py = ld_m3(cur.ux, G.pY, n);
@@ -325,43 +323,40 @@ __global__ void k_adj_se(int N, State<double> cur, AdjState a, double cst, doubl
         atomic_add_m(a.uy, G.mX, n, mul_nd(ux_mx, Qb));
         atomic_add_m(a.ux, G.mX, n, mul(uy_mx, Qb));
     }
-    // transports of phi: commutator terms of E and the pi bracket
-    const Md phi = ld_herm(cur.phi, pos, n);
-    const Md brb = sc(pib, cdt);
-    add_to(phib, sc(brb, -4.));
-    {
-        const Md f = ld_herm(cur.phi, G.pX, n);
-        const Md phx = mul_nd(mul(ux, f), ux);
-        const Md Cb = sc(G1, cdt);
-        Md phxb = icomm(phi, Cb);
-        add_to(phib, icomm(Cb, phx));
-        add_to(phxb, brb);
-        add_to(uxb, sc(mul(mul(phxb, ux), f), 2.));
-        atomic_add_m(a.phi, G.pX, n, mul(mul_dn(ux, phxb), ux));
-    }
-    {
-        const Md f = ld_herm(cur.phi, G.pY, n);
-        const Md phy = mul_nd(mul(uy, f), uy);
-        const Md Cb = sc(G2, cdt);
-        Md phyb = icomm(phi, Cb);
-        add_to(phib, icomm(Cb, phy));
-        add_to(phyb, brb);
-        add_to(uyb, sc(mul(mul(phyb, uy), f), 2.));
-        atomic_add_m(a.phi, G.pY, n, mul(mul_dn(uy, phyb), uy));
-    }
-    {
-        // U(-x)^dag phi(-x) U(-x): U_bar += 2 phi U C_bar, phi_bar += U C_bar U^dag
-        const Md u = ld_m3(cur.ux, G.mX, n), f = ld_herm(cur.phi, G.mX, n);
-        atomic_add_m(a.ux, G.mX, n, sc(mul(mul(f, u), brb), 2.));
-        atomic_add_m(a.phi, G.mX, n, mul_nd(mul(u, brb), u));
-    }
-    {
-        const Md u = ld_m3(cur.uy, G.mY, n), f = ld_herm(cur.phi, G.mY, n);
-        atomic_add_m(a.uy, G.mY, n, sc(mul(mul(f, u), brb), 2.));
-        atomic_add_m(a.phi, G.mY, n, mul_nd(mul(u, brb), u));
-    }
     atomic_add_m(a.ux, pos, n, uxb);
     atomic_add_m(a.uy, pos, n, uyb);
+}
+
+// S_e, transport part: the commutator terms of E and the pi bracket into the
+// phi and link adjoints (atomic)
+__global__ void __launch_bounds__(128) k_adj_se_phi(int N, State<double> cur, AdjState a,
+                                                    double cdt) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    const StepGeom G = step_geom(N, (int)(pos / N), (int)(pos % N));
+    const Md phi = ld_herm(cur.phi, pos, n);
+    const Md brb = sc(ld_adj(a.pi, pos, n), cdt);
+    Md phib = sc(brb, -4.);
+    for (int d = 0; d < 2; d++) {
+        const size_t q = d ? G.pY : G.pX;
+        const Md u = ld_m3(d ? cur.uy : cur.ux, pos, n);
+        const Md f = ld_herm(cur.phi, q, n);
+        const Md ph = mul_nd(mul(u, f), u);
+        const Md Cb = sc(ld_adj(d ? a.e2 : a.e1, pos, n), cdt);
+        Md phb = icomm(phi, Cb);
+        add_to(phib, icomm(Cb, ph));
+        add_to(phb, brb);
+        atomic_add_m(d ? a.uy : a.ux, pos, n, sc(mul(mul(phb, u), f), 2.));
+        atomic_add_m(a.phi, q, n, mul(mul_dn(u, phb), u));
+    }
+    for (int d = 0; d < 2; d++) {
+        // U(-d)^dag phi(-d) U(-d): U_bar += 2 phi U C_bar, phi_bar += U C_bar U^dag
+        const size_t q = d ? G.mY : G.mX;
+        const Md u = ld_m3(d ? cur.uy : cur.ux, q, n), f = ld_herm(cur.phi, q, n);
+        atomic_add_m(d ? a.uy : a.ux, q, n, sc(mul(mul(f, u), brb), 2.));
+        atomic_add_m(a.phi, q, n, mul_nd(mul(u, brb), u));
+    }
     atomic_add_m(a.phi, pos, n, phib);
 }
 
@@ -692,7 +687,8 @@ void launch_adjoint_step(int N, const State<double> &cur, const State<double> &n
     if (cf.do_pe) {
         const double cst = cf.tau * cf.dt_pe / (2. * cf.g * cf.g);
         const double cdt = cf.dt_pe / cf.tau;
-        k_adj_se<<<blocks(n), 128, 0, st>>>(N, cur, a, cst, cdt);
+        k_adj_se_links<<<blocks(n), 128, 0, st>>>(N, cur, a, cst);
+        k_adj_se_phi<<<blocks(n), 128, 0, st>>>(N, cur, a, cdt);
     }
 }
 
@@ -704,6 +700,22 @@ void launch_adjoint_ttt(int N, const State<double> &s, const double *tbar, const
 
 void launch_adjoint_project(size_t n, const AdjState &a, cudaStream_t st) {
     k_adj_project<<<blocks(n), 128, 0, st>>>(n, a);
+}
+
+// [9 complex planes][n] -> per site 18 doubles, for the host copy
+__global__ void k_planes_to_sites(size_t n, const C<double> *src, double *dst) {
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const C<double> v = src[k * n + pos];
+        dst[18 * pos + 2 * k] = v.r;
+        dst[18 * pos + 2 * k + 1] = v.i;
+    }
+}
+
+void launch_planes_to_sites(size_t n, const C<double> *src, double *dst, cudaStream_t st) {
+    k_planes_to_sites<<<blocks(n), 128, 0, st>>>(n, src, dst);
 }
 
 void launch_adjoint_init_links(const AdjInitArgs &A, cudaStream_t st) {

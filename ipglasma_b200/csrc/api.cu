@@ -86,11 +86,14 @@ struct ipg_ctx {
         bool ready = false;
         double sums[6] = {0};            // W, X, Y, Sxx, Syy, Sxy of the weight
         double sum_ttt = 0, ET = 0, eps2 = 0;
+        double ms_forward = 0, ms_backward = 0;  // device time of the last pair
+        double *sites = nullptr;                 // [n][18] staging for the host copy
         bool from_inputs = false;  // the tau = 0 state came from g2mu + noise
         // initial-condition adjoint: U1/U2 adjoints, V adjoints, a V copy
         C<double> *b1x = nullptr, *b2x = nullptr, *b1y = nullptr, *b2y = nullptr;
         C<double> *vbA = nullptr, *vbB = nullptr, *vcur = nullptr;
-        double *g2mu_bar = nullptr, *rho_stage = nullptr;
+        double *g2mu_bar = nullptr;
+        double *rho_all = nullptr;  // [2][Ny][n][8] rho adjoint, kept on the device
     } aw;
     bool init_from_inputs = false;
 
@@ -323,7 +326,9 @@ StepCoef<double> evolution_coef(const ipg_ctx *c, int s) {
 }
 
 // T^tautau-weighted eccentricity over the cells [2, N-2)^2 (the cells the
-// reference's eccentricity sums over) with the weighted centroid as origin:
+// reference's eccentricity sums over) with the weighted centroid as origin (a
+// smooth weight: a clamp such as max(T^tautau, 0) would put a kink where
+// vacuum cells sit at T^tautau = 0):
 // eps2 = |sum w (x~ + i y~)^2| / sum w (x~^2 + y~^2), from the weight sums
 // W, X = sum w x, Y, Sxx = sum w x^2, Syy, Sxy; d[6] receives d eps2 / d sums.
 double eps2_from_sums(const double *S, double *d) {
@@ -932,8 +937,8 @@ ipg_status backward_inputs(ipg_ctx *c, double *grad_g2mu, double *grad_rho) {
         for (C<double> **p : {&A.b1x, &A.b2x, &A.b1y, &A.b2y, &A.vbA, &A.vbB, &A.vcur})
             IPG_TRY(dalloc(c, p, 9 * n));
         IPG_TRY(dalloc(c, &A.g2mu_bar, 2 * n));
-        IPG_TRY(dalloc(c, &A.rho_stage, 8 * n));
     }
+    if (grad_rho && !A.rho_all) IPG_TRY(dalloc(c, &A.rho_all, 16 * (size_t)Ny * n));
     for (C<double> *p : {A.b1x, A.b2x, A.b1y, A.b2y, A.vbA, A.vbB})
         IPG_CUDA(c, cudaMemsetAsync(p, 0, 9 * n * sizeof(C<double>), c->stream));
     IPG_CUDA(c, cudaMemsetAsync(A.g2mu_bar, 0, 2 * n * sizeof(double), c->stream));
@@ -989,19 +994,13 @@ ipg_status backward_inputs(ipg_ctx *c, double *grad_g2mu, double *grad_rho) {
             launch_poisson_sheets(w, 1, c->stream);  // work = rho_bar_k
             IPG_LAUNCHED(c, 3);
             w.rho_in = nullptr;
-            launch_adjoint_rho(w, k, A.g2mu_bar + nuc * n, grad_rho ? A.rho_stage : nullptr,
+            launch_adjoint_rho(w, k, A.g2mu_bar + nuc * n,
+                               grad_rho ? A.rho_all + ((size_t)nuc * Ny + k) * n * 8 : nullptr,
                                c->stream);
             IPG_LAUNCHED(c, 1);
-            if (grad_rho)
-                IPG_CUDA(c, cudaMemcpyAsync(grad_rho + ((size_t)nuc * Ny + k) * n * 8,
-                                            A.rho_stage, 8 * n * sizeof(double),
-                                            cudaMemcpyDeviceToHost, c->stream));
         }
     }
-    if (grad_g2mu)
-        IPG_CUDA(c, cudaMemcpyAsync(grad_g2mu, A.g2mu_bar, 2 * n * sizeof(double),
-                                    cudaMemcpyDeviceToHost, c->stream));
-    return sync(c);
+    return IPG_OK;
 }
 }  // namespace
 
@@ -1050,6 +1049,7 @@ ipg_status ipg_forward(ipg_ctx *c, int checkpoint_every, double *E_T, double *ep
     A.from_inputs = c->init_from_inputs;
 
     // forward in FP64 from the tau = 0 state (the context's own state is kept)
+    IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     IPG_TRY(copy_state(c, A.w[0], c->s64));
     State<double> cur = A.w[0];
     C<double> *ux_b = A.w[1].ux, *uy_b = A.w[1].uy;
@@ -1073,10 +1073,12 @@ ipg_status ipg_forward(ipg_ctx *c, int checkpoint_every, double *E_T, double *ep
     ta.T10 = c->T10;
     launch_tmunu_diag(ta, c->stream);
     IPG_LAUNCHED(c, 1);
+    IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     std::vector<double> ttt(n);
     IPG_CUDA(c, cudaMemcpyAsync(ttt.data(), c->T10, n * sizeof(double), cudaMemcpyDeviceToHost,
                                 c->stream));
     IPG_TRY(sync(c));
+    A.ms_forward = elapsed(c);
     double sum = 0., S6[6] = {0};
     for (size_t p = 0; p < n; p++) {
         sum += ttt[p];
@@ -1098,6 +1100,13 @@ ipg_status ipg_forward(ipg_ctx *c, int checkpoint_every, double *E_T, double *ep
     A.ready = true;
     if (E_T) *E_T = A.ET;
     if (eps2) *eps2 = A.eps2;
+    return IPG_OK;
+}
+
+ipg_status ipg_adjoint_stats(const ipg_ctx *c, double *ms_forward, double *ms_backward) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (ms_forward) *ms_forward = c->aw.ms_forward;
+    if (ms_backward) *ms_backward = c->aw.ms_backward;
     return IPG_OK;
 }
 
@@ -1128,6 +1137,7 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
     }
     IPG_CUDA(c, cudaMemcpyAsync(A.tbar, tb.data(), n * sizeof(double), cudaMemcpyHostToDevice,
                                 c->stream));
+    IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     for (C<double> *b : {A.adj.ux, A.adj.uy, A.adj.e1, A.adj.e2, A.adj.phi, A.adj.pi})
         IPG_CUDA(c, cudaMemsetAsync(b, 0, 9 * n * sizeof(C<double>), c->stream));
     launch_adjoint_ttt(N, A.fin, A.tbar, A.adj, c->cfg.g, S * c->dtau, c->stream);
@@ -1146,23 +1156,33 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
             IPG_LAUNCHED(c, 2);
         }
         launch_adjoint_step(N, cur, nxt, A.adj, cf, c->stream);
-        IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
+        IPG_LAUNCHED(c, cf.do_pe ? 3 : 1);
         nxt = cur;
     }
     launch_adjoint_project(n, A.adj, c->stream);
     IPG_LAUNCHED(c, 1);
     A.ready = false;  // the reverse sweep overwrote the final state
+    if (grad_g2mu || grad_rho) IPG_TRY(backward_inputs(c, grad_g2mu, grad_rho));
+    IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    IPG_TRY(sync(c));
+    A.ms_backward = elapsed(c);
+    if (grad_g2mu)
+        IPG_CUDA(c, cudaMemcpy(grad_g2mu, A.g2mu_bar, 2 * n * sizeof(double),
+                               cudaMemcpyDeviceToHost));
+    if (grad_rho)
+        IPG_CUDA(c, cudaMemcpy(grad_rho, A.rho_all, 16 * (size_t)c->cfg.Ny * n * sizeof(double),
+                               cudaMemcpyDeviceToHost));
     if (grad_state) {
-        std::vector<double> pl(18 * n);
+        if (!A.sites) IPG_TRY(dalloc(c, &A.sites, 18 * n));
         const C<double> *bufs[6] = {A.adj.ux, A.adj.uy, A.adj.e1, A.adj.e2, A.adj.phi, A.adj.pi};
         for (int f = 0; f < 6; f++) {
-            IPG_CUDA(c, cudaMemcpyAsync(pl.data(), bufs[f], 18 * n * sizeof(double),
-                                        cudaMemcpyDeviceToHost, c->stream));
-            IPG_TRY(sync(c));
-            planes_to_sites_m3(pl, n, grad_state + (size_t)f * 18 * n);
+            launch_planes_to_sites(n, bufs[f], A.sites, c->stream);
+            IPG_LAUNCHED(c, 1);
+            IPG_CUDA(c, cudaMemcpyAsync(grad_state + (size_t)f * 18 * n, A.sites,
+                                        18 * n * sizeof(double), cudaMemcpyDeviceToHost,
+                                        c->stream));
         }
     }
-    if (grad_g2mu || grad_rho) IPG_TRY(backward_inputs(c, grad_g2mu, grad_rho));
     IPG_TRY(sync(c));
     return IPG_OK;
 }

@@ -147,6 +147,8 @@ void launch_adjoint_step(int N, const State<double> &cur, const State<double> &n
 void launch_adjoint_ttt(int N, const State<double> &s, const double *tbar, const AdjState &a,
                         double g, double tau, cudaStream_t st);
 void launch_adjoint_project(size_t n, const AdjState &a, cudaStream_t st);
+// [9 complex planes][n] -> [n][18] doubles
+void launch_planes_to_sites(size_t n, const C<double> *src, double *dst, cudaStream_t st);
 // adjoint of the tau = 0 links and pi: pi_bar, U_bar(tau=0) (in adj) ->
 // U1/U2 adjoints b* (initial-pi stencil, then the Newton solve) -> V_A, V_B
 // adjoints vbA, vbB (link products); b* and vb* must start at zero
