@@ -60,6 +60,9 @@ __device__ __forceinline__ void expm_coeff(const double Q[8], C<double> u[9]) {
     sincos(w, &sw, &cosw);
     const double xi0 = sw / w;
     const double den = 9. * uu * uu - w * w;
+    // one reciprocal for the three f's (a NaN or infinity from den = 0
+    // propagates as with three divisions and is zeroed below)
+    const double rden = 1. / den;
     // e^{-iu} directly, e^{2iu} by the double-angle identities
     double su, cu;
     sincos(uu, &su, &cu);
@@ -70,25 +73,27 @@ __device__ __forceinline__ void expm_coeff(const double Q[8], C<double> u[9]) {
     {
         C<double> inner = {8. * uu * uu * cosw, 2. * uu * xi0 * (3. * uu * uu + w * w)};
         C<double> t = cmul(expmiu, inner);
-        f0 = {(uu * uu - w * w) * exp2iu.r + t.r, (uu * uu - w * w) * exp2iu.i + t.i};
-        f0 = cdiv_real(f0, den);
+        f0 = {((uu * uu - w * w) * exp2iu.r + t.r) * rden,
+              ((uu * uu - w * w) * exp2iu.i + t.i) * rden};
     }
     {
         // f1 = 2u e^{2iu} - e^{-iu} (2u cos w - i (3u^2 - w^2) xi0)
         C<double> inner = {2. * uu * cosw, -(3. * uu * uu - w * w) * xi0};
         C<double> t = cmul(expmiu, inner);
-        f1 = {2. * uu * exp2iu.r - t.r, 2. * uu * exp2iu.i - t.i};
-        f1 = cdiv_real(f1, den);
+        f1 = {(2. * uu * exp2iu.r - t.r) * rden, (2. * uu * exp2iu.i - t.i) * rden};
     }
     {
         // f2 = e^{2iu} - e^{-iu} (cos w + 3 i u xi0)
         C<double> inner = {cosw, 3. * uu * xi0};
         C<double> t = cmul(expmiu, inner);
-        f2 = {exp2iu.r - t.r, exp2iu.i - t.i};
-        f2 = cdiv_real(f2, den);
+        f2 = {(exp2iu.r - t.r) * rden, (exp2iu.i - t.i) * rden};
     }
     C<double> u0 = {f0.r + 2. / 3. * c1 * f2.r, f0.i + 2. / 3. * c1 * f2.i};
-    f1 = cdiv(f1, {0.5 * f2.r, 0.5 * f2.i});
+    // f1 / (f2 / 2) = f1 conj(f2) * 2 / |f2|^2
+    {
+        const double r2 = 2. / (f2.r * f2.r + f2.i * f2.i);
+        f1 = {(f1.r * f2.r + f1.i * f2.i) * r2, (f1.i * f2.r - f1.r * f2.i) * r2};
+    }
     double lin[8];
     lin[0] = Q[3] * Q[5] + Q[4] * Q[6] + 2. / sqrt3 * Q[0] * Q[7];
     lin[1] = 2. * Q[1] * Q[7] / sqrt3 - Q[3] * Q[6] + Q[4] * Q[5];

@@ -63,16 +63,21 @@ __device__ __forceinline__ void normal4(U4 ctr, uint64_t key, double out[4]) {
     out[3] = rad2 * s2;
 }
 
-// one Box-Muller pair of normal4 for the same counter: half 0 gives out[0..1],
-// half 1 gives out[2..3], with the same operations and so the same values
-__device__ __forceinline__ void normal2(U4 ctr, uint64_t key, int half, double out[2]) {
-    const U4 r = philox4x32_10(ctr, (uint32_t)key, (uint32_t)(key >> 32));
-    const uint32_t a = half ? r.z : r.x, b = half ? r.w : r.y;
+// the Box-Muller pair of normal4 made from the words (a, b): (r.x, r.y) give
+// out[0..1] of normal4, (r.z, r.w) give out[2..3], with the same operations
+__device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, double out[2]) {
     const float rad = sqrtf(-2.0f * logf(u01f(a)));
     float s, c;
     sincospif(2.0f * u01f(b), &s, &c);
     out[0] = rad * c;
     out[1] = rad * s;
+}
+
+// one Box-Muller pair of normal4 for the same counter: half 0 gives out[0..1],
+// half 1 gives out[2..3], with the same values
+__device__ __forceinline__ void normal2(U4 ctr, uint64_t key, int half, double out[2]) {
+    const U4 r = philox4x32_10(ctr, (uint32_t)key, (uint32_t)(key >> 32));
+    box_muller(half ? r.z : r.x, half ? r.w : r.y, out);
 }
 
 }  // namespace ipg

@@ -105,8 +105,12 @@ __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_fwd(WilsonArgs w, 
     extern __shared__ __align__(16) unsigned char smraw[];
     C<double> *sm = reinterpret_cast<C<double> *>(smraw);
     const size_t n = (size_t)N * N;
-    const int seq = threadIdx.x / TPS, t = threadIdx.x - seq * TPS;
-    const int rl = seq >> 2, c = seq & 3;
+    // lanes 2i and 2i+1 hold channels 2h and 2h+1 of the same points (they
+    // share one Philox counter); TPS >= 1 sequences of N/8 threads each
+    const int half = threadIdx.x & 1, rest = threadIdx.x >> 1;
+    const int t = rest % TPS, pair = rest / TPS;  // pair = 2 rl + h
+    const int rl = pair >> 1, c = ((pair & 1) << 1) | half;
+    const int seq = 4 * rl + c;
     const int s = blockIdx.y, k = k0 + s;
     const size_t row = (size_t)(blockIdx.x * RPB + rl) * N;
     const C<double> *tw = reinterpret_cast<const C<double> *>(w.twiddle);
@@ -121,20 +125,43 @@ __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_fwd(WilsonArgs w, 
     } else {
         double amp[8], z[8][2];
 #pragma unroll
-        for (int m = 0; m < 8; m++) {
-            const size_t pos = row + t + m * TPS;
-            amp[m] = w.amp[pos];
-            if (w.xi) {
+        for (int m = 0; m < 8; m++) amp[m] = w.amp[row + t + m * TPS];
+        if (w.xi) {
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
                 // colours 2c, 2c+1 of the site
+                const size_t pos = row + t + m * TPS;
                 const double2 v =
                     *reinterpret_cast<const double2 *>(w.xi + ((size_t)k * n + pos) * 8 + 2 * c);
                 z[m][0] = v.x;
                 z[m][1] = v.y;
-            } else {
-                // colours 0-3 come from counter half 0, 4-7 from half 1
-                normal2({(uint32_t)pos, (uint32_t)k, (w.nucleus << 1) | (uint32_t)(c >> 1), 0u},
-                        w.philox_key, c & 1, z[m]);
             }
+        } else {
+            // colours 0-3 come from counter half 0, 4-7 from half 1; channel 2h
+            // uses words (x, y) of the counter, channel 2h+1 words (z, w). Each
+            // lane of the pair draws the counters of four points and hands the
+            // partner's words over
+            const uint32_t hc = (uint32_t)(c >> 1);
+            uint32_t keep[8][2], give[4][2];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int m = 4 * half + j;
+                const U4 r = philox4x32_10(
+                    {(uint32_t)(row + t + m * TPS), (uint32_t)k, (w.nucleus << 1) | hc, 0u},
+                    (uint32_t)w.philox_key, (uint32_t)(w.philox_key >> 32));
+                keep[m][0] = half ? r.z : r.x;
+                keep[m][1] = half ? r.w : r.y;
+                give[j][0] = half ? r.x : r.z;
+                give[j][1] = half ? r.y : r.w;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int m = 4 * (1 - half) + j;
+                keep[m][0] = __shfl_xor_sync(0xffffffffu, give[j][0], 1);
+                keep[m][1] = __shfl_xor_sync(0xffffffffu, give[j][1], 1);
+            }
+#pragma unroll
+            for (int m = 0; m < 8; m++) box_muller(keep[m][0], keep[m][1], z[m]);
         }
 #pragma unroll
         for (int m = 0; m < 8; m++) x[m] = {amp[m] * z[m][0], amp[m] * z[m][1]};
