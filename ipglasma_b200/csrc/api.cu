@@ -395,7 +395,7 @@ ipg_status observables_enqueue(ipg_ctx *c) {
     ta.s = c->s64;
     ta.T10 = c->T10;
     launch_tmunu(ta, c->stream);
-    IPG_LAUNCHED(c, 2);
+    IPG_LAUNCHED(c, 7);
     LandauArgs la;
     la.N = N;
     la.tau_fm = itmax * dtau * c->a;

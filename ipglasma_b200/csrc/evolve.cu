@@ -18,6 +18,7 @@
 
 #include "fields.cuh"
 #include "ipg_internal.h"
+#include "pair2.cuh"
 
 namespace ipg {
 
@@ -94,14 +95,11 @@ __device__ __forceinline__ M3<T> taylor2_update(const H3<T> &e, T c,
     return mul(t, u);
 }
 
+// one site (ix, iy) in full-matrix storage (the FP64 plain form)
 template <typename T, bool REUNIT>
-__global__ void __launch_bounds__(128)
-    k_leapfrog(const EventGeom *__restrict__ ev, State<T> s, C<T> *ux_out,
-               C<T> *uy_out, T *phi_out, StepCoef<T> cf) {
-    const int N = ev->N;
-    const int iy = blockIdx.x * blockDim.x + threadIdx.x;
-    const int ix = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ix >= N || iy >= N) return;
+__device__ __forceinline__ void leapfrog_full_site(int N, int ix, int iy, const State<T> &s,
+                                                   C<T> *ux_out, C<T> *uy_out, T *phi_out,
+                                                   const StepCoef<T> &cf) {
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)ix * N + iy;
 
@@ -198,6 +196,17 @@ __global__ void __launch_bounds__(128)
         if (REUNIT) reunitarize(ny);
         st_m3(uy_out, pos, n, ny);
     }
+}
+
+template <typename T, bool REUNIT>
+__global__ void __launch_bounds__(128)
+    k_leapfrog(const EventGeom *__restrict__ ev, State<T> s, C<T> *ux_out,
+               C<T> *uy_out, T *phi_out, StepCoef<T> cf) {
+    const int N = ev->N;
+    const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ix = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= N || iy >= N) return;
+    leapfrog_full_site<T, REUNIT>(N, ix, iy, s, ux_out, uy_out, phi_out, cf);
 }
 
 // ===========================================================================
@@ -521,123 +530,150 @@ __device__ __forceinline__ H3<T> transport_bwd_minus(const M3<T> &u, const H3<T>
     }
 }
 
-template <typename T>
-__device__ __forceinline__ H3<T> shfl_xor_h(const H3<T> &h, int m) {
-    H3<T> r;
-    r.d0 = __shfl_xor_sync(0xffffffffu, h.d0, m);
-    r.d1 = __shfl_xor_sync(0xffffffffu, h.d1, m);
-    r.d2 = __shfl_xor_sync(0xffffffffu, h.d2, m);
-    r.o01.r = __shfl_xor_sync(0xffffffffu, h.o01.r, m);
-    r.o01.i = __shfl_xor_sync(0xffffffffu, h.o01.i, m);
-    r.o02.r = __shfl_xor_sync(0xffffffffu, h.o02.r, m);
-    r.o02.i = __shfl_xor_sync(0xffffffffu, h.o02.i, m);
-    r.o12.r = __shfl_xor_sync(0xffffffffu, h.o12.r, m);
-    r.o12.i = __shfl_xor_sync(0xffffffffu, h.o12.i, m);
+// ---------------------------------------------------------------------------
+// FP32 deviation form, one thread per site with both directions packed in the
+// two lanes of P2 (pair2.cuh): lane x advances direction d = x (U_d = U_x,
+// U_o = U_y, +d = +x, +o = +y), lane y direction d = y. With the plaquette
+// written in the (d, o) orientation,
+//   P_do  = U_d U_o(+d) U_d(+o)^dag U_o^dag   (for d = x this is U12, for
+//           d = y it is U12^dag, so AH(P_do) = +-h12 as in evolveE),
+//   S_d   = (U_d U_o(+d-o)^dag)(U_d(-o)^dag U_o(-o))   (U1m2 / U2m1),
+// both directions run the same code. Every product of the two directions then costs one
+// packed instruction; pi and phi, which belong to the site, stay scalar and
+// take the sum of the two lanes' brackets.
+// ---------------------------------------------------------------------------
+namespace {
+
+// lane x from px at ix, lane y from py at iy
+__device__ __forceinline__ M3<P2> ld_m3_pair(const C<float> *__restrict__ px, size_t ix,
+                                             const C<float> *__restrict__ py, size_t iy,
+                                             size_t n) {
+    M3<P2> a;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const C<float> u = px[k * n + ix], w = py[k * n + iy];
+        a.m[k] = {P2(u.r, w.r), P2(u.i, w.i)};
+    }
+    return a;
+}
+
+__device__ __forceinline__ void st_m3_pair(C<float> *__restrict__ px, C<float> *__restrict__ py,
+                                           size_t pos, size_t n, const M3<P2> &a) {
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        px[k * n + pos] = {lane_x(a.m[k].r), lane_x(a.m[k].i)};
+        py[k * n + pos] = {lane_y(a.m[k].r), lane_y(a.m[k].i)};
+    }
+}
+
+__device__ __forceinline__ H3<P2> pair_h(const H3<float> &a, const H3<float> &b) {
+    H3<P2> h;
+    h.d0 = P2(a.d0, b.d0);
+    h.d1 = P2(a.d1, b.d1);
+    h.d2 = P2(a.d2, b.d2);
+    h.o01 = {P2(a.o01.r, b.o01.r), P2(a.o01.i, b.o01.i)};
+    h.o02 = {P2(a.o02.r, b.o02.r), P2(a.o02.i, b.o02.i)};
+    h.o12 = {P2(a.o12.r, b.o12.r), P2(a.o12.i, b.o12.i)};
+    return h;
+}
+
+__device__ __forceinline__ H3<float> lane_h(const H3<P2> &h, int y) {
+    auto l = [&](P2 v) { return y ? lane_y(v) : lane_x(v); };
+    H3<float> r;
+    r.d0 = l(h.d0);
+    r.d1 = l(h.d1);
+    r.d2 = l(h.d2);
+    r.o01 = {l(h.o01.r), l(h.o01.i)};
+    r.o02 = {l(h.o02.r), l(h.o02.i)};
+    r.o12 = {l(h.o12.r), l(h.o12.i)};
     return r;
 }
 
-// One direction d of one site (ix, iy) of an N x N lattice (N >= 32). Lanes
-// 2k and 2k+1 of a full warp hold the two directions of one site: the pi
-// bracket is summed across them with a shuffle.
-template <typename T, bool DEV>
-__device__ __forceinline__ void leapfrog_site_dir(int N, int ix, int iy, int d,
-                                                  const State<T> &s, C<T> *ux_out,
-                                                  C<T> *uy_out, T *phi_out,
-                                                  const StepCoef<T> &cf) {
+}  // namespace
+
+__device__ __forceinline__ void leapfrog_pair_site(int N, int ix, int iy, const State<float> &s,
+                                                   C<float> *ux_out, C<float> *uy_out,
+                                                   float *phi_out, const StepCoef<float> &cf) {
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)ix * N + iy;
-    const C<T> *Ud_p = d ? s.uy : s.ux;
-    const C<T> *Uo_p = d ? s.ux : s.uy;
-    T *E_p = d ? s.e2 : s.e1;
-    // neighbour offsets along own (d) and other (o) direction, clamped
-    const int id = d ? iy : ix, io = d ? ix : iy;
-    const long sd = d ? 1 : N, so = d ? N : 1;
-    const long pd = (id + 1 < N) ? sd : 0, md = (id > 0) ? -sd : 0;
-    const long po = (io + 1 < N) ? so : 0, mo = (io > 0) ? -so : 0;
+    const long pdx = (ix + 1 < N) ? N : 0, mdx = (ix > 0) ? -(long)N : 0;
+    const long pdy = (iy + 1 < N) ? 1 : 0, mdy = (iy > 0) ? -1 : 0;
 
-    const M3<T> Ud = ld_m3(Ud_p, pos, n);
-    const H3<T> phi = ld_h(s.phi, pos, n);
-    H3<T> pi = ld_h(s.pi, pos, n);
-    H3<T> Ed = ld_h8(E_p, pos, n);
+    const M3<P2> Ud = ld_m3_pair(s.ux, pos, s.uy, pos, n);
+    const H3<float> phi = ld_h(s.phi, pos, n);
+    H3<float> pi = ld_h(s.pi, pos, n);
+    H3<P2> Ed = pair_h(ld_h8(s.e1, pos, n), ld_h8(s.e2, pos, n));
 
     if (cf.do_pe) {
-        H3<T> stap;
+        const H3<P2> phi2 = pair_h(phi, phi);
+        H3<P2> stap;
         {
             // P_do = (U_d U_o(+d)) (U_o U_d(+o))^dag
-            const M3<T> Uo = ld_m3(Uo_p, pos, n);
-            const M3<T> a = lmul<T, DEV>(Ud, ld_m3(Uo_p, pos + pd, n));
-            const M3<T> b = lmul<T, DEV>(Uo, ld_m3(Ud_p, pos + po, n));
-            stap = i_antiherm(lmul_nd<T, DEV>(a, b));
+            const M3<P2> Uo = ld_m3_pair(s.uy, pos, s.ux, pos, n);
+            const M3<P2> a = dmul(Ud, ld_m3_pair(s.uy, pos + pdx, s.ux, pos + pdy, n));
+            const M3<P2> b = dmul(Uo, ld_m3_pair(s.ux, pos + pdy, s.uy, pos + pdx, n));
+            stap = i_antiherm(dmul_nd(a, b));
         }
         {
             // S_d = (U_d U_o(+d-o)^dag) (U_d(-o)^dag U_o(-o))
-            const M3<T> p = lmul_nd<T, DEV>(Ud, ld_m3(Uo_p, pos + pd + mo, n));
-            const M3<T> q = lmul_dn<T, DEV>(ld_m3(Ud_p, pos + mo, n), ld_m3(Uo_p, pos + mo, n));
-            h_add(stap, i_antiherm(lmul<T, DEV>(p, q)));
+            const M3<P2> p = dmul_nd(Ud, ld_m3_pair(s.uy, pos + pdx + mdy, s.ux, pos + pdy + mdx, n));
+            const M3<P2> q = dmul_dn(ld_m3_pair(s.ux, pos + mdy, s.uy, pos + mdx, n),
+                                     ld_m3_pair(s.uy, pos + mdy, s.ux, pos + mdx, n));
+            h_add(stap, i_antiherm(dmul(p, q)));
         }
         h_traceless(stap);
-        const T cst = cf.tau * cf.dt_pe / (T(2) * cf.g * cf.g);
-        const T cdt = cf.dt_pe / cf.tau;
+        const P2 cst = P2(cf.tau * cf.dt_pe / (2.f * cf.g * cf.g));
+        const P2 cdt = P2(cf.dt_pe / cf.tau);
         h_axpy(Ed, cst, stap);
-        H3<T> br = transport_fwd_minus<T, DEV>(Ud, ld_h(s.phi, pos + pd, n), phi);
-        h_axpy(Ed, cdt, i_commutator(br, phi));  // i[phi~ - phi, phi] = i[phi~, phi]
-        h_add(br, transport_bwd_minus<T, DEV>(ld_m3(Ud_p, pos + md, n),
-                                              ld_h(s.phi, pos + md, n), phi));
-        h_add(br, shfl_xor_h(br, 1));
-        h_axpy(pi, cdt, br);
+        const H3<P2> fp = pair_h(ld_h(s.phi, pos + pdx, n), ld_h(s.phi, pos + pdy, n));
+        H3<P2> br = transport_fwd_minus<P2, true>(Ud, fp, phi2);
+        h_axpy(Ed, cdt, i_commutator(br, phi2));  // i[phi~ - phi, phi] = i[phi~, phi]
+        const H3<P2> fm = pair_h(ld_h(s.phi, pos + mdx, n), ld_h(s.phi, pos + mdy, n));
+        h_add(br, transport_bwd_minus<P2, true>(ld_m3_pair(s.ux, pos + mdx, s.uy, pos + mdy, n),
+                                                fm, phi2));
+        H3<float> brs = lane_h(br, 0);
+        h_add(brs, lane_h(br, 1));
+        h_axpy(pi, cf.dt_pe / cf.tau, brs);
         h_traceless(Ed);
-        st_h8(E_p, pos, n, Ed);
-        if (d == 0) st_h(s.pi, pos, n, pi);
+        st_h8(s.e1, pos, n, lane_h(Ed, 0));
+        st_h8(s.e2, pos, n, lane_h(Ed, 1));
+        st_h(s.pi, pos, n, pi);
     }
     if (cf.do_pu) {
-        const T c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / T(2));
-        M3<T> nu;
-        if constexpr (DEV) {
-            nu = taylor2_update_dev(Ed, c, Ud);
-            reunitarize_dev(nu);
-        } else {
-            nu = taylor2_update(Ed, c, Ud);
-        }
-        st_m3(d ? uy_out : ux_out, pos, n, nu);
-        if (d == 1) {
-            H3<T> phin = phi;
-            h_axpy(phin, (cf.tau + cf.dt_pu / T(2)) * cf.dt_pu, pi);
-            st_h(phi_out, pos, n, phin);
-        }
+        const float c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / 2.f);
+        M3<P2> nu = taylor2_update_dev(Ed, P2(c), Ud);
+        reunitarize_dev(nu);
+        st_m3_pair(ux_out, uy_out, pos, n, nu);
+        H3<float> phin = phi;
+        h_axpy(phin, (cf.tau + cf.dt_pu / 2.f) * cf.dt_pu, pi);
+        st_h(phi_out, pos, n, phin);
     }
 }
 
-// block: 256 threads = 128 sites (32 along y, the fast index, x 4 along x)
-// x 2 directions; lanes 2k and 2k+1 share a site
-template <typename T, bool DEV>
-// FP32: 128 registers, two blocks (16 warps) per SM; FP64: one block per SM
-// (the FP64 state needs ~250 registers per thread without spilling)
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
-    k_leapfrog_split(const EventGeom *__restrict__ ev, State<T> s, C<T> *ux_out,
-                     C<T> *uy_out, T *phi_out, StepCoef<T> cf) {
-    const int N = ev->N;
-    const int d = threadIdx.x & 1;
-    const int iy = blockIdx.x * 32 + ((threadIdx.x >> 1) & 31);
-    const int ix = blockIdx.y * 4 + (threadIdx.x >> 6);
-    // the grid covers the lattice exactly (N a multiple of 32)
-    leapfrog_site_dir<T, DEV>(N, ix, iy, d, s, ux_out, uy_out, phi_out, cf);
+// block: 256 threads = 32 sites along y x 8 along x; the grid covers the
+// lattice exactly (N a multiple of 32)
+__global__ void __launch_bounds__(256, 1)
+    k_leapfrog_pair(const EventGeom *__restrict__ ev, State<float> s, C<float> *ux_out,
+                    C<float> *uy_out, float *phi_out, StepCoef<float> cf) {
+    const int iy = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int ix = blockIdx.y * 8 + (threadIdx.x >> 5);
+    leapfrog_pair_site(ev->N, ix, iy, s, ux_out, uy_out, phi_out, cf);
 }
 
 // ---------------------------------------------------------------------------
 // Batched events: one persistent launch advances every site of every event in
 // a batch (lattices of different N, each a multiple of 32) by one step. The
 // tile list of the batch is the concatenation of the events' tiles (32 sites
-// along y x TX rows along x); event e owns tiles [tile_begin[e],
+// along y x TX rows along x, one thread per site); event e owns tiles [tile_begin[e],
 // tile_begin[e+1]). Each block takes tiles blockIdx.x, blockIdx.x + gridDim.x,
 // ... and finds the owning event by binary search over tile_begin held in
 // shared memory. Per-event pointers and coefficients of this step come from a
 // descriptor table in device memory, so a captured sequence of launches stays
 // valid when the events' buffers swap roles between runs.
 // ---------------------------------------------------------------------------
-template <int TX, typename T, bool DEV>
-// FP32: 128 registers at every tile shape (512 threads per SM); FP64: up to
-// 255 registers (256 threads per SM), so FP64 uses TX = 2 or 4 only
-__global__ void __launch_bounds__(64 * TX, sizeof(T) == 4 ? 8 / TX : (TX <= 4 ? 4 / TX : 1))
+template <int TX, typename T>
+// one thread per site and up to 255 registers in both forms: 256 threads per SM
+__global__ void __launch_bounds__(32 * TX, 8 / TX)
     k_leapfrog_batch(const BatchEvent<T> *__restrict__ evs, int n_events,
                      const int *__restrict__ tile_begin, int total_tiles) {
     // the step's descriptors, then tile_begin[n_events + 1], in shared memory
@@ -652,8 +688,7 @@ __global__ void __launch_bounds__(64 * TX, sizeof(T) == 4 ? 8 / TX : (TX <= 4 ? 
     }
     for (int e = threadIdx.x; e <= n_events; e += blockDim.x) s_begin[e] = tile_begin[e];
     __syncthreads();
-    const int d = threadIdx.x & 1;
-    const int ly = (threadIdx.x >> 1) & 31, lx = threadIdx.x >> 6;
+    const int ly = threadIdx.x & 31, lx = threadIdx.x >> 5;
     for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
         int lo = 0, hi = n_events - 1;  // last e with s_begin[e] <= t
         while (lo < hi) {
@@ -666,8 +701,13 @@ __global__ void __launch_bounds__(64 * TX, sizeof(T) == 4 ? 8 / TX : (TX <= 4 ? 
         const int local = t - s_begin[lo];
         const int tiles_y = E.N >> 5;
         const int ty = local % tiles_y, tx = local / tiles_y;
-        leapfrog_site_dir<T, DEV>(E.N, tx * TX + lx, ty * 32 + ly, d, E.s, E.ux_out,
-                                  E.uy_out, E.phi_out, E.cf);
+        // the same per-site code as the single-event kernels of this precision
+        if constexpr (sizeof(T) == 4)
+            leapfrog_pair_site(E.N, tx * TX + lx, ty * 32 + ly, E.s, E.ux_out, E.uy_out,
+                               E.phi_out, E.cf);
+        else
+            leapfrog_full_site<T, false>(E.N, tx * TX + lx, ty * 32 + ly, E.s, E.ux_out,
+                                         E.uy_out, E.phi_out, E.cf);
     }
 }
 
@@ -683,18 +723,17 @@ int batch_tile_rows(int variant) {
 
 template <typename T>
 const void *batch_kernel(int variant) {
-    constexpr bool DEV = sizeof(T) == 4;
     switch (variant) {
-        case 0: return (const void *)k_leapfrog_batch<2, T, DEV>;
-        case 1: return (const void *)k_leapfrog_batch<4, T, DEV>;
-        default: return (const void *)k_leapfrog_batch<8, T, DEV>;
+        case 0: return (const void *)k_leapfrog_batch<2, T>;
+        case 1: return (const void *)k_leapfrog_batch<4, T>;
+        default: return (const void *)k_leapfrog_batch<8, T>;
     }
 }
 
 template <typename T>
 int batch_max_blocks_per_sm(int variant, int n_events) {
     int nb = 0;
-    const int threads = 64 * batch_tile_rows<T>(variant);
+    const int threads = 32 * batch_tile_rows<T>(variant);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<T>(variant), threads,
                                                   batch_smem<T>(n_events));
     return nb;
@@ -703,20 +742,19 @@ int batch_max_blocks_per_sm(int variant, int n_events) {
 template <typename T>
 void launch_leapfrog_batch(const BatchEvent<T> *d_evs, int n_events, const int *d_tile_begin,
                            int total_tiles, int variant, int grid, cudaStream_t st) {
-    constexpr bool DEV = sizeof(T) == 4;
     const size_t smem = batch_smem<T>(n_events);
     switch (variant) {
         case 0:
-            k_leapfrog_batch<2, T, DEV><<<grid, 128, smem, st>>>(d_evs, n_events, d_tile_begin,
-                                                                 total_tiles);
+            k_leapfrog_batch<2, T><<<grid, 64, smem, st>>>(d_evs, n_events, d_tile_begin,
+                                                           total_tiles);
             break;
         case 1:
-            k_leapfrog_batch<4, T, DEV><<<grid, 256, smem, st>>>(d_evs, n_events, d_tile_begin,
-                                                                 total_tiles);
+            k_leapfrog_batch<4, T><<<grid, 128, smem, st>>>(d_evs, n_events, d_tile_begin,
+                                                            total_tiles);
             break;
         default:
-            k_leapfrog_batch<8, T, DEV><<<grid, 512, smem, st>>>(d_evs, n_events, d_tile_begin,
-                                                                 total_tiles);
+            k_leapfrog_batch<8, T><<<grid, 256, smem, st>>>(d_evs, n_events, d_tile_begin,
+                                                            total_tiles);
             break;
     }
 }
@@ -739,18 +777,18 @@ template <typename T>
 void launch_leapfrog(const EventGeom *d_ev, int N, const State<T> &s,
                      C<T> *ux_out, C<T> *uy_out, T *phi_out,
                      const StepCoef<T> &cf, bool reunit, cudaStream_t st) {
-    if (N >= 32) {
-        // N is a power of two >= 32: every warp is 16 full sites of one row
-        dim3 grid(N / 32, (N + 3) / 4);
-        if constexpr (sizeof(T) == 4) {
+    // FP64 runs one thread per site: at 512^2 it takes 97 us a step against
+    // 108 us for the direction split (both FP64-pipe and latency bound at one
+    // 256-thread block per SM). FP32 runs both directions of a site in the
+    // two lanes of packed FP32 instructions (k_leapfrog_pair).
+    if constexpr (sizeof(T) == 4) {
+        if (N >= 32) {
+            // N is a power of two >= 32: the grid covers the lattice exactly
             (void)reunit;
-            k_leapfrog_split<T, true><<<grid, 256, 0, st>>>(d_ev, s, ux_out, uy_out,
-                                                            phi_out, cf);
-        } else {
-            k_leapfrog_split<T, false><<<grid, 256, 0, st>>>(d_ev, s, ux_out, uy_out,
-                                                             phi_out, cf);
+            k_leapfrog_pair<<<dim3(N / 32, N / 8), 256, 0, st>>>(d_ev, s, ux_out, uy_out, phi_out,
+                                                                 cf);
+            return;
         }
-        return;
     }
     launch_leapfrog_site(d_ev, N, s, ux_out, uy_out, phi_out, cf, reunit, st);
 }

@@ -127,156 +127,200 @@ __global__ void k_tmunu_diag(TmunuArgs A) {
     A.T10[3 * n + pos] = Tee / a6;
 }
 
-// T^taux, T^tauy, T^taueta, T^xy, T^xeta, T^yeta (Evolution.cpp:902-1238)
+// T^taux, T^tauy, T^taueta, T^xy, T^xeta, T^yeta (Evolution.cpp:902-1238),
+// in six launches (one kernel for all six keeps too many FP64 3x3 matrices
+// live and spills). For direction D (0 = x, 1 = y):
+//   PART 2D     the plaquette sums K, K' (Kx, Kxp or Ky, Kyp) and from them
+//               the magnetic traces of T^taud and T^deta, parked in their
+//               output planes;
+//   PART 2D+1   the electric/transport traces, combined with the parked
+//               values into T^taud and T^deta;
+//   PART 4, 5   T^taueta and T^xy.
+struct OffdiagGeom {
+    size_t pos, pX, pY, pXY, mX, mY, mXpY, pXmY, p2X, p2Y, p2XY, pX2Y;
+};
+
+__device__ __forceinline__ OffdiagGeom offdiag_geom(int N, size_t pos) {
+    const int i = (int)(pos / N), j = (int)(pos % N);
+    const int ip = min(N - 1, i + 1), im = max(0, i - 1), i2 = min(N - 1, i + 2);
+    const int jp = min(N - 1, j + 1), jm = max(0, j - 1), j2 = min(N - 1, j + 2);
+    OffdiagGeom G;
+    G.pos = pos;
+    G.pX = idx2(N, ip, j);
+    G.pY = idx2(N, i, jp);
+    G.pXY = idx2(N, ip, jp);
+    G.mX = idx2(N, im, j);
+    G.mY = idx2(N, i, jm);
+    G.mXpY = idx2(N, im, jp);
+    G.pXmY = idx2(N, ip, jm);
+    G.p2X = idx2(N, i2, j);
+    G.p2Y = idx2(N, i, j2);
+    G.p2XY = idx2(N, i2, jp);
+    G.pX2Y = idx2(N, ip, j2);
+    return G;
+}
+
+template <int PART>
 __global__ void __launch_bounds__(128) k_tmunu_offdiag(TmunuArgs A) {
     const int N = A.N;
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
-    const int i = (int)(pos / N), j = (int)(pos % N);
-    const int ip = min(N - 1, i + 1), im = max(0, i - 1), i2 = min(N - 1, i + 2);
-    const int jp = min(N - 1, j + 1), jm = max(0, j - 1), j2 = min(N - 1, j + 2);
-    const size_t pX = idx2(N, ip, j), pY = idx2(N, i, jp), pXY = idx2(N, ip, jp);
-    const size_t mX = idx2(N, im, j), mY = idx2(N, i, jm);
-    const size_t mXpY = idx2(N, im, jp), pXmY = idx2(N, ip, jm);
-    const size_t p2X = idx2(N, i2, j), p2Y = idx2(N, i, j2);
-    const size_t p2XY = idx2(N, i2, jp), pX2Y = idx2(N, ip, j2);
+    const OffdiagGeom G = offdiag_geom(N, pos);
     const State<double> &s = A.s;
     const double g = A.g, tau = A.tau;
-
-    const M3<double> Ux = ld_m3(s.ux, pos, n), Uy = ld_m3(s.uy, pos, n);
-    const M3<double> UxpX = ld_m3(s.ux, pX, n), UxpY = ld_m3(s.ux, pY, n);
-    const M3<double> UypX = ld_m3(s.uy, pX, n), UypY = ld_m3(s.uy, pY, n);
-
-    // anti-Hermitian traceless parts of the four-link products
-    // Pb = Ux UypX UxpY^dag Uy^dag   (plaquette at pos)
-    const M3<double> ahPb = ah(mul_nd(mul(Ux, UypX), mul(Uy, UxpY)));
-    M3<double> Kx, Kxp, Ky, Kyp;
-    {
-        // Q1 = UxmX^dag UymX UxmXpY Uy^dag
-        const M3<double> UxmX = ld_m3(s.ux, mX, n), UymX = ld_m3(s.uy, mX, n);
-        const M3<double> UxmXpY = ld_m3(s.ux, mXpY, n);
-        const M3<double> q1 = mul_nd(mul(mul_dn(UxmX, UymX), UxmXpY), Uy);
-        Kx = ah(q1);
-        sub_from(Kx, ahPb);
-    }
-    {
-        // R1 = UypX UxpXpY Uyp2X^dag UxpX^dag ; S1 = Ux^dag Uy UxpY UypX^dag
-        const M3<double> UxpXpY = ld_m3(s.ux, pXY, n), Uyp2X = ld_m3(s.uy, p2X, n);
-        const M3<double> r1 = mul_nd(mul(UypX, UxpXpY), mul(UxpX, Uyp2X));
-        const M3<double> s1 = mul_nd(mul(mul_dn(Ux, Uy), UxpY), UypX);
-        Kxp = ah(r1);
-        add_to(Kxp, ah(s1));
-    }
-    {
-        // Q3 = UymY^dag UxmY UypXmY Ux^dag
-        const M3<double> UymY = ld_m3(s.uy, mY, n), UxmY = ld_m3(s.ux, mY, n);
-        const M3<double> UypXmY = ld_m3(s.uy, pXmY, n);
-        const M3<double> q3 = mul_nd(mul(mul_dn(UymY, UxmY), UypXmY), Ux);
-        Ky = ah(q3);
-        add_to(Ky, ahPb);
-    }
-    {
-        // R3 = UxpY UypXpY Uxp2Y^dag UypY^dag ; S3 = Uy^dag Ux UypX UxpY^dag
-        const M3<double> UypXpY = ld_m3(s.uy, pXY, n), Uxp2Y = ld_m3(s.ux, p2Y, n);
-        const M3<double> r3 = mul_nd(mul(UxpY, UypXpY), mul(UypY, Uxp2Y));
-        const M3<double> s3 = mul_nd(mul(mul_dn(Uy, Ux), UypX), UxpY);
-        Kyp = ah(r3);
-        add_to(Kyp, ah(s3));
-    }
-
-    const M3<double> phi = hm(s.phi, pos, n), phiX = hm(s.phi, pX, n);
-    const M3<double> phiY = hm(s.phi, pY, n), phiXY = hm(s.phi, pXY, n);
-    const M3<double> ptX = tr_fwd(Ux, phiX);      // phiTildeX
-    const M3<double> ptY = tr_fwd(Uy, phiY);      // phiTildeY
-    const M3<double> ptXY1 = tr_fwd(UxpY, phiXY);
-    const M3<double> ptXY2 = tr_fwd(UypX, phiXY);
-    const M3<double> E1 = hm8(s.e1, pos, n), E1p = hm8(s.e1, pY, n);
-    const M3<double> E2 = hm8(s.e2, pos, n), E2p = hm8(s.e2, pX, n);
-    const M3<double> pi = hm(s.pi, pos, n), piX = hm(s.pi, pX, n);
-    const M3<double> piY = hm(s.pi, pY, n), piXY = hm(s.pi, pXY, n);
-
     const double a4 = pow(A.a, 4.), a5 = pow(A.a, 5.);
 
-    // T^taux
-    {
-        M3<double> c = mul(E2, Kx);
-        add_to(c, mul(E2p, Kxp));
-        const double mag = trace(c).i;
-        M3<double> t = mul(pi, minus(ptX, tr_bwd(ld_m3(s.ux, mX, n), hm(s.phi, mX, n))));
-        {
-            const M3<double> UxmXpY = ld_m3(s.ux, mXpY, n);
-            add_to(t, mul(piY, minus(ptXY1, tr_bwd(UxmXpY, hm(s.phi, mXpY, n)))));
+    if constexpr (PART == 0 || PART == 2) {
+        const M3<double> Ux = ld_m3(s.ux, pos, n), Uy = ld_m3(s.uy, pos, n);
+        const M3<double> UxpY = ld_m3(s.ux, G.pY, n), UypX = ld_m3(s.uy, G.pX, n);
+        // Pb = Ux UypX UxpY^dag Uy^dag   (plaquette at pos)
+        const M3<double> ahPb = ah(mul_nd(mul(Ux, UypX), mul(Uy, UxpY)));
+        M3<double> K, Kp;
+        if constexpr (PART == 0) {
+            {
+                // Q1 = UxmX^dag UymX UxmXpY Uy^dag
+                const M3<double> q1 = mul_nd(
+                    mul(mul_dn(ld_m3(s.ux, G.mX, n), ld_m3(s.uy, G.mX, n)), ld_m3(s.ux, G.mXpY, n)),
+                    Uy);
+                K = ah(q1);
+                sub_from(K, ahPb);
+            }
+            {
+                // R1 = UypX UxpXpY Uyp2X^dag UxpX^dag ; S1 = Ux^dag Uy UxpY UypX^dag
+                const M3<double> r1 = mul_nd(mul(UypX, ld_m3(s.ux, G.pXY, n)),
+                                             mul(ld_m3(s.ux, G.pX, n), ld_m3(s.uy, G.p2X, n)));
+                const M3<double> s1 = mul_nd(mul(mul_dn(Ux, Uy), UxpY), UypX);
+                Kp = ah(r1);
+                add_to(Kp, ah(s1));
+            }
+        } else {
+            {
+                // Q3 = UymY^dag UxmY UypXmY Ux^dag
+                const M3<double> q3 = mul_nd(
+                    mul(mul_dn(ld_m3(s.uy, G.mY, n), ld_m3(s.ux, G.mY, n)), ld_m3(s.uy, G.pXmY, n)),
+                    Ux);
+                K = ah(q3);
+                add_to(K, ahPb);
+            }
+            {
+                // R3 = UxpY UypXpY Uxp2Y^dag UypY^dag ; S3 = Uy^dag Ux UypX UxpY^dag
+                const M3<double> r3 = mul_nd(mul(UxpY, ld_m3(s.uy, G.pXY, n)),
+                                             mul(ld_m3(s.uy, G.pY, n), ld_m3(s.ux, G.p2Y, n)));
+                const M3<double> s3 = mul_nd(mul(mul_dn(Uy, Ux), UypX), UxpY);
+                Kp = ah(r3);
+                add_to(Kp, ah(s3));
+            }
         }
-        add_to(t, mul(piX, minus(tr_fwd(UxpX, hm(s.phi, p2X, n)), tr_bwd(Ux, phi))));
-        add_to(t, mul(piXY, minus(tr_fwd(ld_m3(s.ux, pXY, n), hm(s.phi, p2XY, n)),
-                                  tr_bwd(UxpY, phiY))));
-        const double el = trace(t).r;
-        A.T10[4 * n + pos] = (2. / tau / 8. * mag - 2. / 8. / tau * el) / a4;
-    }
-    // T^tauy
-    {
-        M3<double> c = mul(E1, Ky);
-        add_to(c, mul(E1p, Kyp));
-        const double mag = trace(c).i;
-        M3<double> t = mul(pi, minus(ptY, tr_bwd(ld_m3(s.uy, mY, n), hm(s.phi, mY, n))));
+        // magnetic part of T^taud: Im tr(E K + E' K') with E = E2 (x) or E1 (y)
         {
-            const M3<double> UypXmY = ld_m3(s.uy, pXmY, n);
-            add_to(t, mul(piX, minus(ptXY2, tr_bwd(UypXmY, hm(s.phi, pXmY, n)))));
+            const double *Ep = PART == 0 ? s.e2 : s.e1;
+            M3<double> c = mul(hm8(Ep, pos, n), K);
+            add_to(c, mul(hm8(Ep, PART == 0 ? G.pX : G.pY, n), Kp));
+            A.T10[(PART == 0 ? 4 : 5) * n + pos] = trace(c).i;
         }
-        add_to(t, mul(piY, minus(tr_fwd(UypY, hm(s.phi, p2Y, n)), tr_bwd(Uy, phi))));
-        add_to(t, mul(piXY, minus(tr_fwd(ld_m3(s.uy, pXY, n), hm(s.phi, pX2Y, n)),
-                                  tr_bwd(UypX, phiX))));
-        const double el = trace(t).r;
-        A.T10[5 * n + pos] = (2. / tau / 8. * mag - 2. / 8. / tau * el) / a4;
-    }
-    const M3<double> dX = minus(ptX, phi), dY = minus(ptY, phi);
-    const M3<double> dXY1 = minus(ptXY1, phiY), dXY2 = minus(ptXY2, phiX);
-    // T^taueta
-    {
-        M3<double> t = mul(E1, dX);
-        add_to(t, mul(E1p, dXY1));
-        add_to(t, mul(E2, dY));
-        add_to(t, mul(E2p, dXY2));
-        A.T10[6 * n + pos] = (g / tau / tau / tau * trace(t).r) / a5;
-    }
-    // T^xy
-    {
-        M3<double> ea = E1;
-        add_to(ea, tr_fwd(Uy, E1p));
-        M3<double> eb = E2;
-        add_to(eb, tr_fwd(Ux, E2p));
-        M3<double> t = scaled(mul(ea, eb), -1. / 4. * g * g);
-        const M3<double> wy = tr_fwd(Uy, dXY1);  // Uy (phiTildeXY1 - phiY) Uy^dag
-        const M3<double> wx = tr_fwd(Ux, dXY2);  // Ux (phiTildeXY2 - phiX) Ux^dag
-        M3<double> q = mul(dX, dY);
-        add_to(q, mul(wy, dY));
-        add_to(q, mul(dX, wx));
-        add_to(q, mul(wy, wx));
-        add_to(t, scaled(q, 1. / 4.));
-        A.T10[7 * n + pos] = (2. / tau / tau * trace(t).r) / a4;
-    }
-    // T^xeta
-    {
-        M3<double> e = mul(E1, hm(s.pi, pos, n));
-        add_to(e, mul(E1, tr_fwd(Ux, piX)));
-        add_to(e, mul(E1p, piY));
-        add_to(e, mul(E1p, tr_fwd(UxpY, piXY)));
-        M3<double> m = mul(Kx, dY);
-        add_to(m, mul(Kxp, dXY2));
-        const double v = 1. / 4. * g * trace(e).r + 1. / 8. / g * (-trace(m).i);
-        A.T10[8 * n + pos] = (-2. / tau / tau * v) / a5;
-    }
-    // T^yeta
-    {
-        M3<double> e = mul(E2, pi);
-        add_to(e, mul(E2, tr_fwd(Uy, piY)));
-        add_to(e, mul(E2p, piX));
-        add_to(e, mul(E2p, tr_fwd(UypX, piXY)));
-        M3<double> m = mul(Ky, dX);
-        add_to(m, mul(Kyp, dXY1));
-        const double v = 1. / 4. * g * trace(e).r + 1. / 8. / g * (-trace(m).i);
-        A.T10[9 * n + pos] = (-2. / tau / tau * v) / a5;
+        // magnetic part of T^deta: Im tr(K d + K' d') with the transported phi
+        {
+            const M3<double> phi = hm(s.phi, pos, n), phiXY = hm(s.phi, G.pXY, n);
+            M3<double> m;
+            if constexpr (PART == 0) {
+                const M3<double> dY = minus(tr_fwd(Uy, hm(s.phi, G.pY, n)), phi);
+                const M3<double> dXY2 = minus(tr_fwd(UypX, phiXY), hm(s.phi, G.pX, n));
+                m = mul(K, dY);
+                add_to(m, mul(Kp, dXY2));
+            } else {
+                const M3<double> dX = minus(tr_fwd(Ux, hm(s.phi, G.pX, n)), phi);
+                const M3<double> dXY1 = minus(tr_fwd(UxpY, phiXY), hm(s.phi, G.pY, n));
+                m = mul(K, dX);
+                add_to(m, mul(Kp, dXY1));
+            }
+            A.T10[(PART == 0 ? 8 : 9) * n + pos] = trace(m).i;
+        }
+    } else if constexpr (PART == 1 || PART == 3) {
+        const M3<double> pi = hm(s.pi, pos, n), piX = hm(s.pi, G.pX, n);
+        const M3<double> piY = hm(s.pi, G.pY, n), piXY = hm(s.pi, G.pXY, n);
+        const M3<double> Ux = ld_m3(s.ux, pos, n), Uy = ld_m3(s.uy, pos, n);
+        const M3<double> UxpY = ld_m3(s.ux, G.pY, n), UypX = ld_m3(s.uy, G.pX, n);
+        const M3<double> phi = hm(s.phi, pos, n), phiX = hm(s.phi, G.pX, n);
+        const M3<double> phiY = hm(s.phi, G.pY, n), phiXY = hm(s.phi, G.pXY, n);
+        if constexpr (PART == 1) {
+            // T^taux
+            const double mag = A.T10[4 * n + pos];
+            M3<double> t = mul(pi, minus(tr_fwd(Ux, phiX),
+                                         tr_bwd(ld_m3(s.ux, G.mX, n), hm(s.phi, G.mX, n))));
+            add_to(t, mul(piY, minus(tr_fwd(UxpY, phiXY),
+                                     tr_bwd(ld_m3(s.ux, G.mXpY, n), hm(s.phi, G.mXpY, n)))));
+            add_to(t, mul(piX, minus(tr_fwd(ld_m3(s.ux, G.pX, n), hm(s.phi, G.p2X, n)),
+                                     tr_bwd(Ux, phi))));
+            add_to(t, mul(piXY, minus(tr_fwd(ld_m3(s.ux, G.pXY, n), hm(s.phi, G.p2XY, n)),
+                                      tr_bwd(UxpY, phiY))));
+            const double el = trace(t).r;
+            A.T10[4 * n + pos] = (2. / tau / 8. * mag - 2. / 8. / tau * el) / a4;
+            // T^xeta
+            const double mi = A.T10[8 * n + pos];
+            const M3<double> E1 = hm8(s.e1, pos, n), E1p = hm8(s.e1, G.pY, n);
+            M3<double> e = mul(E1, pi);
+            add_to(e, mul(E1, tr_fwd(Ux, piX)));
+            add_to(e, mul(E1p, piY));
+            add_to(e, mul(E1p, tr_fwd(UxpY, piXY)));
+            const double v = 1. / 4. * g * trace(e).r + 1. / 8. / g * (-mi);
+            A.T10[8 * n + pos] = (-2. / tau / tau * v) / a5;
+        } else {
+            // T^tauy
+            const double mag = A.T10[5 * n + pos];
+            M3<double> t = mul(pi, minus(tr_fwd(Uy, phiY),
+                                         tr_bwd(ld_m3(s.uy, G.mY, n), hm(s.phi, G.mY, n))));
+            add_to(t, mul(piX, minus(tr_fwd(UypX, phiXY),
+                                     tr_bwd(ld_m3(s.uy, G.pXmY, n), hm(s.phi, G.pXmY, n)))));
+            add_to(t, mul(piY, minus(tr_fwd(ld_m3(s.uy, G.pY, n), hm(s.phi, G.p2Y, n)),
+                                     tr_bwd(Uy, phi))));
+            add_to(t, mul(piXY, minus(tr_fwd(ld_m3(s.uy, G.pXY, n), hm(s.phi, G.pX2Y, n)),
+                                      tr_bwd(UypX, phiX))));
+            const double el = trace(t).r;
+            A.T10[5 * n + pos] = (2. / tau / 8. * mag - 2. / 8. / tau * el) / a4;
+            // T^yeta
+            const double mi = A.T10[9 * n + pos];
+            const M3<double> E2 = hm8(s.e2, pos, n), E2p = hm8(s.e2, G.pX, n);
+            M3<double> e = mul(E2, pi);
+            add_to(e, mul(E2, tr_fwd(Uy, piY)));
+            add_to(e, mul(E2p, piX));
+            add_to(e, mul(E2p, tr_fwd(UypX, piXY)));
+            const double v = 1. / 4. * g * trace(e).r + 1. / 8. / g * (-mi);
+            A.T10[9 * n + pos] = (-2. / tau / tau * v) / a5;
+        }
+    } else {
+        const M3<double> Ux = ld_m3(s.ux, pos, n), Uy = ld_m3(s.uy, pos, n);
+        const M3<double> UxpY = ld_m3(s.ux, G.pY, n), UypX = ld_m3(s.uy, G.pX, n);
+        const M3<double> phi = hm(s.phi, pos, n), phiX = hm(s.phi, G.pX, n);
+        const M3<double> phiY = hm(s.phi, G.pY, n), phiXY = hm(s.phi, G.pXY, n);
+        const M3<double> dX = minus(tr_fwd(Ux, phiX), phi), dY = minus(tr_fwd(Uy, phiY), phi);
+        const M3<double> dXY1 = minus(tr_fwd(UxpY, phiXY), phiY);
+        const M3<double> dXY2 = minus(tr_fwd(UypX, phiXY), phiX);
+        const M3<double> E1 = hm8(s.e1, pos, n), E1p = hm8(s.e1, G.pY, n);
+        const M3<double> E2 = hm8(s.e2, pos, n), E2p = hm8(s.e2, G.pX, n);
+        if constexpr (PART == 4) {
+            // T^taueta
+            M3<double> t = mul(E1, dX);
+            add_to(t, mul(E1p, dXY1));
+            add_to(t, mul(E2, dY));
+            add_to(t, mul(E2p, dXY2));
+            A.T10[6 * n + pos] = (g / tau / tau / tau * trace(t).r) / a5;
+        } else {
+            // T^xy
+            M3<double> ea = E1;
+            add_to(ea, tr_fwd(Uy, E1p));
+            M3<double> eb = E2;
+            add_to(eb, tr_fwd(Ux, E2p));
+            M3<double> t = scaled(mul(ea, eb), -1. / 4. * g * g);
+            const M3<double> wy = tr_fwd(Uy, dXY1);  // Uy (phiTildeXY1 - phiY) Uy^dag
+            const M3<double> wx = tr_fwd(Ux, dXY2);  // Ux (phiTildeXY2 - phiX) Ux^dag
+            M3<double> q = mul(dX, dY);
+            add_to(q, mul(wy, dY));
+            add_to(q, mul(dX, wx));
+            add_to(q, mul(wy, wx));
+            add_to(t, scaled(q, 1. / 4.));
+            A.T10[7 * n + pos] = (2. / tau / tau * trace(t).r) / a4;
+        }
     }
 }
 
@@ -288,7 +332,13 @@ void launch_tmunu_diag(const TmunuArgs &a, cudaStream_t st) {
 void launch_tmunu(const TmunuArgs &a, cudaStream_t st) {
     const size_t n = (size_t)a.N * a.N;
     k_tmunu_diag<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a);
-    k_tmunu_offdiag<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a);
+    const unsigned b = (unsigned)((n + 127) / 128);
+    k_tmunu_offdiag<0><<<b, 128, 0, st>>>(a);
+    k_tmunu_offdiag<1><<<b, 128, 0, st>>>(a);
+    k_tmunu_offdiag<2><<<b, 128, 0, st>>>(a);
+    k_tmunu_offdiag<3><<<b, 128, 0, st>>>(a);
+    k_tmunu_offdiag<4><<<b, 128, 0, st>>>(a);
+    k_tmunu_offdiag<5><<<b, 128, 0, st>>>(a);
 }
 
 }  // namespace ipg
