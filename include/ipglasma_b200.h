@@ -263,7 +263,7 @@ typedef struct ipg_batch ipg_batch;
 typedef struct {
     int variant;            /* tile-shape variant */
     int tile_rows;          /* a tile is 32 sites along y x tile_rows along x */
-    int threads_per_block;  /* 2 threads per site */
+    int threads_per_block;  /* one thread per site */
     int blocks_per_sm;      /* resident blocks of the persistent grid */
     int grid;               /* blocks_per_sm x SM count */
     double ms_per_step;     /* measured time of one full step of the batch */

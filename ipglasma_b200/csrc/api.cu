@@ -1484,7 +1484,7 @@ ipg_status ipg_batch_tune(ipg_batch *b, ipg_tune_report *rep) {
         if (!rep) return;
         rep->variant = b->variant;
         rep->tile_rows = tile_rows(b, b->variant);
-        rep->threads_per_block = 64 * rep->tile_rows;
+        rep->threads_per_block = 32 * rep->tile_rows;
         rep->blocks_per_sm = b->blocks_per_sm;
         rep->grid = b->grid;
         rep->ms_per_step = ms;

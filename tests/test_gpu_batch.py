@@ -70,7 +70,7 @@ def test_tune_picks_a_shape_and_caches_it():
         rep = b.tune()
         assert rep.candidates >= 3 and rep.from_cache == 0
         assert rep.ms_per_step > 0
-        assert rep.threads_per_block == 64 * rep.tile_rows
+        assert rep.threads_per_block == 32 * rep.tile_rows
         assert rep.grid % rep.blocks_per_sm == 0
         res = b.run()
     for r in res:

@@ -160,3 +160,34 @@ def test_full_size_invariants_fp64():
     tau = res.tau_final
     norm = u4[0] ** 2 - u4[1] ** 2 - u4[2] ** 2 - tau * tau * u4[3] ** 2
     assert np.abs(norm[hot] - 1).max() < 1e-8
+
+
+def test_fp32_form_error_against_fp64():
+    """The FP32 bulk form against the plain FP64 form on the same event
+    (same noise, same FP64 initial conditions). Bounds, from the 512^2 Pb+Pb
+    measurements (E_T 4e-6, eps2 1e-6 to 6e-6, e rms 5e-5) with margin for a
+    smaller lattice: E_T and eps2 to 1e-4, e per cell (cells above 1% of the
+    maximum) to 1e-3 rms, Gauss law and unitarity at FP32 rounding."""
+    from ipglasma_b200.synthetic import make_event
+
+    # O+O in a 10 fm box: the nuclei fit, so the clamped edges see no field
+    N, L = 128, 10.0
+    A, B, _, _ = make_event(N, L, "O", 1.0, seed=3)
+    out = {}
+    for prec in (ipg.FP64, ipg.FP32):
+        with ipg.Event(ipg.Config(size=N, L=L, Ny=10, maxtime=0.4, seed=9,
+                                  precision=prec)) as ev:
+            ev.set_g2mu(A, B)
+            ev.use_device_noise()
+            ev.init_fields()
+            res = ev.run()
+            out[prec] = (res, ev.observables()[0])
+    (r64, e64), (r32, e32) = out[ipg.FP64], out[ipg.FP32]
+    assert abs(r32.E_T / r64.E_T - 1) < 1e-4
+    assert abs(r32.eccentricity[1] / r64.eccentricity[1] - 1) < 1e-4
+    hot = e64 > 1e-2 * e64.max()
+    rel = np.abs(e32[hot] - e64[hot]) / e64[hot]
+    assert np.sqrt(np.mean(rel ** 2)) < 1e-3
+    # FP32 adds no Gauss-law violation beyond the FP64 form's plus rounding
+    assert r32.gauss_violation <= r64.gauss_violation + 1e-10
+    assert r32.unitarity_max < 1e-6
