@@ -360,12 +360,12 @@ def measure_batched(torch, ipg, rank, dist):
         ev.use_device_noise()
         evs.append(ev)
 
+    batch = ipg.Batch(evs)
+
     def init_all():
-        for ev in evs:
-            ev.init_fields(allow_nonconverged=True)
+        batch.init_fields(allow_nonconverged=True)
 
     init_all()
-    batch = ipg.Batch(evs)
     tune = batch.tune()
     batch.run()  # warm-up: captures the graph
     times, evo = [], []

@@ -274,6 +274,11 @@ typedef struct {
 const char *ipg_batch_last_error(const ipg_batch *batch);
 ipg_status ipg_batch_create(ipg_ctx *const *events, int count, ipg_batch **out);
 ipg_status ipg_batch_destroy(ipg_batch *batch);
+/* ipg_init_fields for every event (g2mu and noise set on each), enqueued on
+ * the events' own streams before any is waited for, so the initial
+ * conditions of small lattices run side by side; reports[count] may be NULL.
+ * Returns IPG_ERR_NEWTON_NONCONVERGED if any event has non-converged links. */
+ipg_status ipg_batch_init(ipg_batch *batch, ipg_init_report *reports);
 /* Time every tile shape and resident-block count on one full step of this
  * batch (events freshly initialised; their E and pi are restored) and keep
  * the fastest. Results are cached per (device, precision, lattice sizes) in

@@ -121,6 +121,7 @@ _SIGNATURES = {
     "ipg_batch_create": (ct.c_int, [ct.POINTER(ct.c_void_p), ct.c_int, ct.POINTER(ct.c_void_p)]),
     "ipg_batch_destroy": (ct.c_int, [ct.c_void_p]),
     "ipg_batch_tune": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
+    "ipg_batch_init": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
     "ipg_batch_run": (ct.c_int, [ct.c_void_p, ct.c_void_p]),
     "ipg_batch_set_shape": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int]),
     "ipg_batch_stats": (ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_double), ct.POINTER(ct.c_double),
@@ -407,6 +408,12 @@ class Batch:
         if st != 0 and st not in allow:
             raise IPGError(st, self._lib.ipg_batch_last_error(self._h).decode())
         return st
+
+    def init_fields(self, allow_nonconverged: bool = False):
+        """Initial conditions of every event, side by side on the GPU."""
+        reps = (_InitReport * len(self.events))()
+        self._check(self._lib.ipg_batch_init(self._h, reps), (3,) if allow_nonconverged else ())
+        return [InitReport(*(getattr(r, f) for f, _ in _InitReport._fields_)) for r in reps]
 
     def tune(self) -> TuneReport:
         rep = _TuneReport()

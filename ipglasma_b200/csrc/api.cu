@@ -71,6 +71,8 @@ struct ipg_ctx {
     EventGeom *d_ev = nullptr;
 
     bool initialized = false, half_done = false, finished = false;
+    cudaEvent_t ie[4] = {nullptr, nullptr, nullptr, nullptr};  // init stage timing
+    bool init_from_wilson = false;                              // of the pending init
     int it = 0;  // completed full steps
     double last_leapfrog_ms = 0;
     int last_leapfrog_launches = 0;
@@ -517,6 +519,7 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
     IPG_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     IPG_CUDA(c, cudaEventCreate(&c->ev0));
     IPG_CUDA(c, cudaEventCreate(&c->ev1));
+    for (cudaEvent_t &x : c->ie) IPG_CUDA(c, cudaEventCreate(&x));
 
     const size_t n = c->n;
     IPG_TRY(dalloc(c, &c->g2mu2A, n));
@@ -586,6 +589,8 @@ ipg_status ipg_destroy(ipg_ctx *ctx) {
     }
     for (void *p : ctx->allocs) cudaFree(p);
     if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
+    for (cudaEvent_t x : ctx->ie)
+        if (x) cudaEventDestroy(x);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -664,15 +669,17 @@ ipg_status ipg_use_device_noise(ipg_ctx *c) {
     return IPG_OK;
 }
 
-// from_wilson: V_A and V_B were loaded with ipg_set_field, skip setV
-static ipg_status init_impl(ipg_ctx *c, ipg_init_report *rep, bool from_wilson) {
+// The initial conditions on the context's stream, without waiting for them
+// (init_finish waits); from_wilson: V_A and V_B were loaded with
+// ipg_set_field, skip setV
+static ipg_status init_enqueue(ipg_ctx *c, bool from_wilson) {
     if (!c) return IPG_ERR_BAD_CONFIG;
     if (!from_wilson && (!c->have_g2mu || !c->have_noise))
         return fail(c, IPG_ERR_STATE, "set g2mu and noise before ipg_init_fields");
     const size_t n = c->n;
     const int N = c->N;
-    cudaEvent_t e[4];
-    for (auto &x : e) IPG_CUDA(c, cudaEventCreate(&x));
+    cudaEvent_t *e = c->ie;
+    c->init_from_wilson = from_wilson;
     IPG_CUDA(c, cudaEventRecord(e[0], c->stream));
 
     // Wilson lines, nucleus A then B (Init.cpp:1688-1847)
@@ -738,10 +745,16 @@ static ipg_status init_impl(ipg_ctx *c, ipg_init_report *rep, bool from_wilson) 
                         c->scal + 40, c->stream);
     IPG_LAUNCHED(c, 2);
     IPG_CUDA(c, cudaEventRecord(e[3], c->stream));
-    double ns[4];
-    IPG_CUDA(c, cudaMemcpyAsync(ns, c->scal + 40, sizeof(ns), cudaMemcpyDeviceToHost,
-                                c->stream));
+    IPG_CUDA(c, cudaMemcpyAsync(c->h_scal + 48, c->scal + 40, 4 * sizeof(double),
+                                cudaMemcpyDeviceToHost, c->stream));
+    return IPG_OK;
+}
+
+static ipg_status init_finish(ipg_ctx *c, ipg_init_report *rep) {
+    const size_t n = c->n;
+    cudaEvent_t *e = c->ie;
     IPG_TRY(sync(c));
+    const double *ns = c->h_scal + 48;
     const int mx = (int)ns[0], restarted = (int)ns[2], failed = (int)ns[3];
     const double sum = ns[1];
     if (rep) {
@@ -758,9 +771,8 @@ static ipg_status init_impl(ipg_ctx *c, ipg_init_report *rep, bool from_wilson) 
         cudaEventElapsedTime(&ms, e[2], e[3]);
         rep->ms_fields = ms;
     }
-    for (auto &x : e) cudaEventDestroy(x);
     c->initialized = true;
-    c->init_from_inputs = !from_wilson;
+    c->init_from_inputs = !c->init_from_wilson;
     c->half_done = false;
     c->finished = false;
     c->it = 0;
@@ -771,11 +783,13 @@ static ipg_status init_impl(ipg_ctx *c, ipg_init_report *rep, bool from_wilson) 
 }
 
 ipg_status ipg_init_fields(ipg_ctx *c, ipg_init_report *rep) {
-    return init_impl(c, rep, false);
+    IPG_TRY(init_enqueue(c, false));
+    return init_finish(c, rep);
 }
 
 ipg_status ipg_init_from_wilson_lines(ipg_ctx *c, ipg_init_report *rep) {
-    return init_impl(c, rep, true);
+    IPG_TRY(init_enqueue(c, true));
+    return init_finish(c, rep);
 }
 
 ipg_status ipg_evolve(ipg_ctx *c, int steps) {
@@ -1474,6 +1488,28 @@ ipg_status ipg_batch_destroy(ipg_batch *b) {
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return IPG_OK;
+}
+
+ipg_status ipg_batch_init(ipg_batch *b, ipg_init_report *reports) {
+    if (!b) return IPG_ERR_BAD_CONFIG;
+    const int E = (int)b->ev.size();
+    // every event's initial conditions on its own stream, then one wait each:
+    // small lattices overlap on the GPU
+    for (int e = 0; e < E; e++) {
+        ipg_status st = init_enqueue(b->ev[e], false);
+        if (st != IPG_OK) return bfail(b, st, "event %d: %s", e, b->ev[e]->err.c_str());
+    }
+    ipg_status worst = IPG_OK;
+    for (int e = 0; e < E; e++) {
+        ipg_status st = init_finish(b->ev[e], reports ? reports + e : nullptr);
+        if (st == IPG_ERR_NEWTON_NONCONVERGED) {
+            worst = st;
+            b->err = "event " + std::to_string(e) + ": " + b->ev[e]->err;
+        } else if (st != IPG_OK) {
+            return bfail(b, st, "event %d: %s", e, b->ev[e]->err.c_str());
+        }
+    }
+    return worst;
 }
 
 ipg_status ipg_batch_tune(ipg_batch *b, ipg_tune_report *rep) {

@@ -56,10 +56,12 @@ def test_batch_matches_single_events_and_replays(prec):
             ms_evo, ms_tot, launches = b.stats()
             assert ms_evo > 0 and ms_tot >= ms_evo
             assert launches == (rep + 1) * events[0].itmax
-            # fresh initial fields for the replay (same seeds, same result)
+            # fresh initial fields for the replay (same seeds, same result),
+            # all events' initial conditions enqueued side by side
             for k, ev in enumerate(events):
                 ev.reseed(100 + k)
-                ev.init_fields()
+            reps = b.init_fields()
+            assert all(r.newton_failed == 0 for r in reps)
     for ev in events:
         ev.close()
 
