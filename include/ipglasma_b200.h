@@ -128,6 +128,19 @@ ipg_status ipg_set_g2mu(ipg_ctx *ctx, const double *g2mu2A,
 ipg_status ipg_set_g2mu_device(ipg_ctx *ctx, const double *d_g2mu2A,
                                const double *d_g2mu2B);
 
+/* g^2 mu^2 maps of both nuclei computed on the device from nucleon
+ * positions: xyz[3*nA], xyz[3*nB] in fm (x, y, z), nucleus A shifted by
+ * -b/2 and B by +b/2 along x. T(x) = sum_k exp(-|x - x_k|^2/(2B))/(2 pi B)
+ * with B = BG hbarc^2 (Init.cpp:1052-1062, no substructure), then
+ * Q_s^2 = QsMax^2 T / max T and g2mu2 = Q_s^2/QsmuRatio^2 a^2/hbarc^2/g^2
+ * (Init.cpp:1403-1408). The reference's IP-Sat Q_s(T) table is not part of
+ * this library; this is the Q_s ~ sqrt(T) map. Replaces the g2mu part of
+ * Init::setColorChargeDensity (Init.cpp:753-1676) for that map. */
+ipg_status ipg_set_nuclei(ipg_ctx *ctx, const double *xyzA, int nA, const double *xyzB, int nB,
+                          double b, double BG, double QsMax, double QsmuRatio);
+/* Copy the current g^2 mu^2 maps ([N*N] each, lattice units) to the host. */
+ipg_status ipg_get_g2mu(ipg_ctx *ctx, double *g2mu2A, double *g2mu2B);
+
 /* Unit Gaussian noise xi[k][pos][a] (k < Ny, a < 8) of both nuclei in the
  * draw order of Init::setV, so rho = g sqrt(g2mu2/Ny) xi reproduces
  * Init.cpp:1695-1705 and 1773-1783. Host arrays of Ny*N*N*8 doubles. */

@@ -99,6 +99,9 @@ _SIGNATURES = {
     "ipg_set_g2mu": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "ipg_set_g2mu_device": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "ipg_set_noise": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "ipg_set_nuclei": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int,
+                                  ct.c_double, ct.c_double, ct.c_double, ct.c_double]),
+    "ipg_get_g2mu": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "ipg_set_noise_device": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "ipg_use_device_noise": (ct.c_int, [ct.c_void_p]),
     "ipg_init_fields": (ct.c_int, [ct.c_void_p, ct.POINTER(_InitReport)]),
@@ -264,6 +267,20 @@ class Event:
     def set_g2mu_device(self, ptr_a: int, ptr_b: int) -> None:
         self._check(self._lib.ipg_set_g2mu_device(self._h, ct.c_void_p(ptr_a),
                                                   ct.c_void_p(ptr_b)))
+
+    def set_nuclei(self, xyzA, xyzB, b: float, BG: float = 4.0, qs_max: float = 1.5,
+                   qsmu_ratio: float = 0.8) -> None:
+        """g2mu maps from nucleon positions ((A, 3) arrays in fm), on the device."""
+        a = np.ascontiguousarray(xyzA, dtype=np.float64).reshape(-1, 3)
+        bb = np.ascontiguousarray(xyzB, dtype=np.float64).reshape(-1, 3)
+        self._check(self._lib.ipg_set_nuclei(self._h, _ptr(a), len(a), _ptr(bb), len(bb), b, BG,
+                                             qs_max, qsmu_ratio))
+
+    def g2mu(self):
+        """The current g2mu maps (2, N*N), lattice units."""
+        out = np.empty((2, self.n))
+        self._check(self._lib.ipg_get_g2mu(self._h, _ptr(out[0]), _ptr(out[1])))
+        return out
 
     def set_noise(self, xiA, xiB) -> None:
         cnt = self.cfg.Ny * self.n * 8

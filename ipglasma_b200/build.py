@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC"]
 CU_SOURCES = ["api.cu", "evolve.cu", "init.cu", "poisson.cu", "observables.cu", "reduce.cu",
-              "noalloc.cu", "adjoint.cu"]
+              "noalloc.cu", "adjoint.cu", "nuclei.cu"]
 CPP_SOURCES = ["writers.cpp"]
 
 

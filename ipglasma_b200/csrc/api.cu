@@ -48,6 +48,8 @@ struct ipg_ctx {
     double *green = nullptr;
     double *amp = nullptr;
     double2 *work = nullptr;
+    double *nuc_xyz = nullptr, *nuc_gx = nullptr, *nuc_gy = nullptr;  // ipg_set_nuclei
+    int nuc_cap = 0;
     int work_sheets = 0;
     C<double> *VA = nullptr, *VB = nullptr;
     C<double> *u1x = nullptr, *u2x = nullptr, *u1y = nullptr, *u2y = nullptr;
@@ -628,6 +630,53 @@ ipg_status ipg_set_g2mu_device(ipg_ctx *c, const double *A, const double *B) {
     IPG_CUDA(c, cudaMemcpyAsync(c->g2mu2B, B, sizeof(double) * c->n,
                                 cudaMemcpyDeviceToDevice, c->stream));
     c->have_g2mu = true;
+    return IPG_OK;
+}
+
+ipg_status ipg_set_nuclei(ipg_ctx *c, const double *xyzA, int nA, const double *xyzB, int nB,
+                          double b, double BG, double QsMax, double QsmuRatio) {
+    if (!c || !xyzA || !xyzB || nA < 1 || nB < 1) return IPG_ERR_BAD_CONFIG;
+    if (!(BG > 0) || !(QsMax > 0) || !(QsmuRatio > 0))
+        return fail(c, IPG_ERR_BAD_CONFIG, "BG, QsMax and QsmuRatio must be > 0");
+    const int amax = std::max(nA, nB);
+    if (amax > c->nuc_cap) {
+        IPG_TRY(dalloc(c, &c->nuc_xyz, 3 * (size_t)amax));
+        IPG_TRY(dalloc(c, &c->nuc_gx, (size_t)amax * c->N));
+        IPG_TRY(dalloc(c, &c->nuc_gy, (size_t)amax * c->N));
+        c->nuc_cap = amax;
+    }
+    for (int nuc = 0; nuc < 2; nuc++) {
+        IPG_CUDA(c, cudaMemcpyAsync(c->nuc_xyz, nuc ? xyzB : xyzA, 3 * sizeof(double) * (nuc ? nB : nA),
+                                    cudaMemcpyHostToDevice, c->stream));
+        NucleiArgs na;
+        na.N = c->N;
+        na.L = c->cfg.L;
+        na.BG = BG;
+        na.QsMax = QsMax;
+        na.QsmuRatio = QsmuRatio;
+        na.g = c->cfg.g;
+        na.A = nuc ? nB : nA;
+        na.xyz = c->nuc_xyz;
+        na.shift = nuc ? b / 2. : -b / 2.;
+        na.gx = c->nuc_gx;
+        na.gy = c->nuc_gy;
+        na.partial = c->partial;
+        na.out = nuc ? c->g2mu2B : c->g2mu2A;
+        launch_g2mu_from_nucleons(na, c->stream);
+        IPG_LAUNCHED(c, 3);
+    }
+    IPG_TRY(sync(c));  // the positions buffer is reused for the second nucleus
+    c->have_g2mu = true;
+    return IPG_OK;
+}
+
+ipg_status ipg_get_g2mu(ipg_ctx *c, double *g2mu2A, double *g2mu2B) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (!c->have_g2mu) return fail(c, IPG_ERR_STATE, "no g2mu maps set");
+    if (g2mu2A)
+        IPG_CUDA(c, cudaMemcpy(g2mu2A, c->g2mu2A, c->n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (g2mu2B)
+        IPG_CUDA(c, cudaMemcpy(g2mu2B, c->g2mu2B, c->n * sizeof(double), cudaMemcpyDeviceToHost));
     return IPG_OK;
 }
 

@@ -117,6 +117,19 @@ void launch_initial_pi(int N, double g, const C<double> *u1x,
                        const C<double> *u2y, const C<double> *ux,
                        const C<double> *uy, double *pi, cudaStream_t st);
 
+// g2mu2 of one nucleus from its nucleon positions (nuclei.cu)
+struct NucleiArgs {
+    int N;
+    double L, BG, QsMax, QsmuRatio, g;
+    int A;               // nucleons
+    const double *xyz;   // [A][3] fm, device
+    double shift;        // added to x (fm)
+    double *gx, *gy;     // [A][N] scratch
+    double *partial;     // [296] scratch
+    double *out;         // [N*N] g2mu2, lattice units
+};
+void launch_g2mu_from_nucleons(const NucleiArgs &a, cudaStream_t st);
+
 // ---- observables ----------------------------------------------------------
 
 struct TmunuArgs {

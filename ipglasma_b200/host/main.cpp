@@ -8,8 +8,9 @@
 //   - reads V_A, V_B from the binary Wilson-line files of
 //     readInitialWilsonLines = 2 (format of Init.cpp:1914-1973 / 2120-2296),
 //   - or samples the two nuclei (Woods-Saxon with minimum distance, the
-//     algorithm of Init.cpp:2749-2816) and builds the g^2 mu^2 maps from the
-//     nucleon thickness: T_A = sum of Gaussians of width BG (GeV^-2), and
+//     algorithm of Init.cpp:2749-2816) on the host and builds the g^2 mu^2
+//     maps on the device (ipg_set_nuclei) from the nucleon thickness:
+//     T_A = sum of Gaussians of width BG (GeV^-2), and
 //     Q_s(x) = QsMax sqrt(T_A(x)/max T_A) with QsMax from the optional key
 //     QsMax (default 1.5 GeV), g^2 mu^2 a^2 = Q_s^2/QsmuRatio^2 a^2/(hbar c)^2/g^2.
 //     (The reference's IP-Sat Q_s(T_p, y) table is not used.)
@@ -161,33 +162,6 @@ std::vector<double> sample_nucleus(std::mt19937_64 &rng, const Species &s, doubl
     return xyz;
 }
 
-// g^2 mu^2 (lattice units) from nucleon positions shifted by xshift along x
-std::vector<double> g2mu_map(const std::vector<double> &xyz, double xshift, int N, double L,
-                             double BG, double g, double QsMax, double QsmuRatio) {
-    const double a = L / N, B = BG * kHbarc * kHbarc;
-    const int A = (int)xyz.size() / 3;
-    std::vector<double> gx((size_t)A * N), gy((size_t)A * N), T((size_t)N * N, 0.0);
-    for (int k = 0; k < A; k++)
-        for (int i = 0; i < N; i++) {
-            const double x = -L / 2. + a * i;
-            gx[(size_t)k * N + i] = std::exp(-(x - xyz[3 * k] - xshift) * (x - xyz[3 * k] - xshift) / (2 * B));
-            gy[(size_t)k * N + i] = std::exp(-(x - xyz[3 * k + 1]) * (x - xyz[3 * k + 1]) / (2 * B));
-        }
-    double tmax = 0;
-    for (int i = 0; i < N; i++)
-        for (int j = 0; j < N; j++) {
-            double s = 0;
-            for (int k = 0; k < A; k++) s += gx[(size_t)k * N + i] * gy[(size_t)k * N + j];
-            T[(size_t)i * N + j] = s / (2 * M_PI * B);
-            tmax = std::max(tmax, T[(size_t)i * N + j]);
-        }
-    for (double &t : T) {
-        const double qs2 = QsMax * QsMax * (tmax > 0 ? t / tmax : 0.0);
-        t = qs2 / (QsmuRatio * QsmuRatio) * a * a / (kHbarc * kHbarc) / (g * g);
-    }
-    return T;
-}
-
 // ------------------------------------------------------------- V files
 void write_vfile(const std::string &name, int N, double L, double y, const std::vector<double> &V) {
     std::ofstream f(name.c_str(), std::ios::out | std::ios::binary);
@@ -322,9 +296,10 @@ int main(int argc, char **argv) {
             const double dmin = in.i("setWSDeformParams") ? in.d("d_min") : 0.4;
             const auto nA = sample_nucleus(rng, sA, dmin);
             const auto nB = sample_nucleus(rng, sB, dmin);
-            const auto gA = g2mu_map(nA, -b / 2., N, cfg.L, BG, cfg.g, QsMax, QsmuRatio);
-            const auto gB = g2mu_map(nB, b / 2., N, cfg.L, BG, cfg.g, QsMax, QsmuRatio);
-            check(ctx, ipg_set_g2mu(ctx, gA.data(), gB.data()), "ipg_set_g2mu");
+            check(ctx,
+                  ipg_set_nuclei(ctx, nA.data(), (int)(nA.size() / 3), nB.data(),
+                                 (int)(nB.size() / 3), b, BG, QsMax, QsmuRatio),
+                  "ipg_set_nuclei");
             check(ctx, ipg_reseed(ctx, seed * 1000003ULL + event_id), "ipg_reseed");
             check(ctx, ipg_use_device_noise(ctx), "ipg_use_device_noise");
             check(ctx, ipg_init_fields(ctx, &rep), "ipg_init_fields");

@@ -83,3 +83,31 @@ def test_executable_reproduces_reference_output_files(ref_harness, tmp_path):
         # Tmunu at 32^2, whose off-diagonal entries are small differences)
         same = sum(x == y for x, y in zip(lo, lt)) / len(lt)
         assert same > 0.8, (name, same)
+
+
+def test_executable_samples_nuclei_on_its_own(tmp_path):
+    """Without input Wilson lines the executable samples the nuclei, builds
+    g2mu on the device (ipg_set_nuclei) and writes finite, positive energy
+    densities in the reference's hydro format; writeInitialWilsonLines 2
+    writes V files of the reference's binary layout."""
+    if not EXE.exists():
+        pytest.skip("executable not built")
+    N, L = 64, 20.0
+    text = (INPUT.format(N=N, L=L, Ny=4, maxtime=0.2)
+            .replace("readInitialWilsonLines 2", "readInitialWilsonLines 0")
+            .replace("writeInitialWilsonLines 0", "writeInitialWilsonLines 2")
+            .replace("useNucleus 0", "useNucleus 1")
+            .replace("Projectile Au", "Projectile O")
+            .replace("Target Au", "Target O")
+            .replace("bmax 0", "bmax 2"))
+    (tmp_path / "input").write_text(text)
+    res = subprocess.run([str(EXE), "input"], cwd=tmp_path, capture_output=True, text=True,
+                         timeout=300)
+    assert res.returncode == 0, res.stderr
+    hydro = numbers(tmp_path / "epsilon-u-Hydro-TauHydro-0.dat")
+    assert hydro.shape == (N * N, 18)
+    assert np.all(np.isfinite(hydro))
+    assert hydro[:, 3].max() > 0
+    for v in ("V-0", "V-1"):
+        raw = (tmp_path / v).read_bytes()
+        assert len(raw) == 4 + 4 + 3 * 8 + N * N * 18 * 8

@@ -191,3 +191,17 @@ def test_fp32_form_error_against_fp64():
     # FP32 adds no Gauss-law violation beyond the FP64 form's plus rounding
     assert r32.gauss_violation <= r64.gauss_violation + 1e-10
     assert r32.unitarity_max < 1e-6
+
+
+def test_g2mu_from_nucleons_matches_host_map():
+    """ipg_set_nuclei builds on the device the same g2mu maps as the host
+    generator (separable Gaussian thickness, Q_s ~ sqrt(T) scaling)."""
+    from ipglasma_b200.synthetic import make_event
+
+    N, L = 128, 20.0
+    A, B, nA, nB = make_event(N, L, "Pb", 4.0, seed=7)  # positions already shifted
+    with ipg.Event(ipg.Config(size=N, L=L, Ny=2, maxtime=0.1)) as ev:
+        ev.set_nuclei(nA, nB, b=0.0)
+        g = ev.g2mu()
+    for dev, host in ((g[0], A), (g[1], B)):
+        assert np.abs(dev - host).max() <= 1e-12 * host.max()
