@@ -77,7 +77,7 @@ def build_library(verbose: bool = False, force: bool = False) -> Path:
     cxx = shutil.which("g++") or "g++"
     for src in CPP_SOURCES:
         obj = objdir / (Path(src).stem + ".o")
-        _run([cxx, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I",
+        _run([cxx, "-O2", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", "-I",
               str(ROOT / "include"), "-c", str(CSRC / src), "-o", str(obj)])
         objs.append(str(obj))
     tmp = LIB.with_suffix(".so.tmp")

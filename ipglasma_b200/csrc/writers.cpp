@@ -7,13 +7,26 @@
 // divided by the OUTPUT spacing, a neighbour pair counts only if both sites
 // have an index strictly greater than 0, e <= 1e-10 GeV/fm^3 (hydro) and
 // T^tautau <= 1e-16 (Tmunu) become placeholder rows, u^tau is recomputed from
-// the normalisation, and numbers are printed with the default iostream format
-// (6 significant digits). Host code, fed from ipg_get_observables.
+// the normalisation, and numbers are printed as an ostream with default flags
+// prints them (printf "%g": 6 significant digits). Host code, fed from
+// ipg_get_observables.
+//
+// The reference streams line by line with a flush per line; here the output
+// rows are formatted in parallel (std::to_chars with precision 6 is specified
+// as printf "%.6g" in the C locale, so the bytes are the same) into one buffer
+// per thread, and the buffers are written in row order with one fwrite each.
+// The hydro file's total energy is summed serially in the reference's loop
+// order from per-point terms, so it is bit-identical too.
+#include <algorithm>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
-#include <fstream>
+#include <cstdlib>
+#include <cstring>
 #include <sstream>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "../../include/ipglasma_b200.h"
 
@@ -63,6 +76,74 @@ double interp(const Stencil &s, int nn, const double *f, bool absval) {
     return (1. - s.fy) * x1 + s.fy * x2;
 }
 
+// Text buffer with the two number formats of an ostream with default flags.
+// A number takes at most 13 characters ("-1.23457e-308"), an int at most 11.
+class Text {
+  public:
+    explicit Text(size_t reserve) { s_.reserve(reserve); }
+    // room for one line of `count` numbers and separators
+    void line(int count) {
+        const size_t need = n_ + (size_t)count * 16 + 2;
+        if (need > s_.size()) s_.resize(std::max(need, 2 * s_.size()));
+    }
+    Text &num(double v) {
+        n_ = std::to_chars(&s_[n_], &s_[0] + s_.size(), v, std::chars_format::general, 6).ptr -
+             &s_[0];
+        return *this;
+    }
+    Text &num(int v) {
+        n_ = std::to_chars(&s_[n_], &s_[0] + s_.size(), v).ptr - &s_[0];
+        return *this;
+    }
+    Text &ch(char c) {
+        s_[n_++] = c;
+        return *this;
+    }
+    const char *data() const { return s_.data(); }
+    size_t size() const { return n_; }
+
+  private:
+    std::string s_;
+    size_t n_ = 0;
+};
+
+// threads used to format a file of `rows` output rows: the host's hardware
+// threads (IPG_WRITER_THREADS overrides), at most one per 4 rows
+int writer_threads(int rows) {
+    int t = (int)std::thread::hardware_concurrency();
+    if (const char *e = std::getenv("IPG_WRITER_THREADS")) t = std::atoi(e);
+    t = std::min({std::max(t, 1), 64, std::max(rows / 4, 1)});
+    return t;
+}
+
+// format rows [0, rows) with body(text, r) split over threads in contiguous
+// chunks, then write the chunks in order after `head`
+template <class Body>
+bool format_and_write(const char *path, const Text &head, int rows, size_t bytes_per_row,
+                      Body body) {
+    const int T = writer_threads(rows);
+    std::vector<Text> parts;
+    parts.reserve(T);
+    for (int t = 0; t < T; t++) parts.emplace_back(bytes_per_row * (rows / T + 1));
+    auto run = [&](int t) {
+        const int r0 = (int)((long long)rows * t / T), r1 = (int)((long long)rows * (t + 1) / T);
+        for (int r = r0; r < r1; r++) body(parts[t], r);
+    };
+    if (T == 1) {
+        run(0);
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 1; t < T; t++) pool.emplace_back(run, t);
+        run(0);
+        for (auto &th : pool) th.join();
+    }
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return false;
+    bool ok = std::fwrite(head.data(), 1, head.size(), f) == head.size();
+    for (const Text &p : parts) ok = ok && std::fwrite(p.data(), 1, p.size(), f) == p.size();
+    return (std::fclose(f) == 0) && ok;
+}
+
 }  // namespace
 
 extern "C" {
@@ -72,68 +153,88 @@ ipg_status ipg_write_hydro(const char *path, int N, double L, int sizeOutput,
                            int it, double dtau, const double *eps,
                            const double *u4, const double *pi10, double gfactor,
                            double *Etot) {
-    if (!path || !eps || !u4 || !pi10 || N < 1 || sizeOutput < 1) return IPG_ERR_BAD_CONFIG;
+    if (!path || !eps || !u4 || !pi10 || N < 1 || sizeOutput < 1 || etaSizeOutput < 0)
+        return IPG_ERR_BAD_CONFIG;
     Grid g{N, L, L / N, sizeOutput, etaSizeOutput, LOutput, LOutput / sizeOutput, detaOutput};
     const int nn = N * N;
     const double a = g.a;
     const double tau0 = it * dtau * a;
-    std::ofstream out(path, std::ios::out);
-    if (!out) return IPG_ERR_BAD_CONFIG;
-    out << "# dummy " << 1 << " etamax= " << g.heta << " xmax= " << g.hx
-        << " ymax= " << g.hx << " deta= " << g.deta << " dx= " << g.ha
-        << " dy= " << g.ha << " tau= " << tau0 << std::endl;
+    Text head(256);
+    head.line(16);
+    for (const char *c = "# dummy "; *c; c++) head.ch(*c);
+    head.num(1);
+    auto label = [&](const char *s) {
+        for (; *s; s++) head.ch(*s);
+    };
+    label(" etamax= "), head.num(g.heta), label(" xmax= "), head.num(g.hx);
+    label(" ymax= "), head.num(g.hx), label(" deta= "), head.num(g.deta);
+    label(" dx= "), head.num(g.ha), label(" dy= "), head.num(g.ha);
+    label(" tau= "), head.num(tau0), head.ch('\n');
     const size_t n = (size_t)nn;
     // pi10 order: tautau xx yy etaeta taux tauy taueta xy xeta yeta
     const double *p00 = pi10, *pxx = pi10 + n, *pyy = pi10 + 2 * n, *pee = pi10 + 3 * n;
     const double *p0x = pi10 + 4 * n, *p0y = pi10 + 5 * n, *p0e = pi10 + 6 * n;
     const double *pxy = pi10 + 7 * n, *pxe = pi10 + 8 * n, *pye = pi10 + 9 * n;
-    double etot = 0.;
-    for (int ieta = 0; ieta < g.heta; ieta++) {
+    // one output row = (ieta, ix): hx lines, and a blank line after each eta slice
+    const int rows = g.heta * g.hx;
+    std::vector<double> term((size_t)rows * g.hx, 0.);
+    auto body = [&](Text &out, int r) {
+        const int ieta = r / g.hx, ix = r - ieta * g.hx;
         const double eta = -(g.heta - 1) / 2. * g.deta + g.deta * ieta;
-        for (int ix = 0; ix < g.hx; ix++) {
-            for (int iy = 0; iy < g.hx; iy++) {
-                const double x = -g.hL / 2. + g.ha * ix;
-                const double y = -g.hL / 2. + g.ha * iy;
-                if (std::abs(x) < L / 2. && std::abs(y) < L / 2.) {
-                    const Stencil s = stencil(g, x, y);
-                    const double e = interp(s, nn, eps, true);
-                    const double ux = interp(s, nn, u4 + n, false);
-                    const double uy = interp(s, nn, u4 + 2 * n, false);
-                    const double ueta = interp(s, nn, u4 + 3 * n, false);
-                    const double q00 = interp(s, nn, p00, false);
-                    const double q0x = interp(s, nn, p0x, false);
-                    const double q0y = interp(s, nn, p0y, false);
-                    const double q0e = interp(s, nn, p0e, false);
-                    const double qxy = interp(s, nn, pxy, false);
-                    const double qxe = interp(s, nn, pxe, false);
-                    const double qye = interp(s, nn, pye, false);
-                    const double qxx = interp(s, nn, pxx, false);
-                    const double qyy = interp(s, nn, pyy, false);
-                    const double qee = interp(s, nn, pee, false);
-                    const double utau =
-                        std::sqrt(1. + ux * ux + uy * uy + tau0 * tau0 * ueta * ueta);
-                    etot += std::abs(kHbarc * e * gfactor) * g.ha * g.ha * it * dtau * a;
-                    if (std::abs(kHbarc * e * gfactor) > 0.0000000001) {
-                        out << eta << " " << x << " " << y << " "
-                            << std::abs(kHbarc * e * gfactor) << " " << utau << " " << ux
-                            << " " << uy << " " << ueta << " " << q00 * gfactor << " "
-                            << q0x * gfactor << " " << q0y * gfactor << " " << q0e * gfactor
-                            << " " << qxx * gfactor << " " << qxy * gfactor << " "
-                            << qxe * gfactor << " " << qyy * gfactor << " " << qye * gfactor
-                            << " " << qee * gfactor << std::endl;
-                        continue;
-                    }
+        for (int iy = 0; iy < g.hx; iy++) {
+            const double x = -g.hL / 2. + g.ha * ix;
+            const double y = -g.hL / 2. + g.ha * iy;
+            out.line(18);
+            out.num(eta).ch(' ').num(x).ch(' ').num(y).ch(' ');
+            if (std::abs(x) < L / 2. && std::abs(y) < L / 2.) {
+                const Stencil s = stencil(g, x, y);
+                const double e = interp(s, nn, eps, true);
+                const double ux = interp(s, nn, u4 + n, false);
+                const double uy = interp(s, nn, u4 + 2 * n, false);
+                const double ueta = interp(s, nn, u4 + 3 * n, false);
+                const double q00 = interp(s, nn, p00, false);
+                const double q0x = interp(s, nn, p0x, false);
+                const double q0y = interp(s, nn, p0y, false);
+                const double q0e = interp(s, nn, p0e, false);
+                const double qxy = interp(s, nn, pxy, false);
+                const double qxe = interp(s, nn, pxe, false);
+                const double qye = interp(s, nn, pye, false);
+                const double qxx = interp(s, nn, pxx, false);
+                const double qyy = interp(s, nn, pyy, false);
+                const double qee = interp(s, nn, pee, false);
+                const double utau = std::sqrt(1. + ux * ux + uy * uy + tau0 * tau0 * ueta * ueta);
+                term[(size_t)r * g.hx + iy] =
+                    std::abs(kHbarc * e * gfactor) * g.ha * g.ha * it * dtau * a;
+                if (std::abs(kHbarc * e * gfactor) > 0.0000000001) {
+                    out.num(std::abs(kHbarc * e * gfactor)).ch(' ').num(utau).ch(' ');
+                    out.num(ux).ch(' ').num(uy).ch(' ').num(ueta).ch(' ');
+                    out.num(q00 * gfactor).ch(' ').num(q0x * gfactor).ch(' ');
+                    out.num(q0y * gfactor).ch(' ').num(q0e * gfactor).ch(' ');
+                    out.num(qxx * gfactor).ch(' ').num(qxy * gfactor).ch(' ');
+                    out.num(qxe * gfactor).ch(' ').num(qyy * gfactor).ch(' ');
+                    out.num(qye * gfactor).ch(' ').num(qee * gfactor).ch('\n');
+                    continue;
                 }
-                out << eta << " " << x << " " << y << " " << 0. << " " << 1. << " " << 0.
-                    << " " << 0. << " " << 0. << " " << 0. << " " << 0. << " " << 0. << " "
-                    << 0. << " " << 0. << " " << 0. << " " << 0. << " " << 0. << " " << 0.
-                    << " " << 0. << std::endl;
             }
+            out.num(0.).ch(' ').num(1.);
+            for (int k = 0; k < 13; k++) out.ch(' ').num(0.);
+            out.ch('\n');
         }
-        out << std::endl;
+        if (ix == g.hx - 1) {
+            out.line(0);
+            out.ch('\n');
+        }
+    };
+    const bool ok = format_and_write(path, head, rows, (size_t)g.hx * 140, body);
+    if (!ok) return IPG_ERR_BAD_CONFIG;
+    if (Etot) {
+        // the reference's running sum, in its loop order; points outside the
+        // lattice hold +0, which leaves a non-negative sum unchanged
+        double etot = 0.;
+        for (double v : term) etot += v;
+        *Etot = etot;
     }
-    if (Etot) *Etot = etot;
-    return out.good() ? IPG_OK : IPG_ERR_BAD_CONFIG;
+    return IPG_OK;
 }
 
 ipg_status ipg_write_tmunu(const char *path, int N, double L, int sizeOutput,
@@ -144,15 +245,22 @@ ipg_status ipg_write_tmunu(const char *path, int N, double L, int sizeOutput,
     const int nn = N * N;
     const size_t n = (size_t)nn;
     const double tau0 = it * dtau * g.a;
-    std::ofstream out(path, std::ios::out);
-    if (!out) return IPG_ERR_BAD_CONFIG;
-    out << "# dummy " << 1 << " etamax= " << g.heta << " xmax= " << g.hx
-        << " ymax= " << g.hx << " deta= " << g.deta << " dx= " << g.ha
-        << " dy= " << g.ha << std::endl;
-    for (int iy = 0; iy < g.hx; iy++) {
+    Text head(256);
+    head.line(16);
+    auto label = [&](const char *s) {
+        for (; *s; s++) head.ch(*s);
+    };
+    label("# dummy "), head.num(1);
+    label(" etamax= "), head.num(g.heta), label(" xmax= "), head.num(g.hx);
+    label(" ymax= "), head.num(g.hx), label(" deta= "), head.num(g.deta);
+    label(" dx= "), head.num(g.ha), label(" dy= "), head.num(g.ha), head.ch('\n');
+    // one output row = iy: hx lines and a blank line
+    auto body = [&](Text &out, int iy) {
         for (int ix = 0; ix < g.hx; ix++) {
             const double x = -g.hL / 2. + g.ha * ix;
             const double y = -g.hL / 2. + g.ha * iy;
+            out.line(12);
+            out.num(ix).ch(' ').num(iy).ch(' ');
             if (std::abs(x) < L / 2. && std::abs(y) < L / 2.) {
                 const Stencil s = stencil(g, x, y);
                 const double t00 = interp(s, nn, T10, false);
@@ -166,23 +274,26 @@ ipg_status ipg_write_tmunu(const char *path, int N, double L, int sizeOutput,
                 const double tye = interp(s, nn, T10 + 9 * n, false);
                 const double tee = interp(s, nn, T10 + 3 * n, false);
                 if (t00 * gfactor * kHbarc > kSmallEps) {
-                    out << ix << " " << iy << " " << t00 * gfactor * kHbarc << " "
-                        << txx * gfactor * kHbarc << " " << tyy * gfactor * kHbarc << " "
-                        << tau0 * tau0 * tee * gfactor * kHbarc << " "
-                        << -t0x * gfactor * kHbarc << " " << -t0y * gfactor * kHbarc << " "
-                        << -tau0 * t0e * gfactor * kHbarc << " " << -txy * gfactor * kHbarc
-                        << " " << -tau0 * tye * gfactor * kHbarc << " "
-                        << -tau0 * txe * gfactor * kHbarc << std::endl;
+                    out.num(t00 * gfactor * kHbarc).ch(' ');
+                    out.num(txx * gfactor * kHbarc).ch(' ').num(tyy * gfactor * kHbarc).ch(' ');
+                    out.num(tau0 * tau0 * tee * gfactor * kHbarc).ch(' ');
+                    out.num(-t0x * gfactor * kHbarc).ch(' ').num(-t0y * gfactor * kHbarc).ch(' ');
+                    out.num(-tau0 * t0e * gfactor * kHbarc).ch(' ');
+                    out.num(-txy * gfactor * kHbarc).ch(' ');
+                    out.num(-tau0 * tye * gfactor * kHbarc).ch(' ');
+                    out.num(-tau0 * txe * gfactor * kHbarc).ch('\n');
                     continue;
                 }
             }
-            out << ix << " " << iy << " " << kSmallEps << " " << kSmallEps / 2. << " "
-                << kSmallEps / 2. << " " << 0.0 << " " << 0.0 << " " << 0.0 << " " << 0.0
-                << " " << 0.0 << " " << 0.0 << " " << 0.0 << std::endl;
+            out.num(kSmallEps).ch(' ').num(kSmallEps / 2.).ch(' ').num(kSmallEps / 2.);
+            for (int k = 0; k < 7; k++) out.ch(' ').num(0.0);
+            out.ch('\n');
         }
-        out << std::endl;
-    }
-    return out.good() ? IPG_OK : IPG_ERR_BAD_CONFIG;
+        out.line(0);
+        out.ch('\n');
+    };
+    return format_and_write(path, head, g.hx, (size_t)g.hx * 110, body) ? IPG_OK
+                                                                        : IPG_ERR_BAD_CONFIG;
 }
 
 // File names of the reference (MyEigen.cpp:376-383, 804-807): the time is

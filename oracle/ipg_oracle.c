@@ -13,6 +13,7 @@
 
 #include <complex.h>
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -1100,4 +1101,132 @@ void ipgo_run_event(int N, int Ny, double L, double g, double m_GeV, double uvda
     free(e);
     free(u);
     free(p10);
+}
+
+/* ---- output files (MyEigen.cpp:329-1045) -------------------------------- */
+
+/* bilinear resampling stencil at output point (x, y): lattice index of the
+ * lower corner by floor((x + L/2)/a + 1e-10) (MyEigen.cpp:409-412), upper
+ * neighbours clamped at N-1, fractions over the OUTPUT spacing ha
+ * (MyEigen.cpp:430, 455) */
+typedef struct {
+    int p[4];
+    double fx, fy;
+} wstencil;
+
+static wstencil w_stencil(int N, double L, double ha, double x, double y) {
+    const double a = L / N;
+    const int xpos = (int)floor((x + L / 2.) / a + 0.0000000001);
+    const int ypos = (int)floor((y + L / 2.) / a + 0.0000000001);
+    const int xup = xpos < N - 1 ? xpos + 1 : xpos;
+    const int yup = ypos < N - 1 ? ypos + 1 : ypos;
+    wstencil s;
+    s.fx = (x - (-L / 2. + a * xpos)) / ha;
+    s.fy = (y - (-L / 2. + a * ypos)) / ha;
+    s.p[0] = xpos * N + ypos;
+    s.p[1] = xup * N + ypos;
+    s.p[2] = xpos * N + yup;
+    s.p[3] = xup * N + yup;
+    return s;
+}
+
+/* one interpolated field; a pair of neighbours counts only if both indices
+ * are in (0, N*N) (MyEigen.cpp:500-514) */
+static double w_interp(const wstencil *s, int nn, const double *f, int absval) {
+    double v[4];
+    for (int k = 0; k < 4; k++) v[k] = absval ? fabs(f[s->p[k]]) : f[s->p[k]];
+    const int ok1 = s->p[0] > 0 && s->p[0] < nn && s->p[1] > 0 && s->p[1] < nn;
+    const int ok2 = s->p[2] > 0 && s->p[2] < nn && s->p[3] > 0 && s->p[3] < nn;
+    const double x1 = ok1 ? (1 - s->fx) * v[0] + s->fx * v[1] : 0.;
+    const double x2 = ok2 ? (1 - s->fx) * v[2] + s->fx * v[3] : 0.;
+    return (1. - s->fy) * x1 + s->fy * x2;
+}
+
+static const double w_hbarc = 0.1973269718;
+
+int ipgo_write_hydro(const char *path, int N, double L, int sizeOutput,
+                     double LOutput, int etaSizeOutput, double detaOutput,
+                     int it, double dtau, const double *eps, const double *u4,
+                     const double *pi10, double gfactor, double *Etot) {
+    const double a = L / N, ha = LOutput / sizeOutput, tau0 = it * dtau * a;
+    const int nn = N * N;
+    const size_t n = (size_t)nn;
+    /* pi10 rows: tautau xx yy etaeta taux tauy taueta xy xeta yeta; printed
+     * as tautau taux tauy taueta xx xy xeta yy yeta etaeta */
+    static const int order[10] = {0, 4, 5, 6, 1, 7, 8, 2, 9, 3};
+    FILE *f = fopen(path, "w");
+    if (!f) return 1;
+    fprintf(f, "# dummy 1 etamax= %d xmax= %d ymax= %d deta= %g dx= %g dy= %g tau= %g\n",
+            etaSizeOutput, sizeOutput, sizeOutput, detaOutput, ha, ha, tau0);
+    double etot = 0.;
+    for (int ieta = 0; ieta < etaSizeOutput; ieta++) {
+        const double eta = -(etaSizeOutput - 1) / 2. * detaOutput + detaOutput * ieta;
+        for (int ix = 0; ix < sizeOutput; ix++) {
+            for (int iy = 0; iy < sizeOutput; iy++) {
+                const double x = -LOutput / 2. + ha * ix;
+                const double y = -LOutput / 2. + ha * iy;
+                fprintf(f, "%g %g %g ", eta, x, y);
+                if (fabs(x) < L / 2. && fabs(y) < L / 2.) {
+                    const wstencil s = w_stencil(N, L, ha, x, y);
+                    const double e = w_interp(&s, nn, eps, 1);
+                    const double ux = w_interp(&s, nn, u4 + n, 0);
+                    const double uy = w_interp(&s, nn, u4 + 2 * n, 0);
+                    const double ue = w_interp(&s, nn, u4 + 3 * n, 0);
+                    /* u^tau from the normalisation (MyEigen.cpp:751-753) */
+                    const double ut = sqrt(1. + ux * ux + uy * uy + tau0 * tau0 * ue * ue);
+                    const double ew = fabs(w_hbarc * e * gfactor);
+                    etot += ew * ha * ha * it * dtau * a;
+                    if (ew > 0.0000000001) {
+                        fprintf(f, "%g %g %g %g %g", ew, ut, ux, uy, ue);
+                        for (int k = 0; k < 10; k++)
+                            fprintf(f, " %g", w_interp(&s, nn, pi10 + order[k] * n, 0) * gfactor);
+                        fputc('\n', f);
+                        continue;
+                    }
+                }
+                fprintf(f, "0 1 0 0 0 0 0 0 0 0 0 0 0 0 0\n");
+            }
+        }
+        fputc('\n', f);
+    }
+    if (Etot) *Etot = etot;
+    return fclose(f) != 0;
+}
+
+int ipgo_write_tmunu(const char *path, int N, double L, int sizeOutput,
+                     double LOutput, int etaSizeOutput, double detaOutput,
+                     int it, double dtau, const double *T10, double gfactor) {
+    const double a = L / N, ha = LOutput / sizeOutput, tau0 = it * dtau * a;
+    const int nn = N * N;
+    const size_t n = (size_t)nn;
+    FILE *f = fopen(path, "w");
+    if (!f) return 1;
+    fprintf(f, "# dummy 1 etamax= %d xmax= %d ymax= %d deta= %g dx= %g dy= %g\n",
+            etaSizeOutput, sizeOutput, sizeOutput, detaOutput, ha, ha);
+    for (int iy = 0; iy < sizeOutput; iy++) {
+        for (int ix = 0; ix < sizeOutput; ix++) {
+            const double x = -LOutput / 2. + ha * ix;
+            const double y = -LOutput / 2. + ha * iy;
+            fprintf(f, "%d %d ", ix, iy);
+            if (fabs(x) < L / 2. && fabs(y) < L / 2.) {
+                const wstencil s = w_stencil(N, L, ha, x, y);
+                double t[10];
+                for (int k = 0; k < 10; k++) t[k] = w_interp(&s, nn, T10 + k * n, 0);
+                /* T10 rows: tautau xx yy etaeta taux tauy taueta xy xeta yeta;
+                 * sign and tau factors of MyEigen.cpp:1017-1027 */
+                if (t[0] * gfactor * w_hbarc > 1e-16) {
+                    fprintf(f, "%g %g %g %g %g %g %g %g %g %g\n", t[0] * gfactor * w_hbarc,
+                            t[1] * gfactor * w_hbarc, t[2] * gfactor * w_hbarc,
+                            tau0 * tau0 * t[3] * gfactor * w_hbarc, -t[4] * gfactor * w_hbarc,
+                            -t[5] * gfactor * w_hbarc, -tau0 * t[6] * gfactor * w_hbarc,
+                            -t[7] * gfactor * w_hbarc, -tau0 * t[9] * gfactor * w_hbarc,
+                            -tau0 * t[8] * gfactor * w_hbarc);
+                    continue;
+                }
+            }
+            fprintf(f, "%g %g %g 0 0 0 0 0 0 0\n", 1e-16, 1e-16 / 2., 1e-16 / 2.);
+        }
+        fputc('\n', f);
+    }
+    return fclose(f) != 0;
 }

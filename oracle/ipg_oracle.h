@@ -86,6 +86,18 @@ void ipgo_run_event(int N, int Ny, double L, double g, double m_GeV,
                     double *tau0_pi, double *eps, double *u4, double *pi10,
                     double *T10, double *scalars);
 
+/* The output files of MyEigen::flowVelocity4D (MyEigen.cpp:380-797 hydro,
+ * 801-1045 Tmunu), written serially with printf "%g" (what an ostream with
+ * default flags prints). Return 0 on success; *Etot gets the hydro file's
+ * total energy (MyEigen.cpp:755). */
+int ipgo_write_hydro(const char *path, int N, double L, int sizeOutput,
+                     double LOutput, int etaSizeOutput, double detaOutput,
+                     int it, double dtau, const double *eps, const double *u4,
+                     const double *pi10, double gfactor, double *Etot);
+int ipgo_write_tmunu(const char *path, int N, double L, int sizeOutput,
+                     double LOutput, int etaSizeOutput, double detaOutput,
+                     int it, double dtau, const double *T10, double gfactor);
+
 #ifdef __cplusplus
 }
 #endif

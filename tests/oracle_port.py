@@ -45,6 +45,8 @@ def lib():
         h.ipgo_run_event.argtypes = [ct.c_int, ct.c_int, ct.c_double, ct.c_double, ct.c_double,
                                      ct.c_double, ct.c_double, ct.c_double, _D, _D, _D, _D,
                                      _D, _D, _D, _D, _D, _D, _D, _D, _D, _D]
+        for fn in (h.ipgo_write_hydro, h.ipgo_write_tmunu):
+            fn.restype = ct.c_int
         _lib = h
     return _lib
 
@@ -109,3 +111,21 @@ def run_event(N, Ny, L, g, m, uvdamp, maxtime, g2muA, g2muB, xiA, xiB, dtau=-1.0
     res.update(eps=eps, u4=u4.reshape(4, n), pi10=pi10.reshape(10, n), T10=T10.reshape(10, n),
                gauss=sc[0], ecc2=sc[1], itmax=int(sc[2]), dtau=sc[3], restarts=int(sc[4]))
     return res
+
+
+def write_hydro(path, N, L, size_out, L_out, eta_size, deta, it, dtau, eps, u4, pi10,
+                gfactor) -> float:
+    D = ct.c_double
+    etot = D()
+    st = lib().ipgo_write_hydro(str(path).encode(), N, D(L), size_out, D(L_out), eta_size,
+                                D(deta), it, D(dtau), _p(_c(eps)), _p(_c(u4)), _p(_c(pi10)),
+                                D(gfactor), ct.byref(etot))
+    assert st == 0
+    return etot.value
+
+
+def write_tmunu(path, N, L, size_out, L_out, eta_size, deta, it, dtau, T10, gfactor) -> None:
+    D = ct.c_double
+    st = lib().ipgo_write_tmunu(str(path).encode(), N, D(L), size_out, D(L_out), eta_size,
+                                D(deta), it, D(dtau), _p(_c(T10)), D(gfactor))
+    assert st == 0
