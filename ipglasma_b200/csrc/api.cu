@@ -204,7 +204,8 @@ ipg_status step_impl(ipg_ctx *c, State<T> &s, C<T> *&uxb, C<T> *&uyb,
     cf.g = (T)c->cfg.g;
     cf.do_pe = do_pe;
     cf.do_pu = do_pu;
-    launch_leapfrog<T>(c->d_ev, c->N, s, uxb, uyb, phib, cf, reunit, c->stream);
+    set_derived(cf);
+    launch_leapfrog<T>(c->d_ev, c->N, s, uxb, uyb, phib, cf, reunit, c->stream, c->scal + 38);
     IPG_LAUNCHED(c, 1);
     if (do_pu) {
         std::swap(s.ux, uxb);
@@ -326,6 +327,7 @@ StepCoef<double> evolution_coef(const ipg_ctx *c, int s) {
     cf.g = c->cfg.g;
     cf.do_pe = s > 0;
     cf.do_pu = 1;
+    set_derived(cf);
     return cf;
 }
 
@@ -428,7 +430,7 @@ ipg_status observables_enqueue(ipg_ctx *c) {
     IPG_LAUNCHED(c, 2);
     launch_cell_flags(n, c->found, c->eps, c->partial, scal + 36, c->stream);
     IPG_LAUNCHED(c, 2);
-    IPG_CUDA(c, cudaMemcpyAsync(c->h_scal, scal, sizeof(double) * 38,
+    IPG_CUDA(c, cudaMemcpyAsync(c->h_scal, scal, sizeof(double) * 39,
                                 cudaMemcpyDeviceToHost, c->stream));
     IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     return IPG_OK;
@@ -465,6 +467,8 @@ ipg_status observables_finish(ipg_ctx *c, ipg_result *res) {
         res->ms_evolution = c->last_leapfrog_ms;
         res->ms_observables = ms_obs;
     }
+    if (h[38] != 0.)
+        return fail(c, IPG_ERR_TIMEOUT, "a leapfrog step gave up waiting for its tile loads");
     if (nan_count) return fail(c, IPG_ERR_NAN, "%d cells with non-finite e", nan_count);
     return IPG_OK;
 }
@@ -730,6 +734,8 @@ static ipg_status init_enqueue(ipg_ctx *c, bool from_wilson) {
     cudaEvent_t *e = c->ie;
     c->init_from_wilson = from_wilson;
     IPG_CUDA(c, cudaEventRecord(e[0], c->stream));
+    // scal[38]: set by a step kernel whose bounded wait gave up
+    IPG_CUDA(c, cudaMemsetAsync(c->scal + 38, 0, sizeof(double), c->stream));
 
     // Wilson lines, nucleus A then B (Init.cpp:1688-1847)
     for (int nuc = 0; nuc < (from_wilson ? 0 : 2); nuc++) {
@@ -1378,6 +1384,7 @@ void fill_table(ipg_batch *b, BatchEvent<T> *tab, int steps, bool full_first = f
             d.cf.g = (T)c->cfg.g;
             d.cf.do_pe = it > 0;
             d.cf.do_pu = 1;
+            set_derived(d.cf);
             d.N = c->N;
             d.active = 1;
             std::swap(s.ux, uxb);

@@ -14,11 +14,16 @@
 //
 // Per site the kernel moves the state once: read U(2x18) E(2x8) phi(9) pi(9)
 // and write the same, 70 reals each way; neighbour reads hit L1/L2.
+#include <cudaTypedefs.h>
+
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 
 #include "fields.cuh"
 #include "ipg_internal.h"
 #include "pair2.cuh"
+#include "tma.cuh"
 
 namespace ipg {
 
@@ -291,6 +296,18 @@ template <typename T>
 __device__ __forceinline__ T inv_sqrt1p_m1(T e) {
     const T s = sqrt(T(1) + e);
     return -e / (s * (T(1) + s));
+}
+
+// the same per lane of the packed form, without a division slow path:
+// with r = 1/sqrt(1 + e) (rsqrtf, a few ulp), r - 1 = -e r / (1 + (1 + e) r),
+// which keeps the relative precision of a small e; the division is the fast
+// one (its denominator is near 2)
+__device__ __forceinline__ float inv_sqrt1p_m1_fast(float e) {
+    const float r = rsqrtf(1.f + e);
+    return __fdividef(-e * r, 1.f + (1.f + e) * r);
+}
+__device__ __forceinline__ P2 inv_sqrt1p_m1(P2 e) {
+    return P2(inv_sqrt1p_m1_fast(e.v.x), inv_sqrt1p_m1_fast(e.v.y));
 }
 
 // Gram-Schmidt reunitarisation of U = 1 + w, in deviation form
@@ -577,6 +594,14 @@ __device__ __forceinline__ H3<P2> pair_h(const H3<float> &a, const H3<float> &b)
     return h;
 }
 
+__device__ __forceinline__ M3<P2> swap_lanes(const M3<P2> &a) {
+    M3<P2> b;
+#pragma unroll
+    for (int k = 0; k < 9; k++)
+        b.m[k] = {P2(a.m[k].r.v.y, a.m[k].r.v.x), P2(a.m[k].i.v.y, a.m[k].i.v.x)};
+    return b;
+}
+
 __device__ __forceinline__ H3<float> lane_h(const H3<P2> &h, int y) {
     auto l = [&](P2 v) { return y ? lane_y(v) : lane_x(v); };
     H3<float> r;
@@ -591,62 +616,110 @@ __device__ __forceinline__ H3<float> lane_h(const H3<P2> &h, int y) {
 
 }  // namespace
 
-__device__ __forceinline__ void leapfrog_pair_site(int N, int ix, int iy, const State<float> &s,
-                                                   C<float> *ux_out, C<float> *uy_out,
-                                                   float *phi_out, const StepCoef<float> &cf) {
-    const size_t n = (size_t)N * N;
-    const size_t pos = (size_t)ix * N + iy;
-    const long pdx = (ix + 1 < N) ? N : 0, mdx = (ix > 0) ? -(long)N : 0;
-    const long pdy = (iy + 1 < N) ? 1 : 0, mdy = (iy > 0) ? -1 : 0;
+// Field selectors of the link loaders: lane x and lane y of a packed link
+// pair each come from Ux (kLx) or Uy (kLy) at a neighbour offset (dx, dy).
+constexpr int kLx = 0, kLy = 1;
 
-    const M3<P2> Ud = ld_m3_pair(s.ux, pos, s.uy, pos, n);
-    const H3<float> phi = ld_h(s.phi, pos, n);
-    H3<float> pi = ld_h(s.pi, pos, n);
-    H3<P2> Ed = pair_h(ld_h8(s.e1, pos, n), ld_h8(s.e2, pos, n));
+// Loads from the global planes, neighbours clamped at the lattice edge
+// (Lattice.cpp:19-28).
+struct PairLoadGlobal {
+    const State<float> &s;
+    size_t pos, n;
+    long ox[3], oy[3];  // index offsets of dx (dy) = -1, 0, +1, clamped
+    __device__ __forceinline__ PairLoadGlobal(const State<float> &s_, int N, int ix, int iy)
+        : s(s_), pos((size_t)ix * N + iy), n((size_t)N * N) {
+        ox[0] = ix > 0 ? -(long)N : 0;
+        ox[1] = 0;
+        ox[2] = ix + 1 < N ? N : 0;
+        oy[0] = iy > 0 ? -1 : 0;
+        oy[1] = 0;
+        oy[2] = iy + 1 < N ? 1 : 0;
+    }
+    template <int FA, int DXA, int DYA, int FB, int DXB, int DYB>
+    __device__ __forceinline__ M3<P2> links() const {
+        return ld_m3_pair(FA == kLy ? s.uy : s.ux, pos + ox[DXA + 1] + oy[DYA + 1],
+                          FB == kLy ? s.uy : s.ux, pos + ox[DXB + 1] + oy[DYB + 1], n);
+    }
+    template <int DX, int DY>
+    __device__ __forceinline__ H3<float> phi() const {
+        return ld_h(s.phi, pos + ox[DX + 1] + oy[DY + 1], n);
+    }
+    __device__ __forceinline__ H3<float> pi() const { return ld_h(s.pi, pos, n); }
+    __device__ __forceinline__ H3<float> e1() const { return ld_h8(s.e1, pos, n); }
+    __device__ __forceinline__ H3<float> e2() const { return ld_h8(s.e2, pos, n); }
+    // E and pi are site-local: written back in place
+    __device__ __forceinline__ void put_e(const H3<float> &a, const H3<float> &b) const {
+        st_h8(s.e1, pos, n, a);
+        st_h8(s.e2, pos, n, b);
+    }
+    __device__ __forceinline__ void put_pi(const H3<float> &h) const { st_h(s.pi, pos, n, h); }
+};
+
+// One site of the FP32 step, both directions in the packed lanes. Loads
+// through `ld` (global planes or a shared-memory tile), writes the new E and
+// pi through it (site-local, so they may go back in place at once) and
+// returns the new links (nu) and phi (phin) when cf.do_pu is set, for the
+// caller to store once no other thread reads the old ones.
+template <class Ld>
+__device__ __forceinline__ void leapfrog_pair_core(const Ld &ld, const StepCoef<float> &cf,
+                                                   M3<P2> &nu, H3<float> &phin) {
+    const M3<P2> Ud = ld.template links<kLx, 0, 0, kLy, 0, 0>();
+    const H3<float> phi = ld.template phi<0, 0>();
+    H3<float> pi = ld.pi();
+    H3<P2> Ed = pair_h(ld.e1(), ld.e2());
 
     if (cf.do_pe) {
         const H3<P2> phi2 = pair_h(phi, phi);
         H3<P2> stap;
         {
-            // P_do = (U_d U_o(+d)) (U_o U_d(+o))^dag
-            const M3<P2> Uo = ld_m3_pair(s.uy, pos, s.ux, pos, n);
-            const M3<P2> a = dmul(Ud, ld_m3_pair(s.uy, pos + pdx, s.ux, pos + pdy, n));
-            const M3<P2> b = dmul(Uo, ld_m3_pair(s.ux, pos + pdy, s.uy, pos + pdx, n));
-            stap = i_antiherm(dmul_nd(a, b));
+            // P_do = (U_d U_o(+d)) (U_o U_d(+o))^dag: lane x of a = U_d U_o(+d)
+            // is Ux Uy(+x), lane y is Uy Ux(+y); U_o U_d(+o) is the same pair
+            // of products with the lanes swapped
+            const M3<P2> a = dmul(Ud, ld.template links<kLy, 1, 0, kLx, 0, 1>());
+            stap = i_antiherm(dmul_nd(a, swap_lanes(a)));
         }
         {
             // S_d = (U_d U_o(+d-o)^dag) (U_d(-o)^dag U_o(-o))
-            const M3<P2> p = dmul_nd(Ud, ld_m3_pair(s.uy, pos + pdx + mdy, s.ux, pos + pdy + mdx, n));
-            const M3<P2> q = dmul_dn(ld_m3_pair(s.ux, pos + mdy, s.uy, pos + mdx, n),
-                                     ld_m3_pair(s.uy, pos + mdy, s.ux, pos + mdx, n));
+            const M3<P2> p = dmul_nd(Ud, ld.template links<kLy, 1, -1, kLx, -1, 1>());
+            const M3<P2> q = dmul_dn(ld.template links<kLx, 0, -1, kLy, -1, 0>(),
+                                     ld.template links<kLy, 0, -1, kLx, -1, 0>());
             h_add(stap, i_antiherm(dmul(p, q)));
         }
         h_traceless(stap);
-        const P2 cst = P2(cf.tau * cf.dt_pe / (2.f * cf.g * cf.g));
-        const P2 cdt = P2(cf.dt_pe / cf.tau);
+        const P2 cst = P2(cf.c_e);
+        const P2 cdt = P2(cf.c_pi);
         h_axpy(Ed, cst, stap);
-        const H3<P2> fp = pair_h(ld_h(s.phi, pos + pdx, n), ld_h(s.phi, pos + pdy, n));
+        const H3<P2> fp = pair_h(ld.template phi<1, 0>(), ld.template phi<0, 1>());
         H3<P2> br = transport_fwd_minus<P2, true>(Ud, fp, phi2);
         h_axpy(Ed, cdt, i_commutator(br, phi2));  // i[phi~ - phi, phi] = i[phi~, phi]
-        const H3<P2> fm = pair_h(ld_h(s.phi, pos + mdx, n), ld_h(s.phi, pos + mdy, n));
-        h_add(br, transport_bwd_minus<P2, true>(ld_m3_pair(s.ux, pos + mdx, s.uy, pos + mdy, n),
-                                                fm, phi2));
+        const H3<P2> fm = pair_h(ld.template phi<-1, 0>(), ld.template phi<0, -1>());
+        h_add(br, transport_bwd_minus<P2, true>(ld.template links<kLx, -1, 0, kLy, 0, -1>(), fm,
+                                                phi2));
         H3<float> brs = lane_h(br, 0);
         h_add(brs, lane_h(br, 1));
-        h_axpy(pi, cf.dt_pe / cf.tau, brs);
+        h_axpy(pi, cf.c_pi, brs);
         h_traceless(Ed);
-        st_h8(s.e1, pos, n, lane_h(Ed, 0));
-        st_h8(s.e2, pos, n, lane_h(Ed, 1));
-        st_h(s.pi, pos, n, pi);
+        ld.put_e(lane_h(Ed, 0), lane_h(Ed, 1));
+        ld.put_pi(pi);
     }
     if (cf.do_pu) {
-        const float c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / 2.f);
-        M3<P2> nu = taylor2_update_dev(Ed, P2(c), Ud);
+        nu = taylor2_update_dev(Ed, P2(cf.c_u), Ud);
         reunitarize_dev(nu);
-        st_m3_pair(ux_out, uy_out, pos, n, nu);
-        H3<float> phin = phi;
-        h_axpy(phin, (cf.tau + cf.dt_pu / 2.f) * cf.dt_pu, pi);
-        st_h(phi_out, pos, n, phin);
+        phin = phi;
+        h_axpy(phin, cf.c_phi, pi);
+    }
+}
+
+__device__ __forceinline__ void leapfrog_pair_site(int N, int ix, int iy, const State<float> &s,
+                                                   C<float> *ux_out, C<float> *uy_out,
+                                                   float *phi_out, const StepCoef<float> &cf) {
+    const PairLoadGlobal ld(s, N, ix, iy);
+    M3<P2> nu;
+    H3<float> phin;
+    leapfrog_pair_core(ld, cf, nu, phin);
+    if (cf.do_pu) {
+        st_m3_pair(ux_out, uy_out, ld.pos, ld.n, nu);
+        st_h(phi_out, ld.pos, ld.n, phin);
     }
 }
 
@@ -658,6 +731,304 @@ __global__ void __launch_bounds__(256, 1)
     const int iy = blockIdx.x * 32 + (threadIdx.x & 31);
     const int ix = blockIdx.y * 8 + (threadIdx.x >> 5);
     leapfrog_pair_site(ev->N, ix, iy, s, ux_out, uy_out, phi_out, cf);
+}
+
+// ---------------------------------------------------------------------------
+// FP32 step with the fields staged in shared memory by TMA. A persistent
+// block per SM walks tiles of 8 rows (x) x 32 columns (y), one thread per
+// site; the loads of tile i+2 are in flight while tile i is computed (two
+// stages). A stage holds, per tile,
+//   Ux, Uy   [9][10][36] complex   rows ix0-1 .. ix0+8, columns iy0-2 .. iy0+33
+//   phi      [9][10][40] real      rows ix0-1 .. ix0+8, columns iy0-4 .. iy0+35
+//   E1, E2   [8][8][32], pi [9][8][32]   the tile's own sites
+// (the column starts keep each box's first column 16-byte aligned, as TMA
+// requires). Boxes reaching past the lattice are zero filled; on edge tiles
+// the halo cells are then overwritten with the clamped neighbours
+// (Lattice.cpp:19-28), so every neighbour read is a fixed offset from the
+// thread's own cell. Results are written back into the same stage (E and pi
+// in place at once, links and phi after a barrier) and leave by TMA stores.
+// ---------------------------------------------------------------------------
+namespace tile {
+constexpr int R = 8, Cn = 32;            // tile rows (x) and columns (y)
+constexpr int UR = R + 2, UC = Cn + 4;   // link box
+constexpr int PR = R + 2, PC = Cn + 8;   // phi box
+constexpr int kU = UR * UC, kP = PR * PC, kS = R * Cn;  // component strides
+constexpr int round128(int b) { return (b + 127) / 128 * 128; }
+constexpr int UX = 0;
+constexpr int UY = UX + round128(9 * kU * 8);
+constexpr int PHI = UY + round128(9 * kU * 8);
+constexpr int E1 = PHI + round128(9 * kP * 4);
+constexpr int E2 = E1 + round128(8 * kS * 4);
+constexpr int PI = E2 + round128(8 * kS * 4);
+constexpr int STAGE = PI + round128(9 * kS * 4);
+constexpr uint32_t TX_BYTES = 2 * 9 * kU * 8 + 9 * kP * 4 + 2 * 8 * kS * 4 + 9 * kS * 4;
+constexpr int SMEM = 2 * STAGE + 64 + 128;  // two stages, barriers, alignment slack
+constexpr uint32_t MAX_POLLS = 1u << 22;
+static_assert(STAGE % 128 == 0, "stage alignment");
+static_assert(SMEM <= 227 * 1024, "shared memory per block");
+}  // namespace tile
+
+struct TileMaps {
+    CUtensorMap ux_in, uy_in, phi_in;     // load boxes with halo
+    CUtensorMap ux_out, uy_out, phi_out;  // store boxes (the tile)
+    CUtensorMap e1, e2, pi;               // the tile, loaded and stored in place
+};
+
+// 32-bit shared-memory accesses by address: one value per instruction, so
+// each lands directly in its lane of a packed pair
+__device__ __forceinline__ float lds_f32(uint32_t a) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ void sts_f32(uint32_t a, float v) {
+    asm volatile("st.shared.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+
+// Loads from one stage; the thread sits at row r, column c of the tile.
+// Addresses are a per-thread base plus compile-time offsets: bu and bp point
+// at the (-1, -1) corner of the thread's 3 x 3 neighbourhood in the link and
+// phi boxes, bs at its cell of the site-local boxes. Imaginary parts of links
+// are read through bi = bu + imag, with imag (= 4) a kernel argument: were the
+// adjacency of a link's real and imaginary parts visible, the compiler would
+// fuse the two 32-bit loads into one 64-bit load, whose register pair is
+// (re, im) of one link while the packed arithmetic needs (re, re) of the two
+// lanes, and every use would then be preceded by moves (measured: 35 M
+// instructions a step at 512^2 instead of 18.5 M).
+struct PairLoadTile {
+    uint32_t bu, bi, bp, bs;
+    __device__ __forceinline__ PairLoadTile(uint32_t stage, int r, int c, uint32_t imag)
+        : bu(stage + (uint32_t)((r * tile::UC + c + 1) * 8)),
+          bi(stage + (uint32_t)((r * tile::UC + c + 1) * 8) + imag),
+          bp(stage + tile::PHI + (uint32_t)((r * tile::PC + c + 3) * 4)),
+          bs(stage + (uint32_t)((r * tile::Cn + c) * 4)) {}
+    template <int FA, int DXA, int DYA, int FB, int DXB, int DYB>
+    __device__ __forceinline__ M3<P2> links() const {
+        constexpr uint32_t oa =
+            (FA == kLy ? tile::UY : tile::UX) + ((DXA + 1) * tile::UC + DYA + 1) * 8;
+        constexpr uint32_t ob =
+            (FB == kLy ? tile::UY : tile::UX) + ((DXB + 1) * tile::UC + DYB + 1) * 8;
+        M3<P2> m;
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            const uint32_t o = k * tile::kU * 8;
+            m.m[k] = {P2(lds_f32(bu + oa + o), lds_f32(bu + ob + o)),
+                      P2(lds_f32(bi + oa + o), lds_f32(bi + ob + o))};
+        }
+        return m;
+    }
+    static __device__ __forceinline__ H3<float> h9(uint32_t a, uint32_t stride) {
+        H3<float> h;
+        h.d0 = lds_f32(a);
+        h.d1 = lds_f32(a + stride);
+        h.d2 = lds_f32(a + 2 * stride);
+        h.o01 = {lds_f32(a + 3 * stride), lds_f32(a + 4 * stride)};
+        h.o02 = {lds_f32(a + 5 * stride), lds_f32(a + 6 * stride)};
+        h.o12 = {lds_f32(a + 7 * stride), lds_f32(a + 8 * stride)};
+        return h;
+    }
+    static __device__ __forceinline__ H3<float> h8(uint32_t a) {
+        constexpr uint32_t S = tile::kS * 4;
+        H3<float> h;
+        h.d0 = lds_f32(a);
+        h.d1 = lds_f32(a + S);
+        h.d2 = -(h.d0 + h.d1);
+        h.o01 = {lds_f32(a + 2 * S), lds_f32(a + 3 * S)};
+        h.o02 = {lds_f32(a + 4 * S), lds_f32(a + 5 * S)};
+        h.o12 = {lds_f32(a + 6 * S), lds_f32(a + 7 * S)};
+        return h;
+    }
+    template <int DX, int DY>
+    __device__ __forceinline__ H3<float> phi() const {
+        return h9(bp + ((DX + 1) * tile::PC + DY + 1) * 4, tile::kP * 4);
+    }
+    __device__ __forceinline__ H3<float> pi() const { return h9(bs + tile::PI, tile::kS * 4); }
+    __device__ __forceinline__ H3<float> e1() const { return h8(bs + tile::E1); }
+    __device__ __forceinline__ H3<float> e2() const { return h8(bs + tile::E2); }
+    static __device__ __forceinline__ void put_h8(uint32_t a, const H3<float> &h) {
+        constexpr uint32_t S = tile::kS * 4;
+        sts_f32(a, h.d0);
+        sts_f32(a + S, h.d1);
+        sts_f32(a + 2 * S, h.o01.r);
+        sts_f32(a + 3 * S, h.o01.i);
+        sts_f32(a + 4 * S, h.o02.r);
+        sts_f32(a + 5 * S, h.o02.i);
+        sts_f32(a + 6 * S, h.o12.r);
+        sts_f32(a + 7 * S, h.o12.i);
+    }
+    static __device__ __forceinline__ void put_h9(uint32_t a, const H3<float> &h) {
+        constexpr uint32_t S = tile::kS * 4;
+        sts_f32(a, h.d0);
+        sts_f32(a + S, h.d1);
+        sts_f32(a + 2 * S, h.d2);
+        sts_f32(a + 3 * S, h.o01.r);
+        sts_f32(a + 4 * S, h.o01.i);
+        sts_f32(a + 5 * S, h.o02.r);
+        sts_f32(a + 6 * S, h.o02.i);
+        sts_f32(a + 7 * S, h.o12.r);
+        sts_f32(a + 8 * S, h.o12.i);
+    }
+    // E and pi go back in place: only this thread reads its own cells
+    __device__ __forceinline__ void put_e(const H3<float> &a, const H3<float> &b) const {
+        put_h8(bs + tile::E1, a);
+        put_h8(bs + tile::E2, b);
+    }
+    __device__ __forceinline__ void put_pi(const H3<float> &h) const { put_h9(bs + tile::PI, h); }
+};
+
+// Edge tiles: halo cells outside the lattice take the clamped neighbour,
+// each coordinate clamped on its own (corners included). Sources are cells of
+// the lattice, which no thread writes here, so one pass suffices.
+__device__ __forceinline__ void fill_edge_halo(unsigned char *st, bool top, bool bottom, bool left,
+                                               bool right) {
+    // destination cells: link box rows 0 / UR-1 over columns 1..UC-2, columns
+    // 1 / UC-2 over rows 0..UR-1; the phi box the same with columns 3..PC-4
+    constexpr int UROW = tile::UC - 2, UCOL = tile::UR;  // cells per halo row / column
+    constexpr int PROW = tile::PC - 8 + 2, PCOL = tile::PR;
+    constexpr int UCELLS = 2 * UROW + 2 * UCOL, PCELLS = 2 * PROW + 2 * PCOL;
+    C<float> *ux = reinterpret_cast<C<float> *>(st + tile::UX);
+    C<float> *uy = reinterpret_cast<C<float> *>(st + tile::UY);
+    float *ph = reinterpret_cast<float *>(st + tile::PHI);
+    for (int w = threadIdx.x; w < 9 * (UCELLS + PCELLS); w += blockDim.x) {
+        const int k = w / (UCELLS + PCELLS);
+        int cell = w - k * (UCELLS + PCELLS);
+        const bool link = cell < UCELLS;
+        if (!link) cell -= UCELLS;
+        const int nrow = link ? UROW : PROW, ncol = link ? UCOL : PCOL;
+        const int rows = link ? tile::UR : tile::PR, cols = link ? tile::UC : tile::PC;
+        const int c_lo = link ? 1 : 3, c_hi = cols - c_lo - 1;  // halo columns
+        int j, m;
+        bool edge;
+        if (cell < 2 * nrow) {
+            const int side = cell / nrow;
+            j = side ? rows - 1 : 0;
+            m = c_lo + cell % nrow;
+            edge = side ? bottom : top;
+        } else {
+            cell -= 2 * nrow;
+            const int side = cell / ncol;
+            j = cell % ncol;
+            m = side ? c_hi : c_lo;
+            edge = side ? right : left;
+        }
+        if (!edge) continue;
+        int sj = j, sm = m;
+        if (top && j == 0) sj = 1;
+        if (bottom && j == rows - 1) sj = rows - 2;
+        if (left && m == c_lo) sm = c_lo + 1;
+        if (right && m == c_hi) sm = c_hi - 1;
+        if (link) {
+            const int d = k * tile::kU + j * cols + m, s = k * tile::kU + sj * cols + sm;
+            ux[d] = ux[s];
+            uy[d] = uy[s];
+        } else {
+            ph[k * tile::kP + j * cols + m] = ph[k * tile::kP + sj * cols + sm];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256, 1)
+    k_leapfrog_tile(const __grid_constant__ TileMaps maps, int N, StepCoef<float> cf,
+                    double *status, uint32_t imag) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // 128-byte aligned start, kept as an offset into the shared array so that
+    // accesses through it stay shared-memory accesses
+    const uint32_t pad = (128u - (smem_addr(smem_raw) & 127u)) & 127u;
+    unsigned char *smem = smem_raw + pad;
+    const uint32_t sbase = smem_addr(smem);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + 2 * tile::STAGE);
+    int *abort_flag = reinterpret_cast<int *>(full + 2);
+    const int tiles_y = N / tile::Cn, tiles_x = N / tile::R, tiles = tiles_x * tiles_y;
+    const int tid = threadIdx.x, r = tid >> 5, c = tid & 31;
+
+    auto issue = [&](int t, int s) {
+        const int iy0 = (t % tiles_y) * tile::Cn, ix0 = (t / tiles_y) * tile::R;
+        unsigned char *st = smem + s * tile::STAGE;
+        mbar_arrive_expect_tx(&full[s], tile::TX_BYTES);
+        tma_load_3d(st + tile::UX, &maps.ux_in, iy0 - 2, ix0 - 1, 0, &full[s]);
+        tma_load_3d(st + tile::UY, &maps.uy_in, iy0 - 2, ix0 - 1, 0, &full[s]);
+        tma_load_3d(st + tile::PHI, &maps.phi_in, iy0 - 4, ix0 - 1, 0, &full[s]);
+        tma_load_3d(st + tile::E1, &maps.e1, iy0, ix0, 0, &full[s]);
+        tma_load_3d(st + tile::E2, &maps.e2, iy0, ix0, 0, &full[s]);
+        tma_load_3d(st + tile::PI, &maps.pi, iy0, ix0, 0, &full[s]);
+    };
+
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        *abort_flag = 0;
+        fence_barrier_init();
+        prefetch_map(&maps.ux_in);
+        prefetch_map(&maps.uy_in);
+        prefetch_map(&maps.phi_in);
+        if (blockIdx.x < tiles) issue(blockIdx.x, 0);
+        if (blockIdx.x + gridDim.x < tiles) issue(blockIdx.x + gridDim.x, 1);
+    }
+    __syncthreads();
+
+    int i = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, i++) {
+        const int s = i & 1;
+        unsigned char *st = smem + s * tile::STAGE;
+        if (!mbar_wait_bounded(&full[s], (i >> 1) & 1, tile::MAX_POLLS)) *abort_flag = 1;
+        __syncthreads();
+        if (*abort_flag) break;
+        const int ty = t % tiles_y, tx = t / tiles_y;
+        const bool top = tx == 0, bottom = tx == tiles_x - 1;
+        const bool left = ty == 0, right = ty == tiles_y - 1;
+        if (top || bottom || left || right) {
+            fill_edge_halo(st, top, bottom, left, right);
+            __syncthreads();
+        }
+
+        const uint32_t sst = sbase + (uint32_t)(s * tile::STAGE);
+        const PairLoadTile ld(sst, r, c, imag);
+        M3<P2> nu;
+        H3<float> phin;
+        leapfrog_pair_core(ld, cf, nu, phin);
+        __syncthreads();  // every read of this stage's links and phi is done
+        if (cf.do_pu) {
+            // the new links [9][8][32] over the link boxes, phi over the phi box
+            const uint32_t o = sst + (uint32_t)((r * tile::Cn + c) * 8);
+#pragma unroll
+            for (int k = 0; k < 9; k++) {
+                const uint32_t ok = o + k * tile::kS * 8;
+                sts_f32(ok + tile::UX, lane_x(nu.m[k].r));
+                sts_f32(ok + tile::UX + 4, lane_x(nu.m[k].i));
+                sts_f32(ok + tile::UY, lane_y(nu.m[k].r));
+                sts_f32(ok + tile::UY + 4, lane_y(nu.m[k].i));
+            }
+            PairLoadTile::put_h9(sst + tile::PHI + (uint32_t)((r * tile::Cn + c) * 4), phin);
+        }
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            const int iy0 = ty * tile::Cn, ix0 = tx * tile::R;
+            if (cf.do_pe) {
+                tma_store_3d(&maps.e1, iy0, ix0, 0, st + tile::E1);
+                tma_store_3d(&maps.e2, iy0, ix0, 0, st + tile::E2);
+                tma_store_3d(&maps.pi, iy0, ix0, 0, st + tile::PI);
+            }
+            if (cf.do_pu) {
+                tma_store_3d(&maps.ux_out, iy0, ix0, 0, st + tile::UX);
+                tma_store_3d(&maps.uy_out, iy0, ix0, 0, st + tile::UY);
+                tma_store_3d(&maps.phi_out, iy0, ix0, 0, st + tile::PHI);
+            }
+            bulk_commit();
+            // the stage is reloaded only after the stores have read it
+            bulk_wait_read_all();
+            if (t + 2 * (int)gridDim.x < tiles) issue(t + 2 * gridDim.x, s);
+        }
+    }
+    if (tid == 0) {
+        bulk_wait_all();
+        if (*abort_flag) {
+            // a load that never completed: report it, and give any other load
+            // in flight a bounded chance to land before the block exits
+            if (status) *status = 1.0;
+            mbar_wait_bounded(&full[(i + 1) & 1], ((i + 1) >> 1) & 1, tile::MAX_POLLS);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -773,23 +1144,94 @@ void launch_leapfrog_site(const EventGeom *d_ev, int N, const State<T> &s,
                           C<T> *ux_out, C<T> *uy_out, T *phi_out,
                           const StepCoef<T> &cf, bool reunit, cudaStream_t st);
 
+bool encode_tiled_3d(CUtensorMap *map, void *base, CUtensorMapDataType type, size_t esize,
+                     uint64_t d0, uint64_t d1, uint64_t d2, uint32_t b0, uint32_t b1,
+                     uint32_t b2) {
+    static const PFN_cuTensorMapEncodeTiled_v12000 encode = [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            fn = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }();
+    if (!encode) return false;
+    const cuuint64_t dims[3] = {d0, d1, d2};
+    const cuuint64_t strides[2] = {d0 * esize, d0 * d1 * esize};
+    const cuuint32_t box[3] = {b0, b1, b2};
+    const cuuint32_t unit[3] = {1, 1, 1};
+    return encode(map, type, 3, base, dims, strides, box, unit, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+namespace {
+
+// The FP32 form's step kernel: the TMA-staged tile kernel unless
+// IPG_FP32_KERNEL=pair selects the plain-load kernel (both run the same
+// per-site code and give the same bits).
+bool use_tile_kernel() {
+    static const bool tile = [] {
+        const char *e = std::getenv("IPG_FP32_KERNEL");
+        return !(e && std::strcmp(e, "pair") == 0);
+    }();
+    return tile;
+}
+
+// false if a tensor map could not be encoded (nothing launched)
+bool launch_leapfrog_tile(int N, const State<float> &s, C<float> *ux_out, C<float> *uy_out,
+                          float *phi_out, const StepCoef<float> &cf, double *status,
+                          cudaStream_t st) {
+    using namespace tile;
+    const uint64_t n = (uint64_t)N;
+    const auto U64 = CU_TENSOR_MAP_DATA_TYPE_UINT64, U32 = CU_TENSOR_MAP_DATA_TYPE_UINT32;
+    TileMaps m;
+    const bool ok =
+        encode_tiled_3d(&m.ux_in, s.ux, U64, 8, n, n, 9, UC, UR, 9) &&
+        encode_tiled_3d(&m.uy_in, s.uy, U64, 8, n, n, 9, UC, UR, 9) &&
+        encode_tiled_3d(&m.phi_in, s.phi, U32, 4, n, n, 9, PC, PR, 9) &&
+        encode_tiled_3d(&m.ux_out, ux_out, U64, 8, n, n, 9, Cn, R, 9) &&
+        encode_tiled_3d(&m.uy_out, uy_out, U64, 8, n, n, 9, Cn, R, 9) &&
+        encode_tiled_3d(&m.phi_out, phi_out, U32, 4, n, n, 9, Cn, R, 9) &&
+        encode_tiled_3d(&m.e1, s.e1, U32, 4, n, n, 8, Cn, R, 8) &&
+        encode_tiled_3d(&m.e2, s.e2, U32, 4, n, n, 8, Cn, R, 8) &&
+        encode_tiled_3d(&m.pi, s.pi, U32, 4, n, n, 9, Cn, R, 9);
+    if (!ok) return false;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(k_leapfrog_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    const int tiles = (N / R) * (N / Cn);
+    // imag = 4: the byte offset of a link's imaginary part
+    k_leapfrog_tile<<<tiles < sms ? tiles : sms, 256, SMEM, st>>>(m, N, cf, status, 4u);
+    return true;
+}
+
+}  // namespace
+
 template <typename T>
 void launch_leapfrog(const EventGeom *d_ev, int N, const State<T> &s,
                      C<T> *ux_out, C<T> *uy_out, T *phi_out,
-                     const StepCoef<T> &cf, bool reunit, cudaStream_t st) {
+                     const StepCoef<T> &cf, bool reunit, cudaStream_t st, double *status) {
     // FP64 runs one thread per site: at 512^2 it takes 97 us a step against
     // 108 us for the direction split (both FP64-pipe and latency bound at one
     // 256-thread block per SM). FP32 runs both directions of a site in the
-    // two lanes of packed FP32 instructions (k_leapfrog_pair).
+    // two lanes of packed FP32 instructions, from shared-memory tiles filled
+    // by TMA (k_leapfrog_tile) or from plain loads (k_leapfrog_pair).
     if constexpr (sizeof(T) == 4) {
         if (N >= 32) {
-            // N is a power of two >= 32: the grid covers the lattice exactly
+            // N is a power of two >= 32: the tiles cover the lattice exactly
             (void)reunit;
+            if (use_tile_kernel() &&
+                launch_leapfrog_tile(N, s, ux_out, uy_out, phi_out, cf, status, st))
+                return;
             k_leapfrog_pair<<<dim3(N / 32, N / 8), 256, 0, st>>>(d_ev, s, ux_out, uy_out, phi_out,
                                                                  cf);
             return;
         }
     }
+    (void)status;
     launch_leapfrog_site(d_ev, N, s, ux_out, uy_out, phi_out, cf, reunit, st);
 }
 
@@ -815,15 +1257,11 @@ void launch_leapfrog_site(const EventGeom *d_ev, int N, const State<T> &s,
     }
 }
 
-template void launch_leapfrog<double>(const EventGeom *, int,
-                                      const State<double> &, C<double> *,
-                                      C<double> *, double *,
-                                      const StepCoef<double> &, bool,
-                                      cudaStream_t);
-template void launch_leapfrog<float>(const EventGeom *, int,
-                                     const State<float> &, C<float> *,
-                                     C<float> *, float *,
-                                     const StepCoef<float> &, bool,
-                                     cudaStream_t);
+template void launch_leapfrog<double>(const EventGeom *, int, const State<double> &,
+                                      C<double> *, C<double> *, double *,
+                                      const StepCoef<double> &, bool, cudaStream_t, double *);
+template void launch_leapfrog<float>(const EventGeom *, int, const State<float> &, C<float> *,
+                                     C<float> *, float *, const StepCoef<float> &, bool,
+                                     cudaStream_t, double *);
 
 }  // namespace ipg

@@ -27,12 +27,29 @@ struct StepCoef {
     T g;
     int do_pe;
     int do_pu;
+    // derived on the host by set_derived, in T arithmetic (the FP32 kernels
+    // read these instead of dividing per thread)
+    T c_e;    // tau dt_pe / (2 g^2): staple term of E
+    T c_pi;   // dt_pe / tau: bracket term of pi and commutator term of E
+    T c_u;    // g^2 dt_pu / (tau + dt_pu/2): the U update's X = i c_u E
+    T c_phi;  // (tau + dt_pu/2) dt_pu: the phi update
 };
 
 template <typename T>
+inline void set_derived(StepCoef<T> &cf) {
+    cf.c_e = cf.tau * cf.dt_pe / (T(2) * cf.g * cf.g);
+    cf.c_pi = cf.dt_pe / cf.tau;
+    cf.c_u = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / T(2));
+    cf.c_phi = (cf.tau + cf.dt_pu / T(2)) * cf.dt_pu;
+}
+
+// status (may be null): set to 1 if a wait of the FP32 tile kernel hit its
+// limit (the step is then incomplete)
+template <typename T>
 void launch_leapfrog(const EventGeom *d_ev, int N, const State<T> &s,
                      C<T> *ux_out, C<T> *uy_out, T *phi_out,
-                     const StepCoef<T> &cf, bool reunit, cudaStream_t st);
+                     const StepCoef<T> &cf, bool reunit, cudaStream_t st,
+                     double *status = nullptr);
 
 // One event of a batched leapfrog launch: its buffers for this step and its
 // step coefficients (inactive events are skipped).
