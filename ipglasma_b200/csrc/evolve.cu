@@ -85,7 +85,7 @@ template <typename T>
 __device__ __forceinline__ M3<T> taylor2_update(const H3<T> &e, T c,
                                                 const M3<T> &u) {
     M3<T> em = from_h(e);
-    M3<T> e2 = mul(em, em);
+    M3<T> e2 = mul_g<false, false, true, true>(em, em);
     M3<T> t;
     const T h = T(-0.5) * c * c;
 #pragma unroll
@@ -100,54 +100,84 @@ __device__ __forceinline__ M3<T> taylor2_update(const H3<T> &e, T c,
     return mul(t, u);
 }
 
-// one site (ix, iy) in full-matrix storage (the FP64 plain form)
-template <typename T, bool REUNIT>
-__device__ __forceinline__ void leapfrog_full_site(int N, int ix, int iy, const State<T> &s,
-                                                   C<T> *ux_out, C<T> *uy_out, T *phi_out,
-                                                   const StepCoef<T> &cf) {
-    const size_t n = (size_t)N * N;
-    const size_t pos = (size_t)ix * N + iy;
+// Field selectors of the link loaders: a link (or lane of a packed link
+// pair) comes from Ux (kLx) or Uy (kLy) at a neighbour offset (dx, dy).
+constexpr int kLx = 0, kLy = 1;
 
+// Full-matrix loads from the global planes, neighbours clamped at the lattice
+// edge (Lattice.cpp:19-28); E and pi are site-local and written back in place.
+template <typename T>
+struct FullLoadGlobal {
+    const State<T> &s;
+    size_t pos, n;
+    long ox[3], oy[3];  // index offsets of dx (dy) = -1, 0, +1, clamped
+    __device__ __forceinline__ FullLoadGlobal(const State<T> &s_, int N, int ix, int iy)
+        : s(s_), pos((size_t)ix * N + iy), n((size_t)N * N) {
+        ox[0] = ix > 0 ? -(long)N : 0;
+        ox[1] = 0;
+        ox[2] = ix + 1 < N ? N : 0;
+        oy[0] = iy > 0 ? -1 : 0;
+        oy[1] = 0;
+        oy[2] = iy + 1 < N ? 1 : 0;
+    }
+    template <int F, int DX, int DY>
+    __device__ __forceinline__ M3<T> link() const {
+        return ld_m3(F == kLy ? s.uy : s.ux, pos + ox[DX + 1] + oy[DY + 1], n);
+    }
+    template <int DX, int DY>
+    __device__ __forceinline__ H3<T> phi() const {
+        return ld_h(s.phi, pos + ox[DX + 1] + oy[DY + 1], n);
+    }
+    __device__ __forceinline__ H3<T> pi() const { return ld_h(s.pi, pos, n); }
+    __device__ __forceinline__ H3<T> e1() const { return ld_h8(s.e1, pos, n); }
+    __device__ __forceinline__ H3<T> e2() const { return ld_h8(s.e2, pos, n); }
+    __device__ __forceinline__ void put_e(const H3<T> &a, const H3<T> &b) const {
+        st_h8(s.e1, pos, n, a);
+        st_h8(s.e2, pos, n, b);
+    }
+    __device__ __forceinline__ void put_pi(const H3<T> &h) const { st_h(s.pi, pos, n, h); }
+};
+
+// One site in full-matrix storage (the FP64 plain form): loads through `ld`,
+// writes the new pi and E through it and returns the new links and phi when
+// cf.do_pu is set.
+template <typename T, bool REUNIT, class Ld>
+__device__ __forceinline__ void leapfrog_full_core(const Ld &ld, const StepCoef<T> &cf,
+                                                   M3<T> &nx, M3<T> &ny, H3<T> &phin) {
     if (cf.do_pe) {
-        const int ixp = min(N - 1, ix + 1), ixm = max(0, ix - 1);
-        const int iyp = min(N - 1, iy + 1), iym = max(0, iy - 1);
-        const size_t pX = (size_t)ixp * N + iy, mX = (size_t)ixm * N + iy;
-        const size_t pY = (size_t)ix * N + iyp, mY = (size_t)ix * N + iym;
-        const size_t mXpY = (size_t)ixm * N + iyp, pXmY = (size_t)ixp * N + iym;
-
-        const M3<T> ux = ld_m3(s.ux, pos, n);
-        const M3<T> uy = ld_m3(s.uy, pos, n);
+        const M3<T> ux = ld.template link<kLx, 0, 0>();
+        const M3<T> uy = ld.template link<kLy, 0, 0>();
 
         // plaquette U12 = Ux Uy(x+1) Ux(y+1)^dag Uy^dag  (Evolution.cpp:228-232)
         H3<T> h12;
         {
-            M3<T> a = mul(ux, ld_m3(s.uy, pX, n));
-            M3<T> b = mul(uy, ld_m3(s.ux, pY, n));
+            M3<T> a = mul(ux, ld.template link<kLy, 1, 0>());
+            M3<T> b = mul(uy, ld.template link<kLx, 0, 1>());
             M3<T> u12 = mul_nd(a, b);
             h12 = i_antiherm(u12);
         }
         // E1 staple sum: U12 + U1m2 - h.c.  (234-257)
         H3<T> t1 = h12;
         {
-            M3<T> p = mul_nd(ux, ld_m3(s.uy, pXmY, n));
-            M3<T> q = mul_dn(ld_m3(s.ux, mY, n), ld_m3(s.uy, mY, n));
+            M3<T> p = mul_nd(ux, ld.template link<kLy, 1, -1>());
+            M3<T> q = mul_dn(ld.template link<kLx, 0, -1>(), ld.template link<kLy, 0, -1>());
             h_add(t1, i_antiherm_mul(p, q));
         }
         // E2 staple sum: U12^dag + U2m1 - h.c.  (240-244, 266-275)
         H3<T> t2;
         {
-            M3<T> p = mul_nd(uy, ld_m3(s.ux, mXpY, n));
-            M3<T> q = mul_dn(ld_m3(s.uy, mX, n), ld_m3(s.ux, mX, n));
+            M3<T> p = mul_nd(uy, ld.template link<kLx, -1, 1>());
+            M3<T> q = mul_dn(ld.template link<kLy, -1, 0>(), ld.template link<kLx, -1, 0>());
             t2 = i_antiherm_mul(p, q);
             h_axpy(t2, T(-1), h12);
         }
         h_traceless(t1);
         h_traceless(t2);
 
-        const H3<T> phi = ld_h(s.phi, pos, n);
-        H3<T> pi = ld_h(s.pi, pos, n);
-        H3<T> e1 = ld_h8(s.e1, pos, n);
-        H3<T> e2 = ld_h8(s.e2, pos, n);
+        const H3<T> phi = ld.template phi<0, 0>();
+        H3<T> pi = ld.pi();
+        H3<T> e1 = ld.e1();
+        H3<T> e2 = ld.e2();
         const T cst = cf.tau * cf.dt_pe / (T(2) * cf.g * cf.g);
         const T cdt = cf.dt_pe / cf.tau;
         h_axpy(e1, cst, t1);
@@ -156,50 +186,59 @@ __device__ __forceinline__ void leapfrog_full_site(int N, int ix, int iy, const 
         // parallel transports of phi (evolvePi 139-157, evolveE 221-223, 278-279)
         H3<T> br;
         {
-            H3<T> phx = conj_h(ux, ld_h(s.phi, pX, n));
+            H3<T> phx = conj_h(ux, ld.template phi<1, 0>());
             h_axpy(e1, cdt, i_commutator(phx, phi));
             br = phx;
         }
         {
-            H3<T> phy = conj_h(uy, ld_h(s.phi, pY, n));
+            H3<T> phy = conj_h(uy, ld.template phi<0, 1>());
             h_axpy(e2, cdt, i_commutator(phy, phi));
             h_add(br, phy);
         }
-        h_add(br, conj_h_dag(ld_m3(s.ux, mX, n), ld_h(s.phi, mX, n)));
-        h_add(br, conj_h_dag(ld_m3(s.uy, mY, n), ld_h(s.phi, mY, n)));
+        h_add(br, conj_h_dag(ld.template link<kLx, -1, 0>(), ld.template phi<-1, 0>()));
+        h_add(br, conj_h_dag(ld.template link<kLy, 0, -1>(), ld.template phi<0, -1>()));
         h_axpy(br, T(-4), phi);
         h_axpy(pi, cdt, br);
         h_traceless(e1);
         h_traceless(e2);
-        st_h(s.pi, pos, n, pi);
-        st_h8(s.e1, pos, n, e1);
-        st_h8(s.e2, pos, n, e2);
+        ld.put_pi(pi);
+        ld.put_e(e1, e2);
 
         if (cf.do_pu) {
-            H3<T> phin = phi;
+            phin = phi;
             h_axpy(phin, (cf.tau + cf.dt_pu / T(2)) * cf.dt_pu, pi);
-            st_h(phi_out, pos, n, phin);
             const T c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / T(2));
-            M3<T> nx = taylor2_update(e1, c, ux);
+            nx = taylor2_update(e1, c, ux);
             if (REUNIT) reunitarize(nx);
-            st_m3(ux_out, pos, n, nx);
-            M3<T> ny = taylor2_update(e2, c, uy);
+            ny = taylor2_update(e2, c, uy);
             if (REUNIT) reunitarize(ny);
-            st_m3(uy_out, pos, n, ny);
         }
     } else if (cf.do_pu) {
         // phi and U only (the tau = 0 half step, Evolution.cpp:393-394)
-        H3<T> phin = ld_h(s.phi, pos, n);
-        const H3<T> pi = ld_h(s.pi, pos, n);
+        phin = ld.template phi<0, 0>();
+        const H3<T> pi = ld.pi();
         h_axpy(phin, (cf.tau + cf.dt_pu / T(2)) * cf.dt_pu, pi);
-        st_h(phi_out, pos, n, phin);
         const T c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / T(2));
-        M3<T> nx = taylor2_update(ld_h8(s.e1, pos, n), c, ld_m3(s.ux, pos, n));
+        nx = taylor2_update(ld.e1(), c, ld.template link<kLx, 0, 0>());
         if (REUNIT) reunitarize(nx);
-        st_m3(ux_out, pos, n, nx);
-        M3<T> ny = taylor2_update(ld_h8(s.e2, pos, n), c, ld_m3(s.uy, pos, n));
+        ny = taylor2_update(ld.e2(), c, ld.template link<kLy, 0, 0>());
         if (REUNIT) reunitarize(ny);
-        st_m3(uy_out, pos, n, ny);
+    }
+}
+
+// one site (ix, iy) from the global planes
+template <typename T, bool REUNIT>
+__device__ __forceinline__ void leapfrog_full_site(int N, int ix, int iy, const State<T> &s,
+                                                   C<T> *ux_out, C<T> *uy_out, T *phi_out,
+                                                   const StepCoef<T> &cf) {
+    const FullLoadGlobal<T> ld(s, N, ix, iy);
+    M3<T> nx, ny;
+    H3<T> phin;
+    leapfrog_full_core<T, REUNIT>(ld, cf, nx, ny, phin);
+    if (cf.do_pu) {
+        st_h(phi_out, ld.pos, ld.n, phin);
+        st_m3(ux_out, ld.pos, ld.n, nx);
+        st_m3(uy_out, ld.pos, ld.n, ny);
     }
 }
 
@@ -253,7 +292,7 @@ __device__ __forceinline__ M3<T> dmul_dn(const M3<T> &a, const M3<T> &b) {
 // X + X^dag + X w^dag with X = w H
 template <typename T>
 __device__ __forceinline__ H3<T> transport_dev(const M3<T> &w, const H3<T> &h) {
-    const M3<T> x = mul(w, from_h(h));
+    const M3<T> x = mul_g<false, false, false, true>(w, from_h(h));
     const M3<T> y = mul_nd(x, w);
     H3<T> o;
     o.d0 = T(2) * x.m[0].r + y.m[0].r;
@@ -267,7 +306,7 @@ __device__ __forceinline__ H3<T> transport_dev(const M3<T> &w, const H3<T> &h) {
 // connection part of (1+w)^dag H (1+w): X + X^dag + w^dag X with X = H w
 template <typename T>
 __device__ __forceinline__ H3<T> transport_dev_back(const M3<T> &w, const H3<T> &h) {
-    const M3<T> x = mul(from_h(h), w);
+    const M3<T> x = mul_g<false, false, true, false>(from_h(h), w);
     const M3<T> y = mul_dn(w, x);
     H3<T> o;
     o.d0 = T(2) * x.m[0].r + y.m[0].r;
@@ -364,7 +403,7 @@ template <typename T>
 __device__ __forceinline__ M3<T> taylor2_update_dev(const H3<T> &e, T c,
                                                     const M3<T> &w) {
     const M3<T> em = from_h(e);
-    const M3<T> e2 = mul(em, em);
+    const M3<T> e2 = mul_g<false, false, true, true>(em, em);
     M3<T> t;
     const T h = T(-0.5) * c * c;
 #pragma unroll
@@ -615,10 +654,6 @@ __device__ __forceinline__ H3<float> lane_h(const H3<P2> &h, int y) {
 }
 
 }  // namespace
-
-// Field selectors of the link loaders: lane x and lane y of a packed link
-// pair each come from Ux (kLx) or Uy (kLy) at a neighbour offset (dx, dy).
-constexpr int kLx = 0, kLy = 1;
 
 // Loads from the global planes, neighbours clamped at the lattice edge
 // (Lattice.cpp:19-28).
@@ -878,51 +913,50 @@ struct PairLoadTile {
 
 // Edge tiles: halo cells outside the lattice take the clamped neighbour,
 // each coordinate clamped on its own (corners included). Sources are cells of
-// the lattice, which no thread writes here, so one pass suffices.
-__device__ __forceinline__ void fill_edge_halo(unsigned char *st, bool top, bool bottom, bool left,
-                                               bool right) {
-    // destination cells: link box rows 0 / UR-1 over columns 1..UC-2, columns
-    // 1 / UC-2 over rows 0..UR-1; the phi box the same with columns 3..PC-4
-    constexpr int UROW = tile::UC - 2, UCOL = tile::UR;  // cells per halo row / column
-    constexpr int PROW = tile::PC - 8 + 2, PCOL = tile::PR;
-    constexpr int UCELLS = 2 * UROW + 2 * UCOL, PCELLS = 2 * PROW + 2 * PCOL;
-    C<float> *ux = reinterpret_cast<C<float> *>(st + tile::UX);
-    C<float> *uy = reinterpret_cast<C<float> *>(st + tile::UY);
-    float *ph = reinterpret_cast<float *>(st + tile::PHI);
-    for (int w = threadIdx.x; w < 9 * (UCELLS + PCELLS); w += blockDim.x) {
-        const int k = w / (UCELLS + PCELLS);
-        int cell = w - k * (UCELLS + PCELLS);
-        const bool link = cell < UCELLS;
-        if (!link) cell -= UCELLS;
-        const int nrow = link ? UROW : PROW, ncol = link ? UCOL : PCOL;
-        const int rows = link ? tile::UR : tile::PR, cols = link ? tile::UC : tile::PC;
-        const int c_lo = link ? 1 : 3, c_hi = cols - c_lo - 1;  // halo columns
+// the lattice, which no thread writes here, so one pass suffices. A box of
+// ROWS rows holds the tile's rows 1 .. ROWS-2 between two halo rows; the
+// halo columns are LO (column -1 of the tile) and LO + 33 (column 32). UT is
+// the link element, PT the phi element; 9 components of each.
+template <class UT, class PT, int ROWS, int UC, int ULO, int PC, int PLO>
+__device__ __forceinline__ void fill_edge_halo(UT *ux, UT *uy, PT *ph, bool top, bool bottom,
+                                               bool left, bool right) {
+    constexpr int ROW = 34, COL = ROWS;  // cells per halo row / halo column
+    constexpr int CELLS = 2 * ROW + 2 * COL;
+    for (int w = threadIdx.x; w < 9 * 2 * CELLS; w += blockDim.x) {
+        const int k = w / (2 * CELLS);
+        int cell = w - k * (2 * CELLS);
+        const bool link = cell < CELLS;
+        if (!link) cell -= CELLS;
+        const int cols = link ? UC : PC;
+        const int c_lo = link ? ULO : PLO, c_hi = c_lo + 33;
         int j, m;
         bool edge;
-        if (cell < 2 * nrow) {
-            const int side = cell / nrow;
-            j = side ? rows - 1 : 0;
-            m = c_lo + cell % nrow;
+        if (cell < 2 * ROW) {
+            const int side = cell / ROW;
+            j = side ? ROWS - 1 : 0;
+            m = c_lo + cell % ROW;
             edge = side ? bottom : top;
         } else {
-            cell -= 2 * nrow;
-            const int side = cell / ncol;
-            j = cell % ncol;
+            cell -= 2 * ROW;
+            const int side = cell / COL;
+            j = cell % COL;
             m = side ? c_hi : c_lo;
             edge = side ? right : left;
         }
         if (!edge) continue;
         int sj = j, sm = m;
         if (top && j == 0) sj = 1;
-        if (bottom && j == rows - 1) sj = rows - 2;
+        if (bottom && j == ROWS - 1) sj = ROWS - 2;
         if (left && m == c_lo) sm = c_lo + 1;
         if (right && m == c_hi) sm = c_hi - 1;
         if (link) {
-            const int d = k * tile::kU + j * cols + m, s = k * tile::kU + sj * cols + sm;
+            constexpr int KU = ROWS * UC;
+            const int d = k * KU + j * cols + m, s = k * KU + sj * cols + sm;
             ux[d] = ux[s];
             uy[d] = uy[s];
         } else {
-            ph[k * tile::kP + j * cols + m] = ph[k * tile::kP + sj * cols + sm];
+            constexpr int KP = ROWS * PC;
+            ph[k * KP + j * cols + m] = ph[k * KP + sj * cols + sm];
         }
     }
 }
@@ -977,7 +1011,10 @@ __global__ void __launch_bounds__(256, 1)
         const bool top = tx == 0, bottom = tx == tiles_x - 1;
         const bool left = ty == 0, right = ty == tiles_y - 1;
         if (top || bottom || left || right) {
-            fill_edge_halo(st, top, bottom, left, right);
+            fill_edge_halo<C<float>, float, tile::UR, tile::UC, 1, tile::PC, 3>(
+                reinterpret_cast<C<float> *>(st + tile::UX),
+                reinterpret_cast<C<float> *>(st + tile::UY),
+                reinterpret_cast<float *>(st + tile::PHI), top, bottom, left, right);
             __syncthreads();
         }
 
@@ -1028,6 +1065,154 @@ __global__ void __launch_bounds__(256, 1)
             if (status) *status = 1.0;
             mbar_wait_bounded(&full[(i + 1) & 1], ((i + 1) >> 1) & 1, tile::MAX_POLLS);
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 step with the fields staged in shared memory by TMA: one block of 128
+// threads per tile of 4 rows (x) x 32 columns (y), one thread per site, two
+// blocks resident per SM (one stage each, so one block's loads overlap the
+// other's arithmetic). The stage holds
+//   Ux, Uy   [9][6][34] complex   rows ix0-1 .. ix0+4, columns iy0-1 .. iy0+32
+//   phi      [9][6][36] real      rows ix0-1 .. ix0+4, columns iy0-2 .. iy0+33
+//   E1, E2   [8][4][32], pi [9][4][32]   the tile's own sites
+// with edge halos clamped as in the FP32 tile kernel. The per-site code is
+// the one of the global-memory kernel (leapfrog_full_core); results go to
+// global memory from registers (E and pi in place).
+// ---------------------------------------------------------------------------
+namespace tile64 {
+constexpr int R = 4, Cn = 32;
+constexpr int UR = R + 2, UC = Cn + 2;  // link box
+constexpr int PR = R + 2, PC = Cn + 4;  // phi box
+constexpr int kU = UR * UC, kP = PR * PC, kS = R * Cn;
+constexpr int UX = 0;
+constexpr int UY = UX + tile::round128(9 * kU * 16);
+constexpr int PHI = UY + tile::round128(9 * kU * 16);
+constexpr int E1 = PHI + tile::round128(9 * kP * 8);
+constexpr int E2 = E1 + tile::round128(8 * kS * 8);
+constexpr int PI = E2 + tile::round128(8 * kS * 8);
+constexpr int STAGE = PI + tile::round128(9 * kS * 8);
+constexpr uint32_t TX_BYTES = 2 * 9 * kU * 16 + 9 * kP * 8 + 2 * 8 * kS * 8 + 9 * kS * 8;
+constexpr int SMEM = STAGE + 64 + 128;
+static_assert(2 * (SMEM + 1024) <= 228 * 1024, "two blocks per SM");
+}  // namespace tile64
+
+struct LoadMaps {
+    CUtensorMap ux, uy, phi, e1, e2, pi;
+};
+
+// Loads from the stage (shared memory); the thread sits at row r, column c.
+// ux/uy/ph point at the (-1, -1) corner of its 3 x 3 neighbourhood, pe1/pe2/
+// ppi at its own cell; E and pi are written to global memory in place.
+struct FullLoadTile64 {
+    const C<double> *ux, *uy;
+    const double *ph, *pe1, *pe2, *ppi;
+    const State<double> &g;
+    size_t pos, n;
+    __device__ __forceinline__ FullLoadTile64(const unsigned char *st, int r, int c,
+                                              const State<double> &g_, size_t pos_, size_t n_)
+        : ux(reinterpret_cast<const C<double> *>(st + tile64::UX) + r * tile64::UC + c),
+          uy(reinterpret_cast<const C<double> *>(st + tile64::UY) + r * tile64::UC + c),
+          ph(reinterpret_cast<const double *>(st + tile64::PHI) + r * tile64::PC + c + 1),
+          pe1(reinterpret_cast<const double *>(st + tile64::E1) + r * tile64::Cn + c),
+          pe2(reinterpret_cast<const double *>(st + tile64::E2) + r * tile64::Cn + c),
+          ppi(reinterpret_cast<const double *>(st + tile64::PI) + r * tile64::Cn + c),
+          g(g_), pos(pos_), n(n_) {}
+    template <int F, int DX, int DY>
+    __device__ __forceinline__ M3<double> link() const {
+        const C<double> *p = (F == kLy ? uy : ux) + (DX + 1) * tile64::UC + DY + 1;
+        M3<double> m;
+#pragma unroll
+        for (int k = 0; k < 9; k++) m.m[k] = p[k * tile64::kU];
+        return m;
+    }
+    static __device__ __forceinline__ H3<double> h9(const double *p, int S) {
+        H3<double> h;
+        h.d0 = p[0];
+        h.d1 = p[S];
+        h.d2 = p[2 * S];
+        h.o01 = {p[3 * S], p[4 * S]};
+        h.o02 = {p[5 * S], p[6 * S]};
+        h.o12 = {p[7 * S], p[8 * S]};
+        return h;
+    }
+    static __device__ __forceinline__ H3<double> h8(const double *p) {
+        constexpr int S = tile64::kS;
+        H3<double> h;
+        h.d0 = p[0];
+        h.d1 = p[S];
+        h.d2 = -(h.d0 + h.d1);
+        h.o01 = {p[2 * S], p[3 * S]};
+        h.o02 = {p[4 * S], p[5 * S]};
+        h.o12 = {p[6 * S], p[7 * S]};
+        return h;
+    }
+    template <int DX, int DY>
+    __device__ __forceinline__ H3<double> phi() const {
+        return h9(ph + (DX + 1) * tile64::PC + DY + 1, tile64::kP);
+    }
+    __device__ __forceinline__ H3<double> pi() const { return h9(ppi, tile64::kS); }
+    __device__ __forceinline__ H3<double> e1() const { return h8(pe1); }
+    __device__ __forceinline__ H3<double> e2() const { return h8(pe2); }
+    __device__ __forceinline__ void put_e(const H3<double> &a, const H3<double> &b) const {
+        st_h8(g.e1, pos, n, a);
+        st_h8(g.e2, pos, n, b);
+    }
+    __device__ __forceinline__ void put_pi(const H3<double> &h) const { st_h(g.pi, pos, n, h); }
+};
+
+__global__ void __launch_bounds__(128, 2)
+    k_leapfrog_tile64(const __grid_constant__ LoadMaps maps, int N, StepCoef<double> cf,
+                      double *status, State<double> s, C<double> *ux_out, C<double> *uy_out,
+                      double *phi_out) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const uint32_t pad = (128u - (smem_addr(smem_raw) & 127u)) & 127u;
+    unsigned char *smem = smem_raw + pad;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + tile64::STAGE);
+    int *abort_flag = reinterpret_cast<int *>(full + 1);
+    const int tiles_y = N / tile64::Cn, tiles_x = N / tile64::R;
+    const int ty = blockIdx.x % tiles_y, tx = blockIdx.x / tiles_y;
+    const int iy0 = ty * tile64::Cn, ix0 = tx * tile64::R;
+    const int tid = threadIdx.x, r = tid >> 5, c = tid & 31;
+    if (tid == 0) {
+        mbar_init(full, 1);
+        *abort_flag = 0;
+        fence_barrier_init();
+        mbar_arrive_expect_tx(full, tile64::TX_BYTES);
+        // links as pairs of 8-byte words: column iy0-1 is word 2 (iy0 - 1)
+        tma_load_3d(smem + tile64::UX, &maps.ux, 2 * (iy0 - 1), ix0 - 1, 0, full);
+        tma_load_3d(smem + tile64::UY, &maps.uy, 2 * (iy0 - 1), ix0 - 1, 0, full);
+        tma_load_3d(smem + tile64::PHI, &maps.phi, iy0 - 2, ix0 - 1, 0, full);
+        tma_load_3d(smem + tile64::E1, &maps.e1, iy0, ix0, 0, full);
+        tma_load_3d(smem + tile64::E2, &maps.e2, iy0, ix0, 0, full);
+        tma_load_3d(smem + tile64::PI, &maps.pi, iy0, ix0, 0, full);
+    }
+    __syncthreads();
+    if (!mbar_wait_bounded(full, 0, tile::MAX_POLLS)) *abort_flag = 1;
+    __syncthreads();
+    if (*abort_flag) {
+        if (tid == 0 && status) *status = 1.0;
+        return;
+    }
+    const bool top = tx == 0, bottom = tx == tiles_x - 1;
+    const bool left = ty == 0, right = ty == tiles_y - 1;
+    if (top || bottom || left || right) {
+        fill_edge_halo<C<double>, double, tile64::UR, tile64::UC, 0, tile64::PC, 1>(
+            reinterpret_cast<C<double> *>(smem + tile64::UX),
+            reinterpret_cast<C<double> *>(smem + tile64::UY),
+            reinterpret_cast<double *>(smem + tile64::PHI), top, bottom, left, right);
+        __syncthreads();
+    }
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)(ix0 + r) * N + iy0 + c;
+    const FullLoadTile64 ld(smem, r, c, s, pos, n);
+    M3<double> nx, ny;
+    H3<double> phin;
+    leapfrog_full_core<double, false>(ld, cf, nx, ny, phin);
+    if (cf.do_pu) {
+        st_h(phi_out, pos, n, phin);
+        st_m3(ux_out, pos, n, nx);
+        st_m3(uy_out, pos, n, ny);
     }
 }
 
@@ -1208,6 +1393,37 @@ bool launch_leapfrog_tile(int N, const State<float> &s, C<float> *ux_out, C<floa
     return true;
 }
 
+// The FP64 form's step kernel: the TMA-staged tile kernel unless
+// IPG_FP64_KERNEL=site selects the plain-load kernel (same per-site code).
+bool use_tile64_kernel() {
+    static const bool tile = [] {
+        const char *e = std::getenv("IPG_FP64_KERNEL");
+        return !(e && std::strcmp(e, "site") == 0);
+    }();
+    return tile;
+}
+
+bool launch_leapfrog_tile64(int N, const State<double> &s, C<double> *ux_out, C<double> *uy_out,
+                            double *phi_out, const StepCoef<double> &cf, double *status,
+                            cudaStream_t st) {
+    using namespace tile64;
+    const uint64_t n = (uint64_t)N;
+    const auto U64 = CU_TENSOR_MAP_DATA_TYPE_UINT64;
+    LoadMaps m;
+    // a complex link entry is two 8-byte words
+    const bool ok = encode_tiled_3d(&m.ux, s.ux, U64, 8, 2 * n, n, 9, 2 * UC, UR, 9) &&
+                    encode_tiled_3d(&m.uy, s.uy, U64, 8, 2 * n, n, 9, 2 * UC, UR, 9) &&
+                    encode_tiled_3d(&m.phi, s.phi, U64, 8, n, n, 9, PC, PR, 9) &&
+                    encode_tiled_3d(&m.e1, s.e1, U64, 8, n, n, 8, Cn, R, 8) &&
+                    encode_tiled_3d(&m.e2, s.e2, U64, 8, n, n, 8, Cn, R, 8) &&
+                    encode_tiled_3d(&m.pi, s.pi, U64, 8, n, n, 9, Cn, R, 9);
+    if (!ok) return false;
+    cudaFuncSetAttribute(k_leapfrog_tile64, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    k_leapfrog_tile64<<<(N / R) * (N / Cn), 128, SMEM, st>>>(m, N, cf, status, s, ux_out, uy_out,
+                                                               phi_out);
+    return true;
+}
+
 }  // namespace
 
 template <typename T>
@@ -1231,7 +1447,11 @@ void launch_leapfrog(const EventGeom *d_ev, int N, const State<T> &s,
             return;
         }
     }
-    (void)status;
+    if constexpr (sizeof(T) == 8) {
+        if (N >= 32 && !reunit && use_tile64_kernel() &&
+            launch_leapfrog_tile64(N, s, ux_out, uy_out, phi_out, cf, status, st))
+            return;
+    }
     launch_leapfrog_site(d_ev, N, s, ux_out, uy_out, phi_out, cf, reunit, st);
 }
 

@@ -78,7 +78,13 @@ __host__ __device__ __forceinline__ M3<T> mul_acc(const M3<T> &a, const M3<T> &b
     return c;
 }
 
-template <bool DA, bool DB, typename T>
+// op(A) op(B). RA (RB): the diagonal of A (B) is known to be real (a
+// Hermitian operand made by from_h), so the products with its zero imaginary
+// parts are left out; the remaining terms keep their order. (Where a zero
+// term is dropped the compiler may fuse a different product of the next sum,
+// which moves FP64 results at the level of the last bit; the packed FP32
+// form fuses explicitly and is unchanged.)
+template <bool DA, bool DB, bool RA = false, bool RB = false, typename T>
 __host__ __device__ __forceinline__ M3<T> mul_g(const M3<T> &a, const M3<T> &b) {
     M3<T> c;
 #pragma unroll
@@ -86,16 +92,25 @@ __host__ __device__ __forceinline__ M3<T> mul_g(const M3<T> &a, const M3<T> &b) 
 #pragma unroll
         for (int s = 0; s < 3; s++) {
             const C<T> x0 = entry<DA>(a, r, 0), y0 = entry<DB>(b, 0, s);
-            T re = x0.r * y0.r, im = x0.r * y0.i;
-            re -= x0.i * y0.i;
-            im += x0.i * y0.r;
+            const bool xr0 = RA && r == 0, yr0 = RB && s == 0;
+            T re = x0.r * y0.r, im;
+            if (!xr0 && !yr0) re -= x0.i * y0.i;
+            if (!yr0) {
+                im = x0.r * y0.i;
+                if (!xr0) im += x0.i * y0.r;
+            } else if (!xr0) {
+                im = x0.i * y0.r;
+            } else {
+                im = T(0);
+            }
 #pragma unroll
             for (int k = 1; k < 3; k++) {
                 const C<T> x = entry<DA>(a, r, k), y = entry<DB>(b, k, s);
+                const bool xr = RA && r == k, yr = RB && k == s;
                 re += x.r * y.r;
-                re -= x.i * y.i;
-                im += x.r * y.i;
-                im += x.i * y.r;
+                if (!xr && !yr) re -= x.i * y.i;
+                if (!yr) im += x.r * y.i;
+                if (!xr) im += x.i * y.r;
             }
             c.m[3 * r + s] = {re, im};
         }
@@ -242,7 +257,7 @@ template <typename T>
 __host__ __device__ __forceinline__ H3<T> conj_h(const M3<T> &u,
                                                  const H3<T> &h) {
     M3<T> hm = from_h(h);
-    M3<T> w = mul(u, hm);  // W = U H
+    M3<T> w = mul_g<false, false, false, true>(u, hm);  // W = U H
     // (W U^dag)[r][s] = sum_k W[r][k] conj(U[s][k])
     H3<T> out;
     T dr[3];
@@ -285,7 +300,7 @@ template <typename T>
 __host__ __device__ __forceinline__ H3<T> conj_h_dag(const M3<T> &u,
                                                      const H3<T> &h) {
     M3<T> hm = from_h(h);
-    M3<T> w = mul(hm, u);  // W = H U
+    M3<T> w = mul_g<false, false, true, false>(hm, u);  // W = H U
     // (U^dag W)[r][s] = sum_k conj(U[k][r]) W[k][s]
     H3<T> out;
     T dr[3];
@@ -355,7 +370,7 @@ template <typename T>
 __host__ __device__ __forceinline__ H3<T> i_commutator(const H3<T> &a,
                                                        const H3<T> &b) {
     M3<T> am = from_h(a), bm = from_h(b);
-    M3<T> ab = mul(am, bm);
+    M3<T> ab = mul_g<false, false, true, true>(am, bm);
     // [A,B] = AB - (AB)^dag ; i*[A,B] entries: i*(x - conj(y))
     H3<T> out;
     // diagonal: AB_rr - conj(AB_rr) = 2 i Im(AB_rr); times i -> -2 Im
