@@ -281,10 +281,10 @@ def run_ours(args, world, rank, local):
     traffic = load_traffic()
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
             "frac": round(achieved / hbm, 4), "traffic": traffic,
-            "kernel": "k_leapfrog_pair (FP32 bulk, both directions in packed f32x2 lanes)",
+            "kernel": "k_leapfrog_tile (FP32 bulk: TMA-staged 8x32 tiles, both directions in packed f32x2 lanes)",
             "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp32"],
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-            "fp64_kernel": {"kernel": "k_leapfrog<double,0>", "achieved": round(su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9, 1),
+            "fp64_kernel": {"kernel": "k_leapfrog_tile64 (FP64 plain form: TMA-staged 4x32 tiles)", "achieved": round(su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9, 1),
                             "frac": round(su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9 / hbm, 4),
                             "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp64"]}}
 

@@ -140,33 +140,32 @@ struct FullLoadGlobal {
 
 // One site in full-matrix storage (the FP64 plain form): loads through `ld`,
 // writes the new pi and E through it and returns the new links and phi when
-// cf.do_pu is set.
+// cf.do_pu is set. The site's own links and phi are loaded again at each use
+// rather than held (from a shared-memory tile that is cheaper than keeping
+// 90 registers live across the site, which spilled).
 template <typename T, bool REUNIT, class Ld>
 __device__ __forceinline__ void leapfrog_full_core(const Ld &ld, const StepCoef<T> &cf,
                                                    M3<T> &nx, M3<T> &ny, H3<T> &phin) {
     if (cf.do_pe) {
-        const M3<T> ux = ld.template link<kLx, 0, 0>();
-        const M3<T> uy = ld.template link<kLy, 0, 0>();
-
         // plaquette U12 = Ux Uy(x+1) Ux(y+1)^dag Uy^dag  (Evolution.cpp:228-232)
         H3<T> h12;
         {
-            M3<T> a = mul(ux, ld.template link<kLy, 1, 0>());
-            M3<T> b = mul(uy, ld.template link<kLx, 0, 1>());
+            M3<T> a = mul(ld.template link<kLx, 0, 0>(), ld.template link<kLy, 1, 0>());
+            M3<T> b = mul(ld.template link<kLy, 0, 0>(), ld.template link<kLx, 0, 1>());
             M3<T> u12 = mul_nd(a, b);
             h12 = i_antiherm(u12);
         }
         // E1 staple sum: U12 + U1m2 - h.c.  (234-257)
         H3<T> t1 = h12;
         {
-            M3<T> p = mul_nd(ux, ld.template link<kLy, 1, -1>());
+            M3<T> p = mul_nd(ld.template link<kLx, 0, 0>(), ld.template link<kLy, 1, -1>());
             M3<T> q = mul_dn(ld.template link<kLx, 0, -1>(), ld.template link<kLy, 0, -1>());
             h_add(t1, i_antiherm_mul(p, q));
         }
         // E2 staple sum: U12^dag + U2m1 - h.c.  (240-244, 266-275)
         H3<T> t2;
         {
-            M3<T> p = mul_nd(uy, ld.template link<kLx, -1, 1>());
+            M3<T> p = mul_nd(ld.template link<kLy, 0, 0>(), ld.template link<kLx, -1, 1>());
             M3<T> q = mul_dn(ld.template link<kLy, -1, 0>(), ld.template link<kLx, -1, 0>());
             t2 = i_antiherm_mul(p, q);
             h_axpy(t2, T(-1), h12);
@@ -174,7 +173,6 @@ __device__ __forceinline__ void leapfrog_full_core(const Ld &ld, const StepCoef<
         h_traceless(t1);
         h_traceless(t2);
 
-        const H3<T> phi = ld.template phi<0, 0>();
         H3<T> pi = ld.pi();
         H3<T> e1 = ld.e1();
         H3<T> e2 = ld.e2();
@@ -186,18 +184,18 @@ __device__ __forceinline__ void leapfrog_full_core(const Ld &ld, const StepCoef<
         // parallel transports of phi (evolvePi 139-157, evolveE 221-223, 278-279)
         H3<T> br;
         {
-            H3<T> phx = conj_h(ux, ld.template phi<1, 0>());
-            h_axpy(e1, cdt, i_commutator(phx, phi));
+            H3<T> phx = conj_h(ld.template link<kLx, 0, 0>(), ld.template phi<1, 0>());
+            h_axpy(e1, cdt, i_commutator(phx, ld.template phi<0, 0>()));
             br = phx;
         }
         {
-            H3<T> phy = conj_h(uy, ld.template phi<0, 1>());
-            h_axpy(e2, cdt, i_commutator(phy, phi));
+            H3<T> phy = conj_h(ld.template link<kLy, 0, 0>(), ld.template phi<0, 1>());
+            h_axpy(e2, cdt, i_commutator(phy, ld.template phi<0, 0>()));
             h_add(br, phy);
         }
         h_add(br, conj_h_dag(ld.template link<kLx, -1, 0>(), ld.template phi<-1, 0>()));
         h_add(br, conj_h_dag(ld.template link<kLy, 0, -1>(), ld.template phi<0, -1>()));
-        h_axpy(br, T(-4), phi);
+        h_axpy(br, T(-4), ld.template phi<0, 0>());
         h_axpy(pi, cdt, br);
         h_traceless(e1);
         h_traceless(e2);
@@ -205,12 +203,12 @@ __device__ __forceinline__ void leapfrog_full_core(const Ld &ld, const StepCoef<
         ld.put_e(e1, e2);
 
         if (cf.do_pu) {
-            phin = phi;
+            phin = ld.template phi<0, 0>();
             h_axpy(phin, (cf.tau + cf.dt_pu / T(2)) * cf.dt_pu, pi);
             const T c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / T(2));
-            nx = taylor2_update(e1, c, ux);
+            nx = taylor2_update(e1, c, ld.template link<kLx, 0, 0>());
             if (REUNIT) reunitarize(nx);
-            ny = taylor2_update(e2, c, uy);
+            ny = taylor2_update(e2, c, ld.template link<kLy, 0, 0>());
             if (REUNIT) reunitarize(ny);
         }
     } else if (cf.do_pu) {
@@ -771,17 +769,20 @@ __global__ void __launch_bounds__(256, 1)
 // ---------------------------------------------------------------------------
 // FP32 step with the fields staged in shared memory by TMA. A persistent
 // block per SM walks tiles of 8 rows (x) x 32 columns (y), one thread per
-// site; the loads of tile i+2 are in flight while tile i is computed (two
-// stages). A stage holds, per tile,
+// site (warp r takes row r); the loads of tile i+2 are in flight while tile i
+// is computed (two stages). A stage holds, per tile,
 //   Ux, Uy   [9][10][36] complex   rows ix0-1 .. ix0+8, columns iy0-2 .. iy0+33
 //   phi      [9][10][40] real      rows ix0-1 .. ix0+8, columns iy0-4 .. iy0+35
 //   E1, E2   [8][8][32], pi [9][8][32]   the tile's own sites
 // (the column starts keep each box's first column 16-byte aligned, as TMA
 // requires). Boxes reaching past the lattice are zero filled; on edge tiles
-// the halo cells are then overwritten with the clamped neighbours
-// (Lattice.cpp:19-28), so every neighbour read is a fixed offset from the
-// thread's own cell. Results are written back into the same stage (E and pi
-// in place at once, links and phi after a barrier) and leave by TMA stores.
+// each warp then overwrites the halo cells of the rows it reads with the
+// clamped neighbours (Lattice.cpp:19-28), so every neighbour read is a fixed
+// offset from the thread's own cell. There is no block-wide barrier in the
+// loop: a stage's "full" barrier completes with its TMA bytes, each warp
+// arrives on its "empty" barrier once it has read the stage, and thread 0
+// waits on "empty" before loading the stage again. Results go to global
+// memory from registers (E and pi in place).
 // ---------------------------------------------------------------------------
 namespace tile {
 constexpr int R = 8, Cn = 32;            // tile rows (x) and columns (y)
@@ -797,16 +798,15 @@ constexpr int E2 = E1 + round128(8 * kS * 4);
 constexpr int PI = E2 + round128(8 * kS * 4);
 constexpr int STAGE = PI + round128(9 * kS * 4);
 constexpr uint32_t TX_BYTES = 2 * 9 * kU * 8 + 9 * kP * 4 + 2 * 8 * kS * 4 + 9 * kS * 4;
-constexpr int SMEM = 2 * STAGE + 64 + 128;  // two stages, barriers, alignment slack
+constexpr int SMEM = 2 * STAGE + 64 + 128;  // two stages, four barriers, alignment slack
 constexpr uint32_t MAX_POLLS = 1u << 22;
 static_assert(STAGE % 128 == 0, "stage alignment");
 static_assert(SMEM <= 227 * 1024, "shared memory per block");
 }  // namespace tile
 
-struct TileMaps {
-    CUtensorMap ux_in, uy_in, phi_in;     // load boxes with halo
-    CUtensorMap ux_out, uy_out, phi_out;  // store boxes (the tile)
-    CUtensorMap e1, e2, pi;               // the tile, loaded and stored in place
+// tensor maps of the six fields for one step's loads
+struct LoadMaps {
+    CUtensorMap ux, uy, phi, e1, e2, pi;
 };
 
 // 32-bit shared-memory accesses by address: one value per instruction, so
@@ -832,11 +832,14 @@ __device__ __forceinline__ void sts_f32(uint32_t a, float v) {
 // instructions a step at 512^2 instead of 18.5 M).
 struct PairLoadTile {
     uint32_t bu, bi, bp, bs;
-    __device__ __forceinline__ PairLoadTile(uint32_t stage, int r, int c, uint32_t imag)
+    const State<float> &g;  // E and pi are written here, in place
+    size_t pos, n;
+    __device__ __forceinline__ PairLoadTile(uint32_t stage, int r, int c, uint32_t imag,
+                                            const State<float> &g_, size_t pos_, size_t n_)
         : bu(stage + (uint32_t)((r * tile::UC + c + 1) * 8)),
           bi(stage + (uint32_t)((r * tile::UC + c + 1) * 8) + imag),
           bp(stage + tile::PHI + (uint32_t)((r * tile::PC + c + 3) * 4)),
-          bs(stage + (uint32_t)((r * tile::Cn + c) * 4)) {}
+          bs(stage + (uint32_t)((r * tile::Cn + c) * 4)), g(g_), pos(pos_), n(n_) {}
     template <int FA, int DXA, int DYA, int FB, int DXB, int DYB>
     __device__ __forceinline__ M3<P2> links() const {
         constexpr uint32_t oa =
@@ -880,35 +883,11 @@ struct PairLoadTile {
     __device__ __forceinline__ H3<float> pi() const { return h9(bs + tile::PI, tile::kS * 4); }
     __device__ __forceinline__ H3<float> e1() const { return h8(bs + tile::E1); }
     __device__ __forceinline__ H3<float> e2() const { return h8(bs + tile::E2); }
-    static __device__ __forceinline__ void put_h8(uint32_t a, const H3<float> &h) {
-        constexpr uint32_t S = tile::kS * 4;
-        sts_f32(a, h.d0);
-        sts_f32(a + S, h.d1);
-        sts_f32(a + 2 * S, h.o01.r);
-        sts_f32(a + 3 * S, h.o01.i);
-        sts_f32(a + 4 * S, h.o02.r);
-        sts_f32(a + 5 * S, h.o02.i);
-        sts_f32(a + 6 * S, h.o12.r);
-        sts_f32(a + 7 * S, h.o12.i);
-    }
-    static __device__ __forceinline__ void put_h9(uint32_t a, const H3<float> &h) {
-        constexpr uint32_t S = tile::kS * 4;
-        sts_f32(a, h.d0);
-        sts_f32(a + S, h.d1);
-        sts_f32(a + 2 * S, h.d2);
-        sts_f32(a + 3 * S, h.o01.r);
-        sts_f32(a + 4 * S, h.o01.i);
-        sts_f32(a + 5 * S, h.o02.r);
-        sts_f32(a + 6 * S, h.o02.i);
-        sts_f32(a + 7 * S, h.o12.r);
-        sts_f32(a + 8 * S, h.o12.i);
-    }
-    // E and pi go back in place: only this thread reads its own cells
     __device__ __forceinline__ void put_e(const H3<float> &a, const H3<float> &b) const {
-        put_h8(bs + tile::E1, a);
-        put_h8(bs + tile::E2, b);
+        st_h8(g.e1, pos, n, a);
+        st_h8(g.e2, pos, n, b);
     }
-    __device__ __forceinline__ void put_pi(const H3<float> &h) const { put_h9(bs + tile::PI, h); }
+    __device__ __forceinline__ void put_pi(const H3<float> &h) const { st_h(g.pi, pos, n, h); }
 };
 
 // Edge tiles: halo cells outside the lattice take the clamped neighbour,
@@ -961,9 +940,50 @@ __device__ __forceinline__ void fill_edge_halo(UT *ux, UT *uy, PT *ph, bool top,
     }
 }
 
+// Edge tiles, one warp: the halo cells of the box rows r .. r+2 that warp r
+// reads (its tile row and the rows on either side) take the clamped
+// neighbour, each coordinate clamped on its own. Sources are lattice cells,
+// which nobody writes; warps whose rows overlap write the same values.
+__device__ __forceinline__ void fill_warp_halo(unsigned char *st, int r, int lane, bool top,
+                                               bool bottom, bool left, bool right) {
+    C<float> *ux = reinterpret_cast<C<float> *>(st + tile::UX);
+    C<float> *uy = reinterpret_cast<C<float> *>(st + tile::UY);
+    float *ph = reinterpret_cast<float *>(st + tile::PHI);
+    auto clamp_j = [&](int j) { return (top && j == 0) ? 1 : ((bottom && j == tile::UR - 1) ? j - 1 : j); };
+    // halo columns (links 1 and 34, phi 3 and 36) of rows r .. r+2
+    if (left || right) {
+        for (int w = lane; w < 9 * 3 * 2; w += 32) {
+            const int k = w / 6, j = r + (w % 6) / 2, side = w & 1;
+            if (side ? !right : !left) continue;
+            const int sj = clamp_j(j);
+            const int mu = side ? 34 : 1, su = side ? 33 : 2;
+            const int mp = side ? 36 : 3, sp = side ? 35 : 4;
+            ux[k * tile::kU + j * tile::UC + mu] = ux[k * tile::kU + sj * tile::UC + su];
+            uy[k * tile::kU + j * tile::UC + mu] = uy[k * tile::kU + sj * tile::UC + su];
+            ph[k * tile::kP + j * tile::PC + mp] = ph[k * tile::kP + sj * tile::PC + sp];
+        }
+    }
+    // the halo row above (warp 0, top edge) or below (warp 7, bottom edge)
+    const bool row_top = top && r == 0, row_bottom = bottom && r == tile::R - 1;
+    if (row_top || row_bottom) {
+        const int j = row_top ? 0 : tile::UR - 1, sj = row_top ? 1 : tile::UR - 2;
+        for (int w = lane; w < 9 * 34; w += 32) {
+            const int k = w / 34, q = w % 34;
+            int mu = 1 + q, mp = 3 + q;  // links 1..34, phi 3..36
+            int su = mu, sp = mp;
+            if (left && q == 0) su = 2, sp = 4;
+            if (right && q == 33) su = 33, sp = 35;
+            ux[k * tile::kU + j * tile::UC + mu] = ux[k * tile::kU + sj * tile::UC + su];
+            uy[k * tile::kU + j * tile::UC + mu] = uy[k * tile::kU + sj * tile::UC + su];
+            ph[k * tile::kP + j * tile::PC + mp] = ph[k * tile::kP + sj * tile::PC + sp];
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256, 1)
-    k_leapfrog_tile(const __grid_constant__ TileMaps maps, int N, StepCoef<float> cf,
-                    double *status, uint32_t imag) {
+    k_leapfrog_tile(const __grid_constant__ LoadMaps maps, int N, StepCoef<float> cf,
+                    double *status, uint32_t imag, State<float> gs, C<float> *ux_out,
+                    C<float> *uy_out, float *phi_out) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // 128-byte aligned start, kept as an offset into the shared array so that
     // accesses through it stay shared-memory accesses
@@ -971,17 +991,18 @@ __global__ void __launch_bounds__(256, 1)
     unsigned char *smem = smem_raw + pad;
     const uint32_t sbase = smem_addr(smem);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + 2 * tile::STAGE);
-    int *abort_flag = reinterpret_cast<int *>(full + 2);
+    uint64_t *empty = full + 2;
     const int tiles_y = N / tile::Cn, tiles_x = N / tile::R, tiles = tiles_x * tiles_y;
     const int tid = threadIdx.x, r = tid >> 5, c = tid & 31;
+    const size_t n = (size_t)N * N;
 
     auto issue = [&](int t, int s) {
         const int iy0 = (t % tiles_y) * tile::Cn, ix0 = (t / tiles_y) * tile::R;
         unsigned char *st = smem + s * tile::STAGE;
         mbar_arrive_expect_tx(&full[s], tile::TX_BYTES);
-        tma_load_3d(st + tile::UX, &maps.ux_in, iy0 - 2, ix0 - 1, 0, &full[s]);
-        tma_load_3d(st + tile::UY, &maps.uy_in, iy0 - 2, ix0 - 1, 0, &full[s]);
-        tma_load_3d(st + tile::PHI, &maps.phi_in, iy0 - 4, ix0 - 1, 0, &full[s]);
+        tma_load_3d(st + tile::UX, &maps.ux, iy0 - 2, ix0 - 1, 0, &full[s]);
+        tma_load_3d(st + tile::UY, &maps.uy, iy0 - 2, ix0 - 1, 0, &full[s]);
+        tma_load_3d(st + tile::PHI, &maps.phi, iy0 - 4, ix0 - 1, 0, &full[s]);
         tma_load_3d(st + tile::E1, &maps.e1, iy0, ix0, 0, &full[s]);
         tma_load_3d(st + tile::E2, &maps.e2, iy0, ix0, 0, &full[s]);
         tma_load_3d(st + tile::PI, &maps.pi, iy0, ix0, 0, &full[s]);
@@ -990,80 +1011,54 @@ __global__ void __launch_bounds__(256, 1)
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
-        *abort_flag = 0;
+        mbar_init(&empty[0], tile::R);  // one arrival per warp
+        mbar_init(&empty[1], tile::R);
         fence_barrier_init();
-        prefetch_map(&maps.ux_in);
-        prefetch_map(&maps.uy_in);
-        prefetch_map(&maps.phi_in);
+        prefetch_map(&maps.ux);
+        prefetch_map(&maps.uy);
+        prefetch_map(&maps.phi);
         if (blockIdx.x < tiles) issue(blockIdx.x, 0);
         if (blockIdx.x + gridDim.x < tiles) issue(blockIdx.x + gridDim.x, 1);
     }
-    __syncthreads();
+    __syncthreads();  // barriers initialised before anyone waits on them
 
     int i = 0;
     for (int t = blockIdx.x; t < tiles; t += gridDim.x, i++) {
         const int s = i & 1;
+        const uint32_t use = (uint32_t)(i >> 1) & 1u;
+        if (!mbar_wait_bounded(&full[s], use, tile::MAX_POLLS)) {
+            if (status) *status = 1.0;  // the tile never arrived
+            break;
+        }
         unsigned char *st = smem + s * tile::STAGE;
-        if (!mbar_wait_bounded(&full[s], (i >> 1) & 1, tile::MAX_POLLS)) *abort_flag = 1;
-        __syncthreads();
-        if (*abort_flag) break;
         const int ty = t % tiles_y, tx = t / tiles_y;
         const bool top = tx == 0, bottom = tx == tiles_x - 1;
         const bool left = ty == 0, right = ty == tiles_y - 1;
-        if (top || bottom || left || right) {
-            fill_edge_halo<C<float>, float, tile::UR, tile::UC, 1, tile::PC, 3>(
-                reinterpret_cast<C<float> *>(st + tile::UX),
-                reinterpret_cast<C<float> *>(st + tile::UY),
-                reinterpret_cast<float *>(st + tile::PHI), top, bottom, left, right);
-            __syncthreads();
+        const bool edge = top || bottom || left || right;
+        if (edge) {
+            fill_warp_halo(st, r, c, top, bottom, left, right);
+            __syncwarp();
         }
-
-        const uint32_t sst = sbase + (uint32_t)(s * tile::STAGE);
-        const PairLoadTile ld(sst, r, c, imag);
+        const size_t pos = (size_t)(tx * tile::R + r) * N + ty * tile::Cn + c;
+        const PairLoadTile ld(sbase + (uint32_t)(s * tile::STAGE), r, c, imag, gs, pos, n);
         M3<P2> nu;
         H3<float> phin;
         leapfrog_pair_core(ld, cf, nu, phin);
-        __syncthreads();  // every read of this stage's links and phi is done
+        // this warp is done with the stage (its halo writes ordered before the
+        // TMA unit writes the stage again)
+        if (edge) fence_async_smem();
+        __syncwarp();
+        if (c == 0) mbar_arrive(&empty[s]);
         if (cf.do_pu) {
-            // the new links [9][8][32] over the link boxes, phi over the phi box
-            const uint32_t o = sst + (uint32_t)((r * tile::Cn + c) * 8);
-#pragma unroll
-            for (int k = 0; k < 9; k++) {
-                const uint32_t ok = o + k * tile::kS * 8;
-                sts_f32(ok + tile::UX, lane_x(nu.m[k].r));
-                sts_f32(ok + tile::UX + 4, lane_x(nu.m[k].i));
-                sts_f32(ok + tile::UY, lane_y(nu.m[k].r));
-                sts_f32(ok + tile::UY + 4, lane_y(nu.m[k].i));
-            }
-            PairLoadTile::put_h9(sst + tile::PHI + (uint32_t)((r * tile::Cn + c) * 4), phin);
+            st_m3_pair(ux_out, uy_out, pos, n, nu);
+            st_h(phi_out, pos, n, phin);
         }
-        fence_async_smem();
-        __syncthreads();
-        if (tid == 0) {
-            const int iy0 = ty * tile::Cn, ix0 = tx * tile::R;
-            if (cf.do_pe) {
-                tma_store_3d(&maps.e1, iy0, ix0, 0, st + tile::E1);
-                tma_store_3d(&maps.e2, iy0, ix0, 0, st + tile::E2);
-                tma_store_3d(&maps.pi, iy0, ix0, 0, st + tile::PI);
+        if (tid == 0 && t + 2 * (int)gridDim.x < tiles) {
+            if (!mbar_wait_bounded(&empty[s], use, tile::MAX_POLLS)) {
+                if (status) *status = 1.0;  // a warp never released the stage
+                break;
             }
-            if (cf.do_pu) {
-                tma_store_3d(&maps.ux_out, iy0, ix0, 0, st + tile::UX);
-                tma_store_3d(&maps.uy_out, iy0, ix0, 0, st + tile::UY);
-                tma_store_3d(&maps.phi_out, iy0, ix0, 0, st + tile::PHI);
-            }
-            bulk_commit();
-            // the stage is reloaded only after the stores have read it
-            bulk_wait_read_all();
-            if (t + 2 * (int)gridDim.x < tiles) issue(t + 2 * gridDim.x, s);
-        }
-    }
-    if (tid == 0) {
-        bulk_wait_all();
-        if (*abort_flag) {
-            // a load that never completed: report it, and give any other load
-            // in flight a bounded chance to land before the block exits
-            if (status) *status = 1.0;
-            mbar_wait_bounded(&full[(i + 1) & 1], ((i + 1) >> 1) & 1, tile::MAX_POLLS);
+            issue(t + 2 * gridDim.x, s);
         }
     }
 }
@@ -1097,63 +1092,70 @@ constexpr int SMEM = STAGE + 64 + 128;
 static_assert(2 * (SMEM + 1024) <= 228 * 1024, "two blocks per SM");
 }  // namespace tile64
 
-struct LoadMaps {
-    CUtensorMap ux, uy, phi, e1, e2, pi;
-};
+// Loads from the stage (shared memory) by 32-bit address; the thread sits at
+// row r, column c. bl and bp point at the (-1, -1) corner of its 3 x 3
+// neighbourhood in the link and phi boxes, bs at its own cell of the
+// site-local boxes. The loads are explicit shared-memory instructions, so a
+// link loaded twice is read twice rather than kept live in registers; E and
+// pi are written to global memory in place.
+__device__ __forceinline__ C<double> lds_c64(uint32_t a) {
+    double re, im;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(re), "=d"(im) : "r"(a));
+    return {re, im};
+}
+__device__ __forceinline__ double lds_f64(uint32_t a) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
+    return v;
+}
 
-// Loads from the stage (shared memory); the thread sits at row r, column c.
-// ux/uy/ph point at the (-1, -1) corner of its 3 x 3 neighbourhood, pe1/pe2/
-// ppi at its own cell; E and pi are written to global memory in place.
 struct FullLoadTile64 {
-    const C<double> *ux, *uy;
-    const double *ph, *pe1, *pe2, *ppi;
+    uint32_t bl, bp, bs;
     const State<double> &g;
     size_t pos, n;
-    __device__ __forceinline__ FullLoadTile64(const unsigned char *st, int r, int c,
+    __device__ __forceinline__ FullLoadTile64(uint32_t stage, int r, int c,
                                               const State<double> &g_, size_t pos_, size_t n_)
-        : ux(reinterpret_cast<const C<double> *>(st + tile64::UX) + r * tile64::UC + c),
-          uy(reinterpret_cast<const C<double> *>(st + tile64::UY) + r * tile64::UC + c),
-          ph(reinterpret_cast<const double *>(st + tile64::PHI) + r * tile64::PC + c + 1),
-          pe1(reinterpret_cast<const double *>(st + tile64::E1) + r * tile64::Cn + c),
-          pe2(reinterpret_cast<const double *>(st + tile64::E2) + r * tile64::Cn + c),
-          ppi(reinterpret_cast<const double *>(st + tile64::PI) + r * tile64::Cn + c),
+        : bl(stage + (uint32_t)((r * tile64::UC + c) * 16)),
+          bp(stage + tile64::PHI + (uint32_t)((r * tile64::PC + c + 1) * 8)),
+          bs(stage + (uint32_t)((r * tile64::Cn + c) * 8)),
           g(g_), pos(pos_), n(n_) {}
     template <int F, int DX, int DY>
     __device__ __forceinline__ M3<double> link() const {
-        const C<double> *p = (F == kLy ? uy : ux) + (DX + 1) * tile64::UC + DY + 1;
+        constexpr uint32_t o =
+            (F == kLy ? tile64::UY : tile64::UX) + ((DX + 1) * tile64::UC + DY + 1) * 16;
         M3<double> m;
 #pragma unroll
-        for (int k = 0; k < 9; k++) m.m[k] = p[k * tile64::kU];
+        for (int k = 0; k < 9; k++) m.m[k] = lds_c64(bl + o + k * tile64::kU * 16);
         return m;
     }
-    static __device__ __forceinline__ H3<double> h9(const double *p, int S) {
+    static __device__ __forceinline__ H3<double> h9(uint32_t a, uint32_t S) {
         H3<double> h;
-        h.d0 = p[0];
-        h.d1 = p[S];
-        h.d2 = p[2 * S];
-        h.o01 = {p[3 * S], p[4 * S]};
-        h.o02 = {p[5 * S], p[6 * S]};
-        h.o12 = {p[7 * S], p[8 * S]};
+        h.d0 = lds_f64(a);
+        h.d1 = lds_f64(a + S);
+        h.d2 = lds_f64(a + 2 * S);
+        h.o01 = {lds_f64(a + 3 * S), lds_f64(a + 4 * S)};
+        h.o02 = {lds_f64(a + 5 * S), lds_f64(a + 6 * S)};
+        h.o12 = {lds_f64(a + 7 * S), lds_f64(a + 8 * S)};
         return h;
     }
-    static __device__ __forceinline__ H3<double> h8(const double *p) {
-        constexpr int S = tile64::kS;
+    static __device__ __forceinline__ H3<double> h8(uint32_t a) {
+        constexpr uint32_t S = tile64::kS * 8;
         H3<double> h;
-        h.d0 = p[0];
-        h.d1 = p[S];
+        h.d0 = lds_f64(a);
+        h.d1 = lds_f64(a + S);
         h.d2 = -(h.d0 + h.d1);
-        h.o01 = {p[2 * S], p[3 * S]};
-        h.o02 = {p[4 * S], p[5 * S]};
-        h.o12 = {p[6 * S], p[7 * S]};
+        h.o01 = {lds_f64(a + 2 * S), lds_f64(a + 3 * S)};
+        h.o02 = {lds_f64(a + 4 * S), lds_f64(a + 5 * S)};
+        h.o12 = {lds_f64(a + 6 * S), lds_f64(a + 7 * S)};
         return h;
     }
     template <int DX, int DY>
     __device__ __forceinline__ H3<double> phi() const {
-        return h9(ph + (DX + 1) * tile64::PC + DY + 1, tile64::kP);
+        return h9(bp + ((DX + 1) * tile64::PC + DY + 1) * 8, tile64::kP * 8);
     }
-    __device__ __forceinline__ H3<double> pi() const { return h9(ppi, tile64::kS); }
-    __device__ __forceinline__ H3<double> e1() const { return h8(pe1); }
-    __device__ __forceinline__ H3<double> e2() const { return h8(pe2); }
+    __device__ __forceinline__ H3<double> pi() const { return h9(bs + tile64::PI, tile64::kS * 8); }
+    __device__ __forceinline__ H3<double> e1() const { return h8(bs + tile64::E1); }
+    __device__ __forceinline__ H3<double> e2() const { return h8(bs + tile64::E2); }
     __device__ __forceinline__ void put_e(const H3<double> &a, const H3<double> &b) const {
         st_h8(g.e1, pos, n, a);
         st_h8(g.e2, pos, n, b);
@@ -1161,7 +1163,10 @@ struct FullLoadTile64 {
     __device__ __forceinline__ void put_pi(const H3<double> &h) const { st_h(g.pi, pos, n, h); }
 };
 
-__global__ void __launch_bounds__(128, 2)
+// (128, 1): ptxas then fits the site in 190 registers without spilling (with
+// a stated minimum of 2 blocks it used 255 and spilled), and two blocks per SM
+// still fit in registers and shared memory
+__global__ void __launch_bounds__(128, 1)
     k_leapfrog_tile64(const __grid_constant__ LoadMaps maps, int N, StepCoef<double> cf,
                       double *status, State<double> s, C<double> *ux_out, C<double> *uy_out,
                       double *phi_out) {
@@ -1205,7 +1210,7 @@ __global__ void __launch_bounds__(128, 2)
     }
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)(ix0 + r) * N + iy0 + c;
-    const FullLoadTile64 ld(smem, r, c, s, pos, n);
+    const FullLoadTile64 ld(smem_addr(smem), r, c, s, pos, n);
     M3<double> nx, ny;
     H3<double> phin;
     leapfrog_full_core<double, false>(ld, cf, nx, ny, phin);
@@ -1371,17 +1376,13 @@ bool launch_leapfrog_tile(int N, const State<float> &s, C<float> *ux_out, C<floa
     using namespace tile;
     const uint64_t n = (uint64_t)N;
     const auto U64 = CU_TENSOR_MAP_DATA_TYPE_UINT64, U32 = CU_TENSOR_MAP_DATA_TYPE_UINT32;
-    TileMaps m;
-    const bool ok =
-        encode_tiled_3d(&m.ux_in, s.ux, U64, 8, n, n, 9, UC, UR, 9) &&
-        encode_tiled_3d(&m.uy_in, s.uy, U64, 8, n, n, 9, UC, UR, 9) &&
-        encode_tiled_3d(&m.phi_in, s.phi, U32, 4, n, n, 9, PC, PR, 9) &&
-        encode_tiled_3d(&m.ux_out, ux_out, U64, 8, n, n, 9, Cn, R, 9) &&
-        encode_tiled_3d(&m.uy_out, uy_out, U64, 8, n, n, 9, Cn, R, 9) &&
-        encode_tiled_3d(&m.phi_out, phi_out, U32, 4, n, n, 9, Cn, R, 9) &&
-        encode_tiled_3d(&m.e1, s.e1, U32, 4, n, n, 8, Cn, R, 8) &&
-        encode_tiled_3d(&m.e2, s.e2, U32, 4, n, n, 8, Cn, R, 8) &&
-        encode_tiled_3d(&m.pi, s.pi, U32, 4, n, n, 9, Cn, R, 9);
+    LoadMaps m;
+    const bool ok = encode_tiled_3d(&m.ux, s.ux, U64, 8, n, n, 9, UC, UR, 9) &&
+                    encode_tiled_3d(&m.uy, s.uy, U64, 8, n, n, 9, UC, UR, 9) &&
+                    encode_tiled_3d(&m.phi, s.phi, U32, 4, n, n, 9, PC, PR, 9) &&
+                    encode_tiled_3d(&m.e1, s.e1, U32, 4, n, n, 8, Cn, R, 8) &&
+                    encode_tiled_3d(&m.e2, s.e2, U32, 4, n, n, 8, Cn, R, 8) &&
+                    encode_tiled_3d(&m.pi, s.pi, U32, 4, n, n, 9, Cn, R, 9);
     if (!ok) return false;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
@@ -1389,7 +1390,8 @@ bool launch_leapfrog_tile(int N, const State<float> &s, C<float> *ux_out, C<floa
     cudaFuncSetAttribute(k_leapfrog_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
     const int tiles = (N / R) * (N / Cn);
     // imag = 4: the byte offset of a link's imaginary part
-    k_leapfrog_tile<<<tiles < sms ? tiles : sms, 256, SMEM, st>>>(m, N, cf, status, 4u);
+    k_leapfrog_tile<<<tiles < sms ? tiles : sms, 256, SMEM, st>>>(m, N, cf, status, 4u, s, ux_out,
+                                                                  uy_out, phi_out);
     return true;
 }
 
