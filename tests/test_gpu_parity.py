@@ -205,3 +205,49 @@ def test_g2mu_from_nucleons_matches_host_map():
         g = ev.g2mu()
     for dev, host in ((g[0], A), (g[1], B)):
         assert np.abs(dev - host).max() <= 1e-12 * host.max()
+
+
+_DUMP = r'''
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+import ipglasma_b200 as ipg
+from ipglasma_b200.synthetic import make_event
+out = {}
+for prec, tag in ((ipg.FP64, "d"), (ipg.FP32, "s")):
+    for N, L in ((64, 20.0), (128, 24.0)):
+        gA, gB, _, _ = make_event(N, L, "Pb", 4.0, 7)
+        cfg = ipg.Config(size=N, L=L, Ny=12, maxtime=0.2, precision=prec, seed=5)
+        with ipg.Event(cfg) as ev:
+            ev.set_g2mu(gA, gB); ev.use_device_noise(); ev.init_fields(); ev.run()
+            for name, f in (("ux", ipg.UX), ("uy", ipg.UY), ("e1", ipg.E1), ("e2", ipg.E2),
+                            ("phi", ipg.PHI), ("pi", ipg.PI)):
+                out[f"{tag}{name}{N}"] = ev.get_field(f)
+np.savez(sys.argv[2], **out)
+'''
+
+
+def test_tile_kernels_match_plain_load_kernels_bit_for_bit(tmp_path):
+    """The TMA-staged tile kernels (default) and the plain-load kernels
+    (IPG_FP32_KERNEL=pair, IPG_FP64_KERNEL=site) run the same per-site code,
+    so whole events agree to the bit in both forms, edge tiles included."""
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = str(Path(__file__).resolve().parent.parent)
+    script = tmp_path / "dump.py"
+    script.write_text(_DUMP)
+    runs = {}
+    for tag, env in (("tile", {}), ("plain", {"IPG_FP32_KERNEL": "pair", "IPG_FP64_KERNEL": "site"})):
+        e = dict(os.environ)
+        e.pop("IPG_FP32_KERNEL", None)
+        e.pop("IPG_FP64_KERNEL", None)
+        e.update(env)
+        out = tmp_path / f"{tag}.npz"
+        subprocess.run([sys.executable, str(script), root, str(out)], env=e, check=True,
+                       timeout=600)
+        runs[tag] = np.load(out)
+    a, b = runs["tile"], runs["plain"]
+    assert sorted(a.files) == sorted(b.files) and len(a.files) == 24
+    for k in a.files:
+        assert np.array_equal(a[k], b[k]), k
