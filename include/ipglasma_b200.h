@@ -121,7 +121,9 @@ ipg_status ipg_time_grid(const ipg_ctx *ctx, double *dtau, int *itmax);
 
 /* g^2 mu^2 maps of both nuclei, lattice units, [N*N] host arrays; replaces
  * Cell::setg2mu2A/B as filled by Init::setColorChargeDensity
- * (Init.cpp:753-1676). */
+ * (Init.cpp:753-1676). The copies are queued on the context's stream: from
+ * page-locked memory they are read after the call returns, so keep the
+ * arrays unchanged until the next call that waits (ipg_init_fields). */
 ipg_status ipg_set_g2mu(ipg_ctx *ctx, const double *g2mu2A,
                         const double *g2mu2B);
 /* same, device pointers (no host copy) */

@@ -886,10 +886,14 @@ ipg_status ipg_get_observables(ipg_ctx *c, double *eps, double *u4,
     if (!c) return IPG_ERR_BAD_CONFIG;
     if (!c->finished) return fail(c, IPG_ERR_STATE, "call ipg_run first");
     const size_t n = c->n;
-    if (eps) IPG_CUDA(c, cudaMemcpy(eps, c->eps, sizeof(double) * n, cudaMemcpyDeviceToHost));
-    if (u4) IPG_CUDA(c, cudaMemcpy(u4, c->u4, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost));
-    if (pi10) IPG_CUDA(c, cudaMemcpy(pi10, c->pi10, sizeof(double) * 10 * n, cudaMemcpyDeviceToHost));
-    if (T10) IPG_CUDA(c, cudaMemcpy(T10, c->T10, sizeof(double) * 10 * n, cudaMemcpyDeviceToHost));
+    // enqueued on the context's stream, one wait at the end (full speed when
+    // the destinations are pinned; pageable ones are staged by the driver)
+    const auto d2h = cudaMemcpyDeviceToHost;
+    if (eps) IPG_CUDA(c, cudaMemcpyAsync(eps, c->eps, sizeof(double) * n, d2h, c->stream));
+    if (u4) IPG_CUDA(c, cudaMemcpyAsync(u4, c->u4, sizeof(double) * 4 * n, d2h, c->stream));
+    if (pi10) IPG_CUDA(c, cudaMemcpyAsync(pi10, c->pi10, sizeof(double) * 10 * n, d2h, c->stream));
+    if (T10) IPG_CUDA(c, cudaMemcpyAsync(T10, c->T10, sizeof(double) * 10 * n, d2h, c->stream));
+    IPG_TRY(sync(c));
     return IPG_OK;
 }
 
