@@ -95,13 +95,20 @@ template <int LOGN>
 constexpr int col_threads() {
     return cols_per_block<LOGN>() * ((1 << LOGN) / 8);
 }
+// sequence stride of the forward row kernel: there lanes 2i and 2i+1 hold the
+// same points of neighbouring sequences (channels 2h, 2h+1), so the stride is
+// made 4 mod 8 (in 16-byte units) to put the pair half a bank cycle apart;
+// with fft_seq_stride (1 mod 8) lane 2i+1 met lane 2i+2 on the same banks
+constexpr int fwd_seq_stride(int N) {
+    return fft_seq_stride(N) + ((12 - fft_seq_stride(N) % 8) % 8);
+}
 
 }  // namespace
 
 template <int LOGN>
 __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_fwd(WilsonArgs w, int k0) {
     constexpr int N = 1 << LOGN, TPS = N / 8, RPB = rows_per_block<LOGN>();
-    constexpr int S = fft_seq_stride(N);
+    constexpr int S = fwd_seq_stride(N);
     extern __shared__ __align__(16) unsigned char smraw[];
     C<double> *sm = reinterpret_cast<C<double> *>(smraw);
     const size_t n = (size_t)N * N;
@@ -250,16 +257,17 @@ static void launch_sheets(const WilsonArgs &w, int k0, int ns, cudaStream_t st) 
     constexpr int N = 1 << LOGN;
     constexpr int RPB = rows_per_block<LOGN>(), JB = cols_per_block<LOGN>();
     const size_t row_smem = sizeof(double2) * RPB * 4 * fft_seq_stride(N);
+    const size_t fwd_smem = sizeof(double2) * RPB * 4 * fwd_seq_stride(N);
     const size_t col_smem = sizeof(double2) * JB * fft_seq_stride(N);
     // the attribute is per device: set it on every launch (a host-side call
     // without a device round trip)
     cudaFuncSetAttribute(k_rows_fwd<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)row_smem);
+                         (int)fwd_smem);
     cudaFuncSetAttribute(k_rows_inv<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)row_smem);
     cudaFuncSetAttribute(k_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)col_smem);
-    k_rows_fwd<LOGN><<<dim3(N / RPB, ns), row_threads<LOGN>(), row_smem, st>>>(w, k0);
+    k_rows_fwd<LOGN><<<dim3(N / RPB, ns), row_threads<LOGN>(), fwd_smem, st>>>(w, k0);
     k_cols<LOGN><<<dim3(N / JB, 4, ns), col_threads<LOGN>(), col_smem, st>>>(w);
     k_rows_inv<LOGN><<<dim3(N / RPB, ns), row_threads<LOGN>(), row_smem, st>>>(w);
     const size_t n = (size_t)N * N;
