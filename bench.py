@@ -41,7 +41,17 @@ WORKLOAD = dict(name="PbPb_512", N=512, L=40.0, nucleus="Pb", b=6.0, Ny=50,
 METRIC = "site-updates/s & events/s: FP32-batched vs plain FP64 at stated err; adjoint/fwd"
 # algorithmic bytes per site-update of the fused leapfrog: every state word read
 # once and written once (links 2 x 18, E 2 x 8, phi 9, pi 9 = 70 reals)
-BYTES_PER_SITE_UPDATE = {"fp32": 2 * 70 * 4, "fp64": 2 * 70 * 8}
+# Algorithmic bytes of one site advanced one full step (each state word read
+# once and written once):
+#   FP32 bulk form: the compact count, two links of 18 reals and four su(3)
+#     fields of 8 reals, 2 x 68 x 4 B = 544 B;
+#   FP64 plain form: the reference's layout, six full 3x3 complex matrices
+#     (Ux, Uy, E1, E2, phi, pi), 2 x 108 x 8 B = 1728 B.
+# The kernels store 70 reals per site (E traceless in 8 reals, phi and pi
+# Hermitian in 9), so they move 560 B (FP32) and 1120 B (FP64) per update;
+# both figures are reported beside the roofline.
+BYTES_PER_SITE_UPDATE = {"fp32": 2 * 68 * 4, "fp64": 2 * 108 * 8}
+BYTES_STORED_PER_SITE_UPDATE = {"fp32": 2 * 70 * 4, "fp64": 2 * 70 * 8}
 
 
 def dist_env():
@@ -283,10 +293,14 @@ def run_ours(args, world, rank, local):
             "frac": round(achieved / hbm, 4), "traffic": traffic,
             "kernel": "k_leapfrog_tile (FP32 bulk: TMA-staged 8x32 tiles, both directions in packed f32x2 lanes)",
             "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp32"],
+            "bytes_stored_per_site_update": BYTES_STORED_PER_SITE_UPDATE["fp32"],
+            "stored_frac": round(su32 * BYTES_STORED_PER_SITE_UPDATE["fp32"] / 1e9 / hbm, 4),
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
             "fp64_kernel": {"kernel": "k_leapfrog_tile64 (FP64 plain form: TMA-staged 4x32 tiles)", "achieved": round(su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9, 1),
                             "frac": round(su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9 / hbm, 4),
-                            "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp64"]}}
+                            "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp64"],
+                            "bytes_stored_per_site_update": BYTES_STORED_PER_SITE_UPDATE["fp64"],
+                            "stored_frac": round(su64 * BYTES_STORED_PER_SITE_UPDATE["fp64"] / 1e9 / hbm, 4)}}
 
     batched = None if args.no_batched else measure_batched(torch, ipg, rank, dist)
     adjoint = None if args.no_adjoint else measure_adjoint(torch, ipg, rank)

@@ -20,7 +20,8 @@
 // followed by k_adj_se_links and k_adj_se_phi (they scatter into neighbouring
 // links and phi with FP64 atomics, so the summation order, not the result,
 // varies between runs).
-// The step is inverted exactly in exact arithmetic (k_inv_su, k_inv_se): this
+// The step is inverted exactly in exact arithmetic (k_inv_su and k_inv_se,
+// the latter in evolve.cu on the forward step's code): this
 // is the time reversal used to walk back between checkpoints.
 #include <cstdint>
 
@@ -102,6 +103,19 @@ __device__ __forceinline__ Md ld_adj(const C<double> *buf, size_t pos, size_t n)
     return ld_m3(buf, pos, n);
 }
 
+// diagonal (real parts) and upper triangle of an adjoint known to be
+// Hermitian; from_h of it rebuilds the stored matrix exactly
+__device__ __forceinline__ H3<double> ld_adj_h(const C<double> *buf, size_t pos, size_t n) {
+    H3<double> h;
+    h.d0 = buf[0 * n + pos].r;
+    h.d1 = buf[4 * n + pos].r;
+    h.d2 = buf[8 * n + pos].r;
+    h.o01 = buf[1 * n + pos];
+    h.o02 = buf[2 * n + pos];
+    h.o12 = buf[5 * n + pos];
+    return h;
+}
+
 // T2(X) = 1 + X + X^2 / 2
 __device__ __forceinline__ Md taylor2(const Md &x) {
     Md r = mul(x, x);
@@ -161,40 +175,6 @@ __device__ __forceinline__ StepGeom step_geom(int N, int ix, int iy) {
     return g;
 }
 
-// the E and pi increments of S_e at one site (before the traceless
-// projection of E): dE1, dE2, dpi
-__device__ __forceinline__ void se_increments(const State<double> &s, const StepGeom &G,
-                                              double cst, double cdt, Md &dE1, Md &dE2,
-                                              Md &dpi) {
-    const size_t n = (size_t)G.N * G.N;
-    const Md ux = ld_m3(s.ux, G.pos, n), uy = ld_m3(s.uy, G.pos, n);
-    const Md a = mul(ux, ld_m3(s.uy, G.pX, n));
-    const Md b = mul(uy, ld_m3(s.ux, G.pY, n));
-    const Md h12 = from_h(i_antiherm(mul_nd(a, b)));
-    Md t1 = h12, t2 = sc(h12, -1.);
-    {
-        const Md p = mul_nd(ux, ld_m3(s.uy, G.pXmY, n));
-        const Md q = mul_dn(ld_m3(s.ux, G.mY, n), ld_m3(s.uy, G.mY, n));
-        add_to(t1, from_h(i_antiherm(mul(p, q))));
-    }
-    {
-        const Md p = mul_nd(uy, ld_m3(s.ux, G.mXpY, n));
-        const Md q = mul_dn(ld_m3(s.uy, G.mX, n), ld_m3(s.ux, G.mX, n));
-        add_to(t2, from_h(i_antiherm(mul(p, q))));
-    }
-    const Md phi = ld_herm(s.phi, G.pos, n);
-    const Md phx = mul_nd(mul(ux, ld_herm(s.phi, G.pX, n)), ux);
-    const Md phy = mul_nd(mul(uy, ld_herm(s.phi, G.pY, n)), uy);
-    const Md ux_m = ld_m3(s.ux, G.mX, n), uy_m = ld_m3(s.uy, G.mY, n);
-    const Md bx = mul(mul_dn(ux_m, ld_herm(s.phi, G.mX, n)), ux_m);
-    const Md by = mul(mul_dn(uy_m, ld_herm(s.phi, G.mY, n)), uy_m);
-    dE1 = addm(sc(tl(t1), cst), sc(icomm(phx, phi), cdt));
-    dE2 = addm(sc(tl(t2), cst), sc(icomm(phy, phi), cdt));
-    Md br = addm(addm(phx, phy), addm(bx, by));
-    add_to(br, sc(phi, -4.));
-    dpi = sc(br, cdt);
-}
-
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -214,29 +194,6 @@ __global__ void k_inv_su(int N, State<double> nxt, State<double> cur, double c, 
     H3<double> phi = ld_h(nxt.phi, pos, n);
     h_axpy(phi, -c2, ld_h(nxt.pi, pos, n));
     st_h(cur.phi, pos, n, phi);
-}
-
-// pi = pi' - dpi(U, phi),  E_d = E_d' - TL(dE_d(U, phi)); do_pe = 0 copies
-__global__ void k_inv_se(int N, State<double> nxt, State<double> cur, double cst, double cdt,
-                         int do_pe) {
-    const size_t n = (size_t)N * N;
-    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (pos >= n) return;
-    H3<double> pi = ld_h(nxt.pi, pos, n);
-    H3<double> e1 = ld_h8(nxt.e1, pos, n), e2 = ld_h8(nxt.e2, pos, n);
-    if (do_pe) {
-        const StepGeom G = step_geom(N, (int)(pos / N), (int)(pos % N));
-        Md dE1, dE2, dpi;
-        se_increments(cur, G, cst, cdt, dE1, dE2, dpi);
-        h_axpy(pi, -1., to_h(dpi));
-        h_axpy(e1, -1., to_h(tl(dE1)));
-        h_axpy(e2, -1., to_h(tl(dE2)));
-        h_traceless(e1);
-        h_traceless(e2);
-    }
-    st_h(cur.pi, pos, n, pi);
-    st_h8(cur.e1, pos, n, e1);
-    st_h8(cur.e2, pos, n, e2);
 }
 
 // ---------------------------------------------------------------------------
@@ -276,6 +233,43 @@ __global__ void k_adj_su(int N, State<double> cur, State<double> nxt, AdjState a
     }
 }
 
+// The time reversal of S_u fused with its adjoint, for steps reached by
+// reversal: U_d = M_d^{-1} U_d' with M_d = T2(i c E_d'), phi = phi' - c2 pi'
+// are written to `cur` (as k_inv_su), then the adjoint of S_u runs with that
+// M_d and U_d (as k_adj_su, which would recompute M_d and reload U_d).
+__global__ void k_inv_adj_su(int N, State<double> nxt, State<double> cur, AdjState a, double c,
+                             double c2) {
+    const size_t n = (size_t)N * N;
+    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pos >= n) return;
+    {
+        H3<double> phi = ld_h(nxt.phi, pos, n);
+        h_axpy(phi, -c2, ld_h(nxt.pi, pos, n));
+        st_h(cur.phi, pos, n, phi);
+    }
+    const Md phib = herm(ld_adj(a.phi, pos, n));
+    Md pib = herm(ld_adj(a.pi, pos, n));
+    add_to(pib, sc(phib, c2));
+    st_m3(a.phi, pos, n, phib);
+    st_m3(a.pi, pos, n, pib);
+    for (int d = 0; d < 2; d++) {
+        C<double> *Ub = d ? a.uy : a.ux;
+        C<double> *Eb = d ? a.e2 : a.e1;
+        const Md X = times_i(ld_herm8(d ? nxt.e2 : nxt.e1, pos, n), c);
+        const Md M = taylor2(X);
+        const Md U = mul(inverse3(M), ld_m3(d ? nxt.uy : nxt.ux, pos, n));
+        st_m3(d ? cur.uy : cur.ux, pos, n, U);
+        const Md Ubar = ld_adj(Ub, pos, n);
+        st_m3(Ub, pos, n, mul_dn(M, Ubar));
+        const Md Mb = mul_nd(Ubar, U);
+        Md Xb = Mb;
+        add_to(Xb, sc(addm(mul_nd(Mb, X), mul_dn(X, Mb)), 0.5));
+        Md Eb_ = ld_adj(Eb, pos, n);
+        add_to(Eb_, herm(times_i(Xb, -c)));
+        st_m3(Eb, pos, n, tl(herm(Eb_)));
+    }
+}
+
 // S_e, link part: the adjoints G_d of E_d' (traceless Hermitian, from
 // k_adj_su) through the plaquette and staple terms into the link adjoints
 // of the site and its neighbours (atomic)
@@ -285,46 +279,51 @@ __global__ void __launch_bounds__(128) k_adj_se_links(int N, State<double> cur, 
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
     const StepGeom G = step_geom(N, (int)(pos / N), (int)(pos % N));
-    const Md t1b = sc(ld_adj(a.e1, pos, n), cst), t2b = sc(ld_adj(a.e2, pos, n), cst);
-    const Md ux = ld_m3(cur.ux, pos, n), uy = ld_m3(cur.uy, pos, n);
-    Md uxb = {}, uyb = {};
-    // plaquette h12 = iAH(a b^dag), a = Ux Uy(+x), b = Uy Ux(+y); enters E1 (+), E2 (-)
-    {
+    // one of the three terms per thread (blockIdx.y: the plaquette, the E1
+    // staple, the E2 staple), which keeps a thread's live matrices within the
+    // register file. The adjoints of E1', E2' are stored exactly Hermitian
+    // (k_adj_su writes their traceless Hermitian part), so their diagonal and
+    // upper triangle are loaded and the full matrix rebuilt where it is used.
+    const int part = blockIdx.y;
+    if (part == 0) {
+        // plaquette h12 = iAH(a b^dag), a = Ux Uy(+x), b = Uy Ux(+y); enters E1 (+), E2 (-)
+        const H3<double> h1 = ld_adj_h(a.e1, pos, n), h2 = ld_adj_h(a.e2, pos, n);
+        const Md ux = ld_m3(cur.ux, pos, n), uy = ld_m3(cur.uy, pos, n);
         const Md uy_px = ld_m3(cur.uy, G.pX, n), ux_py = ld_m3(cur.ux, G.pY, n);
         const Md A = mul(ux, uy_px), B = mul(uy, ux_py);
-        const Md Mb = times_i(minus(t1b, t2b), -2.);
+        const Md Mb = times_i(minus(sc(from_h(h1), cst), sc(from_h(h2), cst)), -2.);
         const Md Ab = mul(Mb, B), Bb = mul_dn(Mb, A);
-        add_to(uxb, mul_nd(Ab, uy_px));
+        atomic_add_m(a.ux, pos, n, mul_nd(Ab, uy_px));
         atomic_add_m(a.uy, G.pX, n, mul_dn(ux, Ab));
-        add_to(uyb, mul_nd(Bb, ux_py));
+        atomic_add_m(a.uy, pos, n, mul_nd(Bb, ux_py));
         atomic_add_m(a.ux, G.pY, n, mul_dn(uy, Bb));
-    }
-    // staple of E1: p = Ux Uy(+x-y)^dag, q = Ux(-y)^dag Uy(-y)
-    {
+    } else if (part == 1) {
+        // staple of E1: p = Ux Uy(+x-y)^dag, q = Ux(-y)^dag Uy(-y)
+        const H3<double> h1 = ld_adj_h(a.e1, pos, n);
+        const Md ux = ld_m3(cur.ux, pos, n);
         const Md uy_pxmy = ld_m3(cur.uy, G.pXmY, n);
         const Md ux_my = ld_m3(cur.ux, G.mY, n), uy_my = ld_m3(cur.uy, G.mY, n);
         const Md P = mul_nd(ux, uy_pxmy), Q = mul_dn(ux_my, uy_my);
-        const Md Mb = times_i(t1b, -2.);
+        const Md Mb = times_i(sc(from_h(h1), cst), -2.);
         const Md Pb = mul_nd(Mb, Q), Qb = mul_dn(P, Mb);
-        add_to(uxb, mul(Pb, uy_pxmy));
+        atomic_add_m(a.ux, pos, n, mul(Pb, uy_pxmy));
         atomic_add_m(a.uy, G.pXmY, n, mul_dn(Pb, ux));
         atomic_add_m(a.ux, G.mY, n, mul_nd(uy_my, Qb));
         atomic_add_m(a.uy, G.mY, n, mul(ux_my, Qb));
-    }
-    // staple of E2: p = Uy Ux(-x+y)^dag, q = Uy(-x)^dag Ux(-x)
-    {
+    } else {
+        // staple of E2: p = Uy Ux(-x+y)^dag, q = Uy(-x)^dag Ux(-x)
+        const H3<double> h2 = ld_adj_h(a.e2, pos, n);
+        const Md uy = ld_m3(cur.uy, pos, n);
         const Md ux_mxpy = ld_m3(cur.ux, G.mXpY, n);
         const Md uy_mx = ld_m3(cur.uy, G.mX, n), ux_mx = ld_m3(cur.ux, G.mX, n);
         const Md P = mul_nd(uy, ux_mxpy), Q = mul_dn(uy_mx, ux_mx);
-        const Md Mb = times_i(t2b, -2.);
+        const Md Mb = times_i(sc(from_h(h2), cst), -2.);
         const Md Pb = mul_nd(Mb, Q), Qb = mul_dn(P, Mb);
-        add_to(uyb, mul(Pb, ux_mxpy));
+        atomic_add_m(a.uy, pos, n, mul(Pb, ux_mxpy));
         atomic_add_m(a.ux, G.mXpY, n, mul_dn(Pb, uy));
         atomic_add_m(a.uy, G.mX, n, mul_nd(ux_mx, Qb));
         atomic_add_m(a.ux, G.mX, n, mul(uy_mx, Qb));
     }
-    atomic_add_m(a.ux, pos, n, uxb);
-    atomic_add_m(a.uy, pos, n, uyb);
 }
 
 // S_e, transport part: the commutator terms of E and the pi bracket into the
@@ -675,7 +674,22 @@ void launch_inverse_step(int N, const State<double> &nxt, const State<double> &c
     const double cst = cf.tau * cf.dt_pe / (2. * cf.g * cf.g);
     const double cdt = cf.tau > 0 ? cf.dt_pe / cf.tau : 0.;
     k_inv_su<<<blocks(n), 128, 0, st>>>(N, nxt, cur, c, c2);
-    k_inv_se<<<blocks(n), 128, 0, st>>>(N, nxt, cur, cst, cdt, cf.do_pe);
+    launch_inverse_se(N, nxt, cur, cf, st);
+}
+
+void launch_inverse_adjoint_step(int N, const State<double> &nxt, const State<double> &cur,
+                                 const AdjState &a, const StepCoef<double> &cf, cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    const double c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / 2.);
+    const double c2 = (cf.tau + cf.dt_pu / 2.) * cf.dt_pu;
+    const double cst = cf.tau * cf.dt_pe / (2. * cf.g * cf.g);
+    const double cdt = cf.tau > 0 ? cf.dt_pe / cf.tau : 0.;
+    k_inv_adj_su<<<blocks(n), 128, 0, st>>>(N, nxt, cur, a, c, c2);
+    launch_inverse_se(N, nxt, cur, cf, st);
+    if (cf.do_pe) {
+        k_adj_se_links<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, cst);
+        k_adj_se_phi<<<blocks(n), 128, 0, st>>>(N, cur, a, cdt);
+    }
 }
 
 void launch_adjoint_step(int N, const State<double> &cur, const State<double> &nxt,
@@ -687,7 +701,7 @@ void launch_adjoint_step(int N, const State<double> &cur, const State<double> &n
     if (cf.do_pe) {
         const double cst = cf.tau * cf.dt_pe / (2. * cf.g * cf.g);
         const double cdt = cf.dt_pe / cf.tau;
-        k_adj_se_links<<<blocks(n), 128, 0, st>>>(N, cur, a, cst);
+        k_adj_se_links<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, cst);
         k_adj_se_phi<<<blocks(n), 128, 0, st>>>(N, cur, a, cdt);
     }
 }

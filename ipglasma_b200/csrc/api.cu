@@ -1222,14 +1222,14 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
     for (int s = S - 1, q = 0; s >= 0; s--, q++) {
         const State<double> cur = sets[q & 1];
         const StepCoef<double> cf = evolution_coef(c, s);
-        if (s % A.k == 0)
+        if (s % A.k == 0) {
             IPG_TRY(copy_state(c, cur, A.cp[s / A.k]));
-        else {
-            launch_inverse_step(N, nxt, cur, cf, c->stream);
-            IPG_LAUNCHED(c, 2);
+            launch_adjoint_step(N, cur, nxt, A.adj, cf, c->stream);
+            IPG_LAUNCHED(c, cf.do_pe ? 3 : 1);
+        } else {
+            launch_inverse_adjoint_step(N, nxt, cur, A.adj, cf, c->stream);
+            IPG_LAUNCHED(c, cf.do_pe ? 4 : 2);
         }
-        launch_adjoint_step(N, cur, nxt, A.adj, cf, c->stream);
-        IPG_LAUNCHED(c, cf.do_pe ? 3 : 1);
         nxt = cur;
     }
     launch_adjoint_project(n, A.adj, c->stream);

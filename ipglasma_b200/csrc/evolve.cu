@@ -143,10 +143,9 @@ struct FullLoadGlobal {
 // cf.do_pu is set. The site's own links and phi are loaded again at each use
 // rather than held (from a shared-memory tile that is cheaper than keeping
 // 90 registers live across the site, which spilled).
-template <typename T, bool REUNIT, class Ld>
-__device__ __forceinline__ void leapfrog_full_core(const Ld &ld, const StepCoef<T> &cf,
-                                                   M3<T> &nx, M3<T> &ny, H3<T> &phin) {
-    if (cf.do_pe) {
+// The staple sums of E1 and E2 at one site, traceless (Evolution.cpp:228-275).
+template <typename T, class Ld>
+__device__ __forceinline__ void full_staples(const Ld &ld, H3<T> &t1, H3<T> &t2) {
         // plaquette U12 = Ux Uy(x+1) Ux(y+1)^dag Uy^dag  (Evolution.cpp:228-232)
         H3<T> h12;
         {
@@ -156,14 +155,13 @@ __device__ __forceinline__ void leapfrog_full_core(const Ld &ld, const StepCoef<
             h12 = i_antiherm(u12);
         }
         // E1 staple sum: U12 + U1m2 - h.c.  (234-257)
-        H3<T> t1 = h12;
+        t1 = h12;
         {
             M3<T> p = mul_nd(ld.template link<kLx, 0, 0>(), ld.template link<kLy, 1, -1>());
             M3<T> q = mul_dn(ld.template link<kLx, 0, -1>(), ld.template link<kLy, 0, -1>());
             h_add(t1, i_antiherm_mul(p, q));
         }
         // E2 staple sum: U12^dag + U2m1 - h.c.  (240-244, 266-275)
-        H3<T> t2;
         {
             M3<T> p = mul_nd(ld.template link<kLy, 0, 0>(), ld.template link<kLx, -1, 1>());
             M3<T> q = mul_dn(ld.template link<kLy, -1, 0>(), ld.template link<kLx, -1, 0>());
@@ -172,6 +170,14 @@ __device__ __forceinline__ void leapfrog_full_core(const Ld &ld, const StepCoef<
         }
         h_traceless(t1);
         h_traceless(t2);
+}
+
+template <typename T, bool REUNIT, class Ld>
+__device__ __forceinline__ void leapfrog_full_core(const Ld &ld, const StepCoef<T> &cf,
+                                                   M3<T> &nx, M3<T> &ny, H3<T> &phin) {
+    if (cf.do_pe) {
+        H3<T> t1, t2;
+        full_staples<T>(ld, t1, t2);
 
         H3<T> pi = ld.pi();
         H3<T> e1 = ld.e1();
@@ -238,6 +244,59 @@ __device__ __forceinline__ void leapfrog_full_site(int N, int ix, int iy, const 
         st_m3(ux_out, ld.pos, ld.n, nx);
         st_m3(uy_out, ld.pos, ld.n, ny);
     }
+}
+
+// Time reversal of the E and pi half of a step (the inverse of S_e): with U
+// and phi of the step's input already recovered in `cur`,
+//   pi = pi' - cdt br(U, phi),   E_d = E_d' - TL(cst t_d + cdt i[U_d phi(+d) U_d^dag, phi])
+// from the same staple and transport code as the forward step.
+__global__ void __launch_bounds__(128)
+    k_inv_se(int N, State<double> nxt, State<double> cur, StepCoef<double> cf) {
+    const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ix = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= N || iy >= N) return;
+    const FullLoadGlobal<double> ld(cur, N, ix, iy);
+    const size_t pos = ld.pos, n = ld.n;
+    H3<double> pi = ld_h(nxt.pi, pos, n);
+    H3<double> e1 = ld_h8(nxt.e1, pos, n), e2 = ld_h8(nxt.e2, pos, n);
+    if (cf.do_pe) {
+        H3<double> t1, t2;
+        full_staples<double>(ld, t1, t2);
+        const double cst = cf.tau * cf.dt_pe / (2. * cf.g * cf.g);
+        const double cdt = cf.dt_pe / cf.tau;
+        H3<double> d1 = {}, d2 = {};
+        h_axpy(d1, cst, t1);
+        h_axpy(d2, cst, t2);
+        H3<double> br;
+        {
+            H3<double> phx = conj_h(ld.template link<kLx, 0, 0>(), ld.template phi<1, 0>());
+            h_axpy(d1, cdt, i_commutator(phx, ld.template phi<0, 0>()));
+            br = phx;
+        }
+        {
+            H3<double> phy = conj_h(ld.template link<kLy, 0, 0>(), ld.template phi<0, 1>());
+            h_axpy(d2, cdt, i_commutator(phy, ld.template phi<0, 0>()));
+            h_add(br, phy);
+        }
+        h_add(br, conj_h_dag(ld.template link<kLx, -1, 0>(), ld.template phi<-1, 0>()));
+        h_add(br, conj_h_dag(ld.template link<kLy, 0, -1>(), ld.template phi<0, -1>()));
+        h_axpy(br, -4., ld.template phi<0, 0>());
+        h_axpy(pi, -cdt, br);
+        h_traceless(d1);
+        h_traceless(d2);
+        h_axpy(e1, -1., d1);
+        h_axpy(e2, -1., d2);
+        h_traceless(e1);
+        h_traceless(e2);
+    }
+    st_h(cur.pi, pos, n, pi);
+    st_h8(cur.e1, pos, n, e1);
+    st_h8(cur.e2, pos, n, e2);
+}
+
+void launch_inverse_se(int N, const State<double> &nxt, const State<double> &cur,
+                       const StepCoef<double> &cf, cudaStream_t st) {
+    k_inv_se<<<dim3((N + 31) / 32, (N + 3) / 4), dim3(32, 4), 0, st>>>(N, nxt, cur, cf);
 }
 
 template <typename T, bool REUNIT>

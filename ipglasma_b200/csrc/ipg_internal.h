@@ -169,6 +169,14 @@ struct AdjState {
 // time reversal of one FP64 step: state after (nxt) -> state before (cur)
 void launch_inverse_step(int N, const State<double> &nxt, const State<double> &cur,
                          const StepCoef<double> &cf, cudaStream_t st);
+// E and pi of the step's input from its output nxt and the recovered U, phi
+// in cur (evolve.cu)
+void launch_inverse_se(int N, const State<double> &nxt, const State<double> &cur,
+                       const StepCoef<double> &cf, cudaStream_t st);
+// the time reversal nxt -> cur and the adjoint step together (fewer launches
+// than launch_inverse_step then launch_adjoint_step, same results)
+void launch_inverse_adjoint_step(int N, const State<double> &nxt, const State<double> &cur,
+                                 const AdjState &a, const StepCoef<double> &cf, cudaStream_t st);
 // adjoints of a step's outputs -> adjoints of its inputs (in place); cur is the
 // state before the step, nxt the state after it
 void launch_adjoint_step(int N, const State<double> &cur, const State<double> &nxt,
