@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_fwd(WilsonArgs w, 
 }
 
 template <int LOGN>
-__global__ void __launch_bounds__(col_threads<LOGN>()) k_cols(WilsonArgs w) {
+__global__ void __launch_bounds__(col_threads<LOGN>(), 2) k_cols(WilsonArgs w) {
     constexpr int N = 1 << LOGN, TPS = N / 8, JB = cols_per_block<LOGN>();
     constexpr int S = fft_seq_stride(N);
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -198,9 +198,11 @@ __global__ void __launch_bounds__(col_threads<LOGN>()) k_cols(WilsonArgs w) {
         const double2 v = base[(size_t)(t + m * TPS) * N];
         x[m] = {v.x, v.y};
     }
+    fft_regs<LOGN, double, false>(x, sm + q * S, t, tw);
+    // the Green factors are loaded after the forward transform: that keeps
+    // the kernel within 64 registers, two 512-thread blocks per SM
 #pragma unroll
     for (int m = 0; m < 8; m++) gk[m] = w.green[(size_t)(t + m * TPS) * N + col];
-    fft_regs<LOGN, double, false>(x, sm + q * S, t, tw);
 #pragma unroll
     for (int m = 0; m < 8; m++) x[m] = {x[m].r * gk[m], x[m].i * gk[m]};
     fft_regs<LOGN, double, true>(x, sm + q * S, t, tw);
@@ -227,9 +229,11 @@ __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_inv(WilsonArgs w) 
         x[m] = {v.x, v.y};
     }
     fft_regs<LOGN, double, true>(x, sm + seq * S, t, tw);
-    const double ntot = (double)n;
+    // n = N^2 is a power of two, so multiplying by 1/n is exact and gives
+    // the same bits as the reference's division by n
+    const double inv_n = 1.0 / (double)n;
 #pragma unroll
-    for (int m = 0; m < 8; m++) p[m * TPS] = make_double2(x[m].r / ntot, x[m].i / ntot);
+    for (int m = 0; m < 8; m++) p[m * TPS] = make_double2(x[m].r * inv_n, x[m].i * inv_n);
 }
 
 // V <- exp(-i A_k.t) V for the sheets of the batch, in ascending k
