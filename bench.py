@@ -336,6 +336,7 @@ def run_ours(args, world, rank, local):
             "e2e": {"value": round(whole_job_rate(world, K, e2e["ms"]), 3), "unit": "events/s",
                     "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
                     "form": "fp32", "host_buffers": e2e["host_buffers"]},
+            "writers": e2e["writers"] if rank == 0 else None,
             "roofline": roof,
             "batched": batched,
             "adjoint": adjoint,
@@ -551,9 +552,43 @@ def measure_e2e(torch, ipg, A, B, K, seed0, l2buf, dist):
         one(seed0 + 10 + k)
         torch.cuda.synchronize()
         total += time.perf_counter() - t0
+    itmax = ev.itmax
+    dtau = ev.dtau
     ev.close()
+    writers = measure_writers(ipg, eps, u4, pi10, T10, itmax, dtau)
     return {"ms": total * 1e3, "h2d": int(2 * n * 8), "d2h": int(25 * n * 8),
-            "host_buffers": "pinned"}
+            "host_buffers": "pinned", "writers": writers}
+
+
+def measure_writers(ipg, eps, u4, pi10, T10, itmax, dtau):
+    """Host output formatting, timed apart from the event rate: the
+    reference's hydro and T^munu files of one event (sizeOutput = N over the
+    lattice, one eta slice) written from its observables into a scratch
+    directory that is removed afterwards."""
+    import ctypes as ct
+    import shutil
+    import tempfile
+    N, L = WORKLOAD["N"], WORKLOAD["L"]
+    lib = ipg.lib()
+    D = ct.c_double
+    V = lambda a: ct.c_void_p(a.ctypes.data)  # noqa: E731
+    d = tempfile.mkdtemp(prefix="ipg_writers_")
+    try:
+        hydro, tmunu = os.path.join(d, "hydro.dat"), os.path.join(d, "tmunu.dat")
+        t0 = time.perf_counter()
+        st = lib.ipg_write_hydro(hydro.encode(), N, D(L), N, D(L), 1, D(0.0), itmax, D(dtau),
+                                 V(eps), V(u4), V(pi10), D(1.0), None)
+        t1 = time.perf_counter()
+        st2 = lib.ipg_write_tmunu(tmunu.encode(), N, D(L), N, D(L), 1, D(0.0), itmax, D(dtau),
+                                  V(T10), D(1.0))
+        t2 = time.perf_counter()
+        sizes = os.path.getsize(hydro) + os.path.getsize(tmunu)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    threads = os.environ.get("IPG_WRITER_THREADS") or str(os.cpu_count())
+    return {"ms_hydro": round((t1 - t0) * 1e3, 1), "ms_tmunu": round((t2 - t1) * 1e3, 1),
+            "bytes": int(sizes), "threads": int(threads), "status": [int(st), int(st2)],
+            "timing": "host wall clock, once per bench run; not part of the event rate"}
 
 
 def load_peaks():
