@@ -71,31 +71,39 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.samples = []
-        self._stop = threading.Event()
+        self._proc = None
         self._t = None
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(
-                    ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                     "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                parts = [p.strip() for p in out.stdout.strip().split(",")]
-                if len(parts) == 7:
-                    self.samples.append(parts)
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        # one streaming nvidia-smi (a line every 50 ms) for the whole region
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.strip().split(",")]
+            if len(parts) == 7:
+                self.samples.append(parts)
 
     def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
-        self._t.start()
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+            time.sleep(0.1)  # the first line before the timed work starts
+        except Exception:
+            self._proc = None
         return self
 
     def __exit__(self, *exc):
-        self._stop.set()
-        if self._t:
-            self._t.join(timeout=10)
+        if self._proc is not None:
+            time.sleep(0.06)  # one more line after the timed work
+            self._proc.terminate()  # this process only, by its handle
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+            if self._t:
+                self._t.join(timeout=5)
 
     def summary(self):
         if not self.samples:
