@@ -60,16 +60,19 @@ void launch_link_products(int N, C<double> *VA, C<double> *VB, C<double> *u1x,
 // ---------------------------------------------------------------------------
 
 // LU with partial pivoting and solve, in the elimination order of the
-// GSL 2.5 routines the reference calls (Init.cpp:47-63)
-__device__ void lu_solve8(double J[64], const double F[8], double x[8]) {
+// GSL 2.5 routines the reference calls (Init.cpp:47-63). Entry (r, c) of the
+// 8 x 8 matrix is J[(8 r + c) * js]: the Newton kernel keeps each thread's
+// matrix in shared memory with a stride of the block size (the pivoting
+// indexes it by data, which would otherwise put it in local memory).
+__device__ void lu_solve8(double *J, int js, const double F[8], double x[8]) {
     int perm[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) perm[i] = i;
     for (int col = 0; col < 7; col++) {
         int piv = col;
-        double best = fabs(J[col * 8 + col]);
+        double best = fabs(J[(col * 8 + col) * js]);
         for (int row = col + 1; row < 8; row++) {
-            double c = fabs(J[row * 8 + col]);
+            double c = fabs(J[(row * 8 + col) * js]);
             if (c > best) {
                 best = c;
                 piv = row;
@@ -77,20 +80,20 @@ __device__ void lu_solve8(double J[64], const double F[8], double x[8]) {
         }
         if (piv != col) {
             for (int k = 0; k < 8; k++) {
-                double t = J[col * 8 + k];
-                J[col * 8 + k] = J[piv * 8 + k];
-                J[piv * 8 + k] = t;
+                double t = J[(col * 8 + k) * js];
+                J[(col * 8 + k) * js] = J[(piv * 8 + k) * js];
+                J[(piv * 8 + k) * js] = t;
             }
             int t = perm[col];
             perm[col] = perm[piv];
             perm[piv] = t;
         }
-        const double d = J[col * 8 + col];
+        const double d = J[(col * 8 + col) * js];
         if (d != 0.0) {
             for (int row = col + 1; row < 8; row++) {
-                const double l = J[row * 8 + col] / d;
-                J[row * 8 + col] = l;
-                for (int k = col + 1; k < 8; k++) J[row * 8 + k] -= l * J[col * 8 + k];
+                const double l = J[(row * 8 + col) * js] / d;
+                J[(row * 8 + col) * js] = l;
+                for (int k = col + 1; k < 8; k++) J[(row * 8 + k) * js] -= l * J[(col * 8 + k) * js];
             }
         }
     }
@@ -98,13 +101,13 @@ __device__ void lu_solve8(double J[64], const double F[8], double x[8]) {
     for (int i = 0; i < 8; i++) y[i] = F[perm[i]];
     for (int i = 1; i < 8; i++) {
         double acc = y[i];
-        for (int j = 0; j < i; j++) acc -= J[i * 8 + j] * y[j];
+        for (int j = 0; j < i; j++) acc -= J[(i * 8 + j) * js] * y[j];
         y[i] = acc;
     }
     for (int i = 7; i >= 0; i--) {
         double acc = y[i];
-        for (int j = i + 1; j < 8; j++) acc -= J[i * 8 + j] * y[j];
-        y[i] = acc / J[i * 8 + i];
+        for (int j = i + 1; j < 8; j++) acc -= J[(i * 8 + j) * js] * y[j];
+        y[i] = acc / J[(i * 8 + i) * js];
     }
     for (int i = 0; i < 8; i++) x[i] = y[i];
 }
@@ -118,7 +121,13 @@ __device__ __forceinline__ void restart_alpha(double alpha[8], uint64_t key,
     for (int a = 0; a < 8; a++) alpha[a] = z[a];
 }
 
-__global__ void __launch_bounds__(128) k_newton(NewtonArgs A) {
+constexpr int kNewtonThreads = 128;
+
+__global__ void __launch_bounds__(kNewtonThreads) k_newton(NewtonArgs A) {
+    // this thread's Jacobian, element k at J[k * kNewtonThreads]
+    extern __shared__ double newton_j[];
+    double *J = newton_j + threadIdx.x;
+    constexpr int js = kNewtonThreads;
     const size_t n = (size_t)A.N * A.N;
     const size_t lid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (lid >= 2 * n) return;
@@ -135,7 +144,7 @@ __global__ void __launch_bounds__(128) k_newton(NewtonArgs A) {
     C<double> traceCache[8];
     trace_ta(minus(S, Sd), traceCache);
 
-    double alpha[8], dalpha[8], Fa[8], J[64];
+    double alpha[8], dalpha[8], Fa[8];
 #pragma unroll
     for (int a = 0; a < 8; a++) alpha[a] = 0.;
     M3<double> Usol = mul(exp_from_coeff(alpha), U0);
@@ -171,8 +180,8 @@ __global__ void __launch_bounds__(128) k_newton(NewtonArgs A) {
             trace_ta(Mt, tl);
             double mcheck = 0.;
             for (int a = 0; a < 8; a++) {
-                J[a * 8 + b] = 2. * tl[a].i / d;
-                mcheck += fabs(J[a * 8 + b]);
+                J[(a * 8 + b) * js] = 2. * tl[a].i / d;
+                mcheck += fabs(J[(a * 8 + b) * js]);
                 if (mcheck < 1e-15) good = false;
             }
             alpha[b] = alpha[b] - d;
@@ -183,11 +192,11 @@ __global__ void __launch_bounds__(128) k_newton(NewtonArgs A) {
                 const M3<double> Mt = ta_mul(b, Usold);
                 for (int a = 0; a < 8; a++) {
                     const M3<double> Ma = ta_mul(a, S);
-                    J[a * 8 + b] = -2. * re_trace_mul(Ma, Mt);
+                    J[(a * 8 + b) * js] = -2. * re_trace_mul(Ma, Mt);
                 }
             }
         }
-        lu_solve8(J, Fa, dalpha);
+        lu_solve8(J, js, Fa, dalpha);
         bool ok = true;
         for (int a = 0; a < 8; a++)
             if (fabs(dalpha[a]) > 1e5) {
@@ -251,9 +260,9 @@ __global__ void __launch_bounds__(128) k_newton(NewtonArgs A) {
                 sub_from(Mt, mul_nd(dU, S));
                 C<double> tl[8];
                 trace_ta(Mt, tl);
-                for (int a = 0; a < 8; a++) J[a * 8 + b] = -tl[a].i;
+                for (int a = 0; a < 8; a++) J[(a * 8 + b) * js] = -tl[a].i;
             }
-            lu_solve8(J, F, dalpha);
+            lu_solve8(J, js, F, dalpha);
             for (int a = 0; a < 8; a++) alpha[a] -= dalpha[a];
             Usol = mul(exp_from_coeff(alpha), U0);
             Usold = dagger(Usol);
@@ -270,7 +279,10 @@ __global__ void __launch_bounds__(128) k_newton(NewtonArgs A) {
 
 void launch_newton(const NewtonArgs &a, cudaStream_t st) {
     const size_t links = 2 * (size_t)a.N * a.N;
-    k_newton<<<(unsigned)((links + 127) / 128), 128, 0, st>>>(a);
+    const size_t smem = sizeof(double) * 64 * kNewtonThreads;  // 64 KB
+    cudaFuncSetAttribute(k_newton, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_newton<<<(unsigned)((links + kNewtonThreads - 1) / kNewtonThreads), kNewtonThreads, smem,
+               st>>>(a);
 }
 
 // ---------------------------------------------------------------------------
