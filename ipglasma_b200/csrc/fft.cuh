@@ -128,11 +128,29 @@ __device__ __forceinline__ void pass_twiddles(int t, const C<T> *__restrict__ tw
         for (int b = 0; b < NB; b++) {
             const int j = t + b * (N / 8);
             const int step = (j & (NS - 1)) * (N / (NS * R));
+            if constexpr (R == 8) {
+                // one table read, the other six powers by products: the
+                // twiddle loads were most of the loads of the row and column
+                // kernels, which are load-latency bound (the products are
+                // within 1e-15 of the table values, a few ulp)
+                C<T> w1 = tw[step];
+                if (INV) w1.i = -w1.i;
+                const C<T> w2 = cmul(w1, w1), w4 = cmul(w2, w2);
+                const C<T> w3 = cmul(w2, w1);
+                w[b * R + 1] = w1;
+                w[b * R + 2] = w2;
+                w[b * R + 3] = w3;
+                w[b * R + 4] = w4;
+                w[b * R + 5] = cmul(w4, w1);
+                w[b * R + 6] = cmul(w4, w2);
+                w[b * R + 7] = cmul(w4, w3);
+            } else {
 #pragma unroll
-            for (int r = 1; r < R; r++) {
-                C<T> x = tw[r * step];
-                if (INV) x.i = -x.i;
-                w[b * R + r] = x;
+                for (int r = 1; r < R; r++) {
+                    C<T> x = tw[r * step];
+                    if (INV) x.i = -x.i;
+                    w[b * R + r] = x;
+                }
             }
         }
     }
