@@ -34,6 +34,11 @@ struct ipg_ctx {
     int itmax = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // Wilson-line stage: the exponential products of a sheet batch run on
+    // stream_v while the next batch's Poisson transforms run on stream, into
+    // the other of two work buffers (work, work2)
+    cudaStream_t stream_v = nullptr;
+    cudaEvent_t ev_fft[2] = {nullptr, nullptr}, ev_prod[2] = {nullptr, nullptr};
     std::string err;
     long long launches = 0;
 
@@ -47,7 +52,7 @@ struct ipg_ctx {
     double2 *twiddle = nullptr;
     double *green = nullptr;
     double *amp = nullptr;
-    double2 *work = nullptr;
+    double2 *work = nullptr, *work2 = nullptr;
     double *nuc_xyz = nullptr, *nuc_gx = nullptr, *nuc_gy = nullptr;  // ipg_set_nuclei
     int nuc_cap = 0;
     int work_sheets = 0;
@@ -523,6 +528,11 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
 
     IPG_CUDA(c, cudaSetDevice(cfg->device));
     IPG_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    IPG_CUDA(c, cudaStreamCreateWithFlags(&c->stream_v, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; i++) {
+        IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_fft[i], cudaEventDisableTiming));
+        IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_prod[i], cudaEventDisableTiming));
+    }
     IPG_CUDA(c, cudaEventCreate(&c->ev0));
     IPG_CUDA(c, cudaEventCreate(&c->ev1));
     for (cudaEvent_t &x : c->ie) IPG_CUDA(c, cudaEventCreate(&x));
@@ -538,6 +548,7 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
     c->work_sheets = (int)std::max<size_t>(1, (64ull << 20) / per_sheet);
     c->work_sheets = std::min(c->work_sheets, cfg->Ny);
     IPG_TRY(dalloc(c, &c->work, (size_t)c->work_sheets * 4 * n));
+    IPG_TRY(dalloc(c, &c->work2, (size_t)c->work_sheets * 4 * n));
     IPG_TRY(dalloc(c, &c->VA, 9 * n));
     IPG_TRY(dalloc(c, &c->VB, 9 * n));
     IPG_TRY(dalloc(c, &c->u1x, 9 * n));
@@ -599,6 +610,14 @@ ipg_status ipg_destroy(ipg_ctx *ctx) {
         if (x) cudaEventDestroy(x);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream_v) {
+        cudaStreamSynchronize(ctx->stream_v);
+        cudaStreamDestroy(ctx->stream_v);
+    }
+    for (int i = 0; i < 2; i++) {
+        if (ctx->ev_fft[i]) cudaEventDestroy(ctx->ev_fft[i]);
+        if (ctx->ev_prod[i]) cudaEventDestroy(ctx->ev_prod[i]);
+    }
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return IPG_OK;
@@ -738,6 +757,7 @@ static ipg_status init_enqueue(ipg_ctx *c, bool from_wilson) {
     IPG_CUDA(c, cudaMemsetAsync(c->scal + 38, 0, sizeof(double), c->stream));
 
     // Wilson lines, nucleus A then B (Init.cpp:1688-1847)
+    int batch = 0;
     for (int nuc = 0; nuc < (from_wilson ? 0 : 2); nuc++) {
         C<double> *V = nuc ? c->VB : c->VA;
         k_identity<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(n, V);
@@ -758,11 +778,25 @@ static ipg_status init_enqueue(ipg_ctx *c, bool from_wilson) {
         w.V = V;
         launch_wilson_amp(w, c->stream);
         IPG_LAUNCHED(c, 1);
-        for (int k0 = 0; k0 < c->cfg.Ny; k0 += c->work_sheets) {
+        for (int k0 = 0; k0 < c->cfg.Ny; k0 += c->work_sheets, batch++) {
             const int ns = std::min(c->work_sheets, c->cfg.Ny - k0);
+            const int i = batch & 1;
+            w.work = i ? c->work2 : c->work;
+            // the buffer is free once the product of two batches ago has read it
+            if (batch >= 2) IPG_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_prod[i], 0));
+            w.no_product = 1;
             launch_wilson_sheets(w, k0, ns, c->stream);
+            IPG_CUDA(c, cudaEventRecord(c->ev_fft[i], c->stream));
+            IPG_CUDA(c, cudaStreamWaitEvent(c->stream_v, c->ev_fft[i], 0));
+            w.no_product = 0;
+            launch_wilson_product(w, ns, c->stream_v);
+            IPG_CUDA(c, cudaEventRecord(c->ev_prod[i], c->stream_v));
             IPG_LAUNCHED(c, 4);
         }
+    }
+    if (batch > 0) {
+        // V_A, V_B complete before anything else on the context stream
+        IPG_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_prod[(batch - 1) & 1], 0));
     }
     IPG_CUDA(c, cudaEventRecord(e[1], c->stream));
 

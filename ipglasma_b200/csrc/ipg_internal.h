@@ -102,6 +102,8 @@ struct WilsonArgs {
 void launch_poisson_sheets(const WilsonArgs &w, int ns, cudaStream_t st);
 void launch_wilson_sheets(const WilsonArgs &w, int k0, int ns,
                           cudaStream_t st);
+// k_wilson alone: V <- exp(-i A_k.t) V for the ns sheets whose A is in w.work
+void launch_wilson_product(const WilsonArgs &w, int ns, cudaStream_t st);
 // charge amplitude of every site, once per nucleus before its sheets
 void launch_wilson_amp(const WilsonArgs &w, cudaStream_t st);
 

@@ -278,6 +278,12 @@ static void launch_sheets(const WilsonArgs &w, int k0, int ns, cudaStream_t st) 
     if (!w.rho_in && !w.no_product) k_wilson<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
 }
 
+// the Wilson-line product of a batch whose A is already in w.work
+void launch_wilson_product(const WilsonArgs &w, int ns, cudaStream_t st) {
+    const size_t n = (size_t)w.N * w.N;
+    k_wilson<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
+}
+
 void launch_poisson_sheets(const WilsonArgs &w, int ns, cudaStream_t st) {
     // launch_sheets skips the Wilson-line product when rho_in is set
     launch_wilson_sheets(w, 0, ns, st);
