@@ -751,11 +751,12 @@ struct PairLoadGlobal {
 // through `ld` (global planes or a shared-memory tile), writes the new E and
 // pi through it (site-local, so they may go back in place at once) and
 // returns the new links (nu) and phi (phin) when cf.do_pu is set, for the
-// caller to store once no other thread reads the old ones.
+// caller to store once no other thread reads the old ones. The site's own
+// link pair is loaded again at each use instead of being held (the tile
+// kernel then fits in 252 registers without spilling).
 template <class Ld>
 __device__ __forceinline__ void leapfrog_pair_core(const Ld &ld, const StepCoef<float> &cf,
                                                    M3<P2> &nu, H3<float> &phin) {
-    const M3<P2> Ud = ld.template links<kLx, 0, 0, kLy, 0, 0>();
     const H3<float> phi = ld.template phi<0, 0>();
     H3<float> pi = ld.pi();
     H3<P2> Ed = pair_h(ld.e1(), ld.e2());
@@ -767,12 +768,12 @@ __device__ __forceinline__ void leapfrog_pair_core(const Ld &ld, const StepCoef<
             // P_do = (U_d U_o(+d)) (U_o U_d(+o))^dag: lane x of a = U_d U_o(+d)
             // is Ux Uy(+x), lane y is Uy Ux(+y); U_o U_d(+o) is the same pair
             // of products with the lanes swapped
-            const M3<P2> a = dmul(Ud, ld.template links<kLy, 1, 0, kLx, 0, 1>());
+            const M3<P2> a = dmul(ld.template links<kLx, 0, 0, kLy, 0, 0>(), ld.template links<kLy, 1, 0, kLx, 0, 1>());
             stap = i_antiherm(dmul_nd(a, swap_lanes(a)));
         }
         {
             // S_d = (U_d U_o(+d-o)^dag) (U_d(-o)^dag U_o(-o))
-            const M3<P2> p = dmul_nd(Ud, ld.template links<kLy, 1, -1, kLx, -1, 1>());
+            const M3<P2> p = dmul_nd(ld.template links<kLx, 0, 0, kLy, 0, 0>(), ld.template links<kLy, 1, -1, kLx, -1, 1>());
             const M3<P2> q = dmul_dn(ld.template links<kLx, 0, -1, kLy, -1, 0>(),
                                      ld.template links<kLy, 0, -1, kLx, -1, 0>());
             h_add(stap, i_antiherm(dmul(p, q)));
@@ -782,7 +783,7 @@ __device__ __forceinline__ void leapfrog_pair_core(const Ld &ld, const StepCoef<
         const P2 cdt = P2(cf.c_pi);
         h_axpy(Ed, cst, stap);
         const H3<P2> fp = pair_h(ld.template phi<1, 0>(), ld.template phi<0, 1>());
-        H3<P2> br = transport_fwd_minus<P2, true>(Ud, fp, phi2);
+        H3<P2> br = transport_fwd_minus<P2, true>(ld.template links<kLx, 0, 0, kLy, 0, 0>(), fp, phi2);
         h_axpy(Ed, cdt, i_commutator(br, phi2));  // i[phi~ - phi, phi] = i[phi~, phi]
         const H3<P2> fm = pair_h(ld.template phi<-1, 0>(), ld.template phi<0, -1>());
         h_add(br, transport_bwd_minus<P2, true>(ld.template links<kLx, -1, 0, kLy, 0, -1>(), fm,
@@ -795,7 +796,7 @@ __device__ __forceinline__ void leapfrog_pair_core(const Ld &ld, const StepCoef<
         ld.put_pi(pi);
     }
     if (cf.do_pu) {
-        nu = taylor2_update_dev(Ed, P2(cf.c_u), Ud);
+        nu = taylor2_update_dev(Ed, P2(cf.c_u), ld.template links<kLx, 0, 0, kLy, 0, 0>());
         reunitarize_dev(nu);
         phin = phi;
         h_axpy(phin, cf.c_phi, pi);
