@@ -726,11 +726,18 @@ struct PairLoadGlobal {
         oy[0] = iy > 0 ? -1 : 0;
         oy[1] = 0;
         oy[2] = iy + 1 < N ? 1 : 0;
+        own = ld_m3_pair(s.ux, pos, s.uy, pos, n);
     }
+    // the site's own pair is loaded once and held (from global memory a
+    // reload costs more than the registers; the tile loader reloads it)
+    M3<P2> own;
     template <int FA, int DXA, int DYA, int FB, int DXB, int DYB>
     __device__ __forceinline__ M3<P2> links() const {
-        return ld_m3_pair(FA == kLy ? s.uy : s.ux, pos + ox[DXA + 1] + oy[DYA + 1],
-                          FB == kLy ? s.uy : s.ux, pos + ox[DXB + 1] + oy[DYB + 1], n);
+        if constexpr (FA == kLx && DXA == 0 && DYA == 0 && FB == kLy && DXB == 0 && DYB == 0)
+            return own;
+        else
+            return ld_m3_pair(FA == kLy ? s.uy : s.ux, pos + ox[DXA + 1] + oy[DYA + 1],
+                              FB == kLy ? s.uy : s.ux, pos + ox[DXB + 1] + oy[DYB + 1], n);
     }
     template <int DX, int DY>
     __device__ __forceinline__ H3<float> phi() const {
