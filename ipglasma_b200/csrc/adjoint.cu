@@ -485,6 +485,144 @@ __device__ __forceinline__ Md dexp(double q[8], int b, double h) {
 
 constexpr double kDexpStep = 1e-5;  // truncation ~1e-10, rounding ~1e-11
 
+// Q = q.t with t^a = lambda_a / 2 (the matrix exp_from_coeff exponentiates)
+__device__ __forceinline__ Md q_matrix(const double q[8]) {
+    const double c8 = IPG_C8, s3 = IPG_INV_SQRT3;
+    Md Q;
+    Q.m[0] = {0.5 * q[2] + c8 * q[7], 0.};
+    Q.m[4] = {-0.5 * q[2] + c8 * q[7], 0.};
+    Q.m[8] = {-s3 * q[7], 0.};
+    Q.m[1] = {0.5 * q[0], -0.5 * q[1]};
+    Q.m[3] = {0.5 * q[0], 0.5 * q[1]};
+    Q.m[2] = {0.5 * q[3], -0.5 * q[4]};
+    Q.m[6] = {0.5 * q[3], 0.5 * q[4]};
+    Q.m[5] = {0.5 * q[5], -0.5 * q[6]};
+    Q.m[7] = {0.5 * q[5], 0.5 * q[6]};
+    return Q;
+}
+
+// tr(a^dag b)
+__device__ __forceinline__ C<double> dot_c(const Md &a, const Md &b) {
+    C<double> s = {0., 0.};
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        s.r += a.m[k].r * b.m[k].r + a.m[k].i * b.m[k].i;
+        s.i += a.m[k].r * b.m[k].i - a.m[k].i * b.m[k].r;
+    }
+    return s;
+}
+
+__device__ __forceinline__ Md cscale(const Md &a, C<double> s) {
+    Md r;
+#pragma unroll
+    for (int k = 0; k < 9; k++) r.m[k] = cmul(a.m[k], s);
+    return r;
+}
+
+__device__ __forceinline__ C<double> cadd(C<double> a, C<double> b) { return {a.r + b.r, a.i + b.i}; }
+__device__ __forceinline__ C<double> csub(C<double> a, C<double> b) { return {a.r - b.r, a.i - b.i}; }
+__device__ __forceinline__ C<double> crs(C<double> a, double s) { return {a.r * s, a.i * s}; }
+__device__ __forceinline__ C<double> cis(C<double> a, double s) { return {-a.i * s, a.r * s}; }  // i s a
+
+// qb_b = Re tr(eb^dag dE/dq_b), b = 0..7, for E = exp(i q.t): the
+// vector-Jacobian product of the exponential without differencing.
+// With Q = q.t, c0 = det Q, c1 = tr(Q^2)/2 and E = f0 + f1 Q + f2 Q^2
+// (Cayley-Hamilton, the f_j of expm_coeff as functions of u and w):
+//   qb_b = Re(P0) tr(Q^2 t^b) + Re(P1) q_b / 2 + Re tr((f1 eb^dag + f2 (Q eb^dag + eb^dag Q)) t^b)
+// where P_i = sum_j (df_j/dc_i) tr(eb^dag Q^j), since dc0/dq_b = tr(Q^2 t^b)
+// (the adjugate of a traceless Q is Q^2 - c1) and dc1/dq_b = q_b / 2. The
+// df_j/dc_i follow from f_j = h_j(u, w) / (9u^2 - w^2) and the derivatives
+// of u, w by c0, c1 (c0 = 2u^3 - 2u w^2, c1 = 3u^2 + w^2 differentiated
+// implicitly: du/dc0 = 1/(2D), du/dc1 = u/D, dw/dc0 = -3u/(2wD), dw/dc1 = (3u^2-w^2)/(2wD)
+// with D = 9u^2 - w^2). For c1 < 1e-7 the Taylor series to third order is
+// used (error below 1e-11). Returns false where two eigenvalues of Q nearly
+// coincide (w or D small against c1) or where exp_from_coeff returns the
+// identity; the caller then differences instead.
+__device__ bool exp_vjp(const double q[8], const Md &eb, double qb[8]) {
+    const Md Q = q_matrix(q);
+    const Md Q2 = mul(Q, Q);
+    const Md ebd = dagger(eb);
+    const Md Qe = mul(Q, ebd), eQ = mul(ebd, Q);
+    double c1 = 0.;
+#pragma unroll
+    for (int a = 0; a < 8; a++) c1 += q[a] * q[a];
+    c1 *= 0.25;
+    Md M;
+    double s1 = 0.;
+    if (c1 < 1e-7) {
+        // d/dq_b of 1 + iQ - Q^2/2 - iQ^3/6:
+        // M = i eb^dag - (Q eb^dag + eb^dag Q)/2 - i (Q^2 eb^dag + Q eb^dag Q + eb^dag Q^2)/6
+        M = times_i(ebd, 1.);
+        sub_from(M, sc(addm(Qe, eQ), 0.5));
+        Md t3 = mul(Q, Qe);
+        add_to(t3, mul(Qe, Q));
+        add_to(t3, mul(ebd, Q2));
+        sub_from(M, times_i(t3, 1. / 6.));
+    } else {
+        const double c0 = re_trace_mul(Q2, Q) / 3.;  // det Q = tr(Q^3)/3
+        const double t3 = c1 / 3., st3 = sqrt(t3);
+        const double c0max = fmax(1e-15, 2. * (t3 * st3));
+        const double theta3 = acos(c0 / c0max) / 3.;
+        double sth, cth;
+        sincos(theta3, &sth, &cth);
+        const double u = st3 * cth, w = sqrt(c1) * sth;
+        const double D = 9. * u * u - w * w;
+        if (!(w >= 1e-3 * sqrt(c1)) || !(fabs(D) >= 1e-3 * c1)) return false;
+        double su, cu, sw, cw;
+        sincos(u, &su, &cu);
+        sincos(w, &sw, &cw);
+        const C<double> E2 = {(cu - su) * (cu + su), 2. * su * cu};  // e^{2iu}
+        const C<double> Em = {cu, -su};                              // e^{-iu}
+        const double xi0 = sw / w, xi0p = (cw - xi0) / w;            // sin w / w, its w-derivative
+        const double uu = u * u, ww = w * w;
+        const C<double> B0 = {8. * uu * cw, 2. * u * (3. * uu + ww) * xi0};
+        const C<double> B1 = {2. * u * cw, -(3. * uu - ww) * xi0};
+        const C<double> B2 = {cw, 3. * u * xi0};
+        const C<double> EB0 = cmul(Em, B0), EB1 = cmul(Em, B1), EB2 = cmul(Em, B2);
+        C<double> h[3], hu[3], hw[3];
+        h[0] = cadd(crs(E2, uu - ww), EB0);
+        h[1] = csub(crs(E2, 2. * u), EB1);
+        h[2] = csub(E2, EB2);
+        hu[0] = cadd(cadd(crs(E2, 2. * u), cis(E2, 2. * (uu - ww))),
+                     csub(cmul(Em, {16. * u * cw, 2. * (9. * uu + ww) * xi0}), cis(EB0, 1.)));
+        hu[1] = cadd(cadd(crs(E2, 2.), cis(E2, 4. * u)),
+                     csub(cis(EB1, 1.), cmul(Em, {2. * cw, -6. * u * xi0})));
+        hu[2] = cadd(cis(E2, 2.), csub(cis(EB2, 1.), cmul(Em, {0., 3. * xi0})));
+        hw[0] = cadd(crs(E2, -2. * w),
+                     cmul(Em, {-8. * uu * sw, 2. * u * (2. * w * xi0 + (3. * uu + ww) * xi0p)}));
+        hw[1] = cmul(Em, {2. * u * sw, -2. * w * xi0 + (3. * uu - ww) * xi0p});
+        hw[2] = cmul(Em, {sw, -3. * u * xi0p});
+        const double rD = 1. / D;
+        const double du0 = 0.5 * rD, du1 = u * rD;
+        const double dw0 = -1.5 * u * rD / w, dw1 = 0.5 * (3. * uu - ww) * rD / w;
+        const C<double> tau[3] = {{trace(eb).r, -trace(eb).i}, dot_c(eb, Q), dot_c(eb, Q2)};
+        C<double> f[3], P0 = {0., 0.}, P1 = {0., 0.};
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            f[j] = crs(h[j], rD);
+            const C<double> fu = crs(csub(hu[j], crs(f[j], 18. * u)), rD);
+            const C<double> fw = crs(cadd(hw[j], crs(f[j], 2. * w)), rD);
+            P0 = cadd(P0, cmul(cadd(crs(fu, du0), crs(fw, dw0)), tau[j]));
+            P1 = cadd(P1, cmul(cadd(crs(fu, du1), crs(fw, dw1)), tau[j]));
+        }
+        // exp_from_coeff returns the identity when |Re u0| < 1e-15
+        if (!(fabs(f[0].r + 2. / 3. * c1 * f[2].r) >= 1e-15)) return false;
+        M = sc(Q2, P0.r);
+        add_to(M, cscale(ebd, f[1]));
+        add_to(M, cscale(addm(Qe, eQ), f[2]));
+        s1 = 0.5 * P1.r;
+    }
+    C<double> tr[8];
+    trace_ta(M, tr);
+    bool ok = true;
+#pragma unroll
+    for (int b = 0; b < 8; b++) {
+        qb[b] = tr[b].r + s1 * q[b];
+        ok = ok && isfinite(qb[b]);
+    }
+    return ok;
+}
+
 }  // namespace
 
 // pi(tau=0) = -i t / (4 g), t the "minus" stencil (init.cu k_initial_pi):
@@ -625,7 +763,8 @@ __global__ void __launch_bounds__(128) k_adj_wilson_sheet(int N, double2 *work, 
     st_m3(V, pos, n, Vprev);
     st_m3(Vb, pos, n, mul_dn(e, Vbk));
     double qb[8];
-    for (int b = 0; b < 8; b++) qb[b] = re_dot(eb, dexp(q, b, kDexpStep));
+    if (!exp_vjp(q, eb, qb))
+        for (int b = 0; b < 8; b++) qb[b] = re_dot(eb, dexp(q, b, kDexpStep));
     for (int c = 0; c < 4; c++) work[(size_t)c * n + pos] = make_double2(-qb[2 * c], -qb[2 * c + 1]);
 }
 
