@@ -351,9 +351,12 @@ class Event:
         return ms.value, k.value
 
     # -- adjoint -------------------------------------------------------------
-    def forward(self, checkpoint_every: int = 20):
+    def forward(self, checkpoint_every: int = 0):
         """E_T and the T^tautau-weighted eps2 from the fresh tau = 0 state;
-        saves checkpoints for :meth:`backward`."""
+        saves checkpoints for :meth:`backward`: every state with
+        checkpoint_every = 1 (no time reversal in the backward), every k-th
+        with k > 1, and 0 picks 1 when the states fit in half of the free
+        device memory, else ~sqrt(steps)."""
         et, e2 = ct.c_double(), ct.c_double()
         self._check(self._lib.ipg_forward(self._h, checkpoint_every, ct.byref(et), ct.byref(e2)))
         return et.value, e2.value

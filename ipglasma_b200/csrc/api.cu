@@ -1120,12 +1120,28 @@ ipg_status ipg_forward(ipg_ctx *c, int checkpoint_every, double *E_T, double *ep
     if (!c) return IPG_ERR_BAD_CONFIG;
     if (!c->initialized || c->half_done || c->finished)
         return fail(c, IPG_ERR_STATE, "ipg_forward needs the fresh tau = 0 state");
-    if (checkpoint_every < 1) return fail(c, IPG_ERR_BAD_CONFIG, "checkpoint_every < 1");
+    if (checkpoint_every < 0) return fail(c, IPG_ERR_BAD_CONFIG, "checkpoint_every < 0");
     const size_t n = c->n;
     const int N = c->N;
     const int S = c->itmax;
     auto &A = c->aw;
-    const int ncp = (S - 1) / checkpoint_every + 1;
+    if (checkpoint_every == 0) {
+        // automatic: every state when the S + 1 states (70 doubles a site
+        // each) take at most half of the free device memory, else a
+        // checkpoint every ~sqrt(S) steps
+        size_t free_b = 0, total_b = 0;
+        IPG_CUDA(c, cudaMemGetInfo(&free_b, &total_b));
+        const size_t have = A.cp.size() * 70 * n * sizeof(double);  // reused
+        const size_t need = (size_t)(S + 1) * 70 * n * sizeof(double);
+        checkpoint_every = need <= (free_b + have) / 2
+                               ? 1
+                               : std::max(2, (int)std::ceil(std::sqrt((double)S)));
+    }
+    // checkpoint_every = 1 keeps every step's state (S + 1 states): the
+    // forward steps from slot s into slot s + 1 and the reverse sweep reads
+    // them without time reversal
+    const bool store_all = checkpoint_every == 1;
+    const int ncp = store_all ? S + 1 : (S - 1) / checkpoint_every + 1;
     auto alloc_state = [&](State<double> &st) -> ipg_status {
         IPG_TRY(dalloc(c, &st.ux, 9 * n));
         IPG_TRY(dalloc(c, &st.uy, 9 * n));
@@ -1157,18 +1173,30 @@ ipg_status ipg_forward(ipg_ctx *c, int checkpoint_every, double *E_T, double *ep
 
     // forward in FP64 from the tau = 0 state (the context's own state is kept)
     IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-    IPG_TRY(copy_state(c, A.w[0], c->s64));
-    State<double> cur = A.w[0];
-    C<double> *ux_b = A.w[1].ux, *uy_b = A.w[1].uy;
-    double *phi_b = A.w[1].phi;
-    for (int s = 0; s < S; s++) {
-        if (s % checkpoint_every == 0) IPG_TRY(copy_state(c, A.cp[s / checkpoint_every], cur));
-        const StepCoef<double> cf = evolution_coef(c, s);
-        launch_leapfrog<double>(c->d_ev, N, cur, ux_b, uy_b, phi_b, cf, false, c->stream);
-        IPG_LAUNCHED(c, 1);
-        std::swap(cur.ux, ux_b);
-        std::swap(cur.uy, uy_b);
-        std::swap(cur.phi, phi_b);
+    State<double> cur;
+    if (store_all) {
+        IPG_TRY(copy_state(c, A.cp[0], c->s64));
+        for (int s = 0; s < S; s++) {
+            launch_leapfrog_into(c->d_ev, N, A.cp[s], A.cp[s + 1], evolution_coef(c, s),
+                                 c->stream);
+            IPG_LAUNCHED(c, 1);
+        }
+        cur = A.cp[S];
+    } else {
+        IPG_TRY(copy_state(c, A.w[0], c->s64));
+        cur = A.w[0];
+        C<double> *ux_b = A.w[1].ux, *uy_b = A.w[1].uy;
+        double *phi_b = A.w[1].phi;
+        for (int s = 0; s < S; s++) {
+            if (s % checkpoint_every == 0)
+                IPG_TRY(copy_state(c, A.cp[s / checkpoint_every], cur));
+            const StepCoef<double> cf = evolution_coef(c, s);
+            launch_leapfrog<double>(c->d_ev, N, cur, ux_b, uy_b, phi_b, cf, false, c->stream);
+            IPG_LAUNCHED(c, 1);
+            std::swap(cur.ux, ux_b);
+            std::swap(cur.uy, uy_b);
+            std::swap(cur.phi, phi_b);
+        }
     }
     A.fin = cur;
     TmunuArgs ta;
@@ -1249,26 +1277,35 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
         IPG_CUDA(c, cudaMemsetAsync(b, 0, 9 * n * sizeof(C<double>), c->stream));
     launch_adjoint_ttt(N, A.fin, A.tbar, A.adj, c->cfg.g, S * c->dtau, c->stream);
     IPG_LAUNCHED(c, 1);
-    // reverse sweep: state s from state s+1 by time reversal, or from the
-    // checkpoint when s is a multiple of k; two state sets alternate
-    State<double> sets[2] = {A.w[2], A.fin};
-    State<double> nxt = A.fin;
-    for (int s = S - 1, q = 0; s >= 0; s--, q++) {
-        const State<double> cur = sets[q & 1];
-        const StepCoef<double> cf = evolution_coef(c, s);
-        if (s % A.k == 0) {
-            IPG_TRY(copy_state(c, cur, A.cp[s / A.k]));
-            launch_adjoint_step(N, cur, nxt, A.adj, cf, c->stream);
+    if (A.k == 1) {
+        // every state stored: no time reversal, nothing overwritten
+        for (int s = S - 1; s >= 0; s--) {
+            const StepCoef<double> cf = evolution_coef(c, s);
+            launch_adjoint_step(N, A.cp[s], A.cp[s + 1], A.adj, cf, c->stream);
             IPG_LAUNCHED(c, cf.do_pe ? 3 : 1);
-        } else {
-            launch_inverse_adjoint_step(N, nxt, cur, A.adj, cf, c->stream);
-            IPG_LAUNCHED(c, cf.do_pe ? 4 : 2);
         }
-        nxt = cur;
+    } else {
+        // reverse sweep: state s from state s+1 by time reversal, or from the
+        // checkpoint when s is a multiple of k; two state sets alternate
+        State<double> sets[2] = {A.w[2], A.fin};
+        State<double> nxt = A.fin;
+        for (int s = S - 1, q = 0; s >= 0; s--, q++) {
+            const State<double> cur = sets[q & 1];
+            const StepCoef<double> cf = evolution_coef(c, s);
+            if (s % A.k == 0) {
+                IPG_TRY(copy_state(c, cur, A.cp[s / A.k]));
+                launch_adjoint_step(N, cur, nxt, A.adj, cf, c->stream);
+                IPG_LAUNCHED(c, cf.do_pe ? 3 : 1);
+            } else {
+                launch_inverse_adjoint_step(N, nxt, cur, A.adj, cf, c->stream);
+                IPG_LAUNCHED(c, cf.do_pe ? 4 : 2);
+            }
+            nxt = cur;
+        }
+        A.ready = false;  // the reverse sweep overwrote the final state
     }
     launch_adjoint_project(n, A.adj, c->stream);
     IPG_LAUNCHED(c, 1);
-    A.ready = false;  // the reverse sweep overwrote the final state
     if (grad_g2mu || grad_rho) IPG_TRY(backward_inputs(c, grad_g2mu, grad_rho));
     IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     IPG_TRY(sync(c));

@@ -1524,6 +1524,48 @@ void launch_leapfrog(const EventGeom *d_ev, int N, const State<T> &s,
     launch_leapfrog_site(d_ev, N, s, ux_out, uy_out, phi_out, cf, reunit, st);
 }
 
+void launch_leapfrog_into(const EventGeom *d_ev, int N, const State<double> &in,
+                          const State<double> &out, const StepCoef<double> &cf, cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    // the step writes E and pi only when it updates them
+    const bool copy_e = !cf.do_pe || N < 32 || !use_tile64_kernel();
+    if (copy_e) {
+        cudaMemcpyAsync(out.e1, in.e1, 8 * n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(out.e2, in.e2, 8 * n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(out.pi, in.pi, 9 * n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    }
+    // links and phi from `in`; E and pi read from `in` (TMA) or, after the
+    // copy, updated in place in `out`
+    State<double> s = in;
+    s.e1 = out.e1;
+    s.e2 = out.e2;
+    s.pi = out.pi;
+    if (!copy_e) {
+        using namespace tile64;
+        const uint64_t nn = (uint64_t)N;
+        const auto U64 = CU_TENSOR_MAP_DATA_TYPE_UINT64;
+        LoadMaps m;
+        const bool ok =
+            encode_tiled_3d(&m.ux, in.ux, U64, 8, 2 * nn, nn, 9, 2 * UC, UR, 9) &&
+            encode_tiled_3d(&m.uy, in.uy, U64, 8, 2 * nn, nn, 9, 2 * UC, UR, 9) &&
+            encode_tiled_3d(&m.phi, in.phi, U64, 8, nn, nn, 9, PC, PR, 9) &&
+            encode_tiled_3d(&m.e1, in.e1, U64, 8, nn, nn, 8, Cn, R, 8) &&
+            encode_tiled_3d(&m.e2, in.e2, U64, 8, nn, nn, 8, Cn, R, 8) &&
+            encode_tiled_3d(&m.pi, in.pi, U64, 8, nn, nn, 9, Cn, R, 9);
+        if (ok) {
+            cudaFuncSetAttribute(k_leapfrog_tile64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 SMEM);
+            k_leapfrog_tile64<<<(N / R) * (N / Cn), 128, SMEM, st>>>(m, N, cf, nullptr, s, out.ux,
+                                                                       out.uy, out.phi);
+            return;
+        }
+        cudaMemcpyAsync(out.e1, in.e1, 8 * n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(out.e2, in.e2, 8 * n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(out.pi, in.pi, 9 * n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    }
+    launch_leapfrog_site<double>(d_ev, N, s, out.ux, out.uy, out.phi, cf, false, st);
+}
+
 // one thread per site (lattices smaller than 32 sites per side)
 template <typename T>
 void launch_leapfrog_site(const EventGeom *d_ev, int N, const State<T> &s,

@@ -51,6 +51,11 @@ void launch_leapfrog(const EventGeom *d_ev, int N, const State<T> &s,
                      const StepCoef<T> &cf, bool reunit, cudaStream_t st,
                      double *status = nullptr);
 
+// One FP64 step from the state `in` into the separate state `out` (all six
+// fields written; `in` is left unchanged)
+void launch_leapfrog_into(const EventGeom *d_ev, int N, const State<double> &in,
+                          const State<double> &out, const StepCoef<double> &cf, cudaStream_t st);
+
 // One event of a batched leapfrog launch: its buffers for this step and its
 // step coefficients (inactive events are skipped).
 template <typename T>

@@ -1,7 +1,8 @@
 """Adjoint of the evolution (ipg_forward / ipg_backward): gradients of E_T and
 of the T^tautau-weighted eps2 with respect to the tau = 0 fields agree with
 central finite differences along random directions, and time reversal between
-checkpoints gives the same gradient as storing every step."""
+checkpoints gives the same gradient as storing every step (and stepping each
+state into its own slot)."""
 import numpy as np
 import pytest
 
@@ -100,6 +101,23 @@ def test_time_reversal_matches_stored_steps(setup):
         a, b = out[0][f], out[1][f]
         scale = max(np.abs(a).max(), 1e-300)
         assert np.abs(a - b).max() <= 1e-8 * scale, f
+
+
+def test_stored_states_allow_repeated_backward(setup):
+    """With every state kept (checkpoint_every = 1) the reverse sweep
+    overwrites nothing: a second backward with other weights needs no new
+    forward and equals the sum of the single-loss gradients."""
+    ev, state = setup
+    for f in FIELDS:
+        ev.set_field(f, state[f])
+    ev.mark_initialized()
+    ev.forward(1)
+    g_et = ev.backward(1.0, 0.0)
+    g_e2 = ev.backward(0.0, 1.0)
+    g_both = ev.backward(1.0, 1.0)
+    for f in FIELDS:
+        scale = max(np.abs(g_both[f]).max(), 1e-300)
+        assert np.abs(g_et[f] + g_e2[f] - g_both[f]).max() <= 1e-10 * scale, f
 
 
 # ---- through the initial conditions: g2mu and rho ---------------------------
