@@ -17,9 +17,8 @@
 //   S_u: phi' = phi + c2 pi',   U_d' = T2(i c E_d') U_d,  T2(X) = 1 + X + X^2/2
 // with cst = tau dtau / (2 g^2), cdt = dtau / tau, c = g^2 dtau / (tau + dtau/2),
 // c2 = (tau + dtau/2) dtau. Its vector-Jacobian product is k_adj_su (local)
-// followed by k_adj_se_links and k_adj_se_phi (they scatter into neighbouring
-// links and phi with FP64 atomics, so the summation order, not the result,
-// varies between runs).
+// followed by k_adj_se (it scatters into neighbouring links and phi with
+// FP64 atomics, so the summation order, not the result, varies between runs).
 // The step is inverted exactly in exact arithmetic (k_inv_su and k_inv_se,
 // the latter in evolve.cu on the forward step's code): this
 // is the time reversal used to walk back between checkpoints.
@@ -97,6 +96,21 @@ __device__ __forceinline__ void atomic_add_m(C<double> *buf, size_t pos, size_t 
         atomicAdd(&buf[k * n + pos].r, a.m[k].r);
         atomicAdd(&buf[k * n + pos].i, a.m[k].i);
     }
+}
+
+// the 9 real components of a Hermitian adjoint (diagonal real parts, upper
+// triangle); buffers updated this way are read back with ld_adj_h
+__device__ __forceinline__ void atomic_add_h(C<double> *buf, size_t pos, size_t n,
+                                             const Md &a) {
+    atomicAdd(&buf[0 * n + pos].r, a.m[0].r);
+    atomicAdd(&buf[4 * n + pos].r, a.m[4].r);
+    atomicAdd(&buf[8 * n + pos].r, a.m[8].r);
+    atomicAdd(&buf[1 * n + pos].r, a.m[1].r);
+    atomicAdd(&buf[1 * n + pos].i, a.m[1].i);
+    atomicAdd(&buf[2 * n + pos].r, a.m[2].r);
+    atomicAdd(&buf[2 * n + pos].i, a.m[2].i);
+    atomicAdd(&buf[5 * n + pos].r, a.m[5].r);
+    atomicAdd(&buf[5 * n + pos].i, a.m[5].i);
 }
 
 __device__ __forceinline__ Md ld_adj(const C<double> *buf, size_t pos, size_t n) {
@@ -208,7 +222,7 @@ __global__ void k_adj_su(int N, State<double> cur, State<double> nxt, AdjState a
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
-    const Md phib = herm(ld_adj(a.phi, pos, n));
+    const Md phib = from_h(ld_adj_h(a.phi, pos, n));
     Md pib = herm(ld_adj(a.pi, pos, n));
     add_to(pib, sc(phib, c2));
     st_m3(a.phi, pos, n, phib);
@@ -247,7 +261,7 @@ __global__ void k_inv_adj_su(int N, State<double> nxt, State<double> cur, AdjSta
         h_axpy(phi, -c2, ld_h(nxt.pi, pos, n));
         st_h(cur.phi, pos, n, phi);
     }
-    const Md phib = herm(ld_adj(a.phi, pos, n));
+    const Md phib = from_h(ld_adj_h(a.phi, pos, n));
     Md pib = herm(ld_adj(a.pi, pos, n));
     add_to(pib, sc(phib, c2));
     st_m3(a.phi, pos, n, phib);
@@ -270,93 +284,124 @@ __global__ void k_inv_adj_su(int N, State<double> nxt, State<double> cur, AdjSta
     }
 }
 
-// S_e, link part: the adjoints G_d of E_d' (traceless Hermitian, from
-// k_adj_su) through the plaquette and staple terms into the link adjoints
-// of the site and its neighbours (atomic)
-__global__ void __launch_bounds__(128) k_adj_se_links(int N, State<double> cur, AdjState a,
-                                                      double cst) {
+// S_e: the adjoints G_d of E_d' (traceless Hermitian, from k_adj_su) and of
+// pi' through the plaquette, the two staples, the commutator terms of E and
+// the pi bracket into the link and phi adjoints of the site and its
+// neighbours (FP64 atomics). Three thread roles (blockIdx.y) split the work
+// by target so that a thread sums every term landing on one link before its
+// atomic update, and phi adjoints take their 9 Hermitian components:
+// 225 atomics a site. With Mb_0 = -2i cst (G_1 - G_2), Mb_1 = -2i cst G_1,
+// Mb_2 = -2i cst G_2, Cb_d = cdt G_d and brb = cdt pi_bar:
+//   plaquette Ux Uy(+x) (Uy Ux(+y))^dag:   A = Ux Uy(+x), B = Uy Ux(+y),
+//       Ab = Mb_0 B, Bb = Mb_0^dag A
+//   E1 staple Ux Uy(+x-y)^dag Ux(-y)^dag Uy(-y):  P = Ux Uy(+x-y)^dag,
+//       Q = Ux(-y)^dag Uy(-y), Pb = Mb_1 Q^dag, Qb = P^dag Mb_1
+//   E2 staple Uy Ux(-x+y)^dag Uy(-x)^dag Ux(-x):  P2, Q2, Pb2, Qb2 likewise
+//   transport: phb_d = i[phi, Cb_d] + brb, ph_d = U_d phi(+d) U_d^dag
+// role 0: Ux += Ab Uy(+x)^dag + Pb Uy(+x-y) + 2 phb_x Ux phi(+x);
+//         Uy(+x) += Ux^dag Ab; Uy(+x-y) += Pb^dag Ux; phi(+x) += Ux^dag phb_x Ux
+// role 1: Uy += Bb Ux(+y)^dag + Pb2 Ux(-x+y) + 2 phb_y Uy phi(+y);
+//         Ux(+y) += Uy^dag Bb; Ux(-x+y) += Pb2^dag Uy; phi(+y) += Uy^dag phb_y Uy;
+//         phi += -4 brb + i[Cb_1, ph_x] + i[Cb_2, ph_y]
+// role 2: Ux(-x) += Uy(-x) Qb2 + 2 phi(-x) Ux(-x) brb; Uy(-x) += Ux(-x) Qb2^dag;
+//         phi(-x) += Ux(-x) brb Ux(-x)^dag; and the same along y with Qb
+__global__ void __launch_bounds__(128) k_adj_se(int N, State<double> cur, AdjState a, double cst,
+                                                double cdt) {
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
     const StepGeom G = step_geom(N, (int)(pos / N), (int)(pos % N));
-    // one of the three terms per thread (blockIdx.y: the plaquette, the E1
-    // staple, the E2 staple), which keeps a thread's live matrices within the
-    // register file. The adjoints of E1', E2' are stored exactly Hermitian
-    // (k_adj_su writes their traceless Hermitian part), so their diagonal and
-    // upper triangle are loaded and the full matrix rebuilt where it is used.
-    const int part = blockIdx.y;
-    if (part == 0) {
-        // plaquette h12 = iAH(a b^dag), a = Ux Uy(+x), b = Uy Ux(+y); enters E1 (+), E2 (-)
-        const H3<double> h1 = ld_adj_h(a.e1, pos, n), h2 = ld_adj_h(a.e2, pos, n);
-        const Md ux = ld_m3(cur.ux, pos, n), uy = ld_m3(cur.uy, pos, n);
-        const Md uy_px = ld_m3(cur.uy, G.pX, n), ux_py = ld_m3(cur.ux, G.pY, n);
-        const Md A = mul(ux, uy_px), B = mul(uy, ux_py);
-        const Md Mb = times_i(minus(sc(from_h(h1), cst), sc(from_h(h2), cst)), -2.);
-        const Md Ab = mul(Mb, B), Bb = mul_dn(Mb, A);
-        atomic_add_m(a.ux, pos, n, mul_nd(Ab, uy_px));
-        atomic_add_m(a.uy, G.pX, n, mul_dn(ux, Ab));
-        atomic_add_m(a.uy, pos, n, mul_nd(Bb, ux_py));
-        atomic_add_m(a.ux, G.pY, n, mul_dn(uy, Bb));
-    } else if (part == 1) {
-        // staple of E1: p = Ux Uy(+x-y)^dag, q = Ux(-y)^dag Uy(-y)
+    const int role = blockIdx.y;
+    if (role == 0) {
         const H3<double> h1 = ld_adj_h(a.e1, pos, n);
         const Md ux = ld_m3(cur.ux, pos, n);
-        const Md uy_pxmy = ld_m3(cur.uy, G.pXmY, n);
-        const Md ux_my = ld_m3(cur.ux, G.mY, n), uy_my = ld_m3(cur.uy, G.mY, n);
-        const Md P = mul_nd(ux, uy_pxmy), Q = mul_dn(ux_my, uy_my);
-        const Md Mb = times_i(sc(from_h(h1), cst), -2.);
-        const Md Pb = mul_nd(Mb, Q), Qb = mul_dn(P, Mb);
-        atomic_add_m(a.ux, pos, n, mul(Pb, uy_pxmy));
-        atomic_add_m(a.uy, G.pXmY, n, mul_dn(Pb, ux));
-        atomic_add_m(a.ux, G.mY, n, mul_nd(uy_my, Qb));
-        atomic_add_m(a.uy, G.mY, n, mul(ux_my, Qb));
-    } else {
-        // staple of E2: p = Uy Ux(-x+y)^dag, q = Uy(-x)^dag Ux(-x)
+        Md acc;
+        {
+            const Md uy_px = ld_m3(cur.uy, G.pX, n);
+            const Md B = mul(ld_m3(cur.uy, pos, n), ld_m3(cur.ux, G.pY, n));
+            const Md Mb = times_i(minus(sc(from_h(h1), cst), sc(from_h(ld_adj_h(a.e2, pos, n)), cst)), -2.);
+            const Md Ab = mul(Mb, B);
+            acc = mul_nd(Ab, uy_px);
+            atomic_add_m(a.uy, G.pX, n, mul_dn(ux, Ab));
+        }
+        {
+            const Md uy_pxmy = ld_m3(cur.uy, G.pXmY, n);
+            const Md Q = mul_dn(ld_m3(cur.ux, G.mY, n), ld_m3(cur.uy, G.mY, n));
+            const Md Pb = mul_nd(times_i(sc(from_h(h1), cst), -2.), Q);
+            add_to(acc, mul(Pb, uy_pxmy));
+            atomic_add_m(a.uy, G.pXmY, n, mul_dn(Pb, ux));
+        }
+        {
+            Md phb = icomm(ld_herm(cur.phi, pos, n), sc(from_h(h1), cdt));
+            add_to(phb, sc(ld_adj(a.pi, pos, n), cdt));
+            add_to(acc, sc(mul(mul(phb, ux), ld_herm(cur.phi, G.pX, n)), 2.));
+            atomic_add_m(a.ux, pos, n, acc);
+            atomic_add_h(a.phi, G.pX, n, mul(mul_dn(ux, phb), ux));
+        }
+    } else if (role == 1) {
         const H3<double> h2 = ld_adj_h(a.e2, pos, n);
         const Md uy = ld_m3(cur.uy, pos, n);
-        const Md ux_mxpy = ld_m3(cur.ux, G.mXpY, n);
-        const Md uy_mx = ld_m3(cur.uy, G.mX, n), ux_mx = ld_m3(cur.ux, G.mX, n);
-        const Md P = mul_nd(uy, ux_mxpy), Q = mul_dn(uy_mx, ux_mx);
-        const Md Mb = times_i(sc(from_h(h2), cst), -2.);
-        const Md Pb = mul_nd(Mb, Q), Qb = mul_dn(P, Mb);
-        atomic_add_m(a.uy, pos, n, mul(Pb, ux_mxpy));
-        atomic_add_m(a.ux, G.mXpY, n, mul_dn(Pb, uy));
-        atomic_add_m(a.uy, G.mX, n, mul_nd(ux_mx, Qb));
-        atomic_add_m(a.ux, G.mX, n, mul(uy_mx, Qb));
+        Md acc;
+        {
+            const Md ux_py = ld_m3(cur.ux, G.pY, n);
+            const Md A = mul(ld_m3(cur.ux, pos, n), ld_m3(cur.uy, G.pX, n));
+            const Md Mb = times_i(minus(sc(from_h(ld_adj_h(a.e1, pos, n)), cst), sc(from_h(h2), cst)), -2.);
+            const Md Bb = mul_dn(Mb, A);
+            acc = mul_nd(Bb, ux_py);
+            atomic_add_m(a.ux, G.pY, n, mul_dn(uy, Bb));
+        }
+        {
+            const Md ux_mxpy = ld_m3(cur.ux, G.mXpY, n);
+            const Md Q = mul_dn(ld_m3(cur.uy, G.mX, n), ld_m3(cur.ux, G.mX, n));
+            const Md Pb = mul_nd(times_i(sc(from_h(h2), cst), -2.), Q);
+            add_to(acc, mul(Pb, ux_mxpy));
+            atomic_add_m(a.ux, G.mXpY, n, mul_dn(Pb, uy));
+        }
+        {
+            Md phb = icomm(ld_herm(cur.phi, pos, n), sc(from_h(h2), cdt));
+            add_to(phb, sc(ld_adj(a.pi, pos, n), cdt));
+            add_to(acc, sc(mul(mul(phb, uy), ld_herm(cur.phi, G.pY, n)), 2.));
+            atomic_add_m(a.uy, pos, n, acc);
+            atomic_add_h(a.phi, G.pY, n, mul(mul_dn(uy, phb), uy));
+        }
+        {
+            // phi += -4 brb + i[Cb_1, ph_x] + i[Cb_2, ph_y]
+            Md phib = icomm(sc(from_h(h2), cdt), mul_nd(mul(uy, ld_herm(cur.phi, G.pY, n)), uy));
+            const Md ux = ld_m3(cur.ux, pos, n);
+            add_to(phib, icomm(sc(from_h(ld_adj_h(a.e1, pos, n)), cdt),
+                               mul_nd(mul(ux, ld_herm(cur.phi, G.pX, n)), ux)));
+            add_to(phib, sc(ld_adj(a.pi, pos, n), -4. * cdt));
+            atomic_add_h(a.phi, pos, n, phib);
+        }
+    } else {
+        const Md brb = sc(ld_adj(a.pi, pos, n), cdt);
+        {
+            // E2 staple's Q side and the -x transport
+            const Md uy = ld_m3(cur.uy, pos, n), ux_mxpy = ld_m3(cur.ux, G.mXpY, n);
+            const Md P = mul_nd(uy, ux_mxpy);
+            const Md Qb = mul_dn(P, times_i(sc(from_h(ld_adj_h(a.e2, pos, n)), cst), -2.));
+            const Md ux_mx = ld_m3(cur.ux, G.mX, n), uy_mx = ld_m3(cur.uy, G.mX, n);
+            const Md f = ld_herm(cur.phi, G.mX, n);
+            atomic_add_m(a.uy, G.mX, n, mul_nd(ux_mx, Qb));
+            Md acc = mul(uy_mx, Qb);
+            add_to(acc, sc(mul(mul(f, ux_mx), brb), 2.));
+            atomic_add_m(a.ux, G.mX, n, acc);
+            atomic_add_h(a.phi, G.mX, n, mul_nd(mul(ux_mx, brb), ux_mx));
+        }
+        {
+            // E1 staple's Q side and the -y transport
+            const Md ux = ld_m3(cur.ux, pos, n), uy_pxmy = ld_m3(cur.uy, G.pXmY, n);
+            const Md P = mul_nd(ux, uy_pxmy);
+            const Md Qb = mul_dn(P, times_i(sc(from_h(ld_adj_h(a.e1, pos, n)), cst), -2.));
+            const Md ux_my = ld_m3(cur.ux, G.mY, n), uy_my = ld_m3(cur.uy, G.mY, n);
+            const Md f = ld_herm(cur.phi, G.mY, n);
+            atomic_add_m(a.ux, G.mY, n, mul_nd(uy_my, Qb));
+            Md acc = mul(ux_my, Qb);
+            add_to(acc, sc(mul(mul(f, uy_my), brb), 2.));
+            atomic_add_m(a.uy, G.mY, n, acc);
+            atomic_add_h(a.phi, G.mY, n, mul_nd(mul(uy_my, brb), uy_my));
+        }
     }
-}
-
-// S_e, transport part: the commutator terms of E and the pi bracket into the
-// phi and link adjoints (atomic)
-__global__ void __launch_bounds__(128) k_adj_se_phi(int N, State<double> cur, AdjState a,
-                                                    double cdt) {
-    const size_t n = (size_t)N * N;
-    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (pos >= n) return;
-    const StepGeom G = step_geom(N, (int)(pos / N), (int)(pos % N));
-    const Md phi = ld_herm(cur.phi, pos, n);
-    const Md brb = sc(ld_adj(a.pi, pos, n), cdt);
-    Md phib = sc(brb, -4.);
-    for (int d = 0; d < 2; d++) {
-        const size_t q = d ? G.pY : G.pX;
-        const Md u = ld_m3(d ? cur.uy : cur.ux, pos, n);
-        const Md f = ld_herm(cur.phi, q, n);
-        const Md ph = mul_nd(mul(u, f), u);
-        const Md Cb = sc(ld_adj(d ? a.e2 : a.e1, pos, n), cdt);
-        Md phb = icomm(phi, Cb);
-        add_to(phib, icomm(Cb, ph));
-        add_to(phb, brb);
-        atomic_add_m(d ? a.uy : a.ux, pos, n, sc(mul(mul(phb, u), f), 2.));
-        atomic_add_m(a.phi, q, n, mul(mul_dn(u, phb), u));
-    }
-    for (int d = 0; d < 2; d++) {
-        // U(-d)^dag phi(-d) U(-d): U_bar += 2 phi U C_bar, phi_bar += U C_bar U^dag
-        const size_t q = d ? G.mY : G.mX;
-        const Md u = ld_m3(d ? cur.uy : cur.ux, q, n), f = ld_herm(cur.phi, q, n);
-        atomic_add_m(d ? a.uy : a.ux, q, n, sc(mul(mul(f, u), brb), 2.));
-        atomic_add_m(a.phi, q, n, mul_nd(mul(u, brb), u));
-    }
-    atomic_add_m(a.phi, pos, n, phib);
 }
 
 // adjoint of T^tautau (k_tmunu_diag, Evolution.cpp:759-900) in lattice units,
@@ -424,7 +469,7 @@ __global__ void k_adj_project(size_t n, AdjState a) {
     if (pos >= n) return;
     st_m3(a.e1, pos, n, tl(herm(ld_adj(a.e1, pos, n))));
     st_m3(a.e2, pos, n, tl(herm(ld_adj(a.e2, pos, n))));
-    st_m3(a.phi, pos, n, herm(ld_adj(a.phi, pos, n)));
+    st_m3(a.phi, pos, n, from_h(ld_adj_h(a.phi, pos, n)));
     st_m3(a.pi, pos, n, herm(ld_adj(a.pi, pos, n)));
 }
 
@@ -826,8 +871,7 @@ void launch_inverse_adjoint_step(int N, const State<double> &nxt, const State<do
     k_inv_adj_su<<<blocks(n), 128, 0, st>>>(N, nxt, cur, a, c, c2);
     launch_inverse_se(N, nxt, cur, cf, st);
     if (cf.do_pe) {
-        k_adj_se_links<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, cst);
-        k_adj_se_phi<<<blocks(n), 128, 0, st>>>(N, cur, a, cdt);
+        k_adj_se<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, cst, cdt);
     }
 }
 
@@ -840,8 +884,7 @@ void launch_adjoint_step(int N, const State<double> &cur, const State<double> &n
     if (cf.do_pe) {
         const double cst = cf.tau * cf.dt_pe / (2. * cf.g * cf.g);
         const double cdt = cf.dt_pe / cf.tau;
-        k_adj_se_links<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, cst);
-        k_adj_se_phi<<<blocks(n), 128, 0, st>>>(N, cur, a, cdt);
+        k_adj_se<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, cst, cdt);
     }
 }
 

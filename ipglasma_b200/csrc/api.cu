@@ -1282,7 +1282,7 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
         for (int s = S - 1; s >= 0; s--) {
             const StepCoef<double> cf = evolution_coef(c, s);
             launch_adjoint_step(N, A.cp[s], A.cp[s + 1], A.adj, cf, c->stream);
-            IPG_LAUNCHED(c, cf.do_pe ? 3 : 1);
+            IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
         }
     } else {
         // reverse sweep: state s from state s+1 by time reversal, or from the
@@ -1295,10 +1295,10 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
             if (s % A.k == 0) {
                 IPG_TRY(copy_state(c, cur, A.cp[s / A.k]));
                 launch_adjoint_step(N, cur, nxt, A.adj, cf, c->stream);
-                IPG_LAUNCHED(c, cf.do_pe ? 3 : 1);
+                IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
             } else {
                 launch_inverse_adjoint_step(N, nxt, cur, A.adj, cf, c->stream);
-                IPG_LAUNCHED(c, cf.do_pe ? 4 : 2);
+                IPG_LAUNCHED(c, cf.do_pe ? 3 : 2);
             }
             nxt = cur;
         }
