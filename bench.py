@@ -574,17 +574,18 @@ def measure_e2e(torch, ipg, A, B, K, seed0, l2buf, dist):
         total += time.perf_counter() - t0
     itmax = ev.itmax
     dtau = ev.dtau
+    writers = measure_writers(ipg, ev, eps, u4, pi10, T10, itmax, dtau)
     ev.close()
-    writers = measure_writers(ipg, eps, u4, pi10, T10, itmax, dtau)
     return {"ms": total * 1e3, "h2d": int(2 * n * 8), "d2h": int(25 * n * 8),
             "host_buffers": "pinned", "writers": writers}
 
 
-def measure_writers(ipg, eps, u4, pi10, T10, itmax, dtau):
-    """Host output formatting, timed apart from the event rate: the
-    reference's hydro and T^munu files of one event (sizeOutput = N over the
-    lattice, one eta slice) written from its observables into a scratch
-    directory that is removed afterwards."""
+def measure_writers(ipg, ev, eps, u4, pi10, T10, itmax, dtau):
+    """Output files, timed apart from the event rate: the reference's hydro
+    and T^munu files of the last event (sizeOutput = N over the lattice, one
+    eta slice) written into a scratch directory that is removed afterwards,
+    by the host writers from its observables and by the GPU writer
+    (ipg_write_outputs) from the device copy; the two must be byte-identical."""
     import ctypes as ct
     import shutil
     import tempfile
@@ -603,12 +604,25 @@ def measure_writers(ipg, eps, u4, pi10, T10, itmax, dtau):
                                   V(T10), D(1.0))
         t2 = time.perf_counter()
         sizes = os.path.getsize(hydro) + os.path.getsize(tmunu)
+        gh, gt = os.path.join(d, "hydro_gpu.dat"), os.path.join(d, "tmunu_gpu.dat")
+        ev.write_outputs(gh, gt)  # warm-up: buffers, first launch
+        gpu_ms = []
+        for path_h, path_t in ((gh, None), (None, gt)):
+            t3 = time.perf_counter()
+            ev.write_outputs(path_h, path_t)
+            gpu_ms.append((time.perf_counter() - t3) * 1e3)
+        same = all(open(a, "rb").read() == open(b, "rb").read()
+                   for a, b in ((hydro, gh), (tmunu, gt)))
     finally:
         shutil.rmtree(d, ignore_errors=True)
     threads = os.environ.get("IPG_WRITER_THREADS") or str(os.cpu_count())
     return {"ms_hydro": round((t1 - t0) * 1e3, 1), "ms_tmunu": round((t2 - t1) * 1e3, 1),
             "bytes": int(sizes), "threads": int(threads), "status": [int(st), int(st2)],
-            "timing": "host wall clock, once per bench run; not part of the event rate"}
+            "gpu_ms_hydro": round(gpu_ms[0], 1), "gpu_ms_tmunu": round(gpu_ms[1], 1),
+            "gpu_files_identical": bool(same),
+            "timing": "wall clock, once per bench run, file write included; not part of the "
+                      "event rate. ms_*: host writers from host observables; gpu_ms_*: "
+                      "ipg_write_outputs from the device observables"}
 
 
 def load_peaks():

@@ -221,6 +221,17 @@ ipg_status ipg_write_hydro(const char *path, int N, double L, int sizeOutput,
 ipg_status ipg_write_tmunu(const char *path, int N, double L, int sizeOutput,
                            double LOutput, int etaSizeOutput, double detaOutput,
                            int it, double dtau, const double *T10, double gfactor);
+/* The same two files from the context's observables after ipg_run, with the
+ * resampling and the number formatting on the GPU: byte-identical to
+ * ipg_write_hydro / ipg_write_tmunu on the ipg_get_observables arrays (same
+ * operation order and rounding, correctly rounded "%.6g"), for L and N of
+ * the context. Either path may be NULL. A file holding a number outside
+ * [1e-130, 1e6) in magnitude (or a NaN) is written by the host writer
+ * instead, with the same result. */
+ipg_status ipg_write_outputs(ipg_ctx *ctx, const char *hydro_path, const char *tmunu_path,
+                             int sizeOutput, double LOutput, int etaSizeOutput,
+                             double detaOutput, int it, double dtau, double gfactor,
+                             double *Etot);
 /* The reference's output file names for an event id (MyEigen.cpp:376-383,
  * 804-807); buffers of at least 64 bytes. */
 ipg_status ipg_output_names(int event_id, int it, double dtau, double a,

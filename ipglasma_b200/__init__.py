@@ -109,6 +109,16 @@ _SIGNATURES = {
     "ipg_evolve": (ct.c_int, [ct.c_void_p, ct.c_int]),
     "ipg_get_observables": (ct.c_int, [ct.c_void_p] + [ct.c_void_p] * 4),
     "ipg_get_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p]),
+    "ipg_write_outputs": (ct.c_int, [ct.c_void_p, ct.c_char_p, ct.c_char_p, ct.c_int,
+                                     ct.c_double, ct.c_int, ct.c_double, ct.c_int, ct.c_double,
+                                     ct.c_double, ct.POINTER(ct.c_double)]),
+    "ipg_write_hydro": (ct.c_int, [ct.c_char_p, ct.c_int, ct.c_double, ct.c_int, ct.c_double,
+                                   ct.c_int, ct.c_double, ct.c_int, ct.c_double, ct.c_void_p,
+                                   ct.c_void_p, ct.c_void_p, ct.c_double,
+                                   ct.POINTER(ct.c_double)]),
+    "ipg_write_tmunu": (ct.c_int, [ct.c_char_p, ct.c_int, ct.c_double, ct.c_int, ct.c_double,
+                                   ct.c_int, ct.c_double, ct.c_int, ct.c_double, ct.c_void_p,
+                                   ct.c_double]),
     "ipg_set_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p]),
     "ipg_mark_initialized": (ct.c_int, [ct.c_void_p]),
     "ipg_get_newton_iterations": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
@@ -326,6 +336,21 @@ class Event:
         self._check(self._lib.ipg_get_observables(self._h, _ptr(eps), _ptr(u4),
                                                   _ptr(pi10), _ptr(T10)))
         return eps, u4, pi10, T10
+
+    def write_outputs(self, hydro=None, tmunu=None, size_output=None, L_output=None,
+                      eta_size=1, deta=0.0, gfactor=1.0):
+        """The hydro and KoMPoST files of the last run (paths; either may be
+        None) with the resampling and formatting on the GPU, byte-identical
+        to the host writers (ipg_write_outputs). Defaults resample onto the
+        lattice itself. Returns the hydro file's Etot (GeV), or None."""
+        size_output = self.N if size_output is None else size_output
+        L_output = self.cfg.L if L_output is None else L_output
+        et = ct.c_double()
+        self._check(self._lib.ipg_write_outputs(
+            self._h, str(hydro).encode() if hydro else None,
+            str(tmunu).encode() if tmunu else None, size_output, L_output, eta_size, deta,
+            self.itmax, self.dtau, gfactor, ct.byref(et)))
+        return et.value if hydro else None
 
     def get_field(self, which: int) -> np.ndarray:
         out = np.empty((self.n, 9), dtype=np.complex128)

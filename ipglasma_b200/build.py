@@ -26,7 +26,10 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC"]
 CU_SOURCES = ["api.cu", "evolve.cu", "init.cu", "poisson.cu", "observables.cu", "reduce.cu",
-              "noalloc.cu", "adjoint.cu", "nuclei.cu"]
+              "noalloc.cu", "adjoint.cu", "nuclei.cu", "writers_gpu.cu"]
+# the GPU writer rounds every sum and product on its own, as the host writer
+# (g++ -ffp-contract=off) does, so its text is byte-identical
+CU_EXTRA_FLAGS = {"writers_gpu.cu": ["-fmad=false"]}
 CPP_SOURCES = ["writers.cpp"]
 
 
@@ -64,8 +67,8 @@ def build_library(verbose: bool = False, force: bool = False) -> Path:
     objs = []
     for src in CU_SOURCES:
         obj = objdir / (Path(src).stem + ".o")
-        cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-I", str(ROOT / "include"), "-c",
-               str(CSRC / src), "-o", str(obj)]
+        cmd = [nvcc, *ARCH, *NVCC_FLAGS, *CU_EXTRA_FLAGS.get(src, []), "-I",
+               str(ROOT / "include"), "-c", str(CSRC / src), "-o", str(obj)]
         if verbose:
             cmd += ["-Xptxas", "-v"]
         out = _run(cmd)

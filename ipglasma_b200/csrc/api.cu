@@ -19,6 +19,7 @@
 
 #include "../../include/ipglasma_b200.h"
 #include "ipg_internal.h"
+#include "writers.h"
 
 using namespace ipg;
 
@@ -104,6 +105,18 @@ struct ipg_ctx {
         double *g2mu_bar = nullptr;
         double *rho_all = nullptr;  // [2][Ny][n][8] rho adjoint, kept on the device
     } aw;
+
+    // output files formatted on the GPU (ipg_write_outputs); freed by ipg_destroy
+    struct {
+        long long cap_lines = 0;
+        char *chunks = nullptr, *text = nullptr;
+        int *chunk_len = nullptr, *bad = nullptr;
+        long long *chunk_off = nullptr;
+        double *term = nullptr;
+        char *h_text = nullptr;     // pinned image of the file body
+        double *h_term = nullptr;   // pinned Etot terms
+        long long *h_small = nullptr;  // pinned: total bytes, bad flag
+    } out;
     bool init_from_inputs = false;
 
     std::vector<void *> allocs;
@@ -606,6 +619,14 @@ ipg_status ipg_destroy(ipg_ctx *ctx) {
     }
     for (void *p : ctx->allocs) cudaFree(p);
     if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
+    {
+        auto &o = ctx->out;
+        for (void *p : {(void *)o.chunks, (void *)o.text, (void *)o.chunk_len, (void *)o.bad,
+                        (void *)o.chunk_off, (void *)o.term})
+            if (p) cudaFree(p);
+        for (void *p : {(void *)o.h_text, (void *)o.h_term, (void *)o.h_small})
+            if (p) cudaFreeHost(p);
+    }
     for (cudaEvent_t x : ctx->ie)
         if (x) cudaEventDestroy(x);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -928,6 +949,109 @@ ipg_status ipg_get_observables(ipg_ctx *c, double *eps, double *u4,
     if (pi10) IPG_CUDA(c, cudaMemcpyAsync(pi10, c->pi10, sizeof(double) * 10 * n, d2h, c->stream));
     if (T10) IPG_CUDA(c, cudaMemcpyAsync(T10, c->T10, sizeof(double) * 10 * n, d2h, c->stream));
     IPG_TRY(sync(c));
+    return IPG_OK;
+}
+
+ipg_status ipg_write_outputs(ipg_ctx *c, const char *hydro_path, const char *tmunu_path,
+                             int sizeOutput, double LOutput, int etaSizeOutput,
+                             double detaOutput, int it, double dtau, double gfactor,
+                             double *Etot) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (!c->finished) return fail(c, IPG_ERR_STATE, "call ipg_run first");
+    if (sizeOutput < 1 || etaSizeOutput < 0)
+        return fail(c, IPG_ERR_BAD_CONFIG, "sizeOutput < 1 or etaSizeOutput < 0");
+    OutputGrid g;
+    g.N = c->N;
+    g.L = c->cfg.L;
+    g.a = g.L / g.N;
+    g.hx = sizeOutput;
+    g.heta = etaSizeOutput;
+    g.hL = LOutput;
+    g.ha = LOutput / sizeOutput;
+    g.deta = detaOutput;
+    g.it = it;
+    g.dtau = dtau;
+    g.gfactor = gfactor;
+    g.tau0 = it * dtau * g.a;
+    const OutputFields f{c->eps, c->u4, c->pi10, c->T10};
+    auto &o = c->out;
+    const long long hydro_lines = (long long)g.heta * g.hx * g.hx;
+    const long long tmunu_lines = (long long)g.hx * g.hx;
+    const long long need = std::max(hydro_path ? hydro_lines : 0, tmunu_path ? tmunu_lines : 0);
+    if (need > o.cap_lines) {
+        for (void *p : {(void *)o.chunks, (void *)o.text, (void *)o.chunk_len,
+                        (void *)o.chunk_off, (void *)o.term, (void *)o.bad})
+            if (p) cudaFree(p);
+        for (void *p : {(void *)o.h_text, (void *)o.h_term, (void *)o.h_small})
+            if (p) cudaFreeHost(p);
+        o = {};
+        const size_t bytes = output_text_capacity(need);
+        const int chunks = output_text_chunks(need);
+        IPG_CUDA(c, cudaMalloc(&o.chunks, bytes));
+        IPG_CUDA(c, cudaMalloc(&o.text, bytes));
+        IPG_CUDA(c, cudaMalloc(&o.chunk_len, sizeof(int) * chunks));
+        IPG_CUDA(c, cudaMalloc(&o.chunk_off, sizeof(long long) * (chunks + 1)));
+        IPG_CUDA(c, cudaMalloc(&o.term, sizeof(double) * need));
+        IPG_CUDA(c, cudaMalloc(&o.bad, sizeof(int)));
+        IPG_CUDA(c, cudaMallocHost(&o.h_text, bytes));
+        IPG_CUDA(c, cudaMallocHost(&o.h_term, sizeof(double) * need));
+        IPG_CUDA(c, cudaMallocHost(&o.h_small, 2 * sizeof(long long)));
+        o.cap_lines = need;
+    }
+    // one file: body on the GPU, then header + body with one fwrite each; a
+    // body that needs the host formatter goes through the host writer
+    auto one = [&](int kind, const char *path, long long lines) -> ipg_status {
+        IPG_CUDA(c, cudaMemsetAsync(o.bad, 0, sizeof(int), c->stream));
+        launch_output_text(kind, g, f, lines, o.chunks, o.chunk_len, o.chunk_off, o.text,
+                           o.term, o.bad, c->stream);
+        IPG_LAUNCHED(c, lines > 0 ? 3 : 0);
+        const int chunks = output_text_chunks(lines);
+        long long *hs = o.h_small;
+        hs[0] = 0;
+        hs[1] = 0;
+        if (lines > 0)
+            IPG_CUDA(c, cudaMemcpyAsync(&hs[0], o.chunk_off + chunks, sizeof(long long),
+                                        cudaMemcpyDeviceToHost, c->stream));
+        IPG_CUDA(c, cudaMemcpyAsync(&hs[1], o.bad, sizeof(int), cudaMemcpyDeviceToHost,
+                                    c->stream));
+        IPG_TRY(sync(c));
+        if ((int)hs[1] != 0) {
+            const size_t n = c->n;
+            std::vector<double> eps(n), u4(4 * n), pi10(10 * n), T10(10 * n);
+            IPG_TRY(ipg_get_observables(c, eps.data(), u4.data(), pi10.data(), T10.data()));
+            return kind == 0 ? ipg_write_hydro(path, g.N, g.L, g.hx, g.hL, g.heta, g.deta, it,
+                                               dtau, eps.data(), u4.data(), pi10.data(),
+                                               gfactor, Etot)
+                             : ipg_write_tmunu(path, g.N, g.L, g.hx, g.hL, g.heta, g.deta, it,
+                                               dtau, T10.data(), gfactor);
+        }
+        const size_t body = (size_t)hs[0];
+        if (body)
+            IPG_CUDA(c, cudaMemcpyAsync(o.h_text, o.text, body, cudaMemcpyDeviceToHost,
+                                        c->stream));
+        if (kind == 0 && Etot && lines > 0)
+            IPG_CUDA(c, cudaMemcpyAsync(o.h_term, o.term, sizeof(double) * lines,
+                                        cudaMemcpyDeviceToHost, c->stream));
+        IPG_TRY(sync(c));
+        const std::string head =
+            kind == 0 ? hydro_header(g.N, g.L, g.hx, g.hL, g.heta, g.deta, it, dtau)
+                      : tmunu_header(g.N, g.L, g.hx, g.hL, g.heta, g.deta);
+        FILE *fp = std::fopen(path, "wb");
+        if (!fp) return fail(c, IPG_ERR_BAD_CONFIG, "cannot open %s", path);
+        bool ok = std::fwrite(head.data(), 1, head.size(), fp) == head.size();
+        ok = ok && std::fwrite(o.h_text, 1, body, fp) == body;
+        ok = (std::fclose(fp) == 0) && ok;
+        if (!ok) return fail(c, IPG_ERR_BAD_CONFIG, "writing %s failed", path);
+        if (kind == 0 && Etot) {
+            // the reference's running sum, in its loop order
+            double etot = 0.;
+            for (long long i = 0; i < lines; i++) etot += o.h_term[i];
+            *Etot = etot;
+        }
+        return IPG_OK;
+    };
+    if (hydro_path) IPG_TRY(one(0, hydro_path, hydro_lines));
+    if (tmunu_path) IPG_TRY(one(1, tmunu_path, tmunu_lines));
     return IPG_OK;
 }
 

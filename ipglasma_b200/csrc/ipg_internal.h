@@ -254,6 +254,31 @@ void launch_newton_stats(size_t links, const int *iters, const int *status,
 void launch_cell_flags(size_t n, const int *found, const double *eps,
                        double *d_partial, double *d_out, cudaStream_t st);
 
+// ---- output files formatted on the GPU (writers_gpu.cu) -------------------
+// resampling grid of writers.cpp: lattice N, L, a = L/N; output hx = sizeOutput
+// points over hL = LOutput (spacing ha), heta eta slices of deta; proper time
+// tau0 = it dtau a
+struct OutputGrid {
+    int N;
+    double L, a;
+    int hx, heta;
+    double hL, ha, deta;
+    int it;
+    double dtau, gfactor, tau0;
+};
+struct OutputFields {
+    const double *eps, *u4, *pi10, *T10;  // device, as ipg_get_observables
+};
+// bytes of the chunk buffer and of the text image for `lines` output lines
+size_t output_text_capacity(long long lines);
+int output_text_chunks(long long lines);
+// kind 0: hydro file lines (heta hx hx, term[line] = the Etot term), kind 1:
+// KoMPoST lines (hx hx); text receives the file body, chunk_off[chunks] its
+// length; *bad is set when a number needs the host formatter
+void launch_output_text(int kind, const OutputGrid &g, const OutputFields &f, long long lines,
+                        char *chunks, int *chunk_len, long long *chunk_off, char *text,
+                        double *term, int *bad, cudaStream_t st);
+
 template <typename T>
 void launch_convert_state(size_t n, const State<T> &src, State<double> &dst,
                           cudaStream_t st);

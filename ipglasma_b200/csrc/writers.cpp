@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "../../include/ipglasma_b200.h"
+#include "writers.h"
 
 namespace {
 
@@ -107,6 +108,25 @@ class Text {
     size_t n_ = 0;
 };
 
+// "# dummy 1 etamax= .. xmax= .. ymax= .. deta= .. dx= .. dy= .." and, for the
+// hydro file, " tau= ..", then a newline
+Text header(const Grid &g, bool with_tau, double tau0) {
+    Text head(256);
+    head.line(16);
+    auto label = [&](const char *s) {
+        for (; *s; s++) head.ch(*s);
+    };
+    label("# dummy "), head.num(1);
+    label(" etamax= "), head.num(g.heta), label(" xmax= "), head.num(g.hx);
+    label(" ymax= "), head.num(g.hx), label(" deta= "), head.num(g.deta);
+    label(" dx= "), head.num(g.ha), label(" dy= "), head.num(g.ha);
+    if (with_tau) label(" tau= "), head.num(tau0);
+    head.ch('\n');
+    return head;
+}
+Text hydro_head(const Grid &g, double tau0) { return header(g, true, tau0); }
+Text tmunu_head(const Grid &g) { return header(g, false, 0.); }
+
 // threads used to format a file of `rows` output rows: the host's hardware
 // threads (IPG_WRITER_THREADS overrides), at most one per 4 rows
 int writer_threads(int rows) {
@@ -146,6 +166,26 @@ bool format_and_write(const char *path, const Text &head, int rows, size_t bytes
 
 }  // namespace
 
+namespace ipg {
+
+std::string hydro_header(int N, double L, int sizeOutput, double LOutput, int etaSizeOutput,
+                         double detaOutput, int it, double dtau) {
+    const Grid g{N, L, L / N, sizeOutput, etaSizeOutput, LOutput, LOutput / sizeOutput,
+                 detaOutput};
+    const Text h = hydro_head(g, it * dtau * g.a);
+    return std::string(h.data(), h.size());
+}
+
+std::string tmunu_header(int N, double L, int sizeOutput, double LOutput, int etaSizeOutput,
+                         double detaOutput) {
+    const Grid g{N, L, L / N, sizeOutput, etaSizeOutput, LOutput, LOutput / sizeOutput,
+                 detaOutput};
+    const Text h = tmunu_head(g);
+    return std::string(h.data(), h.size());
+}
+
+}  // namespace ipg
+
 extern "C" {
 
 ipg_status ipg_write_hydro(const char *path, int N, double L, int sizeOutput,
@@ -159,17 +199,7 @@ ipg_status ipg_write_hydro(const char *path, int N, double L, int sizeOutput,
     const int nn = N * N;
     const double a = g.a;
     const double tau0 = it * dtau * a;
-    Text head(256);
-    head.line(16);
-    for (const char *c = "# dummy "; *c; c++) head.ch(*c);
-    head.num(1);
-    auto label = [&](const char *s) {
-        for (; *s; s++) head.ch(*s);
-    };
-    label(" etamax= "), head.num(g.heta), label(" xmax= "), head.num(g.hx);
-    label(" ymax= "), head.num(g.hx), label(" deta= "), head.num(g.deta);
-    label(" dx= "), head.num(g.ha), label(" dy= "), head.num(g.ha);
-    label(" tau= "), head.num(tau0), head.ch('\n');
+    const Text head = hydro_head(g, tau0);
     const size_t n = (size_t)nn;
     // pi10 order: tautau xx yy etaeta taux tauy taueta xy xeta yeta
     const double *p00 = pi10, *pxx = pi10 + n, *pyy = pi10 + 2 * n, *pee = pi10 + 3 * n;
@@ -245,15 +275,7 @@ ipg_status ipg_write_tmunu(const char *path, int N, double L, int sizeOutput,
     const int nn = N * N;
     const size_t n = (size_t)nn;
     const double tau0 = it * dtau * g.a;
-    Text head(256);
-    head.line(16);
-    auto label = [&](const char *s) {
-        for (; *s; s++) head.ch(*s);
-    };
-    label("# dummy "), head.num(1);
-    label(" etamax= "), head.num(g.heta), label(" xmax= "), head.num(g.hx);
-    label(" ymax= "), head.num(g.hx), label(" deta= "), head.num(g.deta);
-    label(" dx= "), head.num(g.ha), label(" dy= "), head.num(g.ha), head.ch('\n');
+    const Text head = tmunu_head(g);
     // one output row = iy: hx lines and a blank line
     auto body = [&](Text &out, int iy) {
         for (int ix = 0; ix < g.hx; ix++) {

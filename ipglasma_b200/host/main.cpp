@@ -316,20 +316,20 @@ int main(int argc, char **argv) {
         }
         ipg_result res;
         check(ctx, ipg_run(ctx, &res), "ipg_run");
-        std::vector<double> eps(n), u4(4 * n), pi10(10 * n), T10(10 * n);
-        check(ctx, ipg_get_observables(ctx, eps.data(), u4.data(), pi10.data(), T10.data()),
-              "ipg_get_observables");
         char hname[256], tname[256];
         ipg_output_names(event_id, itmax, dtau, a, hname, sizeof(hname), tname, sizeof(tname));
-        if (writeOutputs % 2 == 1) {
+        // both files resampled and formatted on the GPU from the device
+        // observables (the same bytes as the host writers)
+        const bool hydro = writeOutputs % 2 == 1, kompost = writeOutputs / 4 == 1;
+        if (hydro || kompost) {
             double etot = 0;
-            ipg_write_hydro(hname, N, cfg.L, sizeOutput, LOutput, etaSizeOutput, detaOutput,
-                            itmax, dtau, eps.data(), u4.data(), pi10.data(), 1.0, &etot);
-            std::cout << "Etot = " << etot << " GeV " << std::endl;
+            check(ctx,
+                  ipg_write_outputs(ctx, hydro ? hname : nullptr, kompost ? tname : nullptr,
+                                    sizeOutput, LOutput, etaSizeOutput, detaOutput, itmax, dtau,
+                                    1.0, &etot),
+                  "ipg_write_outputs");
+            if (hydro) std::cout << "Etot = " << etot << " GeV " << std::endl;
         }
-        if (writeOutputs / 4 == 1)
-            ipg_write_tmunu(tname, N, cfg.L, sizeOutput, LOutput, etaSizeOutput, detaOutput,
-                            itmax, dtau, T10.data(), 1.0);
         const double sec =
             std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         std::cout << "event " << event_id << ": b=" << b << " fm, itmax=" << res.itmax
