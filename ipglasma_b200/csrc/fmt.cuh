@@ -26,9 +26,10 @@ struct Big {
     uint64_t w[6];
 };
 
-IPG_FMT_HD void mul_small(Big &b, uint64_t f) {
+// b *= f over its nl low limbs (nl grows by the carry out)
+IPG_FMT_HD void mul_small(Big &b, int &nl, uint64_t f) {
     uint64_t carry = 0;
-    for (int i = 0; i < 6; i++) {
+    for (int i = 0; i < nl; i++) {
 #ifdef __CUDA_ARCH__
         const uint64_t lo = b.w[i] * f, hi = __umul64hi(b.w[i], f);
 #else
@@ -39,20 +40,20 @@ IPG_FMT_HD void mul_small(Big &b, uint64_t f) {
         carry = hi + (s < lo ? 1 : 0);
         b.w[i] = s;
     }
+    if (carry && nl < 6) b.w[nl++] = carry;
 }
 
-IPG_FMT_HD int bit_length(const Big &b) {
-    for (int i = 5; i >= 0; i--) {
-        if (b.w[i]) {
-            int l = 64;
-            uint64_t x = b.w[i];
-            while (!(x >> 63)) {
-                x <<= 1;
-                l--;
-            }
-            return 64 * i + l;
-        }
-    }
+IPG_FMT_HD int clz64(uint64_t x) {
+#ifdef __CUDA_ARCH__
+    return __clzll((long long)x);
+#else
+    return __builtin_clzll(x);
+#endif
+}
+
+IPG_FMT_HD int bit_length(const Big &b, int nl) {
+    for (int i = nl - 1; i >= 0; i--)
+        if (b.w[i]) return 64 * i + 64 - clz64(b.w[i]);
     return 0;
 }
 
@@ -77,26 +78,23 @@ IPG_FMT_HD uint64_t bits_from(const Big &b, int r) {
 
 IPG_FMT_HD double abs_d(double v) { return v < 0 ? -v : v; }
 
-// floor(log10(av)) estimate for av in [1e-130, 1e6): exact up to +-1
-IPG_FMT_HD int decade(double av) {
-    int e = 0;
-    if (av >= 1.) {
-        while (av >= 10. && e < 400) {
-            av /= 10.;
-            e++;
-        }
-    } else {
-        // multiply by 1e10 while far below 1, then by 10
-        while (av < 1e-10) {
-            av *= 1e10;
-            e -= 10;
-        }
-        while (av < 1.) {
-            av *= 10.;
-            e--;
-        }
+// floor(log10(v)) for v = m 2^q with the binary exponent eb = q + 52
+// (m in [2^52, 2^53)): floor(eb log10 2) is within one of it; the caller
+// corrects it exactly
+IPG_FMT_HD int decade(int eb) {
+    // 78913 / 2^18 = 0.30102920... (log10 2 = 0.30102999...), exact floor for |eb| < 1700
+    return (eb * 78913) >> 18;
+}
+
+// 5^k for k in [0, 27]
+IPG_FMT_HD uint64_t pow5(int k) {
+    uint64_t r = 1, b = 5;
+    while (k) {
+        if (k & 1) r *= b;
+        b *= b;
+        k >>= 1;
     }
-    return e;
+    return r;
 }
 
 // text of v as printf "%.6g" into p (at most 13 characters); returns the
@@ -124,22 +122,21 @@ IPG_FMT_HD int g6(double v, char *p) {
     if (!(av >= 1e-130 && av < 1e6)) return -1;
     const uint64_t m = mbits | (1ull << 52);  // normal numbers only in this range
     const int q = ebits - 1075;
-    int E = decade(av);
+    int E = decade(q + 52);
     uint64_t N = 0;
     for (int tries = 0;; tries++) {
         const int k = 5 - E;  // v 10^k = m 5^k 2^(k+q) should lie in [1e5, 1e6)
         if (k < 0 || k > 140 || tries > 3) return -1;
         Big P = {{m, 0, 0, 0, 0, 0}};
+        int nl = 1;
         int k5 = k;
         while (k5 >= 27) {
-            mul_small(P, 7450580596923828125ull);  // 5^27
+            mul_small(P, nl, 7450580596923828125ull);  // 5^27
             k5 -= 27;
         }
-        uint64_t f5 = 1;
-        for (int i = 0; i < k5; i++) f5 *= 5;
-        mul_small(P, f5);
+        mul_small(P, nl, pow5(k5));
         const int s = k + q;
-        const int len = bit_length(P);
+        const int len = bit_length(P, nl);
         uint64_t F;
         bool up = false;
         if (s >= 0) {
