@@ -1215,20 +1215,34 @@ ipg_status backward_inputs(ipg_ctx *c, double *grad_g2mu, double *grad_rho) {
         w.no_product = 1;
         launch_wilson_amp(w, c->stream);
         IPG_LAUNCHED(c, 1);
-        for (int k = Ny - 1; k >= 0; k--) {
+        // batches of work_sheets sheets from the top: the transforms of a
+        // batch (A_k, then the Poisson map of A_bar_k) run as one launch each,
+        // the product recursion and the rho adjoint sheet by sheet in the
+        // order k = Ny-1 .. 0 (the accumulation order of g2mu_bar)
+        const int S = c->work_sheets;
+        for (int kb = Ny; kb > 0; kb -= S) {
+            const int k0 = std::max(0, kb - S), ns = kb - k0;
             w.rho_in = nullptr;
-            launch_wilson_sheets(w, k, 1, c->stream);  // work = A_k
+            launch_wilson_sheets(w, k0, ns, c->stream);  // slot k - k0 = A_k
             IPG_LAUNCHED(c, 3);
-            launch_adjoint_wilson_sheet(N, c->work, A.vcur, vb, c->stream);  // work = A_bar_k
-            IPG_LAUNCHED(c, 1);
+            for (int k = kb - 1; k >= k0; k--) {
+                // slot k - k0 becomes A_bar_k
+                launch_adjoint_wilson_sheet(N, c->work + (size_t)(k - k0) * 4 * n, A.vcur, vb,
+                                            c->stream);
+                IPG_LAUNCHED(c, 1);
+            }
             w.rho_in = c->work;
-            launch_poisson_sheets(w, 1, c->stream);  // work = rho_bar_k
+            launch_poisson_sheets(w, ns, c->stream);  // in place: slot k - k0 = rho_bar_k
             IPG_LAUNCHED(c, 3);
             w.rho_in = nullptr;
-            launch_adjoint_rho(w, k, A.g2mu_bar + nuc * n,
-                               grad_rho ? A.rho_all + ((size_t)nuc * Ny + k) * n * 8 : nullptr,
-                               c->stream);
-            IPG_LAUNCHED(c, 1);
+            for (int k = kb - 1; k >= k0; k--) {
+                WilsonArgs ws = w;
+                ws.work = c->work + (size_t)(k - k0) * 4 * n;
+                launch_adjoint_rho(ws, k, A.g2mu_bar + nuc * n,
+                                   grad_rho ? A.rho_all + ((size_t)nuc * Ny + k) * n * 8 : nullptr,
+                                   c->stream);
+                IPG_LAUNCHED(c, 1);
+            }
         }
     }
     return IPG_OK;
