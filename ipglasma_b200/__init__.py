@@ -393,25 +393,37 @@ class Event:
         return f.value, b.value
 
     def backward(self, w_ET: float = 1.0, w_eps2: float = 0.0, inputs: bool = False,
-                 rho: bool = False):
+                 rho: bool = False, out: dict | None = None):
         """Gradient of w_ET E_T + w_eps2 eps2 w.r.t. the tau = 0 fields:
         dict field -> (N*N, 3, 3) complex array (dL/dRe + i dL/dIm). With
         inputs, also "g2mu" -> (2, N*N) (nuclei A, B); with rho, "rho" ->
-        (2, Ny, N*N, 8)."""
-        g = np.empty(6 * 18 * self.n)
-        gm = np.empty(2 * self.n) if inputs else None
-        gr = np.empty(2 * self.cfg.Ny * self.n * 8) if rho else None
+        (2, Ny, N*N, 8). ``out`` may hold float64 arrays to fill instead of
+        new ones (page-locked arrays make the copies run at link speed):
+        "state" (6*18*N*N), "g2mu" (2*N*N), "rho" (16*Ny*N*N); the returned
+        arrays are views of them."""
+        out = out or {}
+        g = out.get("state")
+        g = np.empty(6 * 18 * self.n) if g is None else g
+        gm = (out.get("g2mu") if out.get("g2mu") is not None else np.empty(2 * self.n)) \
+            if inputs else None
+        gr = (out.get("rho") if out.get("rho") is not None
+              else np.empty(2 * self.cfg.Ny * self.n * 8)) if rho else None
+        for a, size in ((g, 6 * 18 * self.n), (gm, 2 * self.n),
+                        (gr, 16 * self.cfg.Ny * self.n)):
+            if a is not None and (a.dtype != np.float64 or a.size != size
+                                  or not a.flags.c_contiguous):
+                raise ValueError(f"output buffer needs {size} contiguous float64")
         self._check(self._lib.ipg_backward(
             self._h, w_ET, w_eps2, _ptr(g), _ptr(gm) if gm is not None else None,
             _ptr(gr) if gr is not None else None))
-        g = g.reshape(6, self.n, 9, 2)
-        z = g[..., 0] + 1j * g[..., 1]
-        out = {f: z[k].reshape(self.n, 3, 3) for k, f in enumerate((UX, UY, E1, E2, PHI, PI))}
+        # (re, im) pairs read as complex numbers without a copy
+        z = g.reshape(6, self.n, 18).view(np.complex128)
+        res = {f: z[k].reshape(self.n, 3, 3) for k, f in enumerate((UX, UY, E1, E2, PHI, PI))}
         if gm is not None:
-            out["g2mu"] = gm.reshape(2, self.n)
+            res["g2mu"] = gm.reshape(2, self.n)
         if gr is not None:
-            out["rho"] = gr.reshape(2, self.cfg.Ny, self.n, 8)
-        return out
+            res["rho"] = gr.reshape(2, self.cfg.Ny, self.n, 8)
+        return res
 
     def kernel_launches(self) -> int:
         c = ct.c_longlong()
