@@ -202,7 +202,7 @@ def main():
                     help="skip the batched uneven-events measurement")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint (forward/backward) measurement")
-    ap.add_argument("--profile", choices=["fp32", "fp64", "both"], default=None,
+    ap.add_argument("--profile", choices=["fp32", "fp64", "both", "adjoint"], default=None,
                     help="run one warm-up and one timed event per form and exit "
                          "(the command profiled under ncu)")
     ap.add_argument("--profile-n", type=int, default=512,
@@ -223,6 +223,25 @@ def run_profile(which, local):
     import ipglasma_b200 as ipg
 
     torch.cuda.set_device(local)
+    if which == "adjoint":
+        # the adjoint workload's event (Au+Au 256^2, Ny 50) over 40 steps, every
+        # state kept (1.5 GB): one forward and one backward
+        from ipglasma_b200.synthetic import make_event
+        w = ADJ
+        a = w["L"] / w["N"]
+        A, B, _, _ = make_event(w["N"], w["L"], w["nucleus"], w["b"], 8000)
+        ev = ipg.Event(ipg.Config(size=w["N"], L=w["L"], Ny=w["Ny"], maxtime=40 * w["dtau"] * a,
+                                  dtau=w["dtau"], precision=ipg.FP64, seed=8100,
+                                  newton_tolerance=1e-12))
+        ev.set_g2mu(A, B)
+        ev.use_device_noise()
+        ev.init_fields(allow_nonconverged=True)
+        et, e2 = ev.forward(1)
+        ev.backward(1.0, 1.0, inputs=True)
+        f, b = ev.adjoint_stats()
+        print(f"adjoint steps={ev.itmax} E_T={et} forward_ms={f} backward_ms={b}")
+        ev.close()
+        return
     A, B = make_inputs()
     d_A = torch.tensor(A, dtype=torch.float64, device="cuda")
     d_B = torch.tensor(B, dtype=torch.float64, device="cuda")
