@@ -183,6 +183,14 @@ ipg_status ipg_evolve(ipg_ctx *ctx, int steps);
  * MyEigen.cpp:259-305, Evolution.cpp:759-1238). Any pointer may be NULL. */
 ipg_status ipg_get_observables(ipg_ctx *ctx, double *eps, double *u4,
                                double *pi10, double *T10);
+/* The same copies started on a second stream, returning at once: they run
+ * while the caller starts the next event on this context, whose observables
+ * stage waits for them before it rewrites the device arrays. The host arrays
+ * are complete after ipg_wait_observables; they should be page-locked for
+ * the copies to overlap. */
+ipg_status ipg_get_observables_async(ipg_ctx *ctx, double *eps, double *u4, double *pi10,
+                                     double *T10);
+ipg_status ipg_wait_observables(ipg_ctx *ctx);
 
 /* Field access for stage-wise checks; which = IPG_UX, IPG_UY, IPG_E1, IPG_E2,
  * IPG_PHI, IPG_PI, IPG_VA, IPG_VB: N*N*18 doubles (Cell::getUx ...,

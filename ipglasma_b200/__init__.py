@@ -108,6 +108,8 @@ _SIGNATURES = {
     "ipg_run": (ct.c_int, [ct.c_void_p, ct.POINTER(_Result)]),
     "ipg_evolve": (ct.c_int, [ct.c_void_p, ct.c_int]),
     "ipg_get_observables": (ct.c_int, [ct.c_void_p] + [ct.c_void_p] * 4),
+    "ipg_get_observables_async": (ct.c_int, [ct.c_void_p] + [ct.c_void_p] * 4),
+    "ipg_wait_observables": (ct.c_int, [ct.c_void_p]),
     "ipg_get_field": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p]),
     "ipg_write_outputs": (ct.c_int, [ct.c_void_p, ct.c_char_p, ct.c_char_p, ct.c_int,
                                      ct.c_double, ct.c_int, ct.c_double, ct.c_int, ct.c_double,
@@ -336,6 +338,19 @@ class Event:
         self._check(self._lib.ipg_get_observables(self._h, _ptr(eps), _ptr(u4),
                                                   _ptr(pi10), _ptr(T10)))
         return eps, u4, pi10, T10
+
+    def observables_async(self, eps, u4, pi10, T10) -> None:
+        """Start copying the observables into the given float64 arrays (shapes
+        of :meth:`observables`; page-locked for overlap) and return at once;
+        they are complete after :meth:`wait_observables`."""
+        for a, size in ((eps, self.n), (u4, 4 * self.n), (pi10, 10 * self.n), (T10, 10 * self.n)):
+            if a.dtype != np.float64 or a.size != size or not a.flags.c_contiguous:
+                raise ValueError(f"observable buffer needs {size} contiguous float64")
+        self._check(self._lib.ipg_get_observables_async(self._h, _ptr(eps), _ptr(u4),
+                                                        _ptr(pi10), _ptr(T10)))
+
+    def wait_observables(self) -> None:
+        self._check(self._lib.ipg_wait_observables(self._h))
 
     def write_outputs(self, hydro=None, tmunu=None, size_output=None, L_output=None,
                       eta_size=1, deta=0.0, gfactor=1.0):

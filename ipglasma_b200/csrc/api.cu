@@ -40,6 +40,11 @@ struct ipg_ctx {
     // the other of two work buffers (work, work2)
     cudaStream_t stream_v = nullptr;
     cudaEvent_t ev_fft[2] = {nullptr, nullptr}, ev_prod[2] = {nullptr, nullptr};
+    // ipg_get_observables_async: the copies run on stream_copy after
+    // ev_obs_ready; the next observables stage waits for ev_obs_copied
+    cudaStream_t stream_copy = nullptr;
+    cudaEvent_t ev_obs_ready = nullptr, ev_obs_copied = nullptr;
+    bool obs_copy_pending = false;
     std::string err;
     long long launches = 0;
 
@@ -409,6 +414,9 @@ ipg_status observables_enqueue(ipg_ctx *c) {
     const double dtau = c->dtau;
     const size_t n = c->n;
     const int N = c->N;
+    // the observable arrays are rewritten below: an asynchronous copy of the
+    // previous event's must have read them first
+    if (c->obs_copy_pending) IPG_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_obs_copied, 0));
     IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     IPG_TRY(state64(c));
     TmunuArgs ta;
@@ -542,6 +550,9 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
     IPG_CUDA(c, cudaSetDevice(cfg->device));
     IPG_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     IPG_CUDA(c, cudaStreamCreateWithFlags(&c->stream_v, cudaStreamNonBlocking));
+    IPG_CUDA(c, cudaStreamCreateWithFlags(&c->stream_copy, cudaStreamNonBlocking));
+    IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_obs_ready, cudaEventDisableTiming));
+    IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_obs_copied, cudaEventDisableTiming));
     for (int i = 0; i < 2; i++) {
         IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_fft[i], cudaEventDisableTiming));
         IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_prod[i], cudaEventDisableTiming));
@@ -631,6 +642,12 @@ ipg_status ipg_destroy(ipg_ctx *ctx) {
         if (x) cudaEventDestroy(x);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream_copy) {
+        cudaStreamSynchronize(ctx->stream_copy);
+        cudaStreamDestroy(ctx->stream_copy);
+    }
+    if (ctx->ev_obs_ready) cudaEventDestroy(ctx->ev_obs_ready);
+    if (ctx->ev_obs_copied) cudaEventDestroy(ctx->ev_obs_copied);
     if (ctx->stream_v) {
         cudaStreamSynchronize(ctx->stream_v);
         cudaStreamDestroy(ctx->stream_v);
@@ -949,6 +966,30 @@ ipg_status ipg_get_observables(ipg_ctx *c, double *eps, double *u4,
     if (pi10) IPG_CUDA(c, cudaMemcpyAsync(pi10, c->pi10, sizeof(double) * 10 * n, d2h, c->stream));
     if (T10) IPG_CUDA(c, cudaMemcpyAsync(T10, c->T10, sizeof(double) * 10 * n, d2h, c->stream));
     IPG_TRY(sync(c));
+    return IPG_OK;
+}
+
+ipg_status ipg_get_observables_async(ipg_ctx *c, double *eps, double *u4, double *pi10,
+                                     double *T10) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (!c->finished) return fail(c, IPG_ERR_STATE, "call ipg_run first");
+    const size_t n = c->n;
+    const auto d2h = cudaMemcpyDeviceToHost;
+    cudaStream_t s = c->stream_copy;
+    IPG_CUDA(c, cudaEventRecord(c->ev_obs_ready, c->stream));
+    IPG_CUDA(c, cudaStreamWaitEvent(s, c->ev_obs_ready, 0));
+    if (eps) IPG_CUDA(c, cudaMemcpyAsync(eps, c->eps, sizeof(double) * n, d2h, s));
+    if (u4) IPG_CUDA(c, cudaMemcpyAsync(u4, c->u4, sizeof(double) * 4 * n, d2h, s));
+    if (pi10) IPG_CUDA(c, cudaMemcpyAsync(pi10, c->pi10, sizeof(double) * 10 * n, d2h, s));
+    if (T10) IPG_CUDA(c, cudaMemcpyAsync(T10, c->T10, sizeof(double) * 10 * n, d2h, s));
+    IPG_CUDA(c, cudaEventRecord(c->ev_obs_copied, s));
+    c->obs_copy_pending = true;
+    return IPG_OK;
+}
+
+ipg_status ipg_wait_observables(ipg_ctx *c) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (c->obs_copy_pending) IPG_CUDA(c, cudaEventSynchronize(c->ev_obs_copied));
     return IPG_OK;
 }
 
