@@ -9,7 +9,8 @@
 // B_bar += A^dag C_bar. Hermitian fields (phi, pi) and traceless Hermitian
 // ones (E1, E2) keep full-matrix adjoint buffers; only their Hermitian
 // (traceless) part is meaningful and it is taken where an adjoint is
-// consumed. Adjoint buffers are 9 complex planes per field and site.
+// consumed. Adjoint buffers hold 18 real planes per field (real and imaginary
+// parts of the 9 entries apart; see adj_planes).
 //
 // One leapfrog step (evolve.cu, Evolution.cpp:35-293) is S = S_u o S_e:
 //   S_e: E_d' = TL(E_d + cst (AH-plaquette + AH-staple)_d + cdt i[U_d phi(+d) U_d^dag, phi])
@@ -89,12 +90,24 @@ __device__ __forceinline__ Md ld_herm8(const double *p, size_t pos, size_t n) {
     return from_h(ld_h8(p, pos, n));
 }
 
+// Adjoint buffers hold 9 complex entries a site as 18 planes of n doubles:
+// the real part of entry k in plane 2k, its imaginary part in plane 2k+1
+// (the buffer is typed as 9 complex planes and has the same size). A warp's
+// FP64 atomics on one plane then fill whole 32-byte sectors.
+__device__ __forceinline__ double *adj_planes(C<double> *buf) {
+    return reinterpret_cast<double *>(buf);
+}
+__device__ __forceinline__ const double *adj_planes(const C<double> *buf) {
+    return reinterpret_cast<const double *>(buf);
+}
+
 __device__ __forceinline__ void atomic_add_m(C<double> *buf, size_t pos, size_t n,
                                              const Md &a) {
+    double *b = adj_planes(buf);
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-        atomicAdd(&buf[k * n + pos].r, a.m[k].r);
-        atomicAdd(&buf[k * n + pos].i, a.m[k].i);
+        atomicAdd(&b[(2 * k) * n + pos], a.m[k].r);
+        atomicAdd(&b[(2 * k + 1) * n + pos], a.m[k].i);
     }
 }
 
@@ -102,31 +115,46 @@ __device__ __forceinline__ void atomic_add_m(C<double> *buf, size_t pos, size_t 
 // triangle); buffers updated this way are read back with ld_adj_h
 __device__ __forceinline__ void atomic_add_h(C<double> *buf, size_t pos, size_t n,
                                              const Md &a) {
-    atomicAdd(&buf[0 * n + pos].r, a.m[0].r);
-    atomicAdd(&buf[4 * n + pos].r, a.m[4].r);
-    atomicAdd(&buf[8 * n + pos].r, a.m[8].r);
-    atomicAdd(&buf[1 * n + pos].r, a.m[1].r);
-    atomicAdd(&buf[1 * n + pos].i, a.m[1].i);
-    atomicAdd(&buf[2 * n + pos].r, a.m[2].r);
-    atomicAdd(&buf[2 * n + pos].i, a.m[2].i);
-    atomicAdd(&buf[5 * n + pos].r, a.m[5].r);
-    atomicAdd(&buf[5 * n + pos].i, a.m[5].i);
+    double *b = adj_planes(buf);
+    atomicAdd(&b[0 * n + pos], a.m[0].r);
+    atomicAdd(&b[8 * n + pos], a.m[4].r);
+    atomicAdd(&b[16 * n + pos], a.m[8].r);
+    atomicAdd(&b[2 * n + pos], a.m[1].r);
+    atomicAdd(&b[3 * n + pos], a.m[1].i);
+    atomicAdd(&b[4 * n + pos], a.m[2].r);
+    atomicAdd(&b[5 * n + pos], a.m[2].i);
+    atomicAdd(&b[10 * n + pos], a.m[5].r);
+    atomicAdd(&b[11 * n + pos], a.m[5].i);
 }
 
 __device__ __forceinline__ Md ld_adj(const C<double> *buf, size_t pos, size_t n) {
-    return ld_m3(buf, pos, n);
+    const double *b = adj_planes(buf);
+    Md m;
+#pragma unroll
+    for (int k = 0; k < 9; k++) m.m[k] = {b[(2 * k) * n + pos], b[(2 * k + 1) * n + pos]};
+    return m;
+}
+
+__device__ __forceinline__ void st_adj(C<double> *buf, size_t pos, size_t n, const Md &m) {
+    double *b = adj_planes(buf);
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        b[(2 * k) * n + pos] = m.m[k].r;
+        b[(2 * k + 1) * n + pos] = m.m[k].i;
+    }
 }
 
 // diagonal (real parts) and upper triangle of an adjoint known to be
 // Hermitian; from_h of it rebuilds the stored matrix exactly
 __device__ __forceinline__ H3<double> ld_adj_h(const C<double> *buf, size_t pos, size_t n) {
+    const double *b = adj_planes(buf);
     H3<double> h;
-    h.d0 = buf[0 * n + pos].r;
-    h.d1 = buf[4 * n + pos].r;
-    h.d2 = buf[8 * n + pos].r;
-    h.o01 = buf[1 * n + pos];
-    h.o02 = buf[2 * n + pos];
-    h.o12 = buf[5 * n + pos];
+    h.d0 = b[0 * n + pos];
+    h.d1 = b[8 * n + pos];
+    h.d2 = b[16 * n + pos];
+    h.o01 = {b[2 * n + pos], b[3 * n + pos]};
+    h.o02 = {b[4 * n + pos], b[5 * n + pos]};
+    h.o12 = {b[10 * n + pos], b[11 * n + pos]};
     return h;
 }
 
@@ -225,8 +253,8 @@ __global__ void k_adj_su(int N, State<double> cur, State<double> nxt, AdjState a
     const Md phib = from_h(ld_adj_h(a.phi, pos, n));
     Md pib = herm(ld_adj(a.pi, pos, n));
     add_to(pib, sc(phib, c2));
-    st_m3(a.phi, pos, n, phib);
-    st_m3(a.pi, pos, n, pib);
+    st_adj(a.phi, pos, n, phib);
+    st_adj(a.pi, pos, n, pib);
     for (int d = 0; d < 2; d++) {
         C<double> *Ub = d ? a.uy : a.ux;
         C<double> *Eb = d ? a.e2 : a.e1;
@@ -234,7 +262,7 @@ __global__ void k_adj_su(int N, State<double> cur, State<double> nxt, AdjState a
         const Md U = ld_m3(d ? cur.uy : cur.ux, pos, n);
         const Md X = times_i(ld_herm8(d ? nxt.e2 : nxt.e1, pos, n), c);
         const Md M = taylor2(X);
-        st_m3(Ub, pos, n, mul_dn(M, Ubar));
+        st_adj(Ub, pos, n, mul_dn(M, Ubar));
         const Md Mb = mul_nd(Ubar, U);
         // X_bar = M_bar + (M_bar X^dag + X^dag M_bar) / 2
         Md Xb = Mb;
@@ -243,7 +271,7 @@ __global__ void k_adj_su(int N, State<double> cur, State<double> nxt, AdjState a
         // which is also the adjoint of E before S_e (E' = TL(E + ...))
         Md Eb_ = ld_adj(Eb, pos, n);
         add_to(Eb_, herm(times_i(Xb, -c)));
-        st_m3(Eb, pos, n, tl(herm(Eb_)));
+        st_adj(Eb, pos, n, tl(herm(Eb_)));
     }
 }
 
@@ -264,8 +292,8 @@ __global__ void k_inv_adj_su(int N, State<double> nxt, State<double> cur, AdjSta
     const Md phib = from_h(ld_adj_h(a.phi, pos, n));
     Md pib = herm(ld_adj(a.pi, pos, n));
     add_to(pib, sc(phib, c2));
-    st_m3(a.phi, pos, n, phib);
-    st_m3(a.pi, pos, n, pib);
+    st_adj(a.phi, pos, n, phib);
+    st_adj(a.pi, pos, n, pib);
     for (int d = 0; d < 2; d++) {
         C<double> *Ub = d ? a.uy : a.ux;
         C<double> *Eb = d ? a.e2 : a.e1;
@@ -274,13 +302,13 @@ __global__ void k_inv_adj_su(int N, State<double> nxt, State<double> cur, AdjSta
         const Md U = mul(inverse3(M), ld_m3(d ? nxt.uy : nxt.ux, pos, n));
         st_m3(d ? cur.uy : cur.ux, pos, n, U);
         const Md Ubar = ld_adj(Ub, pos, n);
-        st_m3(Ub, pos, n, mul_dn(M, Ubar));
+        st_adj(Ub, pos, n, mul_dn(M, Ubar));
         const Md Mb = mul_nd(Ubar, U);
         Md Xb = Mb;
         add_to(Xb, sc(addm(mul_nd(Mb, X), mul_dn(X, Mb)), 0.5));
         Md Eb_ = ld_adj(Eb, pos, n);
         add_to(Eb_, herm(times_i(Xb, -c)));
-        st_m3(Eb, pos, n, tl(herm(Eb_)));
+        st_adj(Eb, pos, n, tl(herm(Eb_)));
     }
 }
 
@@ -467,10 +495,10 @@ __global__ void k_adj_ttt(int N, State<double> s, const double *tbar, AdjState a
 __global__ void k_adj_project(size_t n, AdjState a) {
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
-    st_m3(a.e1, pos, n, tl(herm(ld_adj(a.e1, pos, n))));
-    st_m3(a.e2, pos, n, tl(herm(ld_adj(a.e2, pos, n))));
-    st_m3(a.phi, pos, n, from_h(ld_adj_h(a.phi, pos, n)));
-    st_m3(a.pi, pos, n, herm(ld_adj(a.pi, pos, n)));
+    st_adj(a.e1, pos, n, tl(herm(ld_adj(a.e1, pos, n))));
+    st_adj(a.e2, pos, n, tl(herm(ld_adj(a.e2, pos, n))));
+    st_adj(a.phi, pos, n, from_h(ld_adj_h(a.phi, pos, n)));
+    st_adj(a.pi, pos, n, herm(ld_adj(a.pi, pos, n)));
 }
 
 // ---------------------------------------------------------------------------
@@ -802,11 +830,11 @@ __global__ void __launch_bounds__(128) k_adj_wilson_sheet(int N, double2 *work, 
         q[2 * c + 1] = -v.y;
     }
     const Md e = exp_from_coeff(q);
-    const Md Vk = ld_m3(V, pos, n), Vbk = ld_m3(Vb, pos, n);
+    const Md Vk = ld_m3(V, pos, n), Vbk = ld_adj(Vb, pos, n);
     const Md Vprev = mul_dn(e, Vk);
     const Md eb = mul_nd(Vbk, Vprev);
     st_m3(V, pos, n, Vprev);
-    st_m3(Vb, pos, n, mul_dn(e, Vbk));
+    st_adj(Vb, pos, n, mul_dn(e, Vbk));
     double qb[8];
     if (!exp_vjp(q, eb, qb))
         for (int b = 0; b < 8; b++) qb[b] = re_dot(eb, dexp(q, b, kDexpStep));
@@ -902,11 +930,11 @@ void launch_adjoint_project(size_t n, const AdjState &a, cudaStream_t st) {
 __global__ void k_planes_to_sites(size_t n, const C<double> *src, double *dst) {
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
+    const Md m = ld_adj(src, pos, n);
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-        const C<double> v = src[k * n + pos];
-        dst[18 * pos + 2 * k] = v.r;
-        dst[18 * pos + 2 * k + 1] = v.i;
+        dst[18 * pos + 2 * k] = m.m[k].r;
+        dst[18 * pos + 2 * k + 1] = m.m[k].i;
     }
 }
 

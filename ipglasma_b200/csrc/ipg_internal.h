@@ -169,7 +169,8 @@ void launch_tmunu(const TmunuArgs &a, cudaStream_t st);
 void launch_tmunu_diag(const TmunuArgs &a, cudaStream_t st);
 
 // ---- adjoint ---------------------------------------------------------------
-// Adjoint buffers of the six fields, 9 complex planes each.
+// Adjoint buffers of the six fields, each sized as 9 complex planes and
+// holding 18 real planes (entry k: real part in plane 2k, imaginary in 2k+1).
 struct AdjState {
     C<double> *ux, *uy, *e1, *e2, *phi, *pi;
 };
@@ -192,7 +193,7 @@ void launch_adjoint_step(int N, const State<double> &cur, const State<double> &n
 void launch_adjoint_ttt(int N, const State<double> &s, const double *tbar, const AdjState &a,
                         double g, double tau, cudaStream_t st);
 void launch_adjoint_project(size_t n, const AdjState &a, cudaStream_t st);
-// [9 complex planes][n] -> [n][18] doubles
+// adjoint buffer (18 real planes) -> [n][18] doubles, (re, im) per entry
 void launch_planes_to_sites(size_t n, const C<double> *src, double *dst, cudaStream_t st);
 // adjoint of the tau = 0 links and pi: pi_bar, U_bar(tau=0) (in adj) ->
 // U1/U2 adjoints b* (initial-pi stencil, then the Newton solve) -> V_A, V_B
