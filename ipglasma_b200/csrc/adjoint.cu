@@ -49,19 +49,6 @@ __device__ __forceinline__ Md herm(const Md &a) {
     return r;
 }
 
-__device__ __forceinline__ Md tl(const Md &a) {
-    Md r = a;
-    const double t = (a.m[0].r + a.m[4].r + a.m[8].r) / 3.;
-    const double ti = (a.m[0].i + a.m[4].i + a.m[8].i) / 3.;
-    r.m[0].r -= t;
-    r.m[4].r -= t;
-    r.m[8].r -= t;
-    r.m[0].i -= ti;
-    r.m[4].i -= ti;
-    r.m[8].i -= ti;
-    return r;
-}
-
 // s * i * a
 __device__ __forceinline__ Md times_i(const Md &a, double s) {
     Md r;
@@ -111,22 +98,6 @@ __device__ __forceinline__ void atomic_add_m(C<double> *buf, size_t pos, size_t 
     }
 }
 
-// the 9 real components of a Hermitian adjoint (diagonal real parts, upper
-// triangle); buffers updated this way are read back with ld_adj_h
-__device__ __forceinline__ void atomic_add_h(C<double> *buf, size_t pos, size_t n,
-                                             const Md &a) {
-    double *b = adj_planes(buf);
-    atomicAdd(&b[0 * n + pos], a.m[0].r);
-    atomicAdd(&b[8 * n + pos], a.m[4].r);
-    atomicAdd(&b[16 * n + pos], a.m[8].r);
-    atomicAdd(&b[2 * n + pos], a.m[1].r);
-    atomicAdd(&b[3 * n + pos], a.m[1].i);
-    atomicAdd(&b[4 * n + pos], a.m[2].r);
-    atomicAdd(&b[5 * n + pos], a.m[2].i);
-    atomicAdd(&b[10 * n + pos], a.m[5].r);
-    atomicAdd(&b[11 * n + pos], a.m[5].i);
-}
-
 __device__ __forceinline__ Md ld_adj(const C<double> *buf, size_t pos, size_t n) {
     const double *b = adj_planes(buf);
     Md m;
@@ -144,18 +115,101 @@ __device__ __forceinline__ void st_adj(C<double> *buf, size_t pos, size_t n, con
     }
 }
 
-// diagonal (real parts) and upper triangle of an adjoint known to be
-// Hermitian; from_h of it rebuilds the stored matrix exactly
-__device__ __forceinline__ H3<double> ld_adj_h(const C<double> *buf, size_t pos, size_t n) {
+// During the reverse sweep the adjoints of the Hermitian fields keep only
+// their Hermitian part, the part the loss sees: phi and pi as 9 planes (d0 d1
+// d2, re/im of the 01, 02, 12 entries), E1 and E2 as their traceless part in
+// 8 planes (d0 d1 and the off-diagonals; d2 = -d0 - d1). A contribution M is
+// added as its (traceless) Hermitian part. k_adj_project expands them to full
+// matrices (split planes) at the end of the sweep.
+__device__ __forceinline__ H3<double> ld_h9a(const C<double> *buf, size_t pos, size_t n) {
     const double *b = adj_planes(buf);
     H3<double> h;
-    h.d0 = b[0 * n + pos];
-    h.d1 = b[8 * n + pos];
-    h.d2 = b[16 * n + pos];
+    h.d0 = b[pos];
+    h.d1 = b[n + pos];
+    h.d2 = b[2 * n + pos];
+    h.o01 = {b[3 * n + pos], b[4 * n + pos]};
+    h.o02 = {b[5 * n + pos], b[6 * n + pos]};
+    h.o12 = {b[7 * n + pos], b[8 * n + pos]};
+    return h;
+}
+
+__device__ __forceinline__ void st_h9a(C<double> *buf, size_t pos, size_t n, const H3<double> &h) {
+    double *b = adj_planes(buf);
+    b[pos] = h.d0;
+    b[n + pos] = h.d1;
+    b[2 * n + pos] = h.d2;
+    b[3 * n + pos] = h.o01.r;
+    b[4 * n + pos] = h.o01.i;
+    b[5 * n + pos] = h.o02.r;
+    b[6 * n + pos] = h.o02.i;
+    b[7 * n + pos] = h.o12.r;
+    b[8 * n + pos] = h.o12.i;
+}
+
+__device__ __forceinline__ H3<double> ld_h8a(const C<double> *buf, size_t pos, size_t n) {
+    const double *b = adj_planes(buf);
+    H3<double> h;
+    h.d0 = b[pos];
+    h.d1 = b[n + pos];
+    h.d2 = -(h.d0 + h.d1);
     h.o01 = {b[2 * n + pos], b[3 * n + pos]};
     h.o02 = {b[4 * n + pos], b[5 * n + pos]};
-    h.o12 = {b[10 * n + pos], b[11 * n + pos]};
+    h.o12 = {b[6 * n + pos], b[7 * n + pos]};
     return h;
+}
+
+__device__ __forceinline__ void st_h8a(C<double> *buf, size_t pos, size_t n, const H3<double> &h) {
+    double *b = adj_planes(buf);
+    b[pos] = h.d0;
+    b[n + pos] = h.d1;
+    b[2 * n + pos] = h.o01.r;
+    b[3 * n + pos] = h.o01.i;
+    b[4 * n + pos] = h.o02.r;
+    b[5 * n + pos] = h.o02.i;
+    b[6 * n + pos] = h.o12.r;
+    b[7 * n + pos] = h.o12.i;
+}
+
+// Hermitian part (M + M^dag) / 2
+__device__ __forceinline__ H3<double> herm_part(const Md &m) {
+    H3<double> h;
+    h.d0 = m.m[0].r;
+    h.d1 = m.m[4].r;
+    h.d2 = m.m[8].r;
+    h.o01 = {0.5 * (m.m[1].r + m.m[3].r), 0.5 * (m.m[1].i - m.m[3].i)};
+    h.o02 = {0.5 * (m.m[2].r + m.m[6].r), 0.5 * (m.m[2].i - m.m[6].i)};
+    h.o12 = {0.5 * (m.m[5].r + m.m[7].r), 0.5 * (m.m[5].i - m.m[7].i)};
+    return h;
+}
+
+__device__ __forceinline__ void atomic_add_h9a(C<double> *buf, size_t pos, size_t n,
+                                               const Md &m) {
+    const H3<double> h = herm_part(m);
+    double *b = adj_planes(buf);
+    atomicAdd(&b[pos], h.d0);
+    atomicAdd(&b[n + pos], h.d1);
+    atomicAdd(&b[2 * n + pos], h.d2);
+    atomicAdd(&b[3 * n + pos], h.o01.r);
+    atomicAdd(&b[4 * n + pos], h.o01.i);
+    atomicAdd(&b[5 * n + pos], h.o02.r);
+    atomicAdd(&b[6 * n + pos], h.o02.i);
+    atomicAdd(&b[7 * n + pos], h.o12.r);
+    atomicAdd(&b[8 * n + pos], h.o12.i);
+}
+
+__device__ __forceinline__ void atomic_add_h8a(C<double> *buf, size_t pos, size_t n,
+                                               const Md &m) {
+    const H3<double> h = herm_part(m);
+    const double t = (h.d0 + h.d1 + h.d2) / 3.;
+    double *b = adj_planes(buf);
+    atomicAdd(&b[pos], h.d0 - t);
+    atomicAdd(&b[n + pos], h.d1 - t);
+    atomicAdd(&b[2 * n + pos], h.o01.r);
+    atomicAdd(&b[3 * n + pos], h.o01.i);
+    atomicAdd(&b[4 * n + pos], h.o02.r);
+    atomicAdd(&b[5 * n + pos], h.o02.i);
+    atomicAdd(&b[6 * n + pos], h.o12.r);
+    atomicAdd(&b[7 * n + pos], h.o12.i);
 }
 
 // T2(X) = 1 + X + X^2 / 2
@@ -250,11 +304,12 @@ __global__ void k_adj_su(int N, State<double> cur, State<double> nxt, AdjState a
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
-    const Md phib = from_h(ld_adj_h(a.phi, pos, n));
-    Md pib = herm(ld_adj(a.pi, pos, n));
-    add_to(pib, sc(phib, c2));
-    st_adj(a.phi, pos, n, phib);
-    st_adj(a.pi, pos, n, pib);
+    // pi_bar += c2 phi_bar (phi_bar itself passes through unchanged)
+    {
+        H3<double> pib = ld_h9a(a.pi, pos, n);
+        h_axpy(pib, c2, ld_h9a(a.phi, pos, n));
+        st_h9a(a.pi, pos, n, pib);
+    }
     for (int d = 0; d < 2; d++) {
         C<double> *Ub = d ? a.uy : a.ux;
         C<double> *Eb = d ? a.e2 : a.e1;
@@ -269,9 +324,10 @@ __global__ void k_adj_su(int N, State<double> cur, State<double> nxt, AdjState a
         add_to(Xb, sc(addm(mul_nd(Mb, X), mul_dn(X, Mb)), 0.5));
         // X = i c E  ->  E_bar += Herm(-i c X_bar); stored traceless Hermitian,
         // which is also the adjoint of E before S_e (E' = TL(E + ...))
-        Md Eb_ = ld_adj(Eb, pos, n);
-        add_to(Eb_, herm(times_i(Xb, -c)));
-        st_adj(Eb, pos, n, tl(herm(Eb_)));
+        H3<double> Eb_ = herm_part(times_i(Xb, -c));
+        h_traceless(Eb_);
+        h_add(Eb_, ld_h8a(Eb, pos, n));
+        st_h8a(Eb, pos, n, Eb_);
     }
 }
 
@@ -289,11 +345,12 @@ __global__ void k_inv_adj_su(int N, State<double> nxt, State<double> cur, AdjSta
         h_axpy(phi, -c2, ld_h(nxt.pi, pos, n));
         st_h(cur.phi, pos, n, phi);
     }
-    const Md phib = from_h(ld_adj_h(a.phi, pos, n));
-    Md pib = herm(ld_adj(a.pi, pos, n));
-    add_to(pib, sc(phib, c2));
-    st_adj(a.phi, pos, n, phib);
-    st_adj(a.pi, pos, n, pib);
+    // pi_bar += c2 phi_bar (phi_bar itself passes through unchanged)
+    {
+        H3<double> pib = ld_h9a(a.pi, pos, n);
+        h_axpy(pib, c2, ld_h9a(a.phi, pos, n));
+        st_h9a(a.pi, pos, n, pib);
+    }
     for (int d = 0; d < 2; d++) {
         C<double> *Ub = d ? a.uy : a.ux;
         C<double> *Eb = d ? a.e2 : a.e1;
@@ -306,9 +363,10 @@ __global__ void k_inv_adj_su(int N, State<double> nxt, State<double> cur, AdjSta
         const Md Mb = mul_nd(Ubar, U);
         Md Xb = Mb;
         add_to(Xb, sc(addm(mul_nd(Mb, X), mul_dn(X, Mb)), 0.5));
-        Md Eb_ = ld_adj(Eb, pos, n);
-        add_to(Eb_, herm(times_i(Xb, -c)));
-        st_adj(Eb, pos, n, tl(herm(Eb_)));
+        H3<double> Eb_ = herm_part(times_i(Xb, -c));
+        h_traceless(Eb_);
+        h_add(Eb_, ld_h8a(Eb, pos, n));
+        st_h8a(Eb, pos, n, Eb_);
     }
 }
 
@@ -341,13 +399,13 @@ __global__ void __launch_bounds__(128) k_adj_se(int N, State<double> cur, AdjSta
     const StepGeom G = step_geom(N, (int)(pos / N), (int)(pos % N));
     const int role = blockIdx.y;
     if (role == 0) {
-        const H3<double> h1 = ld_adj_h(a.e1, pos, n);
+        const H3<double> h1 = ld_h8a(a.e1, pos, n);
         const Md ux = ld_m3(cur.ux, pos, n);
         Md acc;
         {
             const Md uy_px = ld_m3(cur.uy, G.pX, n);
             const Md B = mul(ld_m3(cur.uy, pos, n), ld_m3(cur.ux, G.pY, n));
-            const Md Mb = times_i(minus(sc(from_h(h1), cst), sc(from_h(ld_adj_h(a.e2, pos, n)), cst)), -2.);
+            const Md Mb = times_i(minus(sc(from_h(h1), cst), sc(from_h(ld_h8a(a.e2, pos, n)), cst)), -2.);
             const Md Ab = mul(Mb, B);
             acc = mul_nd(Ab, uy_px);
             atomic_add_m(a.uy, G.pX, n, mul_dn(ux, Ab));
@@ -361,19 +419,19 @@ __global__ void __launch_bounds__(128) k_adj_se(int N, State<double> cur, AdjSta
         }
         {
             Md phb = icomm(ld_herm(cur.phi, pos, n), sc(from_h(h1), cdt));
-            add_to(phb, sc(ld_adj(a.pi, pos, n), cdt));
+            add_to(phb, sc(from_h(ld_h9a(a.pi, pos, n)), cdt));
             add_to(acc, sc(mul(mul(phb, ux), ld_herm(cur.phi, G.pX, n)), 2.));
             atomic_add_m(a.ux, pos, n, acc);
-            atomic_add_h(a.phi, G.pX, n, mul(mul_dn(ux, phb), ux));
+            atomic_add_h9a(a.phi, G.pX, n, mul(mul_dn(ux, phb), ux));
         }
     } else if (role == 1) {
-        const H3<double> h2 = ld_adj_h(a.e2, pos, n);
+        const H3<double> h2 = ld_h8a(a.e2, pos, n);
         const Md uy = ld_m3(cur.uy, pos, n);
         Md acc;
         {
             const Md ux_py = ld_m3(cur.ux, G.pY, n);
             const Md A = mul(ld_m3(cur.ux, pos, n), ld_m3(cur.uy, G.pX, n));
-            const Md Mb = times_i(minus(sc(from_h(ld_adj_h(a.e1, pos, n)), cst), sc(from_h(h2), cst)), -2.);
+            const Md Mb = times_i(minus(sc(from_h(ld_h8a(a.e1, pos, n)), cst), sc(from_h(h2), cst)), -2.);
             const Md Bb = mul_dn(Mb, A);
             acc = mul_nd(Bb, ux_py);
             atomic_add_m(a.ux, G.pY, n, mul_dn(uy, Bb));
@@ -387,47 +445,47 @@ __global__ void __launch_bounds__(128) k_adj_se(int N, State<double> cur, AdjSta
         }
         {
             Md phb = icomm(ld_herm(cur.phi, pos, n), sc(from_h(h2), cdt));
-            add_to(phb, sc(ld_adj(a.pi, pos, n), cdt));
+            add_to(phb, sc(from_h(ld_h9a(a.pi, pos, n)), cdt));
             add_to(acc, sc(mul(mul(phb, uy), ld_herm(cur.phi, G.pY, n)), 2.));
             atomic_add_m(a.uy, pos, n, acc);
-            atomic_add_h(a.phi, G.pY, n, mul(mul_dn(uy, phb), uy));
+            atomic_add_h9a(a.phi, G.pY, n, mul(mul_dn(uy, phb), uy));
         }
         {
             // phi += -4 brb + i[Cb_1, ph_x] + i[Cb_2, ph_y]
             Md phib = icomm(sc(from_h(h2), cdt), mul_nd(mul(uy, ld_herm(cur.phi, G.pY, n)), uy));
             const Md ux = ld_m3(cur.ux, pos, n);
-            add_to(phib, icomm(sc(from_h(ld_adj_h(a.e1, pos, n)), cdt),
+            add_to(phib, icomm(sc(from_h(ld_h8a(a.e1, pos, n)), cdt),
                                mul_nd(mul(ux, ld_herm(cur.phi, G.pX, n)), ux)));
-            add_to(phib, sc(ld_adj(a.pi, pos, n), -4. * cdt));
-            atomic_add_h(a.phi, pos, n, phib);
+            add_to(phib, sc(from_h(ld_h9a(a.pi, pos, n)), -4. * cdt));
+            atomic_add_h9a(a.phi, pos, n, phib);
         }
     } else {
-        const Md brb = sc(ld_adj(a.pi, pos, n), cdt);
+        const Md brb = sc(from_h(ld_h9a(a.pi, pos, n)), cdt);
         {
             // E2 staple's Q side and the -x transport
             const Md uy = ld_m3(cur.uy, pos, n), ux_mxpy = ld_m3(cur.ux, G.mXpY, n);
             const Md P = mul_nd(uy, ux_mxpy);
-            const Md Qb = mul_dn(P, times_i(sc(from_h(ld_adj_h(a.e2, pos, n)), cst), -2.));
+            const Md Qb = mul_dn(P, times_i(sc(from_h(ld_h8a(a.e2, pos, n)), cst), -2.));
             const Md ux_mx = ld_m3(cur.ux, G.mX, n), uy_mx = ld_m3(cur.uy, G.mX, n);
             const Md f = ld_herm(cur.phi, G.mX, n);
             atomic_add_m(a.uy, G.mX, n, mul_nd(ux_mx, Qb));
             Md acc = mul(uy_mx, Qb);
             add_to(acc, sc(mul(mul(f, ux_mx), brb), 2.));
             atomic_add_m(a.ux, G.mX, n, acc);
-            atomic_add_h(a.phi, G.mX, n, mul_nd(mul(ux_mx, brb), ux_mx));
+            atomic_add_h9a(a.phi, G.mX, n, mul_nd(mul(ux_mx, brb), ux_mx));
         }
         {
             // E1 staple's Q side and the -y transport
             const Md ux = ld_m3(cur.ux, pos, n), uy_pxmy = ld_m3(cur.uy, G.pXmY, n);
             const Md P = mul_nd(ux, uy_pxmy);
-            const Md Qb = mul_dn(P, times_i(sc(from_h(ld_adj_h(a.e1, pos, n)), cst), -2.));
+            const Md Qb = mul_dn(P, times_i(sc(from_h(ld_h8a(a.e1, pos, n)), cst), -2.));
             const Md ux_my = ld_m3(cur.ux, G.mY, n), uy_my = ld_m3(cur.uy, G.mY, n);
             const Md f = ld_herm(cur.phi, G.mY, n);
             atomic_add_m(a.ux, G.mY, n, mul_nd(uy_my, Qb));
             Md acc = mul(ux_my, Qb);
             add_to(acc, sc(mul(mul(f, uy_my), brb), 2.));
             atomic_add_m(a.uy, G.mY, n, acc);
-            atomic_add_h(a.phi, G.mY, n, mul_nd(mul(uy_my, brb), uy_my));
+            atomic_add_h9a(a.phi, G.mY, n, mul_nd(mul(uy_my, brb), uy_my));
         }
     }
 }
@@ -446,14 +504,14 @@ __global__ void k_adj_ttt(int N, State<double> s, const double *tbar, AdjState a
     const size_t pXY = at(N, min(N - 1, i + 1), min(N - 1, j + 1));
     const double ge = g * g / tau / tau, ht = 0.5 / tau / tau;
     // electric: ge/2 (|E1|^2 + |E1(+y)|^2 + |E2|^2 + |E2(+x)|^2)
-    atomic_add_m(a.e1, pos, n, sc(ld_herm8(s.e1, pos, n), tb * ge));
-    atomic_add_m(a.e1, pY, n, sc(ld_herm8(s.e1, pY, n), tb * ge));
-    atomic_add_m(a.e2, pos, n, sc(ld_herm8(s.e2, pos, n), tb * ge));
-    atomic_add_m(a.e2, pX, n, sc(ld_herm8(s.e2, pX, n), tb * ge));
+    atomic_add_h8a(a.e1, pos, n, sc(ld_herm8(s.e1, pos, n), tb * ge));
+    atomic_add_h8a(a.e1, pY, n, sc(ld_herm8(s.e1, pY, n), tb * ge));
+    atomic_add_h8a(a.e2, pos, n, sc(ld_herm8(s.e2, pos, n), tb * ge));
+    atomic_add_h8a(a.e2, pX, n, sc(ld_herm8(s.e2, pX, n), tb * ge));
     // longitudinal electric: tr pi^2 / 4 over four cells
     const size_t cells[4] = {pos, pX, pY, pXY};
     for (int k = 0; k < 4; k++)
-        atomic_add_m(a.pi, cells[k], n, sc(ld_herm(s.pi, cells[k], n), 0.5 * tb));
+        atomic_add_h9a(a.pi, cells[k], n, sc(ld_herm(s.pi, cells[k], n), 0.5 * tb));
     const Md ux = ld_m3(s.ux, pos, n), uy = ld_m3(s.uy, pos, n);
     // magnetic: 2/g^2 (3 - Re tr(Ux Uy(+x) Ux(+y)^dag Uy^dag)), zero on the last row
     if (i != N - 1) {
@@ -484,10 +542,10 @@ __global__ void k_adj_ttt(int N, State<double> s, const double *tbar, AdjState a
         const Md C = mul_nd(mul(u, fb), u);
         const Md d = minus(ld_herm(s.phi, T.pa, n), C);
         const Md db = sc(d, 2. * ht * tb);
-        atomic_add_m(a.phi, T.pa, n, db);
+        atomic_add_h9a(a.phi, T.pa, n, db);
         const Md Cb = sc(db, -1.);
         atomic_add_m(T.ub, T.pu, n, sc(mul(mul(Cb, u), fb), 2.));
-        atomic_add_m(a.phi, T.pb, n, mul(mul_dn(u, Cb), u));
+        atomic_add_h9a(a.phi, T.pb, n, mul(mul_dn(u, Cb), u));
     }
 }
 
@@ -495,10 +553,14 @@ __global__ void k_adj_ttt(int N, State<double> s, const double *tbar, AdjState a
 __global__ void k_adj_project(size_t n, AdjState a) {
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
-    st_adj(a.e1, pos, n, tl(herm(ld_adj(a.e1, pos, n))));
-    st_adj(a.e2, pos, n, tl(herm(ld_adj(a.e2, pos, n))));
-    st_adj(a.phi, pos, n, from_h(ld_adj_h(a.phi, pos, n)));
-    st_adj(a.pi, pos, n, herm(ld_adj(a.pi, pos, n)));
+    // the sweep's Hermitian storage expanded to full matrices in place (each
+    // thread reads its site's planes before it writes them)
+    const H3<double> e1 = ld_h8a(a.e1, pos, n), e2 = ld_h8a(a.e2, pos, n);
+    const H3<double> phi = ld_h9a(a.phi, pos, n), pi = ld_h9a(a.pi, pos, n);
+    st_adj(a.e1, pos, n, from_h(e1));
+    st_adj(a.e2, pos, n, from_h(e2));
+    st_adj(a.phi, pos, n, from_h(phi));
+    st_adj(a.pi, pos, n, from_h(pi));
 }
 
 // ---------------------------------------------------------------------------
