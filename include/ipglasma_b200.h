@@ -155,6 +155,15 @@ ipg_status ipg_set_noise_device(ipg_ctx *ctx, const double *d_xiA,
  * reading it; replaces the serial Random::Gauss stream (Random.cpp:178-204). */
 ipg_status ipg_use_device_noise(ipg_ctx *ctx);
 
+/* The unit normals ipg_use_device_noise draws for nucleus (0 = A, 1 = B),
+ * sheets [sheet_first, sheet_first + sheet_count), under the context's
+ * current key, written to the host array xi[sheet_count][N*N][8] in the
+ * layout of ipg_set_noise. Feeding them back through ipg_set_noise gives the
+ * same Wilson lines as the device draw; for statistical checks of the
+ * generator that replaces Random::Gauss (Random.cpp:178-204). */
+ipg_status ipg_draw_device_noise(ipg_ctx *ctx, int nucleus, int sheet_first, int sheet_count,
+                                 double *xi);
+
 /* Wilson lines, tau=0 Newton link solve and initial fields; replaces
  * Init::setV (Init.cpp:1678-1849) and the tau=0 block of Init::init
  * (Init.cpp:2437-2691). report may be NULL. Returns

@@ -104,6 +104,8 @@ _SIGNATURES = {
     "ipg_get_g2mu": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "ipg_set_noise_device": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "ipg_use_device_noise": (ct.c_int, [ct.c_void_p]),
+    "ipg_draw_device_noise": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int,
+                                         ct.c_void_p]),
     "ipg_init_fields": (ct.c_int, [ct.c_void_p, ct.POINTER(_InitReport)]),
     "ipg_run": (ct.c_int, [ct.c_void_p, ct.POINTER(_Result)]),
     "ipg_evolve": (ct.c_int, [ct.c_void_p, ct.c_int]),
@@ -256,8 +258,11 @@ class Event:
 
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
+            # ipg_destroy waits for the context's streams, the copy stream of
+            # observables_async included, before the arrays are let go
             self._lib.ipg_destroy(self._h)
             self._h = ct.c_void_p()
+        self._pending_obs = None
 
     def __enter__(self):
         return self
@@ -310,6 +315,15 @@ class Event:
     def use_device_noise(self) -> None:
         self._check(self._lib.ipg_use_device_noise(self._h))
 
+    def draw_device_noise(self, nucleus: int, sheet_first: int = 0, sheet_count=None):
+        """The unit normals the device draw uses for one nucleus (0 = A,
+        1 = B): (sheets, N*N, 8) float64, the layout of :meth:`set_noise`."""
+        cnt = self.cfg.Ny - sheet_first if sheet_count is None else sheet_count
+        out = np.empty((cnt, self.n, 8))
+        self._check(self._lib.ipg_draw_device_noise(self._h, nucleus, sheet_first, cnt,
+                                                    _ptr(out)))
+        return out
+
     # -- stages ---------------------------------------------------------------
     def init_fields(self, allow_nonconverged: bool = False) -> InitReport:
         rep = _InitReport()
@@ -339,18 +353,25 @@ class Event:
                                                   _ptr(pi10), _ptr(T10)))
         return eps, u4, pi10, T10
 
-    def observables_async(self, eps, u4, pi10, T10) -> None:
+    def observables_async(self, eps=None, u4=None, pi10=None, T10=None) -> None:
         """Start copying the observables into the given float64 arrays (shapes
-        of :meth:`observables`; page-locked for overlap) and return at once;
-        they are complete after :meth:`wait_observables`."""
-        for a, size in ((eps, self.n), (u4, 4 * self.n), (pi10, 10 * self.n), (T10, 10 * self.n)):
+        of :meth:`observables`; page-locked for overlap; None skips that
+        copy) and return at once; they are complete after
+        :meth:`wait_observables`. The event keeps the arrays alive until
+        then, so the copy never writes into freed host memory."""
+        bufs = (eps, u4, pi10, T10)
+        for a, size in zip(bufs, (self.n, 4 * self.n, 10 * self.n, 10 * self.n)):
+            if a is None:
+                continue
             if a.dtype != np.float64 or a.size != size or not a.flags.c_contiguous:
                 raise ValueError(f"observable buffer needs {size} contiguous float64")
-        self._check(self._lib.ipg_get_observables_async(self._h, _ptr(eps), _ptr(u4),
-                                                        _ptr(pi10), _ptr(T10)))
+        self._check(self._lib.ipg_get_observables_async(
+            self._h, *(_ptr(a) if a is not None else None for a in bufs)))
+        self._pending_obs = bufs
 
     def wait_observables(self) -> None:
         self._check(self._lib.ipg_wait_observables(self._h))
+        self._pending_obs = None
 
     def write_outputs(self, hydro=None, tmunu=None, size_output=None, L_output=None,
                       eta_size=1, deta=0.0, gfactor=1.0):

@@ -409,14 +409,21 @@ ipg_status run_evolution(ipg_ctx *c) {
 // the last half step of pi and E (426-431), the Gauss law (633-635) and the
 // checks, all enqueued on the context's stream; the scalars are copied to
 // pinned host memory. observables_finish waits and fills the result.
+// Every path that rewrites the observable arrays (eps, u4, pi10, T10) calls
+// this first: an asynchronous copy of the previous contents
+// (ipg_get_observables_async) must have read them before the context's
+// stream overwrites them.
+ipg_status wait_observable_copies(ipg_ctx *c) {
+    if (c->obs_copy_pending) IPG_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_obs_copied, 0));
+    return IPG_OK;
+}
+
 ipg_status observables_enqueue(ipg_ctx *c) {
     const int itmax = c->itmax;
     const double dtau = c->dtau;
     const size_t n = c->n;
     const int N = c->N;
-    // the observable arrays are rewritten below: an asynchronous copy of the
-    // previous event's must have read them first
-    if (c->obs_copy_pending) IPG_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_obs_copied, 0));
+    IPG_TRY(wait_observable_copies(c));
     IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     IPG_TRY(state64(c));
     TmunuArgs ta;
@@ -628,6 +635,8 @@ ipg_status ipg_destroy(ipg_ctx *ctx) {
         cudaSetDevice(ctx->cfg.device);
         cudaStreamSynchronize(ctx->stream);
     }
+    // an observables copy may still be writing the caller's host arrays
+    if (ctx->stream_copy) cudaStreamSynchronize(ctx->stream_copy);
     for (void *p : ctx->allocs) cudaFree(p);
     if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
     {
@@ -777,6 +786,29 @@ ipg_status ipg_use_device_noise(ipg_ctx *c) {
     c->have_noise = true;
     c->device_noise = true;
     return IPG_OK;
+}
+
+ipg_status ipg_draw_device_noise(ipg_ctx *c, int nucleus, int sheet_first, int sheet_count,
+                                 double *xi) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (!xi || nucleus < 0 || nucleus > 1 || sheet_first < 0 || sheet_count < 0 ||
+        sheet_first + sheet_count > c->cfg.Ny)
+        return fail(c, IPG_ERR_BAD_CONFIG, "noise draw: nucleus %d, sheets [%d, %d) of %d",
+                    nucleus, sheet_first, sheet_first + sheet_count, c->cfg.Ny);
+    // staged through the initial-condition work buffer: work_sheets sheets of
+    // 4 complex channels are 8 doubles a site and sheet
+    double *stage = reinterpret_cast<double *>(c->work);
+    const size_t per_sheet = 8 * c->n;
+    for (int k0 = 0; k0 < sheet_count; k0 += c->work_sheets) {
+        const int ns = std::min(c->work_sheets, sheet_count - k0);
+        launch_draw_noise(c->N, sheet_first + k0, ns, c->cfg.seed, (uint32_t)nucleus, stage,
+                          c->stream);
+        IPG_LAUNCHED(c, 1);
+        IPG_CUDA(c, cudaMemcpyAsync(xi + (size_t)k0 * per_sheet, stage,
+                                    sizeof(double) * per_sheet * ns, cudaMemcpyDeviceToHost,
+                                    c->stream));
+    }
+    return sync(c);
 }
 
 // The initial conditions on the context's stream, without waiting for them
@@ -1378,6 +1410,7 @@ ipg_status ipg_forward(ipg_ctx *c, int checkpoint_every, double *E_T, double *ep
         }
     }
     A.fin = cur;
+    IPG_TRY(wait_observable_copies(c));  // T10 is rewritten below
     TmunuArgs ta;
     ta.N = N;
     ta.g = c->cfg.g;
@@ -1465,7 +1498,10 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
         }
     } else {
         // reverse sweep: state s from state s+1 by time reversal, or from the
-        // checkpoint when s is a multiple of k; two state sets alternate
+        // checkpoint when s is a multiple of k; two state sets alternate.
+        // From its second step on the sweep overwrites the final state, so a
+        // failure anywhere below must leave the forward marked as consumed.
+        A.ready = false;
         State<double> sets[2] = {A.w[2], A.fin};
         State<double> nxt = A.fin;
         for (int s = S - 1, q = 0; s >= 0; s--, q++) {
@@ -1481,7 +1517,6 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
             }
             nxt = cur;
         }
-        A.ready = false;  // the reverse sweep overwrote the final state
     }
     launch_adjoint_project(n, A.adj, c->stream);
     IPG_LAUNCHED(c, 1);

@@ -112,6 +112,11 @@ void launch_wilson_product(const WilsonArgs &w, int ns, cudaStream_t st);
 // charge amplitude of every site, once per nucleus before its sheets
 void launch_wilson_amp(const WilsonArgs &w, cudaStream_t st);
 
+// the device noise of sheets [k0, k0+ns) of one nucleus, as the unit normals
+// xi[ns][N*N][8] that k_rows_fwd draws for them
+void launch_draw_noise(int N, int k0, int ns, uint64_t key, uint32_t nucleus, double *out,
+                       cudaStream_t st);
+
 void launch_green(int N, double m_lat, double uvdamp_lat, double *green,
                   cudaStream_t st);
 

@@ -21,8 +21,13 @@
 //     call itself; two calls whose work overlaps on the GPU (different
 //     streams, or different host threads on the same device) race on the
 //     array and give wrong results: serialise them.
+//   - the looked-up address is cached per device index for the life of the
+//     process; it assumes the device's primary context is not reset
+//     (cudaDeviceReset) between calls.
 // The sheets are processed with the same kernels as ipg_init_fields (one
-// sheet per batch), so the result agrees with the regular path.
+// sheet per batch). The twiddle table is built here on the device with
+// sincospi, where ipg_create builds it on the host with cos/sin of 2 pi k/N,
+// so the two paths agree to about 1e-12 on the Wilson lines, not bit for bit.
 #include <cuda_runtime.h>
 
 #include <cmath>

@@ -68,6 +68,39 @@ __global__ void k_amp(int n, double g, double Nyd, const double *g2mu2, double *
     if (p < n) amp[p] = g * sqrt(g2mu2[p] / Nyd);
 }
 
+// The unit normals k_rows_fwd draws in registers when no noise is given,
+// written out as xi[s][pos][a] for sheets k0 .. k0+ns-1: the same counter
+// (pos, k, 2 nucleus + a/4, 0), the same words (x, y) for colours a % 4 < 2
+// and (z, w) otherwise, the same Box-Muller. One thread per (site, counter
+// half), so colours 4h .. 4h+3 of a site come from one thread.
+__global__ void k_draw_noise(int N, int k0, int ns, uint64_t key, uint32_t nucleus,
+                             double *out) {
+    const size_t n = (size_t)N * N;
+    const size_t gid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= 2 * n * (size_t)ns) return;
+    const int hc = (int)(gid & 1);
+    const size_t rest = gid >> 1;
+    const size_t pos = rest % n;
+    const int s = (int)(rest / n);
+    const U4 r = philox4x32_10({(uint32_t)pos, (uint32_t)(k0 + s), (nucleus << 1) | (uint32_t)hc, 0u},
+                               (uint32_t)key, (uint32_t)(key >> 32));
+    double z0[2], z1[2];
+    box_muller(r.x, r.y, z0);  // channel 2 hc: colours 4 hc, 4 hc + 1
+    box_muller(r.z, r.w, z1);  // channel 2 hc + 1: colours 4 hc + 2, 4 hc + 3
+    double *o = out + ((size_t)s * n + pos) * 8 + 4 * hc;
+    o[0] = z0[0];
+    o[1] = z0[1];
+    o[2] = z1[0];
+    o[3] = z1[1];
+}
+
+void launch_draw_noise(int N, int k0, int ns, uint64_t key, uint32_t nucleus, double *out,
+                       cudaStream_t st) {
+    const size_t threads = 2 * (size_t)N * N * ns;
+    k_draw_noise<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(N, k0, ns, key, nucleus,
+                                                                     out);
+}
+
 void launch_wilson_amp(const WilsonArgs &w, cudaStream_t st) {
     const int n = w.N * w.N;
     k_amp<<<(n + 255) / 256, 256, 0, st>>>(n, w.g, (double)w.Ny, w.g2mu2, w.amp);

@@ -17,11 +17,14 @@ def pytest_configure(config):
 def _ensure_oracle(target: str, path: Path) -> None:
     if path.exists():
         return
-    src = os.environ.get("IPG_REF_SRC", "/root/reference/src")
-    if target == "ref" and not Path(src).exists():
+    # the oracle's Makefile knows where the reference sources are;
+    # IPG_REF_SRC overrides it
+    src = [f"REF_SRC={os.environ['IPG_REF_SRC']}"] if os.environ.get("IPG_REF_SRC") else []
+    make = ["make", "-s", "-C", str(ROOT / "oracle")]
+    if target == "ref" and subprocess.run(make + ["have-ref", *src],
+                                          capture_output=True).returncode != 0:
         pytest.skip(f"{path} not built and the reference sources are absent")
-    subprocess.run(["make", "-C", str(ROOT / "oracle"), target, f"REF_SRC={src}"],
-                   check=True, capture_output=True)
+    subprocess.run(make + [target, *src], check=True, capture_output=True)
 
 
 @pytest.fixture(scope="session")
