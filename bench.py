@@ -1,23 +1,31 @@
 """Benchmark of the IP-Glasma hot path on B200.
 
-One step = one Pb+Pb event of the 512^2 workload (L = 40 fm, b = 6 fm,
-Ny = 50, tau up to 0.6 fm/c, 77 leapfrog steps): colour-charge noise ->
-Poisson solve -> Wilson lines -> tau = 0 Newton links -> leapfrog ->
-T^{mu nu} + Landau matching + eccentricities. Each step draws fresh noise
-(device Philox, new key per event) on the same g^2 mu^2 maps, which stay
-resident in HBM.
+Headline workload (one step = one whole batch): 64 O+O events at 256^2
+(L = 20 fm) and 16 Pb+Pb events at 512^2 (L = 40 fm), impact parameters
+uniform in [0, 2R], Ny = 50, tau up to 0.4 fm (52 leapfrog steps for both
+sizes). Per step every event draws fresh colour-charge noise (device Philox,
+a new key per event and step), then colour charges -> Poisson solve -> Wilson
+lines -> tau = 0 Newton links for all events side by side, one persistent
+leapfrog launch per step over all 80 lattices (a replayed CUDA graph, tile
+shape from the autotuner), then T^{mu nu} + Landau matching + eccentricities
+of every event. The g^2 mu^2 maps (seeded Woods-Saxon nuclei) stay resident.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Reported (one JSON line, rank 0):
-  value       events/s of the FP32-bulk form (whole job, all ranks)
-  fp64        the plain FP64 form on the same events
-  error       FP32-bulk vs FP64 on the same event: per-cell e, epsilon_2, E_T
-  e2e         the same events through the C ABI with host buffers: g^2 mu^2
-              maps copied in and e, u, pi, T^{mu nu} copied out every event
-  roofline    the fused leapfrog kernel of the FP32 form against measured HBM
-  cpu_baseline the reference (oracle/_ref, OpenMP, all host cores) on a
-              bounded sample of the same event, scaled to one event
+  value        events/s of the batched FP32-bulk form (whole job, all ranks)
+  fp64         the same batch in the plain FP64 form
+  error        FP32 bulk vs FP64 on every event of the batch
+  e2e          the batch through the C ABI with host buffers: g^2 mu^2 maps in
+               and e, u, pi, T^{mu nu} of every event out, every step
+  roofline     the batched leapfrog kernel against measured HBM
+  large        8 Pb+Pb at 1024^2, Ny 100, tau 1.0 fm, dtau 0.05 a: FP32 and
+               FP64 batches, per-kernel GB/s, error
+  single_event one 512^2 Pb+Pb event (tau 0.6 fm) per form: the tile kernels
+  adjoint      gradient of E_T + eps2 for a 256^2 Au+Au event, 400 steps
+  cpu_baseline the reference (oracle/_ref, OpenMP, all host cores) on one event
+               of each size class of the same workload, combined in the
+               batch's proportions
 """
 from __future__ import annotations
 
@@ -36,8 +44,16 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+# One 512^2 Pb+Pb event (the single-event form: TMA tile kernels)
 WORKLOAD = dict(name="PbPb_512", N=512, L=40.0, nucleus="Pb", b=6.0, Ny=50,
                 maxtime=0.6, g=2.0, m=0.2)
+# Batched workloads: event classes (nucleus, N, L, count, impact parameter
+# range) evolved together on one time grid (same lattice spacing and dtau)
+HEADLINE = dict(name="OO256x64_PbPb512x16", Ny=50, maxtime=0.4, dtau=0.0, g=2.0, m=0.2,
+                classes=[dict(nucleus="O", N=256, L=20.0, count=64, bmax=2 * 2.61),
+                         dict(nucleus="Pb", N=512, L=40.0, count=16, bmax=2 * 6.62)])
+LARGE = dict(name="PbPb1024x8", Ny=100, maxtime=1.0, dtau=0.05, g=2.0, m=0.2,
+             classes=[dict(nucleus="Pb", N=1024, L=40.0, count=8, bmax=14.0)])
 METRIC = "site-updates/s & events/s: FP32-batched vs plain FP64 at stated err; adjoint/fwd"
 # algorithmic bytes per site-update of the fused leapfrog: every state word read
 # once and written once (links 2 x 18, E 2 x 8, phi 9, pi 9 = 70 reals)
@@ -198,8 +214,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-batched", action="store_true",
-                    help="skip the batched uneven-events measurement")
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the 8 x 1024^2 Pb+Pb production batch")
+    ap.add_argument("--no-single", action="store_true",
+                    help="skip the single 512^2 event (tile kernels) measurement")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint (forward/backward) measurement")
     ap.add_argument("--profile", choices=["fp32", "fp64", "both", "adjoint"], default=None,
@@ -254,6 +272,271 @@ def run_profile(which, local):
         ev.close()
 
 
+# ---------------------------------------------------------------------------
+# batched workloads: the whole job's events, LPT-sharded over the ranks
+# ---------------------------------------------------------------------------
+def steps_of(w: dict, cls: dict) -> int:
+    """Leapfrog steps of an event class (the reference's itmax rule,
+    Evolution.cpp:396, with dtau derived as main.cpp:531-534 unless set)."""
+    a = cls["L"] / cls["N"]
+    if w.get("dtau", 0) > 0:
+        dtau = w["dtau"]
+    else:
+        dtau = w["maxtime"] / ((int(10 * w["maxtime"] / a) + 1) * a)
+    return int(w["maxtime"] / (a * dtau) + 0.1)
+
+
+def job_events(w: dict, world: int) -> list[dict]:
+    """Every event of the whole job: `world` copies of the workload's class
+    mix (per-GPU work fixed: weak scaling), each event with its own seed and
+    impact parameter, and its cost N^2 x steps."""
+    rng = np.random.default_rng(20260 + len(w["name"]))
+    out = []
+    for r in range(world):
+        for ci, cls in enumerate(w["classes"]):
+            for k in range(cls["count"]):
+                out.append(dict(nucleus=cls["nucleus"], N=cls["N"], L=cls["L"],
+                                b=float(rng.uniform(0.0, cls["bmax"])),
+                                seed=7000 + 1000 * r + 100 * ci + k, cls=ci,
+                                cost=cls["N"] ** 2 * steps_of(w, cls)))
+    return out
+
+
+def lpt_assign(costs: list[float], world: int) -> list[list[int]]:
+    """Longest-processing-time-first: events in decreasing cost (ties by
+    index) each go to the rank with the least cost assigned so far (ties to
+    the lowest rank). Returns every rank's event indices, ascending."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    out: list[list[int]] = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        out[r].append(i)
+        load[r] += costs[i]
+    return [sorted(x) for x in out]
+
+
+def build_batch(ipg, w: dict, specs: list[dict], precision: int, seed_base: int):
+    """Contexts of the given events (g2mu maps set from the host once) and
+    their batch."""
+    from ipglasma_b200.synthetic import make_event
+    evs, maps = [], []
+    for k, e in enumerate(specs):
+        A, B, _, _ = make_event(e["N"], e["L"], e["nucleus"], e["b"], e["seed"], g=w["g"])
+        ev = ipg.Event(ipg.Config(size=e["N"], L=e["L"], Ny=w["Ny"], g=w["g"], m=w["m"],
+                                  maxtime=w["maxtime"], dtau=w.get("dtau", 0.0),
+                                  precision=precision, seed=seed_base + k))
+        ev.set_g2mu(A, B)
+        ev.use_device_noise()
+        evs.append(ev)
+        maps.append((A, B))
+    return evs, maps, ipg.Batch(evs)
+
+
+def batch_step(evs, batch, key0: int):
+    """One step of a batched workload: new noise keys, the initial conditions
+    of every event, the batched evolution and every event's observables."""
+    for k, ev in enumerate(evs):
+        ev.reseed(key0 + k)
+        ev.use_device_noise()
+    batch.init_fields(allow_nonconverged=True)
+    return batch.run()
+
+
+def timed_batch_steps(torch, evs, batch, K: int, key0: int):
+    """K batch steps: the device ms of each (CUDA events on torch's stream
+    around library calls that wait for their own streams) and the batch's
+    evolution ms of each (CUDA events around the replayed step graph)."""
+    times, evo = [], []
+    for k in range(K):
+        torch.cuda.synchronize()
+        st = torch.cuda.Event(enable_timing=True)
+        en = torch.cuda.Event(enable_timing=True)
+        st.record()
+        batch_step(evs, batch, key0 + 1000 * k)
+        en.record()
+        torch.cuda.synchronize()
+        times.append(st.elapsed_time(en))
+        evo.append(batch.stats()[0])
+    return times, evo
+
+
+def launches_of(evs, batch) -> int:
+    return sum(ev.kernel_launches() for ev in evs) + batch.stats()[2]
+
+
+def batch_errors(evs32, evs64) -> dict:
+    """FP32 bulk against FP64 on every event of a batch (same noise keys, so
+    the same FP64 initial conditions): the worst event of each figure."""
+    out = {}
+    for e32, e64 in zip(evs32, evs64):
+        eps32, eps64 = e32.observables()[0], e64.observables()[0]
+        for frac in (1e-2, 1e-3):
+            m = eps64 > frac * eps64.max()
+            rel = np.abs(eps32[m] - eps64[m]) / np.abs(eps64[m])
+            for key, v in ((f"e_rel_max_gt{frac:g}max", float(rel.max())),
+                           (f"e_rel_rms_gt{frac:g}max", float(np.sqrt(np.mean(rel ** 2))))):
+                out[key] = max(out.get(key, 0.0), v)
+    return out
+
+
+def result_errors(out: dict, r32, r64) -> dict:
+    for a, b in zip(r32, r64):
+        for key, v in (("eps2_rel", abs(a.eccentricity[1] - b.eccentricity[1])
+                        / abs(b.eccentricity[1])),
+                       ("E_T_rel", abs(a.E_T - b.E_T) / abs(b.E_T)),
+                       ("gauss_fp32", a.gauss_violation), ("gauss_fp64", b.gauss_violation),
+                       ("unitarity_fp32", a.unitarity_max), ("unitarity_fp64", b.unitarity_max)):
+            out[key] = max(out.get(key, 0.0), v)
+    out["events_compared"] = len(r32)
+    return out
+
+
+def site_updates(w: dict, specs: list[dict]) -> int:
+    return sum(e["N"] ** 2 * steps_of(w, w["classes"][e["cls"]]) for e in specs)
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+
+def measure_workload(torch, ipg, w, specs, K, W, key0, dist, clocks=None, e2e_steps=0,
+                     fp64_steps=None):
+    """FP32 and FP64 batches of one rank's events: W warm-up and K timed
+    steps of each, the error of FP32 against FP64 on every event, the
+    initial-condition stage rates, and optionally the e2e figure. Times are
+    maxed over ranks."""
+    out = {}
+    evs32, maps, b32 = build_batch(ipg, w, specs, ipg.FP32, key0)
+    batch_step(evs32, b32, key0)
+    out["tune"] = b32.tune()
+    for k in range(W):
+        batch_step(evs32, b32, key0 + 100 + k)
+    l0 = launches_of(evs32, b32)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with (clocks if clocks is not None else _Null()):
+        t32, evo32 = timed_batch_steps(torch, evs32, b32, K, key0 + 10000)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+    out["launches"] = launches_of(evs32, b32) - l0
+    e2e = None
+    if e2e_steps:
+        e2e = measure_batch_e2e(torch, evs32, maps, b32, e2e_steps, key0 + 50000, dist)
+    r32 = batch_step(evs32, b32, key0 + 99999)  # the comparison's noise keys
+    evs64, _, b64 = build_batch(ipg, w, specs, ipg.FP64, key0)
+    batch_step(evs64, b64, key0)
+    b64.tune()
+    for k in range(min(W, 2)):
+        batch_step(evs64, b64, key0 + 100 + k)
+    K64 = K if fp64_steps is None else fp64_steps
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t64, evo64 = timed_batch_steps(torch, evs64, b64, K64, key0 + 10000)
+    if dist:
+        dist.barrier()
+    r64 = batch_step(evs64, b64, key0 + 99999)
+    err = result_errors(batch_errors(evs32, evs64), r32, r64)
+    stages = stage_rates(w, specs, evs64, key0)
+    b32.close()
+    b64.close()
+    for ev in evs32 + evs64:
+        ev.close()
+    ms32, ms64, mevo32, mevo64 = max_over_ranks(
+        dist, [float(np.sum(t32)), float(np.sum(t64)), float(np.mean(evo32)),
+               float(np.mean(evo64))], "cuda")
+    out.update(ms32=ms32, ms64=ms64, K=K, K64=K64, evo32=mevo32, evo64=mevo64, err=err,
+               e2e=e2e, stages=stages)
+    return out
+
+
+def measure_batch_e2e(torch, evs, maps, batch, K, key0, dist):
+    """The batch through the C ABI with host buffers: every step copies each
+    event's g2mu maps from page-locked host memory, runs the batch, and
+    copies each event's e, u, pi and T^{mu nu} back (on the library's copy
+    streams, waited for within the step). Wall clock around K steps."""
+    def pinned(shape):
+        return torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+
+    host_in = []
+    for A, B in maps:
+        hA, hB = pinned(A.shape), pinned(B.shape)
+        hA[...] = A
+        hB[...] = B
+        host_in.append((hA, hB))
+    host_out = [(pinned((ev.n,)), pinned((4, ev.n)), pinned((10, ev.n)), pinned((10, ev.n)))
+                for ev in evs]
+
+    def one(k):
+        for ev, (hA, hB) in zip(evs, host_in):
+            ev.set_g2mu(hA, hB)
+        batch_step(evs, batch, key0 + 1000 * k)
+        for ev, o in zip(evs, host_out):
+            ev.observables_async(*o)
+        for ev in evs:
+            ev.wait_observables()
+    one(0)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(K):
+        one(k + 1)
+    torch.cuda.synchronize()
+    total = time.perf_counter() - t0
+    h2d = sum(2 * ev.n * 8 for ev in evs)
+    d2h = sum(25 * ev.n * 8 for ev in evs)
+    return {"ms": total * 1e3, "h2d": h2d, "d2h": d2h}
+
+
+def stage_rates(w, specs, evs, key0):
+    """Device time of the initial-condition stages of one event per size
+    class, run alone (ipg_init_report: CUDA events in the library), with
+    their algorithmic bytes: the Wilson-line stage reads and writes V once
+    per (site, sheet, nucleus), 2 x 18 x 8 = 288 B; Newton reads U1, U2 (36
+    doubles) and writes U (18) per link, 432 B."""
+    out = {}
+    seen = set()
+    for e, ev in zip(specs, evs):
+        if e["cls"] in seen:
+            continue
+        seen.add(e["cls"])
+        ev.reseed(key0 + 7)
+        ev.use_device_noise()
+        rep = ev.init_fields(allow_nonconverged=True)
+        n = e["N"] ** 2
+        wil = n * w["Ny"] * 2 * 288
+        newt = 2 * n * 432
+        out[f"{e['nucleus']}{e['N']}"] = {
+            "ms_wilson": round(rep.ms_wilson, 3),
+            "wilson_GBs_at_288B": round(wil / (rep.ms_wilson * 1e-3) / 1e9, 1),
+            "ms_newton": round(rep.ms_newton, 3),
+            "newton_GBs_at_432B": round(newt / (rep.ms_newton * 1e-3) / 1e9, 1),
+            "newton_mean_iterations": round(rep.newton_mean_iterations, 2),
+            "ms_fields": round(rep.ms_fields, 3)}
+    return out
+
+
+def workload_config(w: dict, world: int) -> dict:
+    return {"workload": w["name"],
+            "events_per_step": sum(c["count"] for c in w["classes"]) * world,
+            "classes": [{"nucleus": c["nucleus"], "N": c["N"], "L_fm": c["L"],
+                         "count_per_gpu": c["count"], "b_max_fm": round(c["bmax"], 2),
+                         "leapfrog_steps": steps_of(w, c)} for c in w["classes"]],
+            "Ny": w["Ny"], "tau_fm": w["maxtime"],
+            "dtau": (f"{w['dtau']} a" if w.get("dtau") else "derived (main.cpp:531-534)"),
+            "l2": "no flush: a step's state (over 1 GB) is larger than the 126 MB L2",
+            "parallelism": f"events LPT-sharded (cost N^2 x steps) over {world} GPU(s), "
+                           "no collective"}
+
+
 def run_ours(args, world, rank, local):
     import torch
     import ipglasma_b200 as ipg
@@ -266,70 +549,46 @@ def run_ours(args, world, rank, local):
         dist_mod.init_process_group("nccl", timeout=timedelta(seconds=300))
         dist = dist_mod
     K, W = args.steps, max(3, args.warmup)
-    A, B = make_inputs()
-    d_A = torch.tensor(A, dtype=torch.float64, device="cuda")
-    d_B = torch.tensor(B, dtype=torch.float64, device="cuda")
-    l2buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-    N = WORKLOAD["N"]
-    seed_base = rank_seed_base(rank)
-
-    ev32 = ipg.Event(cfg_for(ipg.FP32, seed_base))
-    ev64 = ipg.Event(cfg_for(ipg.FP64, seed_base))
-    itmax = ev32.itmax
-    launches0 = ev32.kernel_launches()
-
-    # warm-up (untimed)
-    run_events(torch, ev32, d_A, d_B, W, seed_base, l2buf)
-    run_events(torch, ev64, d_A, d_B, min(W, 3), seed_base, l2buf)
-
-    def barrier():
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    # --- timed: FP32-bulk form (the headline) -------------------------------
-    launches_before = ev32.kernel_launches()
-    with ClockSampler(local) as clk:
-        barrier()
-        t32, lf32 = run_events(torch, ev32, d_A, d_B, K, seed_base + 100, l2buf)
-        barrier()
-    launches_timed = ev32.kernel_launches() - launches_before
-    # --- timed: plain FP64 form ----------------------------------------------
-    barrier()
-    t64, lf64 = run_events(torch, ev64, d_A, d_B, K, seed_base + 100, l2buf)
-    barrier()
-
-    ms32, ms64 = max_over_ranks(dist, [float(np.sum(t32)), float(np.sum(t64))], "cuda")
-    ev_per_s32 = whole_job_rate(world, K, ms32)
-    ev_per_s64 = whole_job_rate(world, K, ms64)
-    su32 = N * N * itmax / (np.mean(lf32) * 1e-3)
-    su64 = N * N * itmax / (np.mean(lf64) * 1e-3)
-
-    # --- error of the FP32 form against FP64 on one event -------------------
-    err = compare_forms(ev32, ev64, d_A, d_B, seed_base + 7)
-
-    # --- end to end through the C ABI with host buffers ---------------------
-    e2e = measure_e2e(torch, ipg, A, B, K, seed_base + 500, l2buf, dist)
-    e2e["ms"] = max_over_ranks(dist, [e2e["ms"]], "cuda")[0]
-
     peaks = load_peaks()
     hbm = peaks.get("hbm_gbs", 6650.0)
+
+    # --- headline: the batched uneven-events workload ------------------------
+    w = HEADLINE
+    allev = job_events(w, world)
+    mine = [allev[i] for i in lpt_assign([e["cost"] for e in allev], world)[rank]]
+    clk = ClockSampler(local)
+    res = measure_workload(torch, ipg, w, mine, K, W, rank_seed_base(rank) * 100, dist,
+                           clocks=clk, e2e_steps=K)
+    n_ev = len(allev)
+    su = site_updates(w, allev)
+    ev32 = n_ev * K / (res["ms32"] * 1e-3)
+    ev64 = n_ev * res["K64"] / (res["ms64"] * 1e-3)
+    su32 = su / (res["evo32"] * 1e-3)
+    su64 = su / (res["evo64"] * 1e-3)
+    e2e = res["e2e"]
+    e2e_ms = max_over_ranks(dist, [e2e["ms"]], "cuda")[0]
     achieved = su32 * BYTES_PER_SITE_UPDATE["fp32"] / 1e9
-    traffic = load_traffic()
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
-            "frac": round(achieved / hbm, 4), "traffic": traffic,
-            "kernel": "k_leapfrog_tile (FP32 bulk: TMA-staged 8x32 tiles, both directions in packed f32x2 lanes)",
+            "frac": round(achieved / hbm, 4), "traffic": load_traffic(),
+            "kernel": "k_leapfrog_batch<float> (FP32 bulk: all events of the batch in one "
+                      "persistent launch per step)",
             "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp32"],
             "bytes_stored_per_site_update": BYTES_STORED_PER_SITE_UPDATE["fp32"],
             "stored_frac": round(su32 * BYTES_STORED_PER_SITE_UPDATE["fp32"] / 1e9 / hbm, 4),
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-            "fp64_kernel": {"kernel": "k_leapfrog_tile64 (FP64 plain form: TMA-staged 4x32 tiles)", "achieved": round(su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9, 1),
+            "timing": "CUDA events on the batch's stream around the replayed step graph (all "
+                      "leapfrog launches of the batch), mean over the timed steps",
+            "fp64_kernel": {"kernel": "k_leapfrog_batch<double>",
+                            "achieved": round(su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9, 1),
                             "frac": round(su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9 / hbm, 4),
                             "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp64"],
-                            "bytes_stored_per_site_update": BYTES_STORED_PER_SITE_UPDATE["fp64"],
-                            "stored_frac": round(su64 * BYTES_STORED_PER_SITE_UPDATE["fp64"] / 1e9 / hbm, 4)}}
+                            "stored_frac": round(su64 * BYTES_STORED_PER_SITE_UPDATE["fp64"]
+                                                 / 1e9 / hbm, 4)}}
+    tune = res["tune"]
 
-    batched = None if args.no_batched else measure_batched(torch, ipg, rank, dist)
+    large = None if args.no_large else measure_large(torch, ipg, rank, world, dist, hbm)
+    single = None if args.no_single else measure_single(torch, ipg, K, W, rank, world, dist,
+                                                        hbm)
     adjoint = None if args.no_adjoint else measure_adjoint(torch, ipg, rank)
 
     cpu = None
@@ -339,113 +598,128 @@ def run_ours(args, world, rank, local):
     if rank == 0:
         line = {
             "metric": METRIC,
-            "value": round(ev_per_s32, 3),
+            "value": round(ev32, 3),
             "unit": "events/s",
             "n_gpus": world,
             "steps": K,
             "warmup": W,
-            "ms_per_step": round(ms32 / K, 3),
+            "ms_per_step": round(res["ms32"] / K, 3),
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f32 (FP64 Newton, Wilson lines, observables, reductions)",
-            "data": "synthetic (seeded Woods-Saxon Pb+Pb, g2mu ~ sqrt(T_A), device Philox noise)",
-            "config": {"workload": WORKLOAD["name"], "N": N, "L_fm": WORKLOAD["L"],
-                       "Ny": WORKLOAD["Ny"], "b_fm": WORKLOAD["b"], "tau_fm": WORKLOAD["maxtime"],
-                       "leapfrog_steps": itmax, "events_per_gpu": K,
-                       "l2": "flushed (256 MB write) before every event",
-                       "parallelism": f"events sharded over {world} GPU(s), no collective"},
-            "site_updates_per_s": round(world * su32, 1),
-            "fp64": {"events_per_s": round(ev_per_s64, 3), "ms_per_event": round(ms64 / K, 3),
-                     "site_updates_per_s": round(world * su64, 1)},
-            "fp32_over_fp64_events": round(ev_per_s32 / ev_per_s64, 3),
-            "error": err,
-            "e2e": {"value": round(whole_job_rate(world, K, e2e["ms"]), 3), "unit": "events/s",
-                    "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"],
-                    "form": "fp32", "host_buffers": e2e["host_buffers"],
-                    "copies": e2e["copies"]},
-            "writers": e2e["writers"] if rank == 0 else None,
+            "data": "synthetic (seeded Woods-Saxon nuclei, g2mu ~ sqrt(T_A), device Philox "
+                    "noise)",
+            "config": workload_config(w, world),
+            "site_updates_per_s": round(su32, 1),
+            "fp64": {"events_per_s": round(ev64, 3),
+                     "ms_per_step": round(res["ms64"] / res["K64"], 3),
+                     "site_updates_per_s": round(su64, 1), "steps": res["K64"]},
+            "fp32_over_fp64_events": round(ev32 / ev64, 3),
+            "fp32_over_fp64_site_updates": round(su32 / su64, 3),
+            "error": res["err"],
+            "evolution_ms_per_step": {"fp32": round(res["evo32"], 3),
+                                      "fp64": round(res["evo64"], 3)},
+            "initial_condition_stages": res["stages"],
+            "e2e": {"value": round(n_ev * K / (e2e_ms * 1e-3), 3), "unit": "events/s",
+                    "h2d_bytes_per_step": e2e["h2d"] * world,
+                    "d2h_bytes_per_step": e2e["d2h"] * world, "form": "fp32",
+                    "host_buffers": "pinned",
+                    "copies": "every event's g2mu maps in and e, u, pi, T^munu out, every "
+                              "step, inside the wall-clock region"},
             "roofline": roof,
-            "batched": batched,
+            "tuned_shape": {"tile_rows": tune.tile_rows, "threads": tune.threads_per_block,
+                            "blocks_per_sm": tune.blocks_per_sm, "grid": tune.grid,
+                            "candidates": tune.candidates},
+            "large": large,
+            "single_event": single,
             "adjoint": adjoint,
             "cpu_baseline": cpu,
-            "gpu_launches": int(launches_timed),
+            "gpu_launches": int(res["launches"]),
             "clocks": clk.summary(),
         }
         print(json.dumps(line))
-    ev32.close()
-    ev64.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
 
 
-BATCH = dict(oo=64, pb=16, maxtime=0.4, reps=2)
+def measure_large(torch, ipg, rank, world, dist, hbm):
+    """8 Pb+Pb events at 1024^2 (L = 40 fm, Ny = 100, b uniform in [0, 14] fm)
+    to tau = 1.0 fm at dtau = 0.05 a (512 steps): the FP32 batch and the FP64
+    batch, 2 timed steps each after one warm-up, the error of FP32 against
+    FP64 on every event, and the per-kernel rates."""
+    w = LARGE
+    allev = job_events(w, world)
+    mine = [allev[i] for i in lpt_assign([e["cost"] for e in allev], world)[rank]]
+    res = measure_workload(torch, ipg, w, mine, 2, 1, rank_seed_base(rank) * 100 + 50000,
+                           dist)
+    n_ev = len(allev)
+    su = site_updates(w, allev)
+    su32 = su / (res["evo32"] * 1e-3)
+    su64 = su / (res["evo64"] * 1e-3)
+    g32 = su32 * BYTES_PER_SITE_UPDATE["fp32"] / 1e9
+    g64 = su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9
+    return {"config": workload_config(w, world),
+            "events_per_s": {"fp32": round(n_ev * 2 / (res["ms32"] * 1e-3), 3),
+                             "fp64": round(n_ev * 2 / (res["ms64"] * 1e-3), 3)},
+            "ms_per_step": {"fp32": round(res["ms32"] / 2, 1), "fp64": round(res["ms64"] / 2, 1)},
+            "fp32_over_fp64_events": round(res["ms64"] / res["ms32"], 3),
+            "leapfrog": {"fp32": {"kernel": "k_leapfrog_batch<float>",
+                                  "ms_per_batch": round(res["evo32"], 2),
+                                  "site_updates_per_s": round(su32, 1),
+                                  "GBs_at_544B": round(g32, 1), "frac": round(g32 / hbm, 4)},
+                         "fp64": {"kernel": "k_leapfrog_batch<double>",
+                                  "ms_per_batch": round(res["evo64"], 2),
+                                  "site_updates_per_s": round(su64, 1),
+                                  "GBs_at_1728B": round(g64, 1), "frac": round(g64 / hbm, 4)}},
+            "initial_condition_stages": res["stages"],
+            "error": res["err"],
+            "timing": "2 timed batch steps per form after 1 warm-up; CUDA events"}
 
 
-def measure_batched(torch, ipg, rank, dist):
-    """Batched uneven events: 64 O+O at 256^2 (L = 20 fm) and 16 Pb+Pb at 512^2
-    (L = 40 fm), impact parameters uniform in [0, 2R], Ny = 50, FP32 bulk, to
-    tau = 0.4 fm (52 steps for both sizes, a = 0.078125 fm). Per batch: the
-    initial conditions of every event, then one persistent leapfrog launch per
-    step over all 80 lattices (a replayed CUDA graph, launch shape from the
-    autotuner), then the observables of every event."""
-    from ipglasma_b200.synthetic import make_event
-    rng = np.random.default_rng(5 + rank)
-    evs = []
-    for k in range(BATCH["oo"] + BATCH["pb"]):
-        oo = k < BATCH["oo"]
-        N, L, nuc, R = (256, 20.0, "O", 2.61) if oo else (512, 40.0, "Pb", 6.62)
-        A, B, _, _ = make_event(N, L, nuc, rng.uniform(0.0, 2.0 * R), 7000 + 100 * rank + k)
-        ev = ipg.Event(ipg.Config(size=N, L=L, Ny=50, maxtime=BATCH["maxtime"],
-                                  precision=ipg.FP32, seed=rank_seed_base(rank) + 600 + k))
-        ev.set_g2mu(A, B)
-        ev.use_device_noise()
-        evs.append(ev)
-
-    batch = ipg.Batch(evs)
-
-    def init_all():
-        batch.init_fields(allow_nonconverged=True)
-
-    init_all()
-    tune = batch.tune()
-    batch.run()  # warm-up: captures the graph
-    times, evo = [], []
-    for r in range(BATCH["reps"]):
-        torch.cuda.synchronize()
-        st = torch.cuda.Event(enable_timing=True)
-        en = torch.cuda.Event(enable_timing=True)
-        st.record()
-        init_all()
-        batch.run()
-        en.record()
-        torch.cuda.synchronize()
-        times.append(st.elapsed_time(en))
-        evo.append(batch.stats()[0])
-    launches = batch.stats()[2]
-    batch.close()
-    for ev in evs:
+def measure_single(torch, ipg, K, W, rank, world, dist, hbm):
+    """One 512^2 Pb+Pb event per step (tau 0.6 fm, 77 steps) in each form:
+    the single-event TMA tile kernels."""
+    A, B = make_inputs()
+    d_A = torch.tensor(A, dtype=torch.float64, device="cuda")
+    d_B = torch.tensor(B, dtype=torch.float64, device="cuda")
+    l2buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    N = WORKLOAD["N"]
+    Ks = min(K, 10)
+    seed_base = rank_seed_base(rank)
+    out = {}
+    evs = {}
+    for name, prec in (("fp32", ipg.FP32), ("fp64", ipg.FP64)):
+        ev = ipg.Event(cfg_for(prec, seed_base))
+        run_events(torch, ev, d_A, d_B, min(W, 3), seed_base, l2buf)
+        if dist:
+            dist.barrier()
+        t, lf = run_events(torch, ev, d_A, d_B, Ks, seed_base + 100, l2buf)
+        ms, mlf = max_over_ranks(dist, [float(np.sum(t)), float(np.mean(lf))], "cuda")
+        su = N * N * ev.itmax / (mlf * 1e-3)
+        g = su * BYTES_PER_SITE_UPDATE[name] / 1e9
+        out[name] = {"events_per_s": round(world * Ks / (ms * 1e-3), 3),
+                     "ms_per_event": round(ms / Ks, 3), "leapfrog_ms": round(mlf, 3),
+                     "site_updates_per_s": round(su, 1),
+                     "kernel": ("k_leapfrog_tile" if name == "fp32" else "k_leapfrog_tile64"),
+                     "GBs": round(g, 1), "frac": round(g / hbm, 4),
+                     "bytes_per_site_update": BYTES_PER_SITE_UPDATE[name],
+                     "stored_frac": round(su * BYTES_STORED_PER_SITE_UPDATE[name] / 1e9 / hbm,
+                                          4)}
+        evs[name] = ev
+    out["fp32_over_fp64_events"] = round(out["fp32"]["events_per_s"]
+                                         / out["fp64"]["events_per_s"], 3)
+    out["error"] = compare_forms(evs["fp32"], evs["fp64"], d_A, d_B, seed_base + 7)
+    if rank == 0:
+        ev = evs["fp32"]
+        eps, u4, pi10, T10 = ev.observables()
+        out["writers"] = measure_writers(ipg, ev, eps, u4, pi10, T10, ev.itmax, ev.dtau)
+    out["workload"] = "Pb+Pb 512^2, L 40 fm, b 6 fm, Ny 50, tau 0.6 fm (77 steps)"
+    out["l2"] = "flushed (256 MB write) before every event"
+    for ev in evs.values():
         ev.close()
-    ms = max_over_ranks(dist, [float(np.mean(times))], "cuda")[0]
-    n_ev = len(evs)
-    world = dist.get_world_size() if dist else 1
-    sites = BATCH["oo"] * 256 ** 2 + BATCH["pb"] * 512 ** 2
-    steps = evs[0].itmax
-    return {"workload": f"{BATCH['oo']} O+O 256^2 + {BATCH['pb']} Pb+Pb 512^2, "
-                        f"Ny 50, tau {BATCH['maxtime']} fm, FP32 bulk",
-            "events_per_s": round(whole_job_rate(world, n_ev, ms), 2),
-            "ms_per_batch": round(ms, 2),
-            "evolution_ms": round(float(np.mean(evo)), 2),
-            "leapfrog_steps": steps,
-            "site_updates_per_s_evolution": round(sites * steps / (np.mean(evo) * 1e-3), 1),
-            "launches_per_batch_evolution": steps,
-            "cuda_graph": True,
-            "tuned_shape": {"tile_rows": tune.tile_rows, "threads": tune.threads_per_block,
-                            "blocks_per_sm": tune.blocks_per_sm, "grid": tune.grid,
-                            "candidates": tune.candidates},
-            "timing": "CUDA events around init of all events + batched run, mean of "
-                      f"{BATCH['reps']}; total batched launches {launches}"}
+    return out
 
 
 ADJ = dict(N=256, L=30.0, nucleus="Au", b=2.0, Ny=50, steps=400, dtau=0.1, checkpoint=20)
@@ -560,57 +834,6 @@ def compare_forms(ev32, ev64, d_A, d_B, seed):
     return out
 
 
-def measure_e2e(torch, ipg, A, B, K, seed0, l2buf, dist):
-    """Events through the C ABI with host buffers: g2mu maps in, observables
-    out. Each event's observables are copied back on the library's copy
-    stream (ipg_get_observables_async) while the next event starts; the K
-    events, the L2 flush before each, and the last copy are one timed region."""
-    ev = ipg.Event(cfg_for(ipg.FP32, seed0))
-    n = ev.n
-
-    def pinned(shape):
-        # page-locked host memory (torch's pinned allocator), seen as numpy
-        return torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
-
-    hA, hB = pinned(A.shape), pinned(B.shape)
-    hA[...] = A
-    hB[...] = B
-    # two sets of page-locked observable arrays, alternating between events
-    sets = [(pinned((n,)), pinned((4, n)), pinned((10, n)), pinned((10, n))) for _ in range(2)]
-    cur = torch.cuda.current_stream()
-
-    def one(seed, k):
-        flush_l2(torch, l2buf)
-        cur.synchronize()  # torch's stream only: the previous copy keeps running
-        ev_reset(ev, seed)
-        ev.set_g2mu(hA, hB)
-        ev.use_device_noise()
-        ev.init_fields(allow_nonconverged=True)
-        ev.run()
-        ev.observables_async(*sets[k % 2])
-    for k in range(3):
-        one(seed0 + k, k)
-    ev.wait_observables()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for k in range(K):
-        one(seed0 + 10 + k, k)
-    ev.wait_observables()
-    torch.cuda.synchronize()
-    total = time.perf_counter() - t0
-    itmax = ev.itmax
-    dtau = ev.dtau
-    eps, u4, pi10, T10 = sets[(K - 1) % 2]
-    writers = measure_writers(ipg, ev, eps, u4, pi10, T10, itmax, dtau)
-    ev.close()
-    return {"ms": total * 1e3, "h2d": int(2 * n * 8), "d2h": int(25 * n * 8),
-            "host_buffers": "pinned", "writers": writers,
-            "copies": "observables back on a copy stream, overlapping the next event; "
-                      "L2 flush before each event and the last copy inside the timed region"}
-
-
 def measure_writers(ipg, ev, eps, u4, pi10, T10, itmax, dtau):
     """Output files, timed apart from the event rate: the reference's hydro
     and T^munu files of the last event (sizeOutput = N over the lattice, one
@@ -679,61 +902,119 @@ def load_traffic():
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference itself (oracle/_ref), all host cores
+# CPU baseline and reference arm: the reference itself (oracle/_ref), built
+# with the reference's own -Ofast flags (finite-math off, which the reference
+# needs), OpenMP over all host cores, one event at a time as the reference's
+# executable runs them
 # ---------------------------------------------------------------------------
-SAMPLE = dict(N=128, L=10.0, Ny=50)  # same lattice spacing as the 512^2 event
+FFT_NOTE = ("shim FFT, not FFTW: the reference's FFTW calls run on this project's "
+            "single-threaded radix-2 stand-in (FFTW is absent from the image)")
+
+
+def reference_event(spec: dict, w: dict, threads: int) -> dict:
+    """One event of a workload through the reference harness: seconds of the
+    hot path (setV, tau = 0 solve, Evolution::run with T^munu and Landau
+    matching, eccentricity) timed inside the harness, dumps off."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    from refcase import HARNESS_OFAST, run_harness
+    from ipglasma_b200.synthetic import make_event
+    A, B, _, _ = make_event(spec["N"], spec["L"], spec["nucleus"], spec["b"], spec["seed"],
+                            g=w["g"])
+    with tempfile.TemporaryDirectory() as tmp:
+        r = run_harness(Path(tmp) / "ref", A, B, spec["N"], spec["L"], w["Ny"], w["g"], w["m"],
+                        spec["seed"], w["maxtime"], threads=threads, binary=HARNESS_OFAST,
+                        dtau=w.get("dtau") or -1.0, dumps=False)
+    phases = {k: round(r.meta[k], 3) for k in ("t_setV", "t_tau0", "t_evolution",
+                                                "t_eccentricity")}
+    return {"seconds": float(sum(phases.values())), "phases_s": phases,
+            "itmax": r.meta["itmax"]}
+
+
+def reference_available() -> str | None:
+    sys.path.insert(0, str(ROOT / "tests"))
+    from refcase import HARNESS_OFAST
+    if not HARNESS_OFAST.exists():
+        return "oracle/_ref/ipg_ref_harness_ofast is not built (reference sources absent)"
+    return None
 
 
 def cpu_baseline_sample(threads: int | None = None):
-    """Time the reference on a bounded sample of the workload: the same lattice
-    spacing (a = 0.078125 fm), Ny, tau and schedule on a 128^2 patch centred on
-    a Pb+Pb collision; scaled by the site count (512^2 / 128^2 = 16) to one
-    event, which is how every stage of the reference scales (the FFTs by a
-    further log factor, ignored here in the reference's favour)."""
-    sys.path.insert(0, str(ROOT / "tests"))
-    from refcase import HARNESS, run_harness
-    from ipglasma_b200.synthetic import make_event
-    if not HARNESS.exists():
+    """The reference on a bounded sample of the headline workload: the first
+    event of each size class (one O+O 256^2 and one Pb+Pb 512^2 event, 52
+    steps each), combined in the batch's proportions (64 : 16) into the
+    batch's events/s."""
+    why = reference_available()
+    if why:
         return {"value": None, "unit": "events/s", "cores": 0, "kind": "reference",
-                "sample": "oracle/_ref/ipg_ref_harness not built"}
+                "sample": why}
     threads = threads or os.cpu_count() or 1
-    s = SAMPLE
-    A, B, _, _ = make_event(s["N"], s["L"], WORKLOAD["nucleus"], WORKLOAD["b"], seed=11)
-    with tempfile.TemporaryDirectory() as tmp:
-        t0 = time.perf_counter()
-        r = run_harness(Path(tmp) / "ref", A, B, s["N"], s["L"], s["Ny"], WORKLOAD["g"],
-                        WORKLOAD["m"], 5, WORKLOAD["maxtime"], threads=threads)
-        wall = time.perf_counter() - t0
-    scale = (WORKLOAD["N"] / s["N"]) ** 2
-    t_event = wall * scale
-    return {"value": round(1.0 / t_event, 6), "unit": "events/s", "cores": threads,
+    w = HEADLINE
+    evs = job_events(w, 1)
+    per_class = {}
+    for e in evs:
+        if e["cls"] not in per_class:
+            per_class[e["cls"]] = reference_event(e, w, threads)
+    t_batch = sum(c["count"] * per_class[i]["seconds"] for i, c in enumerate(w["classes"]))
+    n = sum(c["count"] for c in w["classes"])
+    return {"value": round(n / t_batch, 6), "unit": "events/s", "cores": threads,
             "kind": "reference",
-            "sample": (f"reference -O2 OpenMP harness, one event at N={s['N']} L={s['L']} fm "
-                       f"(same a, Ny={s['Ny']}, tau={WORKLOAD['maxtime']} fm) in {wall:.1f} s, "
-                       f"x{scale:.0f} sites -> {t_event:.1f} s per 512^2 event"),
-            "phases_s": {k: r.meta[k] for k in ("t_setV", "t_tau0", "t_evolution")}}
+            "sample": "; ".join(f"one {c['nucleus']}+{c['nucleus']} {c['N']}^2 event in "
+                                f"{per_class[i]['seconds']:.1f} s x {c['count']}"
+                                for i, c in enumerate(w["classes"]))
+                      + f" -> {t_batch:.0f} s per {n}-event batch (reference -Ofast build, "
+                        f"OpenMP {threads} threads)",
+            "fft": FFT_NOTE,
+            "phases_s": {w["classes"][i]["nucleus"]: v["phases_s"]
+                         for i, v in per_class.items()}}
 
 
 def run_reference(args, world, rank):
+    """The reference arm: whole events of the headline workload on the host
+    cores, in the batch's class proportions (4 O+O then 1 Pb+Pb, repeating),
+    one event per step, at most 5 steps (one full rotation, the batch's mix
+    exactly) so the run stays within a few minutes. No warm-up: every event
+    is a fresh process, as in the reference's own executable."""
     if rank != 0:
         return
-    K, W = args.steps, args.warmup
+    why = reference_available()
+    if why:
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return
     threads = os.cpu_count() or 1
-    vals = []
-    for k in range(max(1, min(K, 3))):
-        cb = cpu_baseline_sample(threads)
-        if cb["value"] is None:
-            print(json.dumps({"impl": "reference", "unavailable": cb["sample"]}))
-            return
-        vals.append(cb["value"])
-    v = float(np.mean(vals))
+    w = HEADLINE
+    evs = job_events(w, 1)
+    by_class = [[e for e in evs if e["cls"] == i] for i in range(len(w["classes"]))]
+    ratio = [c["count"] for c in w["classes"]]
+    unit = min(ratio)
+    order = []
+    idx = [0] * len(ratio)
+    while len(order) < sum(ratio):
+        for i, r in enumerate(ratio):
+            for _ in range(r // unit):
+                order.append(by_class[i][idx[i] % len(by_class[i])])
+                idx[i] += 1
+    K = max(1, min(args.steps, sum(r // unit for r in ratio)))
+    done = [reference_event(order[k], w, threads) for k in range(K)]
+    total = sum(d["seconds"] for d in done)
+    v = K / total
+    mix = {}
+    for k in range(K):
+        key = f"{order[k]['nucleus']}{order[k]['N']}"
+        mix[key] = mix.get(key, 0) + 1
+    sample = (f"{K} whole events of the workload ("
+              + ", ".join(f"{n} x {k}" for k, n in mix.items())
+              + f") in {total:.1f} s, reference -Ofast build, OpenMP {threads} threads")
     line = {"metric": METRIC, "value": round(v, 6), "unit": "events/s", "n_gpus": world,
-            "steps": len(vals), "warmup": 0, "ms_per_step": round(1e3 / v, 1),
+            "steps": K, "warmup": 0, "ms_per_step": round(1e3 * total / K, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (same generator as the GPU arm)",
-            "config": {"workload": WORKLOAD["name"], "N": WORKLOAD["N"]},
+            "dtype": "f64", "data": "synthetic (same generator and events as the GPU arm)",
+            "config": workload_config(w, world),
             "impl": "reference",
-            "cpu_baseline": dict(cb, value=round(v, 6)),
+            "fft": FFT_NOTE,
+            "per_event_s": [round(d["seconds"], 2) for d in done],
+            "phases_s": [d["phases_s"] for d in done],
+            "cpu_baseline": {"value": round(v, 6), "unit": "events/s", "cores": threads,
+                             "kind": "reference", "sample": sample},
             "e2e": {"value": round(v, 6), "unit": "events/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))

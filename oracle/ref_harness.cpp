@@ -62,6 +62,7 @@ struct Args {
     int write_outputs = 0;
     int size_output = 0;
     double L_output = 0.0;
+    int dumps = 1;  // 0: no state, noise or observable dumps (timing runs)
 };
 
 void usage() {
@@ -69,7 +70,7 @@ void usage() {
                  " [--Ny n] [--g g] [--m GeV] [--uvdamp x] [--seed s]"
                  " [--maxtime fm] [--dtau lattice] [--mode full|steps|init]"
                  " [--steps k] [--write-outputs w] [--size-output n]"
-                 " [--L-output fm]\n";
+                 " [--L-output fm] [--dumps 0|1]\n";
     std::exit(2);
 }
 
@@ -95,6 +96,7 @@ Args parse(int argc, char **argv) {
         else if (k == "--write-outputs") a.write_outputs = std::atoi(v.c_str());
         else if (k == "--size-output") a.size_output = std::atoi(v.c_str());
         else if (k == "--L-output") a.L_output = std::atof(v.c_str());
+        else if (k == "--dumps") a.dumps = std::atoi(v.c_str());
         else usage();
     }
     if (a.g2mu_file.empty()) usage();
@@ -272,6 +274,7 @@ int main(int argc, char **argv) {
     auto t0 = std::chrono::steady_clock::now();
     init.setV(&lat, &param, &rhoRandom);
     const double t_setv = seconds_since(t0);
+    if (A.dumps) {
     dump_matrices("VA.bin", lat, N, &Cell::getU);
     dump_matrices("VB.bin", lat, N, &Cell::getU2);
     {
@@ -287,6 +290,7 @@ int main(int argc, char **argv) {
                             std::ios::out | std::ios::binary);
             f.write((char *)xi.data(), cnt * sizeof(double));
         }
+    }
     }
 
     // (4) tau = 0 fields; count the restart draws made on bootRandom
@@ -308,9 +312,9 @@ int main(int argc, char **argv) {
             }
         }
     }
-    dump_state("tau0", lat, N);
+    if (A.dumps) dump_state("tau0", lat, N);
 
-    double t_evo = 0.0;
+    double t_evo = 0.0, t_ecc = 0.0;
     int itmax = static_cast<int>(param.getMaxtime() / (a * param.getdtau()) + 0.1);
     if (A.mode == "steps") {
         // (5b) leapfrog only, K full steps after the tau=0 half step
@@ -325,16 +329,20 @@ int main(int argc, char **argv) {
             evolution.evolveU(&lat, &param, dtau, it * dtau);
         }
         t_evo = seconds_since(t0);
-        dump_state("steps", lat, N);
+        if (A.dumps) dump_state("steps", lat, N);
         itmax = A.steps;
     } else if (A.mode == "full") {
         // (5a) the reference schedule, then (6) eccentricity
         t0 = std::chrono::steady_clock::now();
         evolution.run(&lat, &group, &param);
         t_evo = seconds_since(t0);
+        t0 = std::chrono::steady_clock::now();
         evolution.eccentricity(&lat, &param, itmax, 0.0, 0);
-        dump_observables("obs.bin", lat, N);
-        dump_state("final", lat, N);
+        t_ecc = seconds_since(t0);
+        if (A.dumps) {
+            dump_observables("obs.bin", lat, N);
+            dump_state("final", lat, N);
+        }
     }
 
     std::ofstream js("harness.json");
@@ -346,6 +354,7 @@ int main(int argc, char **argv) {
        << (A.mode == "full" ? param.getEccentricity2() : 0.0)
        << ", \"newton_restart_draws\": " << restart_draws
        << ", \"t_setV\": " << t_setv << ", \"t_tau0\": " << t_tau0
-       << ", \"t_evolution\": " << t_evo << "}\n";
+       << ", \"t_evolution\": " << t_evo << ", \"t_eccentricity\": " << t_ecc
+       << "}\n";
     return 0;
 }
