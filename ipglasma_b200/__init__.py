@@ -107,6 +107,7 @@ _SIGNATURES = {
     "ipg_draw_device_noise": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int,
                                          ct.c_void_p]),
     "ipg_init_fields": (ct.c_int, [ct.c_void_p, ct.POINTER(_InitReport)]),
+    "ipg_init_from_wilson_lines": (ct.c_int, [ct.c_void_p, ct.POINTER(_InitReport)]),
     "ipg_run": (ct.c_int, [ct.c_void_p, ct.POINTER(_Result)]),
     "ipg_evolve": (ct.c_int, [ct.c_void_p, ct.c_int]),
     "ipg_get_observables": (ct.c_int, [ct.c_void_p] + [ct.c_void_p] * 4),
@@ -329,6 +330,14 @@ class Event:
         rep = _InitReport()
         allow = (3,) if allow_nonconverged else ()
         self._check(self._lib.ipg_init_fields(self._h, ct.byref(rep)), allow)
+        return InitReport(*(getattr(rep, f) for f, _ in _InitReport._fields_))
+
+    def init_from_wilson_lines(self, allow_nonconverged: bool = False) -> InitReport:
+        """tau = 0 Newton links and fields from Wilson lines loaded with
+        set_field(VA / VB) (the READFROMFILE path of Init::init)."""
+        rep = _InitReport()
+        allow = (3,) if allow_nonconverged else ()
+        self._check(self._lib.ipg_init_from_wilson_lines(self._h, ct.byref(rep)), allow)
         return InitReport(*(getattr(rep, f) for f, _ in _InitReport._fields_))
 
     def run(self) -> Result:

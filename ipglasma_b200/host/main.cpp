@@ -5,8 +5,9 @@
 // rules (Setup.cpp:24-104: keys and values alternate, the file ends with
 // EndOfFile, a missing key ends the program), derives dtau like main.cpp:531-534,
 // and for each event either
-//   - reads V_A, V_B from the binary Wilson-line files of
-//     readInitialWilsonLines = 2 (format of Init.cpp:1914-1973 / 2120-2296),
+//   - reads V_A, V_B from the Wilson-line files of readInitialWilsonLines
+//     = 1 (text, Init.cpp:1879-1911 / 2036-2114) or 2 (binary, Init.cpp:
+//     1914-1973 / 2120-2296),
 //   - or samples the two nuclei (Woods-Saxon with minimum distance, the
 //     algorithm of Init.cpp:2749-2816) on the host and builds the g^2 mu^2
 //     maps on the device (ipg_set_nuclei) from the nucleon thickness:
@@ -16,7 +17,7 @@
 //     (The reference's IP-Sat Q_s(T_p, y) table is not used.)
 // then runs the event on the GPU through the C ABI and writes the reference's
 // output files (writeOutputs 1, 4, 5) and, on request, the V files
-// (writeInitialWilsonLines = 2).
+// (writeInitialWilsonLines = 1 text or 2 binary).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -178,6 +179,57 @@ void write_vfile(const std::string &name, int N, double L, double y, const std::
             f.write((const char *)&V[18 * ((size_t)N * iy + ix)], 18 * sizeof(double));
 }
 
+// Text format of writeInitialWilsonLines = 1 (Init.cpp:1879-1911): per site
+// "ix iy" and the 9 entries as (re, im) pairs in column-major order
+// (Matrix::MatrixToString, Matrix.cpp:606-622), 15 significant digits, a
+// blank line after each ix row.
+void write_vtext(const std::string &name, int N, const std::vector<double> &V) {
+    FILE *f = std::fopen(name.c_str(), "w");
+    if (!f) {
+        std::cerr << "cannot write " << name << std::endl;
+        std::exit(1);
+    }
+    static const int colmajor[9] = {0, 3, 6, 1, 4, 7, 2, 5, 8};
+    for (int ix = 0; ix < N; ix++) {
+        for (int iy = 0; iy < N; iy++) {
+            const double *m = &V[18 * ((size_t)ix * N + iy)];
+            std::fprintf(f, "%d %d", ix, iy);
+            for (int k : colmajor) std::fprintf(f, " %.15g %.15g", m[2 * k], m[2 * k + 1]);
+            std::fputc('\n', f);
+        }
+        std::fputc('\n', f);
+    }
+    std::fclose(f);
+}
+
+// Text read of readInitialWilsonLines = 1 (Init.cpp:2036-2114): the entries
+// are taken in row-major order (so a file written by write_vtext comes back
+// transposed, as in the reference), and line i goes to ix = (int)((a i -+ b/2)
+// / a), truncated toward zero; rows with ix < 0 (nucleus A) or ix >= N
+// (nucleus B) are skipped, cells no line reaches keep the identity.
+bool read_vtext(const std::string &name, int N, double L, double shift, std::vector<double> &V) {
+    std::ifstream f(name.c_str());
+    if (!f) return false;
+    V.assign((size_t)18 * N * N, 0.0);
+    for (int k = 0; k < N * N; k++) V[18 * (size_t)k] = V[18 * (size_t)k + 8] = V[18 * (size_t)k + 16] = 1.0;
+    const double a = L / N;
+    double dummy, re[9], im[9];
+    for (int i = 0; i < N; i++) {
+        for (int j = 0; j < N; j++) {
+            f >> dummy >> dummy;
+            for (int k = 0; k < 9; k++) f >> re[k] >> im[k];
+            const int ix = (int)((a * i + shift) / a);
+            if (ix < 0 || ix >= N) continue;
+            double *m = &V[18 * ((size_t)ix * N + j)];
+            for (int k = 0; k < 9; k++) {
+                m[2 * k] = re[k];
+                m[2 * k + 1] = im[k];
+            }
+        }
+    }
+    return true;
+}
+
 bool read_vfile(const std::string &name, int N, double L, double shift, std::vector<double> &V) {
     std::ifstream f(name.c_str(), std::ios::in | std::ios::binary);
     if (!f) return false;
@@ -248,8 +300,10 @@ int main(int argc, char **argv) {
     const double rapidity = in.d("Rapidity");
     unsigned long long seed = in.ull("seed");
     if (in.i("useTimeForSeed") == 1) seed = std::random_device{}();
-    if ((readV != 0 && readV != 2) || (writeV != 0 && writeV != 2)) {
-        std::cerr << "only the binary Wilson-line format (2) is supported" << std::endl;
+    if (readV < 0 || readV > 2 || writeV < 0 || writeV > 2) {
+        std::cerr << "# Unknown Wilson-line format: readInitialWilsonLines " << readV
+                  << ", writeInitialWilsonLines " << writeV << " (supported: 0, 1 text, 2 binary)"
+                  << std::endl;
         return 1;
     }
     std::cout << "Random seed = " << seed << std::endl;
@@ -276,13 +330,17 @@ int main(int argc, char **argv) {
                         : (bmax - bmin) * xb + bmin;
         ipg_init_report rep;
         std::memset(&rep, 0, sizeof(rep));
-        if (readV == 2) {
+        if (readV != 0) {
             std::vector<double> VA, VB;
             std::ostringstream n1, n2;
             n1 << "V-" << event_id + 2 * seed;
             n2 << "V-" << event_id + (1 + 2 * seed);
-            if (!read_vfile(n1.str(), N, cfg.L, -b / 2., VA) ||
-                !read_vfile(n2.str(), N, cfg.L, b / 2., VB)) {
+            if (readV == 1) {
+                n1 << ".txt";
+                n2 << ".txt";
+            }
+            auto rd = readV == 1 ? read_vtext : read_vfile;
+            if (!rd(n1.str(), N, cfg.L, -b / 2., VA) || !rd(n2.str(), N, cfg.L, b / 2., VB)) {
                 std::cerr << "cannot read the Wilson-line files " << n1.str() << ", " << n2.str()
                           << std::endl;
                 return 1;
@@ -303,15 +361,21 @@ int main(int argc, char **argv) {
             check(ctx, ipg_reseed(ctx, seed * 1000003ULL + event_id), "ipg_reseed");
             check(ctx, ipg_use_device_noise(ctx), "ipg_use_device_noise");
             check(ctx, ipg_init_fields(ctx, &rep), "ipg_init_fields");
-            if (writeV == 2) {
+            if (writeV != 0) {
                 std::vector<double> V(18 * n);
                 std::ostringstream n1, n2;
                 n1 << "V-" << event_id + 2 * seed;
                 n2 << "V-" << event_id + (1 + 2 * seed);
+                if (writeV == 1) {
+                    n1 << ".txt";
+                    n2 << ".txt";
+                }
                 check(ctx, ipg_get_field(ctx, IPG_VA, V.data()), "ipg_get_field");
-                write_vfile(n1.str(), N, cfg.L, rapidity, V);
+                if (writeV == 1) write_vtext(n1.str(), N, V);
+                else write_vfile(n1.str(), N, cfg.L, rapidity, V);
                 check(ctx, ipg_get_field(ctx, IPG_VB, V.data()), "ipg_get_field");
-                write_vfile(n2.str(), N, cfg.L, rapidity, V);
+                if (writeV == 1) write_vtext(n2.str(), N, V);
+                else write_vfile(n2.str(), N, cfg.L, rapidity, V);
             }
         }
         ipg_result res;

@@ -111,3 +111,79 @@ def test_executable_samples_nuclei_on_its_own(tmp_path):
     for v in ("V-0", "V-1"):
         raw = (tmp_path / v).read_bytes()
         assert len(raw) == 4 + 4 + 3 * 8 + N * N * 18 * 8
+
+
+def _vtext(V: np.ndarray) -> str:
+    """The reference's text Wilson-line format (Init.cpp:1879-1911,
+    Matrix.cpp:606-622): ix iy and the entries column-major, 15 digits."""
+    N = int(round(np.sqrt(V.shape[0])))
+    out = []
+    for ix in range(N):
+        for iy in range(N):
+            m = V[ix * N + iy].reshape(3, 3)
+            vals = " ".join(f"{z.real:.15g} {z.imag:.15g}" for z in m.T.ravel())
+            out.append(f"{ix} {iy} {vals}\n")
+        out.append("\n")
+    return "".join(out)
+
+
+def _binary_v(path: Path, V: np.ndarray, N: int, L: float) -> None:
+    """Binary format (Init.cpp:1914-1973): record ix*N+iy holds cell N*iy+ix."""
+    with open(path, "wb") as f:
+        np.array([N, 3], dtype="<i4").tofile(f)
+        np.array([L, L / N, 0.0], dtype="<f8").tofile(f)
+        # record a*N + b holds the cell x = b, y = a
+        recs = np.ascontiguousarray(V.reshape(N, N, 9).transpose(1, 0, 2))
+        recs.view(np.float64).astype("<f8").tofile(f)
+
+
+def test_text_wilson_line_files(tmp_path):
+    """writeInitialWilsonLines 1 writes the reference's text format (the same
+    event's binary file gives the values), and readInitialWilsonLines 1 reads
+    it back the reference's way: entries row-major, i.e. transposed, so an
+    event read from text equals the event read from a binary file of the
+    transposed lines."""
+    if not EXE.exists():
+        pytest.skip("executable not built")
+    N, L, Ny, maxtime = 32, 6.0, 3, 0.2
+    base = INPUT.format(N=N, L=L, Ny=Ny, maxtime=maxtime).replace(
+        "readInitialWilsonLines 2", "readInitialWilsonLines 0").replace(
+        "useNucleus 0", "useNucleus 1").replace("bmax 0", "bmax 3").replace(
+        "seed 0", "seed 3")
+    runs = {}
+    for fmt in (1, 2):
+        d = tmp_path / f"w{fmt}"
+        d.mkdir()
+        (d / "input").write_text(base.replace("writeInitialWilsonLines 0",
+                                              f"writeInitialWilsonLines {fmt}"))
+        res = subprocess.run([str(EXE), "input"], cwd=d, capture_output=True, text=True,
+                             timeout=300)
+        assert res.returncode == 0, res.stderr
+        runs[fmt] = d
+    # binary lines of the same event (same seed: same nuclei, same noise)
+    def read_bin(p):
+        raw = np.fromfile(p, dtype=np.uint8)
+        vals = raw[32:].view("<f8").reshape(N, N, 9, 2)  # [ix record][iy] -> cell N*iy+ix
+        z = vals[..., 0] + 1j * vals[..., 1]
+        return np.ascontiguousarray(z.transpose(1, 0, 2)).reshape(N * N, 3, 3)
+    for k in (6, 7):  # V-(0 + 2 seed), V-(0 + 2 seed + 1)
+        V = read_bin(runs[2] / f"V-{k}")
+        assert (runs[1] / f"V-{k}.txt").read_text() == _vtext(V)
+    # read back: text (transposed on reading) == binary of the transposed lines
+    outs = {}
+    for fmt in (1, 2):
+        d = tmp_path / f"r{fmt}"
+        d.mkdir()
+        for k in (0, 1):
+            V = read_bin(runs[2] / f"V-{k + 6}")
+            if fmt == 1:
+                (d / f"V-{k}.txt").write_text(_vtext(V))
+            else:
+                _binary_v(d / f"V-{k}", V.transpose(0, 2, 1), N, L)
+        (d / "input").write_text(INPUT.format(N=N, L=L, Ny=Ny, maxtime=maxtime).replace(
+            "readInitialWilsonLines 2", f"readInitialWilsonLines {fmt}"))
+        res = subprocess.run([str(EXE), "input"], cwd=d, capture_output=True, text=True,
+                             timeout=300)
+        assert res.returncode == 0, res.stderr
+        outs[fmt] = (d / "epsilon-u-Hydro-TauHydro-0.dat").read_text()
+    assert outs[1] == outs[2]
