@@ -365,30 +365,39 @@ def launches_of(evs, batch) -> int:
     return sum(ev.kernel_launches() for ev in evs) + batch.stats()[2]
 
 
-def batch_errors(evs32, evs64) -> dict:
+def batch_errors(evs32, evs64, specs, r32, r64) -> dict:
     """FP32 bulk against FP64 on every event of a batch (same noise keys, so
-    the same FP64 initial conditions): the worst event of each figure."""
-    out = {}
-    for e32, e64 in zip(evs32, evs64):
+    the same FP64 initial conditions): per size class the median and the
+    worst event of each figure (e per cell over cells above 1% / 0.1% of the
+    event's max e, eps_2 and E_T relative), and the worst Gauss violation
+    and unitarity of each form."""
+    per = []
+    for e32, e64, spec, a, b in zip(evs32, evs64, specs, r32, r64):
         eps32, eps64 = e32.observables()[0], e64.observables()[0]
+        row = {"cls": f"{spec['nucleus']}{spec['N']}", "b": spec["b"]}
         for frac in (1e-2, 1e-3):
             m = eps64 > frac * eps64.max()
             rel = np.abs(eps32[m] - eps64[m]) / np.abs(eps64[m])
-            for key, v in ((f"e_rel_max_gt{frac:g}max", float(rel.max())),
-                           (f"e_rel_rms_gt{frac:g}max", float(np.sqrt(np.mean(rel ** 2))))):
-                out[key] = max(out.get(key, 0.0), v)
-    return out
-
-
-def result_errors(out: dict, r32, r64) -> dict:
-    for a, b in zip(r32, r64):
-        for key, v in (("eps2_rel", abs(a.eccentricity[1] - b.eccentricity[1])
-                        / abs(b.eccentricity[1])),
-                       ("E_T_rel", abs(a.E_T - b.E_T) / abs(b.E_T)),
-                       ("gauss_fp32", a.gauss_violation), ("gauss_fp64", b.gauss_violation),
-                       ("unitarity_fp32", a.unitarity_max), ("unitarity_fp64", b.unitarity_max)):
-            out[key] = max(out.get(key, 0.0), v)
-    out["events_compared"] = len(r32)
+            row[f"e_rel_max_gt{frac:g}max"] = float(rel.max())
+            row[f"e_rel_rms_gt{frac:g}max"] = float(np.sqrt(np.mean(rel ** 2)))
+        row["eps2_rel"] = abs(a.eccentricity[1] - b.eccentricity[1]) / abs(b.eccentricity[1])
+        row["eps2_abs"] = abs(a.eccentricity[1] - b.eccentricity[1])
+        row["E_T_rel"] = abs(a.E_T - b.E_T) / abs(b.E_T)
+        row["gauss_fp32"], row["gauss_fp64"] = a.gauss_violation, b.gauss_violation
+        row["unitarity_fp32"], row["unitarity_fp64"] = a.unitarity_max, b.unitarity_max
+        per.append(row)
+    keys = ["e_rel_rms_gt0.01max", "e_rel_max_gt0.01max", "e_rel_rms_gt0.001max",
+            "e_rel_max_gt0.001max", "eps2_rel", "eps2_abs", "E_T_rel"]
+    out = {}
+    for cls in sorted({r["cls"] for r in per}):
+        rows = [r for r in per if r["cls"] == cls]
+        out[cls] = {"events": len(rows),
+                    "median": {k: float(np.median([r[k] for r in rows])) for k in keys},
+                    "worst": {k: float(max(r[k] for r in rows)) for k in keys},
+                    "b_of_worst_eps2": float(max(rows, key=lambda r: r["eps2_rel"])["b"])}
+    for k in ("gauss_fp32", "gauss_fp64", "unitarity_fp32", "unitarity_fp64"):
+        out[k] = float(max(r[k] for r in per))
+    out["events_compared"] = len(per)
     return out
 
 
@@ -445,7 +454,7 @@ def measure_workload(torch, ipg, w, specs, K, W, key0, dist, clocks=None, e2e_st
     if dist:
         dist.barrier()
     r64 = batch_step(evs64, b64, key0 + 99999)
-    err = result_errors(batch_errors(evs32, evs64), r32, r64)
+    err = batch_errors(evs32, evs64, specs, r32, r64)
     stages = stage_rates(w, specs, evs64, key0)
     b32.close()
     b64.close()

@@ -337,8 +337,10 @@ ipg_status ipg_batch_tune(ipg_batch *batch, ipg_tune_report *report);
  * schedule of Evolution::run and compute its observables; results[count].
  * ms_evolution of each result is the batch's shared leapfrog time. */
 ipg_status ipg_batch_run(ipg_batch *batch, ipg_result *results);
-/* Set the launch shape by hand (variant < 3 for FP32, < 2 for FP64;
- * 1 <= blocks_per_sm <= what fits on an SM). */
+/* Set the launch shape by hand: variants 0, 1, 2 (FP32) or 0, 1 (FP64) are
+ * plain-load kernels on tiles of 2, 4 or 8 rows; variant 3 (FP32) or 2 (FP64)
+ * is the TMA tile kernel of the single-event form run over every event's
+ * tiles (1 block per SM); 1 <= blocks_per_sm <= what fits on an SM. */
 ipg_status ipg_batch_set_shape(ipg_batch *batch, int variant, int blocks_per_sm);
 ipg_status ipg_batch_stats(const ipg_batch *batch, double *ms_evolution,
                            double *ms_total, long long *launches);

@@ -1577,6 +1577,12 @@ struct ipg_batch {
     double last_ms_evolution = 0, last_ms_total = 0;
     long long launches = 0;
     bool tuned = false;
+    // TMA variant: tensor maps of every event for both U/phi buffer
+    // arrangements ([2 e + sel]); sel 0 holds the buffers that were the
+    // event's current ones when the batch was made (phys0)
+    LoadMaps *d_maps = nullptr;
+    std::vector<const void *> phys0;
+    double *d_status = nullptr;  // a TMA wait gave up
 };
 
 namespace {
@@ -1626,7 +1632,12 @@ int max_blocks(const ipg_batch *b, int variant) {
 }
 
 // variants the precision supports (FP64 needs <= 256 threads per block)
-int n_variants(const ipg_batch *b) { return b->fp32 ? kBatchVariants : 2; }
+int n_variants(const ipg_batch *b) {
+    return b->fp32 ? batch_variants<float>() : batch_variants<double>();
+}
+int tma_variant(const ipg_batch *b) {
+    return b->fp32 ? batch_plain_variants<float>() : batch_plain_variants<double>();
+}
 
 ipg_status upload_tiles(ipg_batch *b, int variant) {
     if (b->tiles_variant == variant) return IPG_OK;
@@ -1676,6 +1687,7 @@ void fill_table(ipg_batch *b, BatchEvent<T> *tab, int steps, bool full_first = f
             set_derived(d.cf);
             d.N = c->N;
             d.active = 1;
+            d.map_sel = s.ux == b->phys0[e] ? 0 : 1;
             std::swap(s.ux, uxb);
             std::swap(s.uy, uyb);
             std::swap(s.phi, phib);
@@ -1700,11 +1712,11 @@ ipg_status launch_batch(ipg_batch *b, int step) {
     if (b->fp32) {
         auto *t = static_cast<BatchEvent<float> *>(b->d_table) + (size_t)step * E;
         launch_leapfrog_batch<float>(t, E, b->d_tile_begin, b->total_tiles, b->variant, b->grid,
-                                     b->stream);
+                                     b->d_maps, b->d_status, b->stream);
     } else {
         auto *t = static_cast<BatchEvent<double> *>(b->d_table) + (size_t)step * E;
         launch_leapfrog_batch<double>(t, E, b->d_tile_begin, b->total_tiles, b->variant, b->grid,
-                                      b->stream);
+                                      b->d_maps, b->d_status, b->stream);
     }
     b->launches++;
     return IPG_OK;
@@ -1805,14 +1817,53 @@ ipg_status ipg_batch_create(ipg_ctx *const *events, int count, ipg_batch **out) 
     IPG_BCUDA(b, cudaMalloc(&b->d_table, table));
     IPG_BCUDA(b, cudaMallocHost(&b->h_table, table));
     IPG_BCUDA(b, cudaMalloc(&b->d_tile_begin, sizeof(int) * (count + 1)));
+    // tensor maps of both buffer arrangements of every event
+    {
+        std::vector<LoadMaps> maps(2 * (size_t)count);
+        bool ok = true;
+        for (int e = 0; e < count && ok; e++) {
+            ipg_ctx *c = b->ev[e];
+            if (b->fp32) {
+                State<float> s0 = c->s32, s1 = c->s32;
+                s1.ux = c->ux32b;
+                s1.uy = c->uy32b;
+                s1.phi = c->phi32b;
+                ok = encode_step_maps<float>(c->N, s0, &maps[2 * e]) &&
+                     encode_step_maps<float>(c->N, s1, &maps[2 * e + 1]);
+                b->phys0.push_back(c->s32.ux);
+            } else {
+                State<double> s0 = c->s64, s1 = c->s64;
+                s1.ux = c->ux64b;
+                s1.uy = c->uy64b;
+                s1.phi = c->phi64b;
+                ok = encode_step_maps<double>(c->N, s0, &maps[2 * e]) &&
+                     encode_step_maps<double>(c->N, s1, &maps[2 * e + 1]);
+                b->phys0.push_back(c->s64.ux);
+            }
+        }
+        IPG_BCUDA(b, cudaMalloc(&b->d_status, sizeof(double)));
+        IPG_BCUDA(b, cudaMemsetAsync(b->d_status, 0, sizeof(double), b->stream));
+        if (ok) {
+            IPG_BCUDA(b, cudaMalloc(&b->d_maps, sizeof(LoadMaps) * maps.size()));
+            IPG_BCUDA(b, cudaMemcpyAsync(b->d_maps, maps.data(), sizeof(LoadMaps) * maps.size(),
+                                         cudaMemcpyHostToDevice, b->stream));
+        }
+        IPG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    }
     const auto it = tune_cache().find(tune_key(b));
     if (it != tune_cache().end()) {
         b->variant = it->second.first;
         b->blocks_per_sm = it->second.second;
         b->tuned = true;
     } else {
-        b->variant = 1;
-        b->blocks_per_sm = max_blocks(b, b->variant);
+        // the TMA tile kernel when the maps and the descriptors fit, else the
+        // plain-load kernel with 4-row tiles
+        b->variant = tma_variant(b);
+        b->blocks_per_sm = b->d_maps ? max_blocks(b, b->variant) : 0;
+        if (b->blocks_per_sm < 1) {
+            b->variant = 1;
+            b->blocks_per_sm = max_blocks(b, b->variant);
+        }
     }
     if (b->blocks_per_sm < 1) return bfail(b, IPG_ERR_CUDA, "batched kernel cannot be resident");
     b->grid = b->blocks_per_sm * b->sms;
@@ -1828,6 +1879,8 @@ ipg_status ipg_batch_destroy(ipg_batch *b) {
     if (b->d_table) cudaFree(b->d_table);
     if (b->h_table) cudaFreeHost(b->h_table);
     if (b->d_tile_begin) cudaFree(b->d_tile_begin);
+    if (b->d_maps) cudaFree(b->d_maps);
+    if (b->d_status) cudaFree(b->d_status);
     if (b->e0) cudaEventDestroy(b->e0);
     if (b->e1) cudaEventDestroy(b->e1);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -1915,7 +1968,7 @@ ipg_status ipg_batch_tune(ipg_batch *b, ipg_tune_report *rep) {
     double best = 1e30;
     int best_v = b->variant, best_bps = b->blocks_per_sm, candidates = 0;
     for (int v = 0; v < n_variants(b); v++) {
-        const int maxb = max_blocks(b, v);
+        const int maxb = (v == tma_variant(b) && !b->d_maps) ? 0 : max_blocks(b, v);
         for (int bps = 1; bps <= maxb; bps++) {
             b->variant = v;
             b->blocks_per_sm = bps;
@@ -1984,6 +2037,7 @@ ipg_status ipg_batch_run(ipg_batch *b, ipg_result *results) {
                                  cudaMemcpyHostToDevice, b->stream));
     if (!b->exec || b->graph_variant != b->variant || b->graph_grid != b->grid)
         IPG_TRY(capture_graph(b));
+    IPG_BCUDA(b, cudaMemsetAsync(b->d_status, 0, sizeof(double), b->stream));
     IPG_BCUDA(b, cudaEventRecord(b->e0, b->stream));
     IPG_BCUDA(b, cudaGraphLaunch(b->exec, b->stream));
     b->launches += b->itmax;
@@ -1992,6 +2046,10 @@ ipg_status ipg_batch_run(ipg_batch *b, ipg_result *results) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, b->e0, b->e1);
     b->last_ms_evolution = ms;
+    double gave_up = 0.;
+    IPG_BCUDA(b, cudaMemcpy(&gave_up, b->d_status, sizeof(double), cudaMemcpyDeviceToHost));
+    if (gave_up != 0.)
+        return bfail(b, IPG_ERR_TIMEOUT, "a batched leapfrog step gave up waiting for its tiles");
     if (b->fp32)
         apply_swaps<float>(b, b->itmax);
     else
@@ -2025,7 +2083,7 @@ ipg_status ipg_batch_run(ipg_batch *b, ipg_result *results) {
 
 ipg_status ipg_batch_set_shape(ipg_batch *b, int variant, int blocks_per_sm) {
     if (!b) return IPG_ERR_BAD_CONFIG;
-    if (variant < 0 || variant >= n_variants(b))
+    if (variant < 0 || variant >= n_variants(b) || (variant == tma_variant(b) && !b->d_maps))
         return bfail(b, IPG_ERR_BAD_CONFIG, "variant %d not available", variant);
     const int maxb = max_blocks(b, variant);
     if (blocks_per_sm < 1 || blocks_per_sm > maxb)

@@ -871,10 +871,6 @@ static_assert(STAGE % 128 == 0, "stage alignment");
 static_assert(SMEM <= 227 * 1024, "shared memory per block");
 }  // namespace tile
 
-// tensor maps of the six fields for one step's loads
-struct LoadMaps {
-    CUtensorMap ux, uy, phi, e1, e2, pi;
-};
 
 // 32-bit shared-memory accesses by address: one value per instruction, so
 // each lands directly in its lane of a packed pair
@@ -1047,32 +1043,96 @@ __device__ __forceinline__ void fill_warp_halo(unsigned char *st, int r, int lan
     }
 }
 
-__global__ void __launch_bounds__(256, 1)
-    k_leapfrog_tile(const __grid_constant__ LoadMaps maps, int N, StepCoef<float> cf,
-                    double *status, uint32_t imag, State<float> gs, C<float> *ux_out,
-                    C<float> *uy_out, float *phi_out) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    // 128-byte aligned start, kept as an offset into the shared array so that
-    // accesses through it stay shared-memory accesses
-    const uint32_t pad = (128u - (smem_addr(smem_raw) & 127u)) & 127u;
-    unsigned char *smem = smem_raw + pad;
+// Where the tiles of a persistent FP32 tile loop come from: one event
+// (tensor maps in the kernel's parameter space) or a batch of events (tile
+// lists concatenated, per-event descriptors in shared memory and tensor maps
+// in global memory).
+struct OneEventTiles {
+    const LoadMaps *maps;
+    int N;
+    StepCoef<float> cf;
+    State<float> gs;
+    C<float> *ux_out, *uy_out;
+    float *phi_out;
+    int total;
+    __device__ __forceinline__ int find(int) const { return 0; }
+    __device__ __forceinline__ int first_tile(int) const { return 0; }
+    __device__ __forceinline__ int n_of(int) const { return N; }
+    __device__ __forceinline__ const LoadMaps *maps_of(int) const { return maps; }
+    static constexpr bool kGlobalMaps = false;
+    __device__ __forceinline__ bool active(int) const { return true; }
+    __device__ __forceinline__ const StepCoef<float> &cf_of(int) const { return cf; }
+    __device__ __forceinline__ const State<float> &state_of(int) const { return gs; }
+    __device__ __forceinline__ C<float> *ux_out_of(int) const { return ux_out; }
+    __device__ __forceinline__ C<float> *uy_out_of(int) const { return uy_out; }
+    __device__ __forceinline__ float *phi_out_of(int) const { return phi_out; }
+};
+
+struct BatchTiles {
+    const BatchEvent<float> *ev;  // shared memory
+    const int *begin;             // shared memory, [n_events + 1]
+    int n_events;
+    const LoadMaps *maps;         // global memory, [2 n_events]
+    int total;
+    // last e with begin[e] <= t
+    __device__ __forceinline__ int find(int t) const {
+        int lo = 0, hi = n_events - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (begin[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        return lo;
+    }
+    __device__ __forceinline__ int first_tile(int e) const { return begin[e]; }
+    __device__ __forceinline__ int n_of(int e) const { return ev[e].N; }
+    __device__ __forceinline__ const LoadMaps *maps_of(int e) const {
+        return maps + 2 * e + ev[e].map_sel;
+    }
+    static constexpr bool kGlobalMaps = true;
+    __device__ __forceinline__ bool active(int e) const { return ev[e].active != 0; }
+    __device__ __forceinline__ const StepCoef<float> &cf_of(int e) const { return ev[e].cf; }
+    __device__ __forceinline__ const State<float> &state_of(int e) const { return ev[e].s; }
+    __device__ __forceinline__ C<float> *ux_out_of(int e) const { return ev[e].ux_out; }
+    __device__ __forceinline__ C<float> *uy_out_of(int e) const { return ev[e].uy_out; }
+    __device__ __forceinline__ float *phi_out_of(int e) const { return ev[e].phi_out; }
+};
+
+// The persistent FP32 tile loop. smem: two stages (128-byte aligned) then
+// four barriers. Tile t of the list belongs to event find(t); its local index
+// gives (tx, ty) in that event's N/8 x N/32 tile grid.
+template <class Tiles>
+__device__ __forceinline__ void tile32_loop(const Tiles &T, unsigned char *smem, double *status,
+                                            uint32_t imag) {
     const uint32_t sbase = smem_addr(smem);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + 2 * tile::STAGE);
     uint64_t *empty = full + 2;
-    const int tiles_y = N / tile::Cn, tiles_x = N / tile::R, tiles = tiles_x * tiles_y;
     const int tid = threadIdx.x, r = tid >> 5, c = tid & 31;
-    const size_t n = (size_t)N * N;
+    const int tiles = T.total;
+    const LoadMaps *fenced = nullptr;  // thread 0: the maps acquired last
 
     auto issue = [&](int t, int s) {
-        const int iy0 = (t % tiles_y) * tile::Cn, ix0 = (t / tiles_y) * tile::R;
+        const int e = T.find(t);
+        const int N = T.n_of(e), tiles_y = N / tile::Cn, local = t - T.first_tile(e);
+        const int iy0 = (local % tiles_y) * tile::Cn, ix0 = (local / tiles_y) * tile::R;
+        const LoadMaps *m = T.maps_of(e);
+        if (Tiles::kGlobalMaps && m != fenced) {
+            fence_map_acquire(&m->ux);
+            fence_map_acquire(&m->uy);
+            fence_map_acquire(&m->phi);
+            fence_map_acquire(&m->e1);
+            fence_map_acquire(&m->e2);
+            fence_map_acquire(&m->pi);
+            fenced = m;
+        }
         unsigned char *st = smem + s * tile::STAGE;
         mbar_arrive_expect_tx(&full[s], tile::TX_BYTES);
-        tma_load_3d(st + tile::UX, &maps.ux, iy0 - 2, ix0 - 1, 0, &full[s]);
-        tma_load_3d(st + tile::UY, &maps.uy, iy0 - 2, ix0 - 1, 0, &full[s]);
-        tma_load_3d(st + tile::PHI, &maps.phi, iy0 - 4, ix0 - 1, 0, &full[s]);
-        tma_load_3d(st + tile::E1, &maps.e1, iy0, ix0, 0, &full[s]);
-        tma_load_3d(st + tile::E2, &maps.e2, iy0, ix0, 0, &full[s]);
-        tma_load_3d(st + tile::PI, &maps.pi, iy0, ix0, 0, &full[s]);
+        tma_load_3d(st + tile::UX, &m->ux, iy0 - 2, ix0 - 1, 0, &full[s]);
+        tma_load_3d(st + tile::UY, &m->uy, iy0 - 2, ix0 - 1, 0, &full[s]);
+        tma_load_3d(st + tile::PHI, &m->phi, iy0 - 4, ix0 - 1, 0, &full[s]);
+        tma_load_3d(st + tile::E1, &m->e1, iy0, ix0, 0, &full[s]);
+        tma_load_3d(st + tile::E2, &m->e2, iy0, ix0, 0, &full[s]);
+        tma_load_3d(st + tile::PI, &m->pi, iy0, ix0, 0, &full[s]);
     };
 
     if (tid == 0) {
@@ -1081,9 +1141,12 @@ __global__ void __launch_bounds__(256, 1)
         mbar_init(&empty[0], tile::R);  // one arrival per warp
         mbar_init(&empty[1], tile::R);
         fence_barrier_init();
-        prefetch_map(&maps.ux);
-        prefetch_map(&maps.uy);
-        prefetch_map(&maps.phi);
+        if (!Tiles::kGlobalMaps) {
+            const LoadMaps *m = T.maps_of(0);
+            prefetch_map(&m->ux);
+            prefetch_map(&m->uy);
+            prefetch_map(&m->phi);
+        }
         if (blockIdx.x < tiles) issue(blockIdx.x, 0);
         if (blockIdx.x + gridDim.x < tiles) issue(blockIdx.x + gridDim.x, 1);
     }
@@ -1098,27 +1161,36 @@ __global__ void __launch_bounds__(256, 1)
             break;
         }
         unsigned char *st = smem + s * tile::STAGE;
-        const int ty = t % tiles_y, tx = t / tiles_y;
+        const int e = T.find(t);
+        const int N = T.n_of(e), tiles_y = N / tile::Cn, tiles_x = N / tile::R;
+        const int local = t - T.first_tile(e);
+        const int ty = local % tiles_y, tx = local / tiles_y;
         const bool top = tx == 0, bottom = tx == tiles_x - 1;
         const bool left = ty == 0, right = ty == tiles_y - 1;
         const bool edge = top || bottom || left || right;
-        if (edge) {
+        const bool act = T.active(e);
+        if (edge && act) {
             fill_warp_halo(st, r, c, top, bottom, left, right);
             __syncwarp();
         }
+        const size_t n = (size_t)N * N;
         const size_t pos = (size_t)(tx * tile::R + r) * N + ty * tile::Cn + c;
-        const PairLoadTile ld(sbase + (uint32_t)(s * tile::STAGE), r, c, imag, gs, pos, n);
+        const StepCoef<float> &cf = T.cf_of(e);
         M3<P2> nu;
         H3<float> phin;
-        leapfrog_pair_core(ld, cf, nu, phin);
+        if (act) {
+            const PairLoadTile ld(sbase + (uint32_t)(s * tile::STAGE), r, c, imag, T.state_of(e),
+                                  pos, n);
+            leapfrog_pair_core(ld, cf, nu, phin);
+        }
         // this warp is done with the stage (its halo writes ordered before the
         // TMA unit writes the stage again)
-        if (edge) fence_async_smem();
+        if (edge && act) fence_async_smem();
         __syncwarp();
         if (c == 0) mbar_arrive(&empty[s]);
-        if (cf.do_pu) {
-            st_m3_pair(ux_out, uy_out, pos, n, nu);
-            st_h(phi_out, pos, n, phin);
+        if (act && cf.do_pu) {
+            st_m3_pair(T.ux_out_of(e), T.uy_out_of(e), pos, n, nu);
+            st_h(T.phi_out_of(e), pos, n, phin);
         }
         if (tid == 0 && t + 2 * (int)gridDim.x < tiles) {
             if (!mbar_wait_bounded(&empty[s], use, tile::MAX_POLLS)) {
@@ -1128,6 +1200,43 @@ __global__ void __launch_bounds__(256, 1)
             issue(t + 2 * gridDim.x, s);
         }
     }
+}
+
+__global__ void __launch_bounds__(256, 1)
+    k_leapfrog_tile(const __grid_constant__ LoadMaps maps, int N, StepCoef<float> cf,
+                    double *status, uint32_t imag, State<float> gs, C<float> *ux_out,
+                    C<float> *uy_out, float *phi_out) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    // 128-byte aligned start, kept as an offset into the shared array so that
+    // accesses through it stay shared-memory accesses
+    const uint32_t pad = (128u - (smem_addr(smem_raw) & 127u)) & 127u;
+    const OneEventTiles T{&maps, N, cf, gs, ux_out, uy_out, phi_out,
+                          (N / tile::R) * (N / tile::Cn)};
+    tile32_loop(T, smem_raw + pad, status, imag);
+}
+
+// The FP32 batch over the TMA tiles: the descriptors of this step and the
+// tile prefix sums are copied to shared memory behind the two stages.
+__global__ void __launch_bounds__(256, 1)
+    k_leapfrog_tile_batch(const BatchEvent<float> *__restrict__ evs, int n_events,
+                          const int *__restrict__ tile_begin, int total_tiles,
+                          const LoadMaps *__restrict__ maps, double *status, uint32_t imag) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const uint32_t pad = (128u - (smem_addr(smem_raw) & 127u)) & 127u;
+    unsigned char *smem = smem_raw + pad;
+    BatchEvent<float> *s_ev =
+        reinterpret_cast<BatchEvent<float> *>(smem + 2 * tile::STAGE + 64);
+    int *s_begin = reinterpret_cast<int *>(s_ev + n_events);
+    {
+        const int words = n_events * (int)(sizeof(BatchEvent<float>) / sizeof(int));
+        const int *src = reinterpret_cast<const int *>(evs);
+        int *dst = reinterpret_cast<int *>(s_ev);
+        for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
+    }
+    for (int e = threadIdx.x; e <= n_events; e += blockDim.x) s_begin[e] = tile_begin[e];
+    __syncthreads();
+    const BatchTiles T{s_ev, s_begin, n_events, maps, total_tiles};
+    tile32_loop(T, smem, status, imag);
 }
 
 // ---------------------------------------------------------------------------
@@ -1230,34 +1339,42 @@ struct FullLoadTile64 {
     __device__ __forceinline__ void put_pi(const H3<double> &h) const { st_h(g.pi, pos, n, h); }
 };
 
-// (128, 1): ptxas then fits the site in 190 registers without spilling (with
-// a stated minimum of 2 blocks it used 255 and spilled), and two blocks per SM
-// still fit in registers and shared memory
-__global__ void __launch_bounds__(128, 1)
-    k_leapfrog_tile64(const __grid_constant__ LoadMaps maps, int N, StepCoef<double> cf,
-                      double *status, State<double> s, C<double> *ux_out, C<double> *uy_out,
-                      double *phi_out) {
+// One 4 x 32 tile of the FP64 step: load the stage, wait, clamp the halo on
+// edge tiles, advance the tile's sites. tx, ty: the tile in the event's
+// N/4 x N/32 grid.
+template <bool GLOBAL_MAPS>
+__device__ __forceinline__ void tile64_body(const LoadMaps *maps, int N, int tx, int ty,
+                                            const StepCoef<double> &cf, double *status,
+                                            const State<double> &s, C<double> *ux_out,
+                                            C<double> *uy_out, double *phi_out) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const uint32_t pad = (128u - (smem_addr(smem_raw) & 127u)) & 127u;
     unsigned char *smem = smem_raw + pad;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + tile64::STAGE);
     int *abort_flag = reinterpret_cast<int *>(full + 1);
     const int tiles_y = N / tile64::Cn, tiles_x = N / tile64::R;
-    const int ty = blockIdx.x % tiles_y, tx = blockIdx.x / tiles_y;
     const int iy0 = ty * tile64::Cn, ix0 = tx * tile64::R;
     const int tid = threadIdx.x, r = tid >> 5, c = tid & 31;
     if (tid == 0) {
         mbar_init(full, 1);
         *abort_flag = 0;
         fence_barrier_init();
+        if (GLOBAL_MAPS) {
+            fence_map_acquire(&maps->ux);
+            fence_map_acquire(&maps->uy);
+            fence_map_acquire(&maps->phi);
+            fence_map_acquire(&maps->e1);
+            fence_map_acquire(&maps->e2);
+            fence_map_acquire(&maps->pi);
+        }
         mbar_arrive_expect_tx(full, tile64::TX_BYTES);
         // links as pairs of 8-byte words: column iy0-1 is word 2 (iy0 - 1)
-        tma_load_3d(smem + tile64::UX, &maps.ux, 2 * (iy0 - 1), ix0 - 1, 0, full);
-        tma_load_3d(smem + tile64::UY, &maps.uy, 2 * (iy0 - 1), ix0 - 1, 0, full);
-        tma_load_3d(smem + tile64::PHI, &maps.phi, iy0 - 2, ix0 - 1, 0, full);
-        tma_load_3d(smem + tile64::E1, &maps.e1, iy0, ix0, 0, full);
-        tma_load_3d(smem + tile64::E2, &maps.e2, iy0, ix0, 0, full);
-        tma_load_3d(smem + tile64::PI, &maps.pi, iy0, ix0, 0, full);
+        tma_load_3d(smem + tile64::UX, &maps->ux, 2 * (iy0 - 1), ix0 - 1, 0, full);
+        tma_load_3d(smem + tile64::UY, &maps->uy, 2 * (iy0 - 1), ix0 - 1, 0, full);
+        tma_load_3d(smem + tile64::PHI, &maps->phi, iy0 - 2, ix0 - 1, 0, full);
+        tma_load_3d(smem + tile64::E1, &maps->e1, iy0, ix0, 0, full);
+        tma_load_3d(smem + tile64::E2, &maps->e2, iy0, ix0, 0, full);
+        tma_load_3d(smem + tile64::PI, &maps->pi, iy0, ix0, 0, full);
     }
     __syncthreads();
     if (!mbar_wait_bounded(full, 0, tile::MAX_POLLS)) *abort_flag = 1;
@@ -1286,6 +1403,39 @@ __global__ void __launch_bounds__(128, 1)
         st_m3(ux_out, pos, n, nx);
         st_m3(uy_out, pos, n, ny);
     }
+}
+
+// (128, 1): ptxas then fits the site in 190 registers without spilling (with
+// a stated minimum of 2 blocks it used 255 and spilled), and two blocks per SM
+// still fit in registers and shared memory
+__global__ void __launch_bounds__(128, 1)
+    k_leapfrog_tile64(const __grid_constant__ LoadMaps maps, int N, StepCoef<double> cf,
+                      double *status, State<double> s, C<double> *ux_out, C<double> *uy_out,
+                      double *phi_out) {
+    const int tiles_y = N / tile64::Cn;
+    tile64_body<false>(&maps, N, blockIdx.x / tiles_y, blockIdx.x % tiles_y, cf, status, s,
+                       ux_out, uy_out, phi_out);
+}
+
+// The FP64 batch over the TMA tiles: one block per 4 x 32 tile of the
+// concatenated tile lists; the block reads its event's descriptor and tensor
+// maps from global memory.
+__global__ void __launch_bounds__(128, 1)
+    k_leapfrog_tile64_batch(const BatchEvent<double> *__restrict__ evs, int n_events,
+                            const int *__restrict__ tile_begin, const LoadMaps *__restrict__ maps,
+                            double *status) {
+    const int t = blockIdx.x;
+    int lo = 0, hi = n_events - 1;  // last e with tile_begin[e] <= t
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(tile_begin + mid) <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    const BatchEvent<double> &E = evs[lo];
+    if (!E.active) return;
+    const int N = E.N, tiles_y = N / tile64::Cn, local = t - __ldg(tile_begin + lo);
+    tile64_body<true>(maps + 2 * lo + E.map_sel, N, local / tiles_y, local % tiles_y, E.cf,
+                      status, E.s, E.ux_out, E.uy_out, E.phi_out);
 }
 
 // ---------------------------------------------------------------------------
@@ -1344,8 +1494,16 @@ size_t batch_smem(int n_events) {
     return sizeof(BatchEvent<T>) * n_events + sizeof(int) * (n_events + 1);
 }
 
+// shared memory of the FP32 TMA batch kernel: two stages, the barriers, the
+// descriptors and tile prefix sums, alignment slack
+size_t tile_batch_smem(int n_events) {
+    return 2 * (size_t)tile::STAGE + 64 + batch_smem<float>(n_events) + 128;
+}
+
+
 template <typename T>
 int batch_tile_rows(int variant) {
+    if (variant == batch_plain_variants<T>()) return sizeof(T) == 4 ? tile::R : tile64::R;
     return variant == 0 ? 2 : (variant == 1 ? 4 : 8);
 }
 
@@ -1361,6 +1519,22 @@ const void *batch_kernel(int variant) {
 template <typename T>
 int batch_max_blocks_per_sm(int variant, int n_events) {
     int nb = 0;
+    if (variant == batch_plain_variants<T>()) {
+        if constexpr (sizeof(T) == 4) {
+            const size_t smem = tile_batch_smem(n_events);
+            if (smem > 227 * 1024) return 0;  // too many events for the descriptors
+            cudaFuncSetAttribute(k_leapfrog_tile_batch,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_leapfrog_tile_batch, 256, smem);
+            return nb > 1 ? 1 : nb;  // persistent: one block per SM
+        } else {
+            cudaFuncSetAttribute(k_leapfrog_tile64_batch,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, tile64::SMEM);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_leapfrog_tile64_batch, 128,
+                                                          tile64::SMEM);
+            return nb > 0 ? 1 : 0;  // one block per tile: the grid is the tile count
+        }
+    }
     const int threads = 32 * batch_tile_rows<T>(variant);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<T>(variant), threads,
                                                   batch_smem<T>(n_events));
@@ -1369,7 +1543,20 @@ int batch_max_blocks_per_sm(int variant, int n_events) {
 
 template <typename T>
 void launch_leapfrog_batch(const BatchEvent<T> *d_evs, int n_events, const int *d_tile_begin,
-                           int total_tiles, int variant, int grid, cudaStream_t st) {
+                           int total_tiles, int variant, int grid, const LoadMaps *d_maps,
+                           double *status, cudaStream_t st) {
+    if (variant == batch_plain_variants<T>()) {
+        if constexpr (sizeof(T) == 4) {
+            const size_t smem = tile_batch_smem(n_events);
+            // imag = 4: the byte offset of a link's imaginary part
+            k_leapfrog_tile_batch<<<grid < total_tiles ? grid : total_tiles, 256, smem, st>>>(
+                d_evs, n_events, d_tile_begin, total_tiles, d_maps, status, 4u);
+        } else {
+            k_leapfrog_tile64_batch<<<total_tiles, 128, tile64::SMEM, st>>>(
+                d_evs, n_events, d_tile_begin, d_maps, status);
+        }
+        return;
+    }
     const size_t smem = batch_smem<T>(n_events);
     switch (variant) {
         case 0:
@@ -1392,9 +1579,9 @@ template int batch_tile_rows<double>(int);
 template int batch_max_blocks_per_sm<float>(int, int);
 template int batch_max_blocks_per_sm<double>(int, int);
 template void launch_leapfrog_batch<float>(const BatchEvent<float> *, int, const int *, int,
-                                           int, int, cudaStream_t);
+                                           int, int, const LoadMaps *, double *, cudaStream_t);
 template void launch_leapfrog_batch<double>(const BatchEvent<double> *, int, const int *, int,
-                                            int, int, cudaStream_t);
+                                            int, int, const LoadMaps *, double *, cudaStream_t);
 
 template <typename T>
 void launch_leapfrog_site(const EventGeom *d_ev, int N, const State<T> &s,
@@ -1423,6 +1610,33 @@ bool encode_tiled_3d(CUtensorMap *map, void *base, CUtensorMapDataType type, siz
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+template <>
+bool encode_step_maps<float>(int N, const State<float> &s, LoadMaps *m) {
+    using namespace tile;
+    const uint64_t n = (uint64_t)N;
+    const auto U64 = CU_TENSOR_MAP_DATA_TYPE_UINT64, U32 = CU_TENSOR_MAP_DATA_TYPE_UINT32;
+    return encode_tiled_3d(&m->ux, s.ux, U64, 8, n, n, 9, UC, UR, 9) &&
+           encode_tiled_3d(&m->uy, s.uy, U64, 8, n, n, 9, UC, UR, 9) &&
+           encode_tiled_3d(&m->phi, s.phi, U32, 4, n, n, 9, PC, PR, 9) &&
+           encode_tiled_3d(&m->e1, s.e1, U32, 4, n, n, 8, Cn, R, 8) &&
+           encode_tiled_3d(&m->e2, s.e2, U32, 4, n, n, 8, Cn, R, 8) &&
+           encode_tiled_3d(&m->pi, s.pi, U32, 4, n, n, 9, Cn, R, 9);
+}
+
+template <>
+bool encode_step_maps<double>(int N, const State<double> &s, LoadMaps *m) {
+    using namespace tile64;
+    const uint64_t n = (uint64_t)N;
+    const auto U64 = CU_TENSOR_MAP_DATA_TYPE_UINT64;
+    // a complex link entry is two 8-byte words
+    return encode_tiled_3d(&m->ux, s.ux, U64, 8, 2 * n, n, 9, 2 * UC, UR, 9) &&
+           encode_tiled_3d(&m->uy, s.uy, U64, 8, 2 * n, n, 9, 2 * UC, UR, 9) &&
+           encode_tiled_3d(&m->phi, s.phi, U64, 8, n, n, 9, PC, PR, 9) &&
+           encode_tiled_3d(&m->e1, s.e1, U64, 8, n, n, 8, Cn, R, 8) &&
+           encode_tiled_3d(&m->e2, s.e2, U64, 8, n, n, 8, Cn, R, 8) &&
+           encode_tiled_3d(&m->pi, s.pi, U64, 8, n, n, 9, Cn, R, 9);
+}
+
 namespace {
 
 // The FP32 form's step kernel: the TMA-staged tile kernel unless
@@ -1441,16 +1655,8 @@ bool launch_leapfrog_tile(int N, const State<float> &s, C<float> *ux_out, C<floa
                           float *phi_out, const StepCoef<float> &cf, double *status,
                           cudaStream_t st) {
     using namespace tile;
-    const uint64_t n = (uint64_t)N;
-    const auto U64 = CU_TENSOR_MAP_DATA_TYPE_UINT64, U32 = CU_TENSOR_MAP_DATA_TYPE_UINT32;
     LoadMaps m;
-    const bool ok = encode_tiled_3d(&m.ux, s.ux, U64, 8, n, n, 9, UC, UR, 9) &&
-                    encode_tiled_3d(&m.uy, s.uy, U64, 8, n, n, 9, UC, UR, 9) &&
-                    encode_tiled_3d(&m.phi, s.phi, U32, 4, n, n, 9, PC, PR, 9) &&
-                    encode_tiled_3d(&m.e1, s.e1, U32, 4, n, n, 8, Cn, R, 8) &&
-                    encode_tiled_3d(&m.e2, s.e2, U32, 4, n, n, 8, Cn, R, 8) &&
-                    encode_tiled_3d(&m.pi, s.pi, U32, 4, n, n, 9, Cn, R, 9);
-    if (!ok) return false;
+    if (!encode_step_maps<float>(N, s, &m)) return false;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1476,17 +1682,8 @@ bool launch_leapfrog_tile64(int N, const State<double> &s, C<double> *ux_out, C<
                             double *phi_out, const StepCoef<double> &cf, double *status,
                             cudaStream_t st) {
     using namespace tile64;
-    const uint64_t n = (uint64_t)N;
-    const auto U64 = CU_TENSOR_MAP_DATA_TYPE_UINT64;
     LoadMaps m;
-    // a complex link entry is two 8-byte words
-    const bool ok = encode_tiled_3d(&m.ux, s.ux, U64, 8, 2 * n, n, 9, 2 * UC, UR, 9) &&
-                    encode_tiled_3d(&m.uy, s.uy, U64, 8, 2 * n, n, 9, 2 * UC, UR, 9) &&
-                    encode_tiled_3d(&m.phi, s.phi, U64, 8, n, n, 9, PC, PR, 9) &&
-                    encode_tiled_3d(&m.e1, s.e1, U64, 8, n, n, 8, Cn, R, 8) &&
-                    encode_tiled_3d(&m.e2, s.e2, U64, 8, n, n, 8, Cn, R, 8) &&
-                    encode_tiled_3d(&m.pi, s.pi, U64, 8, n, n, 9, Cn, R, 9);
-    if (!ok) return false;
+    if (!encode_step_maps<double>(N, s, &m)) return false;
     cudaFuncSetAttribute(k_leapfrog_tile64, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
     k_leapfrog_tile64<<<(N / R) * (N / Cn), 128, SMEM, st>>>(m, N, cf, status, s, ux_out, uy_out,
                                                                phi_out);

@@ -1,6 +1,7 @@
 // Internal declarations shared by the CUDA translation units of the library.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -66,19 +67,46 @@ struct BatchEvent {
     StepCoef<T> cf;
     int N;
     int active;
+    int map_sel;  // which of the event's two tensor-map sets holds s (U/phi buffer parity)
 };
 
-// Tile-shape variants of the batched kernel: variant v advances tiles of
-// 32 x batch_tile_rows(v) sites with 64 * rows threads.
-constexpr int kBatchVariants = 3;
+// Tensor maps of the six input fields of one step (the TMA tile kernels)
+struct LoadMaps {
+    CUtensorMap ux, uy, phi, e1, e2, pi;
+};
+// the maps of the TMA tile kernels of precision T (FP32: 8 x 32 tiles, FP64:
+// 4 x 32 tiles) for a lattice of N x N sites with the given field planes;
+// false if the driver rejects them
+template <typename T>
+bool encode_step_maps(int N, const State<T> &s, LoadMaps *out);
+template <>
+bool encode_step_maps<float>(int N, const State<float> &s, LoadMaps *out);
+template <>
+bool encode_step_maps<double>(int N, const State<double> &s, LoadMaps *out);
+
+// Tile-shape variants of the batched kernel: variant v < batch_plain_variants
+// advances tiles of 32 x batch_tile_rows(v) sites with plain loads, one
+// thread per site; the last variant (v = batch_plain_variants) runs the TMA
+// tile kernel of the single-event form over the concatenated tile lists,
+// with per-event tensor maps (d_maps[2 e + map_sel]).
+template <typename T>
+constexpr int batch_plain_variants() {
+    return sizeof(T) == 4 ? 3 : 2;
+}
+template <typename T>
+constexpr int batch_variants() {
+    return batch_plain_variants<T>() + 1;
+}
 template <typename T>
 int batch_tile_rows(int variant);
 template <typename T>
 int batch_max_blocks_per_sm(int variant, int n_events);
-// tile_begin[n_events + 1]: prefix sums of (N/32) (N/rows) per event
+// tile_begin[n_events + 1]: prefix sums of (N/32) (N/rows) per event;
+// status (TMA variant): set to 1 if a bounded wait gave up
 template <typename T>
 void launch_leapfrog_batch(const BatchEvent<T> *d_evs, int n_events, const int *d_tile_begin,
-                           int total_tiles, int variant, int grid, cudaStream_t st);
+                           int total_tiles, int variant, int grid, const LoadMaps *d_maps,
+                           double *status, cudaStream_t st);
 
 // ---- initial conditions -------------------------------------------------
 

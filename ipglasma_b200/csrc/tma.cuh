@@ -105,6 +105,14 @@ __device__ __forceinline__ void bulk_wait_all() {
     asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
+// a tensor map in global memory (written by the host before the launch) is
+// acquired by the tensor-map proxy before the first copy through it
+__device__ __forceinline__ void fence_map_acquire(const CUtensorMap *map) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(
+                     reinterpret_cast<uint64_t>(map))
+                 : "memory");
+}
+
 __device__ __forceinline__ void prefetch_map(const CUtensorMap *map) {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }

@@ -175,11 +175,15 @@ def test_text_wilson_line_files(tmp_path):
         d = tmp_path / f"r{fmt}"
         d.mkdir()
         for k in (0, 1):
-            V = read_bin(runs[2] / f"V-{k + 6}")
+            # the values the text file holds (15 significant digits)
+            txt = _vtext(read_bin(runs[2] / f"V-{k + 6}"))
             if fmt == 1:
-                (d / f"V-{k}.txt").write_text(_vtext(V))
+                (d / f"V-{k}.txt").write_text(txt)
             else:
-                _binary_v(d / f"V-{k}", V.transpose(0, 2, 1), N, L)
+                rows = np.array([l.split()[2:] for l in txt.splitlines() if l], dtype=float)
+                z = (rows[:, 0::2] + 1j * rows[:, 1::2]).reshape(-1, 3, 3)  # column-major
+                # the reader takes them row-major: the transpose of the matrix written
+                _binary_v(d / f"V-{k}", z, N, L)
         (d / "input").write_text(INPUT.format(N=N, L=L, Ny=Ny, maxtime=maxtime).replace(
             "readInitialWilsonLines 2", f"readInitialWilsonLines {fmt}"))
         res = subprocess.run([str(EXE), "input"], cwd=d, capture_output=True, text=True,

@@ -24,9 +24,31 @@ def blobs_event(N=32, L=6.0, Ny=3, **kw):
     return ev
 
 
-def test_nan_in_host_noise_is_reported():
-    """A NaN in the caller's noise spreads through the Poisson solve into
-    every field; ipg_run reports IPG_ERR_NAN instead of returning numbers."""
+def test_nan_in_the_fields_is_reported():
+    """A NaN in a field the caller loads (ipg_set_field) spreads through the
+    evolution into e; ipg_run reports IPG_ERR_NAN instead of returning
+    numbers."""
+    N = 32
+    with blobs_event(N, seed=5) as ev:
+        ev.use_device_noise()
+        ev.init_fields()
+        state = {f: ev.get_field(f) for f in (ipg.UX, ipg.UY, ipg.E1, ipg.E2, ipg.PHI, ipg.PI)}
+    state[ipg.PI][N * N // 2 + N // 2, 0, 0] = np.nan
+    with ipg.Event(ipg.Config(size=N, L=6.0, Ny=3, maxtime=0.2)) as ev:
+        for f, v in state.items():
+            ev.set_field(f, v)
+        ev.mark_initialized()
+        with pytest.raises(ipg.IPGError) as exc:
+            ev.run()
+        assert exc.value.status == NAN
+        assert "non-finite" in str(exc.value)
+
+
+def test_nan_in_the_noise_is_absorbed_like_the_reference():
+    """A NaN in the colour-charge noise reaches the exponent of a Wilson-line
+    sheet, where the reference's exponential maps NaN coefficients to 0
+    (Matrix.cpp:416-424): that sheet's factor is the identity wherever the
+    NaN spread, the fields stay finite and the run completes."""
     N, Ny = 32, 3
     rng = np.random.default_rng(5)
     xa = rng.standard_normal(Ny * N * N * 8)
@@ -35,10 +57,9 @@ def test_nan_in_host_noise_is_reported():
     with blobs_event(N, Ny=Ny) as ev:
         ev.set_noise(xa, xb)
         ev.init_fields(allow_nonconverged=True)
-        with pytest.raises(ipg.IPGError) as exc:
-            ev.run()
-        assert exc.value.status == NAN
-        assert "non-finite" in str(exc.value)
+        assert np.all(np.isfinite(ev.get_field(ipg.VA)))
+        res = ev.run()
+        assert np.isfinite(res.E_T)
 
 
 def test_newton_iteration_limit_reports_nonconverged_with_fields_set():
@@ -70,7 +91,8 @@ def test_converged_run_has_no_failures():
         rep = ev.init_fields()
         assert rep.newton_failed == 0
         _, status = ev.newton_iterations()
-        assert np.all(status == 0)
+        # 0: converged, 1: converged after a random restart
+        assert np.all((status == 0) | (status == 1))
 
 
 def test_device_noise_is_the_noise_the_wilson_lines_use():
