@@ -220,7 +220,8 @@ def main():
                     help="skip the single 512^2 event (tile kernels) measurement")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint (forward/backward) measurement")
-    ap.add_argument("--profile", choices=["fp32", "fp64", "both", "adjoint"], default=None,
+    ap.add_argument("--profile", choices=["fp32", "fp64", "both", "adjoint", "batch32",
+                                          "batch64"], default=None,
                     help="run one warm-up and one timed event per form and exit "
                          "(the command profiled under ncu)")
     ap.add_argument("--profile-n", type=int, default=512,
@@ -241,6 +242,21 @@ def run_profile(which, local):
     import ipglasma_b200 as ipg
 
     torch.cuda.set_device(local)
+    if which in ("batch32", "batch64"):
+        # the headline batch (64 O+O 256^2 + 16 Pb+Pb 512^2) on the TMA tile
+        # variant, no tuner: initial conditions, then two batched runs
+        prec = ipg.FP32 if which == "batch32" else ipg.FP64
+        w = HEADLINE
+        specs = job_events(w, 1)
+        evs, _, b = build_batch(ipg, w, specs, prec, 900)
+        b.set_shape(3 if prec == ipg.FP32 else 2, 1)
+        for k in range(2):
+            batch_step(evs, b, 900 + 1000 * k)
+        print(f"batch {which}: evolution ms {b.stats()[0]:.2f}")
+        b.close()
+        for ev in evs:
+            ev.close()
+        return
     if which == "adjoint":
         # the adjoint workload's event (Au+Au 256^2, Ny 50) over 40 steps, every
         # state kept (1.5 GB): one forward and one backward

@@ -187,6 +187,39 @@ struct NucleiArgs {
 };
 void launch_g2mu_from_nucleons(const NucleiArgs &a, cudaStream_t st);
 
+// IP-Sat maps of both nuclei (nuclei.cu): nucleon thickness, saturation-scale
+// table, fluctuating-x fixed point
+struct IpsatArgs {
+    int N;
+    double L, a, g;
+    double BG;                 // nucleon width, GeV^-2
+    double xi;                 // proton anisotropy
+    double nuclei_in_average;  // averageOverNuclei
+    double ratioA, ratioB;     // QsmuRatio of A and B
+    double rapidity, roots, xfactor, rmax;
+    int fluct_x;               // useFluctuatingx
+    int nA, nB;
+    const double *nucA, *nucB;  // [n][4]: x, y (shifted by -+b/2), phi, Q_s normalisation
+    int nT, ny;
+    double dy;
+    const double *Tlist;  // [nT]
+    const double *qs2;    // [nT][ny]
+    double *TA, *TB;      // [N*N] thickness, GeV^2
+    double *g2A, *g2B;    // [N*N] g^2 mu^2, lattice units
+    double *yB;           // [N*N] B's final rapidity
+    int *inside, *prev;   // [N*N]
+    int *row_last;        // [N]
+    int *flags;           // bit 0: y beyond table, 1: T beyond table, 2: no convergence,
+                          // 3: a start rapidity < 0 (run the sequential pass)
+};
+// sequential = false: the parallel passes; true: both fixed points again in
+// the single-threaded site order (after the parallel passes flagged bit 3)
+void launch_ipsat(const IpsatArgs &a, bool sequential, cudaStream_t st);
+// partial[296][8] sums of the event averages; colA/colB: [n][3] x, y (shifted),
+// collided flag of each nucleon; r_cut = sqrt(0.1 sigma_NN / pi) fm
+void launch_ipsat_averages(const IpsatArgs &a, const double *colA, const double *colB,
+                           double r_cut, double *partial, cudaStream_t st);
+
 // ---- observables ----------------------------------------------------------
 
 struct TmunuArgs {
