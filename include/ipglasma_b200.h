@@ -140,6 +140,61 @@ ipg_status ipg_set_g2mu_device(ipg_ctx *ctx, const double *d_g2mu2A,
  * Init::setColorChargeDensity (Init.cpp:753-1676) for that map. */
 ipg_status ipg_set_nuclei(ipg_ctx *ctx, const double *xyzA, int nA, const double *xyzB, int nB,
                           double b, double BG, double QsMax, double QsmuRatio);
+/* IP-Sat colour-charge maps: the parameters of Init::setColorChargeDensity
+ * (Init.cpp:753-1676) that this path reads (the reference's input keys in
+ * brackets). */
+typedef struct {
+    double BG;                /* nucleon width B_G, GeV^-2 (BG) */
+    double QsmuRatio;         /* Q_s / g^2 mu of nucleus A (QsmuRatio) */
+    double QsmuRatioB;        /* of nucleus B; the reference sets it to QsmuRatio */
+    double proton_anisotropy; /* xi of the elliptic nucleon (protonAnisotropy); 0: round */
+    double rapidity;          /* y (Rapidity) */
+    double roots;             /* sqrt(s), GeV (roots) */
+    double x_factor;          /* x = factor Q_s / sqrt(s) e^{-y} (xFromThisFactorTimesQs) */
+    double rmax;              /* nucleon cut-off radius, fm (rmax) */
+    double sigmaNN;           /* inelastic NN cross section, mb (SigmaNN) */
+    int use_fluctuating_x;    /* 1: Q_s at the x of the site's own Q_s (useFluctuatingx) */
+    int average_over_nuclei;  /* T divided by this (averageOverNuclei), >= 1 */
+} ipg_ipsat_params;
+
+/* What setColorChargeDensity reports about the event (Init.cpp:1117-1217,
+ * 1423-1530). */
+typedef struct {
+    int Npart, Ncoll;       /* hard-sphere wounding with d^2 < sigma_NN / (10 pi) */
+    double Tpp;             /* sum of T_A T_B a^2, fm^-2 */
+    double average_Qs;      /* GeV, over the cells near collided nucleons of both nuclei:
+                               sqrt of the mean of max(Q_sA^2, Q_sB^2) */
+    double average_Qs_avg;  /* sqrt of the mean of (Q_sA^2 + Q_sB^2) / 2 */
+    double average_Qs_min;  /* sqrt of the mean of min(Q_sA^2, Q_sB^2) */
+    double Qs2min_ST;       /* sum over all cells of min(Q_sA^2, Q_sB^2) a^2 / hbarc^2 */
+    int overlap_cells;      /* cells counted in the means */
+    int flags;              /* bit 0: y beyond the table, 1: T beyond the table (its
+                               last row used), 2: a fixed point did not converge in
+                               1000 steps, 3: the single-threaded order was needed */
+} ipg_ipsat_report;
+
+/* g^2 mu^2 of both nuclei from nucleon positions with the reference's IP-Sat
+ * construction, on the device: T_A, T_B as sums of nucleon Gaussians
+ * (Init.cpp:1009-1106; optional per-nucleon angle phi and Q_s normalisation,
+ * NULL for 0 and 1), then at cells within rmax of both nuclei Q_s^2 from
+ * the table Q_s^2(T, y) (Init::getNuclearQs2, Init.cpp:686-749: Tlist[nT]
+ * increasing, qs2[nT][ny] at y = k dy) with the fluctuating-x fixed point
+ * (Init.cpp:1219-1410), and g^2 mu^2 = Q_s^2 / QsmuRatio^2 a^2/hbarc^2/g^2.
+ * xyz[3 n] in fm (z unused), nucleus A shifted by -b/2 and B by +b/2 along x.
+ * The fixed point of nucleus A starts from the rapidity nucleus B ended on
+ * at the previous cell, as in the reference's loop run on one thread. The
+ * table is the reference's qs2Adj_vs_Tp_vs_Y_200.in (readNuclearQs,
+ * Init.cpp:441-480: nT = 200, ny = 44, dy = 0.25). rep may be NULL. */
+ipg_status ipg_set_nuclei_ipsat(ipg_ctx *ctx, const double *xyzA, int nA, const double *xyzB,
+                                int nB, const double *phiA, const double *phiB,
+                                const double *normA, const double *normB, double b,
+                                const ipg_ipsat_params *params, const double *Tlist,
+                                const double *qs2, int nT, int ny, double dy,
+                                ipg_ipsat_report *rep);
+/* The nucleon thickness maps T_A, T_B ([N*N], GeV^2) of the last
+ * ipg_set_nuclei_ipsat. */
+ipg_status ipg_get_thickness(ipg_ctx *ctx, double *TA, double *TB);
+
 /* Copy the current g^2 mu^2 maps ([N*N] each, lattice units) to the host. */
 ipg_status ipg_get_g2mu(ipg_ctx *ctx, double *g2mu2A, double *g2mu2B);
 

@@ -27,7 +27,7 @@ from pathlib import Path
 
 import numpy as np
 
-__all__ = ["Config", "Event", "Batch", "IPGError", "lib", "FP64", "FP32",
+__all__ = ["Config", "Event", "Batch", "IPGError", "lib", "FP64", "FP32", "read_qs_table",
            "UX", "UY", "E1", "E2", "PHI", "PI", "VA", "VB", "HBARC"]
 
 HBARC = 0.1973269718  # GeV fm, Phys_consts.h
@@ -69,6 +69,24 @@ class _InitReport(ct.Structure):
     ]
 
 
+class _IpsatParams(ct.Structure):
+    _fields_ = [
+        ("BG", ct.c_double), ("QsmuRatio", ct.c_double), ("QsmuRatioB", ct.c_double),
+        ("proton_anisotropy", ct.c_double), ("rapidity", ct.c_double), ("roots", ct.c_double),
+        ("x_factor", ct.c_double), ("rmax", ct.c_double), ("sigmaNN", ct.c_double),
+        ("use_fluctuating_x", ct.c_int), ("average_over_nuclei", ct.c_int),
+    ]
+
+
+class _IpsatReport(ct.Structure):
+    _fields_ = [
+        ("Npart", ct.c_int), ("Ncoll", ct.c_int), ("Tpp", ct.c_double),
+        ("average_Qs", ct.c_double), ("average_Qs_avg", ct.c_double),
+        ("average_Qs_min", ct.c_double), ("Qs2min_ST", ct.c_double),
+        ("overlap_cells", ct.c_int), ("flags", ct.c_int),
+    ]
+
+
 class _TuneReport(ct.Structure):
     _fields_ = [
         ("variant", ct.c_int), ("tile_rows", ct.c_int), ("threads_per_block", ct.c_int),
@@ -102,6 +120,12 @@ _SIGNATURES = {
     "ipg_set_nuclei": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int,
                                   ct.c_double, ct.c_double, ct.c_double, ct.c_double]),
     "ipg_get_g2mu": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "ipg_set_nuclei_ipsat": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int,
+                                        ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                        ct.c_double, ct.POINTER(_IpsatParams), ct.c_void_p,
+                                        ct.c_void_p, ct.c_int, ct.c_int, ct.c_double,
+                                        ct.POINTER(_IpsatReport)]),
+    "ipg_get_thickness": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "ipg_set_noise_device": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "ipg_use_device_noise": (ct.c_int, [ct.c_void_p]),
     "ipg_draw_device_noise": (ct.c_int, [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int,
@@ -229,6 +253,14 @@ class Result:
     ms_observables: float = 0.0
 
 
+def read_qs_table(path, ny: int = 44):
+    """The reference's Q_s^2(T, y) table file (qs2Adj_vs_Tp_vs_Y_200.in,
+    read by Init::readNuclearQs, Init.cpp:441-480): records "y T Qs^2", ny
+    rapidities per T, T increasing. Returns (Tlist[nT], qs2[nT][ny])."""
+    rec = np.loadtxt(path).reshape(-1, ny, 3)
+    return rec[:, 0, 1].copy(), rec[:, :, 2].copy()
+
+
 class Event:
     """One event on one GPU (an ``ipg_ctx``)."""
 
@@ -293,6 +325,41 @@ class Event:
         bb = np.ascontiguousarray(xyzB, dtype=np.float64).reshape(-1, 3)
         self._check(self._lib.ipg_set_nuclei(self._h, _ptr(a), len(a), _ptr(bb), len(bb), b, BG,
                                              qs_max, qsmu_ratio))
+
+    def set_nuclei_ipsat(self, xyzA, xyzB, b: float, table, *, BG: float = 4.0,
+                         QsmuRatio: float = 0.8, QsmuRatioB: float | None = None,
+                         proton_anisotropy: float = 0.0, rapidity: float = 0.0,
+                         roots: float = 5020.0, x_factor: float = 0.5, rmax: float = 3.0,
+                         sigmaNN: float = 70.0, use_fluctuating_x: bool = True,
+                         average_over_nuclei: int = 1, phiA=None, phiB=None, normA=None,
+                         normB=None, dy: float = 0.25) -> dict:
+        """IP-Sat g2mu maps from nucleon positions ((A, 3) arrays in fm) and the
+        Q_s^2(T, y) table, given as (Tlist[nT], qs2[nT][ny]) with y = k dy
+        (the layout of the reference's qs2Adj_vs_Tp_vs_Y_200.in; see
+        :func:`read_qs_table`). Returns the event report as a dict."""
+        a = np.ascontiguousarray(xyzA, dtype=np.float64).reshape(-1, 3)
+        bb = np.ascontiguousarray(xyzB, dtype=np.float64).reshape(-1, 3)
+        Tlist = np.ascontiguousarray(table[0], dtype=np.float64)
+        qs2 = np.ascontiguousarray(table[1], dtype=np.float64)
+        if qs2.ndim != 2 or qs2.shape[0] != Tlist.size:
+            raise ValueError("table: qs2 must be (len(Tlist), ny)")
+        opt = [None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+               for v in (phiA, phiB, normA, normB)]
+        p = _IpsatParams(BG, QsmuRatio, QsmuRatio if QsmuRatioB is None else QsmuRatioB,
+                         proton_anisotropy, rapidity, roots, x_factor, rmax, sigmaNN,
+                         int(use_fluctuating_x), average_over_nuclei)
+        rep = _IpsatReport()
+        self._check(self._lib.ipg_set_nuclei_ipsat(
+            self._h, _ptr(a), len(a), _ptr(bb), len(bb),
+            *[_ptr(v) if v is not None else None for v in opt], b, ct.byref(p), _ptr(Tlist),
+            _ptr(qs2), Tlist.size, qs2.shape[1], dy, ct.byref(rep)))
+        return {f: getattr(rep, f) for f, _ in _IpsatReport._fields_}
+
+    def thickness(self):
+        """T_A, T_B (2, N*N) in GeV^2 of the last set_nuclei_ipsat."""
+        out = np.empty((2, self.n))
+        self._check(self._lib.ipg_get_thickness(self._h, _ptr(out[0]), _ptr(out[1])))
+        return out
 
     def g2mu(self):
         """The current g2mu maps (2, N*N), lattice units."""

@@ -60,6 +60,15 @@ struct ipg_ctx {
     double *amp = nullptr;
     double2 *work = nullptr, *work2 = nullptr;
     double *nuc_xyz = nullptr, *nuc_gx = nullptr, *nuc_gy = nullptr;  // ipg_set_nuclei
+    struct {  // ipg_set_nuclei_ipsat (allocated by its first call)
+        double *TA = nullptr, *TB = nullptr, *yB = nullptr;
+        int *inside = nullptr, *prev = nullptr, *row_last = nullptr, *flags = nullptr;
+        double *nuc = nullptr, *col = nullptr;  // nucleons of A then B
+        int nuc_cap = 0;
+        double *table = nullptr;
+        size_t table_cap = 0;
+        bool have_T = false;
+    } ips;
     int nuc_cap = 0;
     int work_sheets = 0;
     C<double> *VA = nullptr, *VB = nullptr;
@@ -738,6 +747,170 @@ ipg_status ipg_set_nuclei(ipg_ctx *c, const double *xyzA, int nA, const double *
     IPG_TRY(sync(c));  // the positions buffer is reused for the second nucleus
     c->have_g2mu = true;
     return IPG_OK;
+}
+
+ipg_status ipg_set_nuclei_ipsat(ipg_ctx *c, const double *xyzA, int nA, const double *xyzB,
+                                int nB, const double *phiA, const double *phiB,
+                                const double *normA, const double *normB, double b,
+                                const ipg_ipsat_params *p, const double *Tlist,
+                                const double *qs2, int nT, int ny, double dy,
+                                ipg_ipsat_report *rep) {
+    if (!c || !xyzA || !xyzB || nA < 1 || nB < 1 || !p || !Tlist || !qs2)
+        return IPG_ERR_BAD_CONFIG;
+    if (nT < 2 || ny < 2 || !(dy > 0) || !(p->BG > 0) || !(p->QsmuRatio > 0) ||
+        !(p->QsmuRatioB > 0) || !(p->roots > 0) || p->average_over_nuclei < 1)
+        return fail(c, IPG_ERR_BAD_CONFIG, "IP-Sat parameters or table shape out of range");
+    for (int i = 0; i + 1 < nT; i++)
+        if (!(Tlist[i] < Tlist[i + 1]))
+            return fail(c, IPG_ERR_BAD_CONFIG, "the T column of the table must increase");
+    const size_t n = c->n;
+    auto &S = c->ips;
+    if (!S.TA) {
+        IPG_TRY(dalloc(c, &S.TA, n));
+        IPG_TRY(dalloc(c, &S.TB, n));
+        IPG_TRY(dalloc(c, &S.yB, n));
+        IPG_TRY(dalloc(c, &S.inside, n));
+        IPG_TRY(dalloc(c, &S.prev, n));
+        IPG_TRY(dalloc(c, &S.row_last, (size_t)c->N));
+        IPG_TRY(dalloc(c, &S.flags, 1));
+    }
+    if (nA + nB > S.nuc_cap) {
+        IPG_TRY(dalloc(c, &S.nuc, 4 * (size_t)(nA + nB)));
+        IPG_TRY(dalloc(c, &S.col, 3 * (size_t)(nA + nB)));
+        S.nuc_cap = nA + nB;
+    }
+    const size_t tsz = (size_t)nT + (size_t)nT * ny;
+    if (tsz > S.table_cap) {
+        IPG_TRY(dalloc(c, &S.table, tsz));
+        S.table_cap = tsz;
+    }
+    // nucleon positions shifted by -+ b/2 along x (Init.cpp:855-864, reaction
+    // plane not rotated); wounding with d^2 < sigma_NN / (10 pi) fm^2
+    // (Init.cpp:1125-1141, 1196-1200)
+    std::vector<double> nuc(4 * (size_t)(nA + nB)), col(3 * (size_t)(nA + nB));
+    std::vector<int> hit(nA + nB, 0);
+    for (int k = 0; k < nA + nB; k++) {
+        const bool isB = k >= nA;
+        const int i = isB ? k - nA : k;
+        const double *xyz = isB ? xyzB : xyzA;
+        nuc[4 * k] = isB ? xyz[3 * i] + b / 2. : xyz[3 * i] - b / 2.;
+        nuc[4 * k + 1] = xyz[3 * i + 1];
+        nuc[4 * k + 2] = isB ? (phiB ? phiB[i] : 0.) : (phiA ? phiA[i] : 0.);
+        nuc[4 * k + 3] = isB ? (normB ? normB[i] : 1.) : (normA ? normA[i] : 1.);
+    }
+    const double d2 = p->sigmaNN / (M_PI * 10.);
+    int Ncoll = 0;
+    for (int i = 0; i < nA; i++)
+        for (int j = 0; j < nB; j++) {
+            const double dx = nuc[4 * (nA + j)] - nuc[4 * i];
+            const double dyy = nuc[4 * (nA + j) + 1] - nuc[4 * i + 1];
+            if (dx * dx + dyy * dyy < d2) {
+                Ncoll++;
+                hit[i] = hit[nA + j] = 1;
+            }
+        }
+    if (nA == 1 && nB == 1) hit[0] = hit[1] = 1;  // p+p: collided in any case
+    int Npart = 0;
+    for (int k = 0; k < nA + nB; k++) {
+        Npart += hit[k];
+        col[3 * k] = nuc[4 * k];
+        col[3 * k + 1] = nuc[4 * k + 1];
+        col[3 * k + 2] = hit[k];
+    }
+    IPG_CUDA(c, cudaMemcpyAsync(S.nuc, nuc.data(), sizeof(double) * nuc.size(),
+                                cudaMemcpyHostToDevice, c->stream));
+    IPG_CUDA(c, cudaMemcpyAsync(S.col, col.data(), sizeof(double) * col.size(),
+                                cudaMemcpyHostToDevice, c->stream));
+    IPG_CUDA(c, cudaMemcpyAsync(S.table, Tlist, sizeof(double) * nT, cudaMemcpyHostToDevice,
+                                c->stream));
+    IPG_CUDA(c, cudaMemcpyAsync(S.table + nT, qs2, sizeof(double) * nT * ny,
+                                cudaMemcpyHostToDevice, c->stream));
+    IPG_CUDA(c, cudaMemsetAsync(S.flags, 0, sizeof(int), c->stream));
+    IpsatArgs a;
+    a.N = c->N;
+    a.L = c->cfg.L;
+    a.a = c->a;
+    a.g = c->cfg.g;
+    a.BG = p->BG;
+    a.xi = p->proton_anisotropy;
+    a.nuclei_in_average = (double)p->average_over_nuclei;
+    a.ratioA = p->QsmuRatio;
+    a.ratioB = p->QsmuRatioB;
+    a.rapidity = p->rapidity;
+    a.roots = p->roots;
+    a.xfactor = p->x_factor;
+    a.rmax = p->rmax;
+    a.fluct_x = p->use_fluctuating_x;
+    a.nA = nA;
+    a.nB = nB;
+    a.nucA = S.nuc;
+    a.nucB = S.nuc + 4 * (size_t)nA;
+    a.nT = nT;
+    a.ny = ny;
+    a.dy = dy;
+    a.Tlist = S.table;
+    a.qs2 = S.table + nT;
+    a.TA = S.TA;
+    a.TB = S.TB;
+    a.g2A = c->g2mu2A;
+    a.g2B = c->g2mu2B;
+    a.yB = S.yB;
+    a.inside = S.inside;
+    a.prev = S.prev;
+    a.row_last = S.row_last;
+    a.flags = S.flags;
+    launch_ipsat(a, false, c->stream);
+    IPG_LAUNCHED(c, a.fluct_x ? 5 : 2);
+    int flags = 0;
+    IPG_CUDA(c, cudaMemcpyAsync(&flags, S.flags, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    IPG_TRY(sync(c));
+    if (flags & 8) {
+        // a fixed point started from a negative rapidity, where the reference
+        // carries Q_s from the previous cell: redo both in the sequential order
+        launch_ipsat(a, true, c->stream);
+        IPG_LAUNCHED(c, 1);
+        IPG_CUDA(c, cudaMemcpyAsync(&flags, S.flags, sizeof(int), cudaMemcpyDeviceToHost,
+                                    c->stream));
+        IPG_TRY(sync(c));
+    }
+    S.have_T = true;
+    c->have_g2mu = true;
+    if (rep) {
+        launch_ipsat_averages(a, S.col, S.col + 3 * (size_t)nA,
+                              std::sqrt(0.1 * p->sigmaNN / M_PI), c->partial, c->stream);
+        IPG_LAUNCHED(c, 1);
+        std::vector<double> part(296 * 8);
+        IPG_CUDA(c, cudaMemcpyAsync(part.data(), c->partial, sizeof(double) * part.size(),
+                                    cudaMemcpyDeviceToHost, c->stream));
+        IPG_TRY(sync(c));
+        double sum[8] = {0};
+        for (int blk = 0; blk < 296; blk++)
+            for (int k = 0; k < 8; k++) sum[k] += part[8 * blk + k];
+        const double cnt = sum[4];
+        std::memset(rep, 0, sizeof(*rep));
+        rep->Npart = Npart;
+        rep->Ncoll = Ncoll;
+        rep->Tpp = sum[6];
+        rep->average_Qs = cnt > 0 ? std::sqrt(sum[1] / cnt) : 0.;
+        rep->average_Qs_avg = cnt > 0 ? std::sqrt(sum[3] / cnt) : 0.;
+        rep->average_Qs_min = cnt > 0 ? std::sqrt(sum[2] / cnt) : 0.;
+        rep->Qs2min_ST = sum[5] * c->a * c->a / kHbarc / kHbarc;
+        rep->overlap_cells = (int)cnt;
+        rep->flags = flags;
+    }
+    return IPG_OK;
+}
+
+ipg_status ipg_get_thickness(ipg_ctx *c, double *TA, double *TB) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (!c->ips.have_T) return fail(c, IPG_ERR_STATE, "no IP-Sat maps set");
+    if (TA)
+        IPG_CUDA(c, cudaMemcpyAsync(TA, c->ips.TA, sizeof(double) * c->n, cudaMemcpyDeviceToHost,
+                                    c->stream));
+    if (TB)
+        IPG_CUDA(c, cudaMemcpyAsync(TB, c->ips.TB, sizeof(double) * c->n, cudaMemcpyDeviceToHost,
+                                    c->stream));
+    return sync(c);
 }
 
 ipg_status ipg_get_g2mu(ipg_ctx *c, double *g2mu2A, double *g2mu2B) {

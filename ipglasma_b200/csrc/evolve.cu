@@ -657,6 +657,16 @@ __device__ __forceinline__ H3<T> transport_bwd_minus(const M3<T> &u, const H3<T>
 // ---------------------------------------------------------------------------
 namespace {
 
+// traceless part of a packed pair: (d0 + d1 + d2) / 3 as a product with the
+// rounded 1/3 (an IEEE division per lane costs a range check and, for tiny
+// traces, a slow-path call)
+__device__ __forceinline__ void h_traceless(H3<P2> &h) {
+    const P2 t = (h.d0 + h.d1 + h.d2) * P2(1.f / 3.f);
+    h.d0 -= t;
+    h.d1 -= t;
+    h.d2 -= t;
+}
+
 // lane x from px at ix, lane y from py at iy
 __device__ __forceinline__ M3<P2> ld_m3_pair(const C<float> *__restrict__ px, size_t ix,
                                              const C<float> *__restrict__ py, size_t iy,

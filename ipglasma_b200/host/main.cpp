@@ -13,8 +13,10 @@
 //     maps on the device (ipg_set_nuclei) from the nucleon thickness:
 //     T_A = sum of Gaussians of width BG (GeV^-2), and
 //     Q_s(x) = QsMax sqrt(T_A(x)/max T_A) with QsMax from the optional key
-//     QsMax (default 1.5 GeV), g^2 mu^2 a^2 = Q_s^2/QsmuRatio^2 a^2/(hbar c)^2/g^2.
-//     (The reference's IP-Sat Q_s(T_p, y) table is not used.)
+//     QsMax (default 1.5 GeV), g^2 mu^2 a^2 = Q_s^2/QsmuRatio^2 a^2/(hbar c)^2/g^2;
+//     or, when the input names an existing NucleusQsTableFileName, the
+//     reference's IP-Sat construction from that Q_s(T_p, y) table
+//     (ipg_set_nuclei_ipsat: fluctuating x, rmax cut, hard-sphere wounding).
 // then runs the event on the GPU through the C ABI and writes the reference's
 // output files (writeOutputs 1, 4, 5) and, on request, the V files
 // (writeInitialWilsonLines = 1 text or 2 binary).
@@ -259,6 +261,28 @@ bool read_vfile(const std::string &name, int N, double L, double shift, std::vec
     return true;
 }
 
+// The Q_s^2(T, y) table of readNuclearQs (Init.cpp:441-480): records
+// "y T Q_s^2", ny = 44 rapidities 0.25 apart per T, nT = 200 values of T.
+bool read_qs_table(const std::string &name, std::vector<double> &Tlist, std::vector<double> &qs2,
+                   int nT = 200, int ny = 44) {
+    std::ifstream f(name.c_str());
+    if (!f) return false;
+    Tlist.assign(nT, 0.0);
+    qs2.assign((size_t)nT * ny, 0.0);
+    double y, T, q;
+    for (int iT = 0; iT < nT; iT++)
+        for (int iy = 0; iy < ny; iy++) {
+            if (!(f >> y >> T >> q)) {
+                std::cerr << " End of file reached prematurely. Did the file change? Exiting."
+                          << std::endl;
+                std::exit(1);
+            }
+            Tlist[iT] = T;
+            qs2[(size_t)iT * ny + iy] = q;
+        }
+    return true;
+}
+
 void check(ipg_ctx *ctx, ipg_status st, const char *what) {
     if (st == IPG_OK) return;
     std::cerr << what << " failed (" << st << "): " << ipg_last_error(ctx) << std::endl;
@@ -297,6 +321,31 @@ int main(int argc, char **argv) {
     const int linearb = in.i("samplebFromLinearDistribution");
     const double BG = in.d("BG"), QsmuRatio = in.d("QsmuRatio");
     const double QsMax = in.d_or("QsMax", 1.5);
+    // the IP-Sat Q_s(T, y) table when the input names one that exists,
+    // else the Q_s ~ sqrt(T_A) map with QsMax
+    std::vector<double> Tlist, qs2tab;
+    bool ipsat = false;
+    ipg_ipsat_params ips;
+    std::memset(&ips, 0, sizeof(ips));
+    if (in.has("NucleusQsTableFileName") &&
+        read_qs_table(in.str("NucleusQsTableFileName"), Tlist, qs2tab)) {
+        ipsat = true;
+        ips.BG = in.d("BG");
+        ips.QsmuRatio = ips.QsmuRatioB = in.d("QsmuRatio");
+        ips.proton_anisotropy = in.d_or("protonAnisotropy", 0.0);
+        ips.rapidity = in.d("Rapidity");
+        ips.roots = in.d("roots");
+        ips.x_factor = in.d("xFromThisFactorTimesQs");
+        ips.rmax = in.d("rmax");
+        ips.sigmaNN = in.d("SigmaNN");
+        ips.use_fluctuating_x = in.i("useFluctuatingx");
+        ips.average_over_nuclei = std::max(1, (int)in.d_or("averageOverThisManyNuclei", 1.0));
+        if (ips.proton_anisotropy != 0.0 || in.d_or("smearQs", 0.0) != 0.0 ||
+            in.d_or("useConstituentQuarkProton", 0.0) != 0.0)
+            std::cerr << "note: protonAnisotropy, smearQs and constituent quarks are not used "
+                         "by this executable (round nucleons, unit Q_s normalisation)"
+                      << std::endl;
+    }
     const double rapidity = in.d("Rapidity");
     unsigned long long seed = in.ull("seed");
     if (in.i("useTimeForSeed") == 1) seed = std::random_device{}();
@@ -354,10 +403,22 @@ int main(int argc, char **argv) {
             const double dmin = in.i("setWSDeformParams") ? in.d("d_min") : 0.4;
             const auto nA = sample_nucleus(rng, sA, dmin);
             const auto nB = sample_nucleus(rng, sB, dmin);
-            check(ctx,
-                  ipg_set_nuclei(ctx, nA.data(), (int)(nA.size() / 3), nB.data(),
-                                 (int)(nB.size() / 3), b, BG, QsMax, QsmuRatio),
-                  "ipg_set_nuclei");
+            if (ipsat) {
+                ipg_ipsat_report irep;
+                check(ctx,
+                      ipg_set_nuclei_ipsat(ctx, nA.data(), (int)(nA.size() / 3), nB.data(),
+                                           (int)(nB.size() / 3), nullptr, nullptr, nullptr,
+                                           nullptr, b, &ips, Tlist.data(), qs2tab.data(), 200,
+                                           44, 0.25, &irep),
+                      "ipg_set_nuclei_ipsat");
+                std::cout << "N_part=" << irep.Npart << " N_coll=" << irep.Ncoll
+                          << " Average Qs(max) = " << irep.average_Qs << " GeV" << std::endl;
+            } else {
+                check(ctx,
+                      ipg_set_nuclei(ctx, nA.data(), (int)(nA.size() / 3), nB.data(),
+                                     (int)(nB.size() / 3), b, BG, QsMax, QsmuRatio),
+                      "ipg_set_nuclei");
+            }
             check(ctx, ipg_reseed(ctx, seed * 1000003ULL + event_id), "ipg_reseed");
             check(ctx, ipg_use_device_noise(ctx), "ipg_use_device_noise");
             check(ctx, ipg_init_fields(ctx, &rep), "ipg_init_fields");

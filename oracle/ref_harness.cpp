@@ -34,10 +34,22 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <climits>
+#include <cmath>
+#include <complex>
+#include <map>
+#include <set>
+
 #include "Evolution.h"
 #include "Glauber.h"
 #include "Group.h"
+// The nucleon lists of Init are private; the IP-Sat mode fills them with the
+// test's positions before calling the reference's own setColorChargeDensity
+// (no reference source is changed: the access specifier is lifted for this
+// translation unit's view of the class only).
+#define private public
 #include "Init.h"
+#undef private
 #include "Lattice.h"
 #include "Matrix.h"
 #include "Parameters.h"
@@ -63,6 +75,13 @@ struct Args {
     int size_output = 0;
     double L_output = 0.0;
     int dumps = 1;  // 0: no state, noise or observable dumps (timing runs)
+    // --mode ipsat: nucleon positions (binary: nA, nB as doubles, then x, y of
+    // A, then of B, fm, unshifted), the Q_s table file, impact parameter and
+    // the IP-Sat parameters
+    std::string nucleons, table;
+    double b = 0.0, BG = 4.0, QsmuRatio = 0.8, roots = 5020.0, rapidity = 0.0;
+    double xfactor = 0.5, rmax = 3.0, sigmaNN = 70.0;
+    int fluct = 1;
 };
 
 void usage() {
@@ -70,7 +89,11 @@ void usage() {
                  " [--Ny n] [--g g] [--m GeV] [--uvdamp x] [--seed s]"
                  " [--maxtime fm] [--dtau lattice] [--mode full|steps|init]"
                  " [--steps k] [--write-outputs w] [--size-output n]"
-                 " [--L-output fm] [--dumps 0|1]\n";
+                 " [--L-output fm] [--dumps 0|1]\n"
+                 "       ipg_ref_harness --mode ipsat --nucleons FILE --table FILE --out DIR"
+                 " [--N n] [--L fm] [--g g] [--b fm] [--BG GeV^-2] [--QsmuRatio r]"
+                 " [--roots GeV] [--rapidity y] [--xfactor f] [--rmax fm]"
+                 " [--sigmaNN mb] [--fluct 0|1] [--seed s]\n";
     std::exit(2);
 }
 
@@ -97,9 +120,20 @@ Args parse(int argc, char **argv) {
         else if (k == "--size-output") a.size_output = std::atoi(v.c_str());
         else if (k == "--L-output") a.L_output = std::atof(v.c_str());
         else if (k == "--dumps") a.dumps = std::atoi(v.c_str());
+        else if (k == "--nucleons") a.nucleons = v;
+        else if (k == "--table") a.table = v;
+        else if (k == "--b") a.b = std::atof(v.c_str());
+        else if (k == "--BG") a.BG = std::atof(v.c_str());
+        else if (k == "--QsmuRatio") a.QsmuRatio = std::atof(v.c_str());
+        else if (k == "--roots") a.roots = std::atof(v.c_str());
+        else if (k == "--rapidity") a.rapidity = std::atof(v.c_str());
+        else if (k == "--xfactor") a.xfactor = std::atof(v.c_str());
+        else if (k == "--rmax") a.rmax = std::atof(v.c_str());
+        else if (k == "--sigmaNN") a.sigmaNN = std::atof(v.c_str());
+        else if (k == "--fluct") a.fluct = std::atoi(v.c_str());
         else usage();
     }
-    if (a.g2mu_file.empty()) usage();
+    if (a.g2mu_file.empty() && a.mode != "ipsat") usage();
     if (a.size_output <= 0) a.size_output = a.N;
     if (a.L_output <= 0) a.L_output = a.L;
     return a;
@@ -171,8 +205,118 @@ double seconds_since(std::chrono::steady_clock::time_point t0) {
 
 }  // namespace
 
+void write_doubles(const std::string &name, const std::vector<double> &v) {
+    std::ofstream f(name.c_str(), std::ios::out | std::ios::binary);
+    f.write((const char *)v.data(), v.size() * sizeof(double));
+}
+
+// IP-Sat maps through Init::readNuclearQs and Init::setColorChargeDensity
+// (Init.cpp:441-480, 753-1676) for given nucleon positions; dumps T_A, T_B,
+// g2mu2A, g2mu2B per cell and the event figures.
+int run_ipsat(const Args &A) {
+    const int N = A.N;
+    std::vector<double> raw;
+    {
+        std::ifstream f(A.nucleons.c_str(), std::ios::in | std::ios::binary);
+        double hdr[2];
+        f.read((char *)hdr, sizeof(hdr));
+        if (!f) {
+            std::cerr << "cannot read " << A.nucleons << "\n";
+            return 2;
+        }
+        raw.resize(2 * (size_t)(hdr[0] + hdr[1]) + 2);
+        raw[0] = hdr[0];
+        raw[1] = hdr[1];
+        f.read((char *)(raw.data() + 2), (raw.size() - 2) * sizeof(double));
+        if (!f) {
+            std::cerr << "short nucleon file\n";
+            return 2;
+        }
+    }
+    const int nA = (int)raw[0], nB = (int)raw[1];
+    // the table is opened after the chdir below: resolve it first
+    char resolved[4096];
+    const std::string table =
+        realpath(A.table.c_str(), resolved) ? std::string(resolved) : A.table;
+    mkdir(A.out.c_str(), 0755);
+    if (chdir(A.out.c_str()) != 0) return 2;
+    Parameters param;
+    param.setSize(N);
+    param.setL(A.L);
+    param.setNc(3);
+    param.setg(A.g);
+    param.setEventId(0);
+    param.setUseNucleus(1);
+    param.setb(A.b);
+    param.setBG(A.BG);
+    param.setQsmuRatio(A.QsmuRatio);
+    param.setRoots(A.roots);
+    param.setRapidity(A.rapidity);
+    param.setUsePseudoRapidity(0);
+    param.setxFromThisFactorTimesQs(A.xfactor);
+    param.setRmax(A.rmax);
+    param.setSigmaNN(A.sigmaNN);
+    param.setUseFluctuatingx(A.fluct);
+    param.setProtonAnisotropy(0.0);
+    param.setUseConstituentQuarkProton(0);
+    param.setSmearQs(0);
+    param.setSmearingWidth(0.0);
+    param.setAverageOverNuclei(1);
+    param.setRotateReactionPlane(0);
+    param.setUseSmoothNucleus(0);
+    param.setGaussianWounding(0);
+    param.setUseFixedNpart(0);
+    param.setMinimumQs2ST(0.0);
+    param.setRunningCoupling(0);
+    param.setNucleusQsTableFileName(table);
+    int nn[2] = {N, N};
+    Init init(nn);
+    init.readNuclearQs(&param);
+    for (int k = 0; k < nA + nB; k++) {
+        ReturnValue r;
+        r.x = raw[2 + 2 * k];
+        r.y = raw[2 + 2 * k + 1];
+        r.z = 0.0;
+        r.phi = 0.0;
+        r.collided = 0;
+        r.proton = true;
+        (k < nA ? init.nucleusA_ : init.nucleusB_).push_back(r);
+    }
+    Lattice lat(&param, 3, N);
+    Random random;
+    random.init_genrand64(A.seed);
+    Glauber glauber;
+    glauber.currentA1 = nA;
+    glauber.currentA2 = nB;
+    init.setColorChargeDensity(&lat, &param, &random, &glauber);
+    std::vector<double> out(4 * (size_t)N * N);
+    for (int pos = 0; pos < N * N; pos++) {
+        out[pos] = lat.cells[pos]->getTpA();
+        out[(size_t)N * N + pos] = lat.cells[pos]->getTpB();
+        out[2 * (size_t)N * N + pos] = lat.cells[pos]->getg2mu2A();
+        out[3 * (size_t)N * N + pos] = lat.cells[pos]->getg2mu2B();
+    }
+    write_doubles("ipsat.bin", out);
+    long ncoll = 0;
+    {
+        std::ifstream f("NcollList0.dat");
+        std::string line;
+        while (std::getline(f, line))
+            if (!line.empty()) ncoll++;
+    }
+    std::ofstream js("harness.json");
+    js.precision(17);
+    js << "{\"N\": " << N << ", \"mode\": \"ipsat\", \"Npart\": " << param.getNpart()
+       << ", \"Ncoll\": " << ncoll << ", \"Tpp\": " << param.getTpp()
+       << ", \"average_Qs\": " << param.getAverageQs()
+       << ", \"average_Qs_avg\": " << param.getAverageQsAvg()
+       << ", \"average_Qs_min\": " << param.getAverageQsmin() << "}\n";
+    return 0;
+}
+
 int main(int argc, char **argv) {
     Args A = parse(argc, argv);
+    if (A.mode == "ipsat") return run_ipsat(A);
     const int N = A.N;
 
     std::vector<double> g2mu((size_t)2 * N * N);
