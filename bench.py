@@ -917,9 +917,10 @@ def load_peaks():
 
 
 def load_traffic():
-    """DRAM bytes per launch of the FP32 leapfrog kernel from the committed ncu
-    summary (profiles/leapfrog_fp32_PbPb512.json), or None."""
-    p = ROOT / "profiles" / "leapfrog_fp32_PbPb512.json"
+    """DRAM bytes per launch of the batched FP32 leapfrog kernel on this
+    workload from the committed ncu summary (profiles/leapfrog_batch_fp32.json),
+    or None."""
+    p = ROOT / "profiles" / "leapfrog_batch_fp32.json"
     if p.exists():
         try:
             return json.loads(p.read_text()).get("dram_bytes_per_launch")

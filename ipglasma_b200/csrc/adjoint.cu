@@ -38,42 +38,49 @@ using Md = M3<double>;
 
 __device__ __forceinline__ size_t at(int N, int i, int j) { return (size_t)i * N + j; }
 
-__device__ __forceinline__ Md herm(const Md &a) {
-    Md r;
+template <typename T>
+__device__ __forceinline__ M3<T> herm(const M3<T> &a) {
+    M3<T> r;
 #pragma unroll
     for (int x = 0; x < 3; x++)
 #pragma unroll
         for (int y = 0; y < 3; y++)
-            r.m[3 * x + y] = {0.5 * (a.m[3 * x + y].r + a.m[3 * y + x].r),
-                              0.5 * (a.m[3 * x + y].i - a.m[3 * y + x].i)};
+            r.m[3 * x + y] = {T(0.5) * (a.m[3 * x + y].r + a.m[3 * y + x].r),
+                              T(0.5) * (a.m[3 * x + y].i - a.m[3 * y + x].i)};
     return r;
 }
 
 // s * i * a
-__device__ __forceinline__ Md times_i(const Md &a, double s) {
-    Md r;
+template <typename T>
+__device__ __forceinline__ M3<T> times_i(const M3<T> &a, T s) {
+    M3<T> r;
 #pragma unroll
     for (int k = 0; k < 9; k++) r.m[k] = {-s * a.m[k].i, s * a.m[k].r};
     return r;
 }
 
-__device__ __forceinline__ Md sc(const Md &a, double s) { return scaled(a, s); }
+template <typename T>
+__device__ __forceinline__ M3<T> sc(const M3<T> &a, T s) { return scaled(a, s); }
 
-__device__ __forceinline__ Md addm(const Md &a, const Md &b) {
-    Md r = a;
+template <typename T>
+__device__ __forceinline__ M3<T> addm(const M3<T> &a, const M3<T> &b) {
+    M3<T> r = a;
     add_to(r, b);
     return r;
 }
 
 // i [A, B]
-__device__ __forceinline__ Md icomm(const Md &a, const Md &b) {
-    return times_i(minus(mul(a, b), mul(b, a)), 1.);
+template <typename T>
+__device__ __forceinline__ M3<T> icomm(const M3<T> &a, const M3<T> &b) {
+    return times_i(minus(mul(a, b), mul(b, a)), T(1.));
 }
 
-__device__ __forceinline__ Md ld_herm(const double *p, size_t pos, size_t n) {
+template <typename T>
+__device__ __forceinline__ M3<T> ld_herm(const T *p, size_t pos, size_t n) {
     return from_h(ld_h(p, pos, n));
 }
-__device__ __forceinline__ Md ld_herm8(const double *p, size_t pos, size_t n) {
+template <typename T>
+__device__ __forceinline__ M3<T> ld_herm8(const T *p, size_t pos, size_t n) {
     return from_h(ld_h8(p, pos, n));
 }
 
@@ -81,16 +88,19 @@ __device__ __forceinline__ Md ld_herm8(const double *p, size_t pos, size_t n) {
 // the real part of entry k in plane 2k, its imaginary part in plane 2k+1
 // (the buffer is typed as 9 complex planes and has the same size). A warp's
 // FP64 atomics on one plane then fill whole 32-byte sectors.
-__device__ __forceinline__ double *adj_planes(C<double> *buf) {
-    return reinterpret_cast<double *>(buf);
+template <typename T>
+__device__ __forceinline__ T *adj_planes(C<T> *buf) {
+    return reinterpret_cast<T *>(buf);
 }
-__device__ __forceinline__ const double *adj_planes(const C<double> *buf) {
-    return reinterpret_cast<const double *>(buf);
+template <typename T>
+__device__ __forceinline__ const T *adj_planes(const C<T> *buf) {
+    return reinterpret_cast<const T *>(buf);
 }
 
-__device__ __forceinline__ void atomic_add_m(C<double> *buf, size_t pos, size_t n,
-                                             const Md &a) {
-    double *b = adj_planes(buf);
+template <typename T>
+__device__ __forceinline__ void atomic_add_m(C<T> *buf, size_t pos, size_t n,
+                                             const M3<T> &a) {
+    T *b = adj_planes(buf);
 #pragma unroll
     for (int k = 0; k < 9; k++) {
         atomicAdd(&b[(2 * k) * n + pos], a.m[k].r);
@@ -98,16 +108,18 @@ __device__ __forceinline__ void atomic_add_m(C<double> *buf, size_t pos, size_t 
     }
 }
 
-__device__ __forceinline__ Md ld_adj(const C<double> *buf, size_t pos, size_t n) {
-    const double *b = adj_planes(buf);
-    Md m;
+template <typename T>
+__device__ __forceinline__ M3<T> ld_adj(const C<T> *buf, size_t pos, size_t n) {
+    const T *b = adj_planes(buf);
+    M3<T> m;
 #pragma unroll
     for (int k = 0; k < 9; k++) m.m[k] = {b[(2 * k) * n + pos], b[(2 * k + 1) * n + pos]};
     return m;
 }
 
-__device__ __forceinline__ void st_adj(C<double> *buf, size_t pos, size_t n, const Md &m) {
-    double *b = adj_planes(buf);
+template <typename T>
+__device__ __forceinline__ void st_adj(C<T> *buf, size_t pos, size_t n, const M3<T> &m) {
+    T *b = adj_planes(buf);
 #pragma unroll
     for (int k = 0; k < 9; k++) {
         b[(2 * k) * n + pos] = m.m[k].r;
@@ -121,9 +133,10 @@ __device__ __forceinline__ void st_adj(C<double> *buf, size_t pos, size_t n, con
 // 8 planes (d0 d1 and the off-diagonals; d2 = -d0 - d1). A contribution M is
 // added as its (traceless) Hermitian part. k_adj_project expands them to full
 // matrices (split planes) at the end of the sweep.
-__device__ __forceinline__ H3<double> ld_h9a(const C<double> *buf, size_t pos, size_t n) {
-    const double *b = adj_planes(buf);
-    H3<double> h;
+template <typename T>
+__device__ __forceinline__ H3<T> ld_h9a(const C<T> *buf, size_t pos, size_t n) {
+    const T *b = adj_planes(buf);
+    H3<T> h;
     h.d0 = b[pos];
     h.d1 = b[n + pos];
     h.d2 = b[2 * n + pos];
@@ -133,8 +146,9 @@ __device__ __forceinline__ H3<double> ld_h9a(const C<double> *buf, size_t pos, s
     return h;
 }
 
-__device__ __forceinline__ void st_h9a(C<double> *buf, size_t pos, size_t n, const H3<double> &h) {
-    double *b = adj_planes(buf);
+template <typename T>
+__device__ __forceinline__ void st_h9a(C<T> *buf, size_t pos, size_t n, const H3<T> &h) {
+    T *b = adj_planes(buf);
     b[pos] = h.d0;
     b[n + pos] = h.d1;
     b[2 * n + pos] = h.d2;
@@ -146,9 +160,10 @@ __device__ __forceinline__ void st_h9a(C<double> *buf, size_t pos, size_t n, con
     b[8 * n + pos] = h.o12.i;
 }
 
-__device__ __forceinline__ H3<double> ld_h8a(const C<double> *buf, size_t pos, size_t n) {
-    const double *b = adj_planes(buf);
-    H3<double> h;
+template <typename T>
+__device__ __forceinline__ H3<T> ld_h8a(const C<T> *buf, size_t pos, size_t n) {
+    const T *b = adj_planes(buf);
+    H3<T> h;
     h.d0 = b[pos];
     h.d1 = b[n + pos];
     h.d2 = -(h.d0 + h.d1);
@@ -158,8 +173,9 @@ __device__ __forceinline__ H3<double> ld_h8a(const C<double> *buf, size_t pos, s
     return h;
 }
 
-__device__ __forceinline__ void st_h8a(C<double> *buf, size_t pos, size_t n, const H3<double> &h) {
-    double *b = adj_planes(buf);
+template <typename T>
+__device__ __forceinline__ void st_h8a(C<T> *buf, size_t pos, size_t n, const H3<T> &h) {
+    T *b = adj_planes(buf);
     b[pos] = h.d0;
     b[n + pos] = h.d1;
     b[2 * n + pos] = h.o01.r;
@@ -171,21 +187,23 @@ __device__ __forceinline__ void st_h8a(C<double> *buf, size_t pos, size_t n, con
 }
 
 // Hermitian part (M + M^dag) / 2
-__device__ __forceinline__ H3<double> herm_part(const Md &m) {
-    H3<double> h;
+template <typename T>
+__device__ __forceinline__ H3<T> herm_part(const M3<T> &m) {
+    H3<T> h;
     h.d0 = m.m[0].r;
     h.d1 = m.m[4].r;
     h.d2 = m.m[8].r;
-    h.o01 = {0.5 * (m.m[1].r + m.m[3].r), 0.5 * (m.m[1].i - m.m[3].i)};
-    h.o02 = {0.5 * (m.m[2].r + m.m[6].r), 0.5 * (m.m[2].i - m.m[6].i)};
-    h.o12 = {0.5 * (m.m[5].r + m.m[7].r), 0.5 * (m.m[5].i - m.m[7].i)};
+    h.o01 = {T(0.5) * (m.m[1].r + m.m[3].r), T(0.5) * (m.m[1].i - m.m[3].i)};
+    h.o02 = {T(0.5) * (m.m[2].r + m.m[6].r), T(0.5) * (m.m[2].i - m.m[6].i)};
+    h.o12 = {T(0.5) * (m.m[5].r + m.m[7].r), T(0.5) * (m.m[5].i - m.m[7].i)};
     return h;
 }
 
-__device__ __forceinline__ void atomic_add_h9a(C<double> *buf, size_t pos, size_t n,
-                                               const Md &m) {
-    const H3<double> h = herm_part(m);
-    double *b = adj_planes(buf);
+template <typename T>
+__device__ __forceinline__ void atomic_add_h9a(C<T> *buf, size_t pos, size_t n,
+                                               const M3<T> &m) {
+    const H3<T> h = herm_part(m);
+    T *b = adj_planes(buf);
     atomicAdd(&b[pos], h.d0);
     atomicAdd(&b[n + pos], h.d1);
     atomicAdd(&b[2 * n + pos], h.d2);
@@ -197,11 +215,12 @@ __device__ __forceinline__ void atomic_add_h9a(C<double> *buf, size_t pos, size_
     atomicAdd(&b[8 * n + pos], h.o12.i);
 }
 
-__device__ __forceinline__ void atomic_add_h8a(C<double> *buf, size_t pos, size_t n,
-                                               const Md &m) {
-    const H3<double> h = herm_part(m);
-    const double t = (h.d0 + h.d1 + h.d2) / 3.;
-    double *b = adj_planes(buf);
+template <typename T>
+__device__ __forceinline__ void atomic_add_h8a(C<T> *buf, size_t pos, size_t n,
+                                               const M3<T> &m) {
+    const H3<T> h = herm_part(m);
+    const T t = (h.d0 + h.d1 + h.d2) / T(3.);
+    T *b = adj_planes(buf);
     atomicAdd(&b[pos], h.d0 - t);
     atomicAdd(&b[n + pos], h.d1 - t);
     atomicAdd(&b[2 * n + pos], h.o01.r);
@@ -213,21 +232,23 @@ __device__ __forceinline__ void atomic_add_h8a(C<double> *buf, size_t pos, size_
 }
 
 // T2(X) = 1 + X + X^2 / 2
-__device__ __forceinline__ Md taylor2(const Md &x) {
-    Md r = mul(x, x);
+template <typename T>
+__device__ __forceinline__ M3<T> taylor2(const M3<T> &x) {
+    M3<T> r = mul(x, x);
 #pragma unroll
-    for (int k = 0; k < 9; k++) r.m[k] = {0.5 * r.m[k].r + x.m[k].r, 0.5 * r.m[k].i + x.m[k].i};
-    r.m[0].r += 1.;
-    r.m[4].r += 1.;
-    r.m[8].r += 1.;
+    for (int k = 0; k < 9; k++) r.m[k] = {T(0.5) * r.m[k].r + x.m[k].r, T(0.5) * r.m[k].i + x.m[k].i};
+    r.m[0].r += T(1.);
+    r.m[4].r += T(1.);
+    r.m[8].r += T(1.);
     return r;
 }
 
 // inverse of a 3x3 complex matrix (adjugate / determinant)
-__device__ __forceinline__ Md inverse3(const Md &a) {
+template <typename T>
+__device__ __forceinline__ M3<T> inverse3(const M3<T> &a) {
     auto e = [&](int r, int c) { return a.m[3 * r + c]; };
-    auto sub = [](C<double> x, C<double> y) { return C<double>{x.r - y.r, x.i - y.i}; };
-    Md adj;
+    auto sub = [](C<T> x, C<T> y) { return C<T>{x.r - y.r, x.i - y.i}; };
+    M3<T> adj;
     adj.m[0] = sub(cmul(e(1, 1), e(2, 2)), cmul(e(1, 2), e(2, 1)));
     adj.m[1] = sub(cmul(e(0, 2), e(2, 1)), cmul(e(0, 1), e(2, 2)));
     adj.m[2] = sub(cmul(e(0, 1), e(1, 2)), cmul(e(0, 2), e(1, 1)));
@@ -237,15 +258,15 @@ __device__ __forceinline__ Md inverse3(const Md &a) {
     adj.m[6] = sub(cmul(e(1, 0), e(2, 1)), cmul(e(1, 1), e(2, 0)));
     adj.m[7] = sub(cmul(e(0, 1), e(2, 0)), cmul(e(0, 0), e(2, 1)));
     adj.m[8] = sub(cmul(e(0, 0), e(1, 1)), cmul(e(0, 1), e(1, 0)));
-    C<double> det = {0., 0.};
+    C<T> det = {T(0.), T(0.)};
 #pragma unroll
     for (int k = 0; k < 3; k++) {
-        const C<double> t = cmul(e(0, k), adj.m[3 * k]);
+        const C<T> t = cmul(e(0, k), adj.m[3 * k]);
         det.r += t.r;
         det.i += t.i;
     }
-    const double d2 = det.r * det.r + det.i * det.i;
-    const C<double> inv = {det.r / d2, -det.i / d2};
+    const T d2 = det.r * det.r + det.i * det.i;
+    const C<T> inv = {det.r / d2, -det.i / d2};
 #pragma unroll
     for (int k = 0; k < 9; k++) adj.m[k] = cmul(adj.m[k], inv);
     return adj;
@@ -278,16 +299,17 @@ __device__ __forceinline__ StepGeom step_geom(int N, int ix, int iy) {
 // ---------------------------------------------------------------------------
 
 // U_d = T2(i c E_d')^{-1} U_d',  phi = phi' - c2 pi'
-__global__ void k_inv_su(int N, State<double> nxt, State<double> cur, double c, double c2) {
+template <typename T>
+__global__ void k_inv_su(int N, State<T> nxt, State<T> cur, T c, T c2) {
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
     for (int d = 0; d < 2; d++) {
-        const Md E = ld_herm8(d ? nxt.e2 : nxt.e1, pos, n);
-        const Md M = taylor2(times_i(E, c));
+        const M3<T> E = ld_herm8(d ? nxt.e2 : nxt.e1, pos, n);
+        const M3<T> M = taylor2(times_i(E, c));
         st_m3(d ? cur.uy : cur.ux, pos, n, mul(inverse3(M), ld_m3(d ? nxt.uy : nxt.ux, pos, n)));
     }
-    H3<double> phi = ld_h(nxt.phi, pos, n);
+    H3<T> phi = ld_h(nxt.phi, pos, n);
     h_axpy(phi, -c2, ld_h(nxt.pi, pos, n));
     st_h(cur.phi, pos, n, phi);
 }
@@ -299,32 +321,33 @@ __global__ void k_inv_su(int N, State<double> nxt, State<double> cur, double c, 
 // S_u: reads the adjoints of the step's outputs, leaves the adjoints of its
 // inputs (U before the update, phi before, pi' and E' after S_e). `cur` holds
 // U, phi of the step's input, `nxt` E' of its output.
-__global__ void k_adj_su(int N, State<double> cur, State<double> nxt, AdjState a, double c,
-                         double c2) {
+template <typename T>
+__global__ void k_adj_su(int N, State<T> cur, State<T> nxt, AdjStateT<T> a, T c,
+                         T c2) {
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
     // pi_bar += c2 phi_bar (phi_bar itself passes through unchanged)
     {
-        H3<double> pib = ld_h9a(a.pi, pos, n);
+        H3<T> pib = ld_h9a(a.pi, pos, n);
         h_axpy(pib, c2, ld_h9a(a.phi, pos, n));
         st_h9a(a.pi, pos, n, pib);
     }
     for (int d = 0; d < 2; d++) {
-        C<double> *Ub = d ? a.uy : a.ux;
-        C<double> *Eb = d ? a.e2 : a.e1;
-        const Md Ubar = ld_adj(Ub, pos, n);
-        const Md U = ld_m3(d ? cur.uy : cur.ux, pos, n);
-        const Md X = times_i(ld_herm8(d ? nxt.e2 : nxt.e1, pos, n), c);
-        const Md M = taylor2(X);
+        C<T> *Ub = d ? a.uy : a.ux;
+        C<T> *Eb = d ? a.e2 : a.e1;
+        const M3<T> Ubar = ld_adj(Ub, pos, n);
+        const M3<T> U = ld_m3(d ? cur.uy : cur.ux, pos, n);
+        const M3<T> X = times_i(ld_herm8(d ? nxt.e2 : nxt.e1, pos, n), c);
+        const M3<T> M = taylor2(X);
         st_adj(Ub, pos, n, mul_dn(M, Ubar));
-        const Md Mb = mul_nd(Ubar, U);
+        const M3<T> Mb = mul_nd(Ubar, U);
         // X_bar = M_bar + (M_bar X^dag + X^dag M_bar) / 2
-        Md Xb = Mb;
-        add_to(Xb, sc(addm(mul_nd(Mb, X), mul_dn(X, Mb)), 0.5));
+        M3<T> Xb = Mb;
+        add_to(Xb, sc(addm(mul_nd(Mb, X), mul_dn(X, Mb)), T(0.5)));
         // X = i c E  ->  E_bar += Herm(-i c X_bar); stored traceless Hermitian,
         // which is also the adjoint of E before S_e (E' = TL(E + ...))
-        H3<double> Eb_ = herm_part(times_i(Xb, -c));
+        H3<T> Eb_ = herm_part(times_i(Xb, -c));
         h_traceless(Eb_);
         h_add(Eb_, ld_h8a(Eb, pos, n));
         st_h8a(Eb, pos, n, Eb_);
@@ -335,35 +358,36 @@ __global__ void k_adj_su(int N, State<double> cur, State<double> nxt, AdjState a
 // reversal: U_d = M_d^{-1} U_d' with M_d = T2(i c E_d'), phi = phi' - c2 pi'
 // are written to `cur` (as k_inv_su), then the adjoint of S_u runs with that
 // M_d and U_d (as k_adj_su, which would recompute M_d and reload U_d).
-__global__ void k_inv_adj_su(int N, State<double> nxt, State<double> cur, AdjState a, double c,
-                             double c2) {
+template <typename T>
+__global__ void k_inv_adj_su(int N, State<T> nxt, State<T> cur, AdjStateT<T> a, T c,
+                             T c2) {
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
     {
-        H3<double> phi = ld_h(nxt.phi, pos, n);
+        H3<T> phi = ld_h(nxt.phi, pos, n);
         h_axpy(phi, -c2, ld_h(nxt.pi, pos, n));
         st_h(cur.phi, pos, n, phi);
     }
     // pi_bar += c2 phi_bar (phi_bar itself passes through unchanged)
     {
-        H3<double> pib = ld_h9a(a.pi, pos, n);
+        H3<T> pib = ld_h9a(a.pi, pos, n);
         h_axpy(pib, c2, ld_h9a(a.phi, pos, n));
         st_h9a(a.pi, pos, n, pib);
     }
     for (int d = 0; d < 2; d++) {
-        C<double> *Ub = d ? a.uy : a.ux;
-        C<double> *Eb = d ? a.e2 : a.e1;
-        const Md X = times_i(ld_herm8(d ? nxt.e2 : nxt.e1, pos, n), c);
-        const Md M = taylor2(X);
-        const Md U = mul(inverse3(M), ld_m3(d ? nxt.uy : nxt.ux, pos, n));
+        C<T> *Ub = d ? a.uy : a.ux;
+        C<T> *Eb = d ? a.e2 : a.e1;
+        const M3<T> X = times_i(ld_herm8(d ? nxt.e2 : nxt.e1, pos, n), c);
+        const M3<T> M = taylor2(X);
+        const M3<T> U = mul(inverse3(M), ld_m3(d ? nxt.uy : nxt.ux, pos, n));
         st_m3(d ? cur.uy : cur.ux, pos, n, U);
-        const Md Ubar = ld_adj(Ub, pos, n);
+        const M3<T> Ubar = ld_adj(Ub, pos, n);
         st_adj(Ub, pos, n, mul_dn(M, Ubar));
-        const Md Mb = mul_nd(Ubar, U);
-        Md Xb = Mb;
-        add_to(Xb, sc(addm(mul_nd(Mb, X), mul_dn(X, Mb)), 0.5));
-        H3<double> Eb_ = herm_part(times_i(Xb, -c));
+        const M3<T> Mb = mul_nd(Ubar, U);
+        M3<T> Xb = Mb;
+        add_to(Xb, sc(addm(mul_nd(Mb, X), mul_dn(X, Mb)), T(0.5)));
+        H3<T> Eb_ = herm_part(times_i(Xb, -c));
         h_traceless(Eb_);
         h_add(Eb_, ld_h8a(Eb, pos, n));
         st_h8a(Eb, pos, n, Eb_);
@@ -391,99 +415,100 @@ __global__ void k_inv_adj_su(int N, State<double> nxt, State<double> cur, AdjSta
 //         phi += -4 brb + i[Cb_1, ph_x] + i[Cb_2, ph_y]
 // role 2: Ux(-x) += Uy(-x) Qb2 + 2 phi(-x) Ux(-x) brb; Uy(-x) += Ux(-x) Qb2^dag;
 //         phi(-x) += Ux(-x) brb Ux(-x)^dag; and the same along y with Qb
-__global__ void __launch_bounds__(128) k_adj_se(int N, State<double> cur, AdjState a, double cst,
-                                                double cdt) {
+template <typename T>
+__global__ void __launch_bounds__(128) k_adj_se(int N, State<T> cur, AdjStateT<T> a, T cst,
+                                                T cdt) {
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
     const StepGeom G = step_geom(N, (int)(pos / N), (int)(pos % N));
     const int role = blockIdx.y;
     if (role == 0) {
-        const H3<double> h1 = ld_h8a(a.e1, pos, n);
-        const Md ux = ld_m3(cur.ux, pos, n);
-        Md acc;
+        const H3<T> h1 = ld_h8a(a.e1, pos, n);
+        const M3<T> ux = ld_m3(cur.ux, pos, n);
+        M3<T> acc;
         {
-            const Md uy_px = ld_m3(cur.uy, G.pX, n);
-            const Md B = mul(ld_m3(cur.uy, pos, n), ld_m3(cur.ux, G.pY, n));
-            const Md Mb = times_i(minus(sc(from_h(h1), cst), sc(from_h(ld_h8a(a.e2, pos, n)), cst)), -2.);
-            const Md Ab = mul(Mb, B);
+            const M3<T> uy_px = ld_m3(cur.uy, G.pX, n);
+            const M3<T> B = mul(ld_m3(cur.uy, pos, n), ld_m3(cur.ux, G.pY, n));
+            const M3<T> Mb = times_i(minus(sc(from_h(h1), cst), sc(from_h(ld_h8a(a.e2, pos, n)), cst)), -T(2.));
+            const M3<T> Ab = mul(Mb, B);
             acc = mul_nd(Ab, uy_px);
             atomic_add_m(a.uy, G.pX, n, mul_dn(ux, Ab));
         }
         {
-            const Md uy_pxmy = ld_m3(cur.uy, G.pXmY, n);
-            const Md Q = mul_dn(ld_m3(cur.ux, G.mY, n), ld_m3(cur.uy, G.mY, n));
-            const Md Pb = mul_nd(times_i(sc(from_h(h1), cst), -2.), Q);
+            const M3<T> uy_pxmy = ld_m3(cur.uy, G.pXmY, n);
+            const M3<T> Q = mul_dn(ld_m3(cur.ux, G.mY, n), ld_m3(cur.uy, G.mY, n));
+            const M3<T> Pb = mul_nd(times_i(sc(from_h(h1), cst), -T(2.)), Q);
             add_to(acc, mul(Pb, uy_pxmy));
             atomic_add_m(a.uy, G.pXmY, n, mul_dn(Pb, ux));
         }
         {
-            Md phb = icomm(ld_herm(cur.phi, pos, n), sc(from_h(h1), cdt));
+            M3<T> phb = icomm(ld_herm(cur.phi, pos, n), sc(from_h(h1), cdt));
             add_to(phb, sc(from_h(ld_h9a(a.pi, pos, n)), cdt));
-            add_to(acc, sc(mul(mul(phb, ux), ld_herm(cur.phi, G.pX, n)), 2.));
+            add_to(acc, sc(mul(mul(phb, ux), ld_herm(cur.phi, G.pX, n)), T(2.)));
             atomic_add_m(a.ux, pos, n, acc);
             atomic_add_h9a(a.phi, G.pX, n, mul(mul_dn(ux, phb), ux));
         }
     } else if (role == 1) {
-        const H3<double> h2 = ld_h8a(a.e2, pos, n);
-        const Md uy = ld_m3(cur.uy, pos, n);
-        Md acc;
+        const H3<T> h2 = ld_h8a(a.e2, pos, n);
+        const M3<T> uy = ld_m3(cur.uy, pos, n);
+        M3<T> acc;
         {
-            const Md ux_py = ld_m3(cur.ux, G.pY, n);
-            const Md A = mul(ld_m3(cur.ux, pos, n), ld_m3(cur.uy, G.pX, n));
-            const Md Mb = times_i(minus(sc(from_h(ld_h8a(a.e1, pos, n)), cst), sc(from_h(h2), cst)), -2.);
-            const Md Bb = mul_dn(Mb, A);
+            const M3<T> ux_py = ld_m3(cur.ux, G.pY, n);
+            const M3<T> A = mul(ld_m3(cur.ux, pos, n), ld_m3(cur.uy, G.pX, n));
+            const M3<T> Mb = times_i(minus(sc(from_h(ld_h8a(a.e1, pos, n)), cst), sc(from_h(h2), cst)), -T(2.));
+            const M3<T> Bb = mul_dn(Mb, A);
             acc = mul_nd(Bb, ux_py);
             atomic_add_m(a.ux, G.pY, n, mul_dn(uy, Bb));
         }
         {
-            const Md ux_mxpy = ld_m3(cur.ux, G.mXpY, n);
-            const Md Q = mul_dn(ld_m3(cur.uy, G.mX, n), ld_m3(cur.ux, G.mX, n));
-            const Md Pb = mul_nd(times_i(sc(from_h(h2), cst), -2.), Q);
+            const M3<T> ux_mxpy = ld_m3(cur.ux, G.mXpY, n);
+            const M3<T> Q = mul_dn(ld_m3(cur.uy, G.mX, n), ld_m3(cur.ux, G.mX, n));
+            const M3<T> Pb = mul_nd(times_i(sc(from_h(h2), cst), -T(2.)), Q);
             add_to(acc, mul(Pb, ux_mxpy));
             atomic_add_m(a.ux, G.mXpY, n, mul_dn(Pb, uy));
         }
         {
-            Md phb = icomm(ld_herm(cur.phi, pos, n), sc(from_h(h2), cdt));
+            M3<T> phb = icomm(ld_herm(cur.phi, pos, n), sc(from_h(h2), cdt));
             add_to(phb, sc(from_h(ld_h9a(a.pi, pos, n)), cdt));
-            add_to(acc, sc(mul(mul(phb, uy), ld_herm(cur.phi, G.pY, n)), 2.));
+            add_to(acc, sc(mul(mul(phb, uy), ld_herm(cur.phi, G.pY, n)), T(2.)));
             atomic_add_m(a.uy, pos, n, acc);
             atomic_add_h9a(a.phi, G.pY, n, mul(mul_dn(uy, phb), uy));
         }
         {
             // phi += -4 brb + i[Cb_1, ph_x] + i[Cb_2, ph_y]
-            Md phib = icomm(sc(from_h(h2), cdt), mul_nd(mul(uy, ld_herm(cur.phi, G.pY, n)), uy));
-            const Md ux = ld_m3(cur.ux, pos, n);
+            M3<T> phib = icomm(sc(from_h(h2), cdt), mul_nd(mul(uy, ld_herm(cur.phi, G.pY, n)), uy));
+            const M3<T> ux = ld_m3(cur.ux, pos, n);
             add_to(phib, icomm(sc(from_h(ld_h8a(a.e1, pos, n)), cdt),
                                mul_nd(mul(ux, ld_herm(cur.phi, G.pX, n)), ux)));
-            add_to(phib, sc(from_h(ld_h9a(a.pi, pos, n)), -4. * cdt));
+            add_to(phib, sc(from_h(ld_h9a(a.pi, pos, n)), -T(4.) * cdt));
             atomic_add_h9a(a.phi, pos, n, phib);
         }
     } else {
-        const Md brb = sc(from_h(ld_h9a(a.pi, pos, n)), cdt);
+        const M3<T> brb = sc(from_h(ld_h9a(a.pi, pos, n)), cdt);
         {
             // E2 staple's Q side and the -x transport
-            const Md uy = ld_m3(cur.uy, pos, n), ux_mxpy = ld_m3(cur.ux, G.mXpY, n);
-            const Md P = mul_nd(uy, ux_mxpy);
-            const Md Qb = mul_dn(P, times_i(sc(from_h(ld_h8a(a.e2, pos, n)), cst), -2.));
-            const Md ux_mx = ld_m3(cur.ux, G.mX, n), uy_mx = ld_m3(cur.uy, G.mX, n);
-            const Md f = ld_herm(cur.phi, G.mX, n);
+            const M3<T> uy = ld_m3(cur.uy, pos, n), ux_mxpy = ld_m3(cur.ux, G.mXpY, n);
+            const M3<T> P = mul_nd(uy, ux_mxpy);
+            const M3<T> Qb = mul_dn(P, times_i(sc(from_h(ld_h8a(a.e2, pos, n)), cst), -T(2.)));
+            const M3<T> ux_mx = ld_m3(cur.ux, G.mX, n), uy_mx = ld_m3(cur.uy, G.mX, n);
+            const M3<T> f = ld_herm(cur.phi, G.mX, n);
             atomic_add_m(a.uy, G.mX, n, mul_nd(ux_mx, Qb));
-            Md acc = mul(uy_mx, Qb);
-            add_to(acc, sc(mul(mul(f, ux_mx), brb), 2.));
+            M3<T> acc = mul(uy_mx, Qb);
+            add_to(acc, sc(mul(mul(f, ux_mx), brb), T(2.)));
             atomic_add_m(a.ux, G.mX, n, acc);
             atomic_add_h9a(a.phi, G.mX, n, mul_nd(mul(ux_mx, brb), ux_mx));
         }
         {
             // E1 staple's Q side and the -y transport
-            const Md ux = ld_m3(cur.ux, pos, n), uy_pxmy = ld_m3(cur.uy, G.pXmY, n);
-            const Md P = mul_nd(ux, uy_pxmy);
-            const Md Qb = mul_dn(P, times_i(sc(from_h(ld_h8a(a.e1, pos, n)), cst), -2.));
-            const Md ux_my = ld_m3(cur.ux, G.mY, n), uy_my = ld_m3(cur.uy, G.mY, n);
-            const Md f = ld_herm(cur.phi, G.mY, n);
+            const M3<T> ux = ld_m3(cur.ux, pos, n), uy_pxmy = ld_m3(cur.uy, G.pXmY, n);
+            const M3<T> P = mul_nd(ux, uy_pxmy);
+            const M3<T> Qb = mul_dn(P, times_i(sc(from_h(ld_h8a(a.e1, pos, n)), cst), -T(2.)));
+            const M3<T> ux_my = ld_m3(cur.ux, G.mY, n), uy_my = ld_m3(cur.uy, G.mY, n);
+            const M3<T> f = ld_herm(cur.phi, G.mY, n);
             atomic_add_m(a.ux, G.mY, n, mul_nd(uy_my, Qb));
-            Md acc = mul(ux_my, Qb);
-            add_to(acc, sc(mul(mul(f, uy_my), brb), 2.));
+            M3<T> acc = mul(ux_my, Qb);
+            add_to(acc, sc(mul(mul(f, uy_my), brb), T(2.)));
             atomic_add_m(a.uy, G.mY, n, acc);
             atomic_add_h9a(a.phi, G.mY, n, mul_nd(mul(uy_my, brb), uy_my));
         }
@@ -492,17 +517,18 @@ __global__ void __launch_bounds__(128) k_adj_se(int N, State<double> cur, AdjSta
 
 // adjoint of T^tautau (k_tmunu_diag, Evolution.cpp:759-900) in lattice units,
 // tbar[pos] = dL/dTtt_lat(pos)
-__global__ void k_adj_ttt(int N, State<double> s, const double *tbar, AdjState a, double g,
-                          double tau) {
+template <typename T>
+__global__ void k_adj_ttt(int N, State<T> s, const T *tbar, AdjStateT<T> a, T g,
+                          T tau) {
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
-    const double tb = tbar[pos];
-    if (tb == 0.) return;
+    const T tb = tbar[pos];
+    if (tb == T(0.)) return;
     const int i = (int)(pos / N), j = (int)(pos % N);
     const size_t pX = at(N, min(N - 1, i + 1), j), pY = at(N, i, min(N - 1, j + 1));
     const size_t pXY = at(N, min(N - 1, i + 1), min(N - 1, j + 1));
-    const double ge = g * g / tau / tau, ht = 0.5 / tau / tau;
+    const T ge = g * g / tau / tau, ht = T(0.5) / tau / tau;
     // electric: ge/2 (|E1|^2 + |E1(+y)|^2 + |E2|^2 + |E2(+x)|^2)
     atomic_add_h8a(a.e1, pos, n, sc(ld_herm8(s.e1, pos, n), tb * ge));
     atomic_add_h8a(a.e1, pY, n, sc(ld_herm8(s.e1, pY, n), tb * ge));
@@ -511,15 +537,15 @@ __global__ void k_adj_ttt(int N, State<double> s, const double *tbar, AdjState a
     // longitudinal electric: tr pi^2 / 4 over four cells
     const size_t cells[4] = {pos, pX, pY, pXY};
     for (int k = 0; k < 4; k++)
-        atomic_add_h9a(a.pi, cells[k], n, sc(ld_herm(s.pi, cells[k], n), 0.5 * tb));
-    const Md ux = ld_m3(s.ux, pos, n), uy = ld_m3(s.uy, pos, n);
+        atomic_add_h9a(a.pi, cells[k], n, sc(ld_herm(s.pi, cells[k], n), T(0.5) * tb));
+    const M3<T> ux = ld_m3(s.ux, pos, n), uy = ld_m3(s.uy, pos, n);
     // magnetic: 2/g^2 (3 - Re tr(Ux Uy(+x) Ux(+y)^dag Uy^dag)), zero on the last row
     if (i != N - 1) {
-        const double cb = -2. / (g * g) * tb;
-        const Md uy_px = ld_m3(s.uy, pX, n), ux_py = ld_m3(s.ux, pY, n);
-        const Md A12 = mul(ux, uy_px);
+        const T cb = -T(2.) / (g * g) * tb;
+        const M3<T> uy_px = ld_m3(s.uy, pX, n), ux_py = ld_m3(s.ux, pY, n);
+        const M3<T> A12 = mul(ux, uy_px);
         // plaq = A1 A2 A3 A4 with A1 = Ux, A2 = Uy(+x), A3 = Ux(+y)^dag, A4 = Uy^dag
-        const Md R = mul_nd(mul_nd(uy_px, ux_py), uy);  // A2 A3 A4
+        const M3<T> R = mul_nd(mul_nd(uy_px, ux_py), uy);  // A2 A3 A4
         atomic_add_m(a.ux, pos, n, sc(dagger(R), cb));
         atomic_add_m(a.uy, pX, n, sc(mul_dn(ux, mul(uy, ux_py)), cb));
         atomic_add_m(a.ux, pY, n, sc(mul_dn(uy, A12), cb));
@@ -528,8 +554,8 @@ __global__ void k_adj_ttt(int N, State<double> s, const double *tbar, AdjState a
     // longitudinal magnetic: ht tr(d^2), d = phi_a - U phi_b U^dag
     struct Term {
         size_t pa, pb;
-        const C<double> *u;
-        C<double> *ub;
+        const C<T> *u;
+        C<T> *ub;
         size_t pu;
     };
     const Term terms[4] = {{pos, pX, s.ux, a.ux, pos},
@@ -537,26 +563,27 @@ __global__ void k_adj_ttt(int N, State<double> s, const double *tbar, AdjState a
                            {pY, pXY, s.ux, a.ux, pY},
                            {pX, pXY, s.uy, a.uy, pX}};
     for (int k = 0; k < 4; k++) {
-        const Term &T = terms[k];
-        const Md u = ld_m3(T.u, T.pu, n), fb = ld_herm(s.phi, T.pb, n);
-        const Md C = mul_nd(mul(u, fb), u);
-        const Md d = minus(ld_herm(s.phi, T.pa, n), C);
-        const Md db = sc(d, 2. * ht * tb);
-        atomic_add_h9a(a.phi, T.pa, n, db);
-        const Md Cb = sc(db, -1.);
-        atomic_add_m(T.ub, T.pu, n, sc(mul(mul(Cb, u), fb), 2.));
-        atomic_add_h9a(a.phi, T.pb, n, mul(mul_dn(u, Cb), u));
+        const Term &tm = terms[k];
+        const M3<T> u = ld_m3(tm.u, tm.pu, n), fb = ld_herm(s.phi, tm.pb, n);
+        const M3<T> C = mul_nd(mul(u, fb), u);
+        const M3<T> d = minus(ld_herm(s.phi, tm.pa, n), C);
+        const M3<T> db = sc(d, T(2.) * ht * tb);
+        atomic_add_h9a(a.phi, tm.pa, n, db);
+        const M3<T> Cb = sc(db, -T(1.));
+        atomic_add_m(tm.ub, tm.pu, n, sc(mul(mul(Cb, u), fb), T(2.)));
+        atomic_add_h9a(a.phi, tm.pb, n, mul(mul_dn(u, Cb), u));
     }
 }
 
 // Hermitian (and, for E, traceless) parts of the adjoints
-__global__ void k_adj_project(size_t n, AdjState a) {
+template <typename T>
+__global__ void k_adj_project(size_t n, AdjStateT<T> a) {
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
     // the sweep's Hermitian storage expanded to full matrices in place (each
     // thread reads its site's planes before it writes them)
-    const H3<double> e1 = ld_h8a(a.e1, pos, n), e2 = ld_h8a(a.e2, pos, n);
-    const H3<double> phi = ld_h9a(a.phi, pos, n), pi = ld_h9a(a.pi, pos, n);
+    const H3<T> e1 = ld_h8a(a.e1, pos, n), e2 = ld_h8a(a.e2, pos, n);
+    const H3<T> phi = ld_h9a(a.phi, pos, n), pi = ld_h9a(a.pi, pos, n);
     st_adj(a.e1, pos, n, from_h(e1));
     st_adj(a.e2, pos, n, from_h(e2));
     st_adj(a.phi, pos, n, from_h(phi));
@@ -945,47 +972,85 @@ void launch_inverse_step(int N, const State<double> &nxt, const State<double> &c
     const size_t n = (size_t)N * N;
     const double c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / 2.);
     const double c2 = (cf.tau + cf.dt_pu / 2.) * cf.dt_pu;
-    const double cst = cf.tau * cf.dt_pe / (2. * cf.g * cf.g);
-    const double cdt = cf.tau > 0 ? cf.dt_pe / cf.tau : 0.;
     k_inv_su<<<blocks(n), 128, 0, st>>>(N, nxt, cur, c, c2);
     launch_inverse_se(N, nxt, cur, cf, st);
 }
 
-void launch_inverse_adjoint_step(int N, const State<double> &nxt, const State<double> &cur,
-                                 const AdjState &a, const StepCoef<double> &cf, cudaStream_t st) {
+// the step coefficients in T, from the FP64 ones (one rounding each)
+template <typename T>
+struct AdjCoef {
+    T c, c2, cst, cdt;
+    explicit AdjCoef(const StepCoef<double> &cf)
+        : c((T)(cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / 2.))),
+          c2((T)((cf.tau + cf.dt_pu / 2.) * cf.dt_pu)),
+          cst((T)(cf.tau * cf.dt_pe / (2. * cf.g * cf.g))),
+          cdt((T)(cf.tau > 0 ? cf.dt_pe / cf.tau : 0.)) {}
+};
+
+template <typename T>
+void launch_inverse_adjoint_step(int N, const State<T> &nxt, const State<T> &cur,
+                                 const AdjStateT<T> &a, const StepCoef<double> &cf,
+                                 cudaStream_t st) {
     const size_t n = (size_t)N * N;
-    const double c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / 2.);
-    const double c2 = (cf.tau + cf.dt_pu / 2.) * cf.dt_pu;
-    const double cst = cf.tau * cf.dt_pe / (2. * cf.g * cf.g);
-    const double cdt = cf.tau > 0 ? cf.dt_pe / cf.tau : 0.;
-    k_inv_adj_su<<<blocks(n), 128, 0, st>>>(N, nxt, cur, a, c, c2);
-    launch_inverse_se(N, nxt, cur, cf, st);
-    if (cf.do_pe) {
-        k_adj_se<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, cst, cdt);
-    }
+    const AdjCoef<T> k(cf);
+    k_inv_adj_su<<<blocks(n), 128, 0, st>>>(N, nxt, cur, a, k.c, k.c2);
+    launch_inverse_se<T>(N, nxt, cur, cf, st);
+    if (cf.do_pe) k_adj_se<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, k.cst, k.cdt);
 }
 
-void launch_adjoint_step(int N, const State<double> &cur, const State<double> &nxt,
-                         const AdjState &a, const StepCoef<double> &cf, cudaStream_t st) {
+template <typename T>
+void launch_adjoint_step(int N, const State<T> &cur, const State<T> &nxt, const AdjStateT<T> &a,
+                         const StepCoef<double> &cf, cudaStream_t st) {
     const size_t n = (size_t)N * N;
-    const double c = cf.g * cf.g * cf.dt_pu / (cf.tau + cf.dt_pu / 2.);
-    const double c2 = (cf.tau + cf.dt_pu / 2.) * cf.dt_pu;
-    k_adj_su<<<blocks(n), 128, 0, st>>>(N, cur, nxt, a, c, c2);
-    if (cf.do_pe) {
-        const double cst = cf.tau * cf.dt_pe / (2. * cf.g * cf.g);
-        const double cdt = cf.dt_pe / cf.tau;
-        k_adj_se<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, cst, cdt);
-    }
+    const AdjCoef<T> k(cf);
+    k_adj_su<<<blocks(n), 128, 0, st>>>(N, cur, nxt, a, k.c, k.c2);
+    if (cf.do_pe) k_adj_se<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, k.cst, k.cdt);
 }
 
-void launch_adjoint_ttt(int N, const State<double> &s, const double *tbar, const AdjState &a,
-                        double g, double tau, cudaStream_t st) {
+template <typename T>
+void launch_adjoint_ttt(int N, const State<T> &s, const T *tbar, const AdjStateT<T> &a, double g,
+                        double tau, cudaStream_t st) {
     const size_t n = (size_t)N * N;
-    k_adj_ttt<<<blocks(n), 128, 0, st>>>(N, s, tbar, a, g, tau);
+    k_adj_ttt<<<blocks(n), 128, 0, st>>>(N, s, tbar, a, (T)g, (T)tau);
 }
 
-void launch_adjoint_project(size_t n, const AdjState &a, cudaStream_t st) {
+template <typename T>
+void launch_adjoint_project(size_t n, const AdjStateT<T> &a, cudaStream_t st) {
     k_adj_project<<<blocks(n), 128, 0, st>>>(n, a);
+}
+
+template void launch_inverse_adjoint_step<double>(int, const State<double> &,
+                                                  const State<double> &, const AdjState &,
+                                                  const StepCoef<double> &, cudaStream_t);
+template void launch_inverse_adjoint_step<float>(int, const State<float> &, const State<float> &,
+                                                 const AdjStateT<float> &,
+                                                 const StepCoef<double> &, cudaStream_t);
+template void launch_adjoint_step<double>(int, const State<double> &, const State<double> &,
+                                          const AdjState &, const StepCoef<double> &,
+                                          cudaStream_t);
+template void launch_adjoint_step<float>(int, const State<float> &, const State<float> &,
+                                         const AdjStateT<float> &, const StepCoef<double> &,
+                                         cudaStream_t);
+template void launch_adjoint_ttt<double>(int, const State<double> &, const double *,
+                                         const AdjState &, double, double, cudaStream_t);
+template void launch_adjoint_ttt<float>(int, const State<float> &, const float *,
+                                        const AdjStateT<float> &, double, double, cudaStream_t);
+template void launch_adjoint_project<double>(size_t, const AdjState &, cudaStream_t);
+template void launch_adjoint_project<float>(size_t, const AdjStateT<float> &, cudaStream_t);
+
+// FP32 adjoint buffers (18 real planes a field) -> FP64 adjoint buffers
+__global__ void k_adj_widen(size_t count, const float *src, double *dst) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) dst[i] = (double)src[i];
+}
+
+void launch_adjoint_widen(size_t n, const AdjStateT<float> &src, const AdjState &dst,
+                          cudaStream_t st) {
+    const C<float> *s[6] = {src.ux, src.uy, src.e1, src.e2, src.phi, src.pi};
+    C<double> *d[6] = {dst.ux, dst.uy, dst.e1, dst.e2, dst.phi, dst.pi};
+    for (int f = 0; f < 6; f++)
+        k_adj_widen<<<blocks(18 * n), 128, 0, st>>>(18 * n, reinterpret_cast<const float *>(s[f]),
+                                                    reinterpret_cast<double *>(d[f]));
 }
 
 // [9 complex planes][n] -> per site 18 doubles, for the host copy

@@ -118,6 +118,14 @@ struct ipg_ctx {
         C<double> *vbA = nullptr, *vbB = nullptr, *vcur = nullptr;
         double *g2mu_bar = nullptr;
         double *rho_all = nullptr;  // [2][Ny][n][8] rho adjoint, kept on the device
+        // FP32 adjoint (contexts of the FP32 form): the plain form's states and
+        // adjoints in FP32; the tau = 0 adjoint is widened into adj at the end
+        bool fp32 = false;
+        std::vector<State<float>> cp32;
+        State<float> w32[3]{};
+        State<float> fin32{};
+        AdjStateT<float> adj32{};
+        float *tbar32 = nullptr;
     } aw;
 
     // output files formatted on the GPU (ipg_write_outputs); freed by ipg_destroy
@@ -1545,7 +1553,7 @@ ipg_status ipg_forward(ipg_ctx *c, int checkpoint_every, double *E_T, double *ep
         IPG_TRY(dalloc(c, &A.adj.pi, 9 * n));
         IPG_TRY(dalloc(c, &A.tbar, n));
     }
-    while ((int)A.cp.size() < ncp) {
+    while (!is_fp32(c) && (int)A.cp.size() < ncp) {
         State<double> st{};
         IPG_TRY(alloc_state(st));
         A.cp.push_back(st);
@@ -1554,11 +1562,90 @@ ipg_status ipg_forward(ipg_ctx *c, int checkpoint_every, double *E_T, double *ep
     A.steps = S;
     A.ready = false;
     A.from_inputs = c->init_from_inputs;
+    A.fp32 = is_fp32(c);
+    if (A.fp32) {
+        // FP32 adjoint: the plain form (full links, no reunitarisation) stepped
+        // in FP32 from the FP64 tau = 0 state rounded once
+        auto alloc32 = [&](State<float> &st) -> ipg_status {
+            IPG_TRY(dalloc(c, &st.ux, 9 * n));
+            IPG_TRY(dalloc(c, &st.uy, 9 * n));
+            IPG_TRY(dalloc(c, &st.e1, 8 * n));
+            IPG_TRY(dalloc(c, &st.e2, 8 * n));
+            IPG_TRY(dalloc(c, &st.phi, 9 * n));
+            IPG_TRY(dalloc(c, &st.pi, 9 * n));
+            return IPG_OK;
+        };
+        if (!A.w32[0].ux) {
+            for (auto &st : A.w32) IPG_TRY(alloc32(st));
+            IPG_TRY(dalloc(c, &A.adj32.ux, 9 * n));
+            IPG_TRY(dalloc(c, &A.adj32.uy, 9 * n));
+            IPG_TRY(dalloc(c, &A.adj32.e1, 9 * n));
+            IPG_TRY(dalloc(c, &A.adj32.e2, 9 * n));
+            IPG_TRY(dalloc(c, &A.adj32.phi, 9 * n));
+            IPG_TRY(dalloc(c, &A.adj32.pi, 9 * n));
+            IPG_TRY(dalloc(c, &A.tbar32, n));
+        }
+        while ((int)A.cp32.size() < (store_all ? S + 1 : ncp)) {
+            State<float> st{};
+            IPG_TRY(alloc32(st));
+            A.cp32.push_back(st);
+        }
+    }
 
-    // forward in FP64 from the tau = 0 state (the context's own state is kept)
+    // forward from the tau = 0 state (the context's own state is kept)
     IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     State<double> cur;
-    if (store_all) {
+    if (A.fp32) {
+        auto copy32 = [&](const State<float> &d, const State<float> &s_) -> ipg_status {
+            IPG_CUDA(c, cudaMemcpyAsync(d.ux, s_.ux, 9 * n * sizeof(C<float>),
+                                        cudaMemcpyDeviceToDevice, c->stream));
+            IPG_CUDA(c, cudaMemcpyAsync(d.uy, s_.uy, 9 * n * sizeof(C<float>),
+                                        cudaMemcpyDeviceToDevice, c->stream));
+            IPG_CUDA(c, cudaMemcpyAsync(d.e1, s_.e1, 8 * n * sizeof(float),
+                                        cudaMemcpyDeviceToDevice, c->stream));
+            IPG_CUDA(c, cudaMemcpyAsync(d.e2, s_.e2, 8 * n * sizeof(float),
+                                        cudaMemcpyDeviceToDevice, c->stream));
+            IPG_CUDA(c, cudaMemcpyAsync(d.phi, s_.phi, 9 * n * sizeof(float),
+                                        cudaMemcpyDeviceToDevice, c->stream));
+            IPG_CUDA(c, cudaMemcpyAsync(d.pi, s_.pi, 9 * n * sizeof(float),
+                                        cudaMemcpyDeviceToDevice, c->stream));
+            return IPG_OK;
+        };
+        State<float> c32;
+        if (store_all) {
+            launch_convert_plain<double, float>(n, c->s64, A.cp32[0], c->stream);
+            IPG_LAUNCHED(c, 1);
+            for (int s = 0; s < S; s++) {
+                launch_leapfrog_plain32(c->d_ev, N, A.cp32[s], A.cp32[s + 1],
+                                        evolution_coef(c, s), c->stream);
+                IPG_LAUNCHED(c, 1);
+            }
+            c32 = A.cp32[S];
+        } else {
+            launch_convert_plain<double, float>(n, c->s64, A.w32[0], c->stream);
+            IPG_LAUNCHED(c, 1);
+            c32 = A.w32[0];
+            State<float> other = A.w32[1];
+            for (int s = 0; s < S; s++) {
+                if (s % checkpoint_every == 0)
+                    IPG_TRY(copy32(A.cp32[s / checkpoint_every], c32));
+                State<float> out = c32;  // E and pi in place
+                out.ux = other.ux;
+                out.uy = other.uy;
+                out.phi = other.phi;
+                launch_leapfrog_plain32(c->d_ev, N, c32, out, evolution_coef(c, s), c->stream);
+                IPG_LAUNCHED(c, 1);
+                std::swap(c32.ux, other.ux);
+                std::swap(c32.uy, other.uy);
+                std::swap(c32.phi, other.phi);
+            }
+        }
+        A.fin32 = c32;
+        // T^tautau of the final state in FP64 (the loss), from a widened copy
+        launch_convert_plain<float, double>(n, c32, A.w[2], c->stream);
+        IPG_LAUNCHED(c, 1);
+        cur = A.w[2];
+    } else if (store_all) {
         IPG_TRY(copy_state(c, A.cp[0], c->s64));
         for (int s = 0; s < S; s++) {
             launch_leapfrog_into(c->d_ev, N, A.cp[s], A.cp[s + 1], evolution_coef(c, s),
@@ -1655,12 +1742,65 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
                            d6[5] * i * j);
         tb[p] = v / a4;
     }
+    if (A.fp32) {
+        // the reverse sweep in FP32 on the plain form's FP32 states, then the
+        // tau = 0 adjoint widened to FP64 for the initial conditions
+        std::vector<float> tb32(tb.begin(), tb.end());
+        IPG_CUDA(c, cudaMemcpyAsync(A.tbar32, tb32.data(), n * sizeof(float),
+                                    cudaMemcpyHostToDevice, c->stream));
+        IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+        for (C<float> *b : {A.adj32.ux, A.adj32.uy, A.adj32.e1, A.adj32.e2, A.adj32.phi,
+                            A.adj32.pi})
+            IPG_CUDA(c, cudaMemsetAsync(b, 0, 9 * n * sizeof(C<float>), c->stream));
+        launch_adjoint_ttt<float>(N, A.fin32, A.tbar32, A.adj32, c->cfg.g, S * c->dtau,
+                                  c->stream);
+        IPG_LAUNCHED(c, 1);
+        if (A.k == 1) {
+            for (int s = S - 1; s >= 0; s--) {
+                const StepCoef<double> cf = evolution_coef(c, s);
+                launch_adjoint_step<float>(N, A.cp32[s], A.cp32[s + 1], A.adj32, cf, c->stream);
+                IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
+            }
+        } else {
+            A.ready = false;  // the sweep overwrites the final state
+            State<float> sets[2] = {A.w32[2], A.fin32};
+            State<float> nxt = A.fin32;
+            for (int s = S - 1, q = 0; s >= 0; s--, q++) {
+                const State<float> cur = sets[q & 1];
+                const StepCoef<double> cf = evolution_coef(c, s);
+                if (s % A.k == 0) {
+                    const State<float> &src = A.cp32[s / A.k];
+                    IPG_CUDA(c, cudaMemcpyAsync(cur.ux, src.ux, 9 * n * sizeof(C<float>),
+                                                cudaMemcpyDeviceToDevice, c->stream));
+                    IPG_CUDA(c, cudaMemcpyAsync(cur.uy, src.uy, 9 * n * sizeof(C<float>),
+                                                cudaMemcpyDeviceToDevice, c->stream));
+                    IPG_CUDA(c, cudaMemcpyAsync(cur.e1, src.e1, 8 * n * sizeof(float),
+                                                cudaMemcpyDeviceToDevice, c->stream));
+                    IPG_CUDA(c, cudaMemcpyAsync(cur.e2, src.e2, 8 * n * sizeof(float),
+                                                cudaMemcpyDeviceToDevice, c->stream));
+                    IPG_CUDA(c, cudaMemcpyAsync(cur.phi, src.phi, 9 * n * sizeof(float),
+                                                cudaMemcpyDeviceToDevice, c->stream));
+                    IPG_CUDA(c, cudaMemcpyAsync(cur.pi, src.pi, 9 * n * sizeof(float),
+                                                cudaMemcpyDeviceToDevice, c->stream));
+                    launch_adjoint_step<float>(N, cur, nxt, A.adj32, cf, c->stream);
+                    IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
+                } else {
+                    launch_inverse_adjoint_step<float>(N, nxt, cur, A.adj32, cf, c->stream);
+                    IPG_LAUNCHED(c, cf.do_pe ? 3 : 2);
+                }
+                nxt = cur;
+            }
+        }
+        launch_adjoint_project<float>(n, A.adj32, c->stream);
+        launch_adjoint_widen(n, A.adj32, A.adj, c->stream);
+        IPG_LAUNCHED(c, 7);
+    } else {
     IPG_CUDA(c, cudaMemcpyAsync(A.tbar, tb.data(), n * sizeof(double), cudaMemcpyHostToDevice,
                                 c->stream));
     IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     for (C<double> *b : {A.adj.ux, A.adj.uy, A.adj.e1, A.adj.e2, A.adj.phi, A.adj.pi})
         IPG_CUDA(c, cudaMemsetAsync(b, 0, 9 * n * sizeof(C<double>), c->stream));
-    launch_adjoint_ttt(N, A.fin, A.tbar, A.adj, c->cfg.g, S * c->dtau, c->stream);
+    launch_adjoint_ttt<double>(N, A.fin, A.tbar, A.adj, c->cfg.g, S * c->dtau, c->stream);
     IPG_LAUNCHED(c, 1);
     if (A.k == 1) {
         // every state stored: no time reversal, nothing overwritten
@@ -1691,8 +1831,9 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
             nxt = cur;
         }
     }
-    launch_adjoint_project(n, A.adj, c->stream);
+    launch_adjoint_project<double>(n, A.adj, c->stream);
     IPG_LAUNCHED(c, 1);
+    }
     if (grad_g2mu || grad_rho) IPG_TRY(backward_inputs(c, grad_g2mu, grad_rho));
     IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     IPG_TRY(sync(c));

@@ -250,42 +250,43 @@ __device__ __forceinline__ void leapfrog_full_site(int N, int ix, int iy, const 
 // and phi of the step's input already recovered in `cur`,
 //   pi = pi' - cdt br(U, phi),   E_d = E_d' - TL(cst t_d + cdt i[U_d phi(+d) U_d^dag, phi])
 // from the same staple and transport code as the forward step.
+template <typename T>
 __global__ void __launch_bounds__(128)
-    k_inv_se(int N, State<double> nxt, State<double> cur, StepCoef<double> cf) {
+    k_inv_se(int N, State<T> nxt, State<T> cur, StepCoef<double> cf) {
     const int iy = blockIdx.x * blockDim.x + threadIdx.x;
     const int ix = blockIdx.y * blockDim.y + threadIdx.y;
     if (ix >= N || iy >= N) return;
-    const FullLoadGlobal<double> ld(cur, N, ix, iy);
+    const FullLoadGlobal<T> ld(cur, N, ix, iy);
     const size_t pos = ld.pos, n = ld.n;
-    H3<double> pi = ld_h(nxt.pi, pos, n);
-    H3<double> e1 = ld_h8(nxt.e1, pos, n), e2 = ld_h8(nxt.e2, pos, n);
+    H3<T> pi = ld_h(nxt.pi, pos, n);
+    H3<T> e1 = ld_h8(nxt.e1, pos, n), e2 = ld_h8(nxt.e2, pos, n);
     if (cf.do_pe) {
-        H3<double> t1, t2;
-        full_staples<double>(ld, t1, t2);
-        const double cst = cf.tau * cf.dt_pe / (2. * cf.g * cf.g);
-        const double cdt = cf.dt_pe / cf.tau;
-        H3<double> d1 = {}, d2 = {};
+        H3<T> t1, t2;
+        full_staples<T>(ld, t1, t2);
+        const T cst = (T)(cf.tau * cf.dt_pe / (2. * cf.g * cf.g));
+        const T cdt = (T)(cf.dt_pe / cf.tau);
+        H3<T> d1 = {}, d2 = {};
         h_axpy(d1, cst, t1);
         h_axpy(d2, cst, t2);
-        H3<double> br;
+        H3<T> br;
         {
-            H3<double> phx = conj_h(ld.template link<kLx, 0, 0>(), ld.template phi<1, 0>());
+            H3<T> phx = conj_h(ld.template link<kLx, 0, 0>(), ld.template phi<1, 0>());
             h_axpy(d1, cdt, i_commutator(phx, ld.template phi<0, 0>()));
             br = phx;
         }
         {
-            H3<double> phy = conj_h(ld.template link<kLy, 0, 0>(), ld.template phi<0, 1>());
+            H3<T> phy = conj_h(ld.template link<kLy, 0, 0>(), ld.template phi<0, 1>());
             h_axpy(d2, cdt, i_commutator(phy, ld.template phi<0, 0>()));
             h_add(br, phy);
         }
         h_add(br, conj_h_dag(ld.template link<kLx, -1, 0>(), ld.template phi<-1, 0>()));
         h_add(br, conj_h_dag(ld.template link<kLy, 0, -1>(), ld.template phi<0, -1>()));
-        h_axpy(br, -4., ld.template phi<0, 0>());
+        h_axpy(br, T(-4.), ld.template phi<0, 0>());
         h_axpy(pi, -cdt, br);
         h_traceless(d1);
         h_traceless(d2);
-        h_axpy(e1, -1., d1);
-        h_axpy(e2, -1., d2);
+        h_axpy(e1, T(-1.), d1);
+        h_axpy(e2, T(-1.), d2);
         h_traceless(e1);
         h_traceless(e2);
     }
@@ -294,10 +295,15 @@ __global__ void __launch_bounds__(128)
     st_h8(cur.e2, pos, n, e2);
 }
 
-void launch_inverse_se(int N, const State<double> &nxt, const State<double> &cur,
-                       const StepCoef<double> &cf, cudaStream_t st) {
-    k_inv_se<<<dim3((N + 31) / 32, (N + 3) / 4), dim3(32, 4), 0, st>>>(N, nxt, cur, cf);
+template <typename T>
+void launch_inverse_se(int N, const State<T> &nxt, const State<T> &cur, const StepCoef<double> &cf,
+                       cudaStream_t st) {
+    k_inv_se<T><<<dim3((N + 31) / 32, (N + 3) / 4), dim3(32, 4), 0, st>>>(N, nxt, cur, cf);
 }
+template void launch_inverse_se<double>(int, const State<double> &, const State<double> &,
+                                        const StepCoef<double> &, cudaStream_t);
+template void launch_inverse_se<float>(int, const State<float> &, const State<float> &,
+                                       const StepCoef<double> &, cudaStream_t);
 
 template <typename T, bool REUNIT>
 __global__ void __launch_bounds__(128)
@@ -1771,6 +1777,37 @@ void launch_leapfrog_into(const EventGeom *d_ev, int N, const State<double> &in,
         cudaMemcpyAsync(out.pi, in.pi, 9 * n * sizeof(double), cudaMemcpyDeviceToDevice, st);
     }
     launch_leapfrog_site<double>(d_ev, N, s, out.ux, out.uy, out.phi, cf, false, st);
+}
+
+// One step of the plain form (full links, Taylor-2 update, no
+// reunitarisation) in FP32, from the state `in` into `out` (E and pi copied,
+// then updated in place in `out`; U and phi written to `out`): the forward
+// sweep of the FP32 adjoint. `in` and `out` may be the same state only when
+// out's U/phi are separate buffers (ux_out etc.).
+void launch_leapfrog_plain32(const EventGeom *d_ev, int N, const State<float> &in,
+                             const State<float> &out, const StepCoef<double> &cf,
+                             cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    if (out.e1 != in.e1) {
+        cudaMemcpyAsync(out.e1, in.e1, 8 * n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(out.e2, in.e2, 8 * n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(out.pi, in.pi, 9 * n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    }
+    State<float> s = in;
+    s.e1 = out.e1;
+    s.e2 = out.e2;
+    s.pi = out.pi;
+    StepCoef<float> c;
+    c.tau = (float)cf.tau;
+    c.dt_pe = (float)cf.dt_pe;
+    c.dt_pu = (float)cf.dt_pu;
+    c.g = (float)cf.g;
+    c.do_pe = cf.do_pe;
+    c.do_pu = cf.do_pu;
+    set_derived(c);
+    dim3 block(32, 4);
+    dim3 grid((N + 31) / 32, (N + 3) / 4);
+    k_leapfrog<float, false><<<grid, block, 0, st>>>(d_ev, s, out.ux, out.uy, out.phi, c);
 }
 
 // one thread per site (lattices smaller than 32 sites per side)

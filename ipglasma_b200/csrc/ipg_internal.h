@@ -237,28 +237,40 @@ void launch_tmunu_diag(const TmunuArgs &a, cudaStream_t st);
 // ---- adjoint ---------------------------------------------------------------
 // Adjoint buffers of the six fields, each sized as 9 complex planes and
 // holding 18 real planes (entry k: real part in plane 2k, imaginary in 2k+1).
-struct AdjState {
-    C<double> *ux, *uy, *e1, *e2, *phi, *pi;
+template <typename T>
+struct AdjStateT {
+    C<T> *ux, *uy, *e1, *e2, *phi, *pi;
 };
+using AdjState = AdjStateT<double>;
 // time reversal of one FP64 step: state after (nxt) -> state before (cur)
 void launch_inverse_step(int N, const State<double> &nxt, const State<double> &cur,
                          const StepCoef<double> &cf, cudaStream_t st);
 // E and pi of the step's input from its output nxt and the recovered U, phi
-// in cur (evolve.cu)
-void launch_inverse_se(int N, const State<double> &nxt, const State<double> &cur,
+// in cur (evolve.cu); T = double or float (full links, plain form)
+template <typename T>
+void launch_inverse_se(int N, const State<T> &nxt, const State<T> &cur,
                        const StepCoef<double> &cf, cudaStream_t st);
 // the time reversal nxt -> cur and the adjoint step together (fewer launches
 // than launch_inverse_step then launch_adjoint_step, same results)
-void launch_inverse_adjoint_step(int N, const State<double> &nxt, const State<double> &cur,
-                                 const AdjState &a, const StepCoef<double> &cf, cudaStream_t st);
+template <typename T>
+void launch_inverse_adjoint_step(int N, const State<T> &nxt, const State<T> &cur,
+                                 const AdjStateT<T> &a, const StepCoef<double> &cf,
+                                 cudaStream_t st);
 // adjoints of a step's outputs -> adjoints of its inputs (in place); cur is the
-// state before the step, nxt the state after it
-void launch_adjoint_step(int N, const State<double> &cur, const State<double> &nxt,
-                         const AdjState &a, const StepCoef<double> &cf, cudaStream_t st);
+// state before the step, nxt the state after it. T = double, or float for the
+// FP32 adjoint (states and adjoints in FP32, the plain form's step)
+template <typename T>
+void launch_adjoint_step(int N, const State<T> &cur, const State<T> &nxt, const AdjStateT<T> &a,
+                         const StepCoef<double> &cf, cudaStream_t st);
 // tbar[n] = dL/dTtt (lattice units) -> field adjoints (accumulated)
-void launch_adjoint_ttt(int N, const State<double> &s, const double *tbar, const AdjState &a,
-                        double g, double tau, cudaStream_t st);
-void launch_adjoint_project(size_t n, const AdjState &a, cudaStream_t st);
+template <typename T>
+void launch_adjoint_ttt(int N, const State<T> &s, const T *tbar, const AdjStateT<T> &a, double g,
+                        double tau, cudaStream_t st);
+template <typename T>
+void launch_adjoint_project(size_t n, const AdjStateT<T> &a, cudaStream_t st);
+// FP32 adjoint buffers -> FP64 ones (for the initial-condition adjoint)
+void launch_adjoint_widen(size_t n, const AdjStateT<float> &src, const AdjState &dst,
+                          cudaStream_t st);
 // adjoint buffer (18 real planes) -> [n][18] doubles, (re, im) per entry
 void launch_planes_to_sites(size_t n, const C<double> *src, double *dst, cudaStream_t st);
 // adjoint of the tau = 0 links and pi: pi_bar, U_bar(tau=0) (in adj) ->
@@ -346,6 +358,13 @@ void launch_output_text(int kind, const OutputGrid &g, const OutputFields &f, lo
                         char *chunks, int *chunk_len, long long *chunk_off, char *text,
                         double *term, int *bad, cudaStream_t st);
 
+// plain (full-link) state in one precision -> the other, element by element
+template <typename S, typename D>
+void launch_convert_plain(size_t n, const State<S> &src, const State<D> &dst, cudaStream_t st);
+// one FP32 step of the plain form from `in` into `out` (the FP32 adjoint's forward)
+void launch_leapfrog_plain32(const EventGeom *d_ev, int N, const State<float> &in,
+                             const State<float> &out, const StepCoef<double> &cf,
+                             cudaStream_t st);
 template <typename T>
 void launch_convert_state(size_t n, const State<T> &src, State<double> &dst,
                           cudaStream_t st);
