@@ -687,7 +687,9 @@ def measure_large(torch, ipg, rank, world, dist, hbm):
     su64 = su / (res["evo64"] * 1e-3)
     g32 = su32 * BYTES_PER_SITE_UPDATE["fp32"] / 1e9
     g64 = su64 * BYTES_PER_SITE_UPDATE["fp64"] / 1e9
+    adj = measure_large_adjoint(torch, ipg, w, mine[0])
     return {"config": workload_config(w, world),
+            "adjoint_eps2": adj,
             "events_per_s": {"fp32": round(n_ev * 2 / (res["ms32"] * 1e-3), 3),
                              "fp64": round(n_ev * 2 / (res["ms64"] * 1e-3), 3)},
             "ms_per_step": {"fp32": round(res["ms32"] / 2, 1), "fp64": round(res["ms64"] / 2, 1)},
@@ -703,6 +705,42 @@ def measure_large(torch, ipg, rank, world, dist, hbm):
             "initial_condition_stages": res["stages"],
             "error": res["err"],
             "timing": "2 timed batch steps per form after 1 warm-up; CUDA events"}
+
+
+def measure_large_adjoint(torch, ipg, w, spec):
+    """The gradient of eps2 for one event of the large workload (1024^2,
+    Ny 100, 512 steps) with the FP32 adjoint (an FP32 context) and the FP64
+    adjoint, both with a checkpoint every 23 steps and time reversal between
+    them; the same noise (device Philox, same key), Newton to 1e-12.
+    Forward = initial conditions + evolution storing checkpoints + T^tautau;
+    backward = reverse sweep + initial-condition adjoint (device times)."""
+    from ipglasma_b200.synthetic import make_event
+    A, B, _, _ = make_event(spec["N"], spec["L"], spec["nucleus"], spec["b"], spec["seed"],
+                            g=w["g"])
+    out, grads = {}, {}
+    for name, prec in (("fp32", ipg.FP32), ("fp64", ipg.FP64)):
+        ev = ipg.Event(ipg.Config(size=spec["N"], L=spec["L"], Ny=w["Ny"], g=w["g"], m=w["m"],
+                                  maxtime=w["maxtime"], dtau=w["dtau"], precision=prec,
+                                  seed=4242, newton_tolerance=1e-12))
+        ev.set_g2mu(A, B)
+        ev.use_device_noise()
+        rep = ev.init_fields(allow_nonconverged=True)
+        _, e2 = ev.forward(23)
+        g = ev.backward(0.0, 1.0, inputs=True)
+        f_ms, b_ms = ev.adjoint_stats()
+        init_ms = rep.ms_wilson + rep.ms_newton + rep.ms_fields
+        out[name] = {"eps2": e2, "device_ms_forward": round(init_ms + f_ms, 1),
+                     "device_ms_backward": round(b_ms, 1),
+                     "adjoint_over_forward": round(b_ms / (init_ms + f_ms), 3)}
+        grads[name] = (np.array(g["g2mu"]), np.array(g[ipg.UX]))
+        ev.close()
+    for k, key in enumerate(("grad_g2mu", "grad_Ux_tau0")):
+        a, b = grads["fp32"][k], grads["fp64"][k]
+        out[f"{key}_rel_diff_fp32_vs_fp64"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out["workload"] = (f"one {spec['nucleus']}+{spec['nucleus']} {spec['N']}^2 event of the "
+                       f"batch (b = {spec['b']:.2f} fm), Ny {w['Ny']}, {steps_of(w, w['classes'][0])} "
+                       "steps, loss eps2, checkpoint every 23 steps")
+    return out
 
 
 def measure_single(torch, ipg, K, W, rank, world, dist, hbm):

@@ -311,8 +311,13 @@ ipg_status ipg_output_names(int event_id, int it, double dtau, double a,
                             size_t tmunu_len);
 
 /* ---- adjoint (no counterpart in the reference) ---------------------------
- * Reverse-mode derivatives of the evolution in FP64, with the autograd
- * contract: ipg_forward saves what ipg_backward consumes once. The loss is
+ * Reverse-mode derivatives of the evolution, with the autograd contract:
+ * ipg_forward saves what ipg_backward consumes once. On an FP64 context the
+ * plain form is differentiated in FP64. On an FP32 context (the FP32 adjoint)
+ * the plain form's forward and reverse sweeps run in FP32 (full FP32 links,
+ * no reunitarisation; the FP64 tau = 0 state rounded once), and the adjoint
+ * of the tau = 0 state is widened to FP64 for the initial conditions. The
+ * loss is
  *   L = w_ET * E_T + w_eps2 * eps2
  * at tau = itmax dtau a, from the state after the itmax leapfrog launches of
  * Evolution::run (where the reference evaluates T^{mu nu}):

@@ -1434,8 +1434,10 @@ ipg_status backward_inputs(ipg_ctx *c, double *grad_g2mu, double *grad_rho) {
     ai.u2x = c->u2x;
     ai.u1y = c->u1y;
     ai.u2y = c->u2y;
-    ai.ux = A.cp[0].ux;  // the tau = 0 links kept by ipg_forward
-    ai.uy = A.cp[0].uy;
+    // the tau = 0 links kept by ipg_forward (FP64: checkpoint 0; FP32
+    // adjoint: the FP64 copy in work state 0)
+    ai.ux = A.fp32 ? A.w[0].ux : A.cp[0].ux;
+    ai.uy = A.fp32 ? A.w[0].uy : A.cp[0].uy;
     ai.VA = c->VA;
     ai.VB = c->VB;
     ai.alpha = c->newton_alpha;
@@ -1611,6 +1613,8 @@ ipg_status ipg_forward(ipg_ctx *c, int checkpoint_every, double *E_T, double *ep
                                         cudaMemcpyDeviceToDevice, c->stream));
             return IPG_OK;
         };
+        // the FP64 tau = 0 state, kept for the initial-condition adjoint
+        IPG_TRY(copy_state(c, A.w[0], c->s64));
         State<float> c32;
         if (store_all) {
             launch_convert_plain<double, float>(n, c->s64, A.cp32[0], c->stream);
@@ -1795,44 +1799,44 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
         launch_adjoint_widen(n, A.adj32, A.adj, c->stream);
         IPG_LAUNCHED(c, 7);
     } else {
-    IPG_CUDA(c, cudaMemcpyAsync(A.tbar, tb.data(), n * sizeof(double), cudaMemcpyHostToDevice,
-                                c->stream));
-    IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-    for (C<double> *b : {A.adj.ux, A.adj.uy, A.adj.e1, A.adj.e2, A.adj.phi, A.adj.pi})
-        IPG_CUDA(c, cudaMemsetAsync(b, 0, 9 * n * sizeof(C<double>), c->stream));
-    launch_adjoint_ttt<double>(N, A.fin, A.tbar, A.adj, c->cfg.g, S * c->dtau, c->stream);
-    IPG_LAUNCHED(c, 1);
-    if (A.k == 1) {
-        // every state stored: no time reversal, nothing overwritten
-        for (int s = S - 1; s >= 0; s--) {
-            const StepCoef<double> cf = evolution_coef(c, s);
-            launch_adjoint_step(N, A.cp[s], A.cp[s + 1], A.adj, cf, c->stream);
-            IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
-        }
-    } else {
-        // reverse sweep: state s from state s+1 by time reversal, or from the
-        // checkpoint when s is a multiple of k; two state sets alternate.
-        // From its second step on the sweep overwrites the final state, so a
-        // failure anywhere below must leave the forward marked as consumed.
-        A.ready = false;
-        State<double> sets[2] = {A.w[2], A.fin};
-        State<double> nxt = A.fin;
-        for (int s = S - 1, q = 0; s >= 0; s--, q++) {
-            const State<double> cur = sets[q & 1];
-            const StepCoef<double> cf = evolution_coef(c, s);
-            if (s % A.k == 0) {
-                IPG_TRY(copy_state(c, cur, A.cp[s / A.k]));
-                launch_adjoint_step(N, cur, nxt, A.adj, cf, c->stream);
+        IPG_CUDA(c, cudaMemcpyAsync(A.tbar, tb.data(), n * sizeof(double), cudaMemcpyHostToDevice,
+                                    c->stream));
+        IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+        for (C<double> *b : {A.adj.ux, A.adj.uy, A.adj.e1, A.adj.e2, A.adj.phi, A.adj.pi})
+            IPG_CUDA(c, cudaMemsetAsync(b, 0, 9 * n * sizeof(C<double>), c->stream));
+        launch_adjoint_ttt<double>(N, A.fin, A.tbar, A.adj, c->cfg.g, S * c->dtau, c->stream);
+        IPG_LAUNCHED(c, 1);
+        if (A.k == 1) {
+            // every state stored: no time reversal, nothing overwritten
+            for (int s = S - 1; s >= 0; s--) {
+                const StepCoef<double> cf = evolution_coef(c, s);
+                launch_adjoint_step(N, A.cp[s], A.cp[s + 1], A.adj, cf, c->stream);
                 IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
-            } else {
-                launch_inverse_adjoint_step(N, nxt, cur, A.adj, cf, c->stream);
-                IPG_LAUNCHED(c, cf.do_pe ? 3 : 2);
             }
-            nxt = cur;
+        } else {
+            // reverse sweep: state s from state s+1 by time reversal, or from the
+            // checkpoint when s is a multiple of k; two state sets alternate.
+            // From its second step on the sweep overwrites the final state, so a
+            // failure anywhere below must leave the forward marked as consumed.
+            A.ready = false;
+            State<double> sets[2] = {A.w[2], A.fin};
+            State<double> nxt = A.fin;
+            for (int s = S - 1, q = 0; s >= 0; s--, q++) {
+                const State<double> cur = sets[q & 1];
+                const StepCoef<double> cf = evolution_coef(c, s);
+                if (s % A.k == 0) {
+                    IPG_TRY(copy_state(c, cur, A.cp[s / A.k]));
+                    launch_adjoint_step(N, cur, nxt, A.adj, cf, c->stream);
+                    IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
+                } else {
+                    launch_inverse_adjoint_step(N, nxt, cur, A.adj, cf, c->stream);
+                    IPG_LAUNCHED(c, cf.do_pe ? 3 : 2);
+                }
+                nxt = cur;
+            }
         }
-    }
-    launch_adjoint_project<double>(n, A.adj, c->stream);
-    IPG_LAUNCHED(c, 1);
+        launch_adjoint_project<double>(n, A.adj, c->stream);
+        IPG_LAUNCHED(c, 1);
     }
     if (grad_g2mu || grad_rho) IPG_TRY(backward_inputs(c, grad_g2mu, grad_rho));
     IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
