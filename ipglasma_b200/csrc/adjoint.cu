@@ -84,6 +84,20 @@ __device__ __forceinline__ M3<T> ld_herm8(const T *p, size_t pos, size_t n) {
     return from_h(ld_h8(p, pos, n));
 }
 
+// A link of a stored state: full matrices in FP64; the FP32 adjoint works on
+// the FP32 bulk form's states, which hold the deviation W = U - 1, so the
+// identity is added back (its products with adjoints need no deviation form)
+template <typename T>
+__device__ __forceinline__ M3<T> ld_link(const C<T> *p, size_t pos, size_t n) {
+    M3<T> u = ld_m3(p, pos, n);
+    if constexpr (sizeof(T) == 4) {
+        u.m[0].r += T(1);
+        u.m[4].r += T(1);
+        u.m[8].r += T(1);
+    }
+    return u;
+}
+
 // Adjoint buffers hold 9 complex entries a site as 18 planes of n doubles:
 // the real part of entry k in plane 2k, its imaginary part in plane 2k+1
 // (the buffer is typed as 9 complex planes and has the same size). A warp's
@@ -337,7 +351,7 @@ __global__ void k_adj_su(int N, State<T> cur, State<T> nxt, AdjStateT<T> a, T c,
         C<T> *Ub = d ? a.uy : a.ux;
         C<T> *Eb = d ? a.e2 : a.e1;
         const M3<T> Ubar = ld_adj(Ub, pos, n);
-        const M3<T> U = ld_m3(d ? cur.uy : cur.ux, pos, n);
+        const M3<T> U = ld_link(d ? cur.uy : cur.ux, pos, n);
         const M3<T> X = times_i(ld_herm8(d ? nxt.e2 : nxt.e1, pos, n), c);
         const M3<T> M = taylor2(X);
         st_adj(Ub, pos, n, mul_dn(M, Ubar));
@@ -425,19 +439,19 @@ __global__ void __launch_bounds__(128) k_adj_se(int N, State<T> cur, AdjStateT<T
     const int role = blockIdx.y;
     if (role == 0) {
         const H3<T> h1 = ld_h8a(a.e1, pos, n);
-        const M3<T> ux = ld_m3(cur.ux, pos, n);
+        const M3<T> ux = ld_link(cur.ux, pos, n);
         M3<T> acc;
         {
-            const M3<T> uy_px = ld_m3(cur.uy, G.pX, n);
-            const M3<T> B = mul(ld_m3(cur.uy, pos, n), ld_m3(cur.ux, G.pY, n));
+            const M3<T> uy_px = ld_link(cur.uy, G.pX, n);
+            const M3<T> B = mul(ld_link(cur.uy, pos, n), ld_link(cur.ux, G.pY, n));
             const M3<T> Mb = times_i(minus(sc(from_h(h1), cst), sc(from_h(ld_h8a(a.e2, pos, n)), cst)), -T(2.));
             const M3<T> Ab = mul(Mb, B);
             acc = mul_nd(Ab, uy_px);
             atomic_add_m(a.uy, G.pX, n, mul_dn(ux, Ab));
         }
         {
-            const M3<T> uy_pxmy = ld_m3(cur.uy, G.pXmY, n);
-            const M3<T> Q = mul_dn(ld_m3(cur.ux, G.mY, n), ld_m3(cur.uy, G.mY, n));
+            const M3<T> uy_pxmy = ld_link(cur.uy, G.pXmY, n);
+            const M3<T> Q = mul_dn(ld_link(cur.ux, G.mY, n), ld_link(cur.uy, G.mY, n));
             const M3<T> Pb = mul_nd(times_i(sc(from_h(h1), cst), -T(2.)), Q);
             add_to(acc, mul(Pb, uy_pxmy));
             atomic_add_m(a.uy, G.pXmY, n, mul_dn(Pb, ux));
@@ -451,19 +465,19 @@ __global__ void __launch_bounds__(128) k_adj_se(int N, State<T> cur, AdjStateT<T
         }
     } else if (role == 1) {
         const H3<T> h2 = ld_h8a(a.e2, pos, n);
-        const M3<T> uy = ld_m3(cur.uy, pos, n);
+        const M3<T> uy = ld_link(cur.uy, pos, n);
         M3<T> acc;
         {
-            const M3<T> ux_py = ld_m3(cur.ux, G.pY, n);
-            const M3<T> A = mul(ld_m3(cur.ux, pos, n), ld_m3(cur.uy, G.pX, n));
+            const M3<T> ux_py = ld_link(cur.ux, G.pY, n);
+            const M3<T> A = mul(ld_link(cur.ux, pos, n), ld_link(cur.uy, G.pX, n));
             const M3<T> Mb = times_i(minus(sc(from_h(ld_h8a(a.e1, pos, n)), cst), sc(from_h(h2), cst)), -T(2.));
             const M3<T> Bb = mul_dn(Mb, A);
             acc = mul_nd(Bb, ux_py);
             atomic_add_m(a.ux, G.pY, n, mul_dn(uy, Bb));
         }
         {
-            const M3<T> ux_mxpy = ld_m3(cur.ux, G.mXpY, n);
-            const M3<T> Q = mul_dn(ld_m3(cur.uy, G.mX, n), ld_m3(cur.ux, G.mX, n));
+            const M3<T> ux_mxpy = ld_link(cur.ux, G.mXpY, n);
+            const M3<T> Q = mul_dn(ld_link(cur.uy, G.mX, n), ld_link(cur.ux, G.mX, n));
             const M3<T> Pb = mul_nd(times_i(sc(from_h(h2), cst), -T(2.)), Q);
             add_to(acc, mul(Pb, ux_mxpy));
             atomic_add_m(a.ux, G.mXpY, n, mul_dn(Pb, uy));
@@ -478,7 +492,7 @@ __global__ void __launch_bounds__(128) k_adj_se(int N, State<T> cur, AdjStateT<T
         {
             // phi += -4 brb + i[Cb_1, ph_x] + i[Cb_2, ph_y]
             M3<T> phib = icomm(sc(from_h(h2), cdt), mul_nd(mul(uy, ld_herm(cur.phi, G.pY, n)), uy));
-            const M3<T> ux = ld_m3(cur.ux, pos, n);
+            const M3<T> ux = ld_link(cur.ux, pos, n);
             add_to(phib, icomm(sc(from_h(ld_h8a(a.e1, pos, n)), cdt),
                                mul_nd(mul(ux, ld_herm(cur.phi, G.pX, n)), ux)));
             add_to(phib, sc(from_h(ld_h9a(a.pi, pos, n)), -T(4.) * cdt));
@@ -488,10 +502,10 @@ __global__ void __launch_bounds__(128) k_adj_se(int N, State<T> cur, AdjStateT<T
         const M3<T> brb = sc(from_h(ld_h9a(a.pi, pos, n)), cdt);
         {
             // E2 staple's Q side and the -x transport
-            const M3<T> uy = ld_m3(cur.uy, pos, n), ux_mxpy = ld_m3(cur.ux, G.mXpY, n);
+            const M3<T> uy = ld_link(cur.uy, pos, n), ux_mxpy = ld_link(cur.ux, G.mXpY, n);
             const M3<T> P = mul_nd(uy, ux_mxpy);
             const M3<T> Qb = mul_dn(P, times_i(sc(from_h(ld_h8a(a.e2, pos, n)), cst), -T(2.)));
-            const M3<T> ux_mx = ld_m3(cur.ux, G.mX, n), uy_mx = ld_m3(cur.uy, G.mX, n);
+            const M3<T> ux_mx = ld_link(cur.ux, G.mX, n), uy_mx = ld_link(cur.uy, G.mX, n);
             const M3<T> f = ld_herm(cur.phi, G.mX, n);
             atomic_add_m(a.uy, G.mX, n, mul_nd(ux_mx, Qb));
             M3<T> acc = mul(uy_mx, Qb);
@@ -501,10 +515,10 @@ __global__ void __launch_bounds__(128) k_adj_se(int N, State<T> cur, AdjStateT<T
         }
         {
             // E1 staple's Q side and the -y transport
-            const M3<T> ux = ld_m3(cur.ux, pos, n), uy_pxmy = ld_m3(cur.uy, G.pXmY, n);
+            const M3<T> ux = ld_link(cur.ux, pos, n), uy_pxmy = ld_link(cur.uy, G.pXmY, n);
             const M3<T> P = mul_nd(ux, uy_pxmy);
             const M3<T> Qb = mul_dn(P, times_i(sc(from_h(ld_h8a(a.e1, pos, n)), cst), -T(2.)));
-            const M3<T> ux_my = ld_m3(cur.ux, G.mY, n), uy_my = ld_m3(cur.uy, G.mY, n);
+            const M3<T> ux_my = ld_link(cur.ux, G.mY, n), uy_my = ld_link(cur.uy, G.mY, n);
             const M3<T> f = ld_herm(cur.phi, G.mY, n);
             atomic_add_m(a.ux, G.mY, n, mul_nd(uy_my, Qb));
             M3<T> acc = mul(ux_my, Qb);
@@ -538,11 +552,11 @@ __global__ void k_adj_ttt(int N, State<T> s, const T *tbar, AdjStateT<T> a, T g,
     const size_t cells[4] = {pos, pX, pY, pXY};
     for (int k = 0; k < 4; k++)
         atomic_add_h9a(a.pi, cells[k], n, sc(ld_herm(s.pi, cells[k], n), T(0.5) * tb));
-    const M3<T> ux = ld_m3(s.ux, pos, n), uy = ld_m3(s.uy, pos, n);
+    const M3<T> ux = ld_link(s.ux, pos, n), uy = ld_link(s.uy, pos, n);
     // magnetic: 2/g^2 (3 - Re tr(Ux Uy(+x) Ux(+y)^dag Uy^dag)), zero on the last row
     if (i != N - 1) {
         const T cb = -T(2.) / (g * g) * tb;
-        const M3<T> uy_px = ld_m3(s.uy, pX, n), ux_py = ld_m3(s.ux, pY, n);
+        const M3<T> uy_px = ld_link(s.uy, pX, n), ux_py = ld_link(s.ux, pY, n);
         const M3<T> A12 = mul(ux, uy_px);
         // plaq = A1 A2 A3 A4 with A1 = Ux, A2 = Uy(+x), A3 = Ux(+y)^dag, A4 = Uy^dag
         const M3<T> R = mul_nd(mul_nd(uy_px, ux_py), uy);  // A2 A3 A4
@@ -564,7 +578,7 @@ __global__ void k_adj_ttt(int N, State<T> s, const T *tbar, AdjStateT<T> a, T g,
                            {pX, pXY, s.uy, a.uy, pX}};
     for (int k = 0; k < 4; k++) {
         const Term &tm = terms[k];
-        const M3<T> u = ld_m3(tm.u, tm.pu, n), fb = ld_herm(s.phi, tm.pb, n);
+        const M3<T> u = ld_link(tm.u, tm.pu, n), fb = ld_herm(s.phi, tm.pb, n);
         const M3<T> C = mul_nd(mul(u, fb), u);
         const M3<T> d = minus(ld_herm(s.phi, tm.pa, n), C);
         const M3<T> db = sc(d, T(2.) * ht * tb);
@@ -990,12 +1004,25 @@ struct AdjCoef {
 template <typename T>
 void launch_inverse_adjoint_step(int N, const State<T> &nxt, const State<T> &cur,
                                  const AdjStateT<T> &a, const StepCoef<double> &cf,
-                                 cudaStream_t st) {
+                                 cudaStream_t st, cudaStream_t st2, cudaEvent_t fork,
+                                 cudaEvent_t join) {
     const size_t n = (size_t)N * N;
     const AdjCoef<T> k(cf);
     k_inv_adj_su<<<blocks(n), 128, 0, st>>>(N, nxt, cur, a, k.c, k.c2);
-    launch_inverse_se<T>(N, nxt, cur, cf, st);
+    if (!st2) {
+        launch_inverse_se<T>(N, nxt, cur, cf, st);
+        if (cf.do_pe) k_adj_se<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, k.cst, k.cdt);
+        return;
+    }
+    // E and pi of the recovered state (written to cur.e1, e2, pi) and the S_e
+    // adjoint (reads cur's links and phi, writes only the adjoint buffers)
+    // touch disjoint data: they run side by side, joined before the next step
+    cudaEventRecord(fork, st);
+    cudaStreamWaitEvent(st2, fork, 0);
+    launch_inverse_se<T>(N, nxt, cur, cf, st2);
     if (cf.do_pe) k_adj_se<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, k.cst, k.cdt);
+    cudaEventRecord(join, st2);
+    cudaStreamWaitEvent(st, join, 0);
 }
 
 template <typename T>
@@ -1021,10 +1048,8 @@ void launch_adjoint_project(size_t n, const AdjStateT<T> &a, cudaStream_t st) {
 
 template void launch_inverse_adjoint_step<double>(int, const State<double> &,
                                                   const State<double> &, const AdjState &,
-                                                  const StepCoef<double> &, cudaStream_t);
-template void launch_inverse_adjoint_step<float>(int, const State<float> &, const State<float> &,
-                                                 const AdjStateT<float> &,
-                                                 const StepCoef<double> &, cudaStream_t);
+                                                  const StepCoef<double> &, cudaStream_t,
+                                                  cudaStream_t, cudaEvent_t, cudaEvent_t);
 template void launch_adjoint_step<double>(int, const State<double> &, const State<double> &,
                                           const AdjState &, const StepCoef<double> &,
                                           cudaStream_t);

@@ -40,6 +40,8 @@ struct ipg_ctx {
     // the other of two work buffers (work, work2)
     cudaStream_t stream_v = nullptr;
     cudaEvent_t ev_fft[2] = {nullptr, nullptr}, ev_prod[2] = {nullptr, nullptr};
+    // the reverse sweep's time reversal forks onto stream_v and joins back
+    cudaEvent_t ev_adj_fork = nullptr, ev_adj_join = nullptr;
     // ipg_get_observables_async: the copies run on stream_copy after
     // ev_obs_ready; the next observables stage waits for ev_obs_copied
     cudaStream_t stream_copy = nullptr;
@@ -121,7 +123,8 @@ struct ipg_ctx {
         // FP32 adjoint (contexts of the FP32 form): the plain form's states and
         // adjoints in FP32; the tau = 0 adjoint is widened into adj at the end
         bool fp32 = false;
-        std::vector<State<float>> cp32;
+        std::vector<State<float>> cp32;   // checkpoints (every state when k = 1)
+        std::vector<State<float>> seg32;  // a segment's states, recomputed
         State<float> w32[3]{};
         State<float> fin32{};
         AdjStateT<float> adj32{};
@@ -358,6 +361,52 @@ ipg_status copy_state(ipg_ctx *c, const State<double> &dst, const State<double> 
     return IPG_OK;
 }
 
+ipg_status copy_state32(ipg_ctx *c, const State<float> &dst, const State<float> &src) {
+    const size_t n = c->n;
+    auto cp = [&](void *d, const void *s_, size_t bytes) {
+        return cudaMemcpyAsync(d, s_, bytes, cudaMemcpyDeviceToDevice, c->stream);
+    };
+    IPG_CUDA(c, cp(dst.ux, src.ux, 9 * n * sizeof(C<float>)));
+    IPG_CUDA(c, cp(dst.uy, src.uy, 9 * n * sizeof(C<float>)));
+    IPG_CUDA(c, cp(dst.e1, src.e1, 8 * n * sizeof(float)));
+    IPG_CUDA(c, cp(dst.e2, src.e2, 8 * n * sizeof(float)));
+    IPG_CUDA(c, cp(dst.phi, src.phi, 9 * n * sizeof(float)));
+    IPG_CUDA(c, cp(dst.pi, src.pi, 9 * n * sizeof(float)));
+    return IPG_OK;
+}
+
+// One step of the FP32 bulk form from `in` into `out`: E and pi are copied
+// to `out` first (unless they are the same buffers) and updated there, the
+// new U and phi are written to `out`, whose U/phi buffers differ from `in`'s.
+ipg_status step32_into(ipg_ctx *c, const State<float> &in, const State<float> &out,
+                       const StepCoef<double> &cfd) {
+    const size_t n = c->n;
+    if (out.e1 != in.e1) {
+        IPG_CUDA(c, cudaMemcpyAsync(out.e1, in.e1, 8 * n * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, c->stream));
+        IPG_CUDA(c, cudaMemcpyAsync(out.e2, in.e2, 8 * n * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, c->stream));
+        IPG_CUDA(c, cudaMemcpyAsync(out.pi, in.pi, 9 * n * sizeof(float),
+                                    cudaMemcpyDeviceToDevice, c->stream));
+    }
+    State<float> s = in;
+    s.e1 = out.e1;
+    s.e2 = out.e2;
+    s.pi = out.pi;
+    StepCoef<float> cf;
+    cf.tau = (float)cfd.tau;
+    cf.dt_pe = (float)cfd.dt_pe;
+    cf.dt_pu = (float)cfd.dt_pu;
+    cf.g = (float)cfd.g;
+    cf.do_pe = cfd.do_pe;
+    cf.do_pu = cfd.do_pu;
+    set_derived(cf);
+    launch_leapfrog<float>(c->d_ev, c->N, s, out.ux, out.uy, out.phi, cf, true, c->stream,
+                           c->scal + 38);
+    IPG_LAUNCHED(c, 1);
+    return IPG_OK;
+}
+
 // coefficients of launch s of run_evolution (0: tau = 0 half step)
 StepCoef<double> evolution_coef(const ipg_ctx *c, int s) {
     StepCoef<double> cf;
@@ -581,6 +630,8 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
         IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_fft[i], cudaEventDisableTiming));
         IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_prod[i], cudaEventDisableTiming));
     }
+    IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_adj_fork, cudaEventDisableTiming));
+    IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_adj_join, cudaEventDisableTiming));
     IPG_CUDA(c, cudaEventCreate(&c->ev0));
     IPG_CUDA(c, cudaEventCreate(&c->ev1));
     for (cudaEvent_t &x : c->ie) IPG_CUDA(c, cudaEventCreate(&x));
@@ -682,6 +733,8 @@ ipg_status ipg_destroy(ipg_ctx *ctx) {
         if (ctx->ev_fft[i]) cudaEventDestroy(ctx->ev_fft[i]);
         if (ctx->ev_prod[i]) cudaEventDestroy(ctx->ev_prod[i]);
     }
+    if (ctx->ev_adj_fork) cudaEventDestroy(ctx->ev_adj_fork);
+    if (ctx->ev_adj_join) cudaEventDestroy(ctx->ev_adj_join);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return IPG_OK;
@@ -1592,61 +1645,46 @@ ipg_status ipg_forward(ipg_ctx *c, int checkpoint_every, double *E_T, double *ep
             IPG_TRY(alloc32(st));
             A.cp32.push_back(st);
         }
+        while (!store_all && (int)A.seg32.size() < checkpoint_every + 1) {
+            State<float> st{};
+            IPG_TRY(alloc32(st));
+            A.seg32.push_back(st);
+        }
     }
 
     // forward from the tau = 0 state (the context's own state is kept)
     IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
     State<double> cur;
     if (A.fp32) {
-        auto copy32 = [&](const State<float> &d, const State<float> &s_) -> ipg_status {
-            IPG_CUDA(c, cudaMemcpyAsync(d.ux, s_.ux, 9 * n * sizeof(C<float>),
-                                        cudaMemcpyDeviceToDevice, c->stream));
-            IPG_CUDA(c, cudaMemcpyAsync(d.uy, s_.uy, 9 * n * sizeof(C<float>),
-                                        cudaMemcpyDeviceToDevice, c->stream));
-            IPG_CUDA(c, cudaMemcpyAsync(d.e1, s_.e1, 8 * n * sizeof(float),
-                                        cudaMemcpyDeviceToDevice, c->stream));
-            IPG_CUDA(c, cudaMemcpyAsync(d.e2, s_.e2, 8 * n * sizeof(float),
-                                        cudaMemcpyDeviceToDevice, c->stream));
-            IPG_CUDA(c, cudaMemcpyAsync(d.phi, s_.phi, 9 * n * sizeof(float),
-                                        cudaMemcpyDeviceToDevice, c->stream));
-            IPG_CUDA(c, cudaMemcpyAsync(d.pi, s_.pi, 9 * n * sizeof(float),
-                                        cudaMemcpyDeviceToDevice, c->stream));
-            return IPG_OK;
-        };
-        // the FP64 tau = 0 state, kept for the initial-condition adjoint
-        IPG_TRY(copy_state(c, A.w[0], c->s64));
+        // the FP32 bulk form's own steps (deviation storage W = U - 1,
+        // reunitarised), from the context's FP32 tau = 0 state
+        IPG_TRY(copy_state(c, A.w[0], c->s64));  // FP64 tau = 0 links for the init adjoint
         State<float> c32;
         if (store_all) {
-            launch_convert_plain<double, float>(n, c->s64, A.cp32[0], c->stream);
-            IPG_LAUNCHED(c, 1);
-            for (int s = 0; s < S; s++) {
-                launch_leapfrog_plain32(c->d_ev, N, A.cp32[s], A.cp32[s + 1],
-                                        evolution_coef(c, s), c->stream);
-                IPG_LAUNCHED(c, 1);
-            }
+            IPG_TRY(copy_state32(c, A.cp32[0], c->s32));
+            for (int s = 0; s < S; s++)
+                IPG_TRY(step32_into(c, A.cp32[s], A.cp32[s + 1], evolution_coef(c, s)));
             c32 = A.cp32[S];
         } else {
-            launch_convert_plain<double, float>(n, c->s64, A.w32[0], c->stream);
-            IPG_LAUNCHED(c, 1);
+            IPG_TRY(copy_state32(c, A.w32[0], c->s32));
             c32 = A.w32[0];
             State<float> other = A.w32[1];
             for (int s = 0; s < S; s++) {
                 if (s % checkpoint_every == 0)
-                    IPG_TRY(copy32(A.cp32[s / checkpoint_every], c32));
+                    IPG_TRY(copy_state32(c, A.cp32[s / checkpoint_every], c32));
                 State<float> out = c32;  // E and pi in place
                 out.ux = other.ux;
                 out.uy = other.uy;
                 out.phi = other.phi;
-                launch_leapfrog_plain32(c->d_ev, N, c32, out, evolution_coef(c, s), c->stream);
-                IPG_LAUNCHED(c, 1);
+                IPG_TRY(step32_into(c, c32, out, evolution_coef(c, s)));
                 std::swap(c32.ux, other.ux);
                 std::swap(c32.uy, other.uy);
                 std::swap(c32.phi, other.phi);
             }
         }
         A.fin32 = c32;
-        // T^tautau of the final state in FP64 (the loss), from a widened copy
-        launch_convert_plain<float, double>(n, c32, A.w[2], c->stream);
+        // T^tautau of the final state in FP64 (the loss), from U = 1 + W
+        launch_convert_state<float>(n, c32, A.w[2], c->stream);
         IPG_LAUNCHED(c, 1);
         cur = A.w[2];
     } else if (store_all) {
@@ -1766,33 +1804,21 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
                 IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
             }
         } else {
-            A.ready = false;  // the sweep overwrites the final state
-            State<float> sets[2] = {A.w32[2], A.fin32};
-            State<float> nxt = A.fin32;
-            for (int s = S - 1, q = 0; s >= 0; s--, q++) {
-                const State<float> cur = sets[q & 1];
-                const StepCoef<double> cf = evolution_coef(c, s);
-                if (s % A.k == 0) {
-                    const State<float> &src = A.cp32[s / A.k];
-                    IPG_CUDA(c, cudaMemcpyAsync(cur.ux, src.ux, 9 * n * sizeof(C<float>),
-                                                cudaMemcpyDeviceToDevice, c->stream));
-                    IPG_CUDA(c, cudaMemcpyAsync(cur.uy, src.uy, 9 * n * sizeof(C<float>),
-                                                cudaMemcpyDeviceToDevice, c->stream));
-                    IPG_CUDA(c, cudaMemcpyAsync(cur.e1, src.e1, 8 * n * sizeof(float),
-                                                cudaMemcpyDeviceToDevice, c->stream));
-                    IPG_CUDA(c, cudaMemcpyAsync(cur.e2, src.e2, 8 * n * sizeof(float),
-                                                cudaMemcpyDeviceToDevice, c->stream));
-                    IPG_CUDA(c, cudaMemcpyAsync(cur.phi, src.phi, 9 * n * sizeof(float),
-                                                cudaMemcpyDeviceToDevice, c->stream));
-                    IPG_CUDA(c, cudaMemcpyAsync(cur.pi, src.pi, 9 * n * sizeof(float),
-                                                cudaMemcpyDeviceToDevice, c->stream));
-                    launch_adjoint_step<float>(N, cur, nxt, A.adj32, cf, c->stream);
+            // segment by segment from the last: the segment's states are
+            // recomputed from its checkpoint with the same FP32 steps as the
+            // forward (the exact forward trajectory), then swept backwards
+            for (int j = (S - 1) / A.k; j >= 0; j--) {
+                const int s0 = j * A.k, s1 = std::min(S, s0 + A.k);
+                IPG_TRY(copy_state32(c, A.seg32[0], A.cp32[j]));
+                for (int t = s0; t < s1; t++)
+                    IPG_TRY(step32_into(c, A.seg32[t - s0], A.seg32[t - s0 + 1],
+                                        evolution_coef(c, t)));
+                for (int t = s1 - 1; t >= s0; t--) {
+                    const StepCoef<double> cf = evolution_coef(c, t);
+                    launch_adjoint_step<float>(N, A.seg32[t - s0], A.seg32[t - s0 + 1], A.adj32,
+                                               cf, c->stream);
                     IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
-                } else {
-                    launch_inverse_adjoint_step<float>(N, nxt, cur, A.adj32, cf, c->stream);
-                    IPG_LAUNCHED(c, cf.do_pe ? 3 : 2);
                 }
-                nxt = cur;
             }
         }
         launch_adjoint_project<float>(n, A.adj32, c->stream);
@@ -1829,7 +1855,8 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
                     launch_adjoint_step(N, cur, nxt, A.adj, cf, c->stream);
                     IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
                 } else {
-                    launch_inverse_adjoint_step(N, nxt, cur, A.adj, cf, c->stream);
+                    launch_inverse_adjoint_step(N, nxt, cur, A.adj, cf, c->stream, c->stream_v,
+                                                c->ev_adj_fork, c->ev_adj_join);
                     IPG_LAUNCHED(c, cf.do_pe ? 3 : 2);
                 }
                 nxt = cur;

@@ -302,8 +302,7 @@ void launch_inverse_se(int N, const State<T> &nxt, const State<T> &cur, const St
 }
 template void launch_inverse_se<double>(int, const State<double> &, const State<double> &,
                                         const StepCoef<double> &, cudaStream_t);
-template void launch_inverse_se<float>(int, const State<float> &, const State<float> &,
-                                       const StepCoef<double> &, cudaStream_t);
+
 
 template <typename T, bool REUNIT>
 __global__ void __launch_bounds__(128)
@@ -1777,37 +1776,6 @@ void launch_leapfrog_into(const EventGeom *d_ev, int N, const State<double> &in,
         cudaMemcpyAsync(out.pi, in.pi, 9 * n * sizeof(double), cudaMemcpyDeviceToDevice, st);
     }
     launch_leapfrog_site<double>(d_ev, N, s, out.ux, out.uy, out.phi, cf, false, st);
-}
-
-// One step of the plain form (full links, Taylor-2 update, no
-// reunitarisation) in FP32, from the state `in` into `out` (E and pi copied,
-// then updated in place in `out`; U and phi written to `out`): the forward
-// sweep of the FP32 adjoint. `in` and `out` may be the same state only when
-// out's U/phi are separate buffers (ux_out etc.).
-void launch_leapfrog_plain32(const EventGeom *d_ev, int N, const State<float> &in,
-                             const State<float> &out, const StepCoef<double> &cf,
-                             cudaStream_t st) {
-    const size_t n = (size_t)N * N;
-    if (out.e1 != in.e1) {
-        cudaMemcpyAsync(out.e1, in.e1, 8 * n * sizeof(float), cudaMemcpyDeviceToDevice, st);
-        cudaMemcpyAsync(out.e2, in.e2, 8 * n * sizeof(float), cudaMemcpyDeviceToDevice, st);
-        cudaMemcpyAsync(out.pi, in.pi, 9 * n * sizeof(float), cudaMemcpyDeviceToDevice, st);
-    }
-    State<float> s = in;
-    s.e1 = out.e1;
-    s.e2 = out.e2;
-    s.pi = out.pi;
-    StepCoef<float> c;
-    c.tau = (float)cf.tau;
-    c.dt_pe = (float)cf.dt_pe;
-    c.dt_pu = (float)cf.dt_pu;
-    c.g = (float)cf.g;
-    c.do_pe = cf.do_pe;
-    c.do_pu = cf.do_pu;
-    set_derived(c);
-    dim3 block(32, 4);
-    dim3 grid((N + 31) / 32, (N + 3) / 4);
-    k_leapfrog<float, false><<<grid, block, 0, st>>>(d_ev, s, out.ux, out.uy, out.phi, c);
 }
 
 // one thread per site (lattices smaller than 32 sites per side)

@@ -246,19 +246,24 @@ using AdjState = AdjStateT<double>;
 void launch_inverse_step(int N, const State<double> &nxt, const State<double> &cur,
                          const StepCoef<double> &cf, cudaStream_t st);
 // E and pi of the step's input from its output nxt and the recovered U, phi
-// in cur (evolve.cu); T = double or float (full links, plain form)
+// in cur (evolve.cu; FP64, full links)
 template <typename T>
 void launch_inverse_se(int N, const State<T> &nxt, const State<T> &cur,
                        const StepCoef<double> &cf, cudaStream_t st);
 // the time reversal nxt -> cur and the adjoint step together (fewer launches
-// than launch_inverse_step then launch_adjoint_step, same results)
+// than launch_inverse_step then launch_adjoint_step, same results; FP64);
+// with a second stream st2 (and two events) the E/pi reversal runs beside
+// the S_e adjoint, joined back into st
 template <typename T>
 void launch_inverse_adjoint_step(int N, const State<T> &nxt, const State<T> &cur,
                                  const AdjStateT<T> &a, const StepCoef<double> &cf,
-                                 cudaStream_t st);
+                                 cudaStream_t st, cudaStream_t st2 = nullptr,
+                                 cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr);
 // adjoints of a step's outputs -> adjoints of its inputs (in place); cur is the
 // state before the step, nxt the state after it. T = double, or float for the
-// FP32 adjoint (states and adjoints in FP32, the plain form's step)
+// FP32 adjoint (the FP32 bulk form's states, links as W = U - 1; adjoints in
+// FP32; the step differentiated is the plain form's, without the
+// reunitarisation)
 template <typename T>
 void launch_adjoint_step(int N, const State<T> &cur, const State<T> &nxt, const AdjStateT<T> &a,
                          const StepCoef<double> &cf, cudaStream_t st);
@@ -358,13 +363,6 @@ void launch_output_text(int kind, const OutputGrid &g, const OutputFields &f, lo
                         char *chunks, int *chunk_len, long long *chunk_off, char *text,
                         double *term, int *bad, cudaStream_t st);
 
-// plain (full-link) state in one precision -> the other, element by element
-template <typename S, typename D>
-void launch_convert_plain(size_t n, const State<S> &src, const State<D> &dst, cudaStream_t st);
-// one FP32 step of the plain form from `in` into `out` (the FP32 adjoint's forward)
-void launch_leapfrog_plain32(const EventGeom *d_ev, int N, const State<float> &in,
-                             const State<float> &out, const StepCoef<double> &cf,
-                             cudaStream_t st);
 template <typename T>
 void launch_convert_state(size_t n, const State<T> &src, State<double> &dst,
                           cudaStream_t st);

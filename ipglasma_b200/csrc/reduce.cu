@@ -302,34 +302,6 @@ void launch_convert_state_down(size_t n, const State<double> &src,
     k_convert<double, T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, src, dst);
 }
 
-// element by element, full links (the plain form in either precision)
-template <typename S, typename D>
-__global__ void k_convert_plain(size_t n, State<S> src, State<D> dst) {
-    const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (pos >= n) return;
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-        dst.ux[k * n + pos] = {(D)src.ux[k * n + pos].r, (D)src.ux[k * n + pos].i};
-        dst.uy[k * n + pos] = {(D)src.uy[k * n + pos].r, (D)src.uy[k * n + pos].i};
-        dst.phi[k * n + pos] = (D)src.phi[k * n + pos];
-        dst.pi[k * n + pos] = (D)src.pi[k * n + pos];
-    }
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-        dst.e1[k * n + pos] = (D)src.e1[k * n + pos];
-        dst.e2[k * n + pos] = (D)src.e2[k * n + pos];
-    }
-}
-
-template <typename S, typename D>
-void launch_convert_plain(size_t n, const State<S> &src, const State<D> &dst, cudaStream_t st) {
-    k_convert_plain<S, D><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, src, dst);
-}
-template void launch_convert_plain<double, float>(size_t, const State<double> &,
-                                                  const State<float> &, cudaStream_t);
-template void launch_convert_plain<float, double>(size_t, const State<float> &,
-                                                  const State<double> &, cudaStream_t);
-
 template void launch_convert_state<float>(size_t, const State<float> &,
                                           State<double> &, cudaStream_t);
 template void launch_convert_state_down<float>(size_t, const State<double> &,

