@@ -314,10 +314,11 @@ ipg_status ipg_output_names(int event_id, int it, double dtau, double a,
  * Reverse-mode derivatives of the evolution, with the autograd contract:
  * ipg_forward saves what ipg_backward consumes once. On an FP64 context the
  * plain form is differentiated in FP64. On an FP32 context (the FP32 adjoint)
- * the plain form's forward and reverse sweeps run in FP32 (full FP32 links,
- * no reunitarisation; the FP64 tau = 0 state rounded once), and the adjoint
- * of the tau = 0 state is widened to FP64 for the initial conditions. The
- * loss is
+ * the forward is the FP32 bulk form's own steps (deviation storage, per-step
+ * reunitarisation), the reverse sweep runs in FP32 on those states (with
+ * checkpoints, each segment is recomputed forward from its checkpoint instead
+ * of reversed in time), and the adjoint of the tau = 0 state is widened to
+ * FP64 for the initial conditions, whose adjoint stays FP64. The loss is
  *   L = w_ET * E_T + w_eps2 * eps2
  * at tau = itmax dtau a, from the state after the itmax leapfrog launches of
  * Evolution::run (where the reference evaluates T^{mu nu}):
@@ -329,9 +330,10 @@ ipg_status ipg_output_names(int event_id, int it, double dtau, double a,
  * ipg_forward starts from the context's fresh tau = 0 state (after
  * ipg_init_fields, or ipg_set_field + ipg_mark_initialized) without changing
  * it; it stores the state before every checkpoint_every-th step. ipg_backward
- * walks back by exact time reversal of the step between checkpoints. With
+ * walks back between checkpoints by exact time reversal of the step (FP64)
+ * or by recomputing the segment from its checkpoint (FP32). With
  * checkpoint_every = 1 every state is kept (itmax + 1 states of 560 bytes a
- * site: 14.7 GB for 256^2 sites and 400 steps), each step writes its own
+ * site in FP64: 14.7 GB for 256^2 sites and 400 steps), each step writes its own
  * slot, the reverse sweep needs no time reversal, and ipg_backward may be
  * called again (other weights) without a new ipg_forward; checkpoint_every
  * = 0 takes 1 when those states fit in half of the free device memory, else

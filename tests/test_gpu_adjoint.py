@@ -191,8 +191,9 @@ def test_fp32_adjoint_matches_fp64_adjoint(k):
     """The FP32 adjoint (an FP32 context: the FP32 bulk form's forward, the
     reverse sweep in FP32 on its states, every state kept or checkpoints with
     the segments recomputed; the initial conditions' adjoint in FP64) against
-    the FP64 adjoint of the same event: the gradients with respect to the
-    tau = 0 fields, g^2 mu^2 and rho, and E_T and eps2."""
+    the FP64 adjoint of the same event: E_T and eps2 within 3e-5 (measured
+    9e-6 and 3e-6), the gradients with respect to the tau = 0 fields, g^2 mu^2
+    and rho within 2e-4 in norm (measured 2e-6 to 6e-5)."""
     out = {}
     for prec in (ipg.FP64, ipg.FP32):
         with _event(prec) as ev:
@@ -205,9 +206,9 @@ def test_fp32_adjoint_matches_fp64_adjoint(k):
         a, b = g32[key], g64[key]
         rels[str(key)] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
     print("FP32ADJ", k, rels)
-    assert rels["E_T"] < 1e-4 and rels["eps2"] < 1e-4
+    assert rels["E_T"] < 3e-5 and rels["eps2"] < 3e-5
     for key, v in rels.items():
-        assert v < 1e-2, (key, v)
+        assert v < 2e-4, (key, v)
 
 
 def test_gradient_at_AuAu256_400_steps_32_directions():
@@ -216,8 +217,11 @@ def test_gradient_at_AuAu256_400_steps_32_directions():
     checkpoint every 20 steps with time reversal in between. The gradient of
     E_T + eps2 with respect to g^2 mu^2 (16 directions of relative
     perturbations) and rho (16 directions in the noise) against central
-    finite differences with h = 1e-6 (relative), Newton converged to 1e-12:
-    agreement within 1e-4 relative on every direction."""
+    finite differences with h = 1e-6 (relative): agreement within 1e-4
+    relative on every direction. Newton is polished to 1e-14 (sum of |F_a|):
+    at 1e-12 the loss moves by ~1e-9 between the two evaluations of a
+    difference, which is ~5e-4 of a directional derivative after the
+    division by 2h."""
     from ipglasma_b200.synthetic import make_event
 
     N, L, Ny = 256, 30.0, 50
@@ -226,7 +230,7 @@ def test_gradient_at_AuAu256_400_steps_32_directions():
     rng = np.random.default_rng(8100)
     xi = rng.standard_normal((2, Ny, N * N, 8))
     ev = ipg.Event(ipg.Config(size=N, L=L, Ny=Ny, maxtime=400 * 0.1 * a, dtau=0.1,
-                              precision=ipg.FP64, seed=8100, newton_tolerance=1e-12))
+                              precision=ipg.FP64, seed=8100, newton_tolerance=1e-14))
     assert ev.itmax == 400
 
     def loss(gA, gB, x):
@@ -241,7 +245,7 @@ def test_gradient_at_AuAu256_400_steps_32_directions():
     g = ev.backward(1.0, 1.0, inputs=True, rho=True)
     amp = np.stack([2.0 * np.sqrt(A / Ny), 2.0 * np.sqrt(B / Ny)])
     h = 1e-6
-    worst = 0.0
+    rels = []
     for k in range(32):
         if k < 16:
             dA = A * rng.uniform(-1, 1, A.shape)
@@ -252,8 +256,9 @@ def test_gradient_at_AuAu256_400_steps_32_directions():
             dxi = rng.standard_normal(xi.shape)
             directional = float(np.sum(g["rho"] * amp[:, None, :, None] * dxi))
             fd = (loss(A, B, xi + h * dxi) - loss(A, B, xi - h * dxi)) / (2 * h)
-        rel = abs(directional - fd) / abs(fd)
-        worst = max(worst, rel)
-        assert rel < 1e-4, (k, directional, fd)
-    print(f"FD32 worst relative gap over 32 directions: {worst:.2e}")
+        rels.append((abs(directional - fd) / abs(fd), k, directional, fd))
     ev.close()
+    print("FD32 relative gaps over 32 directions: "
+          + " ".join(f"{r[0]:.1e}" for r in rels))
+    worst = max(rels)
+    assert worst[0] < 1e-4, worst
