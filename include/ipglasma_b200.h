@@ -42,7 +42,10 @@ typedef enum {
     IPG_ERR_NAN = 4,               /* NaN/Inf detected in the fields */
     IPG_ERR_STATE = 5,             /* call out of order */
     IPG_ERR_NOMEM = 6,             /* device allocation failed */
-    IPG_ERR_TIMEOUT = 7            /* a device wait hit its limit */
+    IPG_ERR_TIMEOUT = 7,           /* a device wait hit its limit */
+    IPG_NO_COLLISION = 8           /* the gluon spectrum at it = 1 is zero: the
+                                      evolution stopped there, as the reference's
+                                      does (Evolution.cpp:655, 3111-3122) */
 } ipg_status;
 
 typedef enum {
@@ -309,6 +312,89 @@ ipg_status ipg_write_outputs(ipg_ctx *ctx, const char *hydro_path, const char *t
 ipg_status ipg_output_names(int event_id, int it, double dtau, double a,
                             char *hydro, size_t hydro_len, char *tmunu,
                             size_t tmunu_len);
+
+/* ---- gauge fixing and gluon multiplicity ---------------------------------
+ * GaugeFix::FFTChi (GaugeFix.cpp:17-165) and Evolution::multiplicity
+ * (Evolution.cpp:2284-3188), which the reference runs at it = 1 and
+ * it = itmax when computeGluonMultiplicity is set (Evolution.cpp:644-653).
+ *
+ * ipg_gauge_fix brings the fields to transverse Coulomb gauge by
+ * Fourier-accelerated steepest descent, in place, as the reference does: per
+ * iteration the residual <tr(g^dag g)> / Nc of g = sum_a Im tr(div A t^a) t^a,
+ * the reference's two stopping rules (residual < 1e-9; residual above the one
+ * recorded at the last multiple of 10 iterations and below 1e-6), then the
+ * gauge transformation reu(expm(i chi)) with chi = IFFT(-1.5 / (k~^2 + 1e-9)
+ * FFT(g)). On an FP64 context the live fields are transformed (later steps
+ * continue from them, as in the reference); on an FP32 context an FP64 copy
+ * of the current fields is, and the FP32 state is left alone (the evolution
+ * is gauge covariant). */
+typedef struct {
+    int iterations;         /* gauge transformations applied */
+    int residual_checks;    /* residuals computed (iterations + 1 when a rule
+                               stopped it) */
+    int nan_sites;          /* site transformations that were NaN and were
+                               reset to 1 (GaugeFix.cpp:143-147) */
+    double residual;        /* the last residual computed */
+    double residual_every10[401]; /* at iterations 0, 10, 20, ... (the values
+                               the reference prints); NaN past the last */
+    double ms;              /* device time */
+} ipg_gauge_report;
+
+ipg_status ipg_gauge_fix(ipg_ctx *ctx, int max_iterations, ipg_gauge_report *report);
+
+/* Parameters of Evolution::multiplicity read from the input file. */
+typedef struct {
+    int max_gauge_iterations; /* <= 0 -> 4000 (Evolution.cpp:2333) */
+    int use_pseudorapidity;   /* usePseudoRapidity */
+    double rapidity;          /* Rapidity */
+    double jacobian_m;        /* Jacobianm, GeV */
+    double roots;             /* roots, GeV (the mean p_T estimate of the
+                                 pseudorapidity Jacobian) */
+} ipg_multiplicity_params;
+
+#define IPG_KT_BINS 100
+/* The gluon spectrum of the current fields. dN/dy ("dN/dy 1") sums n(k) over
+ * the lattice momenta; the binned values ("dN/dy 2") integrate the 100 k_T
+ * bins of width 2.83/100 (lattice units); the cuts keep bins with
+ * ik dkt / a hbarc above 3 and 6 GeV. With use_pseudorapidity the Jacobian
+ * factors of Evolution.cpp:2896-2953 and 3098-3108 are applied. */
+typedef struct {
+    int it;                   /* the step of the fields */
+    ipg_gauge_report gauge;
+    double dNdy, dEdy;        /* GeV for E */
+    double dNdy_binned, dEdy_binned;
+    double dNdy_cut3, dEdy_cut3, dNdy_cut6, dEdy_cut6;
+    double mean_pt;           /* dEdy / dNdy, GeV */
+    double n_kt[IPG_KT_BINS]; /* bin averages (dN/d^2k_T in lattice units) */
+    double E_kt[IPG_KT_BINS];
+    int count_kt[IPG_KT_BINS];
+    double ms_spectrum;       /* device time of the spectrum */
+} ipg_multiplicity_result;
+
+/* Gauge fixing followed by the spectrum of the context's current fields:
+ * after ipg_evolve (it = completed steps, >= 1) or after ipg_run
+ * (it = itmax, the fields after the final half step). dNdy == 0 is the
+ * reference's "no collision happened" case (Evolution.cpp:3111-3122). */
+ipg_status ipg_multiplicity(ipg_ctx *ctx, const ipg_multiplicity_params *params,
+                            ipg_multiplicity_result *out);
+/* ipg_run with the reference's computeGluonMultiplicity schedule: the
+ * spectrum at it = 1 (at_first, after the first step; skipped when
+ * itmax = 1) and at it = itmax (at_last, after the observables and the
+ * final half step). The gauge fixing at it = 1 transforms the fields the
+ * remaining steps start from. When dN/dy at it = 1 is zero the call returns
+ * IPG_NO_COLLISION after filling at_first, with the context left at it = 1.
+ * Any of the output pointers may be NULL. */
+ipg_status ipg_run_multiplicity(ipg_ctx *ctx, const ipg_multiplicity_params *params,
+                                ipg_result *result, ipg_multiplicity_result *at_first,
+                                ipg_multiplicity_result *at_last);
+/* The host part of Evolution::multiplicity, without a context: the k sums
+ * dN, dE, the per-bin sums of n and E and the bin counts -> the fields of
+ * out after `it` (it, dNdy .. count_kt; the gauge report and timings are
+ * left alone). a is the lattice spacing in fm. */
+ipg_status ipg_multiplicity_finish(double dN, double dE, const double *n_sum,
+                                   const double *E_sum, const int *count, double a,
+                                   const ipg_multiplicity_params *params,
+                                   ipg_multiplicity_result *out);
 
 /* ---- adjoint (no counterpart in the reference) ---------------------------
  * Reverse-mode derivatives of the evolution, with the autograd contract:

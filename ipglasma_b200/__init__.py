@@ -28,7 +28,8 @@ from pathlib import Path
 import numpy as np
 
 __all__ = ["Config", "Event", "Batch", "IPGError", "lib", "FP64", "FP32", "read_qs_table",
-           "UX", "UY", "E1", "E2", "PHI", "PI", "VA", "VB", "HBARC"]
+           "UX", "UY", "E1", "E2", "PHI", "PI", "VA", "VB", "HBARC", "multiplicity_finish",
+           "KT_BINS"]
 
 HBARC = 0.1973269718  # GeV fm, Phys_consts.h
 FP64, FP32 = 0, 1
@@ -37,7 +38,7 @@ UX, UY, E1, E2, PHI, PI, VA, VB = range(8)
 _STATUS = {
     0: "IPG_OK", 1: "IPG_ERR_BAD_CONFIG", 2: "IPG_ERR_CUDA",
     3: "IPG_ERR_NEWTON_NONCONVERGED", 4: "IPG_ERR_NAN", 5: "IPG_ERR_STATE",
-    6: "IPG_ERR_NOMEM", 7: "IPG_ERR_TIMEOUT",
+    6: "IPG_ERR_NOMEM", 7: "IPG_ERR_TIMEOUT", 8: "IPG_NO_COLLISION",
 }
 
 LIB_PATH = Path(__file__).resolve().parent / "libipglasma_b200.so"
@@ -106,6 +107,75 @@ class _Result(ct.Structure):
     ]
 
 
+class _GaugeReport(ct.Structure):
+    _fields_ = [
+        ("iterations", ct.c_int), ("residual_checks", ct.c_int), ("nan_sites", ct.c_int),
+        ("residual", ct.c_double), ("residual_every10", ct.c_double * 401),
+        ("ms", ct.c_double),
+    ]
+
+
+class _MultParams(ct.Structure):
+    _fields_ = [
+        ("max_gauge_iterations", ct.c_int), ("use_pseudorapidity", ct.c_int),
+        ("rapidity", ct.c_double), ("jacobian_m", ct.c_double), ("roots", ct.c_double),
+    ]
+
+
+KT_BINS = 100
+
+
+class _MultResult(ct.Structure):
+    _fields_ = [
+        ("it", ct.c_int), ("gauge", _GaugeReport),
+        ("dNdy", ct.c_double), ("dEdy", ct.c_double),
+        ("dNdy_binned", ct.c_double), ("dEdy_binned", ct.c_double),
+        ("dNdy_cut3", ct.c_double), ("dEdy_cut3", ct.c_double),
+        ("dNdy_cut6", ct.c_double), ("dEdy_cut6", ct.c_double),
+        ("mean_pt", ct.c_double),
+        ("n_kt", ct.c_double * KT_BINS), ("E_kt", ct.c_double * KT_BINS),
+        ("count_kt", ct.c_int * KT_BINS), ("ms_spectrum", ct.c_double),
+    ]
+
+
+def _gauge_dict(g: _GaugeReport) -> dict:
+    hist = np.array(g.residual_every10[:])
+    return {"iterations": g.iterations, "residual_checks": g.residual_checks,
+            "nan_sites": g.nan_sites, "residual": g.residual,
+            "residual_every10": hist[~np.isnan(hist)], "ms": g.ms}
+
+
+def _mult_dict(m: _MultResult) -> dict:
+    out = {f: getattr(m, f) for f, _ in _MultResult._fields_
+           if f not in ("gauge", "n_kt", "E_kt", "count_kt")}
+    out["gauge"] = _gauge_dict(m.gauge)
+    out["n_kt"] = np.array(m.n_kt[:])
+    out["E_kt"] = np.array(m.E_kt[:])
+    out["count_kt"] = np.array(m.count_kt[:])
+    return out
+
+
+def _mult_params(max_gauge_iterations=4000, use_pseudorapidity=False, rapidity=0.0,
+                 jacobian_m=0.35, roots=200.0) -> _MultParams:
+    return _MultParams(int(max_gauge_iterations), int(bool(use_pseudorapidity)),
+                       float(rapidity), float(jacobian_m), float(roots))
+
+
+def multiplicity_finish(dN, dE, n_sum, E_sum, count, a, **params) -> dict:
+    """The host part of Evolution::multiplicity (ipg_multiplicity_finish):
+    k sums and per-bin sums -> dN/dy, dE/dy, the binned integrals and cuts."""
+    m = _MultResult()
+    n_sum = _f64(n_sum, KT_BINS)
+    E_sum = _f64(E_sum, KT_BINS)
+    cnt = np.ascontiguousarray(count, dtype=np.int32)
+    prm = _mult_params(**params)
+    rc = lib().ipg_multiplicity_finish(float(dN), float(dE), _ptr(n_sum), _ptr(E_sum), _ptr(cnt),
+                                       float(a), ct.byref(prm), ct.byref(m))
+    if rc != 0:
+        raise IPGError(rc, "ipg_multiplicity_finish rejected its arguments")
+    return _mult_dict(m)
+
+
 _lib = None
 
 _SIGNATURES = {
@@ -134,6 +204,15 @@ _SIGNATURES = {
     "ipg_init_from_wilson_lines": (ct.c_int, [ct.c_void_p, ct.POINTER(_InitReport)]),
     "ipg_run": (ct.c_int, [ct.c_void_p, ct.POINTER(_Result)]),
     "ipg_evolve": (ct.c_int, [ct.c_void_p, ct.c_int]),
+    "ipg_gauge_fix": (ct.c_int, [ct.c_void_p, ct.c_int, ct.POINTER(_GaugeReport)]),
+    "ipg_multiplicity": (ct.c_int, [ct.c_void_p, ct.POINTER(_MultParams),
+                                    ct.POINTER(_MultResult)]),
+    "ipg_run_multiplicity": (ct.c_int, [ct.c_void_p, ct.POINTER(_MultParams),
+                                        ct.POINTER(_Result), ct.POINTER(_MultResult),
+                                        ct.POINTER(_MultResult)]),
+    "ipg_multiplicity_finish": (ct.c_int, [ct.c_double, ct.c_double, ct.c_void_p, ct.c_void_p,
+                                           ct.c_void_p, ct.c_double, ct.POINTER(_MultParams),
+                                           ct.POINTER(_MultResult)]),
     "ipg_get_observables": (ct.c_int, [ct.c_void_p] + [ct.c_void_p] * 4),
     "ipg_get_observables_async": (ct.c_int, [ct.c_void_p] + [ct.c_void_p] * 4),
     "ipg_wait_observables": (ct.c_int, [ct.c_void_p]),
@@ -417,6 +496,40 @@ class Event:
 
     def evolve(self, steps: int) -> None:
         self._check(self._lib.ipg_evolve(self._h, steps))
+
+    # -- gauge fixing and gluon multiplicity ----------------------------------
+    def gauge_fix(self, max_iterations: int = 4000) -> dict:
+        """Transverse Coulomb gauge (GaugeFix::FFTChi) of the current fields,
+        in place on an FP64 context."""
+        rep = _GaugeReport()
+        self._check(self._lib.ipg_gauge_fix(self._h, int(max_iterations), ct.byref(rep)))
+        return _gauge_dict(rep)
+
+    def multiplicity(self, **params) -> dict:
+        """Gauge fixing, then the gluon spectrum of the current fields
+        (Evolution::multiplicity); params: max_gauge_iterations,
+        use_pseudorapidity, rapidity, jacobian_m, roots."""
+        m = _MultResult()
+        prm = _mult_params(**params)
+        self._check(self._lib.ipg_multiplicity(self._h, ct.byref(prm), ct.byref(m)))
+        return _mult_dict(m)
+
+    def run_multiplicity(self, **params):
+        """run() with the spectrum at it = 1 and at it = itmax, as the
+        reference's computeGluonMultiplicity schedule; returns
+        (Result, spectrum at it = 1, spectrum at itmax); (None, spectrum at
+        it = 1, None) when no collision happened (dN/dy = 0 at it = 1: the
+        evolution stops there)."""
+        res, m1, m2 = _Result(), _MultResult(), _MultResult()
+        prm = _mult_params(**params)
+        st = self._check(self._lib.ipg_run_multiplicity(self._h, ct.byref(prm), ct.byref(res),
+                                                        ct.byref(m1), ct.byref(m2)), (8,))
+        if st == 8:
+            return None, _mult_dict(m1), None
+        vals = {f: getattr(res, f) for f, _ in _Result._fields_}
+        vals["eccentricity"] = list(res.eccentricity)
+        vals["psi"] = list(res.psi)
+        return Result(**vals), _mult_dict(m1), _mult_dict(m2)
 
     # -- outputs --------------------------------------------------------------
     def observables(self):

@@ -26,7 +26,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC"]
 CU_SOURCES = ["api.cu", "evolve.cu", "init.cu", "poisson.cu", "observables.cu", "reduce.cu",
-              "noalloc.cu", "adjoint.cu", "nuclei.cu", "writers_gpu.cu"]
+              "noalloc.cu", "adjoint.cu", "nuclei.cu", "writers_gpu.cu", "gaugefix.cu"]
 # the GPU writer rounds every sum and product on its own, as the host writer
 # (g++ -ffp-contract=off) does, so its text is byte-identical
 CU_EXTRA_FLAGS = {"writers_gpu.cu": ["-fmad=false"]}

@@ -131,6 +131,19 @@ struct ipg_ctx {
         float *tbar32 = nullptr;
     } aw;
 
+    // gauge fixing and multiplicity (allocated by the first call)
+    struct {
+        double2 *planes = nullptr;   // [16][n]: chi [4][n] and G [9][n] while gauge
+                                     // fixing, the spectrum's planes after
+        double *green = nullptr;     // [n] gauge-fixing multiplier
+        double *sin_half = nullptr;  // [N]
+        double *partial = nullptr;   // [kGaugeBlocks][kMultRow]
+        double *out = nullptr;       // [kMultRow]
+        GaugeFixCtl *ctl = nullptr;
+        GaugeFixCtl *h_ctl = nullptr;  // pinned
+        double *h_out = nullptr;       // pinned [kMultRow]
+    } gf;
+
     // output files formatted on the GPU (ipg_write_outputs); freed by ipg_destroy
     struct {
         long long cap_lines = 0;
@@ -572,6 +585,144 @@ ipg_status observables_finish(ipg_ctx *c, ipg_result *res) {
     return IPG_OK;
 }
 
+// ---- gauge fixing and multiplicity ----------------------------------------
+
+ipg_status gf_alloc(ipg_ctx *c) {
+    auto &g = c->gf;
+    if (g.planes) return IPG_OK;
+    const size_t n = c->n;
+    const int N = c->N;
+    IPG_TRY(dalloc(c, &g.planes, 16 * n));
+    IPG_TRY(dalloc(c, &g.green, n));
+    IPG_TRY(dalloc(c, &g.sin_half, (size_t)N));
+    IPG_TRY(dalloc(c, &g.partial, (size_t)kGaugeBlocks * kMultRow));
+    IPG_TRY(dalloc(c, &g.out, (size_t)kMultRow));
+    IPG_TRY(dalloc(c, &g.ctl, 1));
+    IPG_CUDA(c, cudaMallocHost(&g.h_ctl, sizeof(GaugeFixCtl)));
+    IPG_CUDA(c, cudaMallocHost(&g.h_out, sizeof(double) * kMultRow));
+    // sin(kx / 2) with kx = 2 pi (-0.5 + i / N), the expression of
+    // Evolution.cpp:2507-2513 (and GaugeFix.cpp:120-125), on the host
+    std::vector<double> sh(N);
+    for (int i = 0; i < N; i++) {
+        const double kx = 2. * M_PI * (-0.5 + static_cast<double>(i) / static_cast<double>(N));
+        sh[i] = std::sin(kx / 2.);
+    }
+    IPG_CUDA(c, cudaMemcpyAsync(g.sin_half, sh.data(), sizeof(double) * N,
+                                cudaMemcpyHostToDevice, c->stream));
+    launch_gauge_green(N, g.sin_half, g.green, c->stream);
+    IPG_LAUNCHED(c, 1);
+    return sync(c);
+}
+
+// the FP64 fields the gauge fixing and the spectrum work on: the live state
+// of an FP64 context, a widened copy of an FP32 one
+ipg_status fields64(ipg_ctx *c) { return state64(c); }
+
+ipg_status gauge_fix_run(ipg_ctx *c, int max_iter, ipg_gauge_report *rep) {
+    IPG_TRY(gf_alloc(c));
+    auto &g = c->gf;
+    const size_t n = c->n;
+    GaugeFixCtl *h = g.h_ctl;
+    std::memset(h, 0, sizeof(GaugeFixCtl));
+    h->prev = 10000.;  // GaugeFix.cpp:34
+    h->last = std::nan("");
+    for (int k = 0; k < kGaugeHistory; k++) h->hist[k] = std::nan("");
+    IPG_CUDA(c, cudaMemcpyAsync(g.ctl, h, sizeof(GaugeFixCtl), cudaMemcpyHostToDevice,
+                                c->stream));
+    GaugeFixArgs a;
+    a.s = c->s64;
+    a.N = c->N;
+    a.chi = g.planes;
+    a.G = reinterpret_cast<C<double> *>(g.planes + 4 * n);
+    a.partial = g.partial;
+    a.ctl = g.ctl;
+    WilsonArgs w{};
+    w.N = c->N;
+    w.logN = c->logN;
+    w.twiddle = c->twiddle;
+    w.green = g.green;
+    w.work = g.planes;
+    w.rho_in = g.planes;
+    w.no_product = 1;
+    w.skip = &g.ctl->done;
+    a.fft = w;
+    IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    // iterations are enqueued in chunks; after a stopping rule every kernel
+    // of the remaining iterations returns at once, and the host stops
+    // enqueueing at the next chunk boundary
+    constexpr int kChunk = 16;
+    int launched = 0;
+    while (launched < max_iter) {
+        const int k = std::min(kChunk, max_iter - launched);
+        for (int i = 0; i < k; i++) launch_gauge_fix_iteration(a, c->stream);
+        IPG_LAUNCHED(c, 7 * k);
+        launched += k;
+        IPG_CUDA(c, cudaMemcpyAsync(h, g.ctl, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        IPG_TRY(sync(c));
+        if (h->done) break;
+    }
+    IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    IPG_CUDA(c, cudaMemcpyAsync(h, g.ctl, sizeof(GaugeFixCtl), cudaMemcpyDeviceToHost,
+                                c->stream));
+    IPG_TRY(sync(c));
+    if (rep) {
+        rep->iterations = h->iter;
+        rep->residual_checks = h->checks;
+        rep->nan_sites = h->nan_sites;
+        rep->residual = h->last;
+        std::memcpy(rep->residual_every10, h->hist, sizeof(double) * kGaugeHistory);
+        rep->ms = elapsed(c);
+    }
+    return IPG_OK;
+}
+
+ipg_status multiplicity_run(ipg_ctx *c, const ipg_multiplicity_params *p,
+                            ipg_multiplicity_result *out) {
+    ipg_multiplicity_params prm{};
+    if (p) prm = *p;
+    if (prm.max_gauge_iterations <= 0) prm.max_gauge_iterations = 4000;
+    if (!c->initialized) return fail(c, IPG_ERR_STATE, "no fields: call ipg_init_fields first");
+    const int it = c->it;
+    if (it < 1)
+        return fail(c, IPG_ERR_STATE, "the spectrum needs the fields after a step (it >= 1)");
+    IPG_TRY(fields64(c));
+    ipg_multiplicity_result m;
+    std::memset(&m, 0, sizeof(m));
+    IPG_TRY(gauge_fix_run(c, prm.max_gauge_iterations, &m.gauge));
+    auto &g = c->gf;
+    MultArgs ma;
+    ma.N = c->N;
+    ma.it = it;
+    ma.dtau = c->dtau;
+    ma.g = c->cfg.g;
+    ma.a = c->a;
+    ma.sin_half = g.sin_half;
+    WilsonArgs w{};
+    w.N = c->N;
+    w.logN = c->logN;
+    w.twiddle = c->twiddle;
+    w.work = g.planes;
+    w.rho_in = g.planes;
+    w.no_product = 1;
+    IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    launch_multiplicity(c->s64, ma, g.planes, w, g.partial, g.out, c->stream);
+    IPG_LAUNCHED(c, 5);
+    IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    IPG_CUDA(c, cudaMemcpyAsync(g.h_out, g.out, sizeof(double) * kMultRow,
+                                cudaMemcpyDeviceToHost, c->stream));
+    IPG_TRY(sync(c));
+    const double *o = g.h_out;
+    int cnt[kKtBins];
+    for (int b = 0; b < kKtBins; b++) cnt[b] = (int)o[2 + 2 * kKtBins + b];
+    const ipg_status st =
+        ipg_multiplicity_finish(o[0], o[1], o + 2, o + 2 + kKtBins, cnt, c->a, &prm, &m);
+    if (st != IPG_OK) return fail(c, st, "bad multiplicity parameters");
+    m.it = it;
+    m.ms_spectrum = elapsed(c);
+    if (out) *out = m;
+    return IPG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -707,6 +858,8 @@ ipg_status ipg_destroy(ipg_ctx *ctx) {
     if (ctx->stream_copy) cudaStreamSynchronize(ctx->stream_copy);
     for (void *p : ctx->allocs) cudaFree(p);
     if (ctx->h_scal) cudaFreeHost(ctx->h_scal);
+    if (ctx->gf.h_ctl) cudaFreeHost(ctx->gf.h_ctl);
+    if (ctx->gf.h_out) cudaFreeHost(ctx->gf.h_out);
     {
         auto &o = ctx->out;
         for (void *p : {(void *)o.chunks, (void *)o.text, (void *)o.chunk_len, (void *)o.bad,
@@ -1217,6 +1370,123 @@ ipg_status ipg_run(ipg_ctx *c, ipg_result *res) {
     IPG_TRY(run_evolution(c));
     IPG_TRY(observables_enqueue(c));
     return observables_finish(c, res);
+}
+
+ipg_status ipg_gauge_fix(ipg_ctx *c, int max_iterations, ipg_gauge_report *rep) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (!c->initialized) return fail(c, IPG_ERR_STATE, "no fields: call ipg_init_fields first");
+    if (max_iterations < 0) return fail(c, IPG_ERR_BAD_CONFIG, "max_iterations < 0");
+    IPG_TRY(fields64(c));
+    return gauge_fix_run(c, max_iterations, rep);
+}
+
+ipg_status ipg_multiplicity(ipg_ctx *c, const ipg_multiplicity_params *p,
+                            ipg_multiplicity_result *out) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    return multiplicity_run(c, p, out);
+}
+
+ipg_status ipg_run_multiplicity(ipg_ctx *c, const ipg_multiplicity_params *p, ipg_result *res,
+                                ipg_multiplicity_result *first, ipg_multiplicity_result *last) {
+    if (!c) return IPG_ERR_BAD_CONFIG;
+    if (!c->initialized || c->half_done || c->finished)
+        return fail(c, IPG_ERR_STATE, "ipg_run_multiplicity needs fresh initial fields");
+    // Evolution::run: the first step, the spectrum at it = 1 (when it is not
+    // also the last step), the remaining steps, the observables at itmax with
+    // the final half step, then the spectrum at itmax
+    const int itmax = c->itmax;
+    double ms = 0;
+    if (itmax >= 2) {
+        IPG_TRY(ipg_evolve(c, 1));
+        ms += c->last_leapfrog_ms;
+        ipg_multiplicity_result m1;
+        IPG_TRY(multiplicity_run(c, p, &m1));
+        if (first) *first = m1;
+        if (m1.dNdy == 0.)
+            return fail(c, IPG_NO_COLLISION, "no collision happened: dN/dy at it = 1 is zero");
+        IPG_TRY(ipg_evolve(c, itmax - 2));
+        ms += c->last_leapfrog_ms;
+    } else {
+        IPG_TRY(run_evolution(c));
+        ms += c->last_leapfrog_ms;
+    }
+    c->last_leapfrog_ms = ms;
+    c->last_leapfrog_launches = itmax;
+    IPG_TRY(observables_enqueue(c));
+    IPG_TRY(observables_finish(c, res));
+    ipg_multiplicity_result m;
+    IPG_TRY(multiplicity_run(c, p, &m));
+    if (last) *last = m;
+    if (itmax < 2 && first) *first = m;
+    return IPG_OK;
+}
+
+ipg_status ipg_multiplicity_finish(double dN, double dE, const double *n_sum,
+                                   const double *E_sum, const int *count, double a,
+                                   const ipg_multiplicity_params *p, ipg_multiplicity_result *out) {
+    if (!n_sum || !E_sum || !count || !out || !(a > 0)) return IPG_ERR_BAD_CONFIG;
+    ipg_multiplicity_params prm{};
+    if (p) prm = *p;
+    // Evolution.cpp:2874-2960: bin averages, the binned integrals and the
+    // cuts, in the reference's bin order and operation order
+    const int bins = kKtBins;
+    const double dkt = 2.83 / static_cast<double>(bins);
+    const double m = prm.jacobian_m;
+    const double y = prm.rapidity;
+    double dN2 = 0., dE2 = 0., dNc = 0., dEc = 0., dNc2 = 0., dEc2 = 0.;
+    for (int ik = 0; ik < bins; ik++) {
+        double nk = n_sum[ik], Ek = E_sum[ik];
+        if (count[ik] > 0) {
+            nk = nk / static_cast<double>(count[ik]);
+            Ek = Ek / static_cast<double>(count[ik]);
+            if (prm.use_pseudorapidity == 0) {
+                dN2 += nk * (ik + 0.5) * dkt * dkt * 2. * M_PI;
+                dE2 += Ek * (ik + 0.5) * dkt * dkt * 2. * M_PI;
+                if (ik * dkt / a * kHbarc > 3.) {
+                    dNc += nk * (ik + 0.5) * dkt * dkt * 2. * M_PI;
+                    dEc += Ek * (ik + 0.5) * dkt * dkt * 2. * M_PI;
+                }
+                if (ik * dkt / a * kHbarc > 6.) {
+                    dNc2 += nk * (ik + 0.5) * dkt * dkt * 2. * M_PI;
+                    dEc2 += Ek * (ik + 0.5) * dkt * dkt * 2. * M_PI;
+                }
+            } else {
+                const double pt = (ik + 0.5) * dkt / a * kHbarc;
+                const double den = std::sqrt(std::pow(std::cosh(y), 2.) + m * m / (pt * pt));
+                dN2 += nk * (ik + 0.5) * dkt * dkt * 2. * M_PI * std::cosh(y) / den;
+                dE2 += Ek * (ik + 0.5) * dkt * dkt * 2. * M_PI * std::cosh(y) / den;
+                if (ik * dkt / a * kHbarc > 3.) {
+                    dNc += nk * (ik + 0.5) * dkt * dkt * 2. * M_PI * std::cosh(y) / den;
+                    dEc += Ek * (ik + 0.5) * dkt * dkt * 2. * M_PI * std::cosh(y) / den;
+                }
+                if (ik * dkt / a * kHbarc > 6.) {
+                    dNc2 += nk * (ik + 0.5) * dkt * dkt * 2. * M_PI * std::cosh(y) / den;
+                    dEc2 += Ek * (ik + 0.5) * dkt * dkt * 2. * M_PI * std::cosh(y) / den;
+                }
+            }
+        }
+        out->n_kt[ik] = count[ik] > 0 ? nk : 0.;
+        out->E_kt[ik] = count[ik] > 0 ? Ek : 0.;
+        out->count_kt[ik] = count[ik];
+    }
+    if (prm.use_pseudorapidity == 1) {
+        // Evolution.cpp:3098-3108: the k sums take the Jacobian at the mean
+        // p_T estimate P(sqrt(s))
+        const double P = 0.13 + 0.32 * std::pow(prm.roots / 1000., 0.115);
+        const double J = std::cosh(y) / (std::sqrt(std::pow(std::cosh(y), 2.) + m * m / (P * P)));
+        dN *= J;
+        dE *= J;
+    }
+    out->dNdy = dN;
+    out->dEdy = dE;
+    out->dNdy_binned = dN2;
+    out->dEdy_binned = dE2;
+    out->dNdy_cut3 = dNc;
+    out->dEdy_cut3 = dEc;
+    out->dNdy_cut6 = dNc2;
+    out->dEdy_cut6 = dEc2;
+    out->mean_pt = dE / dN;
+    return IPG_OK;
 }
 
 ipg_status ipg_get_observables(ipg_ctx *c, double *eps, double *u4,

@@ -130,6 +130,9 @@ struct WilsonArgs {
     // generating rho (the adjoint runs the self-adjoint Poisson map on it)
     const double2 *rho_in = nullptr;
     int no_product = 0;  // transform only, leave V alone
+    // when set and nonzero on the device, the transform kernels return at
+    // once (the gauge-fixing loop's stop flag)
+    const int *skip = nullptr;
 };
 // Poisson map only (no Wilson-line product) of w.rho_in -> w.work, sheets [0, ns)
 void launch_poisson_sheets(const WilsonArgs &w, int ns, cudaStream_t st);
@@ -147,6 +150,54 @@ void launch_draw_noise(int N, int k0, int ns, uint64_t key, uint32_t nucleus, do
 
 void launch_green(int N, double m_lat, double uvdamp_lat, double *green,
                   cudaStream_t st);
+// unnormalised forward 2-D DFT of the packed planes w.rho_in ([ns][4][n]
+// complex) into w.work (the same array may be passed for both)
+void launch_fft2_forward(const WilsonArgs &w, int ns, cudaStream_t st);
+
+// ---- Coulomb gauge fixing and gluon multiplicity (gaugefix.cu) ----------
+
+constexpr int kGaugeHistory = 401;  // residuals at iterations 0, 10, ..., 4000
+constexpr int kGaugeBlocks = 592;   // reduction blocks (4 per SM)
+constexpr int kKtBins = 100;        // k_T bins of Evolution::multiplicity
+constexpr int kMultRow = 2 + 3 * kKtBins;  // dN, dE, n[100], E[100], count[100]
+
+// device state of one gauge fixing (the host sets done = iter = nan_sites =
+// 0, prev = 10000 and hist = NaN before the first iteration)
+struct GaugeFixCtl {
+    int done;       // a stopping rule fired: later iterations do nothing
+    int iter;       // gauge transformations applied
+    int checks;     // residuals computed
+    int nan_sites;  // sites whose transformation was NaN and was reset to 1
+    double prev;    // residual at the last multiple of 10 iterations
+    double last;    // the latest residual
+    double hist[kGaugeHistory];
+};
+struct GaugeFixArgs {
+    State<double> s;     // fields, transformed in place
+    int N;
+    double2 *chi;        // [4][n] packed g, then chi
+    C<double> *G;        // [9][n] the transformation of every site
+    double *partial;     // [kGaugeBlocks]
+    GaugeFixCtl *ctl;
+    WilsonArgs fft;      // rho_in = work = chi, green = the gauge multiplier, skip = &ctl->done
+};
+int gauge_fix_blocks(int N);
+// the multiplier -1.5 / (k~^2 + 1e-9) on the DFT grid from sin_half[i] =
+// sin(pi (-0.5 + i / N)) (the reference's centred index i)
+void launch_gauge_green(int N, const double *sin_half, double *green, cudaStream_t st);
+void launch_gauge_fix_iteration(const GaugeFixArgs &a, cudaStream_t st);
+
+struct MultArgs {
+    int N;
+    int it;            // the step whose fields these are
+    double dtau, g, a;  // lattice dtau, coupling, spacing (fm)
+    const double *sin_half;  // [N] sin(kx / 2), kx = 2 pi (-0.5 + i / N)
+};
+// n(k_T) of the fields s: out[kMultRow] = dN, dE, the bin sums of n and E,
+// the bin counts (planes: [16][n] complex scratch; partial:
+// [kGaugeBlocks][kMultRow])
+void launch_multiplicity(const State<double> &s, const MultArgs &m, double2 *planes,
+                         const WilsonArgs &fft, double *partial, double *out, cudaStream_t st);
 
 // V_A, V_B -> link products U1, U2 for both directions (Init.cpp:2462-2491)
 void launch_link_products(int N, C<double> *VA, C<double> *VB,

@@ -140,6 +140,7 @@ constexpr int fwd_seq_stride(int N) {
 
 template <int LOGN>
 __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_fwd(WilsonArgs w, int k0) {
+    if (w.skip && *w.skip) return;
     constexpr int N = 1 << LOGN, TPS = N / 8, RPB = rows_per_block<LOGN>();
     constexpr int S = fwd_seq_stride(N);
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -212,8 +213,11 @@ __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_fwd(WilsonArgs w, 
     for (int m = 0; m < 8; m++) out[m * TPS] = make_double2(x[m].r, x[m].i);
 }
 
-template <int LOGN>
+// CONV: forward transform, Green multiply, inverse transform; otherwise the
+// forward transform only
+template <int LOGN, bool CONV = true>
 __global__ void __launch_bounds__(col_threads<LOGN>(), 2) k_cols(WilsonArgs w) {
+    if (w.skip && *w.skip) return;
     constexpr int N = 1 << LOGN, TPS = N / 8, JB = cols_per_block<LOGN>();
     constexpr int S = fft_seq_stride(N);
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -232,19 +236,22 @@ __global__ void __launch_bounds__(col_threads<LOGN>(), 2) k_cols(WilsonArgs w) {
         x[m] = {v.x, v.y};
     }
     fft_regs<LOGN, double, false>(x, sm + q * S, t, tw);
-    // the Green factors are loaded after the forward transform: that keeps
-    // the kernel within 64 registers, two 512-thread blocks per SM
+    if constexpr (CONV) {
+        // the Green factors are loaded after the forward transform: that
+        // keeps the kernel within 64 registers, two 512-thread blocks per SM
 #pragma unroll
-    for (int m = 0; m < 8; m++) gk[m] = w.green[(size_t)(t + m * TPS) * N + col];
+        for (int m = 0; m < 8; m++) gk[m] = w.green[(size_t)(t + m * TPS) * N + col];
 #pragma unroll
-    for (int m = 0; m < 8; m++) x[m] = {x[m].r * gk[m], x[m].i * gk[m]};
-    fft_regs<LOGN, double, true>(x, sm + q * S, t, tw);
+        for (int m = 0; m < 8; m++) x[m] = {x[m].r * gk[m], x[m].i * gk[m]};
+        fft_regs<LOGN, double, true>(x, sm + q * S, t, tw);
+    }
 #pragma unroll
     for (int m = 0; m < 8; m++) base[(size_t)(t + m * TPS) * N] = make_double2(x[m].r, x[m].i);
 }
 
 template <int LOGN>
 __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_inv(WilsonArgs w) {
+    if (w.skip && *w.skip) return;
     constexpr int N = 1 << LOGN, TPS = N / 8, RPB = rows_per_block<LOGN>();
     constexpr int S = fft_seq_stride(N);
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -309,6 +316,35 @@ static void launch_sheets(const WilsonArgs &w, int k0, int ns, cudaStream_t st) 
     k_rows_inv<LOGN><<<dim3(N / RPB, ns), row_threads<LOGN>(), row_smem, st>>>(w);
     const size_t n = (size_t)N * N;
     if (!w.rho_in && !w.no_product) k_wilson<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
+}
+
+template <int LOGN>
+static void launch_forward(const WilsonArgs &w, int ns, cudaStream_t st) {
+    constexpr int N = 1 << LOGN;
+    constexpr int RPB = rows_per_block<LOGN>(), JB = cols_per_block<LOGN>();
+    const size_t fwd_smem = sizeof(double2) * RPB * 4 * fwd_seq_stride(N);
+    const size_t col_smem = sizeof(double2) * JB * fft_seq_stride(N);
+    cudaFuncSetAttribute(k_rows_fwd<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)fwd_smem);
+    cudaFuncSetAttribute(k_cols<LOGN, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)col_smem);
+    k_rows_fwd<LOGN><<<dim3(N / RPB, ns), row_threads<LOGN>(), fwd_smem, st>>>(w, 0);
+    k_cols<LOGN, false><<<dim3(N / JB, 4, ns), col_threads<LOGN>(), col_smem, st>>>(w);
+}
+
+void launch_fft2_forward(const WilsonArgs &w, int ns, cudaStream_t st) {
+    switch (w.logN) {
+        case 3: launch_forward<3>(w, ns, st); break;
+        case 4: launch_forward<4>(w, ns, st); break;
+        case 5: launch_forward<5>(w, ns, st); break;
+        case 6: launch_forward<6>(w, ns, st); break;
+        case 7: launch_forward<7>(w, ns, st); break;
+        case 8: launch_forward<8>(w, ns, st); break;
+        case 9: launch_forward<9>(w, ns, st); break;
+        case 10: launch_forward<10>(w, ns, st); break;
+        case 11: launch_forward<11>(w, ns, st); break;
+        default: break;
+    }
 }
 
 // the Wilson-line product of a batch whose A is already in w.work

@@ -82,6 +82,11 @@ struct Args {
     double b = 0.0, BG = 4.0, QsmuRatio = 0.8, roots = 5020.0, rapidity = 0.0;
     double xfactor = 0.5, rmax = 3.0, sigmaNN = 70.0;
     int fluct = 1;
+    // --multiplicity 1: Evolution::run with computeGluonMultiplicity set
+    // (gauge fixing and the gluon spectrum at it = 1 and it = itmax); its
+    // printed values come out with 17 digits
+    int multiplicity = 0, pseudo = 0;
+    double jacobian_m = 0.35;
 };
 
 void usage() {
@@ -89,7 +94,8 @@ void usage() {
                  " [--Ny n] [--g g] [--m GeV] [--uvdamp x] [--seed s]"
                  " [--maxtime fm] [--dtau lattice] [--mode full|steps|init]"
                  " [--steps k] [--write-outputs w] [--size-output n]"
-                 " [--L-output fm] [--dumps 0|1]\n"
+                 " [--L-output fm] [--dumps 0|1] [--multiplicity 0|1 [--pseudo 0|1]"
+                 " [--rapidity y] [--jacobian-m GeV] [--roots GeV]]\n"
                  "       ipg_ref_harness --mode ipsat --nucleons FILE --table FILE --out DIR"
                  " [--N n] [--L fm] [--g g] [--b fm] [--BG GeV^-2] [--QsmuRatio r]"
                  " [--roots GeV] [--rapidity y] [--xfactor f] [--rmax fm]"
@@ -131,6 +137,9 @@ Args parse(int argc, char **argv) {
         else if (k == "--rmax") a.rmax = std::atof(v.c_str());
         else if (k == "--sigmaNN") a.sigmaNN = std::atof(v.c_str());
         else if (k == "--fluct") a.fluct = std::atoi(v.c_str());
+        else if (k == "--multiplicity") a.multiplicity = std::atoi(v.c_str());
+        else if (k == "--pseudo") a.pseudo = std::atoi(v.c_str());
+        else if (k == "--jacobian-m") a.jacobian_m = std::atof(v.c_str());
         else usage();
     }
     if (a.g2mu_file.empty() && a.mode != "ipsat") usage();
@@ -366,7 +375,17 @@ int main(int argc, char **argv) {
         int iTimeSteps = static_cast<int>(10 * A.maxtime / a) + 1;
         param.setdtau(A.maxtime / (iTimeSteps * a));
     }
-    param.setComputeGluonMultiplicity(0);
+    param.setComputeGluonMultiplicity(A.multiplicity);
+    if (A.multiplicity) {
+        param.setUsePseudoRapidity(A.pseudo);
+        param.setRapidity(A.rapidity);
+        param.setJacobianm(A.jacobian_m);
+        param.setRoots(A.roots);
+        param.setRunWithkt(0);
+        param.setRandomSeed(A.seed);
+        param.setb(A.b);
+        std::cout.precision(17);
+    }
     param.setWriteOutputs(A.write_outputs);
     param.setSizeOutput(A.size_output);
     param.setEtaSizeOutput(1);

@@ -44,7 +44,7 @@ def run_harness(out: Path, g2mu2A, g2mu2B, N: int, L: float, Ny: int,
                 mode: str = "full", steps: int = 0, write_outputs: int = 0,
                 size_output: int = 0, L_output: float = 0.0, dtau: float = -1.0,
                 threads: int = 1, binary: Path = HARNESS,
-                timeout: float = 3600, dumps: bool = True) -> RefRun:
+                timeout: float = 3600, dumps: bool = True, extra=()) -> RefRun:
     if not binary.exists():
         raise FileNotFoundError(f"{binary} missing: run `make -C oracle`")
     out = Path(out)
@@ -58,7 +58,7 @@ def run_harness(out: Path, g2mu2A, g2mu2B, N: int, L: float, Ny: int,
            "--steps", str(steps), "--write-outputs", str(write_outputs),
            "--size-output", str(size_output or N),
            "--L-output", repr(L_output or L), "--dtau", repr(dtau),
-           "--dumps", "1" if dumps else "0"]
+           "--dumps", "1" if dumps else "0", *extra]
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
     res = subprocess.run(cmd, capture_output=True, text=True, env=env,
                          timeout=timeout)

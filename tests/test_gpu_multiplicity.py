@@ -1,0 +1,198 @@
+"""Transverse Coulomb gauge fixing and the gluon multiplicity against the
+reference's own GaugeFix::FFTChi (GaugeFix.cpp:17-204) and
+Evolution::multiplicity (Evolution.cpp:2284-3188), which the harness runs
+inside Evolution::run with computeGluonMultiplicity set: at it = 1 and at
+it = itmax, printing (with 17 digits) the residual every 10 gauge-fixing
+iterations, dN/dy and dE/dy summed over k, the binned dN/dy and dE/dy, and
+<p_T> (with usePseudoRapidity the cut values too).
+
+Both sides start from the same tau = 0 state (the harness's noise); the gauge
+fixing then follows the same path, so the residual histories agree to
+rounding (bound 1e-8 relative) and stop at the same multiple of 10, and the
+spectra agree to 1e-9 relative. A global colour rotation is left free by the
+gauge condition; its rounding-level drift does not change any of these
+numbers, which are invariant under it.
+"""
+import re
+
+import numpy as np
+import pytest
+
+import ipglasma_b200 as ipg
+
+pytestmark = pytest.mark.gpu
+
+FLOAT = r"([-+0-9.eE]+|nan|inf)"
+
+
+def parse_reference(stdout: str):
+    """The blocks of values the reference prints per multiplicity call."""
+    blocks = []
+    for line in stdout.splitlines():
+        if line.startswith("Measuring multiplicity"):
+            blocks.append({"residuals": []})
+            continue
+        if not blocks:
+            continue
+        b = blocks[-1]
+        m = re.match(r"^(\d+) " + FLOAT + r"$", line)
+        if m:
+            b["residuals"].append((int(m.group(1)), float(m.group(2))))
+            continue
+        m = re.match(r"^dN/d(?:y|eta) (1|2) = " + FLOAT + r", dE/d(?:y|eta) \1 = " + FLOAT, line)
+        if m:
+            b["dN" + m.group(1)] = float(m.group(2))
+            b["dE" + m.group(1)] = float(m.group(3))
+            continue
+        m = re.match(r"^dN/deta_cut (1|2) = " + FLOAT, line)
+        if m:
+            b["cut" + m.group(1)] = float(m.group(2))
+            continue
+        m = re.match(r"^gluon <p_T> = " + FLOAT, line)
+        if m:
+            b["pt"] = float(m.group(1))
+    return blocks
+
+
+CASES = {
+    # N, L, nucleus, b, Ny, maxtime, pseudorapidity parameters
+    "AuAu64_y": (64, 16.0, "Au", 2.0, 4, 0.5, None),
+    "AuAu128_eta": (128, 24.0, "Au", 4.0, 4, 0.4, dict(rapidity=0.3, jacobian_m=0.35, roots=200.0)),
+}
+
+
+def close(a, b, tol):
+    return abs(a - b) <= tol * abs(b)
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_gauge_fixing_and_spectrum_match_reference(case, ref_harness, tmp_path):
+    from ipglasma_b200.synthetic import make_event
+
+    N, L, nuc, b, Ny, maxtime, pseudo = CASES[case]
+    A, B, _, _ = make_event(N, L, nuc, b, seed=31)
+    extra = ["--multiplicity", "1"]
+    params = {}
+    if pseudo:
+        extra += ["--pseudo", "1", "--rapidity", repr(pseudo["rapidity"]),
+                  "--jacobian-m", repr(pseudo["jacobian_m"]), "--roots", repr(pseudo["roots"])]
+        params = dict(use_pseudorapidity=True, **pseudo)
+    ref = ref_harness.run_harness(tmp_path / "ref", A, B, N, L, Ny, 2.0, 0.2, 3, maxtime,
+                                  extra=extra, threads=8)
+    assert ref.meta["newton_restart_draws"] == 0
+    blocks = parse_reference(ref.meta["stdout"])
+    assert len(blocks) == 2, ref.meta["stdout"][-3000:]
+    xa, xb = ref.xi()
+    with ipg.Event(ipg.Config(size=N, L=L, Ny=Ny, g=2.0, m=0.2, maxtime=maxtime)) as ev:
+        ev.set_g2mu(A, B)
+        ev.set_noise(xa, xb)
+        ev.init_fields()
+        res, m1, m2 = ev.run_multiplicity(**params)
+    for blk, m in zip(blocks, (m1, m2)):
+        hist = m["gauge"]["residual_every10"]
+        ref_hist = np.array([r for _, r in blk["residuals"]])
+        assert [k for k, _ in blk["residuals"]] == list(range(0, 10 * len(ref_hist), 10))
+        assert len(hist) == len(ref_hist), (hist, ref_hist)
+        assert np.all(np.abs(hist - ref_hist) <= 1e-8 * ref_hist), (hist, ref_hist)
+        assert m["gauge"]["nan_sites"] == 0
+        assert close(m["dNdy"], blk["dN1"], 1e-9) and close(m["dEdy"], blk["dE1"], 1e-9), (m, blk)
+        assert close(m["dNdy_binned"], blk["dN2"], 1e-9), (m["dNdy_binned"], blk["dN2"])
+        assert close(m["dEdy_binned"], blk["dE2"], 1e-9), (m["dEdy_binned"], blk["dE2"])
+        assert close(m["mean_pt"], blk["pt"], 1e-9)
+        if pseudo:
+            assert close(m["dNdy_cut3"], blk["cut1"], 1e-9) and close(m["dNdy_cut6"], blk["cut2"], 1e-9)
+        print("MULT", case, m["it"], m["gauge"]["iterations"], m["dNdy"], blk["dN1"],
+              m["dNdy_binned"], blk["dN2"])
+    assert m1["it"] == 1 and m2["it"] == res.itmax
+
+
+def _tr_e2(f):
+    """per-site tr(E^2) of a Hermitian field from get_field's [n][18]"""
+    z = f.reshape(-1, 9, 2)
+    return np.sum(z[..., 0] ** 2 + z[..., 1] ** 2, axis=1)
+
+
+def _plaquette(ux, uy, N):
+    """per-site Re tr(U_x(x) U_y(x+x) U_x(x+y)^dag U_y(x)^dag)"""
+    X = ux.reshape(N, N, 9, 2)
+    Y = uy.reshape(N, N, 9, 2)
+    X = (X[..., 0] + 1j * X[..., 1]).reshape(N, N, 3, 3)
+    Y = (Y[..., 0] + 1j * Y[..., 1]).reshape(N, N, 3, 3)
+    Yx = np.roll(Y, -1, axis=0)
+    Xy = np.roll(X, -1, axis=1)
+    P = X @ Yx @ np.conj(np.swapaxes(Xy, -1, -2)) @ np.conj(np.swapaxes(Y, -1, -2))
+    return np.trace(P, axis1=-2, axis2=-1).real
+
+
+def test_gauge_fix_keeps_local_invariants_and_reaches_coulomb_gauge():
+    """512^2 Pb+Pb after 20 steps: ipg_gauge_fix leaves every local gauge
+    invariant (tr E_i^2, tr phi^2, tr pi^2 per site, the plaquette per site)
+    unchanged to 1e-11, and a second call starts from the residual the first
+    one stopped at (no transformation follows the last check)."""
+    from ipglasma_b200.synthetic import make_event
+
+    N, L = 512, 40.0
+    A, B, _, _ = make_event(N, L, "Pb", 6.0, seed=5)
+    with ipg.Event(ipg.Config(size=N, L=L, Ny=10, maxtime=1.0, seed=4)) as ev:
+        ev.set_g2mu(A, B)
+        ev.use_device_noise()
+        ev.init_fields()
+        ev.evolve(20)
+        before = {w: ev.get_field(w) for w in (ipg.UX, ipg.UY, ipg.E1, ipg.E2, ipg.PHI, ipg.PI)}
+        rep = ev.gauge_fix(4000)
+        after = {w: ev.get_field(w) for w in before}
+        again = ev.gauge_fix(4000)
+    assert rep["iterations"] > 0 and rep["nan_sites"] == 0
+    assert rep["residual"] < 1e-6, rep["residual"]
+    assert abs(again["residual_every10"][0] / rep["residual"] - 1) < 1e-9, (rep, again)
+    if rep["residual"] < 1e-9:
+        assert again["iterations"] == 0
+    for w in (ipg.E1, ipg.E2, ipg.PHI, ipg.PI):
+        t0, t1 = _tr_e2(before[w]), _tr_e2(after[w])
+        assert np.abs(t1 - t0).max() <= 1e-11 * t0.max(), w
+    p0 = _plaquette(before[ipg.UX], before[ipg.UY], N)
+    p1 = _plaquette(after[ipg.UX], after[ipg.UY], N)
+    assert np.abs(p1 - p0).max() < 1e-11
+    print("GAUGE512", rep["iterations"], rep["residual"], rep["ms"], again)
+
+
+def test_spectrum_schedule_leaves_observables_unchanged():
+    """The evolution is gauge covariant: the run with the gauge fixing at
+    it = 1 gives the same E_T, eps_2 and energy density as the plain run."""
+    from ipglasma_b200.synthetic import make_event
+
+    N, L = 128, 20.0
+    A, B, _, _ = make_event(N, L, "Au", 3.0, seed=9)
+    out = []
+    for mult in (False, True):
+        with ipg.Event(ipg.Config(size=N, L=L, Ny=8, maxtime=0.4, seed=12)) as ev:
+            ev.set_g2mu(A, B)
+            ev.use_device_noise()
+            ev.init_fields()
+            res = ev.run_multiplicity()[0] if mult else ev.run()
+            out.append((res, ev.observables()[0]))
+    (r0, e0), (r1, e1) = out
+    assert abs(r1.E_T / r0.E_T - 1) < 1e-11
+    assert abs(r1.eccentricity[1] - r0.eccentricity[1]) < 1e-11
+    assert np.abs(e1 - e0).max() < 1e-10 * e0.max()
+
+
+def test_fp32_context_spectrum_close_to_fp64():
+    """On an FP32 context the spectrum is measured on an FP64 copy of the FP32
+    fields: dN/dy within 1e-4 of the FP64 context's."""
+    from ipglasma_b200.synthetic import make_event
+
+    N, L = 256, 30.0
+    A, B, _, _ = make_event(N, L, "Au", 2.0, seed=21)
+    vals = {}
+    for prec in (ipg.FP64, ipg.FP32):
+        with ipg.Event(ipg.Config(size=N, L=L, Ny=10, maxtime=0.4, seed=3, precision=prec)) as ev:
+            ev.set_g2mu(A, B)
+            ev.use_device_noise()
+            ev.init_fields()
+            _, m1, m2 = ev.run_multiplicity()
+            vals[prec] = (m1, m2)
+    for k in range(2):
+        a, b = vals[ipg.FP32][k], vals[ipg.FP64][k]
+        assert close(a["dNdy"], b["dNdy"], 1e-4) and close(a["dEdy"], b["dEdy"], 1e-4), (a, b)
+        print("MULT32", k, a["dNdy"], b["dNdy"], a["gauge"]["iterations"], b["gauge"]["iterations"])
