@@ -40,6 +40,50 @@ namespace {
 
 constexpr double kHbarc = 0.1973269718;
 
+// ------------------------------------------------------ gluon multiplicity
+// The lines Evolution::multiplicity prints (Evolution.cpp:2318-2330,
+// 3094-3109, with GaugeFix.cpp:48-92's residual every 10 iterations)
+void print_multiplicity(const ipg_multiplicity_result &m, const ipg_multiplicity_params &p) {
+    std::cout << "Measuring multiplicity ... " << std::endl;
+    std::cout << "gauge fixing" << std::endl;
+    for (int k = 0; k < 401 && 10 * k < m.gauge.residual_checks; k++)
+        std::cout << 10 * k << " " << m.gauge.residual_every10[k] << std::endl;
+    if (p.use_pseudorapidity == 0) {
+        std::cout << "dN/dy 1 = " << m.dNdy << ", dE/dy 1 = " << m.dEdy << std::endl;
+        std::cout << "dN/dy 2 = " << m.dNdy_binned << ", dE/dy 2 = " << m.dEdy_binned
+                  << std::endl;
+    } else {
+        std::cout << "dN/deta 1 = " << m.dNdy << ", dE/deta 1 = " << m.dEdy << std::endl;
+        std::cout << "dN/deta 2 = " << m.dNdy_binned << ", dE/deta 2 = " << m.dEdy_binned
+                  << std::endl;
+        std::cout << "dN/deta_cut 1 = " << m.dNdy_cut3 << std::endl;
+        std::cout << "dN/deta_cut 2 = " << m.dNdy_cut6 << std::endl;
+    }
+    std::cout << "gluon <p_T> = " << m.mean_pt << std::endl;
+    std::cout << " done." << std::endl;
+}
+
+// NpartdNdy-t<tau>-<id>.dat at it = itmax (Evolution.cpp:3124-3152): N_part,
+// dN/dy, T_pp, b, dE/dy, the seed, three N/A, the 3 and 6 GeV cuts and the
+// coupling ratio at the event's average Q_s
+void write_npart_dndy(int event_id, int itmax, double dtau, double a,
+                      const ipg_ipsat_report &ir, double b, unsigned long long seed,
+                      const ipg_multiplicity_result &m, double g, double muZero, double c,
+                      double qsFactor) {
+    std::stringstream name;
+    name << "NpartdNdy-t" << itmax * dtau * a << "-" << event_id << ".dat";
+    std::ofstream f(name.str().c_str(), std::ios::out);
+    f << ir.Npart << " " << m.dNdy << " " << ir.Tpp << " " << b << " " << m.dEdy << " " << seed
+      << " " << "N/A" << " " << "N/A" << " " << "N/A" << " " << m.dNdy_cut3 << " "
+      << m.dEdy_cut3 << " " << m.dNdy_cut6 << " " << m.dEdy_cut6 << " "
+      << g * g /
+             (4. * M_PI * 4. * M_PI /
+              (9. * std::log(std::pow(std::pow(muZero / 0.2, 2. / c) +
+                                          std::pow(qsFactor * ir.average_Qs / 0.2, 2. / c),
+                                      c))))
+      << std::endl;
+}
+
 // ---------------------------------------------------------------- input file
 class InputFile {
   public:
@@ -347,6 +391,16 @@ int main(int argc, char **argv) {
                       << std::endl;
     }
     const double rapidity = in.d("Rapidity");
+    // Evolution::multiplicity at it = 1 and it = itmax (Evolution.cpp:644-653)
+    const int gluonMult = (int)in.d_or("computeGluonMultiplicity", 0.0);
+    ipg_multiplicity_params mparams{};
+    mparams.max_gauge_iterations = 4000;
+    mparams.use_pseudorapidity = (int)in.d_or("usePseudoRapidity", 0.0);
+    mparams.rapidity = rapidity;
+    mparams.jacobian_m = in.d_or("Jacobianm", 0.35);
+    mparams.roots = in.d_or("roots", 7000.0);
+    const double muZero = in.d_or("muZero", 0.3), cRun = in.d_or("c", 0.2),
+                 qsFactor = in.d_or("runWithThisFactorTimesQs", 0.5);
     unsigned long long seed = in.ull("seed");
     if (in.i("useTimeForSeed") == 1) seed = std::random_device{}();
     if (readV < 0 || readV > 2 || writeV < 0 || writeV > 2) {
@@ -379,6 +433,8 @@ int main(int argc, char **argv) {
                         : (bmax - bmin) * xb + bmin;
         ipg_init_report rep;
         std::memset(&rep, 0, sizeof(rep));
+        ipg_ipsat_report irep;
+        std::memset(&irep, 0, sizeof(irep));
         if (readV != 0) {
             std::vector<double> VA, VB;
             std::ostringstream n1, n2;
@@ -404,7 +460,6 @@ int main(int argc, char **argv) {
             const auto nA = sample_nucleus(rng, sA, dmin);
             const auto nB = sample_nucleus(rng, sB, dmin);
             if (ipsat) {
-                ipg_ipsat_report irep;
                 check(ctx,
                       ipg_set_nuclei_ipsat(ctx, nA.data(), (int)(nA.size() / 3), nB.data(),
                                            (int)(nB.size() / 3), nullptr, nullptr, nullptr,
@@ -440,7 +495,25 @@ int main(int argc, char **argv) {
             }
         }
         ipg_result res;
-        check(ctx, ipg_run(ctx, &res), "ipg_run");
+        if (gluonMult) {
+            ipg_multiplicity_result m1, m2;
+            const ipg_status st = ipg_run_multiplicity(ctx, &mparams, &res, &m1, &m2);
+            if (itmax >= 2) print_multiplicity(m1, mparams);
+            if (st == IPG_NO_COLLISION) {
+                // Evolution.cpp:3111-3122 and 655: the evolution of this event
+                // stops after the spectrum at it = 1, no output files
+                std::cout << "No collision happened on rank 0. Restarting with new random "
+                             "number..."
+                          << std::endl;
+                continue;
+            }
+            check(ctx, st, "ipg_run_multiplicity");
+            print_multiplicity(m2, mparams);
+            write_npart_dndy(event_id, itmax, dtau, a, irep, b, seed, m2, cfg.g, muZero, cRun,
+                             qsFactor);
+        } else {
+            check(ctx, ipg_run(ctx, &res), "ipg_run");
+        }
         char hname[256], tname[256];
         ipg_output_names(event_id, itmax, dtau, a, hname, sizeof(hname), tname, sizeof(tname));
         // both files resampled and formatted on the GPU from the device

@@ -217,11 +217,16 @@ def test_gradient_at_AuAu256_400_steps_32_directions():
     checkpoint every 20 steps with time reversal in between. The gradient of
     E_T + eps2 with respect to g^2 mu^2 (16 directions of relative
     perturbations) and rho (16 directions in the noise) against central
-    finite differences with h = 1e-6 (relative): agreement within 1e-4
-    relative on every direction. Newton is polished to 1e-14 (sum of |F_a|):
-    at 1e-12 the loss moves by ~1e-9 between the two evaluations of a
-    difference, which is ~5e-4 of a directional derivative after the
-    division by 2h."""
+    finite differences with h = 1e-6 (relative), Newton polished to 1e-14.
+
+    Over 400 steps the evolution amplifies a perturbation by a large factor
+    G, so the central difference carries a truncation error of order
+    (h G)^2 that is not small at h = 1e-6 on every direction (measured: a
+    median gap of 2e-5, up to 7e-4). The differences are therefore taken at h
+    and h/2 and combined by Richardson extrapolation,
+    (4 D(h/2) - D(h)) / 3, which removes the h^2 term: every direction agrees
+    with the adjoint within 1e-4 relative, and the median of the plain
+    h = 1e-6 gaps stays below 1e-4."""
     from ipglasma_b200.synthetic import make_event
 
     N, L, Ny = 256, 30.0, 50
@@ -245,20 +250,28 @@ def test_gradient_at_AuAu256_400_steps_32_directions():
     g = ev.backward(1.0, 1.0, inputs=True, rho=True)
     amp = np.stack([2.0 * np.sqrt(A / Ny), 2.0 * np.sqrt(B / Ny)])
     h = 1e-6
-    rels = []
+    rows = []
     for k in range(32):
         if k < 16:
             dA = A * rng.uniform(-1, 1, A.shape)
             dB = B * rng.uniform(-1, 1, B.shape)
             directional = float(np.sum(g["g2mu"][0] * dA) + np.sum(g["g2mu"][1] * dB))
-            fd = (loss(A + h * dA, B + h * dB, xi) - loss(A - h * dA, B - h * dB, xi)) / (2 * h)
+
+            def D(s):
+                return (loss(A + s * dA, B + s * dB, xi) - loss(A - s * dA, B - s * dB, xi)) / (2 * s)
         else:
             dxi = rng.standard_normal(xi.shape)
             directional = float(np.sum(g["rho"] * amp[:, None, :, None] * dxi))
-            fd = (loss(A, B, xi + h * dxi) - loss(A, B, xi - h * dxi)) / (2 * h)
-        rels.append((abs(directional - fd) / abs(fd), k, directional, fd))
+
+            def D(s):
+                return (loss(A, B, xi + s * dxi) - loss(A, B, xi - s * dxi)) / (2 * s)
+        d1, d2 = D(h), D(h / 2)
+        rich = (4 * d2 - d1) / 3
+        rows.append((abs(directional - rich) / abs(rich), abs(directional - d1) / abs(d1), k,
+                     directional, d1, rich))
     ev.close()
-    print("FD32 relative gaps over 32 directions: "
-          + " ".join(f"{r[0]:.1e}" for r in rels))
-    worst = max(rels)
+    print("FD32 h=1e-6 gaps: " + " ".join(f"{r[1]:.1e}" for r in rows))
+    print("FD32 Richardson gaps: " + " ".join(f"{r[0]:.1e}" for r in rows))
+    assert float(np.median([r[1] for r in rows])) < 1e-4
+    worst = max(rows)
     assert worst[0] < 1e-4, worst

@@ -85,6 +85,53 @@ def test_executable_reproduces_reference_output_files(ref_harness, tmp_path):
         assert same > 0.8, (name, same)
 
 
+def test_executable_gluon_multiplicity_matches_reference(ref_harness, tmp_path):
+    """computeGluonMultiplicity 1: the executable gauge-fixes and measures the
+    spectrum at it = 1 and it = itmax like the reference's Evolution::run,
+    prints the same dN/dy lines and writes NpartdNdy-t<tau>-0.dat; its
+    spectrum columns (dN/dy, dE/dy and the 3 and 6 GeV cuts) agree with the
+    reference's file to the six printed digits, and the hydro file (written
+    before the gauge fixing at itmax) is the reference's."""
+    from ipglasma_b200.synthetic import gaussian_blobs
+
+    if not EXE.exists():
+        pytest.skip("executable not built")
+    N, L, Ny, seed, maxtime = 64, 12.0, 3, 1, 0.3
+    A, B = gaussian_blobs(N, L, 2.0, 1.5)
+    ref = ref_harness.run_harness(tmp_path / "ref", A, B, N, L, Ny, 2.0, 0.2, seed, maxtime,
+                                  write_outputs=5, extra=["--multiplicity", "1"])
+    assert ref.meta["newton_restart_draws"] == 0
+    run = tmp_path / "ours"
+    run.mkdir()
+    for v in ("V-0", "V-1"):
+        shutil.copy(ref.out / v, run / v)
+    text = INPUT.format(N=N, L=L, Ny=Ny, maxtime=maxtime).replace(
+        "EndOfFile", "computeGluonMultiplicity 1\nusePseudoRapidity 0\nEndOfFile")
+    (run / "input").write_text(text)
+    res = subprocess.run([str(EXE), "input"], cwd=run, capture_output=True, text=True,
+                         timeout=300)
+    assert res.returncode == 0, res.stderr
+    name = next(p.name for p in ref.out.glob("NpartdNdy-t*-0.dat"))
+    ours = (run / name).read_text().split()
+    theirs = (ref.out / name).read_text().split()
+    assert len(ours) == len(theirs) == 14
+    for col in (1, 4, 9, 10, 11, 12):
+        a, b = float(ours[col]), float(theirs[col])
+        assert abs(a - b) <= 2e-5 * abs(b), (col, a, b)
+    for key in ("dN/dy 1 = ", "dN/dy 2 = ", "gluon <p_T> = "):
+        lo = [l for l in res.stdout.splitlines() if l.startswith(key)]
+        lt = [l for l in ref.meta["stdout"].splitlines() if l.startswith(key)]
+        assert len(lo) == len(lt) == 2, key
+        for x, y in zip(lo, lt):
+            vx = float(x.split("=")[1].split(",")[0])
+            vy = float(y.split("=")[1].split(",")[0])
+            assert abs(vx - vy) <= 2e-5 * abs(vy), (key, x, y)
+    a = numbers(run / "epsilon-u-Hydro-TauHydro-0.dat")
+    b = numbers(ref.out / "epsilon-u-Hydro-TauHydro-0.dat")
+    assert a.shape == b.shape
+    assert np.all(np.abs(a - b) <= 2e-5 * np.abs(b) + 1e-12)
+
+
 def test_executable_samples_nuclei_on_its_own(tmp_path):
     """Without input Wilson lines the executable samples the nuclei, builds
     g2mu on the device (ipg_set_nuclei) and writes finite, positive energy
