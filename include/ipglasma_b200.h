@@ -324,10 +324,14 @@ ipg_status ipg_output_names(int event_id, int it, double dtau, double a,
  * the reference's two stopping rules (residual < 1e-9; residual above the one
  * recorded at the last multiple of 10 iterations and below 1e-6), then the
  * gauge transformation reu(expm(i chi)) with chi = IFFT(-1.5 / (k~^2 + 1e-9)
- * FFT(g)). On an FP64 context the live fields are transformed (later steps
- * continue from them, as in the reference); on an FP32 context an FP64 copy
- * of the current fields is, and the FP32 state is left alone (the evolution
- * is gauge covariant). */
+ * FFT(g)). The live fields are transformed and later steps continue from
+ * them, as in the reference (on an FP32 context an FP64 copy of the fields
+ * is transformed and rounded back). This matters: the reference's lattice
+ * clamps neighbours at its edges (Lattice.cpp:19-27, Evolution.cpp:209-210)
+ * while its gauge fixing is periodic (GaugeFix.cpp:54-66), so the evolution
+ * is not covariant under that transformation at the edges, and a gauge
+ * fixing part-way through changes what follows (by a few 1e-4 of the energy
+ * at 64^2). */
 typedef struct {
     int iterations;         /* gauge transformations applied */
     int residual_checks;    /* residuals computed (iterations + 1 when a rule

@@ -662,6 +662,9 @@ ipg_status gauge_fix_run(ipg_ctx *c, int max_iter, ipg_gauge_report *rep) {
         if (h->done) break;
     }
     IPG_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    // the reference transforms the live fields; later steps of an FP32
+    // context continue from the transformed fields rounded back to FP32
+    IPG_TRY(to_fp32_if_needed(c));
     IPG_CUDA(c, cudaMemcpyAsync(h, g.ctl, sizeof(GaugeFixCtl), cudaMemcpyDeviceToHost,
                                 c->stream));
     IPG_TRY(sync(c));

@@ -70,12 +70,12 @@ __device__ __forceinline__ double block_sum1(double v) {
     return s;
 }
 
-__device__ __forceinline__ C<double> cadd2(C<double> a, C<double> b) { return {a.r + b.r, a.i + b.i}; }
-__device__ __forceinline__ C<double> csub2(C<double> a, C<double> b) { return {a.r - b.r, a.i - b.i}; }
-__device__ __forceinline__ C<double> cconj(C<double> a) { return {a.r, -a.i}; }
-__device__ __forceinline__ C<double> cscale(C<double> a, double s) { return {a.r * s, a.i * s}; }
+__host__ __device__ __forceinline__ C<double> cadd2(C<double> a, C<double> b) { return {a.r + b.r, a.i + b.i}; }
+__host__ __device__ __forceinline__ C<double> csub2(C<double> a, C<double> b) { return {a.r - b.r, a.i - b.i}; }
+__host__ __device__ __forceinline__ C<double> cconj(C<double> a) { return {a.r, -a.i}; }
+__host__ __device__ __forceinline__ C<double> cscale(C<double> a, double s) { return {a.r * s, a.i * s}; }
 // a / b for a complex b (Smith's method, Comm. ACM 5 (1962) 435)
-__device__ __forceinline__ C<double> cdiv(C<double> a, C<double> b) {
+__host__ __device__ __forceinline__ C<double> cdiv(C<double> a, C<double> b) {
     if (fabs(b.r) >= fabs(b.i)) {
         const double r = b.i / b.r, d = b.r + b.i * r;
         return {(a.r + a.i * r) / d, (a.i - a.r * r) / d};
@@ -84,19 +84,19 @@ __device__ __forceinline__ C<double> cdiv(C<double> a, C<double> b) {
     return {(a.r * r + a.i) / d, (a.i * r - a.r) / d};
 }
 
-__device__ __forceinline__ M3<double> madd(const M3<double> &a, const M3<double> &b) {
+__host__ __device__ __forceinline__ M3<double> madd(const M3<double> &a, const M3<double> &b) {
     M3<double> r;
 #pragma unroll
     for (int k = 0; k < 9; k++) r.m[k] = cadd2(a.m[k], b.m[k]);
     return r;
 }
-__device__ __forceinline__ M3<double> mscale(const M3<double> &a, double s) {
+__host__ __device__ __forceinline__ M3<double> mscale(const M3<double> &a, double s) {
     M3<double> r;
 #pragma unroll
     for (int k = 0; k < 9; k++) r.m[k] = cscale(a.m[k], s);
     return r;
 }
-__device__ __forceinline__ void add_diag(M3<double> &a, double s) {
+__host__ __device__ __forceinline__ void add_diag(M3<double> &a, double s) {
     a.m[0].r += s;
     a.m[4].r += s;
     a.m[8].r += s;
@@ -109,7 +109,7 @@ __device__ __forceinline__ void add_diag(M3<double> &a, double s) {
 // |M_ij|, s = max(0, (int)(log2 |M| + 2)) when |M| > 1/2, and the
 // denominator Q - P is inverted by cofactors. A matrix whose norm is zero but
 // that is not zero (NaN entries) returns NaN (the reference exits there).
-__device__ M3<double> expm_pade6(const M3<double> &M) {
+__host__ __device__ M3<double> expm_pade6(const M3<double> &M) {
     const double c[7] = {1., 0.5, 0.1136363636, 0.01515151515, 0.001262626263,
                          6.313131313e-05, 1.503126503e-06};
     double norm = 0.0;
@@ -188,12 +188,12 @@ __device__ M3<double> expm_pade6(const M3<double> &M) {
     return U;
 }
 
-__device__ __forceinline__ double vnorm(const C<double> v[3]) {
+__host__ __device__ __forceinline__ double vnorm(const C<double> v[3]) {
     double s = 0.;
     for (int i = 0; i < 3; i++) s += v[i].r * v[i].r + v[i].i * v[i].i;
     return sqrt(s);
 }
-__device__ __forceinline__ void vnormalize(C<double> v[3]) {
+__host__ __device__ __forceinline__ void vnormalize(C<double> v[3]) {
     const double nv = vnorm(v);
     for (int i = 0; i < 3; i++) v[i] = {v[i].r / nv, v[i].i / nv};
 }
@@ -201,7 +201,7 @@ __device__ __forceinline__ void vnormalize(C<double> v[3]) {
 // Matrix::reu (Matrix.h:67-91): rows 0 and 1 by Gram-Schmidt (the second
 // against the first renormalised once more, as Spinor::GramSchmidt does),
 // row 2 the normalised complex conjugate of their cross product.
-__device__ M3<double> reunitarize(const M3<double> &u) {
+__host__ __device__ M3<double> reunitarize(const M3<double> &u) {
     C<double> e1[3] = {u.m[0], u.m[1], u.m[2]};
     C<double> a2[3] = {u.m[3], u.m[4], u.m[5]};
     vnormalize(e1);

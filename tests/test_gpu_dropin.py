@@ -96,7 +96,7 @@ def test_executable_gluon_multiplicity_matches_reference(ref_harness, tmp_path):
 
     if not EXE.exists():
         pytest.skip("executable not built")
-    N, L, Ny, seed, maxtime = 64, 12.0, 3, 1, 0.3
+    N, L, Ny, seed, maxtime = 64, 7.5, 3, 1, 0.3
     A, B = gaussian_blobs(N, L, 2.0, 1.5)
     ref = ref_harness.run_harness(tmp_path / "ref", A, B, N, L, Ny, 2.0, 0.2, seed, maxtime,
                                   write_outputs=5, extra=["--multiplicity", "1"])

@@ -12,6 +12,13 @@ rounding (bound 1e-8 relative) and stop at the same multiple of 10, and the
 spectra agree to 1e-9 relative. A global colour rotation is left free by the
 gauge condition; its rounding-level drift does not change any of these
 numbers, which are invariant under it.
+
+The gauge fixing at it = 1 transforms the fields the rest of the evolution
+starts from. The reference's lattice clamps neighbours at its edges while
+the gauge fixing is periodic, so that transformation is not a symmetry of
+the evolution there and the final T^{mu nu} differ from a run without it (a
+few 1e-4 of the energy); the final energy density is therefore compared with
+the reference's own run with the same schedule.
 """
 import re
 
@@ -55,9 +62,11 @@ def parse_reference(stdout: str):
 
 
 CASES = {
-    # N, L, nucleus, b, Ny, maxtime, pseudorapidity parameters
-    "AuAu64_y": (64, 16.0, "Au", 2.0, 4, 0.5, None),
-    "AuAu128_eta": (128, 24.0, "Au", 4.0, 4, 0.4, dict(rapidity=0.3, jacobian_m=0.35, roots=200.0)),
+    # N, L, Ny, maxtime, pseudorapidity parameters (a = 0.117 fm: the
+    # reference's Newton needs no random restarts on these maps, which keeps
+    # its tau = 0 links reproducible)
+    "blobs64_y": (64, 7.5, 4, 0.3, None),
+    "blobs128_eta": (128, 15.0, 4, 0.4, dict(rapidity=0.3, jacobian_m=0.35, roots=200.0)),
 }
 
 
@@ -67,10 +76,10 @@ def close(a, b, tol):
 
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_gauge_fixing_and_spectrum_match_reference(case, ref_harness, tmp_path):
-    from ipglasma_b200.synthetic import make_event
+    from ipglasma_b200.synthetic import gaussian_blobs
 
-    N, L, nuc, b, Ny, maxtime, pseudo = CASES[case]
-    A, B, _, _ = make_event(N, L, nuc, b, seed=31)
+    N, L, Ny, maxtime, pseudo = CASES[case]
+    A, B = gaussian_blobs(N, L, 2.0, 1.5)
     extra = ["--multiplicity", "1"]
     params = {}
     if pseudo:
@@ -88,6 +97,10 @@ def test_gauge_fixing_and_spectrum_match_reference(case, ref_harness, tmp_path):
         ev.set_noise(xa, xb)
         ev.init_fields()
         res, m1, m2 = ev.run_multiplicity(**params)
+        eps = ev.observables()[0]
+    ref_eps = ref.observables()[0]
+    e_gap = float(np.abs(eps - ref_eps).max() / ref_eps.max())
+    assert e_gap < 1e-9, e_gap
     for blk, m in zip(blocks, (m1, m2)):
         hist = m["gauge"]["residual_every10"]
         ref_hist = np.array([r for _, r in blk["residuals"]])
@@ -102,22 +115,19 @@ def test_gauge_fixing_and_spectrum_match_reference(case, ref_harness, tmp_path):
         if pseudo:
             assert close(m["dNdy_cut3"], blk["cut1"], 1e-9) and close(m["dNdy_cut6"], blk["cut2"], 1e-9)
         print("MULT", case, m["it"], m["gauge"]["iterations"], m["dNdy"], blk["dN1"],
-              m["dNdy_binned"], blk["dN2"])
+              m["dNdy_binned"], blk["dN2"], "e gap", e_gap)
     assert m1["it"] == 1 and m2["it"] == res.itmax
 
 
 def _tr_e2(f):
-    """per-site tr(E^2) of a Hermitian field from get_field's [n][18]"""
-    z = f.reshape(-1, 9, 2)
-    return np.sum(z[..., 0] ** 2 + z[..., 1] ** 2, axis=1)
+    """per-site tr(E E^dag) of a field from get_field ([n, 3, 3] complex)"""
+    return np.sum(np.abs(f) ** 2, axis=(1, 2))
 
 
 def _plaquette(ux, uy, N):
-    """per-site Re tr(U_x(x) U_y(x+x) U_x(x+y)^dag U_y(x)^dag)"""
-    X = ux.reshape(N, N, 9, 2)
-    Y = uy.reshape(N, N, 9, 2)
-    X = (X[..., 0] + 1j * X[..., 1]).reshape(N, N, 3, 3)
-    Y = (Y[..., 0] + 1j * Y[..., 1]).reshape(N, N, 3, 3)
+    """per-site Re tr(U_x(x) U_y(x+x) U_x(x+y)^dag U_y(x)^dag), periodic"""
+    X = ux.reshape(N, N, 3, 3)
+    Y = uy.reshape(N, N, 3, 3)
     Yx = np.roll(Y, -1, axis=0)
     Xy = np.roll(X, -1, axis=1)
     P = X @ Yx @ np.conj(np.swapaxes(Xy, -1, -2)) @ np.conj(np.swapaxes(Y, -1, -2))
@@ -156,30 +166,10 @@ def test_gauge_fix_keeps_local_invariants_and_reaches_coulomb_gauge():
     print("GAUGE512", rep["iterations"], rep["residual"], rep["ms"], again)
 
 
-def test_spectrum_schedule_leaves_observables_unchanged():
-    """The evolution is gauge covariant: the run with the gauge fixing at
-    it = 1 gives the same E_T, eps_2 and energy density as the plain run."""
-    from ipglasma_b200.synthetic import make_event
-
-    N, L = 128, 20.0
-    A, B, _, _ = make_event(N, L, "Au", 3.0, seed=9)
-    out = []
-    for mult in (False, True):
-        with ipg.Event(ipg.Config(size=N, L=L, Ny=8, maxtime=0.4, seed=12)) as ev:
-            ev.set_g2mu(A, B)
-            ev.use_device_noise()
-            ev.init_fields()
-            res = ev.run_multiplicity()[0] if mult else ev.run()
-            out.append((res, ev.observables()[0]))
-    (r0, e0), (r1, e1) = out
-    assert abs(r1.E_T / r0.E_T - 1) < 1e-11
-    assert abs(r1.eccentricity[1] - r0.eccentricity[1]) < 1e-11
-    assert np.abs(e1 - e0).max() < 1e-10 * e0.max()
-
-
 def test_fp32_context_spectrum_close_to_fp64():
-    """On an FP32 context the spectrum is measured on an FP64 copy of the FP32
-    fields: dN/dy within 1e-4 of the FP64 context's."""
+    """On an FP32 context the gauge fixing and the spectrum run on an FP64
+    copy of the FP32 fields, and the transformed fields are rounded back for
+    the remaining steps: dN/dy and dE/dy within 1e-4 of the FP64 context's."""
     from ipglasma_b200.synthetic import make_event
 
     N, L = 256, 30.0
