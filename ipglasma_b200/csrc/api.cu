@@ -120,8 +120,9 @@ struct ipg_ctx {
         C<double> *vbA = nullptr, *vbB = nullptr, *vcur = nullptr;
         double *g2mu_bar = nullptr;
         double *rho_all = nullptr;  // [2][Ny][n][8] rho adjoint, kept on the device
-        // FP32 adjoint (contexts of the FP32 form): the plain form's states and
-        // adjoints in FP32; the tau = 0 adjoint is widened into adj at the end
+        // FP32 adjoint (contexts of the FP32 form): the bulk form's own states
+        // (deviation storage) and adjoints in FP32; the tau = 0 adjoint is
+        // widened into adj at the end
         bool fp32 = false;
         std::vector<State<float>> cp32;   // checkpoints (every state when k = 1)
         std::vector<State<float>> seg32;  // a segment's states, recomputed
