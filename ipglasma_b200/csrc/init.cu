@@ -60,14 +60,14 @@ void launch_link_products(int N, C<double> *VA, C<double> *VB, C<double> *u1x,
 // ---------------------------------------------------------------------------
 
 // LU with partial pivoting and solve, in the elimination order of the
-// GSL 2.5 routines the reference calls (Init.cpp:47-63). Entry (r, c) of the
-// 8 x 8 matrix is J[(8 r + c) * js]: the Newton kernel keeps each thread's
-// matrix in shared memory with a stride of the block size (the pivoting
-// indexes it by data, which would otherwise put it in local memory).
-__device__ void lu_solve8(double *J, int js, const double F[8], double x[8]) {
-    int perm[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) perm[i] = i;
+// GSL 2.5 routines the reference calls (Init.cpp:47-63). Every operand lives
+// in the thread's slice of shared memory, element k at base[k * js] (js =
+// the block size): entry (r, c) of the 8 x 8 matrix at J[(8 r + c) * js], the
+// right-hand side at F, the solution to x. The pivoting indexes all of them
+// by data, which would put register arrays in local memory. The row swaps
+// are applied to F as they happen, which gives the permuted right-hand side
+// that GSL forms from the permutation afterwards; F is overwritten.
+__device__ void lu_solve8(double *J, double *F, double *x, int js) {
     for (int col = 0; col < 7; col++) {
         int piv = col;
         double best = fabs(J[(col * 8 + col) * js]);
@@ -84,9 +84,9 @@ __device__ void lu_solve8(double *J, int js, const double F[8], double x[8]) {
                 J[(col * 8 + k) * js] = J[(piv * 8 + k) * js];
                 J[(piv * 8 + k) * js] = t;
             }
-            int t = perm[col];
-            perm[col] = perm[piv];
-            perm[piv] = t;
+            const double t = F[col * js];
+            F[col * js] = F[piv * js];
+            F[piv * js] = t;
         }
         const double d = J[(col * 8 + col) * js];
         if (d != 0.0) {
@@ -97,19 +97,17 @@ __device__ void lu_solve8(double *J, int js, const double F[8], double x[8]) {
             }
         }
     }
-    double y[8];
-    for (int i = 0; i < 8; i++) y[i] = F[perm[i]];
     for (int i = 1; i < 8; i++) {
-        double acc = y[i];
-        for (int j = 0; j < i; j++) acc -= J[(i * 8 + j) * js] * y[j];
-        y[i] = acc;
+        double acc = F[i * js];
+        for (int j = 0; j < i; j++) acc -= J[(i * 8 + j) * js] * F[j * js];
+        F[i * js] = acc;
     }
     for (int i = 7; i >= 0; i--) {
-        double acc = y[i];
-        for (int j = i + 1; j < 8; j++) acc -= J[(i * 8 + j) * js] * y[j];
-        y[i] = acc / J[(i * 8 + i) * js];
+        double acc = F[i * js];
+        for (int j = i + 1; j < 8; j++) acc -= J[(i * 8 + j) * js] * F[j * js];
+        F[i * js] = acc / J[(i * 8 + i) * js];
     }
-    for (int i = 0; i < 8; i++) x[i] = y[i];
+    for (int i = 0; i < 8; i++) x[i * js] = F[i * js];
 }
 
 __device__ __forceinline__ void restart_alpha(double alpha[8], uint64_t key,
@@ -122,35 +120,60 @@ __device__ __forceinline__ void restart_alpha(double alpha[8], uint64_t key,
 }
 
 constexpr int kNewtonThreads = 128;
+// doubles of shared memory per thread: J (64), F, dalpha, alpha, best alpha
+constexpr int kNewtonSmem = 64 + 4 * 8;
+
+// the exponent held in shared memory, into registers, entry b replaced by v
+__device__ __forceinline__ void load_alpha(const double *al, int js, double out[8], int b = -1,
+                                           double v = 0.) {
+#pragma unroll
+    for (int k = 0; k < 8; k++) out[k] = (k == b) ? v : al[k * js];
+}
+
+// Im tr(t^a M) of M = S X^dag - X S^dag ... as the 8 values F_a are formed
+__device__ __forceinline__ void im_trace_ta(const M3<double> &m, double out[8]) {
+    C<double> t[8];
+    trace_ta(m, t);
+#pragma unroll
+    for (int a = 0; a < 8; a++) out[a] = t[a].i;
+}
 
 __global__ void __launch_bounds__(kNewtonThreads) k_newton(NewtonArgs A) {
-    // this thread's Jacobian, element k at J[k * kNewtonThreads]
+    // this thread's slice of shared memory, element k at base[k * js]
     extern __shared__ double newton_j[];
-    double *J = newton_j + threadIdx.x;
     constexpr int js = kNewtonThreads;
+    double *J = newton_j + threadIdx.x;
+    double *Fa = J + 64 * js, *dalpha = J + 72 * js, *al = J + 80 * js, *best_al = J + 88 * js;
     const size_t n = (size_t)A.N * A.N;
     const size_t lid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (lid >= 2 * n) return;
     // link order of the reference loop: per site, x then y (Init.cpp:2498-2516)
     const size_t pos = lid >> 1;
     const int dir = (int)(lid & 1);
-    const M3<double> U1 = ld_m3(dir ? A.u1y : A.u1x, pos, n);
-    const M3<double> U2 = ld_m3(dir ? A.u2y : A.u2x, pos, n);
+    // Daggers of S and of the iterate are taken inside the products
+    // (mul_nd: A B^dag), the best iterate is kept as its exponent, and the
+    // small arrays the iteration indexes by data sit in shared memory: that
+    // keeps the live state in registers. The iterates are bit-identical to
+    // forming the daggers and the best matrix.
+    M3<double> U0, S;
+    {
+        const M3<double> U1 = ld_m3(dir ? A.u1y : A.u1x, pos, n);
+        const M3<double> U2 = ld_m3(dir ? A.u2y : A.u2x, pos, n);
+        U0 = mul(U1, U2);
+        S = U1;
+        add_to(S, U2);
+    }
+    double traceCache[8];  // Im tr(t^a (S - S^dag))
+    im_trace_ta(minus(S, dagger(S)), traceCache);
 
-    const M3<double> U0 = mul(U1, U2);
-    M3<double> S = U1;
-    add_to(S, U2);
-    const M3<double> Sd = dagger(S);
-    C<double> traceCache[8];
-    trace_ta(minus(S, Sd), traceCache);
-
-    double alpha[8], dalpha[8], Fa[8];
+    double a8[8];
 #pragma unroll
-    for (int a = 0; a < 8; a++) alpha[a] = 0.;
-    M3<double> Usol = mul(exp_from_coeff(alpha), U0);
-    M3<double> Usold = dagger(Usol);
-    M3<double> best;
-    set_identity(best);
+    for (int a = 0; a < 8; a++) {
+        al[a * js] = 0.;
+        a8[a] = 0.;
+    }
+    M3<double> Usol = mul(exp_from_coeff(a8), U0);
+    bool have_best = false;  // false stands for the identity
     double Fzero = 10., FzeroMin = 1e6;
     int iter = 0, nRestart = 0, total = 0;
     uint32_t draws = 0;
@@ -159,35 +182,41 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton(NewtonArgs A) {
         total++;
         Fzero = 0.;
         {
-            M3<double> Mt = mul(S, Usold);
-            sub_from(Mt, mul(Usol, Sd));
-            C<double> tl[8];
-            trace_ta(Mt, tl);
+            M3<double> Mt = mul_nd(S, Usol);
+            sub_from(Mt, mul_nd(Usol, S));
+            double tl[8];
+            im_trace_ta(Mt, tl);
 #pragma unroll
             for (int a = 0; a < 8; a++) {
                 // -(traceCache + traceLoc), imaginary part
-                Fa[a] = -(traceCache[a].i + tl[a].i);
-                Fzero += fabs(Fa[a]);
+                const double f = -(traceCache[a] + tl[a]);
+                Fa[a * js] = f;
+                Fzero += fabs(f);
             }
         }
         bool good = true;
         for (int b = 0; b < 8; b++) {
-            const double d = fmax(0.001, fmin(10., 0.01 * fabs(alpha[b])));
-            alpha[b] = alpha[b] + d;
-            M3<double> Mt = dagger(mul(exp_from_coeff(alpha), U0));
-            Mt = mul(S, minus(Mt, Usold));
-            C<double> tl[8];
-            trace_ta(Mt, tl);
+            const double ab = al[b * js];
+            const double d = fmax(0.001, fmin(10., 0.01 * fabs(ab)));
+            const double ap = ab + d;
+            load_alpha(al, js, a8, b, ap);
+            const M3<double> Mt = mul_nd(S, minus(mul(exp_from_coeff(a8), U0), Usol));
+            double tl[8];
+            im_trace_ta(Mt, tl);
             double mcheck = 0.;
+#pragma unroll
             for (int a = 0; a < 8; a++) {
-                J[(a * 8 + b) * js] = 2. * tl[a].i / d;
-                mcheck += fabs(J[(a * 8 + b) * js]);
+                const double j = 2. * tl[a] / d;
+                J[(a * 8 + b) * js] = j;
+                mcheck += fabs(j);
                 if (mcheck < 1e-15) good = false;
             }
-            alpha[b] = alpha[b] - d;
+            // the reference adds d and subtracts it again (the rounding stays)
+            al[b * js] = ap - d;
         }
         if (!good) {
             // analytic approximation (Init.cpp:3419-3431)
+            const M3<double> Usold = dagger(Usol);
             for (int b = 0; b < 8; b++) {
                 const M3<double> Mt = ta_mul(b, Usold);
                 for (int a = 0; a < 8; a++) {
@@ -196,90 +225,102 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton(NewtonArgs A) {
                 }
             }
         }
-        lu_solve8(J, js, Fa, dalpha);
+        lu_solve8(J, Fa, dalpha, js);
         bool ok = true;
         for (int a = 0; a < 8; a++)
-            if (fabs(dalpha[a]) > 1e5) {
+            if (fabs(dalpha[a * js]) > 1e5) {
                 ok = false;
                 break;
             }
         if (ok) {
-            for (int a = 0; a < 8; a++) alpha[a] = alpha[a] + dalpha[a];
+#pragma unroll
+            for (int a = 0; a < 8; a++) al[a * js] = al[a * js] + dalpha[a * js];
         } else {
-            restart_alpha(alpha, A.philox_key, (uint32_t)lid, draws++);
+            restart_alpha(a8, A.philox_key, (uint32_t)lid, draws++);
+#pragma unroll
+            for (int a = 0; a < 8; a++) al[a * js] = a8[a];
         }
-        Usol = mul(exp_from_coeff(alpha), U0);
-        Usold = dagger(Usol);
+        load_alpha(al, js, a8);
+        Usol = mul(exp_from_coeff(a8), U0);
         if (Fzero < FzeroMin) {
             FzeroMin = Fzero;
-            best = Usol;
+            have_best = true;
+#pragma unroll
+            for (int a = 0; a < 8; a++) best_al[a * js] = a8[a];
         }
         if (iter == A.max_iter) {
-            restart_alpha(alpha, A.philox_key, (uint32_t)lid, draws++);
-            Usol = mul(exp_from_coeff(alpha), U0);
-            Usold = dagger(Usol);
+            restart_alpha(a8, A.philox_key, (uint32_t)lid, draws++);
+#pragma unroll
+            for (int a = 0; a < 8; a++) al[a * js] = a8[a];
+            Usol = mul(exp_from_coeff(a8), U0);
             nRestart++;
             iter = 0;
         }
     }
     int status = draws ? 1 : 0;
     if (nRestart == A.max_restart) {
-        Usol = best;
+        if (have_best) {
+            load_alpha(best_al, js, a8);
+            Usol = mul(exp_from_coeff(a8), U0);
+        } else {
+            set_identity(Usol);
+        }
         status = 2;
     } else if (A.tol < 1e-6) {
         // polish beyond the reference's criterion (for derivatives through the
         // root): Newton steps with a central-difference Jacobian, no restarts,
         // keeping the iterate with the smallest residual
-        double bestF = 1e300, bestA[8];
+        double bestF = 1e300;
         for (int p = 0; p < 8; p++) {
-            double F[8], s = 0.;
+            double s = 0.;
             {
-                M3<double> Mt = mul(S, Usold);
-                sub_from(Mt, mul(Usol, Sd));
-                C<double> tl[8];
-                trace_ta(Mt, tl);
+                M3<double> Mt = mul_nd(S, Usol);
+                sub_from(Mt, mul_nd(Usol, S));
+                double tl[8];
+                im_trace_ta(Mt, tl);
                 for (int a = 0; a < 8; a++) {
-                    F[a] = -(traceCache[a].i + tl[a].i);
-                    s += fabs(F[a]);
+                    const double f = -(traceCache[a] + tl[a]);
+                    Fa[a * js] = f;
+                    s += fabs(f);
                 }
             }
             if (s < bestF) {
                 bestF = s;
-                for (int a = 0; a < 8; a++) bestA[a] = alpha[a];
+                for (int a = 0; a < 8; a++) best_al[a * js] = al[a * js];
             }
             if (s < A.tol) break;
             for (int b = 0; b < 8; b++) {
-                const double h = 1e-6, a0 = alpha[b];
-                alpha[b] = a0 + h;
-                const M3<double> Up = mul(exp_from_coeff(alpha), U0);
-                alpha[b] = a0 - h;
-                const M3<double> Um = mul(exp_from_coeff(alpha), U0);
-                alpha[b] = a0;
+                const double h = 1e-6, a0 = al[b * js];
+                load_alpha(al, js, a8, b, a0 + h);
+                const M3<double> Up = mul(exp_from_coeff(a8), U0);
+                load_alpha(al, js, a8, b, a0 - h);
+                const M3<double> Um = mul(exp_from_coeff(a8), U0);
                 const M3<double> dU = scaled(minus(Up, Um), 0.5 / h);
                 M3<double> Mt = mul_nd(S, dU);
                 sub_from(Mt, mul_nd(dU, S));
-                C<double> tl[8];
-                trace_ta(Mt, tl);
-                for (int a = 0; a < 8; a++) J[(a * 8 + b) * js] = -tl[a].i;
+                double tl[8];
+                im_trace_ta(Mt, tl);
+                for (int a = 0; a < 8; a++) J[(a * 8 + b) * js] = -tl[a];
             }
-            lu_solve8(J, js, F, dalpha);
-            for (int a = 0; a < 8; a++) alpha[a] -= dalpha[a];
-            Usol = mul(exp_from_coeff(alpha), U0);
-            Usold = dagger(Usol);
+            lu_solve8(J, Fa, dalpha, js);
+            for (int a = 0; a < 8; a++) al[a * js] -= dalpha[a * js];
+            load_alpha(al, js, a8);
+            Usol = mul(exp_from_coeff(a8), U0);
         }
-        for (int a = 0; a < 8; a++) alpha[a] = bestA[a];
-        Usol = mul(exp_from_coeff(alpha), U0);
+        for (int a = 0; a < 8; a++) al[a * js] = best_al[a * js];
+        load_alpha(al, js, a8);
+        Usol = mul(exp_from_coeff(a8), U0);
     }
     st_m3(dir ? A.uy : A.ux, pos, n, Usol);
     if (A.alpha)
-        for (int a = 0; a < 8; a++) A.alpha[(size_t)a * 2 * n + lid] = alpha[a];
+        for (int a = 0; a < 8; a++) A.alpha[(size_t)a * 2 * n + lid] = al[a * js];
     A.iters[lid] = total;
     A.status[lid] = status;
 }
 
 void launch_newton(const NewtonArgs &a, cudaStream_t st) {
     const size_t links = 2 * (size_t)a.N * a.N;
-    const size_t smem = sizeof(double) * 64 * kNewtonThreads;  // 64 KB
+    const size_t smem = sizeof(double) * kNewtonSmem * kNewtonThreads;  // 96 KB
     cudaFuncSetAttribute(k_newton, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_newton<<<(unsigned)((links + kNewtonThreads - 1) / kNewtonThreads), kNewtonThreads, smem,
                st>>>(a);
