@@ -23,6 +23,9 @@ Reported (one JSON line, rank 0):
                FP64 batches, per-kernel GB/s, error
   single_event one 512^2 Pb+Pb event (tau 0.6 fm) per form: the tile kernels
   adjoint      gradient of E_T + eps2 for a 256^2 Au+Au event, 400 steps
+  multiplicity Coulomb gauge fixing and the gluon spectrum of a 512^2 Pb+Pb
+               event after its first step (the computeGluonMultiplicity
+               schedule's it = 1 call)
   cpu_baseline the reference (oracle/_ref, OpenMP, all host cores) on one event
                of each size class of the same workload, combined in the
                batch's proportions
@@ -218,6 +221,8 @@ def main():
                     help="skip the 8 x 1024^2 Pb+Pb production batch")
     ap.add_argument("--no-single", action="store_true",
                     help="skip the single 512^2 event (tile kernels) measurement")
+    ap.add_argument("--no-multiplicity", action="store_true",
+                    help="skip the gauge-fixing and gluon-spectrum leg")
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint (forward/backward) measurement")
     ap.add_argument("--profile", choices=["fp32", "fp64", "both", "adjoint", "batch32",
@@ -617,6 +622,7 @@ def run_ours(args, world, rank, local):
     single = None if args.no_single else measure_single(torch, ipg, K, W, rank, world, dist,
                                                         hbm)
     adjoint = None if args.no_adjoint else measure_adjoint(torch, ipg, rank)
+    mult = None if args.no_multiplicity else measure_multiplicity(ipg, rank, hbm)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -661,6 +667,7 @@ def run_ours(args, world, rank, local):
             "large": large,
             "single_event": single,
             "adjoint": adjoint,
+            "multiplicity": mult,
             "cpu_baseline": cpu,
             "gpu_launches": int(res["launches"]),
             "clocks": clk.summary(),
@@ -669,6 +676,49 @@ def run_ours(args, world, rank, local):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# bytes a site moves in one gauge-fixing iteration: the links read for the
+# divergence (2 x 144), the packed g through the FFT passes (64 written, then
+# 3 passes of 64 read + 64 written), the exponential (64 read, 144 written),
+# the transformation (G 144 read, the state's 70 reals read and written)
+GAUGE_BYTES_PER_SITE_ITERATION = 288 + 64 + 3 * 128 + 64 + 144 + 144 + 2 * 560
+
+
+def measure_multiplicity(ipg, rank, hbm):
+    """Evolution::multiplicity on one Pb+Pb 512^2 event (L = 40 fm, Ny = 50,
+    b = 6 fm) after its first step, as the computeGluonMultiplicity schedule
+    runs it at it = 1: Coulomb gauge fixing (device time, iterations, and the
+    HBM rate at GAUGE_BYTES_PER_SITE_ITERATION a site and iteration), then the
+    spectrum."""
+    if rank != 0:
+        return None
+    from ipglasma_b200.synthetic import make_event
+
+    N, L = 512, 40.0
+    A, B, _, _ = make_event(N, L, "Pb", 6.0, seed=606)
+    out = {}
+    with ipg.Event(ipg.Config(size=N, L=L, Ny=50, maxtime=0.6, seed=606)) as ev:
+        for rep_ in range(2):  # the first pass warms up
+            ev.set_g2mu(A, B)
+            ev.use_device_noise()
+            ev.init_fields()
+            ev.evolve(1)
+            m = ev.multiplicity()
+        g = m["gauge"]
+        per_it = g["ms"] / max(1, g["residual_checks"])
+        gbs = N * N * GAUGE_BYTES_PER_SITE_ITERATION / (per_it * 1e-3) / 1e9
+        out = {"workload": "Pb+Pb 512^2 (L 40 fm, Ny 50, b 6 fm), fields after the first step",
+               "gauge_iterations": g["iterations"], "gauge_residual": g["residual"],
+               "gauge_ms": round(g["ms"], 3), "us_per_iteration": round(1e3 * per_it, 2),
+               "gauge_GBs": round(gbs, 1), "gauge_frac": round(gbs / hbm, 4),
+               "bytes_per_site_iteration": GAUGE_BYTES_PER_SITE_ITERATION,
+               "spectrum_ms": round(m["ms_spectrum"], 3), "dNdy": m["dNdy"],
+               "dNdy_binned": m["dNdy_binned"], "mean_pt": m["mean_pt"],
+               "timing": "device time (CUDA events) of the gauge fixing, its iterations "
+                         "enqueued in chunks of 16 with one flag read per chunk; the "
+                         "iterations after a stopping rule return at once"}
+    return out
 
 
 def measure_large(torch, ipg, rank, world, dist, hbm):

@@ -49,6 +49,9 @@ namespace ipg {
 namespace {
 
 constexpr int GB = 256;  // threads per block of the per-site kernels
+// the exponential and the transformation need ~170 registers a thread:
+// blocks of 128 threads put three blocks (12 warps) on an SM instead of one
+constexpr int GB_HEAVY = 128;
 constexpr double kHbarcGf = 0.1973269718;  // GeV fm (Phys_consts.h)
 
 __device__ __forceinline__ double warp_sum(double x) {
@@ -300,11 +303,11 @@ __global__ void k_gf_green(int N, const double *sin_half, double *green) {
     green[p] = -1.5 * (1. / (kt2 + 1e-9));
 }
 
-__global__ void __launch_bounds__(GB) k_gf_exp(const double2 *chi, int N, C<double> *G,
-                                               GaugeFixCtl *ctl) {
+__global__ void __launch_bounds__(GB_HEAVY) k_gf_exp(const double2 *chi, int N, C<double> *G,
+                                                     GaugeFixCtl *ctl) {
     if (ctl->done) return;
     const size_t n = (size_t)N * N;
-    const size_t pos = (size_t)blockIdx.x * GB + threadIdx.x;
+    const size_t pos = (size_t)blockIdx.x * GB_HEAVY + threadIdx.x;
     if (pos >= n) return;
     const double2 p0 = chi[pos], p1 = chi[n + pos], p2 = chi[2 * n + pos], p3 = chi[3 * n + pos];
     const double d0 = p0.x, d1 = p0.y, d2 = -(d0 + d1);
@@ -328,11 +331,11 @@ __global__ void __launch_bounds__(GB) k_gf_exp(const double2 *chi, int N, C<doub
     st_m3(G, pos, n, g);
 }
 
-__global__ void __launch_bounds__(GB) k_gf_transform(State<double> s, const C<double> *G, int N,
-                                                     const GaugeFixCtl *ctl) {
+__global__ void __launch_bounds__(GB_HEAVY) k_gf_transform(State<double> s, const C<double> *G,
+                                                           int N, const GaugeFixCtl *ctl) {
     if (ctl->done) return;
     const size_t n = (size_t)N * N;
-    const size_t pos = (size_t)blockIdx.x * GB + threadIdx.x;
+    const size_t pos = (size_t)blockIdx.x * GB_HEAVY + threadIdx.x;
     if (pos >= n) return;
     const int ix = (int)(pos / N), iy = (int)(pos % N);
     const size_t px = (size_t)((ix + 1) % N) * N + iy;
@@ -360,12 +363,12 @@ void launch_gauge_green(int N, const double *sin_half, double *green, cudaStream
 void launch_gauge_fix_iteration(const GaugeFixArgs &a, cudaStream_t st) {
     const size_t n = (size_t)a.N * a.N;
     const int blocks = gauge_fix_blocks(a.N);
-    const unsigned sites = (unsigned)((n + GB - 1) / GB);
+    const unsigned heavy = (unsigned)((n + GB_HEAVY - 1) / GB_HEAVY);
     k_gf_chi<<<blocks, GB, 0, st>>>(a.s, a.N, a.chi, a.partial, a.ctl);
     k_gf_control<<<1, GB, 0, st>>>(a.partial, blocks, a.N, a.ctl);
     launch_poisson_sheets(a.fft, 1, st);  // chi -> chi in place, skipped when done
-    k_gf_exp<<<sites, GB, 0, st>>>(a.chi, a.N, a.G, a.ctl);
-    k_gf_transform<<<sites, GB, 0, st>>>(a.s, a.G, a.N, a.ctl);
+    k_gf_exp<<<heavy, GB_HEAVY, 0, st>>>(a.chi, a.N, a.G, a.ctl);
+    k_gf_transform<<<heavy, GB_HEAVY, 0, st>>>(a.s, a.G, a.N, a.ctl);
 }
 
 // -------------------------------------------------------------------------
