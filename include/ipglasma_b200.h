@@ -76,6 +76,15 @@ typedef struct {
     double newton_tolerance; /* stop when sum_a |F_a| < this; <= 0 -> 1e-6, the
                                 reference's criterion (Init.cpp:3372). The
                                 adjoint needs a converged root: use ~1e-12 */
+    int newton_mode;   /* 0: the reference's iteration (Init.cpp:3344-3481),
+                          bit for bit; 1: Newton on the group, U <- exp(i d.t) U
+                          with the exact Jacobian of that step (no numeric
+                          differences, stops as soon as sum_a |F_a| < the
+                          tolerance), for throughput: the same root to the
+                          tolerance, not the same bits; a link it does not
+                          converge in 30 steps takes the reference's
+                          iteration. The adjoint through the initial
+                          conditions needs mode 0. */
 } ipg_config;
 
 /* Summary of the initial-condition stage. */

@@ -58,6 +58,7 @@ class _Config(ct.Structure):
         ("precision", ct.c_int), ("newton_max_iterations", ct.c_int),
         ("newton_max_restarts", ct.c_int), ("seed", ct.c_uint64),
         ("device", ct.c_int), ("newton_tolerance", ct.c_double),
+        ("newton_mode", ct.c_int),
     ]
 
 
@@ -295,12 +296,13 @@ class Config:
     device: int = 0
     Nc: int = 3
     newton_tolerance: float = 0.0
+    newton_mode: int = 0  # 0 the reference's iteration, 1 Newton on the group
 
     def to_c(self) -> _Config:
         return _Config(self.size, self.Nc, self.Ny, self.L, self.g, self.m,
                        self.UVdamp, self.maxtime, self.dtau, self.precision,
                        self.newton_max_iterations, self.newton_max_restarts,
-                       self.seed, self.device, self.newton_tolerance)
+                       self.seed, self.device, self.newton_tolerance, self.newton_mode)
 
 
 @dataclass

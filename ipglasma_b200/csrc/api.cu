@@ -756,6 +756,8 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
         return bad("L, g, maxtime must be > 0 and m, UVdamp >= 0");
     if (cfg->precision != IPG_FP64 && cfg->precision != IPG_FP32)
         return bad("precision must be IPG_FP64 or IPG_FP32");
+    if (cfg->newton_mode != 0 && cfg->newton_mode != 1)
+        return bad("newton_mode must be 0 (the reference's iteration) or 1 (Newton on the group)");
     if (c->cfg.newton_max_iterations <= 0) c->cfg.newton_max_iterations = 2000;
     if (c->cfg.newton_max_restarts <= 0) c->cfg.newton_max_restarts = 200;
     if (!(c->cfg.newton_tolerance > 0)) c->cfg.newton_tolerance = 1e-6;
@@ -1270,6 +1272,7 @@ static ipg_status init_enqueue(ipg_ctx *c, bool from_wilson) {
     na.max_restart = c->cfg.newton_max_restarts;
     na.tol = c->cfg.newton_tolerance;
     na.alpha = c->newton_alpha;
+    na.mode = c->cfg.newton_mode;
     na.philox_key = c->cfg.seed ^ 0x5DEECE66DULL;
     na.u1x = c->u1x;
     na.u2x = c->u2x;
@@ -2041,6 +2044,10 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
     if ((grad_g2mu || grad_rho) && !A.from_inputs)
         return fail(c, IPG_ERR_STATE,
                     "input gradients need a tau = 0 state made by ipg_init_fields");
+    if ((grad_g2mu || grad_rho) && c->cfg.newton_mode != 0)
+        return fail(c, IPG_ERR_STATE,
+                    "input gradients differentiate the reference's Newton iteration: "
+                    "use newton_mode 0");
     const size_t n = c->n;
     const int N = c->N;
     const int S = A.steps;

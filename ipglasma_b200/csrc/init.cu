@@ -147,6 +147,7 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton(NewtonArgs A) {
     const size_t n = (size_t)A.N * A.N;
     const size_t lid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (lid >= 2 * n) return;
+    if (A.redo_only && A.status[lid] != -1) return;
     // link order of the reference loop: per site, x then y (Init.cpp:2498-2516)
     const size_t pos = lid >> 1;
     const int dir = (int)(lid & 1);
@@ -318,12 +319,107 @@ __global__ void __launch_bounds__(kNewtonThreads) k_newton(NewtonArgs A) {
     A.status[lid] = status;
 }
 
+// ---------------------------------------------------------------------------
+// Throughput mode: Newton's method on the group. The same matching condition
+//   F_a(U) = -Im tr(t^a (S - S^dag + S U^dag - U S^dag)) = 0
+// is solved by steps U <- exp(i d.t) U with d = -J^-1 F and the exact
+// Jacobian of that left perturbation: with X = S U^dag,
+//   dF_a / dd_b = Re tr(t^a X t^b + t^a t^b X^dag) = 2 Re tr(t^b t^a X)
+// (checked against central differences), so the convergence is quadratic,
+// no exponential is differenced, and the loop stops as soon as
+// sum_a |F_a| < tol. A link that is not below tol after kFastSteps steps, or
+// that meets a non-finite value, is marked (status -1) for the reference's
+// iteration, which the launcher runs after this kernel.
+// ---------------------------------------------------------------------------
+constexpr int kFastThreads = 128;
+constexpr int kFastSmem = 64 + 2 * 8;  // J, then F and the step d
+constexpr int kFastSteps = 30;
+
+__global__ void __launch_bounds__(kFastThreads) k_newton_fast(NewtonArgs A) {
+    extern __shared__ double newton_f[];
+    constexpr int js = kFastThreads;
+    double *J = newton_f + threadIdx.x;
+    double *Fv = J + 64 * js, *dv = J + 72 * js;
+    const size_t n = (size_t)A.N * A.N;
+    const size_t lid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (lid >= 2 * n) return;
+    const size_t pos = lid >> 1;
+    const int dir = (int)(lid & 1);
+    M3<double> U0, S;
+    {
+        const M3<double> U1 = ld_m3(dir ? A.u1y : A.u1x, pos, n);
+        const M3<double> U2 = ld_m3(dir ? A.u2y : A.u2x, pos, n);
+        U0 = mul(U1, U2);
+        S = U1;
+        add_to(S, U2);
+    }
+    double traceCache[8];
+    im_trace_ta(minus(S, dagger(S)), traceCache);
+    M3<double> U = U0;  // exp(i 0.t) U0
+    int steps = 0;
+    bool done = false;
+    for (; steps <= kFastSteps; steps++) {
+        const M3<double> X = mul_nd(S, U);
+        double tl[8];
+        im_trace_ta(minus(X, dagger(X)), tl);
+        double s = 0.;
+        bool finite = true;
+#pragma unroll
+        for (int a = 0; a < 8; a++) {
+            const double f = -(traceCache[a] + tl[a]);
+            Fv[a * js] = -f;  // the right-hand side of J d = -F
+            s += fabs(f);
+            finite = finite && isfinite(f);
+        }
+        if (!finite) break;
+        if (s < A.tol) {
+            done = true;
+            break;
+        }
+        if (steps == kFastSteps) break;
+        for (int a = 0; a < 8; a++) {
+            C<double> tr[8];
+            trace_ta(ta_mul(a, X), tr);  // tr(t^b t^a X)
+#pragma unroll
+            for (int b = 0; b < 8; b++) J[(a * 8 + b) * js] = 2. * tr[b].r;
+        }
+        lu_solve8(J, Fv, dv, js);
+        double d8[8];
+        bool ok = true;
+#pragma unroll
+        for (int a = 0; a < 8; a++) {
+            d8[a] = dv[a * js];
+            ok = ok && isfinite(d8[a]) && fabs(d8[a]) < 1e3;
+        }
+        if (!ok) break;
+        U = mul(exp_from_coeff(d8), U);
+    }
+    if (done) {
+        st_m3(dir ? A.uy : A.ux, pos, n, U);
+        A.iters[lid] = steps + 1;
+        A.status[lid] = 0;
+        if (A.alpha)
+            for (int a = 0; a < 8; a++) A.alpha[(size_t)a * 2 * n + lid] = nan("");
+    } else {
+        A.status[lid] = -1;  // the reference's iteration takes this link
+    }
+}
+
 void launch_newton(const NewtonArgs &a, cudaStream_t st) {
     const size_t links = 2 * (size_t)a.N * a.N;
     const size_t smem = sizeof(double) * kNewtonSmem * kNewtonThreads;  // 96 KB
     cudaFuncSetAttribute(k_newton, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    NewtonArgs b = a;
+    if (a.mode == 1) {
+        const size_t fsmem = sizeof(double) * kFastSmem * kFastThreads;  // 80 KB
+        cudaFuncSetAttribute(k_newton_fast, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)fsmem);
+        k_newton_fast<<<(unsigned)((links + kFastThreads - 1) / kFastThreads), kFastThreads,
+                        fsmem, st>>>(a);
+        b.redo_only = 1;
+    }
     k_newton<<<(unsigned)((links + kNewtonThreads - 1) / kNewtonThreads), kNewtonThreads, smem,
-               st>>>(a);
+               st>>>(b);
 }
 
 // ---------------------------------------------------------------------------

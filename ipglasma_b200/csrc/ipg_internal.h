@@ -215,6 +215,8 @@ struct NewtonArgs {
     int *status;         // [2n] 0 ok, 1 restarted then converged, 2 failed
     double tol;          // stop when sum_a |F_a| < tol (reference: 1e-6)
     double *alpha;       // [8][2n] the solution's exponent (may be null)
+    int mode = 0;        // 0: the reference's iteration; 1: Newton on the group
+    int redo_only = 0;   // (internal) run only the links whose status is -1
 };
 void launch_newton(const NewtonArgs &a, cudaStream_t st);
 

@@ -1,0 +1,76 @@
+"""The two tau = 0 Newton modes (cfg.newton_mode): 0 is the reference's
+iteration (Init.cpp:3344-3481, numeric one-sided Jacobian, bit for bit), 1 is
+Newton's method on the group with the exact Jacobian of the left
+perturbation U <- exp(i d.t) U, which stops as soon as sum_a |F_a| is below
+the tolerance. Both solve the same matching condition, so with a tight
+tolerance they reach the same links."""
+import numpy as np
+import pytest
+
+import ipglasma_b200 as ipg
+
+pytestmark = pytest.mark.gpu
+
+
+def _links(N, L, nuc, b, mode, tol, prec=ipg.FP64, Ny=20):
+    from ipglasma_b200.synthetic import make_event
+
+    A, B, _, _ = make_event(N, L, nuc, b, seed=44)
+    cfg = ipg.Config(size=N, L=L, Ny=Ny, maxtime=0.4, seed=9, precision=prec,
+                     newton_mode=mode, newton_tolerance=tol)
+    with ipg.Event(cfg) as ev:
+        ev.set_g2mu(A, B)
+        ev.use_device_noise()
+        reps = [ev.init_fields() for _ in range(3)]
+        out = (ev.get_field(ipg.UX), ev.get_field(ipg.UY), ev.get_field(ipg.PI))
+        it, st = ev.newton_iterations()
+        res = ev.run()
+    return out, reps[-1], it, st, res
+
+
+def test_both_modes_reach_the_same_root():
+    """At tolerance 1e-12 (the mirror polishes past the reference's 1e-6) the
+    links of the two modes agree within 1e-12 on a 256^2 Au+Au event, and the
+    group iteration needs no fallback to the reference's."""
+    m0, r0, it0, st0, _ = _links(256, 30.0, "Au", 2.0, 0, 1e-12)
+    m1, r1, it1, st1, _ = _links(256, 30.0, "Au", 2.0, 1, 1e-12)
+    gap = max(np.abs(a - b).max() for a, b in zip(m0[:2], m1[:2]))
+    print("NEWTON same root: gap %.2e, iterations mirror max %d mean %.2f, group max %d mean "
+          "%.2f, ms %.3f vs %.3f" % (gap, it0.max(), it0.mean(), it1.max(), it1.mean(),
+                                     r0.ms_newton, r1.ms_newton))
+    assert r0.newton_failed == 0 and r1.newton_failed == 0
+    assert np.all(st1 == 0)
+    assert gap < 1e-12
+
+
+def test_group_mode_at_default_tolerance():
+    """At the reference's 1e-6 the group iteration's links are within 1e-6 of
+    the reference iteration's, and the event's E_T and eps2 within 1e-6; on
+    512^2 Pb+Pb it takes at most half the Newton time."""
+    m0, r0, it0, st0, e0 = _links(512, 40.0, "Pb", 6.0, 0, 0.0)
+    m1, r1, it1, st1, e1 = _links(512, 40.0, "Pb", 6.0, 1, 0.0)
+    gap = max(np.abs(a - b).max() for a, b in zip(m0[:2], m1[:2]))
+    print("NEWTON 512: gap %.2e, ms mirror %.3f group %.3f, E_T rel %.2e, eps2 rel %.2e, "
+          "fallbacks %d" % (gap, r0.ms_newton, r1.ms_newton, abs(e1.E_T / e0.E_T - 1),
+                            abs(e1.eccentricity[1] / e0.eccentricity[1] - 1),
+                            int((it1 > 30).sum())))
+    assert gap < 1e-6
+    assert abs(e1.E_T / e0.E_T - 1) < 1e-6
+    assert abs(e1.eccentricity[1] / e0.eccentricity[1] - 1) < 1e-6
+    assert r1.ms_newton < 0.5 * r0.ms_newton
+
+
+def test_group_mode_refuses_input_gradients():
+    from ipglasma_b200.synthetic import make_event
+
+    N, L = 64, 16.0
+    A, B, _, _ = make_event(N, L, "Au", 2.0, seed=3)
+    with ipg.Event(ipg.Config(size=N, L=L, Ny=4, maxtime=0.2, seed=1, newton_mode=1,
+                              newton_tolerance=1e-12)) as ev:
+        ev.set_g2mu(A, B)
+        ev.use_device_noise()
+        ev.init_fields()
+        ev.forward(1)
+        with pytest.raises(ipg.IPGError) as err:
+            ev.backward(1.0, 1.0, inputs=True)
+        assert err.value.status == 5
