@@ -171,11 +171,23 @@ def make_inputs():
     return A, B
 
 
+def newton_kw(precision: int) -> dict:
+    """tau = 0 Newton solve per form: the FP32 bulk form uses Newton on the
+    group (exact Jacobian, sum |F_a| < 1e-10), the plain FP64 form the
+    reference's own iteration (numeric Jacobian, 1e-6), bit for bit."""
+    return {"newton_mode": 1, "newton_tolerance": 1e-10} if precision == 1 else {}
+
+
+NEWTON_NOTE = {"fp32": "Newton on the group, exact Jacobian, to sum|F_a| < 1e-10",
+               "fp64": "the reference's iteration (numeric Jacobian, 1e-6), bit for bit"}
+
+
 def cfg_for(precision: int, seed: int):
     import ipglasma_b200 as ipg
     w = WORKLOAD
     return ipg.Config(size=w["N"], L=w["L"], Ny=w["Ny"], g=w["g"], m=w["m"],
-                      maxtime=w["maxtime"], precision=precision, seed=seed)
+                      maxtime=w["maxtime"], precision=precision, seed=seed,
+                      **newton_kw(precision))
 
 
 def flush_l2(torch, buf):
@@ -346,7 +358,8 @@ def build_batch(ipg, w: dict, specs: list[dict], precision: int, seed_base: int)
         A, B, _, _ = make_event(e["N"], e["L"], e["nucleus"], e["b"], e["seed"], g=w["g"])
         ev = ipg.Event(ipg.Config(size=e["N"], L=e["L"], Ny=w["Ny"], g=w["g"], m=w["m"],
                                   maxtime=w["maxtime"], dtau=w.get("dtau", 0.0),
-                                  precision=precision, seed=seed_base + k))
+                                  precision=precision, seed=seed_base + k,
+                                  **newton_kw(precision)))
         ev.set_g2mu(A, B)
         ev.use_device_noise()
         evs.append(ev)
@@ -566,7 +579,8 @@ def workload_config(w: dict, world: int) -> dict:
             "dtau": (f"{w['dtau']} a" if w.get("dtau") else "derived (main.cpp:531-534)"),
             "l2": "no flush: a step's state (over 1 GB) is larger than the 126 MB L2",
             "parallelism": f"events LPT-sharded (cost N^2 x steps) over {world} GPU(s), "
-                           "no collective"}
+                           "no collective",
+            "newton": NEWTON_NOTE}
 
 
 def run_ours(args, world, rank, local):
