@@ -400,6 +400,25 @@ def launches_of(evs, batch) -> int:
     return sum(ev.kernel_launches() for ev in evs) + batch.stats()[2]
 
 
+def cell_errors(eps32, eps64) -> dict:
+    """Relative error of e per cell over the cells above 1% and 0.1% of the
+    maximum: max and rms, and for 0.1% also the 99.9th percentile and the
+    number of cells off by more than 10%. The Landau matching is not
+    continuous: a cell whose time-like eigenvector is not found takes a
+    neighbour's values (MyEigen.cpp:137-216), so a single cell near that
+    branch can differ by O(1) between two forms and set the max alone."""
+    out = {}
+    for frac in (1e-2, 1e-3):
+        m = eps64 > frac * eps64.max()
+        rel = np.abs(eps32[m] - eps64[m]) / np.abs(eps64[m])
+        out[f"e_rel_max_gt{frac:g}max"] = float(rel.max())
+        out[f"e_rel_rms_gt{frac:g}max"] = float(np.sqrt(np.mean(rel ** 2)))
+        if frac == 1e-3:
+            out["e_rel_p999_gt0.001max"] = float(np.percentile(rel, 99.9))
+            out["cells_rel_gt0.1_gt0.001max"] = int((rel > 0.1).sum())
+    return out
+
+
 def batch_errors(evs32, evs64, specs, r32, r64) -> dict:
     """FP32 bulk against FP64 on every event of a batch (same noise keys, so
     the same FP64 initial conditions): per size class the median and the
@@ -410,11 +429,7 @@ def batch_errors(evs32, evs64, specs, r32, r64) -> dict:
     for e32, e64, spec, a, b in zip(evs32, evs64, specs, r32, r64):
         eps32, eps64 = e32.observables()[0], e64.observables()[0]
         row = {"cls": f"{spec['nucleus']}{spec['N']}", "b": spec["b"]}
-        for frac in (1e-2, 1e-3):
-            m = eps64 > frac * eps64.max()
-            rel = np.abs(eps32[m] - eps64[m]) / np.abs(eps64[m])
-            row[f"e_rel_max_gt{frac:g}max"] = float(rel.max())
-            row[f"e_rel_rms_gt{frac:g}max"] = float(np.sqrt(np.mean(rel ** 2)))
+        row.update(cell_errors(eps32, eps64))
         row["eps2_rel"] = abs(a.eccentricity[1] - b.eccentricity[1]) / abs(b.eccentricity[1])
         row["eps2_abs"] = abs(a.eccentricity[1] - b.eccentricity[1])
         row["E_T_rel"] = abs(a.E_T - b.E_T) / abs(b.E_T)
@@ -422,7 +437,8 @@ def batch_errors(evs32, evs64, specs, r32, r64) -> dict:
         row["unitarity_fp32"], row["unitarity_fp64"] = a.unitarity_max, b.unitarity_max
         per.append(row)
     keys = ["e_rel_rms_gt0.01max", "e_rel_max_gt0.01max", "e_rel_rms_gt0.001max",
-            "e_rel_max_gt0.001max", "eps2_rel", "eps2_abs", "E_T_rel"]
+            "e_rel_max_gt0.001max", "e_rel_p999_gt0.001max", "cells_rel_gt0.1_gt0.001max",
+            "eps2_rel", "eps2_abs", "E_T_rel"]
     out = {}
     for cls in sorted({r["cls"] for r in per}):
         rows = [r for r in per if r["cls"] == cls]
@@ -954,12 +970,7 @@ def compare_forms(ev32, ev64, d_A, d_B, seed):
         outs[name] = (eps, res)
     e32, r32 = outs["fp32"]
     e64, r64 = outs["fp64"]
-    out = {}
-    for frac in (1e-2, 1e-3):
-        m = e64 > frac * e64.max()
-        rel = np.abs(e32[m] - e64[m]) / np.abs(e64[m])
-        out[f"e_rel_max_gt{frac:g}max"] = float(rel.max())
-        out[f"e_rel_rms_gt{frac:g}max"] = float(np.sqrt(np.mean(rel ** 2)))
+    out = cell_errors(e32, e64)
     out["eps2_rel"] = abs(r32.eccentricity[1] - r64.eccentricity[1]) / abs(r64.eccentricity[1])
     out["E_T_rel"] = abs(r32.E_T - r64.E_T) / abs(r64.E_T)
     out["gauss_fp32"] = r32.gauss_violation
