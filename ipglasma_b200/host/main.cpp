@@ -353,6 +353,7 @@ int main(int argc, char **argv) {
     cfg.dtau = in.d_or("dtauOverride", 0.0);  // the reference derives dtau
     cfg.precision = in.d_or("precisionFP32", 0.0) > 0 ? IPG_FP32 : IPG_FP64;
     cfg.device = (int)in.d_or("device", 0.0);
+    cfg.newton_mode = (int)in.d_or("newtonMode", 0.0);  // 1: Newton on the group
     const int writeOutputs = in.i("writeOutputs");
     const int sizeOutput = in.i("sizeOutput");
     const double LOutput = in.d("LOutput");
