@@ -239,7 +239,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true",
                     help="skip the adjoint (forward/backward) measurement")
     ap.add_argument("--profile", choices=["fp32", "fp64", "both", "adjoint", "batch32",
-                                          "batch64"], default=None,
+                                          "batch64", "gaugefix"], default=None,
                     help="run one warm-up and one timed event per form and exit "
                          "(the command profiled under ncu)")
     ap.add_argument("--profile-n", type=int, default=512,
@@ -274,6 +274,21 @@ def run_profile(which, local):
         b.close()
         for ev in evs:
             ev.close()
+        return
+    if which == "gaugefix":
+        # Coulomb gauge fixing of a Pb+Pb 512^2 event (L 40 fm, Ny 10) after 20
+        # leapfrog steps, then the gluon spectrum
+        from ipglasma_b200.synthetic import make_event
+        A, B, _, _ = make_event(512, 40.0, "Pb", 6.0, seed=5)
+        with ipg.Event(ipg.Config(size=512, L=40.0, Ny=10, maxtime=1.0, seed=4)) as ev:
+            ev.set_g2mu(A, B)
+            ev.use_device_noise()
+            ev.init_fields()
+            ev.evolve(20)
+            rep = ev.gauge_fix(4000)
+            m = ev.multiplicity()
+        print(f"gauge fixing: {rep['iterations']} iterations in {rep['ms']:.3f} ms, "
+              f"dN/dy {m['dNdy']:.6g}")
         return
     if which == "adjoint":
         # the adjoint workload's event (Au+Au 256^2, Ny 50) over 40 steps, every
