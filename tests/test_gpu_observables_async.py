@@ -44,3 +44,25 @@ def test_async_copies_overlap_the_next_event(prec):
             assert np.array_equal(g, w)
     assert not np.array_equal(first[0], second[0])
     ev.close()
+
+
+def test_forward_waits_for_pending_observable_copies():
+    """ipg_forward rewrites T^{mu nu} on the device: a copy of the previous
+    event's observables still running must finish first, so the host arrays
+    hold that event's values and not the adjoint forward's."""
+    N, L = 128, 20.0
+    A, B, _, _ = make_event(N, L, "Pb", 6.0, 31)
+    cfg = ipg.Config(size=N, L=L, Ny=10, maxtime=0.3, seed=1, newton_tolerance=1e-12)
+    with ipg.Event(cfg) as ev:
+        run(ev, A, B, 303)
+        want = ev.observables()
+        got = buffers(ev.n)
+        run(ev, A, B, 303)
+        ev.observables_async(*got)
+        ev.reseed(404)
+        ev.use_device_noise()
+        ev.init_fields(allow_nonconverged=True)
+        ev.forward(1)
+        ev.wait_observables()
+        for g, w in zip(got, want):
+            assert np.array_equal(g, w)
