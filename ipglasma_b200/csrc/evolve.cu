@@ -591,38 +591,8 @@ __global__ void __launch_bounds__(128)
     }
 }
 
-// ===========================================================================
-// Direction-split leapfrog: two threads per site, thread d (0 = x, 1 = y)
-// owns the link U_d and the field E_d. The update of E_d, U_d and the share
-// of the pi bracket that comes from the +-d neighbours are symmetric under
-// x <-> y once written with the plaquette in the (d, o) orientation:
-//   P_do  = U_d U_o(x+d) U_d(x+o)^dag U_o^dag        (for d = x this is U12,
-//           for d = y it is U12^dag, so AH(P_do) = +-h12 as in evolveE)
-//   S_d   = (U_d U_o(x+d-o)^dag)(U_d(x-o)^dag U_o(x-o))   (U1m2 / U2m1)
-//   E_d  += tau dtau/(2 g^2) TL(AH(P_do) + AH(S_d)) + dtau/tau i[D_+d, phi]
-//   br_d  = D_+d + D_-d,  D_+d = U_d phi(x+d) U_d^dag - phi,
-//                         D_-d = U_d(x-d)^dag phi(x-d) U_d(x-d) - phi
-//   pi   += dtau/tau (br_x + br_y)           (br exchanged with a shuffle)
-// Each thread thus holds one direction's matrices, half the live state of a
-// one-thread-per-site kernel, which doubles the resident warps. DEV selects
-// the FP32 deviation storage W = U - 1 (products (1+a)(1+b) - 1 = a + b + ab,
-// reunitarised every step); otherwise links are full matrices (FP64 plain).
-// ===========================================================================
-template <typename T, bool DEV>
-__device__ __forceinline__ M3<T> lmul(const M3<T> &a, const M3<T> &b) {
-    if constexpr (DEV) return dmul(a, b);
-    else return mul(a, b);
-}
-template <typename T, bool DEV>
-__device__ __forceinline__ M3<T> lmul_nd(const M3<T> &a, const M3<T> &b) {
-    if constexpr (DEV) return dmul_nd(a, b);
-    else return mul_nd(a, b);
-}
-template <typename T, bool DEV>
-__device__ __forceinline__ M3<T> lmul_dn(const M3<T> &a, const M3<T> &b) {
-    if constexpr (DEV) return dmul_dn(a, b);
-    else return mul_dn(a, b);
-}
+// Parallel transport of phi from a neighbour, minus phi itself, for a link
+// in deviation storage (DEV: U = 1 + w, the FP32 bulk form) or full storage.
 // U phi_nb U^dag - phi
 template <typename T, bool DEV>
 __device__ __forceinline__ H3<T> transport_fwd_minus(const M3<T> &u, const H3<T> &nb,
