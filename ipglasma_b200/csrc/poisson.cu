@@ -12,8 +12,8 @@
 // and even, so the two results separate into the real and imaginary parts of
 // the inverse transform.
 //
-// Kernels per batch of sheets (the work buffer of a batch is sized to stay in
-// the 126 MB L2):
+// Kernels per batch of sheets (a work buffer of up to 128 MB per batch: large
+// batches give each launch more parallelism):
 //   k_rows_fwd  rho = g sqrt(g2mu2/Ny) xi (read, or Philox in-kernel), row FFTs
 //   k_cols      column FFT, Green multiply, inverse column FFT
 //   k_rows_inv  inverse row FFTs, 1/N^2
