@@ -348,6 +348,7 @@ class Event:
     def __init__(self, cfg: Config):
         self.cfg = cfg
         self._lib = lib()
+        self._pending_obs = None
         h = ct.c_void_p()
         c = cfg.to_c()
         st = self._lib.ipg_create(ct.byref(c), ct.byref(h))
@@ -558,7 +559,11 @@ class Event:
                 raise ValueError(f"observable buffer needs {size} contiguous float64")
         self._check(self._lib.ipg_get_observables_async(
             self._h, *(_ptr(a) if a is not None else None for a in bufs)))
-        self._pending_obs = bufs
+        # copies queue up on the context's copy stream: every pending set of
+        # arrays stays referenced until wait_observables
+        if self._pending_obs is None:
+            self._pending_obs = []
+        self._pending_obs.append(bufs)
 
     def wait_observables(self) -> None:
         self._check(self._lib.ipg_wait_observables(self._h))
