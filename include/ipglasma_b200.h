@@ -322,6 +322,27 @@ ipg_status ipg_output_names(int event_id, int it, double dtau, double a,
                             char *hydro, size_t hydro_len, char *tmunu,
                             size_t tmunu_len);
 
+/* The remaining figures of the eccentricities<id>.dat line that
+ * Evolution::eccentricity writes (Evolution.cpp:1280-1810, cutoff 0) for the
+ * observables of the last ipg_run: sqrt(<r^2>) (the r^2 moment over
+ * [2, N-2)^2 divided by the weight of all cells), the outermost cells with
+ * weight on the centroid's row and column, the area and mean e of the cells
+ * with e >= 0, Rbar = 1/sqrt(1/<x^2> + 1/<y^2>), and the mean of
+ * Q_sA^2 Q_sB^2 over the same cells times hbarc (QsmuRatio, QsmuRatioB: the
+ * ratios the g2mu maps were made with). The eccentricities and angles are in
+ * ipg_result. */
+typedef struct {
+    double tau;            /* fm */
+    double r_rms;          /* fm */
+    double max_x, max_y;   /* fm, from the centroid; 0 when no cell has weight */
+    double area;           /* fm^2 */
+    double Rbar;           /* fm */
+    double avg_eps;        /* GeV/fm^3 */
+    double avg_qs2a_qs2b;  /* as printed by the reference (times hbarc) */
+} ipg_ecc_report;
+ipg_status ipg_eccentricity_report(ipg_ctx *ctx, double QsmuRatio, double QsmuRatioB,
+                                   ipg_ecc_report *out);
+
 /* ---- gauge fixing and gluon multiplicity ---------------------------------
  * GaugeFix::FFTChi (GaugeFix.cpp:17-165) and Evolution::multiplicity
  * (Evolution.cpp:2284-3188), which the reference runs at it = 1 and

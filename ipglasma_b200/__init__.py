@@ -108,6 +108,11 @@ class _Result(ct.Structure):
     ]
 
 
+class _EccReport(ct.Structure):
+    _fields_ = [(f, ct.c_double) for f in ("tau", "r_rms", "max_x", "max_y", "area", "Rbar",
+                                          "avg_eps", "avg_qs2a_qs2b")]
+
+
 class _GaugeReport(ct.Structure):
     _fields_ = [
         ("iterations", ct.c_int), ("residual_checks", ct.c_int), ("nan_sites", ct.c_int),
@@ -206,6 +211,8 @@ _SIGNATURES = {
     "ipg_run": (ct.c_int, [ct.c_void_p, ct.POINTER(_Result)]),
     "ipg_evolve": (ct.c_int, [ct.c_void_p, ct.c_int]),
     "ipg_gauge_fix": (ct.c_int, [ct.c_void_p, ct.c_int, ct.POINTER(_GaugeReport)]),
+    "ipg_eccentricity_report": (ct.c_int, [ct.c_void_p, ct.c_double, ct.c_double,
+                                           ct.POINTER(_EccReport)]),
     "ipg_multiplicity": (ct.c_int, [ct.c_void_p, ct.POINTER(_MultParams),
                                     ct.POINTER(_MultResult)]),
     "ipg_run_multiplicity": (ct.c_int, [ct.c_void_p, ct.POINTER(_MultParams),
@@ -499,6 +506,15 @@ class Event:
 
     def evolve(self, steps: int) -> None:
         self._check(self._lib.ipg_evolve(self._h, steps))
+
+    def eccentricity_report(self, QsmuRatio=0.8, QsmuRatioB=None) -> dict:
+        """The other figures of the reference's eccentricities<id>.dat line
+        for the last run (ipg_eccentricity_report)."""
+        r = _EccReport()
+        qb = QsmuRatio if QsmuRatioB is None else QsmuRatioB
+        self._check(self._lib.ipg_eccentricity_report(self._h, float(QsmuRatio), float(qb),
+                                                      ct.byref(r)))
+        return {f: getattr(r, f) for f, _ in _EccReport._fields_}
 
     # -- gauge fixing and gluon multiplicity ----------------------------------
     def gauge_fix(self, max_iterations: int = 4000) -> dict:

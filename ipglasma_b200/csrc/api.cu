@@ -132,6 +132,8 @@ struct ipg_ctx {
         float *tbar32 = nullptr;
     } aw;
 
+    double *ecc3 = nullptr;  // [8] ipg_eccentricity_report sums (first call)
+
     // gauge fixing and multiplicity (allocated by the first call)
     struct {
         double2 *planes = nullptr;   // [16][n]: chi [4][n] and G [9][n] while gauge
@@ -796,6 +798,10 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
     const size_t n = c->n;
     IPG_TRY(dalloc(c, &c->g2mu2A, n));
     IPG_TRY(dalloc(c, &c->g2mu2B, n));
+    // an event made from Wilson lines has no g2mu maps: zero, as the
+    // reference's cells keep them
+    IPG_CUDA(c, cudaMemset(c->g2mu2A, 0, sizeof(double) * n));
+    IPG_CUDA(c, cudaMemset(c->g2mu2B, 0, sizeof(double) * n));
     IPG_TRY(dalloc(c, &c->twiddle, (size_t)N));
     IPG_TRY(dalloc(c, &c->green, n));
     IPG_TRY(dalloc(c, &c->amp, n));
@@ -1380,6 +1386,34 @@ ipg_status ipg_run(ipg_ctx *c, ipg_result *res) {
     IPG_TRY(run_evolution(c));
     IPG_TRY(observables_enqueue(c));
     return observables_finish(c, res);
+}
+
+ipg_status ipg_eccentricity_report(ipg_ctx *c, double QsmuRatio, double QsmuRatioB,
+                                   ipg_ecc_report *out) {
+    if (!c || !out) return IPG_ERR_BAD_CONFIG;
+    if (!c->finished) return fail(c, IPG_ERR_STATE, "call ipg_run first");
+    if (!c->ecc3) IPG_TRY(dalloc(c, &c->ecc3, 8));
+    const int N = c->N;
+    const double L = c->cfg.L, a = c->a;
+    IPG_TRY(wait_observable_copies(c));
+    launch_eccentricity_extras(N, L, a, c->eps, c->u4, c->g2mu2A, c->g2mu2B, c->scal + 0,
+                               c->partial, c->ecc3, c->stream);
+    IPG_LAUNCHED(c, 2);
+    double v[8];
+    IPG_CUDA(c, cudaMemcpyAsync(v, c->ecc3, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+    IPG_TRY(sync(c));
+    const double *s1 = c->h_scal, *s2 = c->h_scal + 8;  // copied by ipg_run
+    const double avx = s1[0] / s1[2], avy = s1[1] / s1[2];
+    out->tau = c->itmax * a * c->dtau;
+    out->r_rms = std::sqrt(s2[1] / v[2]);
+    out->max_x = v[6] > 0 ? -L / 2. + a * (v[6] - 1.) - avx : 0.;
+    out->max_y = v[7] > 0 ? -L / 2. + a * (v[7] - 1.) - avy : 0.;
+    out->area = v[3] * a * a;
+    out->Rbar = 1. / std::sqrt(1. / (v[0] / v[2]) + 1. / (v[1] / v[2]));
+    out->avg_eps = v[4] * kHbarc / v[3];
+    out->avg_qs2a_qs2b = v[5] * QsmuRatio * QsmuRatio * QsmuRatioB * QsmuRatioB / a / a / a / a /
+                         v[3] * kHbarc;
+    return IPG_OK;
 }
 
 ipg_status ipg_gauge_fix(ipg_ctx *c, int max_iterations, ipg_gauge_report *rep) {

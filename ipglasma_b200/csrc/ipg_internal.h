@@ -383,6 +383,14 @@ void launch_eccentricity(int N, double L, double a, const double *eps,
                          double *d_partial, double *d_sums1, double *d_sums2,
                          cudaStream_t st);
 
+// out[8] = {sum x^2 w, sum y^2 w, sum w (all cells), cells with eps >= 0,
+// their sum eps, their sum g2mu2A g2mu2B, the largest ix + 1 with w > 0 on
+// the centroid's row, the largest iy + 1 on its column} (see reduce.cu)
+void launch_eccentricity_extras(int N, double L, double a, const double *eps,
+                                const double *utau, const double *g2A, const double *g2B,
+                                const double *d_sums1, double *d_partial, double *d_out,
+                                cudaStream_t st);
+
 // out[4] = {max iterations, sum of iterations, restarted links, failed links};
 // d_partial needs 4 * ceil(links/256) doubles
 void launch_newton_stats(size_t links, const int *iters, const int *status,

@@ -210,6 +210,54 @@ __global__ void __launch_bounds__(RB) k_ecc2(int N, double L, double a, const do
     block_sum<18>(v, partial + (size_t)blockIdx.x * 18);
 }
 
+// pass 3 (Evolution.cpp:1346-1368 and 1669-1790 with cutoff 0): over all
+// cells about the all-cell centroid, sum x^2 w, y^2 w, w; over the cells
+// with eps >= 0, their count, sum eps and sum g2mu2A g2mu2B; over
+// [2, N-2)^2, the largest ix + 1 with w > 0 on the row iy = N/2 + yshift and
+// the largest iy + 1 on the column ix = N/2 + xshift (the reference keeps
+// the last such cell of its loop, Evolution.cpp:1631-1636)
+__global__ void __launch_bounds__(RB) k_ecc3(int N, double L, double a, const double *eps,
+                                             const double *utau, const double *g2A,
+                                             const double *g2B, const double *cent,
+                                             double *partial) {
+    const size_t n = (size_t)N * N;
+    double v[6] = {0., 0., 0., 0., 0., 0.};
+    double row_ix = 0., col_iy = 0.;
+    const double avx = cent[0] / cent[2], avy = cent[1] / cent[2];
+    const int xshift = (int)floor(avx / a + 0.00000000001);
+    const int yshift = (int)floor(avy / a + 0.00000000001);
+    GRID_STRIDE(pos, n) {
+        const int ix = (int)(pos / N), iy = (int)(pos % N);
+        const double x = -L / 2. + a * ix - avx, y = -L / 2. + a * iy - avy;
+        const double e = eps[pos];
+        const double w = (e < 0.) ? 0. : e * utau[pos];
+        v[0] += x * x * w;
+        v[1] += y * y * w;
+        v[2] += w;
+        if (!(e < 0.)) {
+            v[3] += 1.;
+            v[4] += e;
+            v[5] += g2A[pos] * g2B[pos];
+        }
+        if (ix >= 2 && ix < N - 2 && iy >= 2 && iy < N - 2 && w > 0.) {
+            if (iy == N / 2 + yshift) row_ix = fmax(row_ix, ix + 1.);
+            if (ix == N / 2 + xshift) col_iy = fmax(col_iy, iy + 1.);
+        }
+    }
+    block_sum<6>(v, partial + (size_t)blockIdx.x * 8);
+    block_max(row_ix, partial + (size_t)blockIdx.x * 8 + 6);
+    __syncthreads();  // block_max's shared slots are reused by the next call
+    block_max(col_iy, partial + (size_t)blockIdx.x * 8 + 7);
+}
+
+void launch_eccentricity_extras(int N, double L, double a, const double *eps,
+                                const double *utau, const double *g2A, const double *g2B,
+                                const double *d_sums1, double *d_partial, double *d_out,
+                                cudaStream_t st) {
+    k_ecc3<<<RG, RB, 0, st>>>(N, L, a, eps, utau, g2A, g2B, d_sums1, d_partial);
+    k_fold<8><<<1, 32, 0, st>>>(d_partial, d_out, (1u << 6) | (1u << 7));
+}
+
 void launch_eccentricity(int N, double L, double a, const double *eps,
                          const double *utau, const double *Ttt,
                          double *d_partial, double *d_sums1,

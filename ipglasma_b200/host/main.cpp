@@ -63,6 +63,29 @@ void print_multiplicity(const ipg_multiplicity_result &m, const ipg_multiplicity
     std::cout << " done." << std::endl;
 }
 
+// eccentricities<id>.dat, appended, at it = itmax (Evolution.cpp:1800-1810):
+// tau, epsilon_n and Psi_n for n = 1..6, the cutoff (0), sqrt(<r^2>), the
+// outermost weighted cells on the centroid's row and column, b, T_pp, the
+// area, Rbar, the mean e and the mean Q_sA^2 Q_sB^2. The reference also
+// writes a line at it = 1, from energy densities its cells do not hold at
+// that time; that line is not written here.
+void write_eccentricities(ipg_ctx *ctx, int event_id, const ipg_result &r, double b, double Tpp,
+                          double QsmuRatio) {
+    ipg_ecc_report e;
+    if (ipg_eccentricity_report(ctx, QsmuRatio, QsmuRatio, &e) != IPG_OK) {
+        std::cerr << "ipg_eccentricity_report: " << ipg_last_error(ctx) << std::endl;
+        return;
+    }
+    std::stringstream name;
+    name << "eccentricities" << event_id << ".dat";
+    std::ofstream f(name.str().c_str(), std::ios::app);
+    f << e.tau;
+    for (int k = 0; k < 6; k++) f << " " << r.eccentricity[k] << " " << r.psi[k];
+    f << " " << 0. << " " << e.r_rms << " " << e.max_x << " " << e.max_y << " " << b << " "
+      << Tpp << " " << e.area << " " << e.Rbar << " " << e.avg_eps << " " << e.avg_qs2a_qs2b
+      << std::endl;
+}
+
 // NpartdNdy-t<tau>-<id>.dat at it = itmax (Evolution.cpp:3124-3152): N_part,
 // dN/dy, T_pp, b, dE/dy, the seed, three N/A, the 3 and 6 GeV cuts and the
 // coupling ratio at the event's average Q_s
@@ -509,6 +532,7 @@ int main(int argc, char **argv) {
                 continue;
             }
             check(ctx, st, "ipg_run_multiplicity");
+            write_eccentricities(ctx, event_id, res, b, irep.Tpp, QsmuRatio);
             print_multiplicity(m2, mparams);
             write_npart_dndy(event_id, itmax, dtau, a, irep, b, seed, m2, cfg.g, muZero, cRun,
                              qsFactor);

@@ -88,10 +88,10 @@ def test_executable_reproduces_reference_output_files(ref_harness, tmp_path):
 def test_executable_gluon_multiplicity_matches_reference(ref_harness, tmp_path):
     """computeGluonMultiplicity 1: the executable gauge-fixes and measures the
     spectrum at it = 1 and it = itmax like the reference's Evolution::run,
-    prints the same dN/dy lines and writes NpartdNdy-t<tau>-0.dat; its
-    spectrum columns (dN/dy, dE/dy and the 3 and 6 GeV cuts) agree with the
-    reference's file to the six printed digits, and the hydro file (written
-    before the gauge fixing at itmax) is the reference's."""
+    prints the same dN/dy lines and writes NpartdNdy-t<tau>-0.dat and
+    eccentricities0.dat; their columns agree with the reference's files to
+    the six printed digits, and the hydro file (written before the gauge
+    fixing at itmax) is the reference's."""
     from ipglasma_b200.synthetic import gaussian_blobs
 
     if not EXE.exists():
@@ -130,6 +130,16 @@ def test_executable_gluon_multiplicity_matches_reference(ref_harness, tmp_path):
     b = numbers(ref.out / "epsilon-u-Hydro-TauHydro-0.dat")
     assert a.shape == b.shape
     assert np.all(np.abs(a - b) <= 2e-5 * np.abs(b) + 1e-12)
+    # eccentricities0.dat: the reference's it = itmax line (its it = 1 line
+    # reads energy densities its cells do not hold yet, and is not written
+    # here); every column but the last, which averages g2mu maps that an
+    # event read from Wilson-line files does not have
+    ours = [float(x) for x in (run / "eccentricities0.dat").read_text().split()]
+    lines = [l.split() for l in (ref.out / "eccentricities0.dat").read_text().splitlines()]
+    theirs = [float(x) for x in lines[1]]
+    assert len(ours) == len(theirs) == 23
+    for k in range(22):
+        assert abs(ours[k] - theirs[k]) <= 2e-5 * abs(theirs[k]) + 1e-12, (k, ours[k], theirs[k])
 
 
 def test_executable_samples_nuclei_on_its_own(tmp_path):
