@@ -584,7 +584,10 @@ def stage_rates(w, specs, evs, key0):
     class, run alone (ipg_init_report: CUDA events in the library), with
     their algorithmic bytes: the Wilson-line stage reads and writes V once
     per (site, sheet, nucleus), 2 x 18 x 8 = 288 B; Newton reads U1, U2 (36
-    doubles) and writes U (18) per link, 432 B."""
+    doubles) and writes U (18) per link, 432 B. The Wilson-line stage's FFT
+    rate uses the conventional count, 2 x 8 x 5 N^2 log2(N^2) flops per
+    (sheet, nucleus): eight colours, forward and inverse (the kernels pack
+    two real colours into one complex transform, so they execute half)."""
     out = {}
     seen = set()
     for e, ev in zip(specs, evs):
@@ -597,9 +600,11 @@ def stage_rates(w, specs, evs, key0):
         n = e["N"] ** 2
         wil = n * w["Ny"] * 2 * 288
         newt = 2 * n * 432
+        fft = 2 * 8 * 5 * n * np.log2(n) * w["Ny"] * 2
         out[f"{e['nucleus']}{e['N']}"] = {
             "ms_wilson": round(rep.ms_wilson, 3),
             "wilson_GBs_at_288B": round(wil / (rep.ms_wilson * 1e-3) / 1e9, 1),
+            "wilson_fft_TFLOPs_conventional": round(fft / (rep.ms_wilson * 1e-3) / 1e12, 2),
             "ms_newton": round(rep.ms_newton, 3),
             "newton_GBs_at_432B": round(newt / (rep.ms_newton * 1e-3) / 1e9, 1),
             "newton_mean_iterations": round(rep.newton_mean_iterations, 2),
