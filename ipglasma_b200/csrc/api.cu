@@ -658,7 +658,7 @@ ipg_status gauge_fix_run(ipg_ctx *c, int max_iter, ipg_gauge_report *rep) {
     while (launched < max_iter) {
         const int k = std::min(kChunk, max_iter - launched);
         for (int i = 0; i < k; i++) launch_gauge_fix_iteration(a, c->stream);
-        IPG_LAUNCHED(c, 7 * k);
+        IPG_LAUNCHED(c, 6 * k);
         launched += k;
         IPG_CUDA(c, cudaMemcpyAsync(h, g.ctl, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
         IPG_TRY(sync(c));

@@ -9,10 +9,11 @@
 //                   Hermitian traceless, packed into 4 complex planes
 //                   (g00 + i g11, g01, g02, g12); one partial of
 //                   sum tr(g^dag g) / Nc per block
-//   k_gf_control    one block: the residual (the partials folded in order,
-//                   divided by N^2) and the reference's stopping rules
-//                   (residual < 1e-9; residual above the value recorded at
-//                   the last multiple of 10 iterations and below 1e-6)
+//                   the block that finishes last folds the partials in
+//                   order (the residual, divided by N^2) and applies the
+//                   reference's stopping rules (residual < 1e-9; residual
+//                   above the value recorded at the last multiple of 10
+//                   iterations and below 1e-6)
 //   FFT convolution chi <- IFFT(-1.5 / (k~^2 + 1e-9) FFT(g)) with the Poisson
 //                   kernels of poisson.cu (the multiplier is real and even, so
 //                   the packed real components separate again)
@@ -24,7 +25,7 @@
 //   k_gf_transform  per site: U_i(x) <- G(x) U_i(x) G(x+i)^dag,
 //                   E_i, phi, pi <- G E_i G^dag (in place: every site writes
 //                   only its own fields and reads G from its own buffer)
-// Every kernel of an iteration returns at once when the control block has
+// Every kernel of an iteration returns at once when the residual pass has
 // set `done`, so the host enqueues iterations in chunks and reads the flag
 // once per chunk.
 //
@@ -49,8 +50,8 @@ namespace ipg {
 namespace {
 
 constexpr int GB = 256;  // threads per block of the per-site kernels
-// the exponential and the transformation need ~170 registers a thread:
-// blocks of 128 threads put three blocks (12 warps) on an SM instead of one
+// the exponential (128 registers a thread) and the transformation (168):
+// blocks of 128 threads put four and three blocks on an SM
 constexpr int GB_HEAVY = 128;
 constexpr double kHbarcGf = 0.1973269718;  // GeV fm (Phys_consts.h)
 
@@ -105,6 +106,30 @@ __host__ __device__ __forceinline__ void add_diag(M3<double> &a, double s) {
     a.m[8].r += s;
 }
 
+// A B for a product known to be Hermitian (S = 1) or anti-Hermitian
+// (S = -1): the diagonal and the upper triangle are formed, the lower
+// triangle is their (negated) conjugate and the diagonal's imaginary (real)
+// part is zero
+template <int S>
+__host__ __device__ __forceinline__ M3<double> mul_sym(const M3<double> &a, const M3<double> &b) {
+    M3<double> r;
+    const int up[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        const int i = up[q][0], j = up[q][1];
+        C<double> acc = cmul(a.m[3 * i], b.m[j]);
+        acc = cadd2(acc, cmul(a.m[3 * i + 1], b.m[3 + j]));
+        acc = cadd2(acc, cmul(a.m[3 * i + 2], b.m[6 + j]));
+        if (i == j) {
+            if (S == 1) acc.i = 0.;
+            else acc.r = 0.;
+        }
+        r.m[3 * i + j] = acc;
+        if (i != j) r.m[3 * j + i] = S == 1 ? cconj(acc) : C<double>{-acc.r, acc.i};
+    }
+    return r;
+}
+
 // exp(M) by the [6/6] Pade approximant with scaling and squaring, in the
 // steps of Matrix::expm (Matrix.cpp:431-553) for t = 1, p = 6: the
 // coefficients are the reference's 10-digit roundings of
@@ -143,25 +168,24 @@ __host__ __device__ M3<double> expm_pade6(const M3<double> &M) {
     } else {
         U = M;
     }
-    const M3<double> H2 = mul(U, U);
+    // U is anti-Hermitian (a multiple of i chi), so H2 = U^2 and every
+    // polynomial in H2 are Hermitian, and P U is anti-Hermitian: those
+    // products form only the diagonal and the upper triangle
+    const M3<double> H2 = mul_sym<1>(U, U);
     // Horner in H2: Q from c6, c4, c2, c0 and P from c5, c3, c1 (the loop of
-    // Matrix.cpp:492-505 unrolled for p = 6), then P <- P U
-    M3<double> Q, P;
-    set_identity(Q);
-    Q = mscale(Q, c[6]);
-    set_identity(P);
-    P = mscale(P, c[5]);
-    Q = mul(Q, H2);
+    // Matrix.cpp:492-505 unrolled for p = 6; its first products are with
+    // multiples of the identity, c I H2 = c H2 exactly), then P <- P U
+    M3<double> Q = mscale(H2, c[6]);
     add_diag(Q, c[4]);
-    P = mul(P, H2);
+    M3<double> P = mscale(H2, c[5]);
     add_diag(P, c[3]);
-    Q = mul(Q, H2);
+    Q = mul_sym<1>(Q, H2);
     add_diag(Q, c[2]);
-    P = mul(P, H2);
+    P = mul_sym<1>(P, H2);
     add_diag(P, c[1]);
-    Q = mul(Q, H2);
+    Q = mul_sym<1>(Q, H2);
     add_diag(Q, c[0]);
-    P = mul(P, U);
+    P = mul_sym<-1>(P, U);
     sub_from(Q, P);
     // inverse of Q by cofactors (Matrix.cpp:523-541)
     const C<double> *q = Q.m;
@@ -234,8 +258,24 @@ __host__ __device__ M3<double> reunitarize(const M3<double> &u) {
 // gauge fixing
 // -------------------------------------------------------------------------
 
+// the reference's stopping rules on the residual of iteration ctl->iter
+__device__ __forceinline__ void gf_decide(double res, GaugeFixCtl *ctl) {
+    const int it = ctl->iter;
+    if (it % 10 == 0) {
+        ctl->prev = res;
+        if (it / 10 < kGaugeHistory) ctl->hist[it / 10] = res;
+    }
+    ctl->last = res;
+    ctl->checks = it + 1;
+    if (res < 1e-9 || (res > ctl->prev && res < 1e-6)) {
+        ctl->done = 1;  // no transform in this iteration
+    } else {
+        ctl->iter = it + 1;
+    }
+}
+
 __global__ void __launch_bounds__(GB) k_gf_chi(State<double> s, int N, double2 *chi,
-                                               double *partial, const GaugeFixCtl *ctl) {
+                                               double *partial, GaugeFixCtl *ctl) {
     if (ctl->done) return;
     const size_t n = (size_t)N * N;
     double acc = 0.;
@@ -268,28 +308,24 @@ __global__ void __launch_bounds__(GB) k_gf_chi(State<double> s, int N, double2 *
                3.;
     }
     const double b = block_sum1(acc);
-    if (threadIdx.x == 0) partial[blockIdx.x] = b;
-}
-
-__global__ void __launch_bounds__(GB) k_gf_control(const double *partial, int blocks, int N,
-                                                   GaugeFixCtl *ctl) {
-    if (ctl->done) return;
-    double v = 0.;
-    for (int b = threadIdx.x; b < blocks; b += GB) v += partial[b];
-    const double sum = block_sum1(v);
-    if (threadIdx.x != 0) return;
-    const double res = sum / (double)(N * N);
-    const int it = ctl->iter;
-    if (it % 10 == 0) {
-        ctl->prev = res;
-        if (it / 10 < kGaugeHistory) ctl->hist[it / 10] = res;
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = b;
+        __threadfence();  // the partial is visible before the arrival counts
+        last = atomicAdd(&ctl->arrived, 1u) == gridDim.x - 1;
     }
-    ctl->last = res;
-    ctl->checks = it + 1;
-    if (res < 1e-9 || (res > ctl->prev && res < 1e-6)) {
-        ctl->done = 1;  // no transform in this iteration
-    } else {
-        ctl->iter = it + 1;
+    __syncthreads();
+    if (!last) return;
+    // the last block: every partial is written; fold them in block order
+    __threadfence();
+    double v = 0.;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += GB)
+        v += *reinterpret_cast<volatile const double *>(partial + k);
+    __syncthreads();  // block_sum1's shared slots are reused
+    const double sum = block_sum1(v);
+    if (threadIdx.x == 0) {
+        ctl->arrived = 0;
+        gf_decide(sum / (double)(N * N), ctl);
     }
 }
 
@@ -365,7 +401,6 @@ void launch_gauge_fix_iteration(const GaugeFixArgs &a, cudaStream_t st) {
     const int blocks = gauge_fix_blocks(a.N);
     const unsigned heavy = (unsigned)((n + GB_HEAVY - 1) / GB_HEAVY);
     k_gf_chi<<<blocks, GB, 0, st>>>(a.s, a.N, a.chi, a.partial, a.ctl);
-    k_gf_control<<<1, GB, 0, st>>>(a.partial, blocks, a.N, a.ctl);
     launch_poisson_sheets(a.fft, 1, st);  // chi -> chi in place, skipped when done
     k_gf_exp<<<heavy, GB_HEAVY, 0, st>>>(a.chi, a.N, a.G, a.ctl);
     k_gf_transform<<<heavy, GB_HEAVY, 0, st>>>(a.s, a.G, a.N, a.ctl);

@@ -162,12 +162,13 @@ constexpr int kKtBins = 100;        // k_T bins of Evolution::multiplicity
 constexpr int kMultRow = 2 + 3 * kKtBins;  // dN, dE, n[100], E[100], count[100]
 
 // device state of one gauge fixing (the host sets done = iter = nan_sites =
-// 0, prev = 10000 and hist = NaN before the first iteration)
+// arrived = 0, prev = 10000 and hist = NaN before the first iteration)
 struct GaugeFixCtl {
     int done;       // a stopping rule fired: later iterations do nothing
     int iter;       // gauge transformations applied
     int checks;     // residuals computed
     int nan_sites;  // sites whose transformation was NaN and was reset to 1
+    unsigned arrived;  // blocks of the residual pass done (the last one decides)
     double prev;    // residual at the last multiple of 10 iterations
     double last;    // the latest residual
     double hist[kGaugeHistory];
