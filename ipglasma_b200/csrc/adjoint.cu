@@ -334,20 +334,23 @@ __global__ void k_inv_su(int N, State<T> nxt, State<T> cur, T c, T c2) {
 
 // S_u: reads the adjoints of the step's outputs, leaves the adjoints of its
 // inputs (U before the update, phi before, pi' and E' after S_e). `cur` holds
-// U, phi of the step's input, `nxt` E' of its output.
+// U, phi of the step's input, `nxt` E' of its output. One thread per site and
+// link direction (blockIdx.y): twice the warps of one thread per site, at
+// three blocks an SM.
 template <typename T>
-__global__ void k_adj_su(int N, State<T> cur, State<T> nxt, AdjStateT<T> a, T c,
+__global__ void __launch_bounds__(128, 3) k_adj_su(int N, State<T> cur, State<T> nxt, AdjStateT<T> a, T c,
                          T c2) {
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
-    // pi_bar += c2 phi_bar (phi_bar itself passes through unchanged)
-    {
+    const int d = blockIdx.y;  // the link direction of this thread
+    if (d == 0) {
+        // pi_bar += c2 phi_bar (phi_bar itself passes through unchanged)
         H3<T> pib = ld_h9a(a.pi, pos, n);
         h_axpy(pib, c2, ld_h9a(a.phi, pos, n));
         st_h9a(a.pi, pos, n, pib);
     }
-    for (int d = 0; d < 2; d++) {
+    {
         C<T> *Ub = d ? a.uy : a.ux;
         C<T> *Eb = d ? a.e2 : a.e1;
         const M3<T> Ubar = ld_adj(Ub, pos, n);
@@ -371,25 +374,26 @@ __global__ void k_adj_su(int N, State<T> cur, State<T> nxt, AdjStateT<T> a, T c,
 // The time reversal of S_u fused with its adjoint, for steps reached by
 // reversal: U_d = M_d^{-1} U_d' with M_d = T2(i c E_d'), phi = phi' - c2 pi'
 // are written to `cur` (as k_inv_su), then the adjoint of S_u runs with that
-// M_d and U_d (as k_adj_su, which would recompute M_d and reload U_d).
+// M_d and U_d (as k_adj_su, which would recompute M_d and reload U_d). One
+// thread per site and link direction, as k_adj_su; phi goes with direction 1.
 template <typename T>
-__global__ void k_inv_adj_su(int N, State<T> nxt, State<T> cur, AdjStateT<T> a, T c,
+__global__ void __launch_bounds__(128, 3) k_inv_adj_su(int N, State<T> nxt, State<T> cur, AdjStateT<T> a, T c,
                              T c2) {
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
-    {
+    const int d = blockIdx.y;  // the link direction of this thread
+    if (d == 1) {
         H3<T> phi = ld_h(nxt.phi, pos, n);
         h_axpy(phi, -c2, ld_h(nxt.pi, pos, n));
         st_h(cur.phi, pos, n, phi);
-    }
-    // pi_bar += c2 phi_bar (phi_bar itself passes through unchanged)
-    {
+    } else {
+        // pi_bar += c2 phi_bar (phi_bar itself passes through unchanged)
         H3<T> pib = ld_h9a(a.pi, pos, n);
         h_axpy(pib, c2, ld_h9a(a.phi, pos, n));
         st_h9a(a.pi, pos, n, pib);
     }
-    for (int d = 0; d < 2; d++) {
+    {
         C<T> *Ub = d ? a.uy : a.ux;
         C<T> *Eb = d ? a.e2 : a.e1;
         const M3<T> X = times_i(ld_herm8(d ? nxt.e2 : nxt.e1, pos, n), c);
@@ -1004,25 +1008,16 @@ struct AdjCoef {
 template <typename T>
 void launch_inverse_adjoint_step(int N, const State<T> &nxt, const State<T> &cur,
                                  const AdjStateT<T> &a, const StepCoef<double> &cf,
-                                 cudaStream_t st, cudaStream_t st2, cudaEvent_t fork,
-                                 cudaEvent_t join) {
+                                 cudaStream_t st) {
     const size_t n = (size_t)N * N;
     const AdjCoef<T> k(cf);
-    k_inv_adj_su<<<blocks(n), 128, 0, st>>>(N, nxt, cur, a, k.c, k.c2);
-    if (!st2) {
-        launch_inverse_se<T>(N, nxt, cur, cf, st);
-        if (cf.do_pe) k_adj_se<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, k.cst, k.cdt);
-        return;
-    }
-    // E and pi of the recovered state (written to cur.e1, e2, pi) and the S_e
-    // adjoint (reads cur's links and phi, writes only the adjoint buffers)
-    // touch disjoint data: they run side by side, joined before the next step
-    cudaEventRecord(fork, st);
-    cudaStreamWaitEvent(st2, fork, 0);
-    launch_inverse_se<T>(N, nxt, cur, cf, st2);
+    k_inv_adj_su<<<dim3(blocks(n), 2), 128, 0, st>>>(N, nxt, cur, a, k.c, k.c2);
+    // E and pi of the recovered state (written to cur.e1, e2, pi, which the
+    // S_e adjoint does not read). Fusing this into k_adj_se's three roles, or
+    // running it beside k_adj_se on a second stream, was not faster: both
+    // kernels are held to two or three blocks an SM by their registers.
+    launch_inverse_se<T>(N, nxt, cur, cf, st);
     if (cf.do_pe) k_adj_se<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, k.cst, k.cdt);
-    cudaEventRecord(join, st2);
-    cudaStreamWaitEvent(st, join, 0);
 }
 
 template <typename T>
@@ -1030,7 +1025,7 @@ void launch_adjoint_step(int N, const State<T> &cur, const State<T> &nxt, const 
                          const StepCoef<double> &cf, cudaStream_t st) {
     const size_t n = (size_t)N * N;
     const AdjCoef<T> k(cf);
-    k_adj_su<<<blocks(n), 128, 0, st>>>(N, cur, nxt, a, k.c, k.c2);
+    k_adj_su<<<dim3(blocks(n), 2), 128, 0, st>>>(N, cur, nxt, a, k.c, k.c2);
     if (cf.do_pe) k_adj_se<<<dim3(blocks(n), 3), 128, 0, st>>>(N, cur, a, k.cst, k.cdt);
 }
 
@@ -1048,8 +1043,7 @@ void launch_adjoint_project(size_t n, const AdjStateT<T> &a, cudaStream_t st) {
 
 template void launch_inverse_adjoint_step<double>(int, const State<double> &,
                                                   const State<double> &, const AdjState &,
-                                                  const StepCoef<double> &, cudaStream_t,
-                                                  cudaStream_t, cudaEvent_t, cudaEvent_t);
+                                                  const StepCoef<double> &, cudaStream_t);
 template void launch_adjoint_step<double>(int, const State<double> &, const State<double> &,
                                           const AdjState &, const StepCoef<double> &,
                                           cudaStream_t);

@@ -40,8 +40,7 @@ struct ipg_ctx {
     // the other of two work buffers (work, work2)
     cudaStream_t stream_v = nullptr;
     cudaEvent_t ev_fft[2] = {nullptr, nullptr}, ev_prod[2] = {nullptr, nullptr};
-    // the reverse sweep's time reversal forks onto stream_v and joins back
-    cudaEvent_t ev_adj_fork = nullptr, ev_adj_join = nullptr;
+    cudaEvent_t ev_nuc_fork = nullptr, ev_nuc_join = nullptr;  // input adjoint, two nuclei
     // ipg_get_observables_async: the copies run on stream_copy after
     // ev_obs_ready; the next observables stage waits for ev_obs_copied
     cudaStream_t stream_copy = nullptr;
@@ -117,7 +116,8 @@ struct ipg_ctx {
         bool from_inputs = false;  // the tau = 0 state came from g2mu + noise
         // initial-condition adjoint: U1/U2 adjoints, V adjoints, a V copy
         C<double> *b1x = nullptr, *b2x = nullptr, *b1y = nullptr, *b2y = nullptr;
-        C<double> *vbA = nullptr, *vbB = nullptr, *vcur = nullptr;
+        C<double> *vbA = nullptr, *vbB = nullptr, *vcur = nullptr, *vcur2 = nullptr;
+        double *amp2 = nullptr;  // nucleus B's rho amplitude in the input adjoint
         double *g2mu_bar = nullptr;
         double *rho_all = nullptr;  // [2][Ny][n][8] rho adjoint, kept on the device
         // FP32 adjoint (contexts of the FP32 form): the bulk form's own states
@@ -782,6 +782,8 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
     IPG_CUDA(c, cudaSetDevice(cfg->device));
     IPG_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     IPG_CUDA(c, cudaStreamCreateWithFlags(&c->stream_v, cudaStreamNonBlocking));
+    IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_nuc_fork, cudaEventDisableTiming));
+    IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_nuc_join, cudaEventDisableTiming));
     IPG_CUDA(c, cudaStreamCreateWithFlags(&c->stream_copy, cudaStreamNonBlocking));
     IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_obs_ready, cudaEventDisableTiming));
     IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_obs_copied, cudaEventDisableTiming));
@@ -789,8 +791,6 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
         IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_fft[i], cudaEventDisableTiming));
         IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_prod[i], cudaEventDisableTiming));
     }
-    IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_adj_fork, cudaEventDisableTiming));
-    IPG_CUDA(c, cudaEventCreateWithFlags(&c->ev_adj_join, cudaEventDisableTiming));
     IPG_CUDA(c, cudaEventCreate(&c->ev0));
     IPG_CUDA(c, cudaEventCreate(&c->ev1));
     for (cudaEvent_t &x : c->ie) IPG_CUDA(c, cudaEventCreate(&x));
@@ -893,6 +893,8 @@ ipg_status ipg_destroy(ipg_ctx *ctx) {
     }
     if (ctx->ev_obs_ready) cudaEventDestroy(ctx->ev_obs_ready);
     if (ctx->ev_obs_copied) cudaEventDestroy(ctx->ev_obs_copied);
+    if (ctx->ev_nuc_fork) cudaEventDestroy(ctx->ev_nuc_fork);
+    if (ctx->ev_nuc_join) cudaEventDestroy(ctx->ev_nuc_join);
     if (ctx->stream_v) {
         cudaStreamSynchronize(ctx->stream_v);
         cudaStreamDestroy(ctx->stream_v);
@@ -901,8 +903,6 @@ ipg_status ipg_destroy(ipg_ctx *ctx) {
         if (ctx->ev_fft[i]) cudaEventDestroy(ctx->ev_fft[i]);
         if (ctx->ev_prod[i]) cudaEventDestroy(ctx->ev_prod[i]);
     }
-    if (ctx->ev_adj_fork) cudaEventDestroy(ctx->ev_adj_fork);
-    if (ctx->ev_adj_join) cudaEventDestroy(ctx->ev_adj_join);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return IPG_OK;
@@ -1786,9 +1786,10 @@ ipg_status backward_inputs(ipg_ctx *c, double *grad_g2mu, double *grad_rho) {
     const size_t n = c->n;
     const int N = c->N, Ny = c->cfg.Ny;
     if (!A.b1x) {
-        for (C<double> **p : {&A.b1x, &A.b2x, &A.b1y, &A.b2y, &A.vbA, &A.vbB, &A.vcur})
+        for (C<double> **p : {&A.b1x, &A.b2x, &A.b1y, &A.b2y, &A.vbA, &A.vbB, &A.vcur, &A.vcur2})
             IPG_TRY(dalloc(c, p, 9 * n));
         IPG_TRY(dalloc(c, &A.g2mu_bar, 2 * n));
+        IPG_TRY(dalloc(c, &A.amp2, n));
     }
     if (grad_rho && !A.rho_all) IPG_TRY(dalloc(c, &A.rho_all, 16 * (size_t)Ny * n));
     for (C<double> *p : {A.b1x, A.b2x, A.b1y, A.b2y, A.vbA, A.vbB})
@@ -1817,9 +1818,18 @@ ipg_status backward_inputs(ipg_ctx *c, double *grad_g2mu, double *grad_rho) {
     ai.vbB = A.vbB;
     launch_adjoint_init_links(ai, c->stream);
     IPG_LAUNCHED(c, 3);
+    // the two nuclei are independent from here on: nucleus A on the main
+    // stream with work, nucleus B on stream_v with work2 and buffers of its
+    // own, joined at the end (each chain alone fills under one wave of the
+    // GPU on the lattices the adjoint runs on)
+    IPG_CUDA(c, cudaEventRecord(c->ev_nuc_fork, c->stream));
+    IPG_CUDA(c, cudaStreamWaitEvent(c->stream_v, c->ev_nuc_fork, 0));
     for (int nuc = 0; nuc < 2; nuc++) {
-        IPG_CUDA(c, cudaMemcpyAsync(A.vcur, nuc ? c->VB : c->VA, 9 * n * sizeof(C<double>),
-                                    cudaMemcpyDeviceToDevice, c->stream));
+        cudaStream_t st = nuc ? c->stream_v : c->stream;
+        double2 *work = nuc ? c->work2 : c->work;
+        C<double> *vcur = nuc ? A.vcur2 : A.vcur;
+        IPG_CUDA(c, cudaMemcpyAsync(vcur, nuc ? c->VB : c->VA, 9 * n * sizeof(C<double>),
+                                    cudaMemcpyDeviceToDevice, st));
         C<double> *vb = nuc ? A.vbB : A.vbA;
         WilsonArgs w;
         w.N = N;
@@ -1832,11 +1842,11 @@ ipg_status backward_inputs(ipg_ctx *c, double *grad_g2mu, double *grad_rho) {
         w.nucleus = (uint32_t)nuc;
         w.twiddle = c->twiddle;
         w.green = c->green;
-        w.amp = c->amp;
-        w.work = c->work;
-        w.V = A.vcur;
+        w.amp = nuc ? A.amp2 : c->amp;
+        w.work = work;
+        w.V = vcur;
         w.no_product = 1;
-        launch_wilson_amp(w, c->stream);
+        launch_wilson_amp(w, st);
         IPG_LAUNCHED(c, 1);
         // batches of work_sheets sheets from the top: the transforms of a
         // batch (A_k, then the Poisson map of A_bar_k) run as one launch each,
@@ -1846,28 +1856,29 @@ ipg_status backward_inputs(ipg_ctx *c, double *grad_g2mu, double *grad_rho) {
         for (int kb = Ny; kb > 0; kb -= S) {
             const int k0 = std::max(0, kb - S), ns = kb - k0;
             w.rho_in = nullptr;
-            launch_wilson_sheets(w, k0, ns, c->stream);  // slot k - k0 = A_k
+            launch_wilson_sheets(w, k0, ns, st);  // slot k - k0 = A_k
             IPG_LAUNCHED(c, 3);
             for (int k = kb - 1; k >= k0; k--) {
                 // slot k - k0 becomes A_bar_k
-                launch_adjoint_wilson_sheet(N, c->work + (size_t)(k - k0) * 4 * n, A.vcur, vb,
-                                            c->stream);
+                launch_adjoint_wilson_sheet(N, work + (size_t)(k - k0) * 4 * n, vcur, vb, st);
                 IPG_LAUNCHED(c, 1);
             }
-            w.rho_in = c->work;
-            launch_poisson_sheets(w, ns, c->stream);  // in place: slot k - k0 = rho_bar_k
+            w.rho_in = work;
+            launch_poisson_sheets(w, ns, st);  // in place: slot k - k0 = rho_bar_k
             IPG_LAUNCHED(c, 3);
             w.rho_in = nullptr;
             for (int k = kb - 1; k >= k0; k--) {
                 WilsonArgs ws = w;
-                ws.work = c->work + (size_t)(k - k0) * 4 * n;
+                ws.work = work + (size_t)(k - k0) * 4 * n;
                 launch_adjoint_rho(ws, k, A.g2mu_bar + nuc * n,
                                    grad_rho ? A.rho_all + ((size_t)nuc * Ny + k) * n * 8 : nullptr,
-                                   c->stream);
+                                   st);
                 IPG_LAUNCHED(c, 1);
             }
         }
     }
+    IPG_CUDA(c, cudaEventRecord(c->ev_nuc_join, c->stream_v));
+    IPG_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_nuc_join, 0));
     return IPG_OK;
 }
 }  // namespace
@@ -2173,8 +2184,7 @@ ipg_status ipg_backward(ipg_ctx *c, double w_ET, double w_eps2, double *grad_sta
                     launch_adjoint_step(N, cur, nxt, A.adj, cf, c->stream);
                     IPG_LAUNCHED(c, cf.do_pe ? 2 : 1);
                 } else {
-                    launch_inverse_adjoint_step(N, nxt, cur, A.adj, cf, c->stream, c->stream_v,
-                                                c->ev_adj_fork, c->ev_adj_join);
+                    launch_inverse_adjoint_step(N, nxt, cur, A.adj, cf, c->stream);
                     IPG_LAUNCHED(c, cf.do_pe ? 3 : 2);
                 }
                 nxt = cur;

@@ -23,18 +23,12 @@
 #include "fields.cuh"
 #include "ipg_internal.h"
 #include "pair2.cuh"
+#include "stencil.cuh"
 #include "tma.cuh"
 
 namespace ipg {
 
 // i * (P Q - (P Q)^dag) without forming P Q.
-template <typename T>
-__device__ __forceinline__ H3<T> i_antiherm_mul(const M3<T> &p,
-                                                const M3<T> &q) {
-    M3<T> x = mul(p, q);
-    return i_antiherm(x);
-}
-
 template <typename T>
 __device__ __forceinline__ void reunitarize(M3<T> &u) {
     // Gram-Schmidt on the first two rows, third row = conj(row0 x row1),
@@ -99,44 +93,6 @@ __device__ __forceinline__ M3<T> taylor2_update(const H3<T> &e, T c,
     t.m[8].r += T(1);
     return mul(t, u);
 }
-
-// Field selectors of the link loaders: a link (or lane of a packed link
-// pair) comes from Ux (kLx) or Uy (kLy) at a neighbour offset (dx, dy).
-constexpr int kLx = 0, kLy = 1;
-
-// Full-matrix loads from the global planes, neighbours clamped at the lattice
-// edge (Lattice.cpp:19-28); E and pi are site-local and written back in place.
-template <typename T>
-struct FullLoadGlobal {
-    const State<T> &s;
-    size_t pos, n;
-    long ox[3], oy[3];  // index offsets of dx (dy) = -1, 0, +1, clamped
-    __device__ __forceinline__ FullLoadGlobal(const State<T> &s_, int N, int ix, int iy)
-        : s(s_), pos((size_t)ix * N + iy), n((size_t)N * N) {
-        ox[0] = ix > 0 ? -(long)N : 0;
-        ox[1] = 0;
-        ox[2] = ix + 1 < N ? N : 0;
-        oy[0] = iy > 0 ? -1 : 0;
-        oy[1] = 0;
-        oy[2] = iy + 1 < N ? 1 : 0;
-    }
-    template <int F, int DX, int DY>
-    __device__ __forceinline__ M3<T> link() const {
-        return ld_m3(F == kLy ? s.uy : s.ux, pos + ox[DX + 1] + oy[DY + 1], n);
-    }
-    template <int DX, int DY>
-    __device__ __forceinline__ H3<T> phi() const {
-        return ld_h(s.phi, pos + ox[DX + 1] + oy[DY + 1], n);
-    }
-    __device__ __forceinline__ H3<T> pi() const { return ld_h(s.pi, pos, n); }
-    __device__ __forceinline__ H3<T> e1() const { return ld_h8(s.e1, pos, n); }
-    __device__ __forceinline__ H3<T> e2() const { return ld_h8(s.e2, pos, n); }
-    __device__ __forceinline__ void put_e(const H3<T> &a, const H3<T> &b) const {
-        st_h8(s.e1, pos, n, a);
-        st_h8(s.e2, pos, n, b);
-    }
-    __device__ __forceinline__ void put_pi(const H3<T> &h) const { st_h(s.pi, pos, n, h); }
-};
 
 // One site in full-matrix storage (the FP64 plain form): loads through `ld`,
 // writes the new pi and E through it and returns the new links and phi when
@@ -246,59 +202,31 @@ __device__ __forceinline__ void leapfrog_full_site(int N, int ix, int iy, const 
     }
 }
 
-// Time reversal of the E and pi half of a step (the inverse of S_e): with U
-// and phi of the step's input already recovered in `cur`,
-//   pi = pi' - cdt br(U, phi),   E_d = E_d' - TL(cst t_d + cdt i[U_d phi(+d) U_d^dag, phi])
-// from the same staple and transport code as the forward step.
+// Time reversal of the E and pi half of a step: three thread roles per site
+// (blockIdx.y: E1, E2, pi; inverse_se_role), three times the warps of one
+// thread per site at two thirds of the registers
 template <typename T>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 3)
     k_inv_se(int N, State<T> nxt, State<T> cur, StepCoef<double> cf) {
-    const int iy = blockIdx.x * blockDim.x + threadIdx.x;
-    const int ix = blockIdx.y * blockDim.y + threadIdx.y;
-    if (ix >= N || iy >= N) return;
-    const FullLoadGlobal<T> ld(cur, N, ix, iy);
-    const size_t pos = ld.pos, n = ld.n;
-    H3<T> pi = ld_h(nxt.pi, pos, n);
-    H3<T> e1 = ld_h8(nxt.e1, pos, n), e2 = ld_h8(nxt.e2, pos, n);
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (size_t)N * N) return;
+    const int role = blockIdx.y;
     if (cf.do_pe) {
-        H3<T> t1, t2;
-        full_staples<T>(ld, t1, t2);
-        const T cst = (T)(cf.tau * cf.dt_pe / (2. * cf.g * cf.g));
-        const T cdt = (T)(cf.dt_pe / cf.tau);
-        H3<T> d1 = {}, d2 = {};
-        h_axpy(d1, cst, t1);
-        h_axpy(d2, cst, t2);
-        H3<T> br;
-        {
-            H3<T> phx = conj_h(ld.template link<kLx, 0, 0>(), ld.template phi<1, 0>());
-            h_axpy(d1, cdt, i_commutator(phx, ld.template phi<0, 0>()));
-            br = phx;
-        }
-        {
-            H3<T> phy = conj_h(ld.template link<kLy, 0, 0>(), ld.template phi<0, 1>());
-            h_axpy(d2, cdt, i_commutator(phy, ld.template phi<0, 0>()));
-            h_add(br, phy);
-        }
-        h_add(br, conj_h_dag(ld.template link<kLx, -1, 0>(), ld.template phi<-1, 0>()));
-        h_add(br, conj_h_dag(ld.template link<kLy, 0, -1>(), ld.template phi<0, -1>()));
-        h_axpy(br, T(-4.), ld.template phi<0, 0>());
-        h_axpy(pi, -cdt, br);
-        h_traceless(d1);
-        h_traceless(d2);
-        h_axpy(e1, T(-1.), d1);
-        h_axpy(e2, T(-1.), d2);
-        h_traceless(e1);
-        h_traceless(e2);
+        inverse_se_role<T>(N, role, p, nxt, cur, (T)(cf.tau * cf.dt_pe / (2. * cf.g * cf.g)),
+                           (T)(cf.dt_pe / cf.tau));
+    } else if (role == 2) {
+        st_h(cur.pi, p, (size_t)N * N, ld_h(nxt.pi, p, (size_t)N * N));
+    } else {
+        st_h8(role == 0 ? cur.e1 : cur.e2, p, (size_t)N * N,
+              ld_h8(role == 0 ? nxt.e1 : nxt.e2, p, (size_t)N * N));
     }
-    st_h(cur.pi, pos, n, pi);
-    st_h8(cur.e1, pos, n, e1);
-    st_h8(cur.e2, pos, n, e2);
 }
 
 template <typename T>
 void launch_inverse_se(int N, const State<T> &nxt, const State<T> &cur, const StepCoef<double> &cf,
                        cudaStream_t st) {
-    k_inv_se<T><<<dim3((N + 31) / 32, (N + 3) / 4), dim3(32, 4), 0, st>>>(N, nxt, cur, cf);
+    const size_t n = (size_t)N * N;
+    k_inv_se<T><<<dim3((unsigned)((n + 127) / 128), 3), 128, 0, st>>>(N, nxt, cur, cf);
 }
 template void launch_inverse_se<double>(int, const State<double> &, const State<double> &,
                                         const StepCoef<double> &, cudaStream_t);

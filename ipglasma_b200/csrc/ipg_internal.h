@@ -304,15 +304,13 @@ void launch_inverse_step(int N, const State<double> &nxt, const State<double> &c
 template <typename T>
 void launch_inverse_se(int N, const State<T> &nxt, const State<T> &cur,
                        const StepCoef<double> &cf, cudaStream_t st);
-// the time reversal nxt -> cur and the adjoint step together (fewer launches
-// than launch_inverse_step then launch_adjoint_step, same results; FP64);
-// with a second stream st2 (and two events) the E/pi reversal runs beside
-// the S_e adjoint, joined back into st
+// the time reversal nxt -> cur and the adjoint step together (the U/phi
+// reversal fused with the S_u adjoint, then the E/pi reversal and the S_e
+// adjoint; same results as launch_inverse_step then launch_adjoint_step; FP64)
 template <typename T>
 void launch_inverse_adjoint_step(int N, const State<T> &nxt, const State<T> &cur,
                                  const AdjStateT<T> &a, const StepCoef<double> &cf,
-                                 cudaStream_t st, cudaStream_t st2 = nullptr,
-                                 cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr);
+                                 cudaStream_t st);
 // adjoints of a step's outputs -> adjoints of its inputs (in place); cur is the
 // state before the step, nxt the state after it. T = double, or float for the
 // FP32 adjoint (the FP32 bulk form's states, links as W = U - 1; adjoints in
