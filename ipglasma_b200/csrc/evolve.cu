@@ -222,14 +222,6 @@ __global__ void __launch_bounds__(128, 3)
     }
 }
 
-template <typename T>
-void launch_inverse_se(int N, const State<T> &nxt, const State<T> &cur, const StepCoef<double> &cf,
-                       cudaStream_t st) {
-    const size_t n = (size_t)N * N;
-    k_inv_se<T><<<dim3((unsigned)((n + 127) / 128), 3), 128, 0, st>>>(N, nxt, cur, cf);
-}
-template void launch_inverse_se<double>(int, const State<double> &, const State<double> &,
-                                        const StepCoef<double> &, cudaStream_t);
 
 
 template <typename T, bool REUNIT>
@@ -1697,6 +1689,47 @@ void launch_leapfrog_site(const EventGeom *d_ev, int N, const State<T> &s,
                                                         phi_out, cf);
     }
 }
+
+// The E and pi half of a step reversed. S_e with dt_pe negated (cst and cdt
+// change sign) gives E = TL(E' - cst t - cdt i[U phi(+d) U^dag, phi]) and
+// pi = pi' - cdt br, the inverse of the forward update up to rounding, and
+// the step's TMA tile kernel computes exactly that with the U and phi update
+// switched off: links and phi from `cur` (already recovered), E' and pi' from
+// `nxt`, E and pi written to `cur`. Without tiles, k_inv_se.
+template <typename T>
+void launch_inverse_se(int N, const State<T> &nxt, const State<T> &cur, const StepCoef<double> &cf,
+                       cudaStream_t st) {
+    const size_t n = (size_t)N * N;
+    if constexpr (sizeof(T) == 8) {
+        if (cf.do_pe && N >= 32 && use_tile64_kernel()) {
+            using namespace tile64;
+            const uint64_t nn = (uint64_t)N;
+            const auto U64 = CU_TENSOR_MAP_DATA_TYPE_UINT64;
+            LoadMaps m;
+            const bool ok =
+                encode_tiled_3d(&m.ux, cur.ux, U64, 8, 2 * nn, nn, 9, 2 * UC, UR, 9) &&
+                encode_tiled_3d(&m.uy, cur.uy, U64, 8, 2 * nn, nn, 9, 2 * UC, UR, 9) &&
+                encode_tiled_3d(&m.phi, cur.phi, U64, 8, nn, nn, 9, PC, PR, 9) &&
+                encode_tiled_3d(&m.e1, nxt.e1, U64, 8, nn, nn, 8, Cn, R, 8) &&
+                encode_tiled_3d(&m.e2, nxt.e2, U64, 8, nn, nn, 8, Cn, R, 8) &&
+                encode_tiled_3d(&m.pi, nxt.pi, U64, 8, nn, nn, 9, Cn, R, 9);
+            if (ok) {
+                StepCoef<double> rc = cf;
+                rc.dt_pe = -cf.dt_pe;
+                rc.do_pu = 0;
+                set_derived(rc);
+                cudaFuncSetAttribute(k_leapfrog_tile64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     SMEM);
+                k_leapfrog_tile64<<<(N / R) * (N / Cn), 128, SMEM, st>>>(m, N, rc, nullptr, cur,
+                                                                           nullptr, nullptr, nullptr);
+                return;
+            }
+        }
+    }
+    k_inv_se<T><<<dim3((unsigned)((n + 127) / 128), 3), 128, 0, st>>>(N, nxt, cur, cf);
+}
+template void launch_inverse_se<double>(int, const State<double> &, const State<double> &,
+                                        const StepCoef<double> &, cudaStream_t);
 
 template void launch_leapfrog<double>(const EventGeom *, int, const State<double> &,
                                       C<double> *, C<double> *, double *,
