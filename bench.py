@@ -521,7 +521,10 @@ def measure_workload(torch, ipg, w, specs, K, W, key0, dist, clocks=None, e2e_st
         dist.barrier()
     r64 = batch_step(evs64, b64, key0 + 99999)
     err = batch_errors(evs32, evs64, specs, r32, r64)
-    stages = stage_rates(w, specs, evs64, key0)
+    # the FP64 form's stages, and the FP32 form's (FP32 Poisson transforms,
+    # FP64 exponentials and products; Newton on the group)
+    stages = {"fp64": stage_rates(w, specs, evs64, key0),
+              "fp32": stage_rates(w, specs, evs32, key0)}
     b32.close()
     b64.close()
     for ev in evs32 + evs64:

@@ -58,6 +58,10 @@ struct ipg_ctx {
     // initial-condition scratch
     double2 *twiddle = nullptr;
     double *green = nullptr;
+    // FP32 contexts: the Poisson transforms' twiddles and Green function in
+    // FP32 (the transforms of the FP32 form run in FP32)
+    float2 *twiddle32 = nullptr;
+    float *green32 = nullptr;
     double *amp = nullptr;
     double2 *work = nullptr, *work2 = nullptr;
     double *nuc_xyz = nullptr, *nuc_gx = nullptr, *nuc_gy = nullptr;  // ipg_set_nuclei
@@ -858,6 +862,17 @@ ipg_status ipg_create(const ipg_config *cfg, ipg_ctx **out) {
                                 cudaMemcpyHostToDevice, c->stream));
     launch_green(N, c->m_lat, c->uv_lat, c->green, c->stream);
     IPG_LAUNCHED(c, 1);
+    if (is_fp32(c)) {
+        std::vector<float2> tw32(N);
+        for (int k = 0; k < N; k++) tw32[k] = make_float2((float)tw[k].x, (float)tw[k].y);
+        IPG_TRY(dalloc(c, &c->twiddle32, (size_t)N));
+        IPG_TRY(dalloc(c, &c->green32, n));
+        IPG_CUDA(c, cudaMemcpyAsync(c->twiddle32, tw32.data(), sizeof(float2) * N,
+                                    cudaMemcpyHostToDevice, c->stream));
+        launch_round_to_float(n, c->green, c->green32, c->stream);
+        IPG_LAUNCHED(c, 1);
+        IPG_TRY(sync(c));
+    }
     IPG_TRY(sync(c));
     c->err.clear();
     return IPG_OK;
@@ -1248,10 +1263,15 @@ static ipg_status init_enqueue(ipg_ctx *c, bool from_wilson) {
         w.amp = c->amp;
         w.work = c->work;
         w.V = V;
+        // the FP32 form transforms in FP32: twice the sheets fit a work buffer
+        w.fp32 = is_fp32(c) ? 1 : 0;
+        w.twiddle32 = c->twiddle32;
+        w.green32 = c->green32;
+        const int sheets = w.fp32 ? 2 * c->work_sheets : c->work_sheets;
         launch_wilson_amp(w, c->stream);
         IPG_LAUNCHED(c, 1);
-        for (int k0 = 0; k0 < c->cfg.Ny; k0 += c->work_sheets, batch++) {
-            const int ns = std::min(c->work_sheets, c->cfg.Ny - k0);
+        for (int k0 = 0; k0 < c->cfg.Ny; k0 += sheets, batch++) {
+            const int ns = std::min(sheets, c->cfg.Ny - k0);
             const int i = batch & 1;
             w.work = i ? c->work2 : c->work;
             // the buffer is free once the product of two batches ago has read it

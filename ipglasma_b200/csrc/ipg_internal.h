@@ -133,6 +133,12 @@ struct WilsonArgs {
     // when set and nonzero on the device, the transform kernels return at
     // once (the gauge-fixing loop's stop flag)
     const int *skip = nullptr;
+    // the FP32 form's Poisson transforms: work holds float2 values
+    // ([ns][4][n]), with twiddle32 and green32 in place of twiddle and green;
+    // the exponentials and the Wilson-line products stay FP64
+    int fp32 = 0;
+    const float2 *twiddle32 = nullptr;
+    const float *green32 = nullptr;
 };
 // Poisson map only (no Wilson-line product) of w.rho_in -> w.work, sheets [0, ns)
 void launch_poisson_sheets(const WilsonArgs &w, int ns, cudaStream_t st);
@@ -142,6 +148,8 @@ void launch_wilson_sheets(const WilsonArgs &w, int k0, int ns,
 void launch_wilson_product(const WilsonArgs &w, int ns, cudaStream_t st);
 // charge amplitude of every site, once per nucleus before its sheets
 void launch_wilson_amp(const WilsonArgs &w, cudaStream_t st);
+// out[p] = (float)in[p], p < n
+void launch_round_to_float(size_t n, const double *in, float *out, cudaStream_t st);
 
 // the device noise of sheets [k0, k0+ns) of one nucleus, as the unit normals
 // xi[ns][N*N][8] that k_rows_fwd draws for them

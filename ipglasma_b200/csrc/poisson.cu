@@ -101,12 +101,48 @@ void launch_draw_noise(int N, int k0, int ns, uint64_t key, uint32_t nucleus, do
                                                                      out);
 }
 
+__global__ void k_round_to_float(size_t n, const double *in, float *out) {
+    const size_t p = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) out[p] = (float)in[p];
+}
+
+void launch_round_to_float(size_t n, const double *in, float *out, cudaStream_t st) {
+    k_round_to_float<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, in, out);
+}
+
 void launch_wilson_amp(const WilsonArgs &w, cudaStream_t st) {
     const int n = w.N * w.N;
     k_amp<<<(n + 255) / 256, 256, 0, st>>>(n, w.g, (double)w.Ny, w.g2mu2, w.amp);
 }
 
 namespace {
+
+// packed complex storage of the work buffer: double2 (FP64 transforms) or
+// float2 (the FP32 form's transforms, WilsonArgs::fp32)
+template <typename R>
+struct Store2;
+template <>
+struct Store2<double> {
+    using type = double2;
+};
+template <>
+struct Store2<float> {
+    using type = float2;
+};
+template <typename R>
+using store2_t = typename Store2<R>::type;
+
+template <typename R>
+__device__ __forceinline__ store2_t<R> *work_of(const WilsonArgs &w) {
+    return reinterpret_cast<store2_t<R> *>(w.work);
+}
+template <typename R>
+__device__ __forceinline__ const C<R> *twiddles_of(const WilsonArgs &w) {
+    if constexpr (sizeof(R) == 8)
+        return reinterpret_cast<const C<R> *>(w.twiddle);
+    else
+        return reinterpret_cast<const C<R> *>(w.twiddle32);
+}
 
 // rows of one CTA in the row kernels: a CTA is RPB rows x 4 channels x N/8
 // threads, sequence seq = 4 rl + c
@@ -138,13 +174,13 @@ constexpr int fwd_seq_stride(int N) {
 
 }  // namespace
 
-template <int LOGN>
+template <int LOGN, typename R>
 __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_fwd(WilsonArgs w, int k0) {
     if (w.skip && *w.skip) return;
     constexpr int N = 1 << LOGN, TPS = N / 8, RPB = rows_per_block<LOGN>();
     constexpr int S = fwd_seq_stride(N);
     extern __shared__ __align__(16) unsigned char smraw[];
-    C<double> *sm = reinterpret_cast<C<double> *>(smraw);
+    C<R> *sm = reinterpret_cast<C<R> *>(smraw);
     const size_t n = (size_t)N * N;
     // lanes 2i and 2i+1 hold channels 2h and 2h+1 of the same points (they
     // share one Philox counter); TPS >= 1 sequences of N/8 threads each
@@ -154,14 +190,14 @@ __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_fwd(WilsonArgs w, 
     const int seq = 4 * rl + c;
     const int s = blockIdx.y, k = k0 + s;
     const size_t row = (size_t)(blockIdx.x * RPB + rl) * N;
-    const C<double> *tw = reinterpret_cast<const C<double> *>(w.twiddle);
-    C<double> x[8];
+    const C<R> *tw = twiddles_of<R>(w);
+    C<R> x[8];
     if (w.rho_in) {
         const double2 *in = w.rho_in + ((size_t)s * 4 + c) * n + row + t;
 #pragma unroll
         for (int m = 0; m < 8; m++) {
             const double2 v = in[m * TPS];
-            x[m] = {v.x, v.y};
+            x[m] = {(R)v.x, (R)v.y};
         }
     } else {
         double amp[8], z[8][2];
@@ -205,90 +241,95 @@ __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_fwd(WilsonArgs w, 
             for (int m = 0; m < 8; m++) box_muller(keep[m][0], keep[m][1], z[m]);
         }
 #pragma unroll
-        for (int m = 0; m < 8; m++) x[m] = {amp[m] * z[m][0], amp[m] * z[m][1]};
+        for (int m = 0; m < 8; m++) x[m] = {(R)(amp[m] * z[m][0]), (R)(amp[m] * z[m][1])};
     }
-    fft_regs<LOGN, double, false>(x, sm + seq * S, t, tw);
-    double2 *out = w.work + ((size_t)s * 4 + c) * n + row + t;
+    fft_regs<LOGN, R, false>(x, sm + seq * S, t, tw);
+    store2_t<R> *out = work_of<R>(w) + ((size_t)s * 4 + c) * n + row + t;
 #pragma unroll
-    for (int m = 0; m < 8; m++) out[m * TPS] = make_double2(x[m].r, x[m].i);
+    for (int m = 0; m < 8; m++) out[m * TPS] = {x[m].r, x[m].i};
 }
 
 // CONV: forward transform, Green multiply, inverse transform; otherwise the
 // forward transform only
-template <int LOGN, bool CONV = true>
+template <int LOGN, bool CONV = true, typename R = double>
 __global__ void __launch_bounds__(col_threads<LOGN>(), 2) k_cols(WilsonArgs w) {
     if (w.skip && *w.skip) return;
     constexpr int N = 1 << LOGN, TPS = N / 8, JB = cols_per_block<LOGN>();
     constexpr int S = fft_seq_stride(N);
     extern __shared__ __align__(16) unsigned char smraw[];
-    C<double> *sm = reinterpret_cast<C<double> *>(smraw);
+    C<R> *sm = reinterpret_cast<C<R> *>(smraw);
     const size_t n = (size_t)N * N;
     const int q = threadIdx.x & (JB - 1), t = threadIdx.x / JB;
     const int col = blockIdx.x * JB + q;
     const int c = blockIdx.y, s = blockIdx.z;
-    double2 *base = w.work + ((size_t)s * 4 + c) * n + col;
-    const C<double> *tw = reinterpret_cast<const C<double> *>(w.twiddle);
-    C<double> x[8];
-    double gk[8];
+    store2_t<R> *base = work_of<R>(w) + ((size_t)s * 4 + c) * n + col;
+    const C<R> *tw = twiddles_of<R>(w);
+    C<R> x[8];
+    R gk[8];
 #pragma unroll
     for (int m = 0; m < 8; m++) {
-        const double2 v = base[(size_t)(t + m * TPS) * N];
+        const store2_t<R> v = base[(size_t)(t + m * TPS) * N];
         x[m] = {v.x, v.y};
     }
-    fft_regs<LOGN, double, false>(x, sm + q * S, t, tw);
+    fft_regs<LOGN, R, false>(x, sm + q * S, t, tw);
     if constexpr (CONV) {
         // the Green factors are loaded after the forward transform: that
         // keeps the kernel within 64 registers, two 512-thread blocks per SM
+        const R *green = sizeof(R) == 8 ? reinterpret_cast<const R *>(w.green)
+                                        : reinterpret_cast<const R *>(w.green32);
 #pragma unroll
-        for (int m = 0; m < 8; m++) gk[m] = w.green[(size_t)(t + m * TPS) * N + col];
+        for (int m = 0; m < 8; m++) gk[m] = green[(size_t)(t + m * TPS) * N + col];
 #pragma unroll
         for (int m = 0; m < 8; m++) x[m] = {x[m].r * gk[m], x[m].i * gk[m]};
-        fft_regs<LOGN, double, true>(x, sm + q * S, t, tw);
+        fft_regs<LOGN, R, true>(x, sm + q * S, t, tw);
     }
 #pragma unroll
-    for (int m = 0; m < 8; m++) base[(size_t)(t + m * TPS) * N] = make_double2(x[m].r, x[m].i);
+    for (int m = 0; m < 8; m++) base[(size_t)(t + m * TPS) * N] = {x[m].r, x[m].i};
 }
 
-template <int LOGN>
+template <int LOGN, typename R>
 __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_inv(WilsonArgs w) {
     if (w.skip && *w.skip) return;
     constexpr int N = 1 << LOGN, TPS = N / 8, RPB = rows_per_block<LOGN>();
     constexpr int S = fft_seq_stride(N);
     extern __shared__ __align__(16) unsigned char smraw[];
-    C<double> *sm = reinterpret_cast<C<double> *>(smraw);
+    C<R> *sm = reinterpret_cast<C<R> *>(smraw);
     const size_t n = (size_t)N * N;
     const int seq = threadIdx.x / TPS, t = threadIdx.x - seq * TPS;
     const int rl = seq >> 2, c = seq & 3;
     const int s = blockIdx.y;
-    double2 *p = w.work + ((size_t)s * 4 + c) * n + (size_t)(blockIdx.x * RPB + rl) * N + t;
-    const C<double> *tw = reinterpret_cast<const C<double> *>(w.twiddle);
-    C<double> x[8];
+    store2_t<R> *p = work_of<R>(w) + ((size_t)s * 4 + c) * n + (size_t)(blockIdx.x * RPB + rl) * N + t;
+    const C<R> *tw = twiddles_of<R>(w);
+    C<R> x[8];
 #pragma unroll
     for (int m = 0; m < 8; m++) {
-        const double2 v = p[m * TPS];
+        const store2_t<R> v = p[m * TPS];
         x[m] = {v.x, v.y};
     }
-    fft_regs<LOGN, double, true>(x, sm + seq * S, t, tw);
+    fft_regs<LOGN, R, true>(x, sm + seq * S, t, tw);
     // n = N^2 is a power of two, so multiplying by 1/n is exact and gives
     // the same bits as the reference's division by n
-    const double inv_n = 1.0 / (double)n;
+    const R inv_n = R(1) / (R)n;
 #pragma unroll
-    for (int m = 0; m < 8; m++) p[m * TPS] = make_double2(x[m].r * inv_n, x[m].i * inv_n);
+    for (int m = 0; m < 8; m++) p[m * TPS] = {x[m].r * inv_n, x[m].i * inv_n};
 }
 
-// V <- exp(-i A_k.t) V for the sheets of the batch, in ascending k
+// V <- exp(-i A_k.t) V for the sheets of the batch, in ascending k; the
+// exponential and the product in FP64 whatever the transforms' type R
+template <typename R>
 __global__ void __launch_bounds__(128) k_wilson(WilsonArgs w, int ns) {
     const size_t n = (size_t)w.N * w.N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
+    const store2_t<R> *work = work_of<R>(w);
     M3<double> V = ld_m3(w.V, pos, n);
     for (int s = 0; s < ns; s++) {
         double in[8];
 #pragma unroll
         for (int c = 0; c < 4; c++) {
-            const double2 v = w.work[((size_t)s * 4 + c) * n + pos];
-            in[2 * c] = -v.x;
-            in[2 * c + 1] = -v.y;
+            const store2_t<R> v = work[((size_t)s * 4 + c) * n + pos];
+            in[2 * c] = -(double)v.x;
+            in[2 * c + 1] = -(double)v.y;
         }
         const M3<double> e = exp_from_coeff(in);
         V = mul(e, V);
@@ -296,26 +337,35 @@ __global__ void __launch_bounds__(128) k_wilson(WilsonArgs w, int ns) {
     st_m3(w.V, pos, n, V);
 }
 
-template <int LOGN>
-static void launch_sheets(const WilsonArgs &w, int k0, int ns, cudaStream_t st) {
+template <int LOGN, typename R>
+static void launch_sheets_t(const WilsonArgs &w, int k0, int ns, cudaStream_t st) {
     constexpr int N = 1 << LOGN;
     constexpr int RPB = rows_per_block<LOGN>(), JB = cols_per_block<LOGN>();
-    const size_t row_smem = sizeof(double2) * RPB * 4 * fft_seq_stride(N);
-    const size_t fwd_smem = sizeof(double2) * RPB * 4 * fwd_seq_stride(N);
-    const size_t col_smem = sizeof(double2) * JB * fft_seq_stride(N);
+    const size_t row_smem = sizeof(C<R>) * RPB * 4 * fft_seq_stride(N);
+    const size_t fwd_smem = sizeof(C<R>) * RPB * 4 * fwd_seq_stride(N);
+    const size_t col_smem = sizeof(C<R>) * JB * fft_seq_stride(N);
     // the attribute is per device: set it on every launch (a host-side call
     // without a device round trip)
-    cudaFuncSetAttribute(k_rows_fwd<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_rows_fwd<LOGN, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)fwd_smem);
-    cudaFuncSetAttribute(k_rows_inv<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_rows_inv<LOGN, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)row_smem);
-    cudaFuncSetAttribute(k_cols<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_cols<LOGN, true, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)col_smem);
-    k_rows_fwd<LOGN><<<dim3(N / RPB, ns), row_threads<LOGN>(), fwd_smem, st>>>(w, k0);
-    k_cols<LOGN><<<dim3(N / JB, 4, ns), col_threads<LOGN>(), col_smem, st>>>(w);
-    k_rows_inv<LOGN><<<dim3(N / RPB, ns), row_threads<LOGN>(), row_smem, st>>>(w);
+    k_rows_fwd<LOGN, R><<<dim3(N / RPB, ns), row_threads<LOGN>(), fwd_smem, st>>>(w, k0);
+    k_cols<LOGN, true, R><<<dim3(N / JB, 4, ns), col_threads<LOGN>(), col_smem, st>>>(w);
+    k_rows_inv<LOGN, R><<<dim3(N / RPB, ns), row_threads<LOGN>(), row_smem, st>>>(w);
     const size_t n = (size_t)N * N;
-    if (!w.rho_in && !w.no_product) k_wilson<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
+    if (!w.rho_in && !w.no_product)
+        k_wilson<R><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
+}
+
+template <int LOGN>
+static void launch_sheets(const WilsonArgs &w, int k0, int ns, cudaStream_t st) {
+    if (w.fp32)
+        launch_sheets_t<LOGN, float>(w, k0, ns, st);
+    else
+        launch_sheets_t<LOGN, double>(w, k0, ns, st);
 }
 
 template <int LOGN>
@@ -324,11 +374,11 @@ static void launch_forward(const WilsonArgs &w, int ns, cudaStream_t st) {
     constexpr int RPB = rows_per_block<LOGN>(), JB = cols_per_block<LOGN>();
     const size_t fwd_smem = sizeof(double2) * RPB * 4 * fwd_seq_stride(N);
     const size_t col_smem = sizeof(double2) * JB * fft_seq_stride(N);
-    cudaFuncSetAttribute(k_rows_fwd<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(k_rows_fwd<LOGN, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)fwd_smem);
     cudaFuncSetAttribute(k_cols<LOGN, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)col_smem);
-    k_rows_fwd<LOGN><<<dim3(N / RPB, ns), row_threads<LOGN>(), fwd_smem, st>>>(w, 0);
+    k_rows_fwd<LOGN, double><<<dim3(N / RPB, ns), row_threads<LOGN>(), fwd_smem, st>>>(w, 0);
     k_cols<LOGN, false><<<dim3(N / JB, 4, ns), col_threads<LOGN>(), col_smem, st>>>(w);
 }
 
@@ -350,7 +400,10 @@ void launch_fft2_forward(const WilsonArgs &w, int ns, cudaStream_t st) {
 // the Wilson-line product of a batch whose A is already in w.work
 void launch_wilson_product(const WilsonArgs &w, int ns, cudaStream_t st) {
     const size_t n = (size_t)w.N * w.N;
-    k_wilson<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
+    if (w.fp32)
+        k_wilson<float><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
+    else
+        k_wilson<double><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(w, ns);
 }
 
 void launch_poisson_sheets(const WilsonArgs &w, int ns, cudaStream_t st) {
