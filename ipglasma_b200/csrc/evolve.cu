@@ -29,50 +29,6 @@
 namespace ipg {
 
 // i * (P Q - (P Q)^dag) without forming P Q.
-template <typename T>
-__device__ __forceinline__ void reunitarize(M3<T> &u) {
-    // Gram-Schmidt on the first two rows, third row = conj(row0 x row1),
-    // the SU(3) completion used by the reference's Matrix::reu (Matrix.h:67-109).
-    T n0 = u.m[0].r * u.m[0].r + u.m[0].i * u.m[0].i + u.m[1].r * u.m[1].r +
-           u.m[1].i * u.m[1].i + u.m[2].r * u.m[2].r + u.m[2].i * u.m[2].i;
-    T inv0 = rsqrt(n0);
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        u.m[k].r *= inv0;
-        u.m[k].i *= inv0;
-    }
-    // proj = <row0, row1> = sum conj(row0_k) row1_k
-    C<T> pr = {T(0), T(0)};
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        pr.r += u.m[k].r * u.m[3 + k].r + u.m[k].i * u.m[3 + k].i;
-        pr.i += u.m[k].r * u.m[3 + k].i - u.m[k].i * u.m[3 + k].r;
-    }
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        C<T> t = cmul(pr, u.m[k]);
-        u.m[3 + k].r -= t.r;
-        u.m[3 + k].i -= t.i;
-    }
-    T n1 = u.m[3].r * u.m[3].r + u.m[3].i * u.m[3].i + u.m[4].r * u.m[4].r +
-           u.m[4].i * u.m[4].i + u.m[5].r * u.m[5].r + u.m[5].i * u.m[5].i;
-    T inv1 = rsqrt(n1);
-#pragma unroll
-    for (int k = 3; k < 6; k++) {
-        u.m[k].r *= inv1;
-        u.m[k].i *= inv1;
-    }
-    // row2 = conj(row0 x row1)
-    C<T> a0 = u.m[0], a1 = u.m[1], a2 = u.m[2], b0 = u.m[3], b1 = u.m[4],
-         b2 = u.m[5];
-    C<T> c0 = cmul(a1, b2), c0b = cmul(a2, b1);
-    C<T> c1 = cmul(a2, b0), c1b = cmul(a0, b2);
-    C<T> c2 = cmul(a0, b1), c2b = cmul(a1, b0);
-    u.m[6] = {c0.r - c0b.r, -(c0.i - c0b.i)};
-    u.m[7] = {c1.r - c1b.r, -(c1.i - c1b.i)};
-    u.m[8] = {c2.r - c2b.r, -(c2.i - c2b.i)};
-}
-
 // U_new = (1 + X + X^2/2) U with X = i c E, E Hermitian:
 // (1 + X + X^2/2) = (1 - c^2 E^2 / 2) + i c E.
 template <typename T>

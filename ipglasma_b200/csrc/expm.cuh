@@ -143,6 +143,86 @@ __device__ __forceinline__ M3<double> exp_from_coeff(const double in[8]) {
     return r;
 }
 
+// Product of two Hermitian matrices that commute (both polynomials in one
+// Hermitian matrix), which is Hermitian: only the real diagonal and the
+// upper triangle are formed.
+template <typename T>
+__device__ __forceinline__ H3<T> hmul_commuting(const H3<T> &a, const H3<T> &b) {
+    const M3<T> A = from_h(a), B = from_h(b);
+    auto e = [&](int i, int j) {
+        C<T> s = cmul(A.m[3 * i], B.m[j]);
+        const C<T> s1 = cmul(A.m[3 * i + 1], B.m[3 + j]), s2 = cmul(A.m[3 * i + 2], B.m[6 + j]);
+        return C<T>{s.r + s1.r + s2.r, s.i + s1.i + s2.i};
+    };
+    H3<T> r;
+    r.d0 = e(0, 0).r;
+    r.d1 = e(1, 1).r;
+    r.d2 = e(2, 2).r;
+    r.o01 = e(0, 1);
+    r.o02 = e(0, 2);
+    r.o12 = e(1, 2);
+    return r;
+}
+
+// s h + c 1
+template <typename T>
+__device__ __forceinline__ H3<T> h_affine(const H3<T> &h, T s, T c) {
+    return {s * h.d0 + c, s * h.d1 + c, s * h.d2 + c, {s * h.o01.r, s * h.o01.i},
+            {s * h.o02.r, s * h.o02.i}, {s * h.o12.r, s * h.o12.i}};
+}
+
+// exp(i q.t) in FP32 for the FP32 form's Wilson-line factors: scaling and
+// squaring with a Taylor series (Moler & Van Loan, "Nineteen dubious ways to
+// compute the exponential of a matrix", SIAM Review 45 (2003), method 3).
+// H = q.t is scaled by 2^-s until |H|_F = sqrt(sum q^2 / 2) <= 1/2; then
+// exp(iH) = C + iS with the even and odd parts
+//   C = 1 - H^2/2! + H^4/4! - H^6/6! + H^8/8!,  S = H - H^3/3! + H^5/5! - H^7/7!,
+// both Hermitian polynomials in H^2 (Horner, products of commuting Hermitian
+// matrices); the remainder is below 0.5^9/9! = 5.4e-9, under FP32 rounding.
+// The s squarings are full complex products. Unlike the closed form, this
+// stays accurate where eigenvalues of H nearly coincide (weak fields).
+__device__ __forceinline__ M3<float> exp_i_taylor_f32(const float q_in[8]) {
+    float nrm2 = 0.f;
+#pragma unroll
+    for (int a = 0; a < 8; a++) nrm2 += q_in[a] * q_in[a];
+    nrm2 *= 0.5f;
+    int s = 0;
+    while (nrm2 > 0.25f && s < 64) {
+        nrm2 *= 0.25f;
+        s++;
+    }
+    float q[8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) q[a] = ldexpf(q_in[a], -s);
+    // H = sum_a q_a t^a in the generator convention of exp_from_coeff
+    const float c8 = (float)IPG_C8;
+    H3<float> h;
+    h.d0 = 0.5f * q[2] + c8 * q[7];
+    h.d1 = -0.5f * q[2] + c8 * q[7];
+    h.d2 = -2.f * c8 * q[7];
+    h.o01 = {0.5f * q[0], -0.5f * q[1]};
+    h.o02 = {0.5f * q[3], -0.5f * q[4]};
+    h.o12 = {0.5f * q[5], -0.5f * q[6]};
+    const H3<float> h2 = hmul_commuting(h, h);
+    // C = 1 + H2 (-1/2 + H2 (1/24 + H2 (-1/720 + H2 / 40320)))
+    H3<float> c = h_affine(h2, 1.f / 40320.f, -1.f / 720.f);
+    c = h_affine(hmul_commuting(h2, c), 1.f, 1.f / 24.f);
+    c = h_affine(hmul_commuting(h2, c), 1.f, -0.5f);
+    c = h_affine(hmul_commuting(h2, c), 1.f, 1.f);
+    // S = H (1 + H2 (-1/6 + H2 (1/120 - H2 / 5040)))
+    H3<float> r = h_affine(h2, -1.f / 5040.f, 1.f / 120.f);
+    r = h_affine(hmul_commuting(h2, r), 1.f, -1.f / 6.f);
+    r = h_affine(hmul_commuting(h2, r), 1.f, 1.f);
+    const H3<float> sd = hmul_commuting(h, r);
+    // E = C + i S entry by entry (C_ji = conj C_ij, S_ji = conj S_ij)
+    const M3<float> C = from_h(c), S = from_h(sd);
+    M3<float> e;
+#pragma unroll
+    for (int k = 0; k < 9; k++) e.m[k] = {C.m[k].r - S.m[k].i, C.m[k].i + S.m[k].r};
+    for (int k = 0; k < s; k++) e = mul(e, e);
+    return e;
+}
+
 // tr(t^a M) for the Gell-Mann generators, a = 0..7
 __device__ __forceinline__ void trace_ta(const M3<double> &m, C<double> out[8]) {
     const double c8 = IPG_C8, s3 = IPG_INV_SQRT3;

@@ -314,8 +314,12 @@ __global__ void __launch_bounds__(row_threads<LOGN>()) k_rows_inv(WilsonArgs w) 
     for (int m = 0; m < 8; m++) p[m * TPS] = {x[m].r * inv_n, x[m].i * inv_n};
 }
 
-// V <- exp(-i A_k.t) V for the sheets of the batch, in ascending k; the
-// exponential and the product in FP64 whatever the transforms' type R
+// V <- exp(-i A_k.t) V for the sheets of the batch, in ascending k. FP64
+// transforms (R = double): the reference's closed-form exponential in FP64.
+// The FP32 form (R = float): the exponential of the FP32 A in FP32 by
+// scaling and squaring (exp_i_taylor_f32), the product accumulated in FP64
+// and V reunitarised in FP64 at the end of the batch (the FP32 factors are
+// unitary to FP32 rounding).
 template <typename R>
 __global__ void __launch_bounds__(128) k_wilson(WilsonArgs w, int ns) {
     const size_t n = (size_t)w.N * w.N;
@@ -324,16 +328,24 @@ __global__ void __launch_bounds__(128) k_wilson(WilsonArgs w, int ns) {
     const store2_t<R> *work = work_of<R>(w);
     M3<double> V = ld_m3(w.V, pos, n);
     for (int s = 0; s < ns; s++) {
-        double in[8];
+        R in[8];
 #pragma unroll
         for (int c = 0; c < 4; c++) {
             const store2_t<R> v = work[((size_t)s * 4 + c) * n + pos];
-            in[2 * c] = -(double)v.x;
-            in[2 * c + 1] = -(double)v.y;
+            in[2 * c] = -v.x;
+            in[2 * c + 1] = -v.y;
         }
-        const M3<double> e = exp_from_coeff(in);
-        V = mul(e, V);
+        if constexpr (sizeof(R) == 8) {
+            V = mul(exp_from_coeff(in), V);
+        } else {
+            const M3<float> e32 = exp_i_taylor_f32(in);
+            M3<double> e;
+#pragma unroll
+            for (int k = 0; k < 9; k++) e.m[k] = {(double)e32.m[k].r, (double)e32.m[k].i};
+            V = mul(e, V);
+        }
     }
+    if constexpr (sizeof(R) == 4) reunitarize(V);
     st_m3(w.V, pos, n, V);
 }
 
