@@ -20,9 +20,11 @@
 // c2 = (tau + dtau/2) dtau. Its vector-Jacobian product is k_adj_su (local)
 // followed by k_adj_se (it scatters into neighbouring links and phi with
 // FP64 atomics, so the summation order, not the result, varies between runs).
-// The step is inverted exactly in exact arithmetic (k_inv_su and k_inv_se,
-// the latter in evolve.cu on the forward step's code): this
-// is the time reversal used to walk back between checkpoints.
+// The step is inverted exactly in exact arithmetic: U and phi by k_inv_su
+// (or k_inv_adj_su, fused with the S_u adjoint), then E and pi by S_e with
+// dtau negated (launch_inverse_se in evolve.cu: the forward step's tile
+// kernel with the U/phi update off). This is the time reversal used to walk
+// back between checkpoints.
 #include <cstdint>
 
 #include "expm.cuh"
