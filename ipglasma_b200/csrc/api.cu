@@ -511,7 +511,6 @@ ipg_status observables_enqueue(ipg_ctx *c) {
     const int N = c->N;
     IPG_TRY(wait_observable_copies(c));
     IPG_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-    IPG_TRY(state64(c));
     TmunuArgs ta;
     ta.N = N;
     ta.g = c->cfg.g;
@@ -519,6 +518,10 @@ ipg_status observables_enqueue(ipg_ctx *c) {
     ta.a = c->a;
     ta.s = c->s64;
     ta.T10 = c->T10;
+    // FP32 contexts: T^munu reads the FP32 state directly (the FP64 copy is
+    // made once, after the last half step, for the Gauss law and unitarity)
+    ta.from32 = is_fp32(c) ? 1 : 0;
+    ta.s32 = c->s32;
     launch_tmunu(ta, c->stream);
     IPG_LAUNCHED(c, 7);
     LandauArgs la;

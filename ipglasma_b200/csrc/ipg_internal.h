@@ -291,6 +291,10 @@ struct TmunuArgs {
     double a;
     State<double> s;
     double *T10;  // [10][n]: tautau xx yy etaeta taux tauy taueta xy xeta yeta
+    // from32: read the FP32 form's state s32 instead (links stored as U - 1),
+    // widened to FP64 on load; the arithmetic stays FP64
+    State<float> s32{};
+    int from32 = 0;
 };
 void launch_tmunu(const TmunuArgs &a, cudaStream_t st);
 // T^tautau, T^xx, T^yy, T^etaeta only

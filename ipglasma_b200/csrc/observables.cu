@@ -47,6 +47,42 @@ __device__ __forceinline__ M3<double> hm8(const double *p, size_t pos,
                                           size_t n) {
     return from_h(ld_h8(p, pos, n));
 }
+__device__ __forceinline__ H3<double> widen(const H3<float> &h) {
+    return {h.d0, h.d1, h.d2, {h.o01.r, h.o01.i}, {h.o02.r, h.o02.i}, {h.o12.r, h.o12.i}};
+}
+// the FP32 form's fields, widened to FP64 on load (the values an FP64 copy
+// of the state would hold)
+__device__ __forceinline__ M3<double> hm(const float *p, size_t pos, size_t n) {
+    return from_h(widen(ld_h(p, pos, n)));
+}
+__device__ __forceinline__ M3<double> hm8(const float *p, size_t pos, size_t n) {
+    return from_h(widen(ld_h8(p, pos, n)));
+}
+// a link: FP64 as stored; FP32 form stored as W = U - 1, here 1 + W formed in
+// FP64 as the state conversion forms it
+__device__ __forceinline__ M3<double> lnk(const C<double> *p, size_t pos, size_t n) {
+    return ld_m3(p, pos, n);
+}
+__device__ __forceinline__ M3<double> lnk(const C<float> *p, size_t pos, size_t n) {
+    const M3<float> w = ld_m3(p, pos, n);
+    M3<double> u;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const double shift = (k == 0 || k == 4 || k == 8) ? 1.0 : 0.0;
+        u.m[k] = {(double)w.m[k].r + shift, (double)w.m[k].i};
+    }
+    return u;
+}
+template <typename S>
+__device__ __forceinline__ const State<S> &state_of(const TmunuArgs &A);
+template <>
+__device__ __forceinline__ const State<double> &state_of<double>(const TmunuArgs &A) {
+    return A.s;
+}
+template <>
+__device__ __forceinline__ const State<float> &state_of<float>(const TmunuArgs &A) {
+    return A.s32;
+}
 // U A U^dag
 __device__ __forceinline__ M3<double> tr_fwd(const M3<double> &u,
                                              const M3<double> &a) {
@@ -61,6 +97,7 @@ __device__ __forceinline__ M3<double> tr_bwd(const M3<double> &u,
 }  // namespace
 
 // diagonal components: T^tautau, T^xx, T^yy, T^etaeta (Evolution.cpp:735-899)
+template <typename S>
 __global__ void k_tmunu_diag(TmunuArgs A) {
     const int N = A.N;
     const size_t n = (size_t)N * N;
@@ -70,7 +107,7 @@ __global__ void k_tmunu_diag(TmunuArgs A) {
     const size_t pX = idx2(N, min(N - 1, i + 1), j);
     const size_t pY = idx2(N, i, min(N - 1, j + 1));
     const size_t pXY = idx2(N, min(N - 1, i + 1), min(N - 1, j + 1));
-    const State<double> &s = A.s;
+    const State<S> &s = state_of<S>(A);
     const double g = A.g, tau = A.tau;
 
     double trE = 0., trEx = 0., trEy = 0.;
@@ -97,21 +134,21 @@ __global__ void k_tmunu_diag(TmunuArgs A) {
     double Tee = 1. / tau / tau * (ge * trE / 2. - trP / 4.);
 
     // magnetic and longitudinal-gradient part
-    const M3<double> Ux = ld_m3(s.ux, pos, n), Uy = ld_m3(s.uy, pos, n);
+    const M3<double> Ux = lnk(s.ux, pos, n), Uy = lnk(s.uy, pos, n);
     double B;
     if (i == N - 1) {
         B = 0.;  // Uplaq = 1 on the last row (Evolution.cpp:748)
     } else {
         const M3<double> pl =
-            mul(Ux, mul(ld_m3(s.uy, pX, n), mul_nd(dagger(ld_m3(s.ux, pY, n)), Uy)));
+            mul(Ux, mul(lnk(s.uy, pX, n), mul_nd(dagger(lnk(s.ux, pY, n)), Uy)));
         B = 2. / (g * g) * (3. - trace(pl).r);
     }
     const M3<double> phi = hm(s.phi, pos, n), phiX = hm(s.phi, pX, n);
     const M3<double> phiY = hm(s.phi, pY, n), phiXY = hm(s.phi, pXY, n);
     const M3<double> d1 = minus(phi, tr_fwd(Ux, phiX));
     const M3<double> d3 = minus(phi, tr_fwd(Uy, phiY));
-    const M3<double> d2 = minus(phiY, tr_fwd(ld_m3(s.ux, pY, n), phiXY));
-    const M3<double> d4 = minus(phiX, tr_fwd(ld_m3(s.uy, pX, n), phiXY));
+    const M3<double> d2 = minus(phiY, tr_fwd(lnk(s.ux, pY, n), phiXY));
+    const M3<double> d4 = minus(phiX, tr_fwd(lnk(s.uy, pX, n), phiXY));
     const double P1 = re_trace_mul(d1, d1), P2 = re_trace_mul(d2, d2);
     const double P3 = re_trace_mul(d3, d3), P4 = re_trace_mul(d4, d4);
     const double ht = 0.5 / tau / tau;
@@ -160,20 +197,20 @@ __device__ __forceinline__ OffdiagGeom offdiag_geom(int N, size_t pos) {
     return G;
 }
 
-template <int PART>
+template <int PART, typename S>
 __global__ void __launch_bounds__(128) k_tmunu_offdiag(TmunuArgs A) {
     const int N = A.N;
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (pos >= n) return;
     const OffdiagGeom G = offdiag_geom(N, pos);
-    const State<double> &s = A.s;
+    const State<S> &s = state_of<S>(A);
     const double g = A.g, tau = A.tau;
     const double a4 = pow(A.a, 4.), a5 = pow(A.a, 5.);
 
     if constexpr (PART == 0 || PART == 2) {
-        const M3<double> Ux = ld_m3(s.ux, pos, n), Uy = ld_m3(s.uy, pos, n);
-        const M3<double> UxpY = ld_m3(s.ux, G.pY, n), UypX = ld_m3(s.uy, G.pX, n);
+        const M3<double> Ux = lnk(s.ux, pos, n), Uy = lnk(s.uy, pos, n);
+        const M3<double> UxpY = lnk(s.ux, G.pY, n), UypX = lnk(s.uy, G.pX, n);
         // Pb = Ux UypX UxpY^dag Uy^dag   (plaquette at pos)
         const M3<double> ahPb = ah(mul_nd(mul(Ux, UypX), mul(Uy, UxpY)));
         M3<double> K, Kp;
@@ -181,15 +218,15 @@ __global__ void __launch_bounds__(128) k_tmunu_offdiag(TmunuArgs A) {
             {
                 // Q1 = UxmX^dag UymX UxmXpY Uy^dag
                 const M3<double> q1 = mul_nd(
-                    mul(mul_dn(ld_m3(s.ux, G.mX, n), ld_m3(s.uy, G.mX, n)), ld_m3(s.ux, G.mXpY, n)),
+                    mul(mul_dn(lnk(s.ux, G.mX, n), lnk(s.uy, G.mX, n)), lnk(s.ux, G.mXpY, n)),
                     Uy);
                 K = ah(q1);
                 sub_from(K, ahPb);
             }
             {
                 // R1 = UypX UxpXpY Uyp2X^dag UxpX^dag ; S1 = Ux^dag Uy UxpY UypX^dag
-                const M3<double> r1 = mul_nd(mul(UypX, ld_m3(s.ux, G.pXY, n)),
-                                             mul(ld_m3(s.ux, G.pX, n), ld_m3(s.uy, G.p2X, n)));
+                const M3<double> r1 = mul_nd(mul(UypX, lnk(s.ux, G.pXY, n)),
+                                             mul(lnk(s.ux, G.pX, n), lnk(s.uy, G.p2X, n)));
                 const M3<double> s1 = mul_nd(mul(mul_dn(Ux, Uy), UxpY), UypX);
                 Kp = ah(r1);
                 add_to(Kp, ah(s1));
@@ -198,15 +235,15 @@ __global__ void __launch_bounds__(128) k_tmunu_offdiag(TmunuArgs A) {
             {
                 // Q3 = UymY^dag UxmY UypXmY Ux^dag
                 const M3<double> q3 = mul_nd(
-                    mul(mul_dn(ld_m3(s.uy, G.mY, n), ld_m3(s.ux, G.mY, n)), ld_m3(s.uy, G.pXmY, n)),
+                    mul(mul_dn(lnk(s.uy, G.mY, n), lnk(s.ux, G.mY, n)), lnk(s.uy, G.pXmY, n)),
                     Ux);
                 K = ah(q3);
                 add_to(K, ahPb);
             }
             {
                 // R3 = UxpY UypXpY Uxp2Y^dag UypY^dag ; S3 = Uy^dag Ux UypX UxpY^dag
-                const M3<double> r3 = mul_nd(mul(UxpY, ld_m3(s.uy, G.pXY, n)),
-                                             mul(ld_m3(s.uy, G.pY, n), ld_m3(s.ux, G.p2Y, n)));
+                const M3<double> r3 = mul_nd(mul(UxpY, lnk(s.uy, G.pXY, n)),
+                                             mul(lnk(s.uy, G.pY, n), lnk(s.ux, G.p2Y, n)));
                 const M3<double> s3 = mul_nd(mul(mul_dn(Uy, Ux), UypX), UxpY);
                 Kp = ah(r3);
                 add_to(Kp, ah(s3));
@@ -214,7 +251,7 @@ __global__ void __launch_bounds__(128) k_tmunu_offdiag(TmunuArgs A) {
         }
         // magnetic part of T^taud: Im tr(E K + E' K') with E = E2 (x) or E1 (y)
         {
-            const double *Ep = PART == 0 ? s.e2 : s.e1;
+            const S *Ep = PART == 0 ? s.e2 : s.e1;
             M3<double> c = mul(hm8(Ep, pos, n), K);
             add_to(c, mul(hm8(Ep, PART == 0 ? G.pX : G.pY, n), Kp));
             A.T10[(PART == 0 ? 4 : 5) * n + pos] = trace(c).i;
@@ -239,20 +276,20 @@ __global__ void __launch_bounds__(128) k_tmunu_offdiag(TmunuArgs A) {
     } else if constexpr (PART == 1 || PART == 3) {
         const M3<double> pi = hm(s.pi, pos, n), piX = hm(s.pi, G.pX, n);
         const M3<double> piY = hm(s.pi, G.pY, n), piXY = hm(s.pi, G.pXY, n);
-        const M3<double> Ux = ld_m3(s.ux, pos, n), Uy = ld_m3(s.uy, pos, n);
-        const M3<double> UxpY = ld_m3(s.ux, G.pY, n), UypX = ld_m3(s.uy, G.pX, n);
+        const M3<double> Ux = lnk(s.ux, pos, n), Uy = lnk(s.uy, pos, n);
+        const M3<double> UxpY = lnk(s.ux, G.pY, n), UypX = lnk(s.uy, G.pX, n);
         const M3<double> phi = hm(s.phi, pos, n), phiX = hm(s.phi, G.pX, n);
         const M3<double> phiY = hm(s.phi, G.pY, n), phiXY = hm(s.phi, G.pXY, n);
         if constexpr (PART == 1) {
             // T^taux
             const double mag = A.T10[4 * n + pos];
             M3<double> t = mul(pi, minus(tr_fwd(Ux, phiX),
-                                         tr_bwd(ld_m3(s.ux, G.mX, n), hm(s.phi, G.mX, n))));
+                                         tr_bwd(lnk(s.ux, G.mX, n), hm(s.phi, G.mX, n))));
             add_to(t, mul(piY, minus(tr_fwd(UxpY, phiXY),
-                                     tr_bwd(ld_m3(s.ux, G.mXpY, n), hm(s.phi, G.mXpY, n)))));
-            add_to(t, mul(piX, minus(tr_fwd(ld_m3(s.ux, G.pX, n), hm(s.phi, G.p2X, n)),
+                                     tr_bwd(lnk(s.ux, G.mXpY, n), hm(s.phi, G.mXpY, n)))));
+            add_to(t, mul(piX, minus(tr_fwd(lnk(s.ux, G.pX, n), hm(s.phi, G.p2X, n)),
                                      tr_bwd(Ux, phi))));
-            add_to(t, mul(piXY, minus(tr_fwd(ld_m3(s.ux, G.pXY, n), hm(s.phi, G.p2XY, n)),
+            add_to(t, mul(piXY, minus(tr_fwd(lnk(s.ux, G.pXY, n), hm(s.phi, G.p2XY, n)),
                                       tr_bwd(UxpY, phiY))));
             const double el = trace(t).r;
             A.T10[4 * n + pos] = (2. / tau / 8. * mag - 2. / 8. / tau * el) / a4;
@@ -269,12 +306,12 @@ __global__ void __launch_bounds__(128) k_tmunu_offdiag(TmunuArgs A) {
             // T^tauy
             const double mag = A.T10[5 * n + pos];
             M3<double> t = mul(pi, minus(tr_fwd(Uy, phiY),
-                                         tr_bwd(ld_m3(s.uy, G.mY, n), hm(s.phi, G.mY, n))));
+                                         tr_bwd(lnk(s.uy, G.mY, n), hm(s.phi, G.mY, n))));
             add_to(t, mul(piX, minus(tr_fwd(UypX, phiXY),
-                                     tr_bwd(ld_m3(s.uy, G.pXmY, n), hm(s.phi, G.pXmY, n)))));
-            add_to(t, mul(piY, minus(tr_fwd(ld_m3(s.uy, G.pY, n), hm(s.phi, G.p2Y, n)),
+                                     tr_bwd(lnk(s.uy, G.pXmY, n), hm(s.phi, G.pXmY, n)))));
+            add_to(t, mul(piY, minus(tr_fwd(lnk(s.uy, G.pY, n), hm(s.phi, G.p2Y, n)),
                                      tr_bwd(Uy, phi))));
-            add_to(t, mul(piXY, minus(tr_fwd(ld_m3(s.uy, G.pXY, n), hm(s.phi, G.pX2Y, n)),
+            add_to(t, mul(piXY, minus(tr_fwd(lnk(s.uy, G.pXY, n), hm(s.phi, G.pX2Y, n)),
                                       tr_bwd(UypX, phiX))));
             const double el = trace(t).r;
             A.T10[5 * n + pos] = (2. / tau / 8. * mag - 2. / 8. / tau * el) / a4;
@@ -289,8 +326,8 @@ __global__ void __launch_bounds__(128) k_tmunu_offdiag(TmunuArgs A) {
             A.T10[9 * n + pos] = (-2. / tau / tau * v) / a5;
         }
     } else {
-        const M3<double> Ux = ld_m3(s.ux, pos, n), Uy = ld_m3(s.uy, pos, n);
-        const M3<double> UxpY = ld_m3(s.ux, G.pY, n), UypX = ld_m3(s.uy, G.pX, n);
+        const M3<double> Ux = lnk(s.ux, pos, n), Uy = lnk(s.uy, pos, n);
+        const M3<double> UxpY = lnk(s.ux, G.pY, n), UypX = lnk(s.uy, G.pX, n);
         const M3<double> phi = hm(s.phi, pos, n), phiX = hm(s.phi, G.pX, n);
         const M3<double> phiY = hm(s.phi, G.pY, n), phiXY = hm(s.phi, G.pXY, n);
         const M3<double> dX = minus(tr_fwd(Ux, phiX), phi), dY = minus(tr_fwd(Uy, phiY), phi);
@@ -326,19 +363,30 @@ __global__ void __launch_bounds__(128) k_tmunu_offdiag(TmunuArgs A) {
 
 void launch_tmunu_diag(const TmunuArgs &a, cudaStream_t st) {
     const size_t n = (size_t)a.N * a.N;
-    k_tmunu_diag<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a);
+    if (a.from32)
+        k_tmunu_diag<float><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a);
+    else
+        k_tmunu_diag<double><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a);
+}
+
+template <typename S>
+static void launch_tmunu_t(const TmunuArgs &a, cudaStream_t st) {
+    const size_t n = (size_t)a.N * a.N;
+    const unsigned b = (unsigned)((n + 127) / 128);
+    k_tmunu_diag<S><<<b, 128, 0, st>>>(a);
+    k_tmunu_offdiag<0, S><<<b, 128, 0, st>>>(a);
+    k_tmunu_offdiag<1, S><<<b, 128, 0, st>>>(a);
+    k_tmunu_offdiag<2, S><<<b, 128, 0, st>>>(a);
+    k_tmunu_offdiag<3, S><<<b, 128, 0, st>>>(a);
+    k_tmunu_offdiag<4, S><<<b, 128, 0, st>>>(a);
+    k_tmunu_offdiag<5, S><<<b, 128, 0, st>>>(a);
 }
 
 void launch_tmunu(const TmunuArgs &a, cudaStream_t st) {
-    const size_t n = (size_t)a.N * a.N;
-    k_tmunu_diag<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(a);
-    const unsigned b = (unsigned)((n + 127) / 128);
-    k_tmunu_offdiag<0><<<b, 128, 0, st>>>(a);
-    k_tmunu_offdiag<1><<<b, 128, 0, st>>>(a);
-    k_tmunu_offdiag<2><<<b, 128, 0, st>>>(a);
-    k_tmunu_offdiag<3><<<b, 128, 0, st>>>(a);
-    k_tmunu_offdiag<4><<<b, 128, 0, st>>>(a);
-    k_tmunu_offdiag<5><<<b, 128, 0, st>>>(a);
+    if (a.from32)
+        launch_tmunu_t<float>(a, st);
+    else
+        launch_tmunu_t<double>(a, st);
 }
 
 }  // namespace ipg
