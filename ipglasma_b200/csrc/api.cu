@@ -518,8 +518,7 @@ ipg_status observables_enqueue(ipg_ctx *c) {
     ta.a = c->a;
     ta.s = c->s64;
     ta.T10 = c->T10;
-    // FP32 contexts: T^munu reads the FP32 state directly (the FP64 copy is
-    // made once, after the last half step, for the Gauss law and unitarity)
+    // FP32 contexts: T^munu reads the FP32 state directly
     ta.from32 = is_fp32(c) ? 1 : 0;
     ta.s32 = c->s32;
     launch_tmunu(ta, c->stream);
@@ -545,11 +544,17 @@ ipg_status observables_enqueue(ipg_ctx *c) {
 
     IPG_TRY(step(c, itmax * dtau, dtau / 2., dtau, 1, 0));
     c->it = itmax;
-    IPG_TRY(state64(c));
-    launch_gauss_law(N, c->s64, c->partial, scal + 32, c->stream);
-    IPG_LAUNCHED(c, 2);
-    launch_unitarity(N, c->s64.ux, c->s64.uy, c->partial, scal + 33, c->stream);
-    IPG_LAUNCHED(c, 2);
+    // the checks read the live state; on FP32 contexts the FP64 copy is made
+    // only where a caller asks for FP64 fields (ipg_get_field, the gauge
+    // fixing and the spectrum)
+    if (is_fp32(c)) {
+        launch_gauss_law(N, c->s32, c->partial, scal + 32, c->stream);
+        launch_unitarity(N, c->s32.ux, c->s32.uy, c->partial, scal + 33, c->stream);
+    } else {
+        launch_gauss_law(N, c->s64, c->partial, scal + 32, c->stream);
+        launch_unitarity(N, c->s64.ux, c->s64.uy, c->partial, scal + 33, c->stream);
+    }
+    IPG_LAUNCHED(c, 4);
     launch_cell_flags(n, c->found, c->eps, c->partial, scal + 36, c->stream);
     IPG_LAUNCHED(c, 2);
     IPG_CUDA(c, cudaMemcpyAsync(c->h_scal, scal, sizeof(double) * 39,

@@ -100,4 +100,37 @@ __device__ __forceinline__ void st_h8(T *__restrict__ p, size_t pos, size_t n,
     p[7 * n + pos] = h.o12.i;
 }
 
+// FP64 views of either form's stored state, for the observables and checks:
+// fields widened on load, and links as stored (FP64 form) or formed as
+// 1 + W in FP64 from the FP32 form's deviation storage W = U - 1 (the values
+// an FP64 copy of the state holds)
+__device__ __forceinline__ H3<double> widen_h(const H3<float> &h) {
+    return {h.d0, h.d1, h.d2, {h.o01.r, h.o01.i}, {h.o02.r, h.o02.i}, {h.o12.r, h.o12.i}};
+}
+__device__ __forceinline__ H3<double> h64(const double *p, size_t pos, size_t n) {
+    return ld_h(p, pos, n);
+}
+__device__ __forceinline__ H3<double> h64(const float *p, size_t pos, size_t n) {
+    return widen_h(ld_h(p, pos, n));
+}
+__device__ __forceinline__ H3<double> h8_64(const double *p, size_t pos, size_t n) {
+    return ld_h8(p, pos, n);
+}
+__device__ __forceinline__ H3<double> h8_64(const float *p, size_t pos, size_t n) {
+    return widen_h(ld_h8(p, pos, n));
+}
+__device__ __forceinline__ M3<double> link64(const C<double> *p, size_t pos, size_t n) {
+    return ld_m3(p, pos, n);
+}
+__device__ __forceinline__ M3<double> link64(const C<float> *p, size_t pos, size_t n) {
+    const M3<float> w = ld_m3(p, pos, n);
+    M3<double> u;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const double shift = (k == 0 || k == 4 || k == 8) ? 1.0 : 0.0;
+        u.m[k] = {(double)w.m[k].r + shift, (double)w.m[k].i};
+    }
+    return u;
+}
+
 }  // namespace ipg

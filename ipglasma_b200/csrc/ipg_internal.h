@@ -383,10 +383,13 @@ struct Reductions {
     double etot;
 };
 // d_partial needs ceil(N*N/256) * 18 doubles
-void launch_gauss_law(int N, const State<double> &s, double *d_partial,
+// (S = float: the FP32 form's state read directly, links as 1 + W, in FP64)
+template <typename S>
+void launch_gauss_law(int N, const State<S> &s, double *d_partial, double *d_out,
+                      cudaStream_t st);
+template <typename S>
+void launch_unitarity(int N, const C<S> *ux, const C<S> *uy, double *d_partial,
                       double *d_out, cudaStream_t st);
-void launch_unitarity(int N, const C<double> *ux, const C<double> *uy,
-                      double *d_partial, double *d_out, cudaStream_t st);
 // sums1[5] = {sum x w, sum y w, sum w, sum T^tautau, sum eps},
 // sums2[18] = radial moments (see reduce.cu)
 void launch_eccentricity(int N, double L, double a, const double *eps,

@@ -47,31 +47,16 @@ __device__ __forceinline__ M3<double> hm8(const double *p, size_t pos,
                                           size_t n) {
     return from_h(ld_h8(p, pos, n));
 }
-__device__ __forceinline__ H3<double> widen(const H3<float> &h) {
-    return {h.d0, h.d1, h.d2, {h.o01.r, h.o01.i}, {h.o02.r, h.o02.i}, {h.o12.r, h.o12.i}};
-}
-// the FP32 form's fields, widened to FP64 on load (the values an FP64 copy
-// of the state would hold)
+// the FP32 form's fields, widened to FP64 on load (fields.cuh)
 __device__ __forceinline__ M3<double> hm(const float *p, size_t pos, size_t n) {
-    return from_h(widen(ld_h(p, pos, n)));
+    return from_h(h64(p, pos, n));
 }
 __device__ __forceinline__ M3<double> hm8(const float *p, size_t pos, size_t n) {
-    return from_h(widen(ld_h8(p, pos, n)));
+    return from_h(h8_64(p, pos, n));
 }
-// a link: FP64 as stored; FP32 form stored as W = U - 1, here 1 + W formed in
-// FP64 as the state conversion forms it
-__device__ __forceinline__ M3<double> lnk(const C<double> *p, size_t pos, size_t n) {
-    return ld_m3(p, pos, n);
-}
-__device__ __forceinline__ M3<double> lnk(const C<float> *p, size_t pos, size_t n) {
-    const M3<float> w = ld_m3(p, pos, n);
-    M3<double> u;
-#pragma unroll
-    for (int k = 0; k < 9; k++) {
-        const double shift = (k == 0 || k == 4 || k == 8) ? 1.0 : 0.0;
-        u.m[k] = {(double)w.m[k].r + shift, (double)w.m[k].i};
-    }
-    return u;
+template <typename L>
+__device__ __forceinline__ M3<double> lnk(const L *p, size_t pos, size_t n) {
+    return link64(p, pos, n);
 }
 template <typename S>
 __device__ __forceinline__ const State<S> &state_of(const TmunuArgs &A);

@@ -75,20 +75,21 @@ __global__ void k_fold(const double *partial, double *out, unsigned max_mask) {
 // Gauss law: G = UxXm1^dag E1(x-1) UxXm1 - E1 + UyYm1^dag E2(y-1) UyYm1 - E2
 //               - i (phi pi - pi phi);  max over sites of |G|^2 / 2
 // --------------------------------------------------------------------------
-__global__ void __launch_bounds__(RB) k_gauss(int N, State<double> s, double *partial) {
+template <typename S>
+__global__ void __launch_bounds__(RB) k_gauss(int N, State<S> s, double *partial) {
     const size_t n = (size_t)N * N;
     double val = 0.;
     GRID_STRIDE(pos, n) {
         const int ix = (int)(pos / N), iy = (int)(pos % N);
         const size_t mX = (size_t)max(0, ix - 1) * N + iy;
         const size_t mY = (size_t)ix * N + max(0, iy - 1);
-        M3<double> G = mul(mul_dn(ld_m3(s.ux, mX, n), from_h(ld_h8(s.e1, mX, n))),
-                           ld_m3(s.ux, mX, n));
-        sub_from(G, from_h(ld_h8(s.e1, pos, n)));
-        add_to(G, mul(mul_dn(ld_m3(s.uy, mY, n), from_h(ld_h8(s.e2, mY, n))),
-                      ld_m3(s.uy, mY, n)));
-        sub_from(G, from_h(ld_h8(s.e2, pos, n)));
-        const M3<double> ph = from_h(ld_h(s.phi, pos, n)), pi = from_h(ld_h(s.pi, pos, n));
+        M3<double> G = mul(mul_dn(link64(s.ux, mX, n), from_h(h8_64(s.e1, mX, n))),
+                           link64(s.ux, mX, n));
+        sub_from(G, from_h(h8_64(s.e1, pos, n)));
+        add_to(G, mul(mul_dn(link64(s.uy, mY, n), from_h(h8_64(s.e2, mY, n))),
+                      link64(s.uy, mY, n)));
+        sub_from(G, from_h(h8_64(s.e2, pos, n)));
+        const M3<double> ph = from_h(h64(s.phi, pos, n)), pi = from_h(h64(s.pi, pos, n));
         const M3<double> c = minus(mul(ph, pi), mul(pi, ph));
 #pragma unroll
         for (int k = 0; k < 9; k++) {  // - i c
@@ -103,22 +104,28 @@ __global__ void __launch_bounds__(RB) k_gauss(int N, State<double> s, double *pa
     block_max(val, partial + blockIdx.x);
 }
 
-void launch_gauss_law(int N, const State<double> &s, double *d_partial,
-                      double *d_out, cudaStream_t st) {
-    k_gauss<<<RG, RB, 0, st>>>(N, s, d_partial);
+template <typename S>
+void launch_gauss_law(int N, const State<S> &s, double *d_partial, double *d_out,
+                      cudaStream_t st) {
+    k_gauss<S><<<RG, RB, 0, st>>>(N, s, d_partial);
     k_fold<1><<<1, 32, 0, st>>>(d_partial, d_out, 1u);
 }
+template void launch_gauss_law<double>(int, const State<double> &, double *, double *,
+                                       cudaStream_t);
+template void launch_gauss_law<float>(int, const State<float> &, double *, double *,
+                                      cudaStream_t);
 
 // --------------------------------------------------------------------------
 // max over links of the largest |(U^dag U - 1)_ij|
 // --------------------------------------------------------------------------
-__global__ void __launch_bounds__(RB) k_unitarity(int N, const C<double> *ux,
-                                                  const C<double> *uy, double *partial) {
+template <typename S>
+__global__ void __launch_bounds__(RB) k_unitarity(int N, const C<S> *ux, const C<S> *uy,
+                                                  double *partial) {
     const size_t n = (size_t)N * N;
     double val = 0.;
     GRID_STRIDE(pos, n) {
         for (int d = 0; d < 2; d++) {
-            const M3<double> u = ld_m3(d ? uy : ux, pos, n);
+            const M3<double> u = link64(d ? uy : ux, pos, n);
             M3<double> p = mul_dn(u, u);
             p.m[0].r -= 1.;
             p.m[4].r -= 1.;
@@ -131,11 +138,16 @@ __global__ void __launch_bounds__(RB) k_unitarity(int N, const C<double> *ux,
     block_max(val, partial + blockIdx.x);
 }
 
-void launch_unitarity(int N, const C<double> *ux, const C<double> *uy,
-                      double *d_partial, double *d_out, cudaStream_t st) {
-    k_unitarity<<<RG, RB, 0, st>>>(N, ux, uy, d_partial);
+template <typename S>
+void launch_unitarity(int N, const C<S> *ux, const C<S> *uy, double *d_partial,
+                      double *d_out, cudaStream_t st) {
+    k_unitarity<S><<<RG, RB, 0, st>>>(N, ux, uy, d_partial);
     k_fold<1><<<1, 32, 0, st>>>(d_partial, d_out, 1u);
 }
+template void launch_unitarity<double>(int, const C<double> *, const C<double> *, double *,
+                                       double *, cudaStream_t);
+template void launch_unitarity<float>(int, const C<float> *, const C<float> *, double *,
+                                      double *, cudaStream_t);
 
 // --------------------------------------------------------------------------
 // eccentricities
