@@ -391,7 +391,10 @@ struct LandauCell {
     int wrote;
 };
 
-__global__ void k_landau(LandauArgs A, double *carry, int *wrote) {
+// (128, 4): 128 registers without spilling (138 unbounded), four blocks an SM
+// instead of three; the solver's arrays live in local memory either way, and
+// the extra warps hide its latency (same bits)
+__global__ void __launch_bounds__(128, 4) k_landau(LandauArgs A, double *carry, int *wrote) {
     const int N = A.N;
     const size_t n = (size_t)N * N;
     const size_t pos = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
