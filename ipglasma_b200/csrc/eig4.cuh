@@ -166,11 +166,18 @@ __device__ int eig4_qr(double h[4][4], double er[4], double ei[4]) {
     return total;
 }
 
-__device__ void eig4_nullvec(const double a[16], double lr, double li,
-                             double vr[4], double vi[4]) {
+// Every index below is a compile-time constant after unrolling (the pivot
+// rows and columns are applied by selects over the candidates, the rank by
+// guards), so the 4 x 4 complex work matrix and the vector stay in
+// registers instead of local memory; the arithmetic and its order are those
+// of plain complete-pivoting elimination.
+__device__ __forceinline__ void eig4_nullvec(const double a[16], double lr, double li,
+                                             double vr[4], double vi[4]) {
     double mr[4][4], mi[4][4], yr[4], yi[4], scale = 0.0;
     int cp[4], rank = 3;
+#pragma unroll
     for (int i = 0; i < 4; i++)
+#pragma unroll
         for (int j = 0; j < 4; j++) {
             mr[i][j] = a[4 * i + j] - (i == j ? lr : 0.0);
             mi[i][j] = (i == j ? -li : 0.0);
@@ -178,11 +185,17 @@ __device__ void eig4_nullvec(const double a[16], double lr, double li,
                 scale = fabs(mr[i][j]) + fabs(mi[i][j]);
         }
     const double tol2 = (64.0 * DBL_EPSILON * scale) * (64.0 * DBL_EPSILON * scale);
+#pragma unroll
     for (int j = 0; j < 4; j++) cp[j] = j;
+    bool stop = false;
+#pragma unroll
     for (int k = 0; k < 3; k++) {
+        if (stop) continue;
         int pi = k, pj = k;
         double best = -1.0;
+#pragma unroll
         for (int i = k; i < 4; i++)
+#pragma unroll
             for (int j = k; j < 4; j++) {
                 const double m2 = mr[i][j] * mr[i][j] + mi[i][j] * mi[i][j];
                 if (m2 > best) {
@@ -193,34 +206,45 @@ __device__ void eig4_nullvec(const double a[16], double lr, double li,
             }
         if (best <= tol2) {
             rank = k;
-            break;
+            stop = true;
+            continue;
         }
-        if (pi != k)
-            for (int j = 0; j < 4; j++) {
-                double t = mr[k][j];
-                mr[k][j] = mr[pi][j];
-                mr[pi][j] = t;
-                t = mi[k][j];
-                mi[k][j] = mi[pi][j];
-                mi[pi][j] = t;
+        // row k <-> row pi
+#pragma unroll
+        for (int r = k + 1; r < 4; r++)
+            if (pi == r)
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    double t = mr[k][j];
+                    mr[k][j] = mr[r][j];
+                    mr[r][j] = t;
+                    t = mi[k][j];
+                    mi[k][j] = mi[r][j];
+                    mi[r][j] = t;
+                }
+        // column k <-> column pj, and the unknowns' order with it
+#pragma unroll
+        for (int c = k + 1; c < 4; c++)
+            if (pj == c) {
+                const int t = cp[k];
+                cp[k] = cp[c];
+                cp[c] = t;
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    double u = mr[i][k];
+                    mr[i][k] = mr[i][c];
+                    mr[i][c] = u;
+                    u = mi[i][k];
+                    mi[i][k] = mi[i][c];
+                    mi[i][c] = u;
+                }
             }
-        if (pj != k) {
-            const int t = cp[k];
-            cp[k] = cp[pj];
-            cp[pj] = t;
-            for (int i = 0; i < 4; i++) {
-                double s = mr[i][k];
-                mr[i][k] = mr[i][pj];
-                mr[i][pj] = s;
-                s = mi[i][k];
-                mi[i][k] = mi[i][pj];
-                mi[i][pj] = s;
-            }
-        }
         const double dr = mr[k][k], di = mi[k][k], den = dr * dr + di * di;
+#pragma unroll
         for (int i = k + 1; i < 4; i++) {
             const double fr = (mr[i][k] * dr + mi[i][k] * di) / den;
             const double fi = (mi[i][k] * dr - mr[i][k] * di) / den;
+#pragma unroll
             for (int j = k; j < 4; j++) {
                 const double pr = fr * mr[k][j] - fi * mi[k][j];
                 const double pim = fr * mi[k][j] + fi * mr[k][j];
@@ -229,14 +253,18 @@ __device__ void eig4_nullvec(const double a[16], double lr, double li,
             }
         }
     }
+#pragma unroll
     for (int j = 0; j < 4; j++) {
         yr[j] = 0.0;
         yi[j] = 0.0;
     }
     yr[3] = 1.0;
-    for (int i = rank - 1; i >= 0; i--) {
+#pragma unroll
+    for (int i = 2; i >= 0; i--) {
+        if (i >= rank) continue;
         double sr = 0.0, si = 0.0;
         const double dr = mr[i][i], di = mi[i][i];
+#pragma unroll
         for (int j = i + 1; j < 4; j++) {
             sr += mr[i][j] * yr[j] - mi[i][j] * yi[j];
             si += mr[i][j] * yi[j] + mi[i][j] * yr[j];
@@ -245,12 +273,15 @@ __device__ void eig4_nullvec(const double a[16], double lr, double li,
         yr[i] = -(sr * dr + si * di) / den;
         yi[i] = -(si * dr - sr * di) / den;
     }
-    for (int j = 0; j < 4; j++) {
-        vr[cp[j]] = yr[j];
-        vi[cp[j]] = yi[j];
+    // v[cp[j]] = y[j]
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        vr[t] = cp[0] == t ? yr[0] : cp[1] == t ? yr[1] : cp[2] == t ? yr[2] : yr[3];
+        vi[t] = cp[0] == t ? yi[0] : cp[1] == t ? yi[1] : cp[2] == t ? yi[2] : yi[3];
     }
     double n2 = 0.0, best = -1.0;
     int m = 0;
+#pragma unroll
     for (int j = 0; j < 4; j++) {
         const double m2 = vr[j] * vr[j] + vi[j] * vi[j];
         n2 += m2;
@@ -260,14 +291,16 @@ __device__ void eig4_nullvec(const double a[16], double lr, double li,
         }
     }
     const double inv = 1.0 / (sqrt(n2) * sqrt(best));
-    const double pr = vr[m] * inv, pim = -vi[m] * inv;
+    const double vrm = m == 0 ? vr[0] : m == 1 ? vr[1] : m == 2 ? vr[2] : vr[3];
+    const double vim = m == 0 ? vi[0] : m == 1 ? vi[1] : m == 2 ? vi[2] : vi[3];
+    const double pr = vrm * inv, pim = -vim * inv;
+#pragma unroll
     for (int j = 0; j < 4; j++) {
         const double r = vr[j] * pr - vi[j] * pim;
         const double s = vr[j] * pim + vi[j] * pr;
         vr[j] = r;
-        vi[j] = s;
+        vi[j] = j == m ? 0.0 : s;
     }
-    vi[m] = 0.0;
 }
 
 __device__ int eig4(const double a[16], double er[4], double ei[4],
@@ -283,6 +316,7 @@ __device__ int eig4(const double a[16], double er[4], double ei[4],
             ei[i] = 0.0;
         }
     }
+#pragma unroll
     for (int i = 0; i < 4; i++) eig4_nullvec(a, er[i], ei[i], vr + 4 * i, vi + 4 * i);
     return status;
 }

@@ -391,9 +391,11 @@ struct LandauCell {
     int wrote;
 };
 
-// (128, 4): 128 registers without spilling (138 unbounded), four blocks an SM
-// instead of three; the solver's arrays live in local memory either way, and
-// the extra warps hide its latency (same bits)
+// (128, 4): four blocks an SM. The null-vector elimination keeps its matrix
+// in registers (eig4_nullvec), the QR iteration's Hessenberg matrix stays in
+// local memory (its active block moves at run time); at 128 registers part
+// of the rest spills, which the extra warps hide (188 registers unbounded,
+// two blocks an SM, was slower)
 __global__ void __launch_bounds__(128, 4) k_landau(LandauArgs A, double *carry, int *wrote) {
     const int N = A.N;
     const size_t n = (size_t)N * N;
@@ -418,9 +420,11 @@ __global__ void __launch_bounds__(128, 4) k_landau(LandauArgs A, double *carry, 
     double cell_eps = Ttt, cu[4] = {1., 0., 0., 0.};
     int found = 0;
     const double tau2 = A.tau2_fm;  // a*it*dtau*a*it*dtau
+#pragma unroll
     for (int i = 0; i < 4; i++) {
         // square and Euclidean square of the eigenvector (complex products)
         double sqr = 0., sqi = 0., eur = 0., eui = 0.;
+#pragma unroll
         for (int j = 0; j < 4; j++) {
             const double zr = vr[4 * i + j], zi = vi[4 * i + j];
             const double z2r = zr * zr - zi * zi, z2i = zr * zi + zi * zr;
@@ -446,6 +450,7 @@ __global__ void __launch_bounds__(128, 4) k_landau(LandauArgs A, double *carry, 
                 eps = Ttt;
         }
         double s2 = 0.;
+#pragma unroll
         for (int j = 0; j < 4; j++) {
             const double zr = vr[4 * i + j] * factor, zi = vi[4 * i + j] * factor;
             const double z2r = zr * zr - zi * zi;
@@ -461,7 +466,8 @@ __global__ void __launch_bounds__(128, 4) k_landau(LandauArgs A, double *carry, 
         if (s2 > 0) {
             found += 1;
             int change = 0;
-            for (int j = 0; j < 4; j++) {
+    #pragma unroll
+        for (int j = 0; j < 4; j++) {
                 double zr = vr[4 * i + j] * factor, zi = vi[4 * i + j] * factor;
                 if (j == 0 && zr < 0) {
                     change = 1;
