@@ -24,26 +24,36 @@ __device__ __forceinline__ void eig4_hessenberg(double h[4][4]) {
 #pragma unroll
     for (int k = 0; k < 2; k++) {
         double v[4] = {0, 0, 0, 0}, nrm2 = 0.0;
+#pragma unroll
         for (int i = k + 1; i < 4; i++) nrm2 += h[i][k] * h[i][k];
         if (nrm2 == 0.0) continue;
         const double alpha = (h[k + 1][k] >= 0.0 ? -1.0 : 1.0) * sqrt(nrm2);
+#pragma unroll
         for (int i = k + 1; i < 4; i++) v[i] = h[i][k];
         v[k + 1] -= alpha;
         double vtv = 0.0;
+#pragma unroll
         for (int i = k + 1; i < 4; i++) vtv += v[i] * v[i];
         if (vtv == 0.0) continue;
+#pragma unroll
         for (int j = 0; j < 4; j++) {
             double d = 0.0;
+#pragma unroll
             for (int i = k + 1; i < 4; i++) d += v[i] * h[i][j];
             d *= 2.0 / vtv;
+#pragma unroll
             for (int i = k + 1; i < 4; i++) h[i][j] -= d * v[i];
         }
+#pragma unroll
         for (int i = 0; i < 4; i++) {
             double d = 0.0;
+#pragma unroll
             for (int j = k + 1; j < 4; j++) d += h[i][j] * v[j];
             d *= 2.0 / vtv;
+#pragma unroll
             for (int j = k + 1; j < 4; j++) h[i][j] -= d * v[j];
         }
+#pragma unroll
         for (int i = k + 2; i < 4; i++) h[i][k] = 0.0;
     }
 }
@@ -51,11 +61,14 @@ __device__ __forceinline__ void eig4_hessenberg(double h[4][4]) {
 __device__ __forceinline__ int eig4_reflector(int len, const double *x,
                                               double *v, double *beta) {
     double nrm2 = 0.0, vtv = 0.0;
+#pragma unroll
     for (int i = 0; i < len; i++) nrm2 += x[i] * x[i];
     if (nrm2 == 0.0) return 0;
     const double alpha = (x[0] >= 0.0 ? -1.0 : 1.0) * sqrt(nrm2);
+#pragma unroll
     for (int i = 0; i < len; i++) v[i] = x[i];
     v[0] -= alpha;
+#pragma unroll
     for (int i = 0; i < len; i++) vtv += v[i] * v[i];
     if (vtv == 0.0) return 0;
     *beta = 2.0 / vtv;
@@ -65,101 +78,158 @@ __device__ __forceinline__ int eig4_reflector(int len, const double *x,
 __device__ __forceinline__ void eig4_apply(double h[4][4], int len, int r0,
                                            const double *v, double beta, int lo,
                                            int hi, int cfirst, int rlast) {
+#pragma unroll
     for (int j = cfirst; j <= hi; j++) {
         double d = 0.0;
+#pragma unroll
         for (int i = 0; i < len; i++) d += v[i] * h[r0 + i][j];
         d *= beta;
+#pragma unroll
         for (int i = 0; i < len; i++) h[r0 + i][j] -= d * v[i];
     }
+#pragma unroll
     for (int i = lo; i <= rlast; i++) {
         double d = 0.0;
+#pragma unroll
         for (int j = 0; j < len; j++) d += h[i][r0 + j] * v[j];
         d *= beta;
+#pragma unroll
         for (int j = 0; j < len; j++) h[i][r0 + j] -= d * v[j];
     }
 }
 
+// The QR iteration's active block [lo, hi] moves at run time; it is
+// dispatched to code specialised for each (lo, hi) a 4 x 4 matrix can have, so
+// every index into h, er and ei is a compile-time constant and the matrix
+// stays in registers. The arithmetic and its order are those of the
+// textbook iteration.
+
+// deflation scan from HI down: the first negligible subdiagonal entry is set
+// to zero and bounds the active block from below
+template <int HI>
+__device__ __forceinline__ int eig4_find_lo(double h[4][4], double anorm) {
+    int lo = HI;
+    bool found = false;
+#pragma unroll
+    for (int l = HI; l > 0; l--) {
+        if (found) continue;
+        double s = fabs(h[l - 1][l - 1]) + fabs(h[l][l]);
+        if (s == 0.0) s = anorm;
+        if (fabs(h[l][l - 1]) <= DBL_EPSILON * s) {
+            h[l][l - 1] = 0.0;
+            found = true;
+            lo = l;
+        } else {
+            lo = l - 1;
+        }
+    }
+    return lo;
+}
+
+// one Francis double-shift sweep on the unreduced block [LO, HI]
+template <int LO, int HI>
+__device__ __forceinline__ void eig4_sweep(double h[4][4], int its) {
+    double tr, det, x[3], v[3], beta;
+    if (its == 10 || its == 20) {
+        const double w = fabs(h[HI][HI - 1]) + fabs(h[HI - 1][HI - 2]);
+        tr = 1.5 * w;
+        det = w * w;
+    } else {
+        tr = h[HI - 1][HI - 1] + h[HI][HI];
+        det = h[HI - 1][HI - 1] * h[HI][HI] - h[HI - 1][HI] * h[HI][HI - 1];
+    }
+    x[0] = h[LO][LO] * h[LO][LO] + h[LO][LO + 1] * h[LO + 1][LO] - tr * h[LO][LO] + det;
+    x[1] = h[LO + 1][LO] * (h[LO][LO] + h[LO + 1][LO + 1] - tr);
+    x[2] = h[LO + 1][LO] * h[LO + 2][LO + 1];
+#pragma unroll
+    for (int k = LO; k <= HI - 2; k++) {
+        if (k > LO) {
+            x[0] = h[k][k - 1];
+            x[1] = h[k + 1][k - 1];
+            x[2] = h[k + 2][k - 1];
+        }
+        if (eig4_reflector(3, x, v, &beta)) {
+            const int rlast = (k + 3 <= HI) ? k + 3 : HI;
+            eig4_apply(h, 3, k, v, beta, LO, HI, (k > LO ? k - 1 : LO), rlast);
+            if (k > LO) {
+                h[k + 1][k - 1] = 0.0;
+                h[k + 2][k - 1] = 0.0;
+            }
+        }
+    }
+    x[0] = h[HI - 1][HI - 2];
+    x[1] = h[HI][HI - 2];
+    if (eig4_reflector(2, x, v, &beta)) {
+        eig4_apply(h, 2, HI - 1, v, beta, LO, HI, HI - 2, HI);
+        h[HI][HI - 2] = 0.0;
+    }
+}
+
+// the eigenvalues of the 2 x 2 block at rows HI-1, HI
+template <int HI>
+__device__ __forceinline__ void eig4_block2(const double h[4][4], double er[4], double ei[4]) {
+    constexpr int LO = HI - 1;
+    const double a = h[LO][LO], b = h[LO][HI], c = h[HI][LO], d = h[HI][HI];
+    const double half = 0.5 * (a - d);
+    const double disc = half * half + b * c;
+    if (disc >= 0.0) {
+        const double r = sqrt(disc);
+        const double zz = half + (half >= 0.0 ? r : -r);
+        er[LO] = d + zz;
+        er[HI] = (zz != 0.0) ? d - b * c / zz : d + zz;
+        ei[LO] = 0.0;
+        ei[HI] = 0.0;
+    } else {
+        const double r = sqrt(-disc);
+        er[LO] = d + half;
+        er[HI] = d + half;
+        ei[LO] = r;
+        ei[HI] = -r;
+    }
+}
+
 // returns the number of sweeps, or -1 when the sweep limit was reached
-__device__ int eig4_qr(double h[4][4], double er[4], double ei[4]) {
+__device__ __forceinline__ int eig4_qr(double h[4][4], double er[4], double ei[4]) {
     int hi = 3, its = 0, total = 0;
     double anorm = 0.0;
+#pragma unroll
     for (int i = 0; i < 4; i++)
+#pragma unroll
         for (int j = (i > 0 ? i - 1 : 0); j < 4; j++) anorm += fabs(h[i][j]);
     while (hi >= 0) {
-        int lo = hi;
-        while (lo > 0) {
-            double s = fabs(h[lo - 1][lo - 1]) + fabs(h[lo][lo]);
-            if (s == 0.0) s = anorm;
-            if (fabs(h[lo][lo - 1]) <= DBL_EPSILON * s) {
-                h[lo][lo - 1] = 0.0;
-                break;
-            }
-            lo--;
-        }
+        const int lo = hi == 3   ? eig4_find_lo<3>(h, anorm)
+                       : hi == 2 ? eig4_find_lo<2>(h, anorm)
+                       : hi == 1 ? eig4_find_lo<1>(h, anorm)
+                                 : 0;
         if (lo == hi) {
-            er[hi] = h[hi][hi];
-            ei[hi] = 0.0;
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                if (q == hi) {
+                    er[q] = h[q][q];
+                    ei[q] = 0.0;
+                }
             hi -= 1;
             its = 0;
             continue;
         }
         if (lo == hi - 1) {
-            const double a = h[lo][lo], b = h[lo][hi], c = h[hi][lo], d = h[hi][hi];
-            const double half = 0.5 * (a - d);
-            const double disc = half * half + b * c;
-            if (disc >= 0.0) {
-                const double r = sqrt(disc);
-                const double zz = half + (half >= 0.0 ? r : -r);
-                er[lo] = d + zz;
-                er[hi] = (zz != 0.0) ? d - b * c / zz : d + zz;
-                ei[lo] = 0.0;
-                ei[hi] = 0.0;
-            } else {
-                const double r = sqrt(-disc);
-                er[lo] = d + half;
-                er[hi] = d + half;
-                ei[lo] = r;
-                ei[hi] = -r;
-            }
+            if (hi == 3)
+                eig4_block2<3>(h, er, ei);
+            else if (hi == 2)
+                eig4_block2<2>(h, er, ei);
+            else
+                eig4_block2<1>(h, er, ei);
             hi -= 2;
             its = 0;
             continue;
         }
         if (total >= 120) return -1;
-        double tr, det, x[3], v[3], beta;
-        if (its == 10 || its == 20) {
-            const double w = fabs(h[hi][hi - 1]) + fabs(h[hi - 1][hi - 2]);
-            tr = 1.5 * w;
-            det = w * w;
-        } else {
-            tr = h[hi - 1][hi - 1] + h[hi][hi];
-            det = h[hi - 1][hi - 1] * h[hi][hi] - h[hi - 1][hi] * h[hi][hi - 1];
-        }
-        x[0] = h[lo][lo] * h[lo][lo] + h[lo][lo + 1] * h[lo + 1][lo] -
-               tr * h[lo][lo] + det;
-        x[1] = h[lo + 1][lo] * (h[lo][lo] + h[lo + 1][lo + 1] - tr);
-        x[2] = h[lo + 1][lo] * h[lo + 2][lo + 1];
-        for (int k = lo; k <= hi - 2; k++) {
-            if (k > lo) {
-                x[0] = h[k][k - 1];
-                x[1] = h[k + 1][k - 1];
-                x[2] = h[k + 2][k - 1];
-            }
-            if (eig4_reflector(3, x, v, &beta)) {
-                const int rlast = (k + 3 <= hi) ? k + 3 : hi;
-                eig4_apply(h, 3, k, v, beta, lo, hi, (k > lo ? k - 1 : lo), rlast);
-                if (k > lo) {
-                    h[k + 1][k - 1] = 0.0;
-                    h[k + 2][k - 1] = 0.0;
-                }
-            }
-        }
-        x[0] = h[hi - 1][hi - 2];
-        x[1] = h[hi][hi - 2];
-        if (eig4_reflector(2, x, v, &beta)) {
-            eig4_apply(h, 2, hi - 1, v, beta, lo, hi, hi - 2, hi);
-            h[hi][hi - 2] = 0.0;
-        }
+        if (hi == 3 && lo == 0)
+            eig4_sweep<0, 3>(h, its);
+        else if (hi == 3)
+            eig4_sweep<1, 3>(h, its);
+        else
+            eig4_sweep<0, 2>(h, its);
         its++;
         total++;
     }
@@ -303,14 +373,17 @@ __device__ __forceinline__ void eig4_nullvec(const double a[16], double lr, doub
     }
 }
 
-__device__ int eig4(const double a[16], double er[4], double ei[4],
+__device__ __forceinline__ int eig4(const double a[16], double er[4], double ei[4],
                     double vr[16], double vi[16]) {
     double h[4][4];
+#pragma unroll
     for (int i = 0; i < 4; i++)
+#pragma unroll
         for (int j = 0; j < 4; j++) h[i][j] = a[4 * i + j];
     eig4_hessenberg(h);
     const int status = eig4_qr(h, er, ei);
     if (status < 0) {
+#pragma unroll
         for (int i = 0; i < 4; i++) {
             er[i] = h[i][i];
             ei[i] = 0.0;

@@ -391,11 +391,10 @@ struct LandauCell {
     int wrote;
 };
 
-// (128, 4): four blocks an SM. The null-vector elimination keeps its matrix
-// in registers (eig4_nullvec), the QR iteration's Hessenberg matrix stays in
-// local memory (its active block moves at run time); at 128 registers part
-// of the rest spills, which the extra warps hide (188 registers unbounded,
-// two blocks an SM, was slower)
+// (128, 4): four blocks an SM. Every index of the eigen-solver is static
+// (eig4.cuh), so unbounded it needs 194 registers and no local memory; at
+// 128 registers part of it spills, which the extra warps hide (447 against
+// 443 events/s at three blocks an SM and 437 at two)
 __global__ void __launch_bounds__(128, 4) k_landau(LandauArgs A, double *carry, int *wrote) {
     const int N = A.N;
     const size_t n = (size_t)N * N;
